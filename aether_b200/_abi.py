@@ -1,0 +1,126 @@
+"""ctypes mirror of the C ABI structures declared in include/aefdtd.h.
+
+Kept field-for-field identical to the header; tests check the struct sizes
+against the compiled library (aefdtd_abi_sizes)."""
+import ctypes as C
+
+ABI_VERSION = 1
+MAX_TERMS = 4
+
+MODE_NORMAL, MODE_CUSTOM = 0, 1
+FP64, FP32 = 0, 1
+EX, EY, EZ, HX, HY, HZ = range(6)
+NORMAL_X, NORMAL_XM, NORMAL_Y, NORMAL_YM, NORMAL_Z, NORMAL_ZM = range(6)
+XM, XP, YM, YP, ZM, ZP = range(6)
+OP_BLOCK, OP_LAYER, OP_SPHERE, OP_CYLINDER = range(4)
+
+STATUS = {
+    0: "OK", 1: "BAD_ARG", 2: "OOM", 3: "TIMEOUT", 4: "CUDA_ERROR",
+    5: "NOT_READY", 6: "NO_DEVICE",
+}
+
+
+class GridDesc(C.Structure):
+    _fields_ = [
+        ("abi_version", C.c_int32), ("mode", C.c_int32), ("precision", C.c_int32),
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+        ("nt", C.c_int32), ("tapering", C.c_int32),
+        ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
+        ("dt", C.c_double), ("time_mod", C.c_double),
+        ("pml", C.c_int32 * 6), ("pad", C.c_int32 * 6),
+        ("pml_kappa", C.c_double * 6), ("pml_sigma", C.c_double * 6),
+        ("pml_alpha", C.c_double * 6),
+        ("pml_m", C.c_int32), ("pml_ma", C.c_int32),
+        ("device", C.c_int32), ("dft_block", C.c_int32),
+    ]
+
+
+class MaterialDesc(C.Structure):
+    _fields_ = [
+        ("eps_inf", C.c_double),
+        ("n_debye", C.c_int32), ("n_drude", C.c_int32),
+        ("n_lorentz", C.c_int32), ("n_critpoint", C.c_int32),
+        ("debye", (C.c_double * 2) * MAX_TERMS),
+        ("drude", (C.c_double * 2) * MAX_TERMS),
+        ("lorentz", (C.c_double * 3) * MAX_TERMS),
+        ("critpoint", (C.c_double * 4) * MAX_TERMS),
+    ]
+
+
+class NormalDesc(C.Structure):
+    _fields_ = [
+        ("polarization", C.c_int32), ("nl", C.c_int32),
+        ("lambda_min", C.c_double), ("lambda_max", C.c_double),
+    ]
+
+
+class SensorDesc(C.Structure):
+    _fields_ = [
+        ("orientation", C.c_int32), ("box", C.c_int32 * 6), ("nl", C.c_int32),
+        ("lambda_min", C.c_double), ("lambda_max", C.c_double),
+    ]
+
+
+class SourceDesc(C.Structure):
+    _fields_ = [
+        ("orientation", C.c_int32), ("box", C.c_int32 * 6),
+        ("lambda_min", C.c_double), ("lambda_max", C.c_double),
+    ]
+
+
+class Dims(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+        ("xs_s", C.c_int32), ("xs_e", C.c_int32), ("ys_s", C.c_int32),
+        ("ys_e", C.c_int32), ("zs_s", C.c_int32), ("zs_e", C.c_int32),
+        ("n_materials", C.c_int32), ("step", C.c_int32),
+        ("dt", C.c_double), ("device_bytes", C.c_size_t),
+    ]
+
+
+class StructureOp(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("mat_index", C.c_int32), ("p", C.c_double * 8)]
+
+
+def material_desc(eps_inf=1.0, debye=(), drude=(), lorentz=(), critpoint=()):
+    """Builds a MaterialDesc from term lists (same parameter order as the
+    reference's add_debye/add_drude/add_lorentz/add_crit_point)."""
+    m = MaterialDesc()
+    m.eps_inf = float(eps_inf)
+    for name, terms, width in (("debye", debye, 2), ("drude", drude, 2),
+                               ("lorentz", lorentz, 3), ("critpoint", critpoint, 4)):
+        terms = list(terms)
+        if len(terms) > MAX_TERMS:
+            raise ValueError(f"at most {MAX_TERMS} {name} terms per material")
+        setattr(m, "n_" + name, len(terms))
+        arr = getattr(m, name)
+        for i, t in enumerate(terms):
+            if len(t) != width:
+                raise ValueError(f"{name} term needs {width} parameters")
+            for j, v in enumerate(t):
+                arr[i][j] = float(v)
+    return m
+
+
+def grid_desc(nx, ny, nz, dx, dy=None, dz=None, *, mode=MODE_NORMAL, precision=FP64,
+              nt=0, tapering=0, dt=0.0, time_mod=1.0, pml=(0,) * 6, pad=(0,) * 6,
+              kappa=(1.0,) * 6, sigma=(1.0,) * 6, alpha=(0.0,) * 6, pml_m=0, pml_ma=0,
+              device=0, dft_block=0):
+    g = GridDesc()
+    g.abi_version = ABI_VERSION
+    g.mode, g.precision = mode, precision
+    g.nx, g.ny, g.nz = nx, ny, nz
+    g.nt, g.tapering = nt, tapering
+    g.dx = dx
+    g.dy = dx if dy is None else dy
+    g.dz = dx if dz is None else dz
+    g.dt, g.time_mod = dt, time_mod
+    for i in range(6):
+        g.pml[i] = int(pml[i])
+        g.pad[i] = int(pad[i])
+        g.pml_kappa[i] = float(kappa[i])
+        g.pml_sigma[i] = float(sigma[i])
+        g.pml_alpha[i] = float(alpha[i])
+    g.pml_m, g.pml_ma = pml_m, pml_ma
+    g.device, g.dft_block = device, dft_block
+    return g

@@ -1,0 +1,263 @@
+/* aefdtd.h — C ABI of the B200-native 3D FDTD time-stepping core.
+ *
+ * The reference exposes this path as the C++ class `FDTD`
+ * (src/finite_differences/FDTD/core/fdtd_core.h:26-285) driven by the mode
+ * functions FDTD_normal_incidence (src/finite_differences/FDTD/modes/
+ * normal_incidence.cpp:161-607) and mode_default_fdtd
+ * (src/finite_differences/FDTD/modes/default_fdtd.cpp:24-210), with sensors
+ * (src/finite_differences/FDTD/core/sensors.h:87-171) and sources
+ * (src/finite_differences/FDTD/core/sources.h:219-240) holding the FDTD
+ * object by reference. The reference has no C ABI or FFI; every entry point
+ * below names the reference call it replaces.
+ *
+ * Conventions
+ *  - Plain pointers and sizes only. Every call returns aefdtd_status; no
+ *    exception crosses the ABI. aefdtd_last_error() gives a message.
+ *  - One owning host thread per handle. Device work of a handle is ordered
+ *    on that handle's own CUDA stream.
+ *  - Field arrays use the reference Grid3 layout: element (i,j,k) at
+ *    i + j*Nx + k*Nx*Ny (src/common/grid.h:862-868), over the TOTAL grid
+ *    (structure + pads + PML).
+ *  - Lengths in metres, times in seconds, angular frequencies in rad/s.
+ */
+#ifndef AEFDTD_H
+#define AEFDTD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AEFDTD_ABI_VERSION 1
+
+typedef enum aefdtd_status {
+    AEFDTD_OK = 0,
+    AEFDTD_BAD_ARG = 1,     /* invalid descriptor, index or size */
+    AEFDTD_OOM = 2,         /* device allocation or admission refused */
+    AEFDTD_TIMEOUT = 3,     /* a bounded device or host wait ran out */
+    AEFDTD_CUDA_ERROR = 4,  /* a CUDA runtime call failed */
+    AEFDTD_NOT_READY = 5,   /* call out of order (e.g. step before setup) */
+    AEFDTD_NO_DEVICE = 6    /* no CUDA device visible: there is no CPU path */
+} aefdtd_status;
+
+/* Driver orderings. NORMAL = "fdtd_normal" (normal_incidence.cpp:325-436):
+ * E, E-plane injection, H, H-plane injection, sensor feed, R/T plane sums.
+ * CUSTOM = "fdtd" (default_fdtd.cpp:156-204): E, source inject_E, H, sensor
+ * feed, source inject_H. The grid padding rules follow the FDTD constructor
+ * (fdtd_core.cpp:158-251) for modes "NORM" and "CUSTOM". */
+typedef enum aefdtd_mode { AEFDTD_MODE_NORMAL = 0, AEFDTD_MODE_CUSTOM = 1 } aefdtd_mode;
+
+/* FP64: bit-compatible operation order with the reference CPU core.
+ * FP32: fields, CPML and dispersive state in FP32; coefficients generated in
+ * FP64; DFT sensors accumulate in split precision; flux integration in FP64. */
+typedef enum aefdtd_precision { AEFDTD_FP64 = 0, AEFDTD_FP32 = 1 } aefdtd_precision;
+
+/* Field components, same order as EX_FIELD..HZ_FIELD (src/common/phys_constants.h:28-35). */
+enum { AEFDTD_EX = 0, AEFDTD_EY, AEFDTD_EZ, AEFDTD_HX, AEFDTD_HY, AEFDTD_HZ };
+
+/* Plane orientations, same meaning as NORMAL_X..NORMAL_ZM
+ * (src/common/enum_constants.h:30-35). */
+enum {
+    AEFDTD_NORMAL_X = 0, AEFDTD_NORMAL_XM, AEFDTD_NORMAL_Y, AEFDTD_NORMAL_YM,
+    AEFDTD_NORMAL_Z, AEFDTD_NORMAL_ZM
+};
+
+/* Faces in descriptor arrays: xm, xp, ym, yp, zm, zp. */
+enum { AEFDTD_XM = 0, AEFDTD_XP, AEFDTD_YM, AEFDTD_YP, AEFDTD_ZM, AEFDTD_ZP };
+
+#define AEFDTD_MAX_TERMS 4 /* per model family, per material */
+
+/* Grid and boundary description: the FDTD constructor arguments
+ * (fdtd_core.h:86-94) plus set_pml_* (fdtd_pml.cpp:457-497) and
+ * set_tapering (fdtd_utils.cpp:915-918). */
+typedef struct aefdtd_grid_desc {
+    int32_t abi_version;   /* = AEFDTD_ABI_VERSION */
+    int32_t mode;          /* aefdtd_mode */
+    int32_t precision;     /* aefdtd_precision */
+    int32_t nx, ny, nz;    /* structure cells, before pads and PML */
+    int32_t nt;            /* planned number of steps (sensor tapering) */
+    int32_t tapering;      /* Ntap: s-curve over the last Ntap steps */
+    double dx, dy, dz;
+    double dt;             /* time step; <= 0 means the mode drivers' rule
+                              min(D)/(sqrt(3)c)*0.99*time_mod (normal_incidence.cpp:191) */
+    double time_mod;
+    int32_t pml[6];        /* PML cells per face */
+    int32_t pad[6];        /* pad cells per face (raised to 5 on PML axes) */
+    double pml_kappa[6];   /* kappa_max per face */
+    double pml_sigma[6];   /* scale on 0.8(m+1)/(eta0*D) (fdtd_pml.cpp:445-447) */
+    double pml_alpha[6];   /* alpha_max per face, S/m */
+    int32_t pml_m;         /* sigma/kappa grading order; 0 -> 4 (fdtd_pml.cpp:309) */
+    int32_t pml_ma;        /* alpha grading order; 0 -> 2 (fdtd_pml.cpp:310) */
+    int32_t device;        /* CUDA device ordinal */
+    int32_t dft_block;     /* K: time steps buffered per DFT-sensor block; 0 -> 64 */
+} aefdtd_grid_desc;
+
+/* Material: Material (src/materials/material.h:33-93) restricted to the
+ * FDTD-compatible models: eps_inf plus Debye (ds, t0), Drude (wd, g),
+ * Lorentz (A, O, G) and critical-point (A, O, P, G) terms
+ * (src/materials/dielec_models.cpp:197-454). */
+typedef struct aefdtd_material_desc {
+    double eps_inf;
+    int32_t n_debye, n_drude, n_lorentz, n_critpoint;
+    double debye[AEFDTD_MAX_TERMS][2];
+    double drude[AEFDTD_MAX_TERMS][2];
+    double lorentz[AEFDTD_MAX_TERMS][3];
+    double critpoint[AEFDTD_MAX_TERMS][4];
+} aefdtd_material_desc;
+
+/* Normal-incidence excitation and R/T analysis (normal_incidence.cpp:228-249,
+ * 387-415, 442-570). polarization: 0 = "TE" (Ey), 1 = "TM" (Ex). */
+typedef struct aefdtd_normal_desc {
+    int32_t polarization;
+    int32_t nl;
+    double lambda_min, lambda_max;
+} aefdtd_normal_desc;
+
+/* Planar spectral Poynting sensor (Spect_Poynting, s_spec_power.cpp:32-119;
+ * generate_fdtd_sensor, sensors.cpp:402-417). box: x1,x2,y1,y2,z1,z2 in
+ * structure-grid cells, shifted by the structure origin and clamped as in
+ * Sensor::link (sensors.cpp:196-230). */
+typedef struct aefdtd_sensor_desc {
+    int32_t orientation;   /* AEFDTD_NORMAL_* */
+    int32_t box[6];
+    int32_t nl;
+    double lambda_min, lambda_max;
+} aefdtd_sensor_desc;
+
+/* Oscillator point/box source (Oscillator, sc_oscillator.cpp:34-84). */
+typedef struct aefdtd_source_desc {
+    int32_t orientation;   /* AEFDTD_NORMAL_*: X/XM -> Ex, Y/YM -> Ey, Z/ZM -> Ez */
+    int32_t box[6];        /* structure-grid cells, as for sensors */
+    double lambda_min, lambda_max;
+} aefdtd_source_desc;
+
+/* Total-grid geometry after construction (FDTD members Nx..zs_e, Dt). */
+typedef struct aefdtd_dims {
+    int32_t nx, ny, nz;
+    int32_t xs_s, xs_e, ys_s, ys_e, zs_s, zs_e;
+    int32_t n_materials;
+    int32_t step;          /* tstep */
+    double dt;
+    size_t device_bytes;   /* device memory held by the handle */
+} aefdtd_dims;
+
+typedef struct aefdtd_sim aefdtd_sim;
+
+/* ---- lifecycle -------------------------------------------------------- */
+
+/* Replaces FDTD::FDTD(...) (fdtd_core.cpp:158-285) + alloc_DEBH/bootstrap
+ * (fdtd_core.cpp:1073-1135) + set_pml_* + set_tapering. Allocates fields and
+ * CPML state on the device. */
+aefdtd_status aefdtd_create(const aefdtd_grid_desc *desc, aefdtd_sim **out);
+/* Replaces FDTD::~FDTD (fdtd_core.cpp:287-303). */
+aefdtd_status aefdtd_destroy(aefdtd_sim *sim);
+aefdtd_status aefdtd_get_dims(const aefdtd_sim *sim, aefdtd_dims *out);
+const char *aefdtd_last_error(const aefdtd_sim *sim);
+const char *aefdtd_status_string(aefdtd_status status);
+
+/* ---- structure and materials ----------------------------------------- */
+
+/* Replaces FDTD::set_matsgrid (fdtd_utils.cpp:572-796): copies a structure
+ * map of nx*ny*nz material indices (x fastest) into the grid and replicates
+ * edge slices into pads and PML. */
+aefdtd_status aefdtd_set_material_map(aefdtd_sim *sim, const uint32_t *map, size_t count);
+/* Replaces FDTD::set_material (fdtd_utils.cpp:810-820): FDTD_Material
+ * link_grid + set_base_mat (mats.cpp:394-464) with recursive-convolution
+ * coefficients generated in FP64 (mats_RC.cpp:126-184, mats_const.cpp:71-80). */
+aefdtd_status aefdtd_set_material(aefdtd_sim *sim, uint32_t index, const aefdtd_material_desc *mat);
+
+/* Structure discretisation on the device (Structure::discretize,
+ * structure.cpp:94-113, with Add_Block/Add_Layer/Add_Sphere/Add_Cylinder
+ * ::index, structure_primitives.cpp:34-39,266-284,323-339,490-499). Operation
+ * kinds and parameter layouts are listed with aefdtd_voxelize. */
+enum {
+    AEFDTD_OP_BLOCK = 0,    /* x1,x2,y1,y2,z1,z2 */
+    AEFDTD_OP_LAYER = 1,    /* axis(0/1/2 as double), z1, z2 */
+    AEFDTD_OP_SPHERE = 2,   /* x, y, z, r */
+    AEFDTD_OP_CYLINDER = 3  /* x1,y1,z1,x2,y2,z2,r */
+};
+typedef struct aefdtd_structure_op {
+    int32_t kind;
+    int32_t mat_index;
+    double p[8];
+} aefdtd_structure_op;
+/* Tags every cell corner (i*dx, j*dy, k*dz) of an nx*ny*nz structure grid
+ * with the material of the last operation containing it, else
+ * default_material; writes the map to host memory (out_map, nx*ny*nz) and,
+ * when sim is not NULL, also installs it as aefdtd_set_material_map does.
+ * periodic[3] and lengths l[3] reproduce Structure::index's periodic images
+ * (structure.cpp:228-258). */
+aefdtd_status aefdtd_voxelize(aefdtd_sim *sim, int32_t nx, int32_t ny, int32_t nz,
+                              double dx, double dy, double dz,
+                              const aefdtd_structure_op *ops, int32_t n_ops,
+                              int32_t default_material, const int32_t periodic[3],
+                              const double lengths[3], uint32_t *out_map, int32_t device);
+
+/* ---- excitation and sensors ------------------------------------------ */
+
+/* Sets up the normal-incidence drive: Gaussian plane-wave pulse (ChpIn::
+ * init_pulse, chpin.cpp:479-545) injected one-way at plane zs_e-1, the
+ * plane-sum R/T sensors and their spectrum (normal_incidence.cpp:228-262).
+ * Requires mode NORMAL and a material map with materials set. */
+aefdtd_status aefdtd_setup_normal(aefdtd_sim *sim, const aefdtd_normal_desc *nd);
+/* Replaces generate_fdtd_source(...Oscillator) + Source::link (sources.cpp:252-283). */
+aefdtd_status aefdtd_add_oscillator(aefdtd_sim *sim, const aefdtd_source_desc *src, int32_t *source_id);
+/* Replaces generate_fdtd_sensor(...PLANAR_SPECTRAL_POYNTING) (sensors.cpp:402-417). */
+aefdtd_status aefdtd_add_planar_sensor(aefdtd_sim *sim, const aefdtd_sensor_desc *sd, int32_t *sensor_id);
+
+/* ---- time stepping ---------------------------------------------------- */
+
+/* Advances n full steps in the mode's driver order (see aefdtd_mode): the
+ * loop bodies of normal_incidence.cpp:325-436 / default_fdtd.cpp:156-204,
+ * with FDTD::update_E/update_H (fdtd_core.cpp:1163-1335) as fused device
+ * kernels. Launches are asynchronous on the handle's stream; the call
+ * returns once they are queued (aefdtd_synchronize waits). */
+aefdtd_status aefdtd_step(aefdtd_sim *sim, int32_t n);
+aefdtd_status aefdtd_synchronize(aefdtd_sim *sim);
+/* Zeroes fields, CPML and dispersive state and all sensor accumulators and
+ * sets tstep to 0 (FDTD::reset_fields, fdtd_utils.cpp:855-881). */
+aefdtd_status aefdtd_reset(aefdtd_sim *sim);
+
+/* ---- results ---------------------------------------------------------- */
+
+/* Copies one field component of the total grid (Nx*Ny*Nz values) into host
+ * memory as double regardless of precision (replaces reading FDTD::Ex..Hz). */
+aefdtd_status aefdtd_get_field(aefdtd_sim *sim, int32_t component, double *out, size_t count);
+/* Overwrites one field component from host memory (checkpoint restore). */
+aefdtd_status aefdtd_set_field(aefdtd_sim *sim, int32_t component, const double *in, size_t count);
+/* Device pointer of a field component (precision's element type) for
+ * zero-copy consumers on the same device; valid until aefdtd_destroy. */
+aefdtd_status aefdtd_field_device_ptr(aefdtd_sim *sim, int32_t component, void **ptr);
+
+/* Normal-incidence plane sums per completed step, 12 series of `steps`
+ * values in this order: BRx BRy BRz Rx Ry Rz BTx BTy BTz Tx Ty Tz
+ * (normal_incidence.cpp:255-259,387-415). */
+aefdtd_status aefdtd_get_plane_sums(aefdtd_sim *sim, double *out, int32_t steps);
+/* Normal-incidence spectra over nl wavelengths, 15 columns per wavelength:
+ * lambda, r, t  (spectdata_norm, normal_incidence.cpp:510-522), then
+ * |rx| arg(rx) |rx|^2 |ry| arg(ry) |ry|^2 |tx| arg(tx) Tx |ty| arg(ty) Ty
+ * (spectdata_norm2, normal_incidence.cpp:534-567). */
+aefdtd_status aefdtd_get_normal_spectra(aefdtd_sim *sim, double *out, int32_t nl);
+/* Flux spectrum of a planar sensor: rsp_result per wavelength
+ * (Spect_Poynting::treat, s_spec_power.cpp:44-119), FP64. */
+aefdtd_status aefdtd_get_sensor_flux(aefdtd_sim *sim, int32_t sensor_id, double *out, int32_t nl);
+/* Raw DFT accumulators of a planar sensor: 6 components (Ex..Hz) x span1 x
+ * span2 x nl complex values as interleaved double (re, im), i fastest. */
+aefdtd_status aefdtd_get_sensor_dft(aefdtd_sim *sim, int32_t sensor_id, double *out, size_t count);
+aefdtd_status aefdtd_get_sensor_shape(aefdtd_sim *sim, int32_t sensor_id, int32_t *span1, int32_t *span2, int32_t *nl);
+
+/* Per-launch device timings of the most recent aefdtd_step call, measured
+ * with CUDA events on the handle's stream: milliseconds spent in the E
+ * half-step kernels, the H half-step kernels and the sensor kernels. */
+aefdtd_status aefdtd_get_timings(aefdtd_sim *sim, double *e_ms, double *h_ms, double *sensor_ms);
+aefdtd_status aefdtd_enable_timing(aefdtd_sim *sim, int32_t enable);
+/* Number of device kernel launches issued by this handle since creation. */
+aefdtd_status aefdtd_get_launch_count(aefdtd_sim *sim, uint64_t *launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AEFDTD_H */

@@ -1,0 +1,309 @@
+/* Reference-core driver for the oracle build — TEST INFRASTRUCTURE ONLY.
+ *
+ * Links against the reference's own FDTD core sources, compiled unmodified
+ * from the reference tree by oracle/Makefile into oracle/_ref/. This file is
+ * project-written: it replays the time loops of the two reference mode
+ * drivers without Lua (Lua 5.4 is not installed here), building the FDTD,
+ * Material, Spect_Poynting and Oscillator objects directly:
+ *   - aeref_run with mode NORMAL replays FDTD_normal_incidence
+ *     (src/finite_differences/FDTD/modes/normal_incidence.cpp:161-570,
+ *     minus PNG previews and result files);
+ *   - mode CUSTOM replays mode_default_fdtd
+ *     (src/finite_differences/FDTD/modes/default_fdtd.cpp:24-210).
+ * Only tests/, bench.py's reference arm and the golden-fixture script call it;
+ * the product library never links or loads it.
+ */
+#include <fdtd_core.h>
+#include <sensors.h>
+#include <sources.h>
+#include <material.h>
+
+#include <chrono>
+#include <cmath>
+#include <complex>
+#include <fstream>
+#include <iostream>
+#include <sstream>
+#include <vector>
+
+#include "../include/aefdtd.h"
+
+extern const Imdouble Im;
+
+namespace {
+
+int ref_orientation(int o) {
+    static const int tbl[6] = {NORMAL_X, NORMAL_XM, NORMAL_Y, NORMAL_YM, NORMAL_Z, NORMAL_ZM};
+    return (o >= 0 && o < 6) ? tbl[o] : NORMAL_UNDEF;
+}
+
+Material make_material(const aefdtd_material_desc &d) {
+    Material m;
+    m.eps_inf = d.eps_inf;
+    for (int i = 0; i < d.n_debye; i++) { DebyeModel x; x.set(d.debye[i][0], d.debye[i][1]); m.debye.push_back(x); }
+    for (int i = 0; i < d.n_drude; i++) { DrudeModel x; x.set(d.drude[i][0], d.drude[i][1]); m.drude.push_back(x); }
+    for (int i = 0; i < d.n_lorentz; i++) { LorentzModel x; x.set(d.lorentz[i][0], d.lorentz[i][1], d.lorentz[i][2]); m.lorentz.push_back(x); }
+    for (int i = 0; i < d.n_critpoint; i++) {
+        CritpointModel x; x.set(d.critpoint[i][0], d.critpoint[i][1], d.critpoint[i][2], d.critpoint[i][3]);
+        m.critpoint.push_back(x);
+    }
+    return m;
+}
+
+struct CoutSilencer {
+    std::streambuf *old;
+    std::ostringstream sink;
+    CoutSilencer() : old(std::cout.rdbuf(sink.rdbuf())) {}
+    ~CoutSilencer() { std::cout.rdbuf(old); }
+};
+
+void copy_fields(FDTD const &f, double *out) {
+    size_t n = size_t(f.Nx) * f.Ny * f.Nz;
+    Grid3<double> const *g[6] = {&f.Ex, &f.Ey, &f.Ez, &f.Hx, &f.Hy, &f.Hz};
+    for (int c = 0; c < 6; c++)
+        for (int k = 0; k < f.Nz; k++)
+            for (int j = 0; j < f.Ny; j++)
+                for (int i = 0; i < f.Nx; i++)
+                    out[c * n + i + size_t(j) * f.Nx + size_t(k) * f.Nx * f.Ny] = (*g[c])(i, j, k);
+}
+
+}  // namespace
+
+extern "C" {
+
+/* Runs one simulation through the reference core.
+ *   map: nx*ny*nz structure material indices, x fastest.
+ *   nsteps: time-loop count (the reference's Nt for post-processing).
+ * Outputs (each may be NULL):
+ *   fields_out: 6 * Ntot doubles, Ex..Hz on the total grid after the loop;
+ *   plane_sums_out: 12 * nsteps (normal mode), order of aefdtd_get_plane_sums;
+ *   spectra_out: 15 * nl (normal mode), layout of aefdtd_get_normal_spectra;
+ *   flux_out: concatenated rsp_result of every sensor;
+ *   dims_out: 10 ints Nx Ny Nz xs_s xs_e ys_s ys_e zs_s zs_e Nmat;
+ *   loop_seconds: wall time of the time loop alone.
+ * Returns 0 on success, nonzero on a bad argument. */
+int aeref_run(const aefdtd_grid_desc *g, const uint32_t *map,
+              const aefdtd_material_desc *mats, int32_t nmat,
+              const aefdtd_normal_desc *nd,
+              const aefdtd_source_desc *srcs, int32_t nsrc,
+              const aefdtd_sensor_desc *sens, int32_t nsens,
+              int32_t nsteps, int32_t quiet,
+              double *fields_out, double *plane_sums_out, double *spectra_out,
+              double *flux_out, int32_t *dims_out, double *loop_seconds) {
+    if (!g || !map || !mats || nmat <= 0 || nsteps < 0) return 1;
+    if (g->mode == AEFDTD_MODE_NORMAL && !nd) return 2;
+    CoutSilencer *silence = quiet ? new CoutSilencer() : nullptr;
+
+    int Nx = g->nx, Ny = g->ny, Nz = g->nz, Nt = g->nt > 0 ? g->nt : nsteps;
+    double Dx = g->dx, Dy = g->dy, Dz = g->dz;
+
+    Grid3<unsigned int> matsgrid(Nx, Ny, Nz, 0);
+    for (int k = 0; k < Nz; k++)
+        for (int j = 0; j < Ny; j++)
+            for (int i = 0; i < Nx; i++)
+                matsgrid(i, j, k) = map[i + size_t(j) * Nx + size_t(k) * Nx * Ny];
+
+    double Dt = g->dt;
+    if (Dt <= 0) Dt = std::min(std::min(Dx, Dy), Dz) / (std::sqrt(3.0) * c_light) * 0.99 * g->time_mod;
+
+    FDTD *fp = nullptr;
+    if (g->mode == AEFDTD_MODE_NORMAL) {
+        // normal_incidence.cpp:188-200
+        int pad_zm = std::max(5, g->pad[AEFDTD_ZM]);
+        int pad_zp = std::max(5, g->pad[AEFDTD_ZP]);
+        fp = new FDTD(Nx, Ny, Nz, Nt, Dx, Dy, Dz, Dt, "NORM",
+                      0, 0, 0, 0, g->pml[AEFDTD_ZM], g->pml[AEFDTD_ZP],
+                      0, 0, 0, 0, pad_zm, pad_zp);
+        fp->set_pml_zm(g->pml_kappa[AEFDTD_ZM], g->pml_sigma[AEFDTD_ZM], g->pml_alpha[AEFDTD_ZM]);
+        fp->set_pml_zp(g->pml_kappa[AEFDTD_ZP], g->pml_sigma[AEFDTD_ZP], g->pml_alpha[AEFDTD_ZP]);
+    } else {
+        // default_fdtd.cpp:47-62
+        fp = new FDTD(Nx, Ny, Nz, Nt, Dx, Dy, Dz, Dt, "CUSTOM",
+                      g->pml[0], g->pml[1], g->pml[2], g->pml[3], g->pml[4], g->pml[5],
+                      g->pad[0], g->pad[1], g->pad[2], g->pad[3], g->pad[4], g->pad[5]);
+        fp->set_pml_xm(g->pml_kappa[0], g->pml_sigma[0], g->pml_alpha[0]);
+        fp->set_pml_xp(g->pml_kappa[1], g->pml_sigma[1], g->pml_alpha[1]);
+        fp->set_pml_ym(g->pml_kappa[2], g->pml_sigma[2], g->pml_alpha[2]);
+        fp->set_pml_yp(g->pml_kappa[3], g->pml_sigma[3], g->pml_alpha[3]);
+        fp->set_pml_zm(g->pml_kappa[4], g->pml_sigma[4], g->pml_alpha[4]);
+        fp->set_pml_zp(g->pml_kappa[5], g->pml_sigma[5], g->pml_alpha[5]);
+    }
+    FDTD &fdtd = *fp;
+    fdtd.set_tapering(g->tapering);
+    fdtd.set_matsgrid(matsgrid);
+    for (int m = 0; m < nmat; m++) fdtd.set_material(m, make_material(mats[m]));
+    fdtd.bootstrap();
+
+    Nx = fdtd.Nx; Ny = fdtd.Ny; Nz = fdtd.Nz;
+    if (dims_out) {
+        int d[10] = {fdtd.Nx, fdtd.Ny, fdtd.Nz, fdtd.xs_s, fdtd.xs_e, fdtd.ys_s, fdtd.ys_e,
+                     fdtd.zs_s, fdtd.zs_e, int(fdtd.Nmat)};
+        for (int i = 0; i < 10; i++) dims_out[i] = d[i];
+    }
+
+    std::vector<Sensor *> sensors;
+    for (int s = 0; s < nsens; s++) {
+        Spect_Poynting *sp = new Spect_Poynting(ref_orientation(sens[s].orientation),
+                                                sens[s].box[0], sens[s].box[1], sens[s].box[2],
+                                                sens[s].box[3], sens[s].box[4], sens[s].box[5]);
+        sp->set_spectrum(sens[s].nl, sens[s].lambda_min, sens[s].lambda_max);
+        sp->name = "aeref_sensor";
+        sp->link(fdtd, std::filesystem::path("."));
+        sp->set_silent(true);
+        sensors.push_back(sp);
+    }
+    std::vector<Source *> sources;
+    if (g->mode == AEFDTD_MODE_CUSTOM) {
+        for (int s = 0; s < nsrc; s++) {
+            Oscillator *o = new Oscillator(ref_orientation(srcs[s].orientation),
+                                           srcs[s].box[0], srcs[s].box[1], srcs[s].box[2],
+                                           srcs[s].box[3], srcs[s].box[4], srcs[s].box[5]);
+            o->set_spectrum(srcs[s].lambda_min, srcs[s].lambda_max);
+            o->link(fdtd);
+            sources.push_back(o);
+        }
+    }
+
+    auto t0 = std::chrono::steady_clock::now();
+
+    if (g->mode == AEFDTD_MODE_NORMAL) {
+        int zs_s = fdtd.zs_s, zs_e = fdtd.zs_e;
+        int Nl = nd->nl;
+        std::vector<double> Lambda(Nl), w(Nl);
+        for (int l = 0; l < Nl; l++) Lambda[l] = nd->lambda_min + (nd->lambda_max - nd->lambda_min) * l / (Nl - 1.0);
+        for (int l = 0; l < Nl; l++) w[l] = 2.0 * Pi * c_light / Lambda[l];
+        double pol = nd->polarization == 1 ? 90 : 0;
+        double eps_sub = fdtd.mats[fdtd.matsgrid(0, 0, zs_s)].ei;
+        double eps_sup = fdtd.mats[fdtd.matsgrid(0, 0, zs_e)].ei;
+        double index_sub = std::sqrt(eps_sub);
+        double index_sup = std::sqrt(eps_sup);
+        ChpIn inj_chp;
+        inj_chp.init_pulse(nd->lambda_min, nd->lambda_max, 0, pol, 0, 0, 0, (zs_e - 1) * Dz, index_sup);
+
+        int NtR = nsteps;
+        std::vector<double> S[12];
+        for (auto &v : S) v.assign(NtR, 0.0);
+        double tb = 0;
+        for (int t = 0; t < NtR; t++) {
+            fdtd.update_E();
+            tb = t * Dt;
+            double inj_Hx = inj_chp.Hx(0, 0, (zs_e - 1 + 0.5) * Dz, tb);
+            double inj_Hy = inj_chp.Hy(0, 0, (zs_e - 1 + 0.5) * Dz, tb);
+            for (int j = 0; j < Ny; j++)
+                for (int i = 0; i < Nx; i++) {
+                    fdtd.Ex(i, j, zs_e - 1) -= fdtd.dtdez * inj_Hy / eps_sup;
+                    fdtd.Ey(i, j, zs_e - 1) += fdtd.dtdez * inj_Hx / eps_sup;
+                }
+            fdtd.update_H();
+            tb = (t + 0.5) * Dt;
+            double inj_Ex = inj_chp.Ex(0, 0, (zs_e - 1) * Dz, tb);
+            double inj_Ey = inj_chp.Ey(0, 0, (zs_e - 1) * Dz, tb);
+            for (int j = 0; j < Ny; j++)
+                for (int i = 0; i < Nx; i++) {
+                    fdtd.Hx(i, j, zs_e - 1) += fdtd.dtdmz * inj_Ey;
+                    fdtd.Hy(i, j, zs_e - 1) -= fdtd.dtdmz * inj_Ex;
+                }
+            for (auto *s : sensors) s->feed(fdtd);
+
+            tb = (t + 0.5) * Dt;
+            double Dx2 = Dx / 2.0, Dy2 = Dy / 2.0, Dz2 = Dz / 2.0;
+            double tapering = 1.0;
+            if (t >= Nt - g->tapering) tapering = s_curve(t, Nt - 1.0, Nt - g->tapering);
+            for (int j = 0; j < Ny; j++) {
+                double y = j * Dy;
+                for (int i = 0; i < Nx; i++) {
+                    double x = i * Dx;
+                    double z = (zs_e - 2) * Dz;
+                    S[0][t] += inj_chp.Ex(x + Dx2, y, z, tb) * tapering;
+                    S[1][t] += inj_chp.Ey(x, y + Dy2, z, tb) * tapering;
+                    S[2][t] += inj_chp.Ez(x, y, z + Dz2, tb) * tapering;
+                    S[3][t] += (fdtd.Ex(i, j, zs_e - 2) - inj_chp.Ex(x + Dx2, y, z, tb)) * tapering;
+                    S[4][t] += (fdtd.Ey(i, j, zs_e - 2) - inj_chp.Ey(x, y + Dy2, z, tb)) * tapering;
+                    S[5][t] += (fdtd.Ez(i, j, zs_e - 2) - inj_chp.Ez(x, y, z + Dz2, tb)) * tapering;
+                    z = (zs_s)*Dz;
+                    S[6][t] += inj_chp.Ex(x + Dx2, y, z, tb) * tapering;
+                    S[7][t] += inj_chp.Ey(x, y + Dy2, z, tb) * tapering;
+                    S[8][t] += inj_chp.Ez(x, y, z + Dz2, tb) * tapering;
+                    S[9][t] += fdtd.Ex(i, j, zs_s) * tapering;
+                    S[10][t] += fdtd.Ey(i, j, zs_s) * tapering;
+                    S[11][t] += fdtd.Ez(i, j, zs_s) * tapering;
+                }
+            }
+        }
+        if (loop_seconds) loop_seconds[0] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (plane_sums_out)
+            for (int c = 0; c < 12; c++)
+                for (int t = 0; t < NtR; t++) plane_sums_out[size_t(c) * NtR + t] = S[c][t];
+
+        if (spectra_out) {
+            // normal_incidence.cpp:442-570 with Nt = number of steps run.
+            int NtP = NtR;
+            double hsup, hsub, hstruc;
+            fdtd.find_slab(zs_s, zs_e - 1, hsub, hstruc, hsup);
+            hsup -= Dz / 2.0;
+            hsub -= Dz / 2.0;
+            for (int l = 0; l < Nl; l++) {
+                Imdouble ref1x = 0, ref1y = 0, ref1z = 0, ref2x = 0, ref2y = 0, ref2z = 0;
+                Imdouble trans1x = 0, trans1y = 0, trans1z = 0, trans2x = 0, trans2y = 0, trans2z = 0;
+                double k0 = -w[l] / c_light;
+                double k1 = k0 * index_sup;
+                double k3 = k0 * index_sub;
+                Imdouble tmp_sup = std::exp(2.0 * k1 * hsup * Im);
+                Imdouble tmp_sub = std::exp((k3 * hsub - k0 * (hstruc + hsub)) * Im);
+                for (int t = 0; t < NtP; t++) {
+                    Imdouble tmp1 = std::exp(t * Dt * w[l] * Im) / (NtP - 1.0);
+                    Imdouble tmp2 = tmp1 * tmp_sup;
+                    Imdouble tmp3 = tmp1 * tmp_sub;
+                    ref1x += S[0][t] * tmp1; ref1y += S[1][t] * tmp1; ref1z += S[2][t] * tmp1;
+                    ref2x += S[3][t] * tmp2; ref2y += S[4][t] * tmp2; ref2z += S[5][t] * tmp2;
+                    trans1x += S[6][t] * tmp1; trans1y += S[7][t] * tmp1; trans1z += S[8][t] * tmp1;
+                    trans2x += S[9][t] * tmp3; trans2y += S[10][t] * tmp3; trans2z += S[11][t] * tmp3;
+                }
+                double *o = spectra_out + size_t(l) * 15;
+                o[0] = Lambda[l];
+                double a = std::sqrt(std::norm(ref2x) + std::norm(ref2y) + std::norm(ref2z));
+                double b = std::sqrt(std::norm(ref1x) + std::norm(ref1y) + std::norm(ref1z));
+                o[1] = a / b;
+                a = std::sqrt(std::norm(trans2x) + std::norm(trans2y) + std::norm(trans2z));
+                b = std::sqrt(std::norm(trans1x) + std::norm(trans1y) + std::norm(trans1z));
+                o[2] = a / b;
+                Imdouble ref0 = ref1y, trans0 = trans1y;
+                if (nd->polarization == 1) { ref0 = ref1x; trans0 = trans1x; }
+                Imdouble refx = ref2x / ref0, refy = ref2y / ref0;
+                Imdouble transx = trans2x / trans0, transy = trans2y / trans0;
+                o[3] = std::abs(refx); o[4] = std::arg(refx); o[5] = std::norm(refx);
+                o[6] = std::abs(refy); o[7] = std::arg(refy); o[8] = std::norm(refy);
+                o[9] = std::abs(transx); o[10] = std::arg(transx); o[11] = std::norm(transx) * index_sub / index_sup;
+                o[12] = std::abs(transy); o[13] = std::arg(transy); o[14] = std::norm(transy) * index_sub / index_sup;
+            }
+        }
+    } else {
+        for (int t = 0; t < nsteps; t++) {
+            fdtd.update_E();
+            for (auto *s : sources) s->inject_E(fdtd);
+            fdtd.update_H();
+            for (auto *s : sensors) s->feed(fdtd);
+            for (auto *s : sources) s->inject_H(fdtd);
+        }
+        if (loop_seconds) loop_seconds[0] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+
+    if (fields_out) copy_fields(fdtd, fields_out);
+    size_t off = 0;
+    for (size_t s = 0; s < sensors.size(); s++) {
+        sensors[s]->treat();
+        if (flux_out)
+            for (int l = 0; l < sensors[s]->Nl; l++) flux_out[off + l] = sensors[s]->rsp_result[l];
+        off += sensors[s]->Nl;
+    }
+    for (auto *s : sensors) delete s;
+    for (auto *s : sources) delete s;
+    delete fp;
+    delete silence;
+    return 0;
+}
+
+/* Number of worker threads the reference core uses per FDTD object. */
+int aeref_threads(void) { return max_threads_number(); }
+
+}  // extern "C"

@@ -1,0 +1,92 @@
+"""Loads the oracle libraries (test infrastructure) and runs a Scene through
+them.
+
+  port: oracle/liboracle_fdtd.so — the CPU restatement (oracle/fdtd_oracle.cpp)
+  ref:  oracle/_ref/libaeref.so — the reference's own FDTD core compiled from
+        source by oracle/Makefile (only where it was built)
+Both export the same entry point signature, so results are directly
+comparable."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from aether_b200 import _abi as A
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PORT_PATH = os.path.join(ROOT, "oracle", "liboracle_fdtd.so")
+REF_PATH = os.path.join(ROOT, "oracle", "_ref", "libaeref.so")
+
+_P = C.POINTER
+_libs = {}
+
+
+def _bind(path, sym):
+    lib = C.CDLL(path)
+    fn = getattr(lib, sym)
+    fn.argtypes = [_P(A.GridDesc), _P(C.c_uint32), _P(A.MaterialDesc), C.c_int32, _P(A.NormalDesc),
+                   _P(A.SourceDesc), C.c_int32, _P(A.SensorDesc), C.c_int32, C.c_int32, C.c_int32,
+                   _P(C.c_double), _P(C.c_double), _P(C.c_double), _P(C.c_double), _P(C.c_int32),
+                   _P(C.c_double)]
+    fn.restype = C.c_int
+    return lib, fn
+
+
+def available(which: str) -> bool:
+    return os.path.exists(PORT_PATH if which == "port" else REF_PATH)
+
+
+def get(which: str):
+    if which not in _libs:
+        if which == "port":
+            _libs[which] = _bind(PORT_PATH, "aeoracle_run")
+        elif which == "ref":
+            _libs[which] = _bind(REF_PATH, "aeref_run")
+        else:
+            raise ValueError(which)
+    return _libs[which][1]
+
+
+def _dptr(a):
+    return None if a is None else a.ctypes.data_as(_P(C.c_double))
+
+
+def run(scene, which="port", nsteps=None, want_fields=True):
+    """Runs the scene for nsteps (default scene.nsteps) and returns a dict with
+    fields (6, nz, ny, nx), plane_sums (12, nsteps), spectra (nl, 15), flux
+    (list per sensor), dims (10,), seconds."""
+    fn = get(which)
+    nsteps = scene.nsteps if nsteps is None else nsteps
+    nx, ny, nz = scene.total_dims()
+    ntot = nx * ny * nz
+    fields = np.zeros(6 * ntot) if want_fields else None
+    ps = np.zeros(12 * max(nsteps, 1)) if scene.normal is not None else None
+    nl = scene.normal.nl if scene.normal is not None else 0
+    spectra = np.zeros(15 * nl) if scene.normal is not None else None
+    nflux = sum(s.nl for s in scene.sensors)
+    flux = np.zeros(max(nflux, 1))
+    dims = (C.c_int32 * 10)()
+    secs = C.c_double(0)
+    mats = (A.MaterialDesc * len(scene.materials))(*scene.materials)
+    sens = (A.SensorDesc * max(len(scene.sensors), 1))(*scene.sensors) if scene.sensors else None
+    srcs = (A.SourceDesc * max(len(scene.sources), 1))(*scene.sources) if scene.sources else None
+    rc = fn(C.byref(scene.grid), scene.map.ctypes.data_as(_P(C.c_uint32)), mats, len(scene.materials),
+            C.byref(scene.normal) if scene.normal is not None else None,
+            srcs, len(scene.sources), sens, len(scene.sensors), nsteps, 1,
+            _dptr(fields), _dptr(ps), _dptr(spectra), _dptr(flux), dims, C.byref(secs))
+    if rc != 0:
+        raise RuntimeError(f"{which} oracle run failed with code {rc}")
+    d = list(dims)
+    assert (d[0], d[1], d[2]) == (nx, ny, nz), (d, (nx, ny, nz))
+    out = {"dims": np.array(d), "seconds": secs.value}
+    out["fields"] = fields.reshape(6, nz, ny, nx) if want_fields else None
+    out["plane_sums"] = ps.reshape(12, nsteps) if ps is not None else None
+    out["spectra"] = spectra.reshape(nl, 15) if spectra is not None else None
+    fl, off = [], 0
+    for s in scene.sensors:
+        fl.append(flux[off:off + s.nl].copy())
+        off += s.nl
+    out["flux"] = fl
+    return out
