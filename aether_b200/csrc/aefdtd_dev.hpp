@@ -1,0 +1,126 @@
+// aefdtd_dev.hpp — data layouts shared by the host runtime and the kernels.
+//
+// HBM layout of one simulation (total grid Nx x Ny x Nz, x fastest, the
+// reference Grid3 order, src/common/grid.h:862-868):
+//   Ex Ey Ez Hx Hy Hz    : Nx*Ny*Nz reals each (FP64 or FP32)
+//   mat                  : Nx*Ny*Nz material ids (uint8, or uint16 above 256 materials)
+//   CPML psi             : slab-compact arrays as in FDTD::allocate_pml
+//                          (src/finite_differences/FDTD/core/fdtd_pml.cpp:26-86):
+//                          x: (pml_xm+pml_xp) x Ny x Nz, y: Nx x (pml_ym+pml_yp) x Nz,
+//                          z: Nx x Ny x (pml_zm+pml_zp); 4 arrays per axis
+//   dispersive psi       : per dispersive material, its bounding box x 3*Np complex
+//                          values, component-major (like FDTD_Material::m_Psi_c,
+//                          src/finite_differences/FDTD/core/mats.cpp:394-496)
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <vector_types.h>
+
+namespace aefdtd {
+
+constexpr int kMaxPoles = 16;  // 4 terms x 4 model families
+
+template <typename T> struct Cplx { T re, im; };
+
+// Per-material update coefficients: FDTD_Material C1, C2x, C2y, C2z, C3, C4
+// (src/finite_differences/FDTD/core/fdtd_material.h:46).
+template <typename T> struct MatCoef {
+    T C1, C2x, C2y, C2z, C3, C4;
+};
+
+// Dispersive (recursive-convolution) material record, one per material id.
+// np == 0 for constant materials.
+struct DispInfo {
+    int np;
+    int pole_off;            // first pole in the pole tables
+    int x1, y1, z1, xs, ys, zs;
+    long long psi_off;       // complex-element offset of this material's psi block
+    long long box;           // xs*ys*zs
+};
+
+// Parameters of one fused half-step launch. Pointers are device pointers.
+template <typename T, typename Tid> struct StepArgs {
+    int Nx, Ny, Nz;
+    long long NxNy;
+    T *Ex, *Ey, *Ez, *Hx, *Hy, *Hz;
+    const Tid *mat;
+    const MatCoef<T> *coef;
+    const DispInfo *disp;           // nullptr when no material is dispersive
+    const Cplx<T> *crec;            // FP64: Crec; FP32: Crec - 1
+    const Cplx<T> *dchi;
+    Cplx<T> *psi;
+    // CPML (fdtd_pml.cpp): thicknesses and per-index coefficient tables
+    int pml_xm, pml_xp, pml_ym, pml_yp, pml_zm, pml_zp;
+    bool px, py, pz;                // axis has any PML
+    const T *ikx, *iky, *ikz;       // 1/kappa for the Yee update (reference selection rules)
+    const T *bx, *by, *bz;          // FP64: b; FP32: b - 1
+    const T *cx, *cy, *cz;          // c / D
+    T *psi_x0, *psi_x1;             // E: PsiEyx, PsiEzx  H: PsiHyx, PsiHzx
+    T *psi_y0, *psi_y1;             // E: PsiExy, PsiEzy  H: PsiHxy, PsiHzy
+    T *psi_z0, *psi_z1;             // E: PsiExz, PsiEyz  H: PsiHxz, PsiHyz
+    // H-side constants
+    T dtdmx, dtdmy, dtdmz, dtm;
+    // plane injection (normal mode): subtract/add on plane kinj, or kinj < 0
+    int kinj;
+    T inj_a, inj_b;                 // E: a=(dtdez*Hy_inc)/eps_sup subtracted from Ex, b added to Ey
+                                    // H: a=dtdmz*Ey_inc added to Hx, b=dtdmz*Ex_inc subtracted from Hy
+    // box sources (custom mode, E only): up to kMaxSrc boxes
+    int nsrc;
+    int src_box[4][6];
+    int src_comp[4];
+    T src_val[4];
+    int kchunk;                     // z planes per thread
+};
+
+// ---- sensor-path launch arguments (kernels in sensors.cuh)
+
+struct PulseDev {
+    double k, omega, kx, ky, kz, n_ind, dz, C1;
+    double Ex0, Ey0, Ez0;
+};
+
+template <typename T> struct PlaneSumArgs {
+    int Nx, Ny;
+    long long NxNy;
+    const T *Ex, *Ey, *Ez;
+    int kr, kt;              // zs_e-2, zs_s
+    double Dx, Dy, Dz, tb, tapering;
+    PulseDev P;
+    double *out;             // 12 sums of this step
+};
+
+template <typename T> struct GatherArgs {
+    int Nx, Ny, Nz;
+    long long NxNy;
+    const T *Ex, *Ey, *Ez, *Hx, *Hy, *Hz;
+    int type;                // 0/1: x-normal, 2/3: y-normal, 4/5: z-normal
+    int x1, y1, z1, span1, span2;
+    T *S;                    // slot base: [6][span1*span2]
+};
+
+struct PhasorArgs {
+    int nk, nl, step0, Nt, Ntap;
+    double Dt;
+    const double *w;         // angular frequencies, nl
+    double2 *WE, *WH;        // [nk][nl]
+};
+
+template <typename T> struct AccumArgs {
+    int P, nl, nk;
+    const T *S;              // [K][6][P]
+    const double2 *WE, *WH;  // [nk][nl]
+    double2 *acc;            // [6][nl][P]
+};
+
+struct FluxArgs {
+    int P, nl, type;
+    double area_factor;      // Dy*Dz, Dx*Dz or Dx*Dy
+    const double2 *acc;      // [6][nl][P]
+    double *out;             // nl
+};
+
+constexpr int kDftFTile = 8;
+constexpr int kDftKTile = 16;
+
+}  // namespace aefdtd

@@ -1,0 +1,1166 @@
+// runtime.cpp — host runtime of the FDTD core behind the C ABI (include/aefdtd.h).
+//
+// Owns the device state of one simulation, generates every coefficient in
+// FP64 on the host with the reference's formulas and operation order, and
+// issues the fused kernels on the handle's stream in the mode driver's order.
+// There is no CPU compute path: without a CUDA device every call that would
+// touch the device returns AEFDTD_NO_DEVICE.
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <numbers>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/aefdtd.h"
+#include "kernels.hpp"
+
+namespace aefdtd {
+
+cudaError_t launch_voxelize(int nx, int ny, int nz, double dx, double dy, double dz, const aefdtd_structure_op *ops,
+                            int nops, int def, const int per[3], const double l[3], uint32_t *d_out, cudaStream_t s);
+
+namespace phys {
+// src/common/phys_constants.h:18-20
+constexpr double e0 = 8.854187817e-12;
+constexpr double mu0 = 12.566370614e-7;
+constexpr double c_light = 299792458.0;
+constexpr double Pi = std::numbers::pi_v<double>;
+}  // namespace phys
+using namespace phys;
+typedef std::complex<double> cplx;
+
+struct Error {
+    aefdtd_status st;
+    std::string msg;
+};
+
+#define AE_CUDA(call)                                                                        \
+    do {                                                                                     \
+        cudaError_t e__ = (call);                                                            \
+        if (e__ != cudaSuccess)                                                              \
+            throw Error{e__ == cudaErrorMemoryAllocation ? AEFDTD_OOM : AEFDTD_CUDA_ERROR,   \
+                        std::string(#call) + ": " + cudaGetErrorString(e__)};                 \
+    } while (0)
+
+static void fail(aefdtd_status st, const std::string &m) { throw Error{st, m}; }
+
+// Device buffer with byte size bookkeeping.
+struct DBuf {
+    void *p = nullptr;
+    size_t n = 0;
+    void alloc(size_t bytes, size_t &total) {
+        release(total);
+        if (bytes == 0) return;
+        AE_CUDA(cudaMalloc(&p, bytes));
+        n = bytes;
+        total += bytes;
+    }
+    void release(size_t &total) {
+        if (p) { cudaFree(p); total -= n; }
+        p = nullptr;
+        n = 0;
+    }
+    template <typename T> T *as() const { return static_cast<T *>(p); }
+};
+
+// Per-material coefficients (FDTD_Material, fdtd_material.h:38-268).
+struct HostMat {
+    bool set = false, rc = false;
+    int np = 0;
+    double C1 = 1, C2x = 0, C2y = 0, C2z = 0, C3 = 0, C4 = 0, ei = 1, sig = 0;
+    std::vector<cplx> crec, dchi, chi;
+    int x1 = 0, x2 = -1, y1 = 0, y2 = -1, z1 = 0, z2 = -1;   // bounding box in the total grid
+};
+
+struct Pulse {
+    // ChpIn (chpin.cpp:44-90, 479-545) at incidence 0, direction 0.
+    double k, omega, kx, ky, kz, n_ind, dz, C1, Ex0, Ey0, Ez0, Hx0, Hy0, Hz0;
+    void init(double li, double lf, double poli, double startz, double n_ind_i) {
+        double wi = 2.0 * Pi * c_light / li, wf = 2.0 * Pi * c_light / lf;
+        double w0 = (wi + wf) / 2.0;
+        double lambda = 2.0 * Pi * c_light / w0;
+        double dw = std::abs(0.5 * (wi - w0));
+        n_ind = n_ind_i;
+        double inc = 0 * Pi / 180.0, pol = poli * Pi / 180.0, dir = 0 * Pi / 180.0;
+        dz = 2.0 * c_light / dw / n_ind;
+        k = 2.0 * Pi / lambda * n_ind;
+        omega = 2.0 * Pi * c_light / lambda;
+        double incr = Pi / 2.0 - inc;
+        double Ca = std::cos(incr), Sa = std::sin(incr), Cb = std::cos(dir), Sb = std::sin(dir);
+        double Cc = std::cos(pol), Sc = std::sin(pol);
+        kx = k * (Ca * Cb); ky = k * (Ca * Sb); kz = k * (-Sa);
+        Ex0 = (Sa * Cb * Sc - Sb * Cc) * 1.0; Ey0 = (Sa * Sb * Sc + Cb * Cc) * 1.0; Ez0 = Ca * Sc * 1.0;
+        double tmp = 1.0 / (c_light * mu0) * 1.0 * n_ind;
+        Hx0 = tmp * (Sa * Cb * Cc + Sb * Sc); Hy0 = tmp * (Sa * Sb * Cc - Cb * Sc); Hz0 = tmp * (Ca * Cc);
+        C1 = -1.0 / k * (kx * 0 + ky * 0 + kz * startz) + dz * std::sqrt(-std::log(1e-4));
+    }
+    double f(double A0, double x, double y, double z, double t) const {
+        double p = kx * x + ky * y + kz * z;
+        double a = p - omega * t;
+        double b = (1.0 / k * p - c_light * t / n_ind + C1) / dz;
+        return A0 * std::exp(-b * b) * std::cos(a);
+    }
+};
+
+struct Osc {
+    int comp, box[6], step = 0, tshift;
+    double w0, dw;
+};
+
+struct PlaneSensor {
+    aefdtd_sensor_desc d;
+    int type, x1, x2, y1, y2, z1, z2, span1, span2, P, nl;
+    std::vector<double> lambda, w;
+    int step = 0;          // steps fed
+    int nbuf = 0;          // filled slots of the sample buffer
+    int buf_step0 = 0;     // step of slot 0
+    DBuf S, acc, wdev, WE, WH, flux;
+};
+
+static inline double s_curve(double x, double xmin, double xmax) {
+    // src/common/mathUT.cpp:1186-1193
+    double u = (x - xmin) / (xmax - xmin);
+    if (u <= 0) return 0;
+    else if (u >= 1.0) return 1.0;
+    else return u * u * (3.0 - 2.0 * u);
+}
+
+}  // namespace aefdtd
+
+using namespace aefdtd;
+
+struct aefdtd_sim {
+    aefdtd_grid_desc g{};
+    std::string last_error;
+    bool fp64 = true;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    size_t dev_bytes = 0;
+    uint64_t launches = 0;
+
+    // geometry (FDTD members)
+    int Nx = 0, Ny = 0, Nz = 0, Nx_s = 0, Ny_s = 0, Nz_s = 0;
+    int xs_s = 0, xs_e = 0, ys_s = 0, ys_e = 0, zs_s = 0, zs_e = 0;
+    int pml[6] = {0}, pad[6] = {0};
+    double Dx = 0, Dy = 0, Dz = 0, Dt = 0, dtm = 0, dtdez = 0, dtdmx = 0, dtdmy = 0, dtdmz = 0;
+    double pml_kappa[6], pml_sigma[6], pml_alpha[6];
+    double pml_m = 4, pml_ma = 2;
+    int Nt = 0, Ntap = 0, dft_k = 64;
+    int tstep = 0;
+
+    // fields and state
+    DBuf F[6], mat;
+    int id_bytes = 1;
+    std::vector<uint32_t> map;      // total-grid material ids
+    bool map_set = false;
+    unsigned Nmat = 1;
+    std::vector<HostMat> mats;
+    bool tables_dirty = true;
+    DBuf coef, disp, crec, dchi, psi;
+    bool any_disp = false;
+    // CPML
+    DBuf ik[6], bE[3], cE[3], bH[3], cH[3];
+    DBuf psiE[6], psiH[6];          // x0,x1,y0,y1,z0,z1
+    // normal mode
+    bool normal = false;
+    aefdtd_normal_desc nd{};
+    Pulse pulse{};
+    double eps_sup = 1, eps_sub = 1, index_sup = 1, index_sub = 1;
+    DBuf psums;
+    int psums_cap = 0;
+    std::vector<double> psums_host;
+    // custom mode
+    std::vector<Osc> oscs;
+    std::vector<PlaneSensor *> sensors;
+    // timing: one event quadruple per step of the last aefdtd_step call
+    // (before E, after E, after H, after sensors), summed on query
+    bool timing = false;
+    std::vector<cudaEvent_t> tev;
+    int tev_used = 0;
+    // launch shape
+    int kchunk = 8;
+
+    ~aefdtd_sim();
+    void construct(const aefdtd_grid_desc *d);
+    void set_device() const { cudaSetDevice(device); }
+    void build_pml_tables();
+    void set_map(const uint32_t *m, size_t count);
+    void set_material(uint32_t idx, const aefdtd_material_desc *md);
+    void finalize_tables();
+    template <typename T, typename Tid> void fill_args(StepArgs<T, Tid> &a, bool e_side);
+    template <typename T, typename Tid> void run_steps(int n);
+    template <typename T> void feed_sensors();
+    template <typename T> void flush_sensor(PlaneSensor &s);
+    void step(int n);
+    void zero_state();
+};
+
+aefdtd_sim::~aefdtd_sim() {
+    set_device();
+    if (stream) cudaStreamSynchronize(stream);
+    size_t t = 0;
+    for (auto &b : F) b.release(t);
+    mat.release(t); coef.release(t); disp.release(t); crec.release(t); dchi.release(t); psi.release(t);
+    for (auto &b : ik) b.release(t);
+    for (int a = 0; a < 3; a++) { bE[a].release(t); cE[a].release(t); bH[a].release(t); cH[a].release(t); }
+    for (auto &b : psiE) b.release(t);
+    for (auto &b : psiH) b.release(t);
+    psums.release(t);
+    for (auto *s : sensors) {
+        s->S.release(t); s->acc.release(t); s->wdev.release(t); s->WE.release(t); s->WH.release(t); s->flux.release(t);
+        delete s;
+    }
+    for (auto &e : tev) if (e) cudaEventDestroy(e);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+// FDTD::FDTD (fdtd_core.cpp:158-285) for modes NORM and CUSTOM, with the
+// normal-incidence driver's own argument choice (normal_incidence.cpp:188-200).
+void aefdtd_sim::construct(const aefdtd_grid_desc *d) {
+    g = *d;
+    if (g.abi_version != AEFDTD_ABI_VERSION) fail(AEFDTD_BAD_ARG, "abi_version mismatch");
+    if (g.mode != AEFDTD_MODE_NORMAL && g.mode != AEFDTD_MODE_CUSTOM) fail(AEFDTD_BAD_ARG, "unknown mode");
+    if (g.precision != AEFDTD_FP64 && g.precision != AEFDTD_FP32) fail(AEFDTD_BAD_ARG, "unknown precision");
+    if (g.nx < 1 || g.ny < 1 || g.nz < 1) fail(AEFDTD_BAD_ARG, "grid sizes must be positive");
+    if (!(g.dx > 0 && g.dy > 0 && g.dz > 0)) fail(AEFDTD_BAD_ARG, "cell sizes must be positive");
+    fp64 = g.precision == AEFDTD_FP64;
+    device = g.device;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) fail(AEFDTD_NO_DEVICE, "no CUDA device visible");
+    if (device < 0 || device >= ndev) fail(AEFDTD_BAD_ARG, "device ordinal out of range");
+    AE_CUDA(cudaSetDevice(device));
+    AE_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+
+    Dx = g.dx; Dy = g.dy; Dz = g.dz;
+    Dt = g.dt > 0 ? g.dt : std::min(std::min(Dx, Dy), Dz) / (std::sqrt(3.0) * c_light) * 0.99 * g.time_mod;
+    if (!(Dt > 0)) fail(AEFDTD_BAD_ARG, "time step must be positive (dt or time_mod)");
+    Nt = g.nt;
+    Ntap = g.tapering;
+    dft_k = g.dft_block > 0 ? g.dft_block : 64;
+    if (g.pml_m > 0) pml_m = g.pml_m;
+    if (g.pml_ma > 0) pml_ma = g.pml_ma;
+    for (int f = 0; f < 6; f++) { pml[f] = g.pml[f]; pad[f] = g.pad[f]; }
+    for (int f = 0; f < 6; f++) if (pml[f] < 0 || pad[f] < 0) fail(AEFDTD_BAD_ARG, "negative PML or pad");
+    if (g.mode == AEFDTD_MODE_NORMAL) {
+        for (int f = 0; f < 4; f++) { pml[f] = 0; pad[f] = 0; }
+        pad[4] = std::max(5, pad[4]);
+        pad[5] = std::max(5, pad[5]);
+    } else {
+        for (int a = 0; a < 3; a++)
+            if (pml[2 * a] || pml[2 * a + 1]) {
+                pad[2 * a] = std::max(5, pad[2 * a]);
+                pad[2 * a + 1] = std::max(5, pad[2 * a + 1]);
+            }
+    }
+    Nx_s = g.nx; Ny_s = g.ny; Nz_s = g.nz;
+    Nx = Nx_s + pml[0] + pad[0] + pad[1] + pml[1];
+    Ny = Ny_s + pml[2] + pad[2] + pad[3] + pml[3];
+    Nz = Nz_s + pml[4] + pad[4] + pad[5] + pml[5];
+    xs_s = pml[0] + pad[0]; xs_e = xs_s + Nx_s;
+    ys_s = pml[2] + pad[2]; ys_e = ys_s + Ny_s;
+    zs_s = pml[4] + pad[4]; zs_e = zs_s + Nz_s;
+    if ((long long)Nx * Ny * Nz > (1LL << 40)) fail(AEFDTD_BAD_ARG, "grid too large");
+    // basic_differentials_compute (fdtd_core.cpp:1137-1148)
+    dtm = Dt / mu0;
+    dtdez = Dt / (Dz * e0);
+    dtdmx = Dt / (Dx * mu0); dtdmy = Dt / (Dy * mu0); dtdmz = Dt / (Dz * mu0);
+    // set_pml_* (fdtd_pml.cpp:445-497): sigma_max = 0.8(m+1)/(eta0 D) * scale
+    for (int f = 0; f < 6; f++) {
+        double D = f < 2 ? Dx : (f < 4 ? Dy : Dz);
+        pml_kappa[f] = g.pml_kappa[f];
+        pml_sigma[f] = 0.8 * (pml_m + 1.0) / (std::sqrt(mu0 / e0) * D) * g.pml_sigma[f];
+        pml_alpha[f] = g.pml_alpha[f];
+    }
+    size_t es = fp64 ? 8 : 4;
+    size_t N = size_t(Nx) * Ny * Nz;
+    for (auto &b : F) { b.alloc(N * es, dev_bytes); AE_CUDA(cudaMemsetAsync(b.p, 0, b.n, stream)); }
+    // CPML psi, slab-compact (allocate_pml, fdtd_pml.cpp:26-86)
+    size_t nxs = pml[0] + pml[1], nys = pml[2] + pml[3], nzs = pml[4] + pml[5];
+    for (int s = 0; s < 2; s++) {
+        DBuf *P = s == 0 ? psiE : psiH;
+        for (int q = 0; q < 2; q++) {
+            P[q].alloc(nxs * Ny * Nz * es, dev_bytes);
+            P[2 + q].alloc(Nx * nys * Nz * es, dev_bytes);
+            P[4 + q].alloc(size_t(Nx) * Ny * nzs * es, dev_bytes);
+        }
+        for (int q = 0; q < 6; q++) if (P[q].p) AE_CUDA(cudaMemsetAsync(P[q].p, 0, P[q].n, stream));
+    }
+    build_pml_tables();
+    map.assign(N, 0);
+    Nmat = 1;
+    mats.assign(1, HostMat());
+    // column-parallel launch shape: enough z chunks for ~4 waves of 148 SMs
+    long long cols = (long long)Nx * Ny;
+    long long want = 148LL * 2048 * 4;
+    int chunks = (int)std::max(1LL, std::min((long long)Nz, want / std::max(1LL, cols)));
+    kchunk = std::max(1, (Nz + chunks - 1) / chunks);
+    AE_CUDA(cudaStreamSynchronize(stream));
+}
+
+// pml_coeff_calc and pml_{x,y,z}_coeffs (fdtd_pml.cpp:305-433) evaluated once
+// with the final set_pml_* parameters; 1/kappa follows the selection rules of
+// advE*/advH* (x: pml_xm||pml_xp, y: pml_ym||pml_xp, z: pml_zm||pml_zp;
+// fdtd_core.cpp:378,397,457,504,523,561,580,631,669,688).
+void aefdtd_sim::build_pml_tables() {
+    auto coeffs = [&](double ind, int N, int pm, int pp, int f, double &kappa, double &b, double &c) {
+        kappa = 1.0;
+        if (ind < pm) {
+            double x = (pm - ind) / static_cast<double>(pm);
+            kappa = 1.0 + (pml_kappa[f] - 1.0) * std::pow(x, pml_m);
+            double sig = pml_sigma[f] * std::pow(x, pml_m);
+            double alp = pml_alpha[f] * std::pow(1.0 - x, pml_ma);
+            b = std::exp(-(sig / kappa + alp) * Dt / e0);
+            c = sig / (sig * kappa + kappa * kappa * alp) * (b - 1.0);
+        }
+        if (ind > N - pp) {
+            double x = (ind - (N - pp)) / static_cast<double>(pp);
+            kappa = 1.0 + (pml_kappa[f + 1] - 1.0) * std::pow(x, pml_m);
+            double sig = pml_sigma[f + 1] * std::pow(x, pml_m);
+            double alp = pml_alpha[f + 1] * std::pow(1.0 - x, pml_ma);
+            b = std::exp(-(sig / kappa + alp) * Dt / e0);
+            c = sig / (sig * kappa + kappa * kappa * alp) * (b - 1.0);
+        }
+    };
+    int Ns[3] = {Nx, Ny, Nz};
+    double invD[3] = {1.0 / Dx, 1.0 / Dy, 1.0 / Dz};
+    bool kappa_sel[3] = {pml[0] || pml[1], pml[2] || pml[1], pml[4] || pml[5]};
+    for (int ax = 0; ax < 3; ax++) {
+        int N = Ns[ax], pm = pml[2 * ax], pp = pml[2 * ax + 1];
+        std::vector<double> kE(N, 1.0), kH(N, 1.0), be(N, 0.0), bh(N, 0.0), ce(N, 0.0), ch(N, 0.0);
+        if (pm || pp)
+            for (int i = 0; i < N; i++) {
+                coeffs(i, N, pm, pp, 2 * ax, kE[i], be[i], ce[i]);
+                coeffs(i + 0.5, N, pm, pp, 2 * ax, kH[i], bh[i], ch[i]);
+            }
+        std::vector<double> ikE(N), ikH(N), bE64(N), bH64(N), cE64(N), cH64(N);
+        for (int i = 0; i < N; i++) {
+            ikE[i] = 1.0 / (kappa_sel[ax] ? kE[i] : 1.0);
+            ikH[i] = 1.0 / (kappa_sel[ax] ? kH[i] : 1.0);
+            // the reference multiplies c by 1/D inside the psi update: c*inv_D*(diff)
+            cE64[i] = ce[i] * invD[ax];
+            cH64[i] = ch[i] * invD[ax];
+            bE64[i] = fp64 ? be[i] : be[i] - 1.0;
+            bH64[i] = fp64 ? bh[i] : bh[i] - 1.0;
+        }
+        auto up = [&](DBuf &b, const std::vector<double> &v) {
+            size_t es = fp64 ? 8 : 4;
+            b.alloc(v.size() * es, dev_bytes);
+            if (fp64) AE_CUDA(cudaMemcpy(b.p, v.data(), v.size() * 8, cudaMemcpyHostToDevice));
+            else {
+                std::vector<float> f(v.begin(), v.end());
+                AE_CUDA(cudaMemcpy(b.p, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
+            }
+        };
+        up(ik[ax], ikE); up(ik[3 + ax], ikH);
+        up(bE[ax], bE64); up(cE[ax], cE64); up(bH[ax], bH64); up(cH[ax], cH64);
+    }
+}
+
+// FDTD::set_matsgrid (fdtd_utils.cpp:572-766): structure map into the grid,
+// edge slices replicated into pads and PML.
+void aefdtd_sim::set_map(const uint32_t *m, size_t count) {
+    if (!m) fail(AEFDTD_BAD_ARG, "null map");
+    if (count != size_t(Nx_s) * Ny_s * Nz_s) fail(AEFDTD_BAD_ARG, "map size must be nx*ny*nz of the structure grid");
+    auto M = [&](int i, int j, int k) -> uint32_t & { return map[i + size_t(j) * Nx + size_t(k) * Nx * Ny]; };
+    for (int k = zs_s; k < zs_e; k++)
+        for (int j = ys_s; j < ys_e; j++) {
+            const uint32_t *src = m + size_t(j - ys_s) * Nx_s + size_t(k - zs_s) * Nx_s * Ny_s;
+            std::memcpy(&M(xs_s, j, k), src, Nx_s * sizeof(uint32_t));
+            for (int i = 0; i < xs_s; i++) M(i, j, k) = M(xs_s, j, k);
+            for (int i = xs_e; i < Nx; i++) M(i, j, k) = M(xs_e - 1, j, k);
+        }
+    for (int k = zs_s; k < zs_e; k++) {
+        for (int j = 0; j < ys_s; j++) std::memcpy(&M(0, j, k), &M(0, ys_s, k), Nx * sizeof(uint32_t));
+        for (int j = ys_e; j < Ny; j++) std::memcpy(&M(0, j, k), &M(0, ys_e - 1, k), Nx * sizeof(uint32_t));
+    }
+    for (int k = 0; k < zs_s; k++) std::memcpy(&M(0, 0, k), &M(0, 0, zs_s), size_t(Nx) * Ny * sizeof(uint32_t));
+    for (int k = zs_e; k < Nz; k++) std::memcpy(&M(0, 0, k), &M(0, 0, zs_e - 1), size_t(Nx) * Ny * sizeof(uint32_t));
+    uint32_t mx = 0;
+    for (uint32_t v : map) mx = std::max(mx, v);
+    if (mx >= 65535u) fail(AEFDTD_BAD_ARG, "at most 65535 material indices");
+    Nmat = mx + 1;
+    mats.assign(Nmat, HostMat());
+    // bounding boxes for every index in one pass (FDTD_Material::link_grid, mats.cpp:394-443)
+    for (int k = 0; k < Nz; k++)
+        for (int j = 0; j < Ny; j++) {
+            const uint32_t *row = &M(0, j, k);
+            for (int i = 0; i < Nx; i++) {
+                HostMat &h = mats[row[i]];
+                if (h.x2 < h.x1) { h.x1 = h.x2 = i; h.y1 = h.y2 = j; h.z1 = h.z2 = k; continue; }
+                h.x1 = std::min(h.x1, i); h.x2 = std::max(h.x2, i);
+                h.y1 = std::min(h.y1, j); h.y2 = std::max(h.y2, j);
+                h.z1 = std::min(h.z1, k); h.z2 = std::max(h.z2, k);
+            }
+        }
+    id_bytes = Nmat <= 256 ? 1 : 2;
+    size_t N = size_t(Nx) * Ny * Nz;
+    mat.alloc(N * id_bytes, dev_bytes);
+    if (id_bytes == 1) {
+        std::vector<uint8_t> v(N);
+        for (size_t q = 0; q < N; q++) v[q] = (uint8_t)map[q];
+        AE_CUDA(cudaMemcpy(mat.p, v.data(), N, cudaMemcpyHostToDevice));
+    } else {
+        std::vector<uint16_t> v(N);
+        for (size_t q = 0; q < N; q++) v[q] = (uint16_t)map[q];
+        AE_CUDA(cudaMemcpy(mat.p, v.data(), N * 2, cudaMemcpyHostToDevice));
+    }
+    map_set = true;
+    tables_dirty = true;
+}
+
+// FDTD::set_material (fdtd_utils.cpp:810-820): FDTD_Material::set_base_mat
+// (mats.cpp:445-464), const_recalc (mats_const.cpp:71-80), RC_dielec_treat and
+// RC_recalc (mats_RC.cpp:126-184), pole pairs of Dielec_model::get_time_exp
+// (dielec_models.cpp:71-107) and DrudeModel::get_sigma (dielec_models.cpp:287-290).
+void aefdtd_sim::set_material(uint32_t idx, const aefdtd_material_desc *md) {
+    if (!map_set) fail(AEFDTD_NOT_READY, "set the material map first");
+    if (!md) fail(AEFDTD_BAD_ARG, "null material");
+    if (md->n_debye < 0 || md->n_drude < 0 || md->n_lorentz < 0 || md->n_critpoint < 0 ||
+        md->n_debye > AEFDTD_MAX_TERMS || md->n_drude > AEFDTD_MAX_TERMS ||
+        md->n_lorentz > AEFDTD_MAX_TERMS || md->n_critpoint > AEFDTD_MAX_TERMS)
+        fail(AEFDTD_BAD_ARG, "term counts out of range");
+    if (idx >= Nmat || mats[idx].x2 < mats[idx].x1) return;   // not in the grid: ignored, as mats_in_grid
+    HostMat &h = mats[idx];
+    h.set = true;
+    const cplx Im(0, 1);
+    int nmod = md->n_debye + md->n_drude + md->n_lorentz + md->n_critpoint;
+    h.ei = md->eps_inf;
+    if (nmod == 0) {
+        h.rc = false; h.np = 0; h.sig = 0;
+        h.C1 = 1;
+        h.C2x = Dt / (Dx * e0 * h.ei);
+        h.C2y = Dt / (Dy * e0 * h.ei);
+        h.C2z = Dt / (Dz * e0 * h.ei);
+        h.C3 = 0;
+        h.C4 = Dt / (e0 * h.ei);
+        tables_dirty = true;
+        return;
+    }
+    std::vector<cplx> pa, pb;
+    for (int n = 0; n < md->n_debye; n++) {
+        double ds = md->debye[n][0], t0 = md->debye[n][1];
+        pa.push_back(ds / t0);
+        pb.push_back(-1.0 / t0);
+    }
+    for (int n = 0; n < md->n_drude; n++) {
+        double wd = md->drude[n][0], gm = md->drude[n][1];
+        double wd2 = wd * wd;
+        pa.push_back(-wd2 / gm);
+        pb.push_back(-gm);
+    }
+    for (int n = 0; n < md->n_lorentz; n++) {
+        double A = md->lorentz[n][0], O = md->lorentz[n][1], G = md->lorentz[n][2];
+        double alp = G / 2.0;
+        cplx bet = std::sqrt(O * O - alp * alp);
+        cplx eta = A * O * O / bet;
+        pa.push_back(-eta * Im);
+        pb.push_back(-alp + bet * Im);
+    }
+    for (int n = 0; n < md->n_critpoint; n++) {
+        double A = md->critpoint[n][0], O = md->critpoint[n][1], P = md->critpoint[n][2], G = md->critpoint[n][3];
+        pa.push_back(-2.0 * A * O * std::exp(-P * Im) * Im);
+        pb.push_back(-G + O * Im);
+    }
+    double sig = 0;
+    for (int n = 0; n < md->n_drude; n++) {
+        double wd = md->drude[n][0], gm = md->drude[n][1];
+        sig += e0 * (wd * wd) / gm;
+    }
+    h.rc = true; h.np = nmod; h.sig = sig;
+    h.crec.resize(nmod); h.chi.resize(nmod); h.dchi.resize(nmod);
+    for (int n = 0; n < nmod; n++) {
+        h.crec[n] = std::exp(pb[n] * Dt);
+        h.chi[n] = pa[n] / pb[n] * (std::exp(pb[n] * Dt) - 1.0);
+        h.dchi[n] = -pa[n] / pb[n] * std::pow(1.0 - std::exp(pb[n] * Dt), 2.0);
+    }
+    double chitmp = 0;
+    for (int n = 0; n < nmod; n++) chitmp += std::real(h.chi[n]);
+    double e_eff = h.ei + chitmp + h.sig * Dt / e0;
+    h.C1 = h.ei / e_eff;
+    h.C2x = Dt / (Dx * e0 * e_eff);
+    h.C2y = Dt / (Dy * e0 * e_eff);
+    h.C2z = Dt / (Dz * e0 * e_eff);
+    h.C3 = 1.0 / e_eff;
+    h.C4 = Dt / (e0 * e_eff);
+    tables_dirty = true;
+}
+
+// Device tables of material coefficients and the dispersive-state layout.
+void aefdtd_sim::finalize_tables() {
+    if (!tables_dirty) return;
+    if (!map_set) fail(AEFDTD_NOT_READY, "no material map");
+    std::vector<double> cf(size_t(Nmat) * 6);
+    std::vector<DispInfo> di(Nmat);
+    std::vector<double> cr, dc;
+    long long off = 0;
+    int poles = 0;
+    any_disp = false;
+    for (unsigned m = 0; m < Nmat; m++) {
+        HostMat &h = mats[m];
+        double v[6] = {h.C1, h.C2x, h.C2y, h.C2z, h.C3, h.C4};
+        for (int q = 0; q < 6; q++) cf[m * 6 + q] = v[q];
+        DispInfo d{};
+        if (h.rc && h.np > 0) {
+            any_disp = true;
+            d.np = h.np;
+            d.pole_off = poles;
+            d.x1 = h.x1; d.y1 = h.y1; d.z1 = h.z1;
+            d.xs = h.x2 + 1 - h.x1; d.ys = h.y2 + 1 - h.y1; d.zs = h.z2 + 1 - h.z1;
+            d.box = (long long)d.xs * d.ys * d.zs;
+            d.psi_off = off;
+            off += d.box * 3 * h.np;
+            for (int p = 0; p < h.np; p++) {
+                cplx c = h.crec[p];
+                // FP32 stores Crec-1: the decrement is small next to 1 for weakly damped poles
+                cr.push_back(fp64 ? c.real() : c.real() - 1.0);
+                cr.push_back(c.imag());
+                dc.push_back(h.dchi[p].real());
+                dc.push_back(h.dchi[p].imag());
+            }
+            poles += h.np;
+        }
+        di[m] = d;
+    }
+    auto up = [&](DBuf &b, const std::vector<double> &v) {
+        size_t es = fp64 ? 8 : 4;
+        b.alloc(std::max<size_t>(v.size(), 1) * es, dev_bytes);
+        if (v.empty()) return;
+        if (fp64) AE_CUDA(cudaMemcpy(b.p, v.data(), v.size() * 8, cudaMemcpyHostToDevice));
+        else {
+            std::vector<float> f(v.begin(), v.end());
+            AE_CUDA(cudaMemcpy(b.p, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
+        }
+    };
+    up(coef, cf);
+    up(crec, cr);
+    up(dchi, dc);
+    disp.alloc(sizeof(DispInfo) * Nmat, dev_bytes);
+    AE_CUDA(cudaMemcpy(disp.p, di.data(), sizeof(DispInfo) * Nmat, cudaMemcpyHostToDevice));
+    size_t es = fp64 ? 16 : 8;
+    if ((size_t)off * es != psi.n) {
+        psi.alloc(size_t(off) * es, dev_bytes);
+        if (psi.p) AE_CUDA(cudaMemsetAsync(psi.p, 0, psi.n, stream));
+    }
+    AE_CUDA(cudaStreamSynchronize(stream));
+    tables_dirty = false;
+}
+
+template <typename T, typename Tid>
+void aefdtd_sim::fill_args(StepArgs<T, Tid> &a, bool e_side) {
+    std::memset(&a, 0, sizeof(a));
+    a.Nx = Nx; a.Ny = Ny; a.Nz = Nz;
+    a.NxNy = (long long)Nx * Ny;
+    a.Ex = F[0].as<T>(); a.Ey = F[1].as<T>(); a.Ez = F[2].as<T>();
+    a.Hx = F[3].as<T>(); a.Hy = F[4].as<T>(); a.Hz = F[5].as<T>();
+    a.mat = mat.as<Tid>();
+    a.coef = coef.as<MatCoef<T>>();
+    a.disp = any_disp ? disp.as<DispInfo>() : nullptr;
+    a.crec = crec.as<Cplx<T>>();
+    a.dchi = dchi.as<Cplx<T>>();
+    a.psi = psi.as<Cplx<T>>();
+    a.pml_xm = pml[0]; a.pml_xp = pml[1]; a.pml_ym = pml[2]; a.pml_yp = pml[3]; a.pml_zm = pml[4]; a.pml_zp = pml[5];
+    a.px = pml[0] || pml[1]; a.py = pml[2] || pml[3]; a.pz = pml[4] || pml[5];
+    int o = e_side ? 0 : 3;
+    a.ikx = ik[o + 0].as<T>(); a.iky = ik[o + 1].as<T>(); a.ikz = ik[o + 2].as<T>();
+    DBuf *B = e_side ? bE : bH, *Cc = e_side ? cE : cH, *P = e_side ? psiE : psiH;
+    a.bx = B[0].as<T>(); a.by = B[1].as<T>(); a.bz = B[2].as<T>();
+    a.cx = Cc[0].as<T>(); a.cy = Cc[1].as<T>(); a.cz = Cc[2].as<T>();
+    a.psi_x0 = P[0].as<T>(); a.psi_x1 = P[1].as<T>();
+    a.psi_y0 = P[2].as<T>(); a.psi_y1 = P[3].as<T>();
+    a.psi_z0 = P[4].as<T>(); a.psi_z1 = P[5].as<T>();
+    a.dtdmx = (T)dtdmx; a.dtdmy = (T)dtdmy; a.dtdmz = (T)dtdmz; a.dtm = (T)dtm;
+    a.kinj = -1;
+    a.kchunk = kchunk;
+}
+
+template <typename T>
+void aefdtd_sim::flush_sensor(PlaneSensor &s) {
+    if (s.nbuf == 0) return;
+    PhasorArgs pa{s.nbuf, s.nl, s.buf_step0, Nt, Ntap, Dt, s.wdev.as<double>(), s.WE.as<double2>(), s.WH.as<double2>()};
+    launch_phasors(pa, stream);
+    AccumArgs<T> aa{s.P, s.nl, s.nbuf, s.S.as<T>(), s.WE.as<double2>(), s.WH.as<double2>(), s.acc.as<double2>()};
+    launch_accumulate(aa, stream);
+    launches += 2;
+    s.nbuf = 0;
+}
+
+template <typename T>
+void aefdtd_sim::feed_sensors() {
+    for (PlaneSensor *sp : sensors) {
+        PlaneSensor &s = *sp;
+        if (s.nbuf == 0) s.buf_step0 = s.step;
+        GatherArgs<T> ga{Nx, Ny, Nz, (long long)Nx * Ny,
+                         F[0].as<T>(), F[1].as<T>(), F[2].as<T>(), F[3].as<T>(), F[4].as<T>(), F[5].as<T>(),
+                         s.type, s.x1, s.y1, s.z1, s.span1, s.span2,
+                         s.S.as<T>() + (size_t)s.nbuf * 6 * s.P};
+        launch_gather(ga, stream);
+        launches++;
+        s.nbuf++;
+        s.step++;
+        if (s.nbuf == dft_k) flush_sensor<T>(s);
+    }
+}
+
+template <typename T, typename Tid>
+void aefdtd_sim::run_steps(int n) {
+    StepArgs<T, Tid> ea, ha;
+    fill_args(ea, true);
+    fill_args(ha, false);
+    dim3 blk(32, 4, 1);
+    dim3 grd((Nx + 31) / 32, (Ny + 3) / 4, (Nz + kchunk - 1) / kchunk);
+    if (normal && tstep + n > psums_cap) {
+        int cap = std::max(tstep + n, std::max(2 * psums_cap, 1024));
+        DBuf nb;
+        nb.alloc(size_t(cap) * 12 * 8, dev_bytes);
+        if (psums.p) AE_CUDA(cudaMemcpyAsync(nb.p, psums.p, size_t(psums_cap) * 12 * 8, cudaMemcpyDeviceToDevice, stream));
+        AE_CUDA(cudaStreamSynchronize(stream));
+        psums.release(dev_bytes);
+        psums = nb;
+        psums_cap = cap;
+    }
+    if (timing) {
+        while ((int)tev.size() < 4 * n) {
+            cudaEvent_t e;
+            AE_CUDA(cudaEventCreate(&e));
+            tev.push_back(e);
+        }
+        tev_used = n;
+    }
+    for (int q = 0; q < n; q++) {
+        int t = tstep;
+        if (timing) AE_CUDA(cudaEventRecord(tev[4 * q + 0], stream));
+        // ---- E half-step + E-side excitation
+        if (normal) {
+            double tb = t * Dt;
+            double inj_Hx = pulse.f(pulse.Hx0, 0, 0, (zs_e - 1 + 0.5) * Dz, tb);
+            double inj_Hy = pulse.f(pulse.Hy0, 0, 0, (zs_e - 1 + 0.5) * Dz, tb);
+            ea.kinj = zs_e - 1;
+            ea.inj_a = (T)(dtdez * inj_Hy / eps_sup);
+            ea.inj_b = (T)(dtdez * inj_Hx / eps_sup);
+        }
+        ea.nsrc = 0;
+        for (size_t s = 0; s < oscs.size() && s < 4; s++) {
+            Osc &o = oscs[s];
+            // Oscillator::deep_inject_E (sc_oscillator.cpp:38-39)
+            const cplx Im(0, 1);
+            cplx im_val = std::exp(-o.w0 * o.step * Dt * Im) * std::exp(-std::pow(o.dw / 2.0 * ((o.step - o.tshift) * Dt), 2.0));
+            double val = std::real(im_val) * 50;
+            std::memcpy(ea.src_box[s], o.box, sizeof(o.box));
+            ea.src_comp[s] = o.comp;
+            ea.src_val[s] = (T)val;
+            ea.nsrc++;
+        }
+        launch_e(ea, grd, blk, stream);
+        if (timing) AE_CUDA(cudaEventRecord(tev[4 * q + 1], stream));
+        // ---- H half-step + H-side excitation
+        if (normal) {
+            double tb = (t + 0.5) * Dt;
+            double inj_Ex = pulse.f(pulse.Ex0, 0, 0, (zs_e - 1) * Dz, tb);
+            double inj_Ey = pulse.f(pulse.Ey0, 0, 0, (zs_e - 1) * Dz, tb);
+            ha.kinj = zs_e - 1;
+            ha.inj_a = (T)(dtdmz * inj_Ey);
+            ha.inj_b = (T)(dtdmz * inj_Ex);
+        }
+        launch_h(ha, grd, blk, stream);
+        launches += 2;
+        if (timing) AE_CUDA(cudaEventRecord(tev[4 * q + 2], stream));
+        // ---- sensors (fed after H in both drivers; custom inject_H is a no-op
+        //      for oscillators apart from the step counter)
+        feed_sensors<T>();
+        for (auto &o : oscs) o.step += 1;
+        if (normal) {
+            PlaneSumArgs<T> pa{};
+            pa.Nx = Nx; pa.Ny = Ny; pa.NxNy = (long long)Nx * Ny;
+            pa.Ex = F[0].as<T>(); pa.Ey = F[1].as<T>(); pa.Ez = F[2].as<T>();
+            pa.kr = zs_e - 2; pa.kt = zs_s;
+            pa.Dx = Dx; pa.Dy = Dy; pa.Dz = Dz;
+            pa.tb = (t + 0.5) * Dt;
+            double tapering = 1.0;
+            if (t >= Nt - Ntap) tapering = s_curve(t, Nt - 1.0, Nt - Ntap);
+            pa.tapering = tapering;
+            pa.P = PulseDev{pulse.k, pulse.omega, pulse.kx, pulse.ky, pulse.kz, pulse.n_ind, pulse.dz, pulse.C1,
+                            pulse.Ex0, pulse.Ey0, pulse.Ez0};
+            pa.out = psums.as<double>() + size_t(t) * 12;
+            launch_plane_sums(pa, stream);
+            launches++;
+        }
+        if (timing) AE_CUDA(cudaEventRecord(tev[4 * q + 3], stream));
+        tstep++;
+    }
+    AE_CUDA(cudaGetLastError());
+}
+
+void aefdtd_sim::step(int n) {
+    if (n < 0) fail(AEFDTD_BAD_ARG, "negative step count");
+    if (!map_set) fail(AEFDTD_NOT_READY, "no material map");
+    if (g.mode == AEFDTD_MODE_NORMAL && !normal) fail(AEFDTD_NOT_READY, "normal mode needs aefdtd_setup_normal");
+    set_device();
+    finalize_tables();
+    if (fp64) {
+        if (id_bytes == 1) run_steps<double, uint8_t>(n); else run_steps<double, uint16_t>(n);
+    } else {
+        if (id_bytes == 1) run_steps<float, uint8_t>(n); else run_steps<float, uint16_t>(n);
+    }
+}
+
+void aefdtd_sim::zero_state() {
+    set_device();
+    for (auto &b : F) if (b.p) AE_CUDA(cudaMemsetAsync(b.p, 0, b.n, stream));
+    for (auto &b : psiE) if (b.p) AE_CUDA(cudaMemsetAsync(b.p, 0, b.n, stream));
+    for (auto &b : psiH) if (b.p) AE_CUDA(cudaMemsetAsync(b.p, 0, b.n, stream));
+    if (psi.p) AE_CUDA(cudaMemsetAsync(psi.p, 0, psi.n, stream));
+    for (auto *s : sensors) {
+        if (s->acc.p) AE_CUDA(cudaMemsetAsync(s->acc.p, 0, s->acc.n, stream));
+        s->step = 0; s->nbuf = 0;
+    }
+    for (auto &o : oscs) o.step = 0;
+    tstep = 0;
+    AE_CUDA(cudaStreamSynchronize(stream));
+}
+
+// ------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------
+
+template <typename F> static aefdtd_status guarded(aefdtd_sim *s, F &&f) {
+    try {
+        f();
+        if (s) s->last_error.clear();
+        return AEFDTD_OK;
+    } catch (Error &e) {
+        if (s) s->last_error = e.msg;
+        return e.st;
+    } catch (std::bad_alloc &) {
+        if (s) s->last_error = "host allocation failed";
+        return AEFDTD_OOM;
+    } catch (std::exception &e) {
+        if (s) s->last_error = e.what();
+        return AEFDTD_BAD_ARG;
+    }
+}
+
+static thread_local std::string g_create_error;
+
+extern "C" {
+
+aefdtd_status aefdtd_create(const aefdtd_grid_desc *desc, aefdtd_sim **out) {
+    if (!desc || !out) return AEFDTD_BAD_ARG;
+    *out = nullptr;
+    aefdtd_sim *s = new (std::nothrow) aefdtd_sim();
+    if (!s) return AEFDTD_OOM;
+    aefdtd_status st = guarded(s, [&] { s->construct(desc); });
+    if (st != AEFDTD_OK) {
+        g_create_error = s->last_error;
+        delete s;
+        return st;
+    }
+    *out = s;
+    return AEFDTD_OK;
+}
+
+aefdtd_status aefdtd_destroy(aefdtd_sim *s) {
+    if (!s) return AEFDTD_BAD_ARG;
+    delete s;
+    return AEFDTD_OK;
+}
+
+const char *aefdtd_last_error(const aefdtd_sim *s) {
+    return s ? s->last_error.c_str() : g_create_error.c_str();
+}
+
+const char *aefdtd_status_string(aefdtd_status st) {
+    switch (st) {
+        case AEFDTD_OK: return "ok";
+        case AEFDTD_BAD_ARG: return "bad argument";
+        case AEFDTD_OOM: return "out of device memory";
+        case AEFDTD_TIMEOUT: return "timeout";
+        case AEFDTD_CUDA_ERROR: return "CUDA error";
+        case AEFDTD_NOT_READY: return "not ready";
+        case AEFDTD_NO_DEVICE: return "no CUDA device";
+    }
+    return "unknown status";
+}
+
+aefdtd_status aefdtd_get_dims(const aefdtd_sim *s, aefdtd_dims *o) {
+    if (!s || !o) return AEFDTD_BAD_ARG;
+    o->nx = s->Nx; o->ny = s->Ny; o->nz = s->Nz;
+    o->xs_s = s->xs_s; o->xs_e = s->xs_e; o->ys_s = s->ys_s; o->ys_e = s->ys_e; o->zs_s = s->zs_s; o->zs_e = s->zs_e;
+    o->n_materials = (int32_t)s->Nmat;
+    o->step = s->tstep;
+    o->dt = s->Dt;
+    o->device_bytes = s->dev_bytes;
+    return AEFDTD_OK;
+}
+
+aefdtd_status aefdtd_set_material_map(aefdtd_sim *s, const uint32_t *map, size_t count) {
+    if (!s) return AEFDTD_BAD_ARG;
+    return guarded(s, [&] { s->set_device(); s->set_map(map, count); });
+}
+
+aefdtd_status aefdtd_set_material(aefdtd_sim *s, uint32_t index, const aefdtd_material_desc *m) {
+    if (!s) return AEFDTD_BAD_ARG;
+    return guarded(s, [&] { s->set_material(index, m); });
+}
+
+aefdtd_status aefdtd_setup_normal(aefdtd_sim *s, const aefdtd_normal_desc *nd) {
+    if (!s || !nd) return AEFDTD_BAD_ARG;
+    return guarded(s, [&] {
+        if (s->g.mode != AEFDTD_MODE_NORMAL) fail(AEFDTD_BAD_ARG, "setup_normal needs mode NORMAL");
+        if (!s->map_set) fail(AEFDTD_NOT_READY, "set the material map first");
+        if (nd->nl < 2 || !(nd->lambda_min > 0) || !(nd->lambda_max > 0)) fail(AEFDTD_BAD_ARG, "bad spectrum");
+        s->nd = *nd;
+        // normal_incidence.cpp:238-249: superstrate/substrate from the map at
+        // (0,0,zs_e) and (0,0,zs_s); ei is eps_inf of the material.
+        auto M = [&](int i, int j, int k) { return s->map[i + size_t(j) * s->Nx + size_t(k) * s->Nx * s->Ny]; };
+        s->eps_sub = s->mats[M(0, 0, s->zs_s)].ei;
+        s->eps_sup = s->mats[M(0, 0, s->zs_e)].ei;
+        s->index_sub = std::sqrt(s->eps_sub);
+        s->index_sup = std::sqrt(s->eps_sup);
+        double pol = nd->polarization == 1 ? 90 : 0;
+        s->pulse.init(nd->lambda_min, nd->lambda_max, pol, (s->zs_e - 1) * s->Dz, s->index_sup);
+        s->normal = true;
+    });
+}
+
+aefdtd_status aefdtd_add_oscillator(aefdtd_sim *s, const aefdtd_source_desc *d, int32_t *id) {
+    if (!s || !d) return AEFDTD_BAD_ARG;
+    return guarded(s, [&] {
+        if (s->g.mode != AEFDTD_MODE_CUSTOM) fail(AEFDTD_BAD_ARG, "oscillators need mode CUSTOM");
+        if (s->oscs.size() >= 4) fail(AEFDTD_BAD_ARG, "at most 4 oscillators");
+        if (d->orientation < 0 || d->orientation > 5) fail(AEFDTD_BAD_ARG, "bad orientation");
+        if (!(d->lambda_min > 0 && d->lambda_max > 0)) fail(AEFDTD_BAD_ARG, "bad spectrum");
+        Osc o;
+        o.comp = d->orientation <= 1 ? 0 : (d->orientation <= 3 ? 1 : 2);
+        // Source::link (sources.cpp:252-283)
+        o.box[0] = std::clamp(d->box[0] + s->xs_s, 0, s->Nx); o.box[1] = std::clamp(d->box[1] + s->xs_s, 0, s->Nx);
+        o.box[2] = std::clamp(d->box[2] + s->ys_s, 0, s->Ny); o.box[3] = std::clamp(d->box[3] + s->ys_s, 0, s->Ny);
+        o.box[4] = std::clamp(d->box[4] + s->zs_s, 0, s->Nz); o.box[5] = std::clamp(d->box[5] + s->zs_s, 0, s->Nz);
+        // Oscillator::initialize (sc_oscillator.cpp:69-84)
+        double alp = std::sqrt(0.1), bet = 1e-7;
+        double w1 = 2.0 * Pi * c_light / d->lambda_max, w2 = 2.0 * Pi * c_light / d->lambda_min;
+        o.w0 = (w1 + w2) / 2.0;
+        o.dw = std::abs(w2 - w1) / (2.0 * std::sqrt(-std::log(alp)));
+        o.tshift = (int)(std::sqrt(-4.0 / (o.dw * o.dw) * std::log(bet)) / s->Dt);
+        o.step = s->tstep;
+        s->oscs.push_back(o);
+        if (id) *id = (int32_t)s->oscs.size() - 1;
+    });
+}
+
+aefdtd_status aefdtd_add_planar_sensor(aefdtd_sim *s, const aefdtd_sensor_desc *d, int32_t *id) {
+    if (!s || !d) return AEFDTD_BAD_ARG;
+    return guarded(s, [&] {
+        if (d->orientation < 0 || d->orientation > 5) fail(AEFDTD_BAD_ARG, "bad orientation");
+        if (d->nl < 1) fail(AEFDTD_BAD_ARG, "nl must be positive");
+        if (!(d->lambda_min > 0 && d->lambda_max > 0)) fail(AEFDTD_BAD_ARG, "bad spectrum");
+        s->set_device();
+        PlaneSensor *p = new PlaneSensor();
+        p->d = *d;
+        p->type = d->orientation;
+        // Sensor::link (sensors.cpp:196-230) and SensorFieldHolder::initialize (sensors.cpp:496-527)
+        p->x1 = std::clamp(d->box[0] + s->xs_s, 0, s->Nx); p->x2 = std::clamp(d->box[1] + s->xs_s, 0, s->Nx);
+        p->y1 = std::clamp(d->box[2] + s->ys_s, 0, s->Ny); p->y2 = std::clamp(d->box[3] + s->ys_s, 0, s->Ny);
+        p->z1 = std::clamp(d->box[4] + s->zs_s, 0, s->Nz); p->z2 = std::clamp(d->box[5] + s->zs_s, 0, s->Nz);
+        if (p->type <= 1) { p->span1 = p->y2 - p->y1; p->span2 = p->z2 - p->z1; }
+        else if (p->type <= 3) { p->span1 = p->x2 - p->x1; p->span2 = p->z2 - p->z1; }
+        else { p->span1 = p->x2 - p->x1; p->span2 = p->y2 - p->y1; }
+        if (p->span1 <= 0 || p->span2 <= 0) { delete p; fail(AEFDTD_BAD_ARG, "sensor plane is empty"); }
+        int plane_i = p->type <= 1 ? p->x1 : (p->type <= 3 ? p->y1 : p->z1);
+        int plane_n = p->type <= 1 ? s->Nx : (p->type <= 3 ? s->Ny : s->Nz);
+        if (plane_i >= plane_n) { delete p; fail(AEFDTD_BAD_ARG, "sensor plane outside the grid"); }
+        p->P = p->span1 * p->span2;
+        p->nl = d->nl;
+        p->lambda.resize(p->nl);
+        p->w.resize(p->nl);
+        for (int l = 0; l < p->nl; l++) {
+            p->lambda[l] = d->nl > 1 ? d->lambda_min + (d->lambda_max - d->lambda_min) * l / (d->nl - 1.0) : d->lambda_min;
+            p->w[l] = 2.0 * Pi * c_light / p->lambda[l];
+        }
+        size_t es = s->fp64 ? 8 : 4;
+        try {
+            p->S.alloc(size_t(s->dft_k) * 6 * p->P * es, s->dev_bytes);
+            p->acc.alloc(size_t(6) * p->nl * p->P * 16, s->dev_bytes);
+            p->wdev.alloc(size_t(p->nl) * 8, s->dev_bytes);
+            p->WE.alloc(size_t(s->dft_k) * p->nl * 16, s->dev_bytes);
+            p->WH.alloc(size_t(s->dft_k) * p->nl * 16, s->dev_bytes);
+            p->flux.alloc(size_t(p->nl) * 8, s->dev_bytes);
+            AE_CUDA(cudaMemsetAsync(p->acc.p, 0, p->acc.n, s->stream));
+            AE_CUDA(cudaMemcpyAsync(p->wdev.p, p->w.data(), p->nl * 8, cudaMemcpyHostToDevice, s->stream));
+            AE_CUDA(cudaStreamSynchronize(s->stream));
+        } catch (...) {
+            p->S.release(s->dev_bytes); p->acc.release(s->dev_bytes); p->wdev.release(s->dev_bytes);
+            p->WE.release(s->dev_bytes); p->WH.release(s->dev_bytes); p->flux.release(s->dev_bytes);
+            delete p;
+            throw;
+        }
+        p->step = s->tstep;
+        s->sensors.push_back(p);
+        if (id) *id = (int32_t)s->sensors.size() - 1;
+    });
+}
+
+aefdtd_status aefdtd_step(aefdtd_sim *s, int32_t n) {
+    if (!s) return AEFDTD_BAD_ARG;
+    return guarded(s, [&] { s->step(n); });
+}
+
+aefdtd_status aefdtd_synchronize(aefdtd_sim *s) {
+    if (!s) return AEFDTD_BAD_ARG;
+    return guarded(s, [&] { s->set_device(); AE_CUDA(cudaStreamSynchronize(s->stream)); });
+}
+
+aefdtd_status aefdtd_reset(aefdtd_sim *s) {
+    if (!s) return AEFDTD_BAD_ARG;
+    return guarded(s, [&] { s->zero_state(); });
+}
+
+aefdtd_status aefdtd_get_field(aefdtd_sim *s, int32_t c, double *out, size_t count) {
+    if (!s || !out) return AEFDTD_BAD_ARG;
+    return guarded(s, [&] {
+        if (c < 0 || c > 5) fail(AEFDTD_BAD_ARG, "component out of range");
+        size_t N = size_t(s->Nx) * s->Ny * s->Nz;
+        if (count != N) fail(AEFDTD_BAD_ARG, "count must be Nx*Ny*Nz of the total grid");
+        s->set_device();
+        if (s->fp64) {
+            AE_CUDA(cudaMemcpyAsync(out, s->F[c].p, N * 8, cudaMemcpyDeviceToHost, s->stream));
+            AE_CUDA(cudaStreamSynchronize(s->stream));
+        } else {
+            std::vector<float> tmp(N);
+            AE_CUDA(cudaMemcpyAsync(tmp.data(), s->F[c].p, N * 4, cudaMemcpyDeviceToHost, s->stream));
+            AE_CUDA(cudaStreamSynchronize(s->stream));
+            for (size_t q = 0; q < N; q++) out[q] = tmp[q];
+        }
+    });
+}
+
+aefdtd_status aefdtd_set_field(aefdtd_sim *s, int32_t c, const double *in, size_t count) {
+    if (!s || !in) return AEFDTD_BAD_ARG;
+    return guarded(s, [&] {
+        if (c < 0 || c > 5) fail(AEFDTD_BAD_ARG, "component out of range");
+        size_t N = size_t(s->Nx) * s->Ny * s->Nz;
+        if (count != N) fail(AEFDTD_BAD_ARG, "count must be Nx*Ny*Nz of the total grid");
+        s->set_device();
+        if (s->fp64) {
+            AE_CUDA(cudaMemcpyAsync(s->F[c].p, in, N * 8, cudaMemcpyHostToDevice, s->stream));
+        } else {
+            std::vector<float> tmp(in, in + N);
+            AE_CUDA(cudaMemcpyAsync(s->F[c].p, tmp.data(), N * 4, cudaMemcpyHostToDevice, s->stream));
+        }
+        AE_CUDA(cudaStreamSynchronize(s->stream));
+    });
+}
+
+aefdtd_status aefdtd_field_device_ptr(aefdtd_sim *s, int32_t c, void **ptr) {
+    if (!s || !ptr || c < 0 || c > 5) return AEFDTD_BAD_ARG;
+    *ptr = s->F[c].p;
+    return AEFDTD_OK;
+}
+
+aefdtd_status aefdtd_get_plane_sums(aefdtd_sim *s, double *out, int32_t steps) {
+    if (!s || !out) return AEFDTD_BAD_ARG;
+    return guarded(s, [&] {
+        if (!s->normal) fail(AEFDTD_NOT_READY, "plane sums exist in normal mode only");
+        if (steps != s->tstep) fail(AEFDTD_BAD_ARG, "steps must equal the number of completed steps");
+        s->set_device();
+        std::vector<double> tmp(size_t(steps) * 12);
+        if (steps > 0) {
+            AE_CUDA(cudaMemcpyAsync(tmp.data(), s->psums.p, tmp.size() * 8, cudaMemcpyDeviceToHost, s->stream));
+            AE_CUDA(cudaStreamSynchronize(s->stream));
+        }
+        for (int c = 0; c < 12; c++)
+            for (int t = 0; t < steps; t++) out[size_t(c) * steps + t] = tmp[size_t(t) * 12 + c];
+    });
+}
+
+// Post-processing of FDTD_normal_incidence (normal_incidence.cpp:442-570),
+// FP64 on the host over the completed steps.
+aefdtd_status aefdtd_get_normal_spectra(aefdtd_sim *s, double *out, int32_t nl) {
+    if (!s || !out) return AEFDTD_BAD_ARG;
+    return guarded(s, [&] {
+        if (!s->normal) fail(AEFDTD_NOT_READY, "spectra exist in normal mode only");
+        if (nl != s->nd.nl) fail(AEFDTD_BAD_ARG, "nl must equal the normal-mode spectrum size");
+        int NtP = s->tstep;
+        if (NtP < 2) fail(AEFDTD_NOT_READY, "run at least two steps");
+        std::vector<double> S(size_t(NtP) * 12);
+        aefdtd_status st = aefdtd_get_plane_sums(s, S.data(), NtP);
+        if (st != AEFDTD_OK) fail(st, s->last_error);
+        auto M = [&](int i, int j, int k) { return s->map[i + size_t(j) * s->Nx + size_t(k) * s->Nx * s->Ny]; };
+        // FDTD::find_slab (fdtd_utils.cpp:347-392)
+        int sub_ref = s->zs_s, sup_ref = s->zs_e - 1;
+        int Nsub = 0, Nsup = 0, IDmoy = 0, IDsup = 0, IDsub = 0, k;
+        for (int i = s->xs_s; i < s->xs_e; i++)
+            for (int j = s->ys_s; j < s->ys_e; j++) { IDsup += M(i, j, s->zs_e); IDsub += M(i, j, s->zs_s); }
+        IDmoy = IDsub; k = sub_ref;
+        while (IDmoy == IDsub && k < sup_ref) {
+            IDmoy = 0;
+            for (int i = s->xs_s; i < s->xs_e; i++) for (int j = s->ys_s; j < s->ys_e; j++) IDmoy += M(i, j, k + 1);
+            Nsub++; k++;
+        }
+        IDmoy = IDsup; k = sup_ref;
+        while (IDmoy == IDsup && k >= sub_ref) {
+            IDmoy = 0;
+            for (int i = s->xs_s; i < s->xs_e; i++) for (int j = s->ys_s; j < s->ys_e; j++) IDmoy += M(i, j, k - 1);
+            Nsup++; k--;
+        }
+        double Dz = s->Dz, Dt = s->Dt;
+        double hsup = (Nsup - 1) * Dz, hsub = Nsub * Dz, hstruc = (s->Nz_s - Nsup - Nsub) * Dz;
+        hsup -= Dz / 2.0;
+        hsub -= Dz / 2.0;
+        const cplx Im(0, 1);
+        const double *SS[12];
+        for (int c = 0; c < 12; c++) SS[c] = S.data() + size_t(c) * NtP;
+        for (int l = 0; l < nl; l++) {
+            double lam = s->nd.lambda_min + (s->nd.lambda_max - s->nd.lambda_min) * l / (nl - 1.0);
+            double w = 2.0 * Pi * c_light / lam;
+            cplx r1x = 0, r1y = 0, r1z = 0, r2x = 0, r2y = 0, r2z = 0, t1x = 0, t1y = 0, t1z = 0, t2x = 0, t2y = 0, t2z = 0;
+            double k0 = -w / c_light, k1 = k0 * s->index_sup, k3 = k0 * s->index_sub;
+            cplx tmp_sup = std::exp(2.0 * k1 * hsup * Im);
+            cplx tmp_sub = std::exp((k3 * hsub - k0 * (hstruc + hsub)) * Im);
+            for (int t = 0; t < NtP; t++) {
+                cplx tmp1 = std::exp(t * Dt * w * Im) / (NtP - 1.0);
+                cplx tmp2 = tmp1 * tmp_sup, tmp3 = tmp1 * tmp_sub;
+                r1x += SS[0][t] * tmp1; r1y += SS[1][t] * tmp1; r1z += SS[2][t] * tmp1;
+                r2x += SS[3][t] * tmp2; r2y += SS[4][t] * tmp2; r2z += SS[5][t] * tmp2;
+                t1x += SS[6][t] * tmp1; t1y += SS[7][t] * tmp1; t1z += SS[8][t] * tmp1;
+                t2x += SS[9][t] * tmp3; t2y += SS[10][t] * tmp3; t2z += SS[11][t] * tmp3;
+            }
+            double *o = out + size_t(l) * 15;
+            o[0] = lam;
+            double a = std::sqrt(std::norm(r2x) + std::norm(r2y) + std::norm(r2z));
+            double b = std::sqrt(std::norm(r1x) + std::norm(r1y) + std::norm(r1z));
+            o[1] = a / b;
+            a = std::sqrt(std::norm(t2x) + std::norm(t2y) + std::norm(t2z));
+            b = std::sqrt(std::norm(t1x) + std::norm(t1y) + std::norm(t1z));
+            o[2] = a / b;
+            cplx ref0 = r1y, trans0 = t1y;
+            if (s->nd.polarization == 1) { ref0 = r1x; trans0 = t1x; }
+            cplx refx = r2x / ref0, refy = r2y / ref0, transx = t2x / trans0, transy = t2y / trans0;
+            o[3] = std::abs(refx); o[4] = std::arg(refx); o[5] = std::norm(refx);
+            o[6] = std::abs(refy); o[7] = std::arg(refy); o[8] = std::norm(refy);
+            o[9] = std::abs(transx); o[10] = std::arg(transx); o[11] = std::norm(transx) * s->index_sub / s->index_sup;
+            o[12] = std::abs(transy); o[13] = std::arg(transy); o[14] = std::norm(transy) * s->index_sub / s->index_sup;
+        }
+    });
+}
+
+aefdtd_status aefdtd_get_sensor_shape(aefdtd_sim *s, int32_t id, int32_t *span1, int32_t *span2, int32_t *nl) {
+    if (!s || id < 0 || id >= (int)s->sensors.size()) return AEFDTD_BAD_ARG;
+    if (span1) *span1 = s->sensors[id]->span1;
+    if (span2) *span2 = s->sensors[id]->span2;
+    if (nl) *nl = s->sensors[id]->nl;
+    return AEFDTD_OK;
+}
+
+aefdtd_status aefdtd_get_sensor_flux(aefdtd_sim *s, int32_t id, double *out, int32_t nl) {
+    if (!s || !out) return AEFDTD_BAD_ARG;
+    return guarded(s, [&] {
+        if (id < 0 || id >= (int)s->sensors.size()) fail(AEFDTD_BAD_ARG, "unknown sensor");
+        PlaneSensor &p = *s->sensors[id];
+        if (nl != p.nl) fail(AEFDTD_BAD_ARG, "nl must equal the sensor's spectrum size");
+        s->set_device();
+        if (s->fp64) s->flush_sensor<double>(p); else s->flush_sensor<float>(p);
+        double af = p.type <= 1 ? s->Dy * s->Dz : (p.type <= 3 ? s->Dx * s->Dz : s->Dx * s->Dy);
+        FluxArgs fa{p.P, p.nl, p.type, af, p.acc.as<double2>(), p.flux.as<double>()};
+        launch_flux(fa, s->stream);
+        s->launches++;
+        AE_CUDA(cudaMemcpyAsync(out, p.flux.p, size_t(nl) * 8, cudaMemcpyDeviceToHost, s->stream));
+        AE_CUDA(cudaStreamSynchronize(s->stream));
+        AE_CUDA(cudaGetLastError());
+    });
+}
+
+aefdtd_status aefdtd_get_sensor_dft(aefdtd_sim *s, int32_t id, double *out, size_t count) {
+    if (!s || !out) return AEFDTD_BAD_ARG;
+    return guarded(s, [&] {
+        if (id < 0 || id >= (int)s->sensors.size()) fail(AEFDTD_BAD_ARG, "unknown sensor");
+        PlaneSensor &p = *s->sensors[id];
+        if (count != size_t(6) * p.P * p.nl * 2) fail(AEFDTD_BAD_ARG, "count must be 6*span1*span2*nl*2");
+        s->set_device();
+        if (s->fp64) s->flush_sensor<double>(p); else s->flush_sensor<float>(p);
+        AE_CUDA(cudaMemcpyAsync(out, p.acc.p, count * 8, cudaMemcpyDeviceToHost, s->stream));
+        AE_CUDA(cudaStreamSynchronize(s->stream));
+    });
+}
+
+aefdtd_status aefdtd_voxelize(aefdtd_sim *sim, int32_t nx, int32_t ny, int32_t nz, double dx, double dy, double dz,
+                              const aefdtd_structure_op *ops, int32_t n_ops, int32_t default_material,
+                              const int32_t periodic[3], const double lengths[3], uint32_t *out_map, int32_t device) {
+    if (nx < 1 || ny < 1 || nz < 1 || n_ops < 0 || n_ops > 256 || (n_ops > 0 && !ops) || !out_map) return AEFDTD_BAD_ARG;
+    return guarded(sim, [&] {
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) fail(AEFDTD_NO_DEVICE, "no CUDA device visible");
+        int dev = sim ? sim->device : device;
+        AE_CUDA(cudaSetDevice(dev));
+        for (int q = 0; q < n_ops; q++)
+            if (ops[q].kind < AEFDTD_OP_BLOCK || ops[q].kind > AEFDTD_OP_CYLINDER || ops[q].mat_index < 0)
+                fail(AEFDTD_BAD_ARG, "bad structure operation");
+        int per[3] = {0, 0, 0};
+        double L[3] = {0, 0, 0};
+        for (int a = 0; a < 3; a++) {
+            per[a] = periodic ? (periodic[a] ? 1 : 0) : 0;
+            L[a] = lengths ? lengths[a] : 0;
+            if (per[a] && !(L[a] > 0)) fail(AEFDTD_BAD_ARG, "periodic axis needs a positive length");
+        }
+        size_t n = size_t(nx) * ny * nz;
+        cudaStream_t st = sim ? sim->stream : nullptr;
+        uint32_t *d = nullptr;
+        AE_CUDA(cudaMallocAsync((void **)&d, n * 4, st));
+        cudaError_t e = launch_voxelize(nx, ny, nz, dx, dy, dz, ops, n_ops, default_material, per, L, d, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(out_map, d, n * 4, cudaMemcpyDeviceToHost, st);
+        cudaFreeAsync(d, st);
+        cudaError_t e2 = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) fail(AEFDTD_CUDA_ERROR, std::string("voxelize: ") + cudaGetErrorString(e));
+        if (e2 != cudaSuccess) fail(AEFDTD_CUDA_ERROR, std::string("voxelize: ") + cudaGetErrorString(e2));
+        if (sim) {
+            sim->launches++;
+            if (nx != sim->Nx_s || ny != sim->Ny_s || nz != sim->Nz_s) fail(AEFDTD_BAD_ARG, "map size differs from the structure grid");
+            sim->set_map(out_map, n);
+        }
+    });
+}
+
+aefdtd_status aefdtd_get_timings(aefdtd_sim *s, double *e_ms, double *h_ms, double *sensor_ms) {
+    if (!s) return AEFDTD_BAD_ARG;
+    return guarded(s, [&] {
+        double te = 0, th = 0, ts = 0;
+        if (s->timing && s->tev_used > 0) {
+            s->set_device();
+            AE_CUDA(cudaEventSynchronize(s->tev[4 * s->tev_used - 1]));
+            for (int q = 0; q < s->tev_used; q++) {
+                float a = 0, b = 0, c = 0;
+                AE_CUDA(cudaEventElapsedTime(&a, s->tev[4 * q + 0], s->tev[4 * q + 1]));
+                AE_CUDA(cudaEventElapsedTime(&b, s->tev[4 * q + 1], s->tev[4 * q + 2]));
+                AE_CUDA(cudaEventElapsedTime(&c, s->tev[4 * q + 2], s->tev[4 * q + 3]));
+                te += a; th += b; ts += c;
+            }
+        }
+        if (e_ms) *e_ms = te;
+        if (h_ms) *h_ms = th;
+        if (sensor_ms) *sensor_ms = ts;
+    });
+}
+
+aefdtd_status aefdtd_enable_timing(aefdtd_sim *s, int32_t enable) {
+    if (!s) return AEFDTD_BAD_ARG;
+    s->timing = enable != 0;
+    return AEFDTD_OK;
+}
+
+aefdtd_status aefdtd_get_stream(aefdtd_sim *s, void **stream) {
+    if (!s || !stream) return AEFDTD_BAD_ARG;
+    *stream = (void *)s->stream;
+    return AEFDTD_OK;
+}
+
+aefdtd_status aefdtd_get_launch_count(aefdtd_sim *s, uint64_t *launches) {
+    if (!s || !launches) return AEFDTD_BAD_ARG;
+    *launches = s->launches;
+    return AEFDTD_OK;
+}
+
+}  // extern "C"

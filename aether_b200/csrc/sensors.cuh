@@ -1,0 +1,230 @@
+// sensors.cuh — device kernels of the sensor path.
+//
+//  * plane_sums: the normal-incidence R/T plane sums of one step
+//    (normal_incidence.cpp:378-415), with the analytic incident pulse
+//    (ChpIn::PulseE*, chpin.cpp:44-90) evaluated per cell in FP64.
+//  * dft_gather: interpolated plane samples of one step into the K-step
+//    sample buffer (SensorFieldHolder::update_t_interp, sensors.cpp:601-644,
+//    with FDTD::local_E*/H*, fdtd_utils.cpp:457-507).
+//  * dft_phasors / dft_accumulate: the buffered DFT of K steps,
+//    acc[c][l][p] += sum_k S[k][c][p] * W_c[k][l] with
+//    W_E = taper_E * exp(i w_l step Dt), W_H = taper_H * exp(i w_l (step+1/2) Dt)
+//    (SensorFieldHolder::FT_comp, sensors.cpp:456-479; tapering from
+//    Sensor::feed, sensors.cpp:232-243). With one buffered step the sum is the
+//    reference's per-step update exactly.
+//  * flux: Spect_Poynting::treat (s_spec_power.cpp:44-119) in FP64.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "aefdtd_dev.hpp"
+
+namespace aefdtd {
+
+
+
+__device__ __forceinline__ double pulse_eval(const PulseDev &P, double A0, double x, double y, double z, double t) {
+    const double p = P.kx * x + P.ky * y + P.kz * z;
+    const double a = p - P.omega * t;
+    const double b = (1.0 / P.k * p - 299792458.0 * t / P.n_ind + P.C1) / P.dz;
+    return A0 * exp(-b * b) * cos(a);
+}
+
+
+
+// One block per step; deterministic tree reduction.
+template <typename T>
+__global__ void __launch_bounds__(512) plane_sums(PlaneSumArgs<T> a) {
+    double acc[12];
+#pragma unroll
+    for (int c = 0; c < 12; ++c) acc[c] = 0;
+    const int n = a.Nx * a.Ny;
+    const double Dx2 = a.Dx / 2.0, Dy2 = a.Dy / 2.0, Dz2 = a.Dz / 2.0;
+    const double zr = a.kr * a.Dz, zt = a.kt * a.Dz;
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+        const int i = q % a.Nx, j = q / a.Nx;
+        const double x = i * a.Dx, y = j * a.Dy;
+        const double bx = pulse_eval(a.P, a.P.Ex0, x + Dx2, y, zr, a.tb);
+        const double by = pulse_eval(a.P, a.P.Ey0, x, y + Dy2, zr, a.tb);
+        const double bz = pulse_eval(a.P, a.P.Ez0, x, y, zr + Dz2, a.tb);
+        const double tx = pulse_eval(a.P, a.P.Ex0, x + Dx2, y, zt, a.tb);
+        const double ty = pulse_eval(a.P, a.P.Ey0, x, y + Dy2, zt, a.tb);
+        const double tz = pulse_eval(a.P, a.P.Ez0, x, y, zt + Dz2, a.tb);
+        const long long ir = q + a.kr * a.NxNy, it = q + a.kt * a.NxNy;
+        acc[0] += bx * a.tapering;
+        acc[1] += by * a.tapering;
+        acc[2] += bz * a.tapering;
+        acc[3] += ((double)a.Ex[ir] - bx) * a.tapering;
+        acc[4] += ((double)a.Ey[ir] - by) * a.tapering;
+        acc[5] += ((double)a.Ez[ir] - bz) * a.tapering;
+        acc[6] += tx * a.tapering;
+        acc[7] += ty * a.tapering;
+        acc[8] += tz * a.tapering;
+        acc[9] += (double)a.Ex[it] * a.tapering;
+        acc[10] += (double)a.Ey[it] * a.tapering;
+        acc[11] += (double)a.Ez[it] * a.tapering;
+    }
+    __shared__ double red[12][512];
+#pragma unroll
+    for (int c = 0; c < 12; ++c) red[c][threadIdx.x] = acc[c];
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s)
+#pragma unroll
+            for (int c = 0; c < 12; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x < 12) a.out[threadIdx.x] = red[threadIdx.x][0];
+}
+
+
+
+template <typename T>
+__global__ void dft_gather(GatherArgs<T> a) {
+    const int P = a.span1 * a.span2;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= P) return;
+    const int u = q % a.span1, v = q / a.span1;
+    int i, j, k;
+    if (a.type <= 1) { i = a.x1; j = a.y1 + u; k = a.z1 + v; }
+    else if (a.type <= 3) { i = a.x1 + u; j = a.y1; k = a.z1 + v; }
+    else { i = a.x1 + u; j = a.y1 + v; k = a.z1; }
+    const int ip = (i + 1 == a.Nx) ? 0 : i + 1;
+    const int jp = (j + 1 == a.Ny) ? 0 : j + 1;
+    const int kp = (k + 1 == a.Nz) ? 0 : k + 1;
+    auto I = [&](int x, int y, int z) { return x + (long long)y * a.Nx + (long long)z * a.NxNy; };
+    const T ex = (a.Ex[I(i, j, k)] + a.Ex[I(i, jp, k)] + a.Ex[I(i, j, kp)] + a.Ex[I(i, jp, kp)]) / T(4.0);
+    const T ey = (a.Ey[I(i, j, k)] + a.Ey[I(ip, j, k)] + a.Ey[I(i, j, kp)] + a.Ey[I(ip, j, kp)]) / T(4.0);
+    const T ez = (a.Ez[I(i, j, k)] + a.Ez[I(ip, j, k)] + a.Ez[I(i, jp, k)] + a.Ez[I(ip, jp, k)]) / T(4.0);
+    const T hx = (a.Hx[I(i, j, k)] + a.Hx[I(ip, j, k)]) / T(2.0);
+    const T hy = (a.Hy[I(i, j, k)] + a.Hy[I(i, jp, k)]) / T(2.0);
+    const T hz = (a.Hz[I(i, j, k)] + a.Hz[I(i, j, kp)]) / T(2.0);
+    a.S[0 * (long long)P + q] = ex;
+    a.S[1 * (long long)P + q] = ey;
+    a.S[2 * (long long)P + q] = ez;
+    a.S[3 * (long long)P + q] = hx;
+    a.S[4 * (long long)P + q] = hy;
+    a.S[5 * (long long)P + q] = hz;
+}
+
+
+
+// s_curve (src/common/mathUT.cpp:1186-1193)
+__device__ __forceinline__ double s_curve_dev(double x, double xmin, double xmax) {
+    const double u = (x - xmin) / (xmax - xmin);
+    if (u <= 0) return 0;
+    if (u >= 1.0) return 1.0;
+    return u * u * (3.0 - 2.0 * u);
+}
+
+__global__ void dft_phasors(PhasorArgs a) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.nk * a.nl) return;
+    const int kk = t / a.nl, l = t % a.nl;
+    const int step = a.step0 + kk;
+    // tapering_E/H in effect at `step` were set after feeding step-1.
+    double tE = 1.0, tH = 1.0;
+    if (step - 1 >= a.Nt - a.Ntap && step >= 1) {
+        tE = s_curve_dev(step - 1, a.Nt - 1.0, a.Nt - a.Ntap);
+        tH = s_curve_dev(step - 1 + 0.5, a.Nt - 1.0, a.Nt - a.Ntap);
+    }
+    const double w = a.w[l];
+    double sE, cE, sH, cH;
+    sincos(w * step * a.Dt, &sE, &cE);
+    sincos(w * (step + 0.5) * a.Dt, &sH, &cH);
+    a.WE[t] = make_double2(tE * cE, tE * sE);
+    a.WH[t] = make_double2(tH * cH, tH * sH);
+}
+
+
+
+
+// grid: (ceil(P/128), ceil(nl/kDftFTile), 6); block 128
+template <typename T>
+__global__ void __launch_bounds__(128) dft_accumulate(AccumArgs<T> a) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int l0 = blockIdx.y * kDftFTile;
+    const int c = blockIdx.z;
+    const double2 *W = (c < 3) ? a.WE : a.WH;
+    __shared__ double2 sw[kDftKTile][kDftFTile];
+    double re[kDftFTile], im[kDftFTile];
+#pragma unroll
+    for (int f = 0; f < kDftFTile; ++f) { re[f] = 0; im[f] = 0; }
+    for (int kt = 0; kt < a.nk; kt += kDftKTile) {
+        __syncthreads();
+        for (int t = threadIdx.x; t < kDftKTile * kDftFTile; t += blockDim.x) {
+            const int kk = kt + t / kDftFTile, l = l0 + t % kDftFTile;
+            sw[t / kDftFTile][t % kDftFTile] = (kk < a.nk && l < a.nl) ? W[kk * a.nl + l] : make_double2(0, 0);
+        }
+        __syncthreads();
+        if (p < a.P) {
+            const int kend = min(kDftKTile, a.nk - kt);
+            for (int kk = 0; kk < kend; ++kk) {
+                const double s = (double)a.S[((long long)(kt + kk) * 6 + c) * a.P + p];
+#pragma unroll
+                for (int f = 0; f < kDftFTile; ++f) {
+                    re[f] = re[f] + s * sw[kk][f].x;
+                    im[f] = im[f] + s * sw[kk][f].y;
+                }
+            }
+        }
+    }
+    if (p >= a.P) return;
+#pragma unroll
+    for (int f = 0; f < kDftFTile; ++f) {
+        const int l = l0 + f;
+        if (l < a.nl) {
+            double2 *q = a.acc + ((long long)c * a.nl + l) * a.P + p;
+            double2 v = *q;
+            v.x = v.x + re[f];
+            v.y = v.y + im[f];
+            *q = v;
+        }
+    }
+}
+
+
+
+// One block per wavelength; deterministic reduction.
+__global__ void __launch_bounds__(256) flux_reduce(FluxArgs a) {
+    const int l = blockIdx.x;
+    double sx = 0, sy = 0, sz = 0;
+    const double2 *ex = a.acc + ((long long)0 * a.nl + l) * a.P, *ey = a.acc + ((long long)1 * a.nl + l) * a.P;
+    const double2 *ez = a.acc + ((long long)2 * a.nl + l) * a.P, *hx = a.acc + ((long long)3 * a.nl + l) * a.P;
+    const double2 *hy = a.acc + ((long long)4 * a.nl + l) * a.P, *hz = a.acc + ((long long)5 * a.nl + l) * a.P;
+    for (int p = threadIdx.x; p < a.P; p += blockDim.x) {
+        const double2 Ex = ex[p], Ey = ey[p], Ez = ez[p], Hx = hx[p], Hy = hy[p], Hz = hz[p];
+        // Re(A*conj(B)) = A.re*B.re + A.im*B.im
+        sx += (Ey.x * Hz.x + Ey.y * Hz.y) - (Ez.x * Hy.x + Ez.y * Hy.y);
+        sy += (Ez.x * Hx.x + Ez.y * Hx.y) - (Ex.x * Hz.x + Ex.y * Hz.y);
+        sz += (Ex.x * Hy.x + Ex.y * Hy.y) - (Ey.x * Hx.x + Ey.y * Hx.y);
+    }
+    __shared__ double red[3][256];
+    red[0][threadIdx.x] = sx;
+    red[1][threadIdx.x] = sy;
+    red[2][threadIdx.x] = sz;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            red[0][threadIdx.x] += red[0][threadIdx.x + s];
+            red[1][threadIdx.x] += red[1][threadIdx.x + s];
+            red[2][threadIdx.x] += red[2][threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double Sx = red[0][0] * a.area_factor, Sy = red[1][0] * a.area_factor, Sz = red[2][0] * a.area_factor;
+        double r = 0;
+        switch (a.type) {
+            case 0: r = Sx; break;
+            case 1: r = -Sx; break;
+            case 2: r = Sy; break;
+            case 3: r = -Sy; break;
+            case 4: r = Sz; break;
+            case 5: r = -Sz; break;
+        }
+        a.out[l] = r;
+    }
+}
+
+}  // namespace aefdtd

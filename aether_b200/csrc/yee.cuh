@@ -1,0 +1,312 @@
+// yee.cuh — fused E and H half-step kernels (one launch per half-step).
+//
+// The E kernel fuses, per cell, the six phases of FDTD::update_E
+// (src/finite_differences/FDTD/core/fdtd_core.cpp:1163-1218 driving
+// fdtd_threads.cpp:32-150): recursive-convolution "ante" update with E^n
+// (mats_RC.cpp:21-36), the Yee curl update (fdtd_core.cpp:363-541), the RC
+// apply (mats_RC.cpp:38-50), the CPML psi updates and PEC planes in the
+// reference's order (fdtd_pml.cpp:504-735), then the normal-mode plane
+// injection (normal_incidence.cpp:338-342) or Oscillator boxes
+// (sc_oscillator.cpp:34-67). The H kernel fuses advHx/Hy/Hz
+// (fdtd_core.cpp:546-698), app_pml_H* (fdtd_pml.cpp:737-929) and the H plane
+// injection (normal_incidence.cpp:353-357). Every phase of the reference only
+// reads the other field family plus the cell's own state, so fusing them per
+// cell is exact.
+//
+// Threads own one (i, j) column and march kchunk planes along z, carrying the
+// z-1 (E kernel) or z+1 (H kernel) plane in registers; x and y neighbours
+// come through L1. Loads along x are coalesced (x is the fastest index).
+//
+// FP64 instantiation (compiled with --fmad=false): operation order equals the
+// reference's expression order, so results are bit-identical to the CPU
+// core. FP32 instantiation: FP32 fields and state; CPML b and RC Crec are
+// applied as (b-1) and (Crec-1) to keep their small decrements exact.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <type_traits>
+
+#include "aefdtd_dev.hpp"
+
+namespace aefdtd {
+
+template <typename T> struct Exact { static constexpr bool value = std::is_same<T, double>::value; };
+
+// psi_new = b*psi + c*diff (FP64, reference order) or psi + ((b-1)*psi + c*diff) (FP32)
+template <typename T> __device__ __forceinline__ T cpml_rec(T b, T psi, T c, T diff) {
+    if constexpr (Exact<T>::value) return b * psi + c * diff;
+    else return psi + (b * psi + c * diff);
+}
+
+template <typename T, typename Tid>
+__global__ void __launch_bounds__(128) e_half_step(StepArgs<T, Tid> a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= a.Nx || j >= a.Ny) return;
+    const int k0 = blockIdx.z * a.kchunk;
+    const int k1 = min(a.Nz, k0 + a.kchunk);
+    const long long NxNy = a.NxNy;
+    const int im = (i == 0) ? a.Nx - 1 : i - 1;
+    const int jm = (j == 0) ? a.Ny - 1 : j - 1;
+    const long long col = i + (long long)j * a.Nx;
+    const long long colx = im + (long long)j * a.Nx;
+    const long long coly = i + (long long)jm * a.Nx;
+    const T ikx = a.ikx[i];
+    const T iky = a.iky[j];
+
+    // E-side CPML index ranges: [1, pml_m) and [N - pml_p + 1, N) (fdtd_pml.cpp:518,527,547,559)
+    const bool xe = a.px && ((i >= 1 && i < a.pml_xm) || (i >= a.Nx - a.pml_xp + 1));
+    const bool ye = a.py && ((j >= 1 && j < a.pml_ym) || (j >= a.Ny - a.pml_yp + 1));
+    const int nxs = a.pml_xm + a.pml_xp, nys = a.pml_ym + a.pml_yp, nzs = a.pml_zm + a.pml_zp;
+    const int xn = (i < a.pml_xm) ? i : i - (a.Nx - a.pml_xp) + a.pml_xm;
+    const int yn = (j < a.pml_ym) ? j : j - (a.Ny - a.pml_yp) + a.pml_ym;
+    T bxi = 0, cxi = 0, byj = 0, cyj = 0;
+    if (xe) { bxi = a.bx[i]; cxi = a.cx[i]; }
+    if (ye) { byj = a.by[j]; cyj = a.cy[j]; }
+
+    const int kmi = (k0 == 0) ? a.Nz - 1 : k0 - 1;
+    T hx_km = a.Hx[col + kmi * NxNy];
+    T hy_km = a.Hy[col + kmi * NxNy];
+
+    for (int k = k0; k < k1; ++k) {
+        const long long id = col + k * NxNy;
+        const T hx = a.Hx[id], hy = a.Hy[id], hz = a.Hz[id];
+        const T hz_jm = a.Hz[coly + k * NxNy], hx_jm = a.Hx[coly + k * NxNy];
+        const T hz_im = a.Hz[colx + k * NxNy], hy_im = a.Hy[colx + k * NxNy];
+        const T ex = a.Ex[id], ey = a.Ey[id], ez = a.Ez[id];
+        const int m = a.mat[id];
+        const MatCoef<T> c = a.coef[m];
+        const T ikz = a.ikz[k];
+
+        // Recursive-convolution "ante" with E^n; sums of Re(psi) per component.
+        T s0 = 0, s1 = 0, s2 = 0;
+        bool disp = false;
+        if (a.disp != nullptr) {
+            const DispInfo d = a.disp[m];
+            if (d.np > 0) {
+                disp = true;
+                const long long q = (i - d.x1) + (long long)(j - d.y1) * d.xs + (long long)(k - d.z1) * d.xs * d.ys;
+                Cplx<T> *P = a.psi + d.psi_off + q;
+                for (int p = 0; p < d.np; ++p) {
+                    const Cplx<T> cr = a.crec[d.pole_off + p];
+                    const Cplx<T> dc = a.dchi[d.pole_off + p];
+                    const T ev[3] = {ex, ey, ez};
+#pragma unroll
+                    for (int dd = 0; dd < 3; ++dd) {
+                        Cplx<T> *pp = P + (long long)(3 * p + dd) * d.box;
+                        const Cplx<T> v = *pp;
+                        Cplx<T> r;
+                        if constexpr (Exact<T>::value) {
+                            // Crec*psi + Dchi*E with std::complex<double> rounding order
+                            r.re = (cr.re * v.re - cr.im * v.im) + dc.re * ev[dd];
+                            r.im = (cr.re * v.im + cr.im * v.re) + dc.im * ev[dd];
+                        } else {
+                            // (Crec-1) stored: psi + ((Crec-1)*psi + Dchi*E)
+                            r.re = v.re + ((cr.re * v.re - cr.im * v.im) + dc.re * ev[dd]);
+                            r.im = v.im + ((cr.re * v.im + cr.im * v.re) + dc.im * ev[dd]);
+                        }
+                        *pp = r;
+                        if (dd == 0) s0 = s0 + r.re;
+                        else if (dd == 1) s1 = s1 + r.re;
+                        else s2 = s2 + r.re;
+                    }
+                }
+            }
+        }
+
+        const T dHz_y = hz - hz_jm, dHy_z = hy - hy_km;
+        const T dHx_z = hx - hx_km, dHz_x = hz - hz_im;
+        const T dHy_x = hy - hy_im, dHx_y = hx - hx_jm;
+        T nex = (c.C1 * ex + (c.C2y * iky) * dHz_y) - (c.C2z * ikz) * dHy_z;
+        T ney = (c.C1 * ey + (c.C2z * ikz) * dHx_z) - (c.C2x * ikx) * dHz_x;
+        T nez = (c.C1 * ez + (c.C2x * ikx) * dHy_x) - (c.C2y * iky) * dHx_y;
+        if (disp) {
+            nex += c.C3 * s0;
+            ney += c.C3 * s1;
+            nez += c.C3 * s2;
+        }
+
+        // CPML and PEC planes in app_pml_Ex / Ey / Ez order.
+        const bool ze = a.pz && ((k >= 1 && k < a.pml_zm) || (k >= a.Nz - a.pml_zp + 1));
+        const int zn = (k < a.pml_zm) ? k : k - (a.Nz - a.pml_zp) + a.pml_zm;
+        T bzk = 0, czk = 0;
+        if (ze) { bzk = a.bz[k]; czk = a.cz[k]; }
+        // Ex: y block, then z block
+        if (ye) {
+            T *pp = a.psi_y0 + i + (long long)yn * a.Nx + (long long)k * a.Nx * nys;
+            const T ps = cpml_rec(byj, *pp, cyj, dHz_y);
+            *pp = ps;
+            nex += c.C4 * ps;
+        }
+        if (a.py && j == 0) nex = 0;
+        if (ze) {
+            T *pp = a.psi_z0 + col + (long long)zn * NxNy;
+            const T ps = cpml_rec(bzk, *pp, czk, dHy_z);
+            *pp = ps;
+            nex -= c.C4 * ps;
+        }
+        if (a.pz && k == 0) nex = 0;
+        // Ey: x block, then z block
+        if (xe) {
+            T *pp = a.psi_x0 + xn + (long long)j * nxs + (long long)k * nxs * a.Ny;
+            const T ps = cpml_rec(bxi, *pp, cxi, dHz_x);
+            *pp = ps;
+            ney -= c.C4 * ps;
+        }
+        if (a.px && i == 0) ney = 0;
+        if (ze) {
+            T *pp = a.psi_z1 + col + (long long)zn * NxNy;
+            const T ps = cpml_rec(bzk, *pp, czk, dHx_z);
+            *pp = ps;
+            ney += c.C4 * ps;
+        }
+        if (a.pz && k == 0) ney = 0;
+        // Ez: x block, then y block
+        if (xe) {
+            T *pp = a.psi_x1 + xn + (long long)j * nxs + (long long)k * nxs * a.Ny;
+            const T ps = cpml_rec(bxi, *pp, cxi, dHy_x);
+            *pp = ps;
+            nez += c.C4 * ps;
+        }
+        if (a.px && i == 0) nez = 0;
+        if (ye) {
+            T *pp = a.psi_y1 + i + (long long)yn * a.Nx + (long long)k * a.Nx * nys;
+            const T ps = cpml_rec(byj, *pp, cyj, dHx_y);
+            *pp = ps;
+            nez -= c.C4 * ps;
+        }
+        if (a.py && j == 0) nez = 0;
+
+        // Normal-incidence plane injection after update_E (normal_incidence.cpp:338-342)
+        if (k == a.kinj) {
+            nex = nex - a.inj_a;
+            ney = ney + a.inj_b;
+        }
+        // Oscillator boxes after update_E (sc_oscillator.cpp:43-63)
+        for (int s = 0; s < a.nsrc; ++s) {
+            const int *b = a.src_box[s];
+            if (i >= b[0] && i < b[1] && j >= b[2] && j < b[3] && k >= b[4] && k < b[5]) {
+                if (a.src_comp[s] == 0) nex += a.src_val[s];
+                else if (a.src_comp[s] == 1) ney += a.src_val[s];
+                else nez += a.src_val[s];
+            }
+        }
+
+        a.Ex[id] = nex;
+        a.Ey[id] = ney;
+        a.Ez[id] = nez;
+        hx_km = hx;
+        hy_km = hy;
+    }
+}
+
+template <typename T, typename Tid>
+__global__ void __launch_bounds__(128) h_half_step(StepArgs<T, Tid> a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= a.Nx || j >= a.Ny) return;
+    const int k0 = blockIdx.z * a.kchunk;
+    const int k1 = min(a.Nz, k0 + a.kchunk);
+    const long long NxNy = a.NxNy;
+    const int ip = (i == a.Nx - 1) ? 0 : i + 1;
+    const int jp = (j == a.Ny - 1) ? 0 : j + 1;
+    const long long col = i + (long long)j * a.Nx;
+    const long long colx = ip + (long long)j * a.Nx;
+    const long long coly = i + (long long)jp * a.Nx;
+    const T ax = a.dtdmx * a.ikx[i];
+    const T ay = a.dtdmy * a.iky[j];
+
+    // H-side CPML index ranges: [0, pml_m) and [N - pml_p, N - 1) (fdtd_pml.cpp:750,756,775,784)
+    const bool xh = a.px && ((i < a.pml_xm) || (i >= a.Nx - a.pml_xp && i < a.Nx - 1));
+    const bool yh = a.py && ((j < a.pml_ym) || (j >= a.Ny - a.pml_yp && j < a.Ny - 1));
+    const int nxs = a.pml_xm + a.pml_xp, nys = a.pml_ym + a.pml_yp;
+    const int xn = (i < a.pml_xm) ? i : i - (a.Nx - a.pml_xp) + a.pml_xm;
+    const int yn = (j < a.pml_ym) ? j : j - (a.Ny - a.pml_yp) + a.pml_ym;
+    T bxi = 0, cxi = 0, byj = 0, cyj = 0;
+    if (xh) { bxi = a.bx[i]; cxi = a.cx[i]; }
+    if (yh) { byj = a.by[j]; cyj = a.cy[j]; }
+
+    T ex = a.Ex[col + k0 * NxNy];
+    T ey = a.Ey[col + k0 * NxNy];
+
+    for (int k = k0; k < k1; ++k) {
+        const long long id = col + k * NxNy;
+        const int kp = (k == a.Nz - 1) ? 0 : k + 1;
+        const T ex_kp = a.Ex[col + kp * NxNy], ey_kp = a.Ey[col + kp * NxNy];
+        const T ez = a.Ez[id];
+        const T ez_jp = a.Ez[coly + k * NxNy], ex_jp = a.Ex[coly + k * NxNy];
+        const T ez_ip = a.Ez[colx + k * NxNy], ey_ip = a.Ey[colx + k * NxNy];
+        const T hx = a.Hx[id], hy = a.Hy[id], hz = a.Hz[id];
+        const T az = a.dtdmz * a.ikz[k];
+
+        const T dEy_z = ey_kp - ey, dEz_y = ez_jp - ez;
+        const T dEz_x = ez_ip - ez, dEx_z = ex_kp - ex;
+        const T dEx_y = ex_jp - ex, dEy_x = ey_ip - ey;
+        T nhx = hx + (az * dEy_z - ay * dEz_y);
+        T nhy = hy + (ax * dEz_x - az * dEx_z);
+        T nhz = hz + (ay * dEx_y - ax * dEy_x);
+
+        const bool zh = a.pz && ((k < a.pml_zm) || (k >= a.Nz - a.pml_zp && k < a.Nz - 1));
+        const int zn = (k < a.pml_zm) ? k : k - (a.Nz - a.pml_zp) + a.pml_zm;
+        T bzk = 0, czk = 0;
+        if (zh) { bzk = a.bz[k]; czk = a.cz[k]; }
+        // Hx: y block, then z block
+        if (yh) {
+            T *pp = a.psi_y0 + i + (long long)yn * a.Nx + (long long)k * a.Nx * nys;
+            const T ps = cpml_rec(byj, *pp, cyj, dEz_y);
+            *pp = ps;
+            nhx -= a.dtm * ps;
+        }
+        if (a.py && j == a.Ny - 1) nhx = 0;
+        if (zh) {
+            T *pp = a.psi_z0 + col + (long long)zn * NxNy;
+            const T ps = cpml_rec(bzk, *pp, czk, dEy_z);
+            *pp = ps;
+            nhx += a.dtm * ps;
+        }
+        if (a.pz && k == a.Nz - 1) nhx = 0;
+        // Hy: x block, then z block
+        if (xh) {
+            T *pp = a.psi_x0 + xn + (long long)j * nxs + (long long)k * nxs * a.Ny;
+            const T ps = cpml_rec(bxi, *pp, cxi, dEz_x);
+            *pp = ps;
+            nhy += a.dtm * ps;
+        }
+        if (a.px && i == a.Nx - 1) nhy = 0;
+        if (zh) {
+            T *pp = a.psi_z1 + col + (long long)zn * NxNy;
+            const T ps = cpml_rec(bzk, *pp, czk, dEx_z);
+            *pp = ps;
+            nhy -= a.dtm * ps;
+        }
+        if (a.pz && k == a.Nz - 1) nhy = 0;
+        // Hz: x block, then y block
+        if (xh) {
+            T *pp = a.psi_x1 + xn + (long long)j * nxs + (long long)k * nxs * a.Ny;
+            const T ps = cpml_rec(bxi, *pp, cxi, dEy_x);
+            *pp = ps;
+            nhz -= a.dtm * ps;
+        }
+        if (a.px && i == a.Nx - 1) nhz = 0;
+        if (yh) {
+            T *pp = a.psi_y1 + i + (long long)yn * a.Nx + (long long)k * a.Nx * nys;
+            const T ps = cpml_rec(byj, *pp, cyj, dEx_y);
+            *pp = ps;
+            nhz += a.dtm * ps;
+        }
+        if (a.py && j == a.Ny - 1) nhz = 0;
+
+        // H plane injection after update_H (normal_incidence.cpp:353-357)
+        if (k == a.kinj) {
+            nhx = nhx + a.inj_a;
+            nhy = nhy - a.inj_b;
+        }
+        a.Hx[id] = nhx;
+        a.Hy[id] = nhy;
+        a.Hz[id] = nhz;
+        ex = ex_kp;
+        ey = ey_kp;
+    }
+}
+
+}  // namespace aefdtd

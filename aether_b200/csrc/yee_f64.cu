@@ -1,0 +1,11 @@
+// FP64 instantiation of the fused half-step kernels. Built with --fmad=false
+// so that every multiply and add rounds separately, in the reference's order.
+#include "kernels.hpp"
+#include "yee.cuh"
+
+namespace aefdtd {
+void launch_e(const StepArgs<double, uint8_t> &a, dim3 g, dim3 b, cudaStream_t s) { e_half_step<<<g, b, 0, s>>>(a); }
+void launch_e(const StepArgs<double, uint16_t> &a, dim3 g, dim3 b, cudaStream_t s) { e_half_step<<<g, b, 0, s>>>(a); }
+void launch_h(const StepArgs<double, uint8_t> &a, dim3 g, dim3 b, cudaStream_t s) { h_half_step<<<g, b, 0, s>>>(a); }
+void launch_h(const StepArgs<double, uint16_t> &a, dim3 g, dim3 b, cudaStream_t s) { h_half_step<<<g, b, 0, s>>>(a); }
+}  // namespace aefdtd

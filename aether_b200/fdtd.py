@@ -1,0 +1,189 @@
+"""Simulation handle over the C ABI, and `run(scene)` — the counterpart of the
+reference mode drivers FDTD_normal_incidence / mode_default_fdtd
+(src/finite_differences/FDTD/modes/normal_incidence.cpp:161-607,
+default_fdtd.cpp:24-210) for a Scene."""
+from __future__ import annotations
+
+import ctypes as C
+import time
+
+import numpy as np
+
+from . import _abi as A
+from ._lib import check, load
+
+_P = C.POINTER
+
+
+class Simulation:
+    """One FDTD grid on one GPU (the reference's `FDTD` object plus its mode
+    driver's sensors and sources)."""
+
+    def __init__(self, grid: A.GridDesc):
+        self._lib = load()
+        self._h = C.c_void_p()
+        st = self._lib.aefdtd_create(C.byref(grid), C.byref(self._h))
+        check(st, None)
+        self.grid = grid
+        self.sensor_nl = []
+
+    # -- lifecycle
+    def close(self):
+        if self._h:
+            self._lib.aefdtd_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _c(self, st):
+        check(st, self._h)
+
+    # -- setup
+    def dims(self) -> A.Dims:
+        d = A.Dims()
+        self._c(self._lib.aefdtd_get_dims(self._h, C.byref(d)))
+        return d
+
+    def set_material_map(self, m: np.ndarray):
+        m = np.ascontiguousarray(m, dtype=np.uint32)
+        self._c(self._lib.aefdtd_set_material_map(self._h, m.ctypes.data_as(_P(C.c_uint32)), m.size))
+
+    def set_material(self, idx: int, mat: A.MaterialDesc):
+        self._c(self._lib.aefdtd_set_material(self._h, idx, C.byref(mat)))
+
+    def setup_normal(self, nd: A.NormalDesc):
+        self._c(self._lib.aefdtd_setup_normal(self._h, C.byref(nd)))
+        self.normal_nl = nd.nl
+
+    def add_oscillator(self, src: A.SourceDesc) -> int:
+        i = C.c_int32()
+        self._c(self._lib.aefdtd_add_oscillator(self._h, C.byref(src), C.byref(i)))
+        return i.value
+
+    def add_planar_sensor(self, s: A.SensorDesc) -> int:
+        i = C.c_int32()
+        self._c(self._lib.aefdtd_add_planar_sensor(self._h, C.byref(s), C.byref(i)))
+        self.sensor_nl.append(s.nl)
+        return i.value
+
+    # -- stepping
+    def step(self, n: int):
+        self._c(self._lib.aefdtd_step(self._h, int(n)))
+
+    def synchronize(self):
+        self._c(self._lib.aefdtd_synchronize(self._h))
+
+    def reset(self):
+        self._c(self._lib.aefdtd_reset(self._h))
+
+    def enable_timing(self, on=True):
+        self._c(self._lib.aefdtd_enable_timing(self._h, 1 if on else 0))
+
+    def timings(self):
+        e, h, s = C.c_double(), C.c_double(), C.c_double()
+        self._c(self._lib.aefdtd_get_timings(self._h, C.byref(e), C.byref(h), C.byref(s)))
+        return e.value, h.value, s.value
+
+    def stream_ptr(self) -> int:
+        p = C.c_void_p()
+        self._c(self._lib.aefdtd_get_stream(self._h, C.byref(p)))
+        return p.value or 0
+
+    def launch_count(self) -> int:
+        n = C.c_uint64()
+        self._c(self._lib.aefdtd_get_launch_count(self._h, C.byref(n)))
+        return n.value
+
+    # -- results
+    def field(self, comp: int) -> np.ndarray:
+        d = self.dims()
+        out = np.empty(d.nx * d.ny * d.nz)
+        self._c(self._lib.aefdtd_get_field(self._h, comp, out.ctypes.data_as(_P(C.c_double)), out.size))
+        return out.reshape(d.nz, d.ny, d.nx)
+
+    def fields(self) -> np.ndarray:
+        return np.stack([self.field(c) for c in range(6)])
+
+    def set_field(self, comp: int, values: np.ndarray):
+        v = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        self._c(self._lib.aefdtd_set_field(self._h, comp, v.ctypes.data_as(_P(C.c_double)), v.size))
+
+    def plane_sums(self) -> np.ndarray:
+        n = self.dims().step
+        out = np.empty(12 * n)
+        self._c(self._lib.aefdtd_get_plane_sums(self._h, out.ctypes.data_as(_P(C.c_double)), n))
+        return out.reshape(12, n)
+
+    def normal_spectra(self) -> np.ndarray:
+        out = np.empty(15 * self.normal_nl)
+        self._c(self._lib.aefdtd_get_normal_spectra(self._h, out.ctypes.data_as(_P(C.c_double)), self.normal_nl))
+        return out.reshape(self.normal_nl, 15)
+
+    def sensor_flux(self, sid: int) -> np.ndarray:
+        nl = self.sensor_nl[sid]
+        out = np.empty(nl)
+        self._c(self._lib.aefdtd_get_sensor_flux(self._h, sid, out.ctypes.data_as(_P(C.c_double)), nl))
+        return out
+
+    def sensor_dft(self, sid: int) -> np.ndarray:
+        s1, s2, nl = C.c_int32(), C.c_int32(), C.c_int32()
+        self._c(self._lib.aefdtd_get_sensor_shape(self._h, sid, C.byref(s1), C.byref(s2), C.byref(nl)))
+        out = np.empty(6 * s1.value * s2.value * nl.value * 2)
+        self._c(self._lib.aefdtd_get_sensor_dft(self._h, sid, out.ctypes.data_as(_P(C.c_double)), out.size))
+        z = out.view(np.complex128)
+        return z.reshape(6, nl.value, s2.value, s1.value)
+
+
+def build_simulation(scene) -> Simulation:
+    """Creates the device simulation of a Scene (grid, map, materials,
+    excitation, sensors), in the order of the reference drivers."""
+    sim = Simulation(scene.grid)
+    try:
+        sim.set_material_map(scene.map)
+        for i, m in enumerate(scene.materials):
+            sim.set_material(i, m)
+        if scene.grid.mode == A.MODE_NORMAL:
+            sim.setup_normal(scene.normal)
+        for s in scene.sources:
+            sim.add_oscillator(s)
+        for s in scene.sensors:
+            sim.add_planar_sensor(s)
+    except Exception:
+        sim.close()
+        raise
+    return sim
+
+
+def run(scene, nsteps=None, want_fields=True):
+    """Runs a Scene on the GPU and returns the same dict as the oracle
+    runner: fields (6, nz, ny, nx) as float64, plane_sums, spectra, flux,
+    dims, seconds (device time of the steps, host clock)."""
+    nsteps = scene.nsteps if nsteps is None else nsteps
+    with build_simulation(scene) as sim:
+        t0 = time.perf_counter()
+        sim.step(nsteps)
+        sim.synchronize()
+        secs = time.perf_counter() - t0
+        d = sim.dims()
+        out = {"dims": np.array([d.nx, d.ny, d.nz, d.xs_s, d.xs_e, d.ys_s, d.ys_e, d.zs_s, d.zs_e, d.n_materials]),
+               "seconds": secs}
+        out["fields"] = sim.fields() if want_fields else None
+        if scene.grid.mode == A.MODE_NORMAL:
+            out["plane_sums"] = sim.plane_sums()
+            out["spectra"] = sim.normal_spectra() if nsteps >= 2 else None
+        else:
+            out["plane_sums"] = None
+            out["spectra"] = None
+        out["flux"] = [sim.sensor_flux(i) for i in range(len(scene.sensors))]
+        out["launches"] = sim.launch_count()
+        return out

@@ -1,0 +1,72 @@
+"""Algorithmic byte counts of the fused half-step kernels (the roofline
+numerator) and the Gcell-updates/s metric.
+
+Per interior cell-update the E and H half-steps together move 18*s + b_id
+bytes (s = 8 for FP64, 4 for FP32; b_id = 1 or 2): each kernel reads its own
+3 components and the other family's 3 components once and writes its 3
+components, assuming perfect neighbour reuse, and the E kernel reads the
+material id. Add-ons: per CPML axis a cell lies in, the E (H) kernel
+read-modify-writes two psi arrays (+4*s each side); a dispersive cell with
+Np poles read-modify-writes 3*Np complex psi values in the E kernel
+(+12*Np*s)."""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _abi as A
+
+
+def cell_counts(scene):
+    """Counts cells in each CPML range and dispersive cells of the total grid."""
+    nx, ny, nz = scene.total_dims()
+    pml, pad = scene.padded_faces()
+    g = scene.grid
+
+    def ranges(n, pm, pp, e_side):
+        idx = np.arange(n)
+        if not (pm or pp):
+            return np.zeros(n, bool)
+        if e_side:
+            return ((idx >= 1) & (idx < pm)) | (idx >= n - pp + 1)
+        return (idx < pm) | ((idx >= n - pp) & (idx < n - 1))
+
+    out = {"cells": nx * ny * nz}
+    for side in ("E", "H"):
+        e = side == "E"
+        rx = ranges(nx, pml[0], pml[1], e).sum() * ny * nz
+        ry = ranges(ny, pml[2], pml[3], e).sum() * nx * nz
+        rz = ranges(nz, pml[4], pml[5], e).sum() * nx * ny
+        out[f"pml_{side}"] = int(rx + ry + rz)
+    # dispersive cells: structure map cells (pads replicate edge slices)
+    poles = np.zeros(len(scene.materials), np.int64)
+    for i, m in enumerate(scene.materials):
+        poles[i] = m.n_debye + m.n_drude + m.n_lorentz + m.n_critpoint
+    total_map = expand_map(scene)
+    out["disp_pole_cells"] = int(poles[np.minimum(total_map, len(poles) - 1)].sum())
+    out["id_bytes"] = 1 if total_map.max() < 256 else 2
+    return out
+
+
+def expand_map(scene):
+    """Total-grid material map with pad/PML replication (FDTD::set_matsgrid)."""
+    nx, ny, nz = scene.total_dims()
+    pml, pad = scene.padded_faces()
+    xs, ys, zs = pml[0] + pad[0], pml[2] + pad[2], pml[4] + pad[4]
+    m = scene.map
+    xi = np.clip(np.arange(nx) - xs, 0, m.shape[2] - 1)
+    yi = np.clip(np.arange(ny) - ys, 0, m.shape[1] - 1)
+    zi = np.clip(np.arange(nz) - zs, 0, m.shape[0] - 1)
+    return m[np.ix_(zi, yi, xi)]
+
+
+def kernel_bytes(scene, precision=None):
+    """Algorithmic bytes per launch of the E and H half-step kernels."""
+    s = 8 if (scene.grid.precision if precision is None else precision) == A.FP64 else 4
+    c = cell_counts(scene)
+    e = c["cells"] * (9 * s + c["id_bytes"]) + c["pml_E"] * 4 * s + c["disp_pole_cells"] * 12 * s
+    h = c["cells"] * 9 * s + c["pml_H"] * 4 * s
+    return {"E": int(e), "H": int(h), "cells": c["cells"], "detail": c, "elem_bytes": s}
+
+
+def gcells(cells, steps, seconds):
+    return cells * steps / seconds / 1e9

@@ -1,0 +1,344 @@
+"""Benchmark of the FDTD time-stepping core on one B200.
+
+Workload: the dispersive unit cell — 128x128x256 total cells at 2.5 nm,
+periodic x/y, 24-cell CPML on z, a 40 nm gold-like sphere (Drude + 2 critical
+points) on an n=1.45 substrate, normal-incidence 400-1000 nm pulse, two planar
+flux sensors at 201 wavelengths with K=64 buffered steps per DFT block
+(seeded synthetic geometry; no dataset). One bench step = 64 FDTD time steps
+(one DFT block), inputs resident in HBM. The FP32 path is the headline value;
+the FP64 path is measured alongside.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Metric: Gcell-updates/s = total cells x time steps / s / 1e9."""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+STEPS_PER_BENCH_STEP = 64
+METRIC = "Gcell-updates/s"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def workload(precision):
+    from aether_b200 import configs as CF
+    return CF.sphere_scene(nx=128, ny=128, nz_total=256, dx=2.5e-9, pml=24, radius=40e-9, nsteps=20000,
+                           nl=201, precision=precision)
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.25)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.15)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                p = [x.strip() for x in line.split(",")]
+                if len(p) >= 9:
+                    rows.append(p)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except Exception:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel, precision):
+    """DRAM bytes per launch from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    try:
+        for line in open(path):
+            p = line.split()
+            if len(p) >= 3 and not line.startswith("#") and p[0] == kernel and p[1] == precision:
+                return float(p[2])
+    except Exception:
+        pass
+    return None
+
+
+def run_gpu_arm(args):
+    import torch
+    from aether_b200 import _abi as A
+    from aether_b200 import fdtd
+    from aether_b200 import metrics as MT
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+
+    # Replicas only: every rank advances its own copy of the workload; no
+    # data-path collective exists on this path.
+    results = {}
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
+    for prec_name, prec in (("fp32", A.FP32), ("fp64", A.FP64)):
+        scene = workload(prec)
+        scene.grid.device = dev
+        sim = fdtd.build_simulation(scene)
+        ext = torch.cuda.ExternalStream(sim.stream_ptr())
+        cells = scene.cells
+        kb = MT.kernel_bytes(scene)
+        for _ in range(args.warmup):
+            sim.step(STEPS_PER_BENCH_STEP)
+        sim.synchronize()
+        launches0 = sim.launch_count()
+        times = []
+        sim.enable_timing(True)
+        e_ms = h_ms = s_ms = 0.0
+        with ClockSampler(dev) as cs:
+            if ws > 1:
+                torch.distributed.barrier()
+            torch.cuda.synchronize()
+            for _ in range(args.steps):
+                with torch.cuda.stream(ext):
+                    flush.zero_()   # L2 flush between timed steps
+                    ev0 = torch.cuda.Event(enable_timing=True)
+                    ev1 = torch.cuda.Event(enable_timing=True)
+                    ev0.record(ext)
+                sim.step(STEPS_PER_BENCH_STEP)
+                with torch.cuda.stream(ext):
+                    ev1.record(ext)
+                a, b, c = sim.timings()
+                e_ms += a; h_ms += b; s_ms += c
+                times.append((ev0, ev1))
+            torch.cuda.synchronize()
+            if ws > 1:
+                torch.distributed.barrier()
+        sim.enable_timing(False)
+        launches = sim.launch_count() - launches0
+        ms = sum(a.elapsed_time(b) for a, b in times)
+        if ws > 1:
+            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        nsteps = args.steps * STEPS_PER_BENCH_STEP
+        results[prec_name] = {
+            "gcells": MT.gcells(cells, nsteps, ms / 1e3) * ws,
+            "ms_per_step": ms / args.steps,
+            "e_ms": e_ms / nsteps, "h_ms": h_ms / nsteps, "s_ms": s_ms / nsteps,
+            "bytes": kb, "launches": launches, "clocks": cs.summary(), "cells": cells,
+        }
+        sim.close()
+        log(f"[{prec_name}] {results[prec_name]['gcells']:.2f} Gcell/s  E {e_ms / nsteps * 1e3:.1f} us  "
+            f"H {h_ms / nsteps * 1e3:.1f} us  sensors {s_ms / nsteps * 1e3:.1f} us per time step")
+    return results, ws, rank
+
+
+def e2e_job(precision, nsteps):
+    """One complete job through the public API from host buffers: geometry and
+    materials uploaded, all steps run, spectra read back."""
+    from aether_b200 import fdtd
+    scene = workload(precision)
+    t0 = time.perf_counter()
+    with fdtd.build_simulation(scene) as sim:
+        sim.step(nsteps)
+        spec = sim.normal_spectra()
+        flux = [sim.sensor_flux(i) for i in range(len(scene.sensors))]
+    dt = time.perf_counter() - t0
+    h2d = scene.map.nbytes + sum(len(bytes(m)) for m in scene.materials)
+    d2h = spec.nbytes + sum(f.nbytes for f in flux) + 12 * 8 * nsteps
+    return dt, h2d, d2h, scene.cells
+
+
+def cpu_baseline(scene_fn, seconds_budget=20.0):
+    """The reference's own FDTD core (oracle/_ref, compiled from source) on a
+    bounded sample of the workload on the host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib
+    if not oracle_lib.available("ref"):
+        which, kind = "port", "port"
+    else:
+        which, kind = "ref", "reference"
+    from aether_b200 import _abi as A
+    scene = scene_fn(A.FP64)
+    nsteps = 4
+    r = oracle_lib.run(scene, which, nsteps=nsteps, want_fields=False)
+    per_step = r["seconds"] / nsteps
+    n2 = max(4, min(64, int(seconds_budget / max(per_step, 1e-6))))
+    r = oracle_lib.run(scene, which, nsteps=n2, want_fields=False)
+    cores = 1
+    if kind == "reference":
+        import ctypes as C
+        lib = C.CDLL(oracle_lib.REF_PATH)
+        cores = int(lib.aeref_threads())
+    val = scene.cells * n2 / r["seconds"] / 1e9
+    return {"value": val, "unit": METRIC, "cores": cores, "kind": kind,
+            "sample": f"{n2} time steps of the full 128x128x256 FP64 workload incl. 2x201-lambda DFT sensors "
+                      f"(time loop only, {r['seconds']:.2f} s)"}
+
+
+def reference_arm(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib
+    from aether_b200 import _abi as A
+    which = "ref" if oracle_lib.available("ref") else "port"
+    kind = "reference" if which == "ref" else "port"
+    scene = workload(A.FP64)
+    sample_steps = 4
+    for _ in range(args.warmup):
+        oracle_lib.run(scene, which, nsteps=1, want_fields=False)
+    secs = 0.0
+    for _ in range(args.steps):
+        r = oracle_lib.run(scene, which, nsteps=sample_steps, want_fields=False)
+        secs += r["seconds"]
+    nsteps = args.steps * sample_steps
+    val = scene.cells * nsteps / secs / 1e9
+    cores = 1
+    if which == "ref":
+        import ctypes as C
+        cores = int(C.CDLL(oracle_lib.REF_PATH).aeref_threads())
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": METRIC, "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "dispersive unit cell 128x128x256 @2.5nm, gold Drude+2CP sphere r=40nm on "
+                               "n=1.45 substrate, 24-cell CPML z, 2 DFT planes x 201 lambda",
+                   "step": f"{sample_steps} FDTD time steps per bench step (bounded CPU sample)"},
+        "cpu_baseline": {"value": val, "unit": METRIC, "cores": cores, "kind": kind,
+                         "sample": f"{sample_steps} time steps per bench step, reference time loop"},
+        "e2e": {"value": val, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="aefdtd")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+
+    res, ws, rank = run_gpu_arm(args)
+    if rank != 0:
+        return
+    from aether_b200 import _abi as A
+    r32, r64 = res["fp32"], res["fp64"]
+    peak, peak_kind = measured_peaks()
+    e_bytes = r32["bytes"]["E"]
+    achieved = e_bytes / (r32["e_ms"] * 1e-3) / 1e9
+    traffic = profiled_traffic("e_half_step", "fp32")
+    line = {
+        "metric": METRIC, "value": r32["gcells"], "unit": METRIC, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r32["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "dispersive unit cell 128x128x256 @2.5nm, gold Drude+2CP sphere r=40nm on "
+                               "n=1.45 substrate, 24-cell CPML z, normal incidence 400-1000nm, "
+                               "2 DFT planes x 201 lambda, K=64",
+                   "step": f"{STEPS_PER_BENCH_STEP} FDTD time steps (one DFT block)",
+                   "l2": "256 MiB buffer written between timed steps",
+                   "parallelism": f"replicas x{ws}"},
+        "fp64": {"value": r64["gcells"], "ms_per_step": r64["ms_per_step"],
+                 "e_us": r64["e_ms"] * 1e3, "h_us": r64["h_ms"] * 1e3,
+                 "roofline_frac": r64["bytes"]["E"] / (r64["e_ms"] * 1e-3) / 1e9 / peak},
+        "fp32_over_fp64": r32["gcells"] / r64["gcells"],
+        "roofline": {"bound": "hbm", "kernel": "e_half_step<float>", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": traffic, "algorithmic_bytes_per_launch": e_bytes,
+                     "h_half_step_frac": r32["bytes"]["H"] / (r32["h_ms"] * 1e-3) / 1e9 / peak},
+        "kernel_us_per_time_step": {"e": r32["e_ms"] * 1e3, "h": r32["h_ms"] * 1e3, "sensors": r32["s_ms"] * 1e3},
+        "gpu_launches": r32["launches"],
+        "clocks": r32["clocks"],
+    }
+    if not args.no_e2e:
+        e2e_job(A.FP32, 2 * STEPS_PER_BENCH_STEP)
+        dt, h2d, d2h, cells = e2e_job(A.FP32, 20000)
+        line["e2e"] = {"value": cells * 20000 / dt / 1e9, "unit": METRIC, "h2d_bytes_per_step": h2d,
+                       "d2h_bytes_per_step": d2h,
+                       "step": "one complete 20000-step job from host buffers (geometry upload, "
+                               "all steps, spectra read back)", "seconds": dt}
+    if not args.no_cpu:
+        try:
+            line["cpu_baseline"] = cpu_baseline(workload)
+        except Exception as e:  # pragma: no cover
+            line["cpu_baseline"] = {"value": None, "error": str(e)}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -253,6 +253,9 @@ aefdtd_status aefdtd_get_sensor_shape(aefdtd_sim *sim, int32_t sensor_id, int32_
  * half-step kernels, the H half-step kernels and the sensor kernels. */
 aefdtd_status aefdtd_get_timings(aefdtd_sim *sim, double *e_ms, double *h_ms, double *sensor_ms);
 aefdtd_status aefdtd_enable_timing(aefdtd_sim *sim, int32_t enable);
+/* The handle's CUDA stream (a cudaStream_t), for callers that order their
+ * own device work or timing events with the simulation's kernels. */
+aefdtd_status aefdtd_get_stream(aefdtd_sim *sim, void **stream);
 /* Number of device kernel launches issued by this handle since creation. */
 aefdtd_status aefdtd_get_launch_count(aefdtd_sim *sim, uint64_t *launches);
 

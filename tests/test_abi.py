@@ -1,0 +1,92 @@
+"""The C-ABI library: loads, exports every entry point include/aefdtd.h
+declares, and its struct layouts match the ctypes mirror. No compute calls
+unless a GPU is present."""
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+from aether_b200 import _abi as A
+from aether_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "aefdtd.h")
+
+
+def declared_functions():
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?[a-z_]+\s*\*?\s*(aefdtd_[a-z_0-9]+)\s*\(", txt, re.M)))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    assert "aefdtd_create" in names and "aefdtd_step" in names and len(names) >= 20
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    lib = _lib.load()
+    for name in declared_functions():
+        assert hasattr(lib, name), name
+    assert set(declared_functions()) == set(_lib.exported_symbols())
+
+
+def test_no_cpu_fallback_symbols():
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    exported = [l.split()[-1] for l in out.splitlines() if " T " in l]
+    assert all(n.startswith("aefdtd_") for n in exported if not n.startswith("_")), exported
+
+
+def test_struct_layouts_match_header():
+    src = """
+#include <stdio.h>
+#include <stddef.h>
+#include "aefdtd.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu %zu %zu\\n", sizeof(aefdtd_grid_desc), sizeof(aefdtd_material_desc),
+         sizeof(aefdtd_normal_desc), sizeof(aefdtd_sensor_desc), sizeof(aefdtd_source_desc),
+         sizeof(aefdtd_dims), sizeof(aefdtd_structure_op));
+  printf("%zu %zu %zu\\n", offsetof(aefdtd_grid_desc, pml_kappa), offsetof(aefdtd_grid_desc, dft_block),
+         offsetof(aefdtd_material_desc, critpoint));
+  return 0;
+}
+"""
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "t.c")
+        open(c, "w").write(src)
+        exe = os.path.join(d, "t")
+        subprocess.run(["gcc", "-std=c11", "-I", os.path.dirname(HEADER), c, "-o", exe], check=True)
+        lines = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split("\n")
+    sizes = [int(x) for x in lines[0].split()]
+    offs = [int(x) for x in lines[1].split()]
+    assert sizes == [C.sizeof(A.GridDesc), C.sizeof(A.MaterialDesc), C.sizeof(A.NormalDesc),
+                     C.sizeof(A.SensorDesc), C.sizeof(A.SourceDesc), C.sizeof(A.Dims), C.sizeof(A.StructureOp)]
+    assert offs == [A.GridDesc.pml_kappa.offset, A.GridDesc.dft_block.offset, A.MaterialDesc.critpoint.offset]
+
+
+def test_status_strings():
+    lib = _lib.load()
+    for st in range(7):
+        assert lib.aefdtd_status_string(st)
+
+
+def test_bad_descriptor_rejected_before_device_use():
+    lib = _lib.load()
+    h = C.c_void_p()
+    g = A.grid_desc(8, 8, 8, 5e-9)
+    g.abi_version = 999
+    st = lib.aefdtd_create(C.byref(g), C.byref(h))
+    assert st in (1, 6)  # BAD_ARG, or NO_DEVICE where no GPU is visible
+    assert not h
+
+
+def test_create_without_gpu_reports_no_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    lib = _lib.load()
+    h = C.c_void_p()
+    g = A.grid_desc(8, 8, 8, 5e-9)
+    assert lib.aefdtd_create(C.byref(g), C.byref(h)) == 6

@@ -1,0 +1,122 @@
+"""GPU parity: the CUDA library (through its C ABI) against the reference.
+
+FP64 path: fields bit-identical to the reference core (SHA-256 of the golden
+fixtures, which come from the reference compiled from source) and to the CPU
+restatement; plane sums, R/T spectra and flux spectra within the relative
+tolerances below (they differ only by device reduction order and 1-ulp
+phasors). FP32 path: R/T and flux spectra within 1e-4 absolute of the FP64
+reference (relative for flux), fields within relative L2 1e-3."""
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+import oracle_lib
+import scenes
+from aether_b200 import _abi as A
+from aether_b200 import fdtd
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+GOLDEN = ["slab_tm", "slab_te", "gold_sphere", "debye_lorentz_sphere", "custom_box", "thin_column"]
+
+RTOL_PLANE = 1e-12      # plane sums: reduction order only
+RTOL_SPECTRA = 1e-10    # R/T spectra (ratios of DFTs of the plane sums)
+RTOL_FLUX = 1e-10       # flux spectra: DFT block sums + reduction order
+FP32_ABS_RT = 1e-4      # FP32 R/T vs FP64 oracle, absolute
+FP32_REL_FIELD = 1e-3   # FP32 fields, relative L2
+
+
+def sha(fields):
+    f = np.ascontiguousarray(fields, dtype=np.float64)
+    return [hashlib.sha256(f[c].tobytes()).hexdigest() for c in range(6)]
+
+
+def rel(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+@pytest.mark.parametrize("name", GOLDEN)
+def test_fp64_bit_identical_to_reference_golden(name):
+    g = np.load(os.path.join(GOLDEN_DIR, f"{name}.npz"))
+    r = fdtd.run(scenes.ALL[name]())
+    assert np.array_equal(r["dims"], g["dims"])
+    assert sha(r["fields"]) == list(g["field_sha256"]), "FP64 fields differ from the reference core"
+    if "plane_sums" in g:
+        assert rel(r["plane_sums"], g["plane_sums"]) < RTOL_PLANE
+        assert rel(r["spectra"], g["spectra"]) < RTOL_SPECTRA
+    for i, f in enumerate(r["flux"]):
+        assert rel(f, g[f"flux{i}"]) < RTOL_FLUX, (i, f, g[f"flux{i}"])
+    assert r["launches"] > 0
+
+
+def test_fp64_many_materials_uint16_ids():
+    sc = scenes.custom_many_materials(nsteps=60)
+    assert sc.map.max() > 255
+    a = oracle_lib.run(sc, "port")
+    b = fdtd.run(sc)
+    assert np.array_equal(a["fields"], b["fields"])
+
+
+def test_fp64_exact_dft_with_one_step_blocks():
+    sc = scenes.gold_sphere(nsteps=200)
+    sc.grid.dft_block = 1
+    a = oracle_lib.run(sc, "port")
+    b = fdtd.run(sc)
+    for fa, fb in zip(a["flux"], b["flux"]):
+        assert rel(fb, fa) < 1e-12
+
+
+@pytest.mark.parametrize("block", [7, 64])
+def test_fp64_dft_block_sizes_agree(block):
+    sc = scenes.slab_tm(nsteps=150)
+    sc.grid.dft_block = block
+    a = oracle_lib.run(sc, "port")
+    b = fdtd.run(sc)
+    for fa, fb in zip(a["flux"], b["flux"]):
+        assert rel(fb, fa) < RTOL_FLUX
+
+
+def test_fp64_step_in_pieces_equals_one_call():
+    sc = scenes.gold_sphere(nsteps=90)
+    with fdtd.build_simulation(sc) as s1, fdtd.build_simulation(sc) as s2:
+        s1.step(90)
+        for n in (1, 10, 33, 46):
+            s2.step(n)
+        assert np.array_equal(s1.fields(), s2.fields())
+        assert np.array_equal(s1.plane_sums(), s2.plane_sums())
+        for i in range(2):
+            assert np.array_equal(s1.sensor_flux(i), s2.sensor_flux(i))
+
+
+def test_reset_restarts_bitwise():
+    sc = scenes.slab_te(nsteps=60)
+    with fdtd.build_simulation(sc) as s:
+        s.step(60)
+        f1 = s.fields()
+        s.reset()
+        s.step(60)
+        assert np.array_equal(f1, s.fields())
+
+
+@pytest.mark.parametrize("name", ["slab_tm", "gold_sphere", "debye_lorentz_sphere"])
+def test_fp32_spectra_close_to_fp64_oracle(name):
+    sc64 = scenes.ALL[name](nsteps=400)
+    sc32 = scenes.ALL[name](precision=A.FP32, nsteps=400)
+    a = oracle_lib.run(sc64, "port")
+    b = fdtd.run(sc32)
+    assert rel(b["fields"], a["fields"]) < FP32_REL_FIELD
+    # columns 1, 2: |r|, |t| amplitude ratios (spectdata_norm)
+    assert np.max(np.abs(b["spectra"][:, 1:3] - a["spectra"][:, 1:3])) < FP32_ABS_RT
+    for fa, fb in zip(a["flux"], b["flux"]):
+        assert np.max(np.abs(fb - fa)) <= 1e-3 * np.max(np.abs(fa)) + 1e-300
+
+
+def test_fp32_custom_mode_close_to_fp64_oracle():
+    a = oracle_lib.run(scenes.custom_box(nsteps=100), "port")
+    b = fdtd.run(scenes.custom_box(precision=A.FP32, nsteps=100))
+    assert rel(b["fields"], a["fields"]) < FP32_REL_FIELD
