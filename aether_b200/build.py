@@ -30,7 +30,8 @@ CXXFLAGS = ["-std=c++20", "-O2", "-fPIC", "-ffp-contract=off", "-Wall", "-Wno-un
 UNITS = [
     ("yee_f64.cu", ["--fmad=false"]),
     ("yee_f32.cu", []),
-    ("sensors.cu", ["--fmad=false"]),
+    ("sensors.cu", []),
+    ("dft_tc.cu", []),
     ("voxel.cu", ["--fmad=false"]),
     ("runtime.cpp", None),
 ]

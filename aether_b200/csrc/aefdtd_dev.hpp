@@ -39,13 +39,26 @@ struct DispInfo {
     long long box;           // xs*ys*zs
 };
 
+// Per-step scalars of the excitation and sensors, computed on the host in
+// FP64 and read by the kernels from a device table, so that a captured
+// sequence of steps replays with new values.
+struct StepScalars {
+    double inj_eA, inj_eB;   // E plane injection: subtracted from Ex / added to Ey
+    double inj_hA, inj_hB;   // H plane injection: added to Hx / subtracted from Hy
+    double src[4];           // oscillator values
+    double tb, taper;        // plane-sum sample time (t + 1/2) Dt and tapering
+    int step, pad;           // global step index
+};
+
 // Parameters of one fused half-step launch. Pointers are device pointers.
 template <typename T, typename Tid> struct StepArgs {
     int Nx, Ny, Nz;
     long long NxNy;
     T *Ex, *Ey, *Ez, *Hx, *Hy, *Hz;
-    const Tid *mat;
+    const Tid *mat;                 // pitched: (mpitch x Ny x Nz)
+    int mpitch;                     // material-id row pitch, elements (multiple of 16 bytes)
     const MatCoef<T> *coef;
+    int nmat;                       // entries in coef / disp
     const DispInfo *disp;           // nullptr when no material is dispersive
     const Cplx<T> *crec;            // FP64: Crec; FP32: Crec - 1
     const Cplx<T> *dchi;
@@ -63,14 +76,15 @@ template <typename T, typename Tid> struct StepArgs {
     T dtdmx, dtdmy, dtdmz, dtm;
     // plane injection (normal mode): subtract/add on plane kinj, or kinj < 0
     int kinj;
-    T inj_a, inj_b;                 // E: a=(dtdez*Hy_inc)/eps_sup subtracted from Ex, b added to Ey
-                                    // H: a=dtdmz*Ey_inc added to Hx, b=dtdmz*Ex_inc subtracted from Hy
-    // box sources (custom mode, E only): up to kMaxSrc boxes
+    // box sources (custom mode, E only): up to 4 boxes
     int nsrc;
     int src_box[4][6];
     int src_comp[4];
-    T src_val[4];
+    // this step's scalars: sc[q] (injection values, oscillator values)
+    const StepScalars *sc;
+    int q;
     int kchunk;                     // z planes per thread
+    int *err;                       // device error flag (bounded waits)
 };
 
 // ---- sensor-path launch arguments (kernels in sensors.cuh)
@@ -80,27 +94,36 @@ struct PulseDev {
     double Ex0, Ey0, Ez0;
 };
 
-template <typename T> struct PlaneSumArgs {
-    int Nx, Ny;
-    long long NxNy;
-    const T *Ex, *Ey, *Ez;
-    int kr, kt;              // zs_e-2, zs_s
-    double Dx, Dy, Dz, tb, tapering;
-    PulseDev P;
-    double *out;             // 12 sums of this step
+struct GatherDesc {
+    int type;                // 0/1: x-normal, 2/3: y-normal, 4/5: z-normal
+    int x1, y1, z1, span1, span2, P;
+    int block0, nblocks;     // blocks of the fused launch serving this sensor
+    void *S;                 // sample slot of this step: [6][P] of T
 };
 
-template <typename T> struct GatherArgs {
+constexpr int kMaxGather = 8;
+
+// One launch per step: normal-incidence plane-sum partials (blocks
+// [0, nbp)) and the interpolated samples of every DFT plane (the rest).
+template <typename T> struct SensorStepArgs {
     int Nx, Ny, Nz;
     long long NxNy;
     const T *Ex, *Ey, *Ez, *Hx, *Hy, *Hz;
-    int type;                // 0/1: x-normal, 2/3: y-normal, 4/5: z-normal
-    int x1, y1, z1, span1, span2;
-    T *S;                    // slot base: [6][span1*span2]
+    int nbp;                 // plane-sum blocks (0 outside normal mode)
+    int kr, kt;              // zs_e-2, zs_s
+    double Dx, Dy, Dz;
+    PulseDev P;
+    const StepScalars *sc;
+    int q;
+    double *partial;         // [nbp][12] of this step
+    int ng;
+    GatherDesc g[kMaxGather];
 };
 
 struct PhasorArgs {
-    int nk, nl, step0, Nt, Ntap;
+    int nk, nl, Nt, Ntap;
+    const int *step_ptr;     // step of buffer slot 0 = (*step_ptr if set) + step_add
+    int step_add;
     double Dt;
     const double *w;         // angular frequencies, nl
     double2 *WE, *WH;        // [nk][nl]
@@ -120,6 +143,30 @@ struct FluxArgs {
     double *out;             // nl
 };
 
+// Tensor-core DFT (dft_tc.cu). B image: per tile [E hi, E lo, H hi, H lo] of
+// R x K floats in the K-major core-matrix layout, tiles tile_stride apart.
+struct DftTcPhasorArgs {
+    int K, nk, nl, N0, N1, Nt, Ntap;
+    const int *step_ptr;
+    int step_add;
+    double Dt;
+    const double *w;
+    float *B;
+    size_t tile_stride;
+};
+struct DftTcArgs {
+    int K, nk, nl, P, N0, N1;
+    const float *S;          // [K][6][P]
+    const float *B;
+    size_t tile_stride;
+    double2 *acc;            // [6][nl][P]
+    int *err;
+};
+constexpr int kDftTcMaxK = 64;
+constexpr int kDftTcSmem = (128 * kDftTcMaxK * 2 + 256 * kDftTcMaxK * 2) * 4 + 64;
+
+constexpr int kPlaneBlocks = 64;    // plane-sum stage-1 blocks
+constexpr int kPlaneThreads = 256;
 constexpr int kDftFTile = 8;
 constexpr int kDftKTile = 16;
 

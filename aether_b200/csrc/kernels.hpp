@@ -7,26 +7,35 @@
 
 #include "aefdtd_dev.hpp"
 
+
 namespace aefdtd {
 
-// yee_f64.cu (compiled with --fmad=false) and yee_f32.cu
-void launch_e(const StepArgs<double, uint8_t> &a, dim3 g, dim3 b, cudaStream_t s);
-void launch_e(const StepArgs<double, uint16_t> &a, dim3 g, dim3 b, cudaStream_t s);
-void launch_h(const StepArgs<double, uint8_t> &a, dim3 g, dim3 b, cudaStream_t s);
-void launch_h(const StepArgs<double, uint16_t> &a, dim3 g, dim3 b, cudaStream_t s);
-void launch_e(const StepArgs<float, uint8_t> &a, dim3 g, dim3 b, cudaStream_t s);
-void launch_e(const StepArgs<float, uint16_t> &a, dim3 g, dim3 b, cudaStream_t s);
-void launch_h(const StepArgs<float, uint8_t> &a, dim3 g, dim3 b, cudaStream_t s);
-void launch_h(const StepArgs<float, uint16_t> &a, dim3 g, dim3 b, cudaStream_t s);
+// yee_f64.cu (compiled with --fmad=false) and yee_f32.cu: the interior and
+// boundary half-step kernels over a device list of n work items
+// (x0, y0, k0, k1); one 32 x 4 CTA per item.
+#define AEFDTD_DECL_YEE(T, Tid)                                                                          \
+    void launch_e_interior(const StepArgs<T, Tid> &a, const int4 *items, int n, cudaStream_t s);        \
+    void launch_e_boundary(const StepArgs<T, Tid> &a, const int4 *items, int n, cudaStream_t s);        \
+    void launch_h_interior(const StepArgs<T, Tid> &a, const int4 *items, int n, cudaStream_t s);        \
+    void launch_h_boundary(const StepArgs<T, Tid> &a, const int4 *items, int n, cudaStream_t s);
+AEFDTD_DECL_YEE(double, uint8_t)
+AEFDTD_DECL_YEE(double, uint16_t)
+AEFDTD_DECL_YEE(float, uint8_t)
+AEFDTD_DECL_YEE(float, uint16_t)
+#undef AEFDTD_DECL_YEE
 
 // sensors.cu (compiled with --fmad=false)
-void launch_plane_sums(const PlaneSumArgs<double> &a, cudaStream_t s);
-void launch_plane_sums(const PlaneSumArgs<float> &a, cudaStream_t s);
-void launch_gather(const GatherArgs<double> &a, cudaStream_t s);
-void launch_gather(const GatherArgs<float> &a, cudaStream_t s);
+void launch_sensor_step(const SensorStepArgs<double> &a, cudaStream_t s);
+void launch_sensor_step(const SensorStepArgs<float> &a, cudaStream_t s);
+void launch_plane_reduce(const double *partial, int nbp, const StepScalars *sc, double *out, int steps,
+                         cudaStream_t s);
 void launch_phasors(const PhasorArgs &a, cudaStream_t s);
 void launch_accumulate(const AccumArgs<double> &a, cudaStream_t s);
 void launch_accumulate(const AccumArgs<float> &a, cudaStream_t s);
 void launch_flux(const FluxArgs &a, cudaStream_t s);
+
+// dft_tc.cu: FP32 DFT blocks on the tensor cores (tcgen05, 3xTF32)
+void launch_phasors_tc(const DftTcPhasorArgs &a, cudaStream_t s);
+void launch_accumulate_tc(const DftTcArgs &a, cudaStream_t s);
 
 }  // namespace aefdtd

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <complex>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numbers>
 #include <string>
@@ -18,6 +19,10 @@
 
 #include "../../include/aefdtd.h"
 #include "kernels.hpp"
+
+namespace aefdtd {
+constexpr int kTileXHost = 32, kTileYHost = 4;   // kTileX, kTileY of yee.cuh
+}
 
 namespace aefdtd {
 
@@ -120,6 +125,8 @@ struct PlaneSensor {
     int nbuf = 0;          // filled slots of the sample buffer
     int buf_step0 = 0;     // step of slot 0
     DBuf S, acc, wdev, WE, WH, flux;
+    DBuf Btc;              // tensor-core phasor image (FP32 path)
+    int N0 = 0, N1 = 0;
 };
 
 static inline double s_curve(double x, double xmin, double xmax) {
@@ -156,6 +163,7 @@ struct aefdtd_sim {
     // fields and state
     DBuf F[6], mat;
     int id_bytes = 1;
+    int mpitch = 0;
     std::vector<uint32_t> map;      // total-grid material ids
     bool map_set = false;
     unsigned Nmat = 1;
@@ -171,19 +179,26 @@ struct aefdtd_sim {
     aefdtd_normal_desc nd{};
     Pulse pulse{};
     double eps_sup = 1, eps_sub = 1, index_sup = 1, index_sub = 1;
-    DBuf psums;
+    DBuf psums, psum_partial;
     int psums_cap = 0;
     std::vector<double> psums_host;
     // custom mode
     std::vector<Osc> oscs;
     std::vector<PlaneSensor *> sensors;
+    // half-step work lists: (x0, y0, k0, k1) items of 32 x 4 columns x a z-chunk
+    bool work_dirty = true;
+    int kchunk = 0;
+    int n_interior = 0, n_boundary = 0;
+    DBuf items_interior, items_boundary;
+    void build_work();
+    DBuf err;
+    void check_err();
     // timing: one event quadruple per step of the last aefdtd_step call
     // (before E, after E, after H, after sensors), summed on query
     bool timing = false;
     std::vector<cudaEvent_t> tev;
-    int tev_used = 0;
-    // launch shape
-    int kchunk = 8;
+    int tev_steps = 0;
+    double t_e = 0, t_h = 0, t_s = 0;
 
     ~aefdtd_sim();
     void construct(const aefdtd_grid_desc *d);
@@ -194,10 +209,27 @@ struct aefdtd_sim {
     void finalize_tables();
     template <typename T, typename Tid> void fill_args(StepArgs<T, Tid> &a, bool e_side);
     template <typename T, typename Tid> void run_steps(int n);
-    template <typename T> void feed_sensors();
-    template <typename T> void flush_sensor(PlaneSensor &s);
+    template <typename T> void flush_sensor(PlaneSensor &s, const StepScalars *step0_ptr = nullptr);
+    template <typename T, typename Tid> void enqueue_segment(int L, StepScalars *tbl, bool record);
+    void fill_scalars(int t, int osc_offset, StepScalars &s) const;
+    void drop_graphs();
+    void accumulate_timing(int L);
+    int plane_blocks() const {
+        const int n = Nx * Ny;
+        return n >= kPlaneBlocks * kPlaneThreads ? kPlaneBlocks : (n + kPlaneThreads - 1) / kPlaneThreads;
+    }
+    // step segments: device tables of per-step scalars (two slots) and the
+    // CUDA graphs of full segments, one per slot
+    int seg_len = 64;
+    int seg_slot = 0;
+    DBuf tables;
+    bool use_graphs = true;
+    bool graphs_dirty = true;
+    cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
+    uint64_t graph_launches = 0;
     void step(int n);
     void zero_state();
+    int kchunk_override = 0;
 };
 
 aefdtd_sim::~aefdtd_sim() {
@@ -211,8 +243,15 @@ aefdtd_sim::~aefdtd_sim() {
     for (auto &b : psiE) b.release(t);
     for (auto &b : psiH) b.release(t);
     psums.release(t);
+    psum_partial.release(t);
+    err.release(t);
+    tables.release(t);
+    for (auto &gx : graph_exec) if (gx) cudaGraphExecDestroy(gx);
+    items_interior.release(t);
+    items_boundary.release(t);
     for (auto *s : sensors) {
         s->S.release(t); s->acc.release(t); s->wdev.release(t); s->WE.release(t); s->WH.release(t); s->flux.release(t);
+        s->Btc.release(t);
         delete s;
     }
     for (auto &e : tev) if (e) cudaEventDestroy(e);
@@ -291,14 +330,15 @@ void aefdtd_sim::construct(const aefdtd_grid_desc *d) {
         for (int q = 0; q < 6; q++) if (P[q].p) AE_CUDA(cudaMemsetAsync(P[q].p, 0, P[q].n, stream));
     }
     build_pml_tables();
+    seg_len = dft_k;
+    tables.alloc(sizeof(StepScalars) * 2 * seg_len, dev_bytes);
+    if (std::getenv("AEFDTD_NO_GRAPHS")) use_graphs = false;
+    err.alloc(sizeof(int), dev_bytes);
+    AE_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), stream));
     map.assign(N, 0);
     Nmat = 1;
     mats.assign(1, HostMat());
-    // column-parallel launch shape: enough z chunks for ~4 waves of 148 SMs
-    long long cols = (long long)Nx * Ny;
-    long long want = 148LL * 2048 * 4;
-    int chunks = (int)std::max(1LL, std::min((long long)Nz, want / std::max(1LL, cols)));
-    kchunk = std::max(1, (Nz + chunks - 1) / chunks);
+    if (const char *kc = std::getenv("AEFDTD_KCHUNK")) kchunk_override = std::max(0, atoi(kc));
     AE_CUDA(cudaStreamSynchronize(stream));
 }
 
@@ -398,17 +438,22 @@ void aefdtd_sim::set_map(const uint32_t *m, size_t count) {
             }
         }
     id_bytes = Nmat <= 256 ? 1 : 2;
-    size_t N = size_t(Nx) * Ny * Nz;
-    mat.alloc(N * id_bytes, dev_bytes);
+    // device copy with a 16-byte row pitch (TMA strides), padding columns = 0
+    mpitch = (Nx + (16 / id_bytes) - 1) / (16 / id_bytes) * (16 / id_bytes);
+    size_t NP = size_t(mpitch) * Ny * Nz;
+    mat.alloc(NP * id_bytes, dev_bytes);
     if (id_bytes == 1) {
-        std::vector<uint8_t> v(N);
-        for (size_t q = 0; q < N; q++) v[q] = (uint8_t)map[q];
-        AE_CUDA(cudaMemcpy(mat.p, v.data(), N, cudaMemcpyHostToDevice));
+        std::vector<uint8_t> v(NP, 0);
+        for (size_t r = 0; r < size_t(Ny) * Nz; r++)
+            for (int i = 0; i < Nx; i++) v[r * mpitch + i] = (uint8_t)map[r * Nx + i];
+        AE_CUDA(cudaMemcpy(mat.p, v.data(), NP, cudaMemcpyHostToDevice));
     } else {
-        std::vector<uint16_t> v(N);
-        for (size_t q = 0; q < N; q++) v[q] = (uint16_t)map[q];
-        AE_CUDA(cudaMemcpy(mat.p, v.data(), N * 2, cudaMemcpyHostToDevice));
+        std::vector<uint16_t> v(NP, 0);
+        for (size_t r = 0; r < size_t(Ny) * Nz; r++)
+            for (int i = 0; i < Nx; i++) v[r * mpitch + i] = (uint16_t)map[r * Nx + i];
+        AE_CUDA(cudaMemcpy(mat.p, v.data(), NP * 2, cudaMemcpyHostToDevice));
     }
+    work_dirty = true;
     map_set = true;
     tables_dirty = true;
 }
@@ -488,6 +533,8 @@ void aefdtd_sim::set_material(uint32_t idx, const aefdtd_material_desc *md) {
     h.C3 = 1.0 / e_eff;
     h.C4 = Dt / (e0 * e_eff);
     tables_dirty = true;
+    work_dirty = true;
+    graphs_dirty = true;
 }
 
 // Device tables of material coefficients and the dispersive-state layout.
@@ -558,7 +605,9 @@ void aefdtd_sim::fill_args(StepArgs<T, Tid> &a, bool e_side) {
     a.Ex = F[0].as<T>(); a.Ey = F[1].as<T>(); a.Ez = F[2].as<T>();
     a.Hx = F[3].as<T>(); a.Hy = F[4].as<T>(); a.Hz = F[5].as<T>();
     a.mat = mat.as<Tid>();
+    a.mpitch = mpitch;
     a.coef = coef.as<MatCoef<T>>();
+    a.nmat = (int)Nmat;
     a.disp = any_disp ? disp.as<DispInfo>() : nullptr;
     a.crec = crec.as<Cplx<T>>();
     a.dchi = dchi.as<Cplx<T>>();
@@ -575,13 +624,27 @@ void aefdtd_sim::fill_args(StepArgs<T, Tid> &a, bool e_side) {
     a.psi_z0 = P[4].as<T>(); a.psi_z1 = P[5].as<T>();
     a.dtdmx = (T)dtdmx; a.dtdmy = (T)dtdmy; a.dtdmz = (T)dtdmz; a.dtm = (T)dtm;
     a.kinj = -1;
-    a.kchunk = kchunk;
+    a.err = err.as<int>();
 }
 
 template <typename T>
-void aefdtd_sim::flush_sensor(PlaneSensor &s) {
+void aefdtd_sim::flush_sensor(PlaneSensor &s, const StepScalars *step0_ptr) {
     if (s.nbuf == 0) return;
-    PhasorArgs pa{s.nbuf, s.nl, s.buf_step0, Nt, Ntap, Dt, s.wdev.as<double>(), s.WE.as<double2>(), s.WH.as<double2>()};
+    if (!fp64 && s.Btc.p) {
+        // tensor-core DFT: phasors split into TF32 hi/lo in the B image, then the GEMM
+        DftTcPhasorArgs pa{dft_k, s.nbuf, s.nl, s.N0, s.N1, Nt, Ntap, step0_ptr ? &step0_ptr->step : nullptr,
+                           step0_ptr ? 0 : s.buf_step0, Dt, s.wdev.as<double>(), s.Btc.as<float>(),
+                           size_t(4) * 256 * dft_k};
+        launch_phasors_tc(pa, stream);
+        DftTcArgs aa{dft_k, s.nbuf, s.nl, s.P, s.N0, s.N1, s.S.as<float>(), s.Btc.as<float>(),
+                     size_t(4) * 256 * dft_k, s.acc.as<double2>(), err.as<int>()};
+        launch_accumulate_tc(aa, stream);
+        launches += 2;
+        s.nbuf = 0;
+        return;
+    }
+    PhasorArgs pa{s.nbuf, s.nl, Nt, Ntap, step0_ptr ? &step0_ptr->step : nullptr, step0_ptr ? 0 : s.buf_step0, Dt,
+                  s.wdev.as<double>(), s.WE.as<double2>(), s.WH.as<double2>()};
     launch_phasors(pa, stream);
     AccumArgs<T> aa{s.P, s.nl, s.nbuf, s.S.as<T>(), s.WE.as<double2>(), s.WH.as<double2>(), s.acc.as<double2>()};
     launch_accumulate(aa, stream);
@@ -589,30 +652,118 @@ void aefdtd_sim::flush_sensor(PlaneSensor &s) {
     s.nbuf = 0;
 }
 
-template <typename T>
-void aefdtd_sim::feed_sensors() {
-    for (PlaneSensor *sp : sensors) {
-        PlaneSensor &s = *sp;
-        if (s.nbuf == 0) s.buf_step0 = s.step;
-        GatherArgs<T> ga{Nx, Ny, Nz, (long long)Nx * Ny,
-                         F[0].as<T>(), F[1].as<T>(), F[2].as<T>(), F[3].as<T>(), F[4].as<T>(), F[5].as<T>(),
-                         s.type, s.x1, s.y1, s.z1, s.span1, s.span2,
-                         s.S.as<T>() + (size_t)s.nbuf * 6 * s.P};
-        launch_gather(ga, stream);
+// Host values of one step's scalars (excitation, sensors), FP64.
+void aefdtd_sim::fill_scalars(int t, int osc_offset, StepScalars &s) const {
+    std::memset(&s, 0, sizeof(s));
+    s.step = t;
+    if (normal) {
+        // normal_incidence.cpp:334-357
+        double tb = t * Dt;
+        double inj_Hx = pulse.f(pulse.Hx0, 0, 0, (zs_e - 1 + 0.5) * Dz, tb);
+        double inj_Hy = pulse.f(pulse.Hy0, 0, 0, (zs_e - 1 + 0.5) * Dz, tb);
+        s.inj_eA = dtdez * inj_Hy / eps_sup;
+        s.inj_eB = dtdez * inj_Hx / eps_sup;
+        tb = (t + 0.5) * Dt;
+        double inj_Ex = pulse.f(pulse.Ex0, 0, 0, (zs_e - 1) * Dz, tb);
+        double inj_Ey = pulse.f(pulse.Ey0, 0, 0, (zs_e - 1) * Dz, tb);
+        s.inj_hA = dtdmz * inj_Ey;
+        s.inj_hB = dtdmz * inj_Ex;
+        // plane sums (normal_incidence.cpp:378-386)
+        s.tb = (t + 0.5) * Dt;
+        double tapering = 1.0;
+        if (t >= Nt - Ntap) tapering = s_curve(t, Nt - 1.0, Nt - Ntap);
+        s.taper = tapering;
+    }
+    for (size_t k = 0; k < oscs.size() && k < 4; k++) {
+        // Oscillator::deep_inject_E (sc_oscillator.cpp:38-39)
+        const Osc &o = oscs[k];
+        const int st = o.step + osc_offset;
+        const cplx Im(0, 1);
+        cplx im_val = std::exp(-o.w0 * st * Dt * Im) * std::exp(-std::pow(o.dw / 2.0 * ((st - o.tshift) * Dt), 2.0));
+        s.src[k] = std::real(im_val) * 50;
+    }
+}
+
+// Enqueues the kernels of L consecutive steps on the stream: for each step
+// the E half-step (interior + boundary items), the H half-step, and the fused
+// sensor launch; then the plane-sum reduction of the L steps and, when a DFT
+// buffer fills, its accumulation. `tbl` is the device table of the L steps'
+// scalars. With record = true per-step timing events are recorded.
+template <typename T, typename Tid>
+void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
+    StepArgs<T, Tid> ea, ha;
+    fill_args(ea, true);
+    fill_args(ha, false);
+    ea.kchunk = ha.kchunk = kchunk;
+    ea.sc = ha.sc = tbl;
+    if (normal) ea.kinj = ha.kinj = zs_e - 1;
+    ea.nsrc = 0;
+    for (size_t s = 0; s < oscs.size() && s < 4; s++) {
+        std::memcpy(ea.src_box[s], oscs[s].box, sizeof(oscs[s].box));
+        ea.src_comp[s] = oscs[s].comp;
+        ea.nsrc++;
+    }
+    const int4 *wi = items_interior.as<int4>(), *wb = items_boundary.as<int4>();
+    SensorStepArgs<T> sa{};
+    sa.Nx = Nx; sa.Ny = Ny; sa.Nz = Nz; sa.NxNy = (long long)Nx * Ny;
+    sa.Ex = F[0].as<T>(); sa.Ey = F[1].as<T>(); sa.Ez = F[2].as<T>();
+    sa.Hx = F[3].as<T>(); sa.Hy = F[4].as<T>(); sa.Hz = F[5].as<T>();
+    sa.sc = tbl;
+    if (normal) {
+        sa.nbp = plane_blocks();
+        sa.kr = zs_e - 2; sa.kt = zs_s;
+        sa.Dx = Dx; sa.Dy = Dy; sa.Dz = Dz;
+        sa.P = PulseDev{pulse.k, pulse.omega, pulse.kx, pulse.ky, pulse.kz, pulse.n_ind, pulse.dz, pulse.C1,
+                        pulse.Ex0, pulse.Ey0, pulse.Ez0};
+    }
+    for (int q = 0; q < L; q++) {
+        if (record) AE_CUDA(cudaEventRecord(tev[4 * q + 0], stream));
+        ea.q = ha.q = q;
+        launch_e_interior(ea, wi, n_interior, stream);
+        launch_e_boundary(ea, wb, n_boundary, stream);
+        if (record) AE_CUDA(cudaEventRecord(tev[4 * q + 1], stream));
+        launch_h_interior(ha, wi, n_interior, stream);
+        launch_h_boundary(ha, wb, n_boundary, stream);
+        launches += (n_interior > 0) * 2 + (n_boundary > 0) * 2;
+        if (record) AE_CUDA(cudaEventRecord(tev[4 * q + 2], stream));
+        // sensors: fed after H in both drivers; plane sums read E of this step
+        sa.q = q;
+        sa.partial = psum_partial.as<double>() + size_t(q) * std::max(sa.nbp, 1) * 12;
+        sa.ng = 0;
+        int blk = sa.nbp;
+        for (PlaneSensor *ps : sensors) {
+            if (sa.ng >= kMaxGather) break;
+            PlaneSensor &s = *ps;
+            if (s.nbuf == 0) s.buf_step0 = s.step;
+            GatherDesc &g = sa.g[sa.ng++];
+            g.type = s.type; g.x1 = s.x1; g.y1 = s.y1; g.z1 = s.z1; g.span1 = s.span1; g.span2 = s.span2; g.P = s.P;
+            g.block0 = blk;
+            g.nblocks = (s.P + kPlaneThreads - 1) / kPlaneThreads;
+            blk += g.nblocks;
+            g.S = s.S.as<T>() + (size_t)s.nbuf * 6 * s.P;
+        }
+        if (sa.nbp > 0 || sa.ng > 0) {
+            launch_sensor_step(sa, stream);
+            launches++;
+        }
+        for (PlaneSensor *ps : sensors) {
+            ps->nbuf++;
+            ps->step++;
+            if (ps->nbuf == dft_k) flush_sensor<T>(*ps, ps->buf_step0 == tstep + q + 1 - dft_k && q + 1 == dft_k ? tbl : nullptr);
+        }
+        if (record) AE_CUDA(cudaEventRecord(tev[4 * q + 3], stream));
+    }
+    if (normal) {
+        launch_plane_reduce(psum_partial.as<double>(), sa.nbp, tbl, psums.as<double>(), L, stream);
         launches++;
-        s.nbuf++;
-        s.step++;
-        if (s.nbuf == dft_k) flush_sensor<T>(s);
     }
 }
 
 template <typename T, typename Tid>
 void aefdtd_sim::run_steps(int n) {
-    StepArgs<T, Tid> ea, ha;
-    fill_args(ea, true);
-    fill_args(ha, false);
-    dim3 blk(32, 4, 1);
-    dim3 grd((Nx + 31) / 32, (Ny + 3) / 4, (Nz + kchunk - 1) / kchunk);
+    if (work_dirty) { build_work(); graphs_dirty = true; }
+    if (graphs_dirty) drop_graphs();
+    // capacity of the plane-sum history
     if (normal && tstep + n > psums_cap) {
         int cap = std::max(tstep + n, std::max(2 * psums_cap, 1024));
         DBuf nb;
@@ -622,77 +773,166 @@ void aefdtd_sim::run_steps(int n) {
         psums.release(dev_bytes);
         psums = nb;
         psums_cap = cap;
+        graphs_dirty = true;
+        drop_graphs();
     }
     if (timing) {
-        while ((int)tev.size() < 4 * n) {
+        while ((int)tev.size() < 4 * seg_len) {
             cudaEvent_t e;
             AE_CUDA(cudaEventCreate(&e));
             tev.push_back(e);
         }
-        tev_used = n;
+        t_e = t_h = t_s = 0;
+        tev_steps = 0;
     }
-    for (int q = 0; q < n; q++) {
-        int t = tstep;
-        if (timing) AE_CUDA(cudaEventRecord(tev[4 * q + 0], stream));
-        // ---- E half-step + E-side excitation
-        if (normal) {
-            double tb = t * Dt;
-            double inj_Hx = pulse.f(pulse.Hx0, 0, 0, (zs_e - 1 + 0.5) * Dz, tb);
-            double inj_Hy = pulse.f(pulse.Hy0, 0, 0, (zs_e - 1 + 0.5) * Dz, tb);
-            ea.kinj = zs_e - 1;
-            ea.inj_a = (T)(dtdez * inj_Hy / eps_sup);
-            ea.inj_b = (T)(dtdez * inj_Hx / eps_sup);
+    std::vector<StepScalars> host(seg_len);
+    int done = 0;
+    while (done < n) {
+        // a segment ends where the DFT buffers fill, so captured segments start empty
+        int L = std::min(n - done, seg_len);
+        if (!sensors.empty()) L = std::min(L, dft_k - sensors[0]->nbuf);
+        const int slot = seg_slot;
+        seg_slot ^= 1;
+        StepScalars *tbl = tables.as<StepScalars>() + size_t(slot) * seg_len;
+        for (int q = 0; q < L; q++) fill_scalars(tstep + q, q, host[q]);
+        AE_CUDA(cudaMemcpyAsync(tbl, host.data(), sizeof(StepScalars) * L, cudaMemcpyHostToDevice, stream));
+        const bool full = (L == seg_len) && (sensors.empty() || sensors[0]->nbuf == 0);
+        if (timing) {
+            enqueue_segment<T, Tid>(L, tbl, true);
+            accumulate_timing(L);
+        } else if (full && use_graphs) {
+            if (!graph_exec[slot]) {
+                // capture once; the sequence reads every per-step value from the table
+                std::vector<int> nb0, st0;
+                for (auto *s : sensors) { nb0.push_back(s->nbuf); st0.push_back(s->step); }
+                uint64_t l0 = launches;
+                AE_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+                enqueue_segment<T, Tid>(L, tbl, false);
+                cudaGraph_t gr = nullptr;
+                AE_CUDA(cudaStreamEndCapture(stream, &gr));
+                AE_CUDA(cudaGraphInstantiate(&graph_exec[slot], gr, 0));
+                cudaGraphDestroy(gr);
+                graph_launches = launches - l0;
+                launches = l0;
+                for (size_t s = 0; s < sensors.size(); s++) { sensors[s]->nbuf = nb0[s]; sensors[s]->step = st0[s]; }
+            }
+            AE_CUDA(cudaGraphLaunch(graph_exec[slot], stream));
+            launches += graph_launches;
+            for (auto *s : sensors) { s->step += L; s->buf_step0 = s->step; s->nbuf = 0; }
+        } else {
+            enqueue_segment<T, Tid>(L, tbl, false);
         }
-        ea.nsrc = 0;
-        for (size_t s = 0; s < oscs.size() && s < 4; s++) {
-            Osc &o = oscs[s];
-            // Oscillator::deep_inject_E (sc_oscillator.cpp:38-39)
-            const cplx Im(0, 1);
-            cplx im_val = std::exp(-o.w0 * o.step * Dt * Im) * std::exp(-std::pow(o.dw / 2.0 * ((o.step - o.tshift) * Dt), 2.0));
-            double val = std::real(im_val) * 50;
-            std::memcpy(ea.src_box[s], o.box, sizeof(o.box));
-            ea.src_comp[s] = o.comp;
-            ea.src_val[s] = (T)val;
-            ea.nsrc++;
-        }
-        launch_e(ea, grd, blk, stream);
-        if (timing) AE_CUDA(cudaEventRecord(tev[4 * q + 1], stream));
-        // ---- H half-step + H-side excitation
-        if (normal) {
-            double tb = (t + 0.5) * Dt;
-            double inj_Ex = pulse.f(pulse.Ex0, 0, 0, (zs_e - 1) * Dz, tb);
-            double inj_Ey = pulse.f(pulse.Ey0, 0, 0, (zs_e - 1) * Dz, tb);
-            ha.kinj = zs_e - 1;
-            ha.inj_a = (T)(dtdmz * inj_Ey);
-            ha.inj_b = (T)(dtdmz * inj_Ex);
-        }
-        launch_h(ha, grd, blk, stream);
-        launches += 2;
-        if (timing) AE_CUDA(cudaEventRecord(tev[4 * q + 2], stream));
-        // ---- sensors (fed after H in both drivers; custom inject_H is a no-op
-        //      for oscillators apart from the step counter)
-        feed_sensors<T>();
-        for (auto &o : oscs) o.step += 1;
-        if (normal) {
-            PlaneSumArgs<T> pa{};
-            pa.Nx = Nx; pa.Ny = Ny; pa.NxNy = (long long)Nx * Ny;
-            pa.Ex = F[0].as<T>(); pa.Ey = F[1].as<T>(); pa.Ez = F[2].as<T>();
-            pa.kr = zs_e - 2; pa.kt = zs_s;
-            pa.Dx = Dx; pa.Dy = Dy; pa.Dz = Dz;
-            pa.tb = (t + 0.5) * Dt;
-            double tapering = 1.0;
-            if (t >= Nt - Ntap) tapering = s_curve(t, Nt - 1.0, Nt - Ntap);
-            pa.tapering = tapering;
-            pa.P = PulseDev{pulse.k, pulse.omega, pulse.kx, pulse.ky, pulse.kz, pulse.n_ind, pulse.dz, pulse.C1,
-                            pulse.Ex0, pulse.Ey0, pulse.Ez0};
-            pa.out = psums.as<double>() + size_t(t) * 12;
-            launch_plane_sums(pa, stream);
-            launches++;
-        }
-        if (timing) AE_CUDA(cudaEventRecord(tev[4 * q + 3], stream));
-        tstep++;
+        for (auto &o : oscs) o.step += L;
+        tstep += L;
+        done += L;
     }
     AE_CUDA(cudaGetLastError());
+}
+
+void aefdtd_sim::drop_graphs() {
+    for (auto &g : graph_exec)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    graphs_dirty = false;
+}
+
+void aefdtd_sim::accumulate_timing(int L) {
+    AE_CUDA(cudaEventSynchronize(tev[4 * L - 1]));
+    for (int q = 0; q < L; q++) {
+        float a = 0, b = 0, c = 0;
+        AE_CUDA(cudaEventElapsedTime(&a, tev[4 * q + 0], tev[4 * q + 1]));
+        AE_CUDA(cudaEventElapsedTime(&b, tev[4 * q + 1], tev[4 * q + 2]));
+        AE_CUDA(cudaEventElapsedTime(&c, tev[4 * q + 2], tev[4 * q + 3]));
+        t_e += a; t_h += b; t_s += c;
+    }
+    tev_steps += L;
+}
+
+// Work lists of the half-step kernels. The grid is cut into items of 32 x 4
+// columns by kchunk planes; an item is "boundary" when any of its cells is in
+// a CPML range or PEC plane of either half-step, on the injection plane, in
+// an oscillator box, or of a dispersive material; all others are "interior"
+// and run the curl-only kernels.
+void aefdtd_sim::build_work() {
+    const int tx = kTileXHost, ty = kTileYHost;
+    const int ntx = (Nx + tx - 1) / tx, nty = (Ny + ty - 1) / ty;
+    const long long tiles = (long long)ntx * nty;
+    if (kchunk_override > 0) kchunk = kchunk_override;
+    else {
+        // 8 planes per item unless that leaves fewer than three waves of
+        // 148 SMs x 12 resident items; never fewer than 4 planes
+        long long want = 148LL * 12 * 3;
+        kchunk = 8;
+        while (kchunk > 4 && tiles * ((Nz + kchunk - 1) / kchunk) < want) kchunk /= 2;
+    }
+    const int nch = (Nz + kchunk - 1) / kchunk;
+    std::vector<char> special(size_t(tiles) * nch, 0);   // 1: boundary, 2: boundary with dispersive cells
+    auto mark_range = [&](int x0, int x1, int y0, int y1, int z0, int z1) {   // half-open cell ranges
+        if (x0 >= x1 || y0 >= y1 || z0 >= z1) return;
+        for (int c = z0 / kchunk; c <= (z1 - 1) / kchunk; c++)
+            for (int b = y0 / ty; b <= (y1 - 1) / ty; b++)
+                for (int a = x0 / tx; a <= (x1 - 1) / tx; a++) special[(size_t(c) * nty + b) * ntx + a] = 1;
+    };
+    const bool px = pml[0] || pml[1], py = pml[2] || pml[3], pz = pml[4] || pml[5];
+    if (px) {
+        mark_range(0, std::max(pml[0], 1), 0, Ny, 0, Nz);
+        mark_range(Nx - std::max(pml[1], 1), Nx, 0, Ny, 0, Nz);
+    }
+    if (py) {
+        mark_range(0, Nx, 0, std::max(pml[2], 1), 0, Nz);
+        mark_range(0, Nx, Ny - std::max(pml[3], 1), Ny, 0, Nz);
+    }
+    if (pz) {
+        mark_range(0, Nx, 0, Ny, 0, std::max(pml[4], 1));
+        mark_range(0, Nx, 0, Ny, Nz - std::max(pml[5], 1), Nz);
+    }
+    if (normal) mark_range(0, Nx, 0, Ny, zs_e - 1, zs_e);
+    for (auto &o : oscs) mark_range(o.box[0], o.box[1], o.box[2], o.box[3], o.box[4], o.box[5]);
+    for (unsigned m = 0; m < Nmat; m++) {
+        HostMat &h = mats[m];
+        if (!(h.rc && h.np > 0)) continue;
+        for (int k = h.z1; k <= h.z2; k++)
+            for (int j = h.y1; j <= h.y2; j++) {
+                const uint32_t *row = &map[size_t(j) * Nx + size_t(k) * Nx * Ny];
+                for (int i = h.x1; i <= h.x2; i++)
+                    if (row[i] == m) special[(size_t(k / kchunk) * nty + j / ty) * ntx + i / tx] = 2;
+            }
+    }
+    // AEFDTD_ALL_BOUNDARY=1 routes every item through the full kernels (same results)
+    const bool all_boundary = std::getenv("AEFDTD_ALL_BOUNDARY") != nullptr;
+    if (all_boundary) std::fill(special.begin(), special.end(), 1);
+    std::vector<int> vi, vb;
+    for (int c = 0; c < nch; c++)
+        for (int b = 0; b < nty; b++)
+            for (int a = 0; a < ntx; a++) {
+                const char sp = special[(size_t(c) * nty + b) * ntx + a];
+                std::vector<int> &v = sp ? vb : vi;
+                const int z0 = c * kchunk, z1 = std::min(Nz, (c + 1) * kchunk);
+                const int step = (sp == 2) ? 1 : kchunk;   // dispersive items: one plane each
+                for (int z = z0; z < z1; z += step) {
+                    v.push_back(a * tx);
+                    v.push_back(b * ty);
+                    v.push_back(z);
+                    v.push_back(std::min(z1, z + step));
+                }
+            }
+    n_interior = (int)(vi.size() / 4);
+    n_boundary = (int)(vb.size() / 4);
+    items_interior.alloc(std::max<size_t>(vi.size(), 4) * sizeof(int), dev_bytes);
+    items_boundary.alloc(std::max<size_t>(vb.size(), 4) * sizeof(int), dev_bytes);
+    if (!vi.empty()) AE_CUDA(cudaMemcpy(items_interior.p, vi.data(), vi.size() * sizeof(int), cudaMemcpyHostToDevice));
+    if (!vb.empty()) AE_CUDA(cudaMemcpy(items_boundary.p, vb.data(), vb.size() * sizeof(int), cudaMemcpyHostToDevice));
+    work_dirty = false;
+}
+
+// Reads the device error flag set by a bounded wait that ran out.
+void aefdtd_sim::check_err() {
+    int h = 0;
+    AE_CUDA(cudaMemcpyAsync(&h, err.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    AE_CUDA(cudaStreamSynchronize(stream));
+    if (h) {
+        AE_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), stream));
+        fail(AEFDTD_TIMEOUT, "a bounded device wait ran out");
+    }
 }
 
 void aefdtd_sim::step(int n) {
@@ -823,7 +1063,10 @@ aefdtd_status aefdtd_setup_normal(aefdtd_sim *s, const aefdtd_normal_desc *nd) {
         s->index_sup = std::sqrt(s->eps_sup);
         double pol = nd->polarization == 1 ? 90 : 0;
         s->pulse.init(nd->lambda_min, nd->lambda_max, pol, (s->zs_e - 1) * s->Dz, s->index_sup);
+        if (!s->psum_partial.p) s->psum_partial.alloc(size_t(s->seg_len) * kPlaneBlocks * 12 * 8, s->dev_bytes);
+        s->graphs_dirty = true;
         s->normal = true;
+        s->work_dirty = true;
     });
 }
 
@@ -848,6 +1091,8 @@ aefdtd_status aefdtd_add_oscillator(aefdtd_sim *s, const aefdtd_source_desc *d, 
         o.tshift = (int)(std::sqrt(-4.0 / (o.dw * o.dw) * std::log(bet)) / s->Dt);
         o.step = s->tstep;
         s->oscs.push_back(o);
+        s->work_dirty = true;
+        s->graphs_dirty = true;
         if (id) *id = (int32_t)s->oscs.size() - 1;
     });
 }
@@ -890,16 +1135,37 @@ aefdtd_status aefdtd_add_planar_sensor(aefdtd_sim *s, const aefdtd_sensor_desc *
             p->WH.alloc(size_t(s->dft_k) * p->nl * 16, s->dev_bytes);
             p->flux.alloc(size_t(p->nl) * 8, s->dev_bytes);
             AE_CUDA(cudaMemsetAsync(p->acc.p, 0, p->acc.n, s->stream));
+            AE_CUDA(cudaMemsetAsync(p->S.p, 0, p->S.n, s->stream));
+            // FP32 path: DFT blocks on the tensor cores when K is a multiple of 8
+            // (at most 64) and 2 nl columns fit two 256-wide tiles
+            if (!s->fp64 && s->dft_k % 8 == 0 && s->dft_k <= kDftTcMaxK && p->nl <= 256 &&
+                !std::getenv("AEFDTD_NO_TC")) {
+                int n2 = 2 * p->nl;
+                p->N0 = std::min(256, (n2 + 15) / 16 * 16);
+                p->N1 = n2 > 256 ? (n2 - 256 + 15) / 16 * 16 : 0;
+                p->Btc.alloc(size_t(2) * 4 * 256 * s->dft_k * sizeof(float), s->dev_bytes);
+                AE_CUDA(cudaMemsetAsync(p->Btc.p, 0, p->Btc.n, s->stream));
+            }
             AE_CUDA(cudaMemcpyAsync(p->wdev.p, p->w.data(), p->nl * 8, cudaMemcpyHostToDevice, s->stream));
             AE_CUDA(cudaStreamSynchronize(s->stream));
         } catch (...) {
             p->S.release(s->dev_bytes); p->acc.release(s->dev_bytes); p->wdev.release(s->dev_bytes);
             p->WE.release(s->dev_bytes); p->WH.release(s->dev_bytes); p->flux.release(s->dev_bytes);
+            p->Btc.release(s->dev_bytes);
             delete p;
             throw;
         }
         p->step = s->tstep;
+        if (s->sensors.size() >= (size_t)kMaxGather) {
+            p->S.release(s->dev_bytes); p->acc.release(s->dev_bytes); p->wdev.release(s->dev_bytes);
+            p->WE.release(s->dev_bytes); p->WH.release(s->dev_bytes); p->flux.release(s->dev_bytes);
+            delete p;
+            fail(AEFDTD_BAD_ARG, "at most 8 planar sensors per simulation");
+        }
+        if (!s->sensors.empty() && s->sensors[0]->nbuf != 0)
+            for (auto *o : s->sensors) { if (s->fp64) s->flush_sensor<double>(*o); else s->flush_sensor<float>(*o); }
         s->sensors.push_back(p);
+        s->graphs_dirty = true;
         if (id) *id = (int32_t)s->sensors.size() - 1;
     });
 }
@@ -911,7 +1177,11 @@ aefdtd_status aefdtd_step(aefdtd_sim *s, int32_t n) {
 
 aefdtd_status aefdtd_synchronize(aefdtd_sim *s) {
     if (!s) return AEFDTD_BAD_ARG;
-    return guarded(s, [&] { s->set_device(); AE_CUDA(cudaStreamSynchronize(s->stream)); });
+    return guarded(s, [&] {
+        s->set_device();
+        AE_CUDA(cudaStreamSynchronize(s->stream));
+        s->check_err();
+    });
 }
 
 aefdtd_status aefdtd_reset(aefdtd_sim *s) {
@@ -1064,6 +1334,7 @@ aefdtd_status aefdtd_get_sensor_flux(aefdtd_sim *s, int32_t id, double *out, int
         if (nl != p.nl) fail(AEFDTD_BAD_ARG, "nl must equal the sensor's spectrum size");
         s->set_device();
         if (s->fp64) s->flush_sensor<double>(p); else s->flush_sensor<float>(p);
+        s->graphs_dirty = true;
         double af = p.type <= 1 ? s->Dy * s->Dz : (p.type <= 3 ? s->Dx * s->Dz : s->Dx * s->Dy);
         FluxArgs fa{p.P, p.nl, p.type, af, p.acc.as<double2>(), p.flux.as<double>()};
         launch_flux(fa, s->stream);
@@ -1082,6 +1353,7 @@ aefdtd_status aefdtd_get_sensor_dft(aefdtd_sim *s, int32_t id, double *out, size
         if (count != size_t(6) * p.P * p.nl * 2) fail(AEFDTD_BAD_ARG, "count must be 6*span1*span2*nl*2");
         s->set_device();
         if (s->fp64) s->flush_sensor<double>(p); else s->flush_sensor<float>(p);
+        s->graphs_dirty = true;
         AE_CUDA(cudaMemcpyAsync(out, p.acc.p, count * 8, cudaMemcpyDeviceToHost, s->stream));
         AE_CUDA(cudaStreamSynchronize(s->stream));
     });
@@ -1126,23 +1398,10 @@ aefdtd_status aefdtd_voxelize(aefdtd_sim *sim, int32_t nx, int32_t ny, int32_t n
 
 aefdtd_status aefdtd_get_timings(aefdtd_sim *s, double *e_ms, double *h_ms, double *sensor_ms) {
     if (!s) return AEFDTD_BAD_ARG;
-    return guarded(s, [&] {
-        double te = 0, th = 0, ts = 0;
-        if (s->timing && s->tev_used > 0) {
-            s->set_device();
-            AE_CUDA(cudaEventSynchronize(s->tev[4 * s->tev_used - 1]));
-            for (int q = 0; q < s->tev_used; q++) {
-                float a = 0, b = 0, c = 0;
-                AE_CUDA(cudaEventElapsedTime(&a, s->tev[4 * q + 0], s->tev[4 * q + 1]));
-                AE_CUDA(cudaEventElapsedTime(&b, s->tev[4 * q + 1], s->tev[4 * q + 2]));
-                AE_CUDA(cudaEventElapsedTime(&c, s->tev[4 * q + 2], s->tev[4 * q + 3]));
-                te += a; th += b; ts += c;
-            }
-        }
-        if (e_ms) *e_ms = te;
-        if (h_ms) *h_ms = th;
-        if (sensor_ms) *sensor_ms = ts;
-    });
+    if (e_ms) *e_ms = s->t_e;
+    if (h_ms) *h_ms = s->t_h;
+    if (sensor_ms) *sensor_ms = s->t_s;
+    return AEFDTD_OK;
 }
 
 aefdtd_status aefdtd_enable_timing(aefdtd_sim *s, int32_t enable) {

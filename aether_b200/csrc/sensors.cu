@@ -1,18 +1,22 @@
-// Sensor-path kernels. Built with --fmad=false: with one buffered step the
-// DFT update is the reference's acc + coeff*t exactly.
+// Sensor-path kernels. Contraction is allowed: the SIMT DFT accumulates its
+// K-step partial sums with FMA starting from zero, so with one buffered step
+// the update is still the reference's acc + round(coeff*t) exactly.
 #include "kernels.hpp"
 #include "sensors.cuh"
 
+#include <algorithm>
+
 namespace aefdtd {
-void launch_plane_sums(const PlaneSumArgs<double> &a, cudaStream_t s) { plane_sums<<<1, 512, 0, s>>>(a); }
-void launch_plane_sums(const PlaneSumArgs<float> &a, cudaStream_t s) { plane_sums<<<1, 512, 0, s>>>(a); }
-void launch_gather(const GatherArgs<double> &a, cudaStream_t s) {
-    const int P = a.span1 * a.span2;
-    dft_gather<<<(P + 255) / 256, 256, 0, s>>>(a);
+template <typename T> static void step_impl(const SensorStepArgs<T> &a, cudaStream_t s) {
+    int nb = a.nbp;
+    for (int g = 0; g < a.ng; ++g) nb = std::max(nb, a.g[g].block0 + a.g[g].nblocks);
+    if (nb > 0) sensor_step<<<nb, kPlaneThreads, 0, s>>>(a);
 }
-void launch_gather(const GatherArgs<float> &a, cudaStream_t s) {
-    const int P = a.span1 * a.span2;
-    dft_gather<<<(P + 255) / 256, 256, 0, s>>>(a);
+void launch_sensor_step(const SensorStepArgs<double> &a, cudaStream_t s) { step_impl(a, s); }
+void launch_sensor_step(const SensorStepArgs<float> &a, cudaStream_t s) { step_impl(a, s); }
+void launch_plane_reduce(const double *partial, int nbp, const StepScalars *sc, double *out, int steps,
+                         cudaStream_t s) {
+    if (steps > 0) plane_sums_reduce<<<steps, 32, 0, s>>>(partial, nbp, sc, out);
 }
 void launch_phasors(const PhasorArgs &a, cudaStream_t s) {
     const int n = a.nk * a.nl;

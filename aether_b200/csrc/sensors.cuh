@@ -32,39 +32,41 @@ __device__ __forceinline__ double pulse_eval(const PulseDev &P, double A0, doubl
 
 
 
-// One block per step; deterministic tree reduction.
 template <typename T>
-__global__ void __launch_bounds__(512) plane_sums(PlaneSumArgs<T> a) {
+__device__ __forceinline__ void plane_partial(const SensorStepArgs<T> &a, int b) {
     double acc[12];
 #pragma unroll
     for (int c = 0; c < 12; ++c) acc[c] = 0;
     const int n = a.Nx * a.Ny;
+    const int per = (n + a.nbp - 1) / a.nbp;
+    const int q0 = b * per, q1 = min(n, q0 + per);
     const double Dx2 = a.Dx / 2.0, Dy2 = a.Dy / 2.0, Dz2 = a.Dz / 2.0;
     const double zr = a.kr * a.Dz, zt = a.kt * a.Dz;
-    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+    const double tb = a.sc[a.q].tb, tap = a.sc[a.q].taper;
+    for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
         const int i = q % a.Nx, j = q / a.Nx;
         const double x = i * a.Dx, y = j * a.Dy;
-        const double bx = pulse_eval(a.P, a.P.Ex0, x + Dx2, y, zr, a.tb);
-        const double by = pulse_eval(a.P, a.P.Ey0, x, y + Dy2, zr, a.tb);
-        const double bz = pulse_eval(a.P, a.P.Ez0, x, y, zr + Dz2, a.tb);
-        const double tx = pulse_eval(a.P, a.P.Ex0, x + Dx2, y, zt, a.tb);
-        const double ty = pulse_eval(a.P, a.P.Ey0, x, y + Dy2, zt, a.tb);
-        const double tz = pulse_eval(a.P, a.P.Ez0, x, y, zt + Dz2, a.tb);
+        const double bx = pulse_eval(a.P, a.P.Ex0, x + Dx2, y, zr, tb);
+        const double by = pulse_eval(a.P, a.P.Ey0, x, y + Dy2, zr, tb);
+        const double bz = pulse_eval(a.P, a.P.Ez0, x, y, zr + Dz2, tb);
+        const double tx = pulse_eval(a.P, a.P.Ex0, x + Dx2, y, zt, tb);
+        const double ty = pulse_eval(a.P, a.P.Ey0, x, y + Dy2, zt, tb);
+        const double tz = pulse_eval(a.P, a.P.Ez0, x, y, zt + Dz2, tb);
         const long long ir = q + a.kr * a.NxNy, it = q + a.kt * a.NxNy;
-        acc[0] += bx * a.tapering;
-        acc[1] += by * a.tapering;
-        acc[2] += bz * a.tapering;
-        acc[3] += ((double)a.Ex[ir] - bx) * a.tapering;
-        acc[4] += ((double)a.Ey[ir] - by) * a.tapering;
-        acc[5] += ((double)a.Ez[ir] - bz) * a.tapering;
-        acc[6] += tx * a.tapering;
-        acc[7] += ty * a.tapering;
-        acc[8] += tz * a.tapering;
-        acc[9] += (double)a.Ex[it] * a.tapering;
-        acc[10] += (double)a.Ey[it] * a.tapering;
-        acc[11] += (double)a.Ez[it] * a.tapering;
+        acc[0] += bx * tap;
+        acc[1] += by * tap;
+        acc[2] += bz * tap;
+        acc[3] += ((double)a.Ex[ir] - bx) * tap;
+        acc[4] += ((double)a.Ey[ir] - by) * tap;
+        acc[5] += ((double)a.Ez[ir] - bz) * tap;
+        acc[6] += tx * tap;
+        acc[7] += ty * tap;
+        acc[8] += tz * tap;
+        acc[9] += (double)a.Ex[it] * tap;
+        acc[10] += (double)a.Ey[it] * tap;
+        acc[11] += (double)a.Ez[it] * tap;
     }
-    __shared__ double red[12][512];
+    __shared__ double red[12][kPlaneThreads];
 #pragma unroll
     for (int c = 0; c < 12; ++c) red[c][threadIdx.x] = acc[c];
     __syncthreads();
@@ -74,21 +76,18 @@ __global__ void __launch_bounds__(512) plane_sums(PlaneSumArgs<T> a) {
             for (int c = 0; c < 12; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + s];
         __syncthreads();
     }
-    if (threadIdx.x < 12) a.out[threadIdx.x] = red[threadIdx.x][0];
+    if (threadIdx.x < 12) a.partial[b * 12 + threadIdx.x] = red[threadIdx.x][0];
 }
 
-
-
 template <typename T>
-__global__ void dft_gather(GatherArgs<T> a) {
-    const int P = a.span1 * a.span2;
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= P) return;
-    const int u = q % a.span1, v = q / a.span1;
+__device__ __forceinline__ void gather_one(const SensorStepArgs<T> &a, const GatherDesc &g, int b) {
+    const int q = (b - g.block0) * blockDim.x + threadIdx.x;
+    if (q >= g.P) return;
+    const int u = q % g.span1, v = q / g.span1;
     int i, j, k;
-    if (a.type <= 1) { i = a.x1; j = a.y1 + u; k = a.z1 + v; }
-    else if (a.type <= 3) { i = a.x1 + u; j = a.y1; k = a.z1 + v; }
-    else { i = a.x1 + u; j = a.y1 + v; k = a.z1; }
+    if (g.type <= 1) { i = g.x1; j = g.y1 + u; k = g.z1 + v; }
+    else if (g.type <= 3) { i = g.x1 + u; j = g.y1; k = g.z1 + v; }
+    else { i = g.x1 + u; j = g.y1 + v; k = g.z1; }
     const int ip = (i + 1 == a.Nx) ? 0 : i + 1;
     const int jp = (j + 1 == a.Ny) ? 0 : j + 1;
     const int kp = (k + 1 == a.Nz) ? 0 : k + 1;
@@ -99,15 +98,39 @@ __global__ void dft_gather(GatherArgs<T> a) {
     const T hx = (a.Hx[I(i, j, k)] + a.Hx[I(ip, j, k)]) / T(2.0);
     const T hy = (a.Hy[I(i, j, k)] + a.Hy[I(i, jp, k)]) / T(2.0);
     const T hz = (a.Hz[I(i, j, k)] + a.Hz[I(i, j, kp)]) / T(2.0);
-    a.S[0 * (long long)P + q] = ex;
-    a.S[1 * (long long)P + q] = ey;
-    a.S[2 * (long long)P + q] = ez;
-    a.S[3 * (long long)P + q] = hx;
-    a.S[4 * (long long)P + q] = hy;
-    a.S[5 * (long long)P + q] = hz;
+    T *S = static_cast<T *>(g.S);
+    S[0 * (long long)g.P + q] = ex;
+    S[1 * (long long)g.P + q] = ey;
+    S[2 * (long long)g.P + q] = ez;
+    S[3 * (long long)g.P + q] = hx;
+    S[4 * (long long)g.P + q] = hy;
+    S[5 * (long long)g.P + q] = hz;
 }
 
+template <typename T>
+__global__ void __launch_bounds__(kPlaneThreads) sensor_step(const __grid_constant__ SensorStepArgs<T> a) {
+    const int b = blockIdx.x;
+    if (b < a.nbp) {
+        plane_partial(a, b);
+        return;
+    }
+    for (int s = 0; s < a.ng; ++s)
+        if (b >= a.g[s].block0 && b < a.g[s].block0 + a.g[s].nblocks) {
+            gather_one(a, a.g[s], b);
+            return;
+        }
+}
 
+// Plane sums of L steps from their block partials, block q summing step q's
+// partials in block order; out[(sc[0].step + q) * 12 + c].
+__global__ void plane_sums_reduce(const double *partial, int nbp, const StepScalars *sc, double *out) {
+    const int q = blockIdx.x, c = threadIdx.x;
+    if (c >= 12) return;
+    double s = 0;
+    const double *p = partial + (long long)q * nbp * 12;
+    for (int b = 0; b < nbp; ++b) s += p[b * 12 + c];
+    out[((long long)sc[0].step + q) * 12 + c] = s;
+}
 
 // s_curve (src/common/mathUT.cpp:1186-1193)
 __device__ __forceinline__ double s_curve_dev(double x, double xmin, double xmax) {
@@ -121,7 +144,7 @@ __global__ void dft_phasors(PhasorArgs a) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= a.nk * a.nl) return;
     const int kk = t / a.nl, l = t % a.nl;
-    const int step = a.step0 + kk;
+    const int step = (a.step_ptr ? *a.step_ptr : 0) + a.step_add + kk;
     // tapering_E/H in effect at `step` were set after feeding step-1.
     double tE = 1.0, tH = 1.0;
     if (step - 1 >= a.Nt - a.Ntap && step >= 1) {

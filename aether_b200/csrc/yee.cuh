@@ -1,21 +1,28 @@
-// yee.cuh — fused E and H half-step kernels (one launch per half-step).
+// yee.cuh — fused E and H half-step kernels.
 //
-// The E kernel fuses, per cell, the six phases of FDTD::update_E
+// The E half-step fuses, per cell, the six phases of FDTD::update_E
 // (src/finite_differences/FDTD/core/fdtd_core.cpp:1163-1218 driving
 // fdtd_threads.cpp:32-150): recursive-convolution "ante" update with E^n
 // (mats_RC.cpp:21-36), the Yee curl update (fdtd_core.cpp:363-541), the RC
 // apply (mats_RC.cpp:38-50), the CPML psi updates and PEC planes in the
 // reference's order (fdtd_pml.cpp:504-735), then the normal-mode plane
 // injection (normal_incidence.cpp:338-342) or Oscillator boxes
-// (sc_oscillator.cpp:34-67). The H kernel fuses advHx/Hy/Hz
+// (sc_oscillator.cpp:34-67). The H half-step fuses advHx/Hy/Hz
 // (fdtd_core.cpp:546-698), app_pml_H* (fdtd_pml.cpp:737-929) and the H plane
 // injection (normal_incidence.cpp:353-357). Every phase of the reference only
 // reads the other field family plus the cell's own state, so fusing them per
 // cell is exact.
 //
-// Threads own one (i, j) column and march kchunk planes along z, carrying the
-// z-1 (E kernel) or z+1 (H kernel) plane in registers; x and y neighbours
-// come through L1. Loads along x are coalesced (x is the fastest index).
+// Work decomposition. The grid is cut into work items: a 32 x 4 tile of
+// (i, j) columns times a z-chunk. A CTA of 32 x 4 threads takes one item;
+// each thread owns one column and marches the chunk along z, carrying the z-1
+// (E) or z+1 (H) plane in registers, with x and y neighbours through L1. The
+// host sorts the items into two lists (runtime.cpp, build_work): "interior"
+// items, in which no cell is in a CPML range or PEC plane, dispersive, on the
+// injection plane or inside a source box, run a lean kernel that does only the
+// curl update (few registers, full occupancy); the other items run the full
+// kernel. Both lists are launched for every half-step and cover each cell
+// exactly once.
 //
 // FP64 instantiation (compiled with --fmad=false): operation order equals the
 // reference's expression order, so results are bit-identical to the CPU
@@ -32,32 +39,121 @@ namespace aefdtd {
 
 template <typename T> struct Exact { static constexpr bool value = std::is_same<T, double>::value; };
 
+constexpr int kTileX = 32;
+constexpr int kTileY = 4;
+
 // psi_new = b*psi + c*diff (FP64, reference order) or psi + ((b-1)*psi + c*diff) (FP32)
 template <typename T> __device__ __forceinline__ T cpml_rec(T b, T psi, T c, T diff) {
     if constexpr (Exact<T>::value) return b * psi + c * diff;
     else return psi + (b * psi + c * diff);
 }
 
+// ---- interior items: curl update only -----------------------------------
 template <typename T, typename Tid>
-__global__ void __launch_bounds__(128) e_half_step(StepArgs<T, Tid> a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+__global__ void __launch_bounds__(kTileX * kTileY, 12) e_interior(const __grid_constant__ StepArgs<T, Tid> a,
+                                                                  const int4 *__restrict__ items) {
+    // coefficients through the read-only path: short-lived CTAs skip a table fill and barrier
+    const int4 it = items[blockIdx.x];
+    const int i = it.x + threadIdx.x, j = it.y + threadIdx.y;
     if (i >= a.Nx || j >= a.Ny) return;
-    const int k0 = blockIdx.z * a.kchunk;
-    const int k1 = min(a.Nz, k0 + a.kchunk);
     const long long NxNy = a.NxNy;
     const int im = (i == 0) ? a.Nx - 1 : i - 1;
     const int jm = (j == 0) ? a.Ny - 1 : j - 1;
     const long long col = i + (long long)j * a.Nx;
     const long long colx = im + (long long)j * a.Nx;
     const long long coly = i + (long long)jm * a.Nx;
+    const long long colm = i + (long long)j * a.mpitch;
+    const long long mNxNy = (long long)a.mpitch * a.Ny;
+    const T *__restrict__ Hx = a.Hx;
+    const T *__restrict__ Hy = a.Hy;
+    const T *__restrict__ Hz = a.Hz;
+    T *__restrict__ Ex = a.Ex;
+    T *__restrict__ Ey = a.Ey;
+    T *__restrict__ Ez = a.Ez;
+    const T ikx = a.ikx[i], iky = a.iky[j];
+    const int kmi = (it.z == 0) ? a.Nz - 1 : it.z - 1;
+    T hx_km = __ldg(Hx + col + kmi * NxNy);
+    T hy_km = __ldg(Hy + col + kmi * NxNy);
+    for (int k = it.z; k < it.w; ++k) {
+        const long long id = col + k * NxNy;
+        const T hx = __ldg(Hx + id), hy = __ldg(Hy + id), hz = __ldg(Hz + id);
+        const T hz_jm = __ldg(Hz + coly + k * NxNy), hx_jm = __ldg(Hx + coly + k * NxNy);
+        const T hz_im = __ldg(Hz + colx + k * NxNy), hy_im = __ldg(Hy + colx + k * NxNy);
+        const T ex = Ex[id], ey = Ey[id], ez = Ez[id];
+        const int m = __ldg(a.mat + colm + k * mNxNy);
+        const MatCoef<T> *cp = a.coef + m;
+        const MatCoef<T> c{__ldg(&cp->C1), __ldg(&cp->C2x), __ldg(&cp->C2y), __ldg(&cp->C2z), T(0), T(0)};
+        const T ikz = a.ikz[k];
+        Ex[id] = (c.C1 * ex + (c.C2y * iky) * (hz - hz_jm)) - (c.C2z * ikz) * (hy - hy_km);
+        Ey[id] = (c.C1 * ey + (c.C2z * ikz) * (hx - hx_km)) - (c.C2x * ikx) * (hz - hz_im);
+        Ez[id] = (c.C1 * ez + (c.C2x * ikx) * (hy - hy_im)) - (c.C2y * iky) * (hx - hx_jm);
+        hx_km = hx;
+        hy_km = hy;
+    }
+}
+
+template <typename T, typename Tid>
+__global__ void __launch_bounds__(kTileX * kTileY, 12) h_interior(const __grid_constant__ StepArgs<T, Tid> a,
+                                                                  const int4 *__restrict__ items) {
+    const int4 it = items[blockIdx.x];
+    const int i = it.x + threadIdx.x, j = it.y + threadIdx.y;
+    if (i >= a.Nx || j >= a.Ny) return;
+    const long long NxNy = a.NxNy;
+    const int ip = (i == a.Nx - 1) ? 0 : i + 1;
+    const int jp = (j == a.Ny - 1) ? 0 : j + 1;
+    const long long col = i + (long long)j * a.Nx;
+    const long long colx = ip + (long long)j * a.Nx;
+    const long long coly = i + (long long)jp * a.Nx;
+    const T *__restrict__ Ex = a.Ex;
+    const T *__restrict__ Ey = a.Ey;
+    const T *__restrict__ Ez = a.Ez;
+    T *__restrict__ Hx = a.Hx;
+    T *__restrict__ Hy = a.Hy;
+    T *__restrict__ Hz = a.Hz;
+    const T ax = a.dtdmx * a.ikx[i];
+    const T ay = a.dtdmy * a.iky[j];
+    T ex = __ldg(Ex + col + it.z * NxNy);
+    T ey = __ldg(Ey + col + it.z * NxNy);
+    for (int k = it.z; k < it.w; ++k) {
+        const long long id = col + k * NxNy;
+        const int kp = (k == a.Nz - 1) ? 0 : k + 1;
+        const T ex_kp = __ldg(Ex + col + kp * NxNy), ey_kp = __ldg(Ey + col + kp * NxNy);
+        const T ez = __ldg(Ez + id);
+        const T ez_jp = __ldg(Ez + coly + k * NxNy), ex_jp = __ldg(Ex + coly + k * NxNy);
+        const T ez_ip = __ldg(Ez + colx + k * NxNy), ey_ip = __ldg(Ey + colx + k * NxNy);
+        const T hx = Hx[id], hy = Hy[id], hz = Hz[id];
+        const T az = a.dtdmz * a.ikz[k];
+        Hx[id] = hx + (az * (ey_kp - ey) - ay * (ez_jp - ez));
+        Hy[id] = hy + (ax * (ez_ip - ez) - az * (ex_kp - ex));
+        Hz[id] = hz + (ay * (ex_jp - ex) - ax * (ey_ip - ey));
+        ex = ex_kp;
+        ey = ey_kp;
+    }
+}
+
+// ---- boundary items: every phase ------------------------------------------
+template <typename T, typename Tid>
+__global__ void __launch_bounds__(kTileX * kTileY) e_boundary(const __grid_constant__ StepArgs<T, Tid> a,
+                                                              const int4 *__restrict__ items) {
+    const int4 it = items[blockIdx.x];
+    const int i = it.x + threadIdx.x, j = it.y + threadIdx.y;
+    if (i >= a.Nx || j >= a.Ny) return;
+    const int k0 = it.z, k1 = it.w;
+    const long long NxNy = a.NxNy;
+    const int im = (i == 0) ? a.Nx - 1 : i - 1;
+    const int jm = (j == 0) ? a.Ny - 1 : j - 1;
+    const long long col = i + (long long)j * a.Nx;
+    const long long colx = im + (long long)j * a.Nx;
+    const long long coly = i + (long long)jm * a.Nx;
+    const long long colm = i + (long long)j * a.mpitch;
+    const long long mNxNy = (long long)a.mpitch * a.Ny;
     const T ikx = a.ikx[i];
     const T iky = a.iky[j];
 
     // E-side CPML index ranges: [1, pml_m) and [N - pml_p + 1, N) (fdtd_pml.cpp:518,527,547,559)
     const bool xe = a.px && ((i >= 1 && i < a.pml_xm) || (i >= a.Nx - a.pml_xp + 1));
     const bool ye = a.py && ((j >= 1 && j < a.pml_ym) || (j >= a.Ny - a.pml_yp + 1));
-    const int nxs = a.pml_xm + a.pml_xp, nys = a.pml_ym + a.pml_yp, nzs = a.pml_zm + a.pml_zp;
+    const int nxs = a.pml_xm + a.pml_xp, nys = a.pml_ym + a.pml_yp;
     const int xn = (i < a.pml_xm) ? i : i - (a.Nx - a.pml_xp) + a.pml_xm;
     const int yn = (j < a.pml_ym) ? j : j - (a.Ny - a.pml_yp) + a.pml_ym;
     T bxi = 0, cxi = 0, byj = 0, cyj = 0;
@@ -74,42 +170,39 @@ __global__ void __launch_bounds__(128) e_half_step(StepArgs<T, Tid> a) {
         const T hz_jm = a.Hz[coly + k * NxNy], hx_jm = a.Hx[coly + k * NxNy];
         const T hz_im = a.Hz[colx + k * NxNy], hy_im = a.Hy[colx + k * NxNy];
         const T ex = a.Ex[id], ey = a.Ey[id], ez = a.Ez[id];
-        const int m = a.mat[id];
+        const int m = __ldg(a.mat + colm + k * mNxNy);
         const MatCoef<T> c = a.coef[m];
+        const int np_m = a.disp ? __ldg(&a.disp[m].np) : 0;
         const T ikz = a.ikz[k];
 
         // Recursive-convolution "ante" with E^n; sums of Re(psi) per component.
         T s0 = 0, s1 = 0, s2 = 0;
-        bool disp = false;
-        if (a.disp != nullptr) {
+        if (np_m > 0) {
             const DispInfo d = a.disp[m];
-            if (d.np > 0) {
-                disp = true;
-                const long long q = (i - d.x1) + (long long)(j - d.y1) * d.xs + (long long)(k - d.z1) * d.xs * d.ys;
-                Cplx<T> *P = a.psi + d.psi_off + q;
-                for (int p = 0; p < d.np; ++p) {
-                    const Cplx<T> cr = a.crec[d.pole_off + p];
-                    const Cplx<T> dc = a.dchi[d.pole_off + p];
-                    const T ev[3] = {ex, ey, ez};
+            const long long q = (i - d.x1) + (long long)(j - d.y1) * d.xs + (long long)(k - d.z1) * d.xs * d.ys;
+            Cplx<T> *P = a.psi + d.psi_off + q;
+            for (int p = 0; p < d.np; ++p) {
+                const Cplx<T> cr = a.crec[d.pole_off + p];
+                const Cplx<T> dc = a.dchi[d.pole_off + p];
+                const T ev[3] = {ex, ey, ez};
 #pragma unroll
-                    for (int dd = 0; dd < 3; ++dd) {
-                        Cplx<T> *pp = P + (long long)(3 * p + dd) * d.box;
-                        const Cplx<T> v = *pp;
-                        Cplx<T> r;
-                        if constexpr (Exact<T>::value) {
-                            // Crec*psi + Dchi*E with std::complex<double> rounding order
-                            r.re = (cr.re * v.re - cr.im * v.im) + dc.re * ev[dd];
-                            r.im = (cr.re * v.im + cr.im * v.re) + dc.im * ev[dd];
-                        } else {
-                            // (Crec-1) stored: psi + ((Crec-1)*psi + Dchi*E)
-                            r.re = v.re + ((cr.re * v.re - cr.im * v.im) + dc.re * ev[dd]);
-                            r.im = v.im + ((cr.re * v.im + cr.im * v.re) + dc.im * ev[dd]);
-                        }
-                        *pp = r;
-                        if (dd == 0) s0 = s0 + r.re;
-                        else if (dd == 1) s1 = s1 + r.re;
-                        else s2 = s2 + r.re;
+                for (int dd = 0; dd < 3; ++dd) {
+                    Cplx<T> *pp = P + (long long)(3 * p + dd) * d.box;
+                    const Cplx<T> v = *pp;
+                    Cplx<T> r;
+                    if constexpr (Exact<T>::value) {
+                        // Crec*psi + Dchi*E with std::complex<double> rounding order
+                        r.re = (cr.re * v.re - cr.im * v.im) + dc.re * ev[dd];
+                        r.im = (cr.re * v.im + cr.im * v.re) + dc.im * ev[dd];
+                    } else {
+                        // (Crec-1) stored: psi + ((Crec-1)*psi + Dchi*E)
+                        r.re = v.re + ((cr.re * v.re - cr.im * v.im) + dc.re * ev[dd]);
+                        r.im = v.im + ((cr.re * v.im + cr.im * v.re) + dc.im * ev[dd]);
                     }
+                    *pp = r;
+                    if (dd == 0) s0 = s0 + r.re;
+                    else if (dd == 1) s1 = s1 + r.re;
+                    else s2 = s2 + r.re;
                 }
             }
         }
@@ -120,7 +213,7 @@ __global__ void __launch_bounds__(128) e_half_step(StepArgs<T, Tid> a) {
         T nex = (c.C1 * ex + (c.C2y * iky) * dHz_y) - (c.C2z * ikz) * dHy_z;
         T ney = (c.C1 * ey + (c.C2z * ikz) * dHx_z) - (c.C2x * ikx) * dHz_x;
         T nez = (c.C1 * ez + (c.C2x * ikx) * dHy_x) - (c.C2y * iky) * dHx_y;
-        if (disp) {
+        if (np_m > 0) {
             nex += c.C3 * s0;
             ney += c.C3 * s1;
             nez += c.C3 * s2;
@@ -179,16 +272,17 @@ __global__ void __launch_bounds__(128) e_half_step(StepArgs<T, Tid> a) {
 
         // Normal-incidence plane injection after update_E (normal_incidence.cpp:338-342)
         if (k == a.kinj) {
-            nex = nex - a.inj_a;
-            ney = ney + a.inj_b;
+            nex = nex - (T)a.sc[a.q].inj_eA;
+            ney = ney + (T)a.sc[a.q].inj_eB;
         }
         // Oscillator boxes after update_E (sc_oscillator.cpp:43-63)
         for (int s = 0; s < a.nsrc; ++s) {
             const int *b = a.src_box[s];
             if (i >= b[0] && i < b[1] && j >= b[2] && j < b[3] && k >= b[4] && k < b[5]) {
-                if (a.src_comp[s] == 0) nex += a.src_val[s];
-                else if (a.src_comp[s] == 1) ney += a.src_val[s];
-                else nez += a.src_val[s];
+                const T v = (T)a.sc[a.q].src[s];
+                if (a.src_comp[s] == 0) nex += v;
+                else if (a.src_comp[s] == 1) ney += v;
+                else nez += v;
             }
         }
 
@@ -201,12 +295,12 @@ __global__ void __launch_bounds__(128) e_half_step(StepArgs<T, Tid> a) {
 }
 
 template <typename T, typename Tid>
-__global__ void __launch_bounds__(128) h_half_step(StepArgs<T, Tid> a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+__global__ void __launch_bounds__(kTileX * kTileY) h_boundary(const __grid_constant__ StepArgs<T, Tid> a,
+                                                              const int4 *__restrict__ items) {
+    const int4 it = items[blockIdx.x];
+    const int i = it.x + threadIdx.x, j = it.y + threadIdx.y;
     if (i >= a.Nx || j >= a.Ny) return;
-    const int k0 = blockIdx.z * a.kchunk;
-    const int k1 = min(a.Nz, k0 + a.kchunk);
+    const int k0 = it.z, k1 = it.w;
     const long long NxNy = a.NxNy;
     const int ip = (i == a.Nx - 1) ? 0 : i + 1;
     const int jp = (j == a.Ny - 1) ? 0 : j + 1;
@@ -298,8 +392,8 @@ __global__ void __launch_bounds__(128) h_half_step(StepArgs<T, Tid> a) {
 
         // H plane injection after update_H (normal_incidence.cpp:353-357)
         if (k == a.kinj) {
-            nhx = nhx + a.inj_a;
-            nhy = nhy - a.inj_b;
+            nhx = nhx + (T)a.sc[a.q].inj_hA;
+            nhy = nhy - (T)a.sc[a.q].inj_hB;
         }
         a.Hx[id] = nhx;
         a.Hy[id] = nhy;

@@ -4,8 +4,28 @@
 #include "yee.cuh"
 
 namespace aefdtd {
-void launch_e(const StepArgs<double, uint8_t> &a, dim3 g, dim3 b, cudaStream_t s) { e_half_step<<<g, b, 0, s>>>(a); }
-void launch_e(const StepArgs<double, uint16_t> &a, dim3 g, dim3 b, cudaStream_t s) { e_half_step<<<g, b, 0, s>>>(a); }
-void launch_h(const StepArgs<double, uint8_t> &a, dim3 g, dim3 b, cudaStream_t s) { h_half_step<<<g, b, 0, s>>>(a); }
-void launch_h(const StepArgs<double, uint16_t> &a, dim3 g, dim3 b, cudaStream_t s) { h_half_step<<<g, b, 0, s>>>(a); }
+void launch_e_interior(const StepArgs<double, uint8_t> &a, const int4 *items, int n, cudaStream_t s) {
+    if (n > 0) e_interior<double, uint8_t><<<n, dim3(kTileX, kTileY), 0, s>>>(a, items);
+}
+void launch_e_boundary(const StepArgs<double, uint8_t> &a, const int4 *items, int n, cudaStream_t s) {
+    if (n > 0) e_boundary<double, uint8_t><<<n, dim3(kTileX, kTileY), 0, s>>>(a, items);
+}
+void launch_h_interior(const StepArgs<double, uint8_t> &a, const int4 *items, int n, cudaStream_t s) {
+    if (n > 0) h_interior<double, uint8_t><<<n, dim3(kTileX, kTileY), 0, s>>>(a, items);
+}
+void launch_h_boundary(const StepArgs<double, uint8_t> &a, const int4 *items, int n, cudaStream_t s) {
+    if (n > 0) h_boundary<double, uint8_t><<<n, dim3(kTileX, kTileY), 0, s>>>(a, items);
+}
+void launch_e_interior(const StepArgs<double, uint16_t> &a, const int4 *items, int n, cudaStream_t s) {
+    if (n > 0) e_interior<double, uint16_t><<<n, dim3(kTileX, kTileY), 0, s>>>(a, items);
+}
+void launch_e_boundary(const StepArgs<double, uint16_t> &a, const int4 *items, int n, cudaStream_t s) {
+    if (n > 0) e_boundary<double, uint16_t><<<n, dim3(kTileX, kTileY), 0, s>>>(a, items);
+}
+void launch_h_interior(const StepArgs<double, uint16_t> &a, const int4 *items, int n, cudaStream_t s) {
+    if (n > 0) h_interior<double, uint16_t><<<n, dim3(kTileX, kTileY), 0, s>>>(a, items);
+}
+void launch_h_boundary(const StepArgs<double, uint16_t> &a, const int4 *items, int n, cudaStream_t s) {
+    if (n > 0) h_boundary<double, uint16_t><<<n, dim3(kTileX, kTileY), 0, s>>>(a, items);
+}
 }  // namespace aefdtd

@@ -917,3 +917,95 @@ extern "C" int aeoracle_run(const aefdtd_grid_desc *g, const uint32_t *map,
     }
     return 0;
 }
+
+// ---------------------------------------------------------------------------
+// Structure discretisation: Structure::discretize (src/structure/structure.cpp:94-113)
+// with Structure::index (structure.cpp:228-258, no flips) and the primitive
+// tests Add_Block::index (structure_primitives.cpp:24-39), Add_Layer::index
+// (:317-339), Add_Sphere::index (:484-499), Add_Cylinder (:255-285, with
+// Vector3::norm/normalize, src/common/vector23.cpp:266-282, and
+// scalar_prod, vector23.cpp:702-705).
+namespace {
+struct OOp {
+    int kind, mat;
+    double p[8];
+    double bx, by, bz, length;
+};
+
+int oop_index(const OOp &o, double x, double y, double z) {
+    switch (o.kind) {
+        case AEFDTD_OP_BLOCK:
+            if (x < o.p[0] || x >= o.p[1] || y < o.p[2] || y >= o.p[3] || z < o.p[4] || z >= o.p[5]) return -1;
+            return o.mat;
+        case AEFDTD_OP_LAYER: {
+            int t = (int)o.p[0];
+            if (t == 0 && x >= o.p[1] && x < o.p[2]) return o.mat;
+            if (t == 1 && y >= o.p[1] && y < o.p[2]) return o.mat;
+            if (t == 2 && z >= o.p[1] && z < o.p[2]) return o.mat;
+            return -1;
+        }
+        case AEFDTD_OP_SPHERE: {
+            x = x - o.p[0]; y = y - o.p[1]; z = z - o.p[2];
+            if (x * x + y * y + z * z <= o.p[3] * o.p[3]) return o.mat;
+            return -1;
+        }
+        case AEFDTD_OP_CYLINDER: {
+            double x1 = o.p[0], y1 = o.p[1], z1 = o.p[2], x2 = o.p[3], y2 = o.p[4], z2 = o.p[5], r = o.p[6];
+            if (x < std::min(x1, x2) - r || x > std::max(x1, x2) + r || y < std::min(y1, y2) - r ||
+                y > std::max(y1, y2) + r || z < std::min(z1, z2) - r || z > std::max(z1, z2) + r)
+                return -1;
+            double dx = x - x1, dy = y - y1, dz = z - z1;
+            double proj = o.bx * dx + o.by * dy + o.bz * dz;
+            if (proj >= 0 && proj <= o.length) {
+                dx = dx - proj * o.bx; dy = dy - proj * o.by; dz = dz - proj * o.bz;
+                double rt = dx * dx + dy * dy + dz * dz;
+                if (rt <= r * r) return o.mat;
+            }
+            return -1;
+        }
+    }
+    return -1;
+}
+}  // namespace
+
+extern "C" int aeoracle_voxelize(int32_t nx, int32_t ny, int32_t nz, double dx, double dy, double dz,
+                                 const aefdtd_structure_op *ops, int32_t n_ops, int32_t def,
+                                 const int32_t periodic[3], const double lengths[3], uint32_t *out) {
+    std::vector<OOp> v(n_ops);
+    for (int q = 0; q < n_ops; q++) {
+        OOp &o = v[q];
+        o.kind = ops[q].kind; o.mat = ops[q].mat_index;
+        for (int t = 0; t < 8; t++) o.p[t] = ops[q].p[t];
+        o.bx = o.by = o.bz = o.length = 0;
+        if (o.kind == AEFDTD_OP_BLOCK)
+            for (int a = 0; a < 3; a++) if (o.p[2 * a] > o.p[2 * a + 1]) std::swap(o.p[2 * a], o.p[2 * a + 1]);
+        if (o.kind == AEFDTD_OP_CYLINDER) {
+            double vx = o.p[3] - o.p[0], vy = o.p[4] - o.p[1], vz = o.p[5] - o.p[2];
+            double n = std::sqrt(vx * vx + vy * vy + vz * vz);
+            o.length = n;
+            o.bx = vx / n; o.by = vy / n; o.bz = vz / n;
+        }
+    }
+    int per[3] = {periodic ? (periodic[0] ? 1 : 0) : 0, periodic ? (periodic[1] ? 1 : 0) : 0,
+                  periodic ? (periodic[2] ? 1 : 0) : 0};
+    double L[3] = {lengths ? lengths[0] : 0, lengths ? lengths[1] : 0, lengths ? lengths[2] : 0};
+    for (int i = 0; i < nx; i++)
+        for (int j = 0; j < ny; j++)
+            for (int k = 0; k < nz; k++) {
+                double x = i * dx, y = j * dy, z = k * dz;
+                if (per[0]) { while (x < 0) x += L[0]; while (x >= L[0]) x -= L[0]; }
+                if (per[1]) { while (y < 0) y += L[1]; while (y >= L[1]) y -= L[1]; }
+                if (per[2]) { while (z < 0) z += L[2]; while (z >= L[2]) z -= L[2]; }
+                int res = def;
+                bool found = false;
+                for (int l = n_ops - 1; l >= 0 && !found; l--)
+                    for (int a = -per[0]; a <= per[0] && !found; a++)
+                        for (int b = -per[1]; b <= per[1] && !found; b++)
+                            for (int c = -per[2]; c <= per[2] && !found; c++) {
+                                int h = oop_index(v[l], x + a * L[0], y + b * L[1], z + c * L[2]);
+                                if (h != -1) { res = h; found = true; }
+                            }
+                out[i + size_t(j) * nx + size_t(k) * nx * ny] = (uint32_t)res;
+            }
+    return 0;
+}

@@ -120,3 +120,74 @@ def test_fp32_custom_mode_close_to_fp64_oracle():
     a = oracle_lib.run(scenes.custom_box(nsteps=100), "port")
     b = fdtd.run(scenes.custom_box(precision=A.FP32, nsteps=100))
     assert rel(b["fields"], a["fields"]) < FP32_REL_FIELD
+
+
+@pytest.mark.parametrize("prec", [A.FP64, A.FP32])
+def test_interior_and_boundary_kernels_agree(prec, monkeypatch):
+    """Items run by the curl-only interior kernels give the same cells as the
+    full kernels: bit-identical in FP64, 1e-6 relative in FP32."""
+    sc = scenes.gold_sphere(precision=prec, nsteps=80)
+    a = fdtd.run(sc)
+    monkeypatch.setenv("AEFDTD_ALL_BOUNDARY", "1")
+    b = fdtd.run(sc)
+    if prec == A.FP64:
+        assert np.array_equal(a["fields"], b["fields"])
+    else:
+        assert rel(a["fields"], b["fields"]) < 1e-6
+
+
+@pytest.mark.parametrize("kchunk", ["1", "3", "1000"])
+def test_z_chunking_does_not_change_results(kchunk, monkeypatch):
+    sc = scenes.custom_box(nsteps=40)
+    a = fdtd.run(sc)
+    monkeypatch.setenv("AEFDTD_KCHUNK", kchunk)
+    b = fdtd.run(sc)
+    assert np.array_equal(a["fields"], b["fields"])
+
+
+def test_graph_replay_matches_direct_launches(monkeypatch):
+    """Whole 64-step segments replayed from CUDA graphs (default) against the
+    same steps launched one by one."""
+    sc = scenes.gold_sphere(nsteps=200)
+    a = fdtd.run(sc)
+    monkeypatch.setenv("AEFDTD_NO_GRAPHS", "1")
+    b = fdtd.run(sc)
+    assert np.array_equal(a["fields"], b["fields"])
+    assert np.array_equal(a["plane_sums"], b["plane_sums"])
+    for fa, fb in zip(a["flux"], b["flux"]):
+        assert np.array_equal(fa, fb)
+    assert a["launches"] == b["launches"]
+
+
+def test_timing_mode_does_not_change_results():
+    sc = scenes.slab_tm(nsteps=100)
+    with fdtd.build_simulation(sc) as s1, fdtd.build_simulation(sc) as s2:
+        s1.step(100)
+        s2.enable_timing(True)
+        s2.step(100)
+        e, h, s = s2.timings()
+        assert e > 0 and h > 0 and s >= 0
+        assert np.array_equal(s1.fields(), s2.fields())
+
+
+def test_fp32_tensor_core_dft_matches_simt_dft(monkeypatch):
+    """FP32 path: the DFT blocks on the tensor cores (tcgen05, 3xTF32) against
+    the FP64 SIMT accumulation of the same samples."""
+    sc = scenes.gold_sphere(precision=A.FP32, nsteps=192)
+    a = fdtd.run(sc, want_fields=False)
+    monkeypatch.setenv("AEFDTD_NO_TC", "1")
+    b = fdtd.run(sc, want_fields=False)
+    for fa, fb in zip(a["flux"], b["flux"]):
+        assert np.max(np.abs(fa - fb)) <= 1e-5 * np.max(np.abs(fb))
+
+
+def test_fp32_tensor_core_dft_many_wavelengths():
+    """Two N tiles (2 nl > 256 columns) and a partial last block."""
+    sc64 = scenes.slab_tm(nsteps=150)
+    sc32 = scenes.slab_tm(precision=A.FP32, nsteps=150)
+    for s in sc64.sensors + sc32.sensors:
+        s.nl = 201
+    a = oracle_lib.run(sc64, "port", want_fields=False)
+    b = fdtd.run(sc32, want_fields=False)
+    for fa, fb in zip(a["flux"], b["flux"]):
+        assert np.max(np.abs(fb - fa)) <= 2e-3 * np.max(np.abs(fa))
