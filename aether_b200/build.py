@@ -33,6 +33,7 @@ UNITS = [
     ("sensors.cu", []),
     ("dft_tc.cu", []),
     ("voxel.cu", ["--fmad=false"]),
+    ("plane_static.cu", []),
     ("runtime.cpp", None),
 ]
 HEADERS = ["aefdtd_dev.hpp", "kernels.hpp", "sensors.cuh", "yee.cuh"]

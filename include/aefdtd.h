@@ -259,6 +259,31 @@ aefdtd_status aefdtd_get_stream(aefdtd_sim *sim, void **stream);
 /* Number of device kernel launches issued by this handle since creation. */
 aefdtd_status aefdtd_get_launch_count(aefdtd_sim *sim, uint64_t *launches);
 
+/* ---- allocation-free diagnostics -------------------------------------- */
+
+/* No counterpart in the reference: an entry point for callers that must not
+ * allocate device memory (a process whose device memory is committed up
+ * front, e.g. a batch or serving loop admitted to a fixed share of HBM).
+ *
+ * out[p*3 + c] = sum over the whole x-y plane planes[p] of weight * fields[c],
+ * summed in FP64 in the same order as the stepping path's transmission-plane
+ * sums (aefdtd_get_plane_sums slots 9..11 for plane zs_s). fields: host array
+ * of 3 device pointers, each nx*ny*nz values (x fastest) of the given
+ * precision on the current device; out: 3*n_planes doubles of device memory
+ * on the current device. Kernels are enqueued on `stream` (a cudaStream_t,
+ * NULL = default stream); the call does not wait for them.
+ *
+ * Calls no allocating routine. Its scratch is a fixed 96 KiB device array
+ * held by every device that loads the library until exit, which caps a call
+ * at AEFDTD_STATIC_MAX_PLANES planes: more returns AEFDTD_BAD_ARG with the
+ * reason in errbuf (may be NULL). The first call on a device resolves that
+ * array's address there; make it before any stream capture on the device.
+ * All calls share the array, so calls that overlap on the device race. */
+#define AEFDTD_STATIC_MAX_PLANES 64
+aefdtd_status aefdtd_plane_sums_static(const void *const *fields, int32_t precision, int32_t nx, int32_t ny,
+                                       int32_t nz, const int32_t *planes, int32_t n_planes, double weight,
+                                       double *out, void *stream, char *errbuf, size_t errbuf_len);
+
 #ifdef __cplusplus
 }
 #endif
