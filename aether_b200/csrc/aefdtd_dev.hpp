@@ -87,6 +87,15 @@ template <typename T, typename Tid> struct StepArgs {
     int *err;                       // device error flag (bounded waits)
 };
 
+// Item groups of one half-step: a device array of int4 items (x0, y0, k0,
+// k1) sorted by group; group g is items [off[g], off[g] + n[g]).
+enum { kGroupInterior = 0, kGroupPmlZ = 1, kGroupDisp = 2, kGroupAll = 3, kGroups = 4 };
+struct WorkSplit {
+    int off[kGroups];
+    int n[kGroups];
+    int unroll;                     // z-planes per iteration of the interior kernels (1 or 2)
+};
+
 // ---- sensor-path launch arguments (kernels in sensors.cuh)
 
 struct PulseDev {
@@ -163,6 +172,7 @@ struct DftTcArgs {
     int *err;
 };
 constexpr int kDftTcMaxK = 64;
+constexpr int kDftTcThreads = 512;   // 16 warps: 4 per TMEM lane quarter
 constexpr int kDftTcSmem = (128 * kDftTcMaxK * 2 + 256 * kDftTcMaxK * 2) * 4 + 64;
 
 constexpr int kPlaneBlocks = 64;    // plane-sum stage-1 blocks

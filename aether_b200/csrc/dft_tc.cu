@@ -160,8 +160,12 @@ __global__ void dft_phasors_tc(DftTcPhasorArgs a) {
     base[3 * part + off] = __uint_as_float(to_tf32(vH - __uint_as_float(hh)));
 }
 
-// grid: (ceil(P / 128), 6); block 128; dynamic smem kDftTcSmem
-__global__ void __launch_bounds__(128, 1) dft_accumulate_tc(const __grid_constant__ DftTcArgs a) {
+// grid: (ceil(P / 128), 6); block kDftTcThreads (16 warps); dynamic smem
+// kDftTcSmem. Warp w reads TMEM lanes 32 (w % 4) .. 32 (w % 4) + 31 (the
+// lane quarter a warp may access) and the 16-column chunks w / 4, w / 4 + 4,
+// ... of the tile, so four warps share each lane quarter and the FP64
+// accumulator read-modify-write has 16 warps of loads in flight per SM.
+__global__ void __launch_bounds__(kDftTcThreads, 1) dft_accumulate_tc(const __grid_constant__ DftTcArgs a) {
     extern __shared__ __align__(1024) unsigned char sm[];
     const int K = a.K;
     float *Ahi = reinterpret_cast<float *>(sm);
@@ -170,7 +174,7 @@ __global__ void __launch_bounds__(128, 1) dft_accumulate_tc(const __grid_constan
     float *Blo = Bhi + 256 * K;
     uint64_t *bars = reinterpret_cast<uint64_t *>(Blo + 256 * K);   // [0]: B copies, [1]: MMA done
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2);
-    const int tid = threadIdx.x, warp = tid >> 5;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int c = blockIdx.y;
     const int p0 = blockIdx.x * 128;
     const int fam = c < 3 ? 0 : 2;   // E or H phasors
@@ -189,11 +193,12 @@ __global__ void __launch_bounds__(128, 1) dft_accumulate_tc(const __grid_constan
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    // A: this CTA's 128 points of component c, TF32 hi / lo
+    // A: this CTA's 128 points of component c, TF32 hi / lo; thread (m, kq)
+    // converts steps kq, kq + 4, ... of point m
     {
-        const int m = tid;
+        const int m = tid & 127, kq = tid >> 7;
         const int p = p0 + m;
-        for (int k = 0; k < K; ++k) {
+        for (int k = kq; k < K; k += kDftTcThreads / 128) {
             const float v = (p < a.P && k < a.nk) ? a.S[((size_t)k * 6 + c) * a.P + p] : 0.f;
             const uint32_t h = to_tf32(v);
             const uint32_t o = km_off(m, k, 128) / 4;
@@ -204,6 +209,9 @@ __global__ void __launch_bounds__(128, 1) dft_accumulate_tc(const __grid_constan
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
 
+    const int lq = warp & 3, cg = warp >> 2;
+    const int p = p0 + lq * 32 + lane;
+    const uint32_t tlane = (uint32_t)(lq * 32) << 16;
     bool ok = true;
     const int ntiles = a.N1 > 0 ? 2 : 1;
     for (int t = 0; t < ntiles && ok; ++t) {
@@ -215,8 +223,8 @@ __global__ void __launch_bounds__(128, 1) dft_accumulate_tc(const __grid_constan
             bulk_g2s(Bhi, src, part, &bars[0]);
             bulk_g2s(Blo, src + (size_t)Nt * K, part, &bars[0]);
         }
-        if (!bar_wait(&bars[0], t & 1)) { ok = false; break; }
-        if (tid == 0) {
+        if (!bar_wait(&bars[0], t & 1)) ok = false;
+        if (tid == 0 && ok) {
             tc_fence_after();
             const uint32_t idesc = instr_desc(Nt);
             const uint32_t lboA = 16 * 128, lboB = (uint32_t)(Nt / 8) * 128;   // between the two K chunks
@@ -231,26 +239,31 @@ __global__ void __launch_bounds__(128, 1) dft_accumulate_tc(const __grid_constan
             }
             mma_commit(&bars[1]);
         }
-        if (!bar_wait(&bars[1], t & 1)) { ok = false; break; }
+        if (ok && !bar_wait(&bars[1], t & 1)) ok = false;
+        // every thread leaves the tile loop together: a failed wait on any
+        // thread stops all of them before the next tile's copies
+        ok = __syncthreads_and(ok);
+        if (!ok) break;
         tc_fence_after();
-        // epilogue: lanes 32w..32w+31 are points p0 + 32w + lane
-        const int p = p0 + warp * 32 + (tid & 31);
-        for (int col = 0; col < Nt; col += 16) {
-            float v[16];
-            ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)col, v);
+        for (int col = 16 * cg; col < Nt; col += 64) {
+            const int gn0 = 256 * t + col;
+            double2 o[8];
             if (p < a.P) {
 #pragma unroll
-                for (int q = 0; q < 16; q += 2) {
-                    const int gn = 256 * t + col + q;
-                    if (gn < 2 * a.nl) {
-                        const int l = gn >> 1;
-                        double2 *dst = a.acc + ((size_t)c * a.nl + l) * a.P + p;
-                        double2 o = *dst;
-                        o.x += (double)v[q];
-                        o.y += (double)v[q + 1];
-                        *dst = o;
+                for (int q = 0; q < 8; ++q)
+                    if (gn0 + 2 * q < 2 * a.nl)
+                        o[q] = __ldcs(a.acc + ((size_t)c * a.nl + ((gn0 >> 1) + q)) * a.P + p);
+            }
+            float v[16];
+            ld16(tmem + tlane + (uint32_t)col, v);
+            if (p < a.P) {
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    if (gn0 + 2 * q < 2 * a.nl) {
+                        o[q].x += (double)v[2 * q];
+                        o[q].y += (double)v[2 * q + 1];
+                        __stcs(a.acc + ((size_t)c * a.nl + ((gn0 >> 1) + q)) * a.P + p, o[q]);
                     }
-                }
             }
         }
         tc_fence_before();
@@ -276,7 +289,7 @@ void launch_accumulate_tc(const DftTcArgs &a, cudaStream_t s) {
         attr = true;
     }
     dim3 g((a.P + 127) / 128, 6);
-    dft_accumulate_tc<<<g, 128, kDftTcSmem, s>>>(a);
+    dft_accumulate_tc<<<g, kDftTcThreads, kDftTcSmem, s>>>(a);
 }
 
 }  // namespace aefdtd

@@ -10,14 +10,13 @@
 
 namespace aefdtd {
 
-// yee_f64.cu (compiled with --fmad=false) and yee_f32.cu: the interior and
-// boundary half-step kernels over a device list of n work items
-// (x0, y0, k0, k1); one 32 x 4 CTA per item.
+// yee_f64.cu (compiled with --fmad=false) and yee_f32.cu: group g of an E or
+// H half-step's WorkSplit, one 32 x 4 CTA per item (nothing when empty).
 #define AEFDTD_DECL_YEE(T, Tid)                                                                          \
-    void launch_e_interior(const StepArgs<T, Tid> &a, const int4 *items, int n, cudaStream_t s);        \
-    void launch_e_boundary(const StepArgs<T, Tid> &a, const int4 *items, int n, cudaStream_t s);        \
-    void launch_h_interior(const StepArgs<T, Tid> &a, const int4 *items, int n, cudaStream_t s);        \
-    void launch_h_boundary(const StepArgs<T, Tid> &a, const int4 *items, int n, cudaStream_t s);
+    void launch_e_group(const StepArgs<T, Tid> &a, const int4 *items, const WorkSplit &w, int g,        \
+                        cudaStream_t s);                                                                  \
+    void launch_h_group(const StepArgs<T, Tid> &a, const int4 *items, const WorkSplit &w, int g,        \
+                        cudaStream_t s);
 AEFDTD_DECL_YEE(double, uint8_t)
 AEFDTD_DECL_YEE(double, uint16_t)
 AEFDTD_DECL_YEE(float, uint8_t)

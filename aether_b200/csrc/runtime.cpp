@@ -147,6 +147,12 @@ struct aefdtd_sim {
     bool fp64 = true;
     int device = 0;
     cudaStream_t stream = nullptr;
+    // side streams for the boundary groups of a half-step, forked from and
+    // joined back into `stream` by events (parallel branches in the graphs)
+    cudaStream_t side[kGroups - 1] = {};
+    cudaEvent_t ev_fork = nullptr, ev_join[kGroups - 1] = {};
+    bool concurrent_groups = true;
+    template <typename Launch> void run_groups(const WorkSplit &w, Launch &&launch);
     size_t dev_bytes = 0;
     uint64_t launches = 0;
 
@@ -185,11 +191,12 @@ struct aefdtd_sim {
     // custom mode
     std::vector<Osc> oscs;
     std::vector<PlaneSensor *> sensors;
-    // half-step work lists: (x0, y0, k0, k1) items of 32 x 4 columns x a z-chunk
+    // half-step work lists: (x0, y0, k0, k1) items of 32 x 4 columns x a
+    // z-chunk, in one device array: the E groups, then the H groups
     bool work_dirty = true;
     int kchunk = 0;
-    int n_interior = 0, n_boundary = 0;
-    DBuf items_interior, items_boundary;
+    WorkSplit wsE{}, wsH{};
+    DBuf items;
     void build_work();
     DBuf err;
     void check_err();
@@ -230,6 +237,7 @@ struct aefdtd_sim {
     void step(int n);
     void zero_state();
     int kchunk_override = 0;
+    int zunroll = 2;
 };
 
 aefdtd_sim::~aefdtd_sim() {
@@ -247,14 +255,16 @@ aefdtd_sim::~aefdtd_sim() {
     err.release(t);
     tables.release(t);
     for (auto &gx : graph_exec) if (gx) cudaGraphExecDestroy(gx);
-    items_interior.release(t);
-    items_boundary.release(t);
+    items.release(t);
     for (auto *s : sensors) {
         s->S.release(t); s->acc.release(t); s->wdev.release(t); s->WE.release(t); s->WH.release(t); s->flux.release(t);
         s->Btc.release(t);
         delete s;
     }
     for (auto &e : tev) if (e) cudaEventDestroy(e);
+    for (auto &e : ev_join) if (e) cudaEventDestroy(e);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    for (auto &x : side) if (x) cudaStreamDestroy(x);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -274,6 +284,10 @@ void aefdtd_sim::construct(const aefdtd_grid_desc *d) {
     if (device < 0 || device >= ndev) fail(AEFDTD_BAD_ARG, "device ordinal out of range");
     AE_CUDA(cudaSetDevice(device));
     AE_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    for (auto &x : side) AE_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+    AE_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    for (auto &e : ev_join) AE_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    concurrent_groups = std::getenv("AEFDTD_SERIAL_GROUPS") == nullptr;
 
     Dx = g.dx; Dy = g.dy; Dz = g.dz;
     Dt = g.dt > 0 ? g.dt : std::min(std::min(Dx, Dy), Dz) / (std::sqrt(3.0) * c_light) * 0.99 * g.time_mod;
@@ -339,6 +353,7 @@ void aefdtd_sim::construct(const aefdtd_grid_desc *d) {
     Nmat = 1;
     mats.assign(1, HostMat());
     if (const char *kc = std::getenv("AEFDTD_KCHUNK")) kchunk_override = std::max(0, atoi(kc));
+    if (const char *zu = std::getenv("AEFDTD_ZUNROLL")) zunroll = atoi(zu) >= 2 ? 2 : 1;
     AE_CUDA(cudaStreamSynchronize(stream));
 }
 
@@ -684,6 +699,31 @@ void aefdtd_sim::fill_scalars(int t, int osc_offset, StepScalars &s) const {
     }
 }
 
+// Launches the groups of one half-step. The groups update disjoint cells and
+// read only the other field family, so the boundary groups run on side
+// streams forked from the main stream, concurrently with the interior group,
+// and are joined back before the next half-step. Under stream capture this
+// records parallel graph branches.
+template <typename Launch> void aefdtd_sim::run_groups(const WorkSplit &w, Launch &&launch) {
+    int nside = 0;
+    for (int g = 1; g < kGroups; g++) nside += w.n[g] > 0;
+    if (!concurrent_groups || nside == 0) {
+        for (int g = 0; g < kGroups; g++) launch(g, stream);
+        return;
+    }
+    AE_CUDA(cudaEventRecord(ev_fork, stream));
+    int si = 0;
+    for (int g = 1; g < kGroups; g++) {
+        if (w.n[g] <= 0) continue;
+        AE_CUDA(cudaStreamWaitEvent(side[si], ev_fork, 0));
+        launch(g, side[si]);
+        AE_CUDA(cudaEventRecord(ev_join[si], side[si]));
+        si++;
+    }
+    launch(kGroupInterior, stream);
+    for (int k = 0; k < si; k++) AE_CUDA(cudaStreamWaitEvent(stream, ev_join[k], 0));
+}
+
 // Enqueues the kernels of L consecutive steps on the stream: for each step
 // the E half-step (interior + boundary items), the H half-step, and the fused
 // sensor launch; then the plane-sum reduction of the L steps and, when a DFT
@@ -703,7 +743,9 @@ void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
         ea.src_comp[s] = oscs[s].comp;
         ea.nsrc++;
     }
-    const int4 *wi = items_interior.as<int4>(), *wb = items_boundary.as<int4>();
+    const int4 *wi = items.as<int4>();
+    int groups = 0;
+    for (int g = 0; g < kGroups; g++) groups += (wsE.n[g] > 0) + (wsH.n[g] > 0);
     SensorStepArgs<T> sa{};
     sa.Nx = Nx; sa.Ny = Ny; sa.Nz = Nz; sa.NxNy = (long long)Nx * Ny;
     sa.Ex = F[0].as<T>(); sa.Ey = F[1].as<T>(); sa.Ez = F[2].as<T>();
@@ -719,12 +761,10 @@ void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
     for (int q = 0; q < L; q++) {
         if (record) AE_CUDA(cudaEventRecord(tev[4 * q + 0], stream));
         ea.q = ha.q = q;
-        launch_e_interior(ea, wi, n_interior, stream);
-        launch_e_boundary(ea, wb, n_boundary, stream);
+        run_groups(wsE, [&](int g, cudaStream_t st) { launch_e_group(ea, wi, wsE, g, st); });
         if (record) AE_CUDA(cudaEventRecord(tev[4 * q + 1], stream));
-        launch_h_interior(ha, wi, n_interior, stream);
-        launch_h_boundary(ha, wb, n_boundary, stream);
-        launches += (n_interior > 0) * 2 + (n_boundary > 0) * 2;
+        run_groups(wsH, [&](int g, cudaStream_t st) { launch_h_group(ha, wi, wsH, g, st); });
+        launches += groups;
         if (record) AE_CUDA(cudaEventRecord(tev[4 * q + 2], stream));
         // sensors: fed after H in both drivers; plane sums read E of this step
         sa.q = q;
@@ -865,28 +905,30 @@ void aefdtd_sim::build_work() {
         while (kchunk > 4 && tiles * ((Nz + kchunk - 1) / kchunk) < want) kchunk /= 2;
     }
     const int nch = (Nz + kchunk - 1) / kchunk;
-    std::vector<char> special(size_t(tiles) * nch, 0);   // 1: boundary, 2: boundary with dispersive cells
-    auto mark_range = [&](int x0, int x1, int y0, int y1, int z0, int z1) {   // half-open cell ranges
+    // feature mask per (tile, plane) (kF* of yee.cuh); oscillator boxes matter to E only
+    constexpr unsigned kPXY = 1, kPZ = 2, kDISP = 4, kMISC = 8, kOSC = 16;
+    std::vector<unsigned char> feat(size_t(tiles) * Nz, 0);
+    auto mark_range = [&](int x0, int x1, int y0, int y1, int z0, int z1, unsigned f) {   // half-open cell ranges
         if (x0 >= x1 || y0 >= y1 || z0 >= z1) return;
-        for (int c = z0 / kchunk; c <= (z1 - 1) / kchunk; c++)
+        for (int k = z0; k < z1; k++)
             for (int b = y0 / ty; b <= (y1 - 1) / ty; b++)
-                for (int a = x0 / tx; a <= (x1 - 1) / tx; a++) special[(size_t(c) * nty + b) * ntx + a] = 1;
+                for (int a = x0 / tx; a <= (x1 - 1) / tx; a++) feat[(size_t(k) * nty + b) * ntx + a] |= f;
     };
     const bool px = pml[0] || pml[1], py = pml[2] || pml[3], pz = pml[4] || pml[5];
     if (px) {
-        mark_range(0, std::max(pml[0], 1), 0, Ny, 0, Nz);
-        mark_range(Nx - std::max(pml[1], 1), Nx, 0, Ny, 0, Nz);
+        mark_range(0, std::max(pml[0], 1), 0, Ny, 0, Nz, kPXY);
+        mark_range(Nx - std::max(pml[1], 1), Nx, 0, Ny, 0, Nz, kPXY);
     }
     if (py) {
-        mark_range(0, Nx, 0, std::max(pml[2], 1), 0, Nz);
-        mark_range(0, Nx, Ny - std::max(pml[3], 1), Ny, 0, Nz);
+        mark_range(0, Nx, 0, std::max(pml[2], 1), 0, Nz, kPXY);
+        mark_range(0, Nx, Ny - std::max(pml[3], 1), Ny, 0, Nz, kPXY);
     }
     if (pz) {
-        mark_range(0, Nx, 0, Ny, 0, std::max(pml[4], 1));
-        mark_range(0, Nx, 0, Ny, Nz - std::max(pml[5], 1), Nz);
+        mark_range(0, Nx, 0, Ny, 0, std::max(pml[4], 1), kPZ);
+        mark_range(0, Nx, 0, Ny, Nz - std::max(pml[5], 1), Nz, kPZ);
     }
-    if (normal) mark_range(0, Nx, 0, Ny, zs_e - 1, zs_e);
-    for (auto &o : oscs) mark_range(o.box[0], o.box[1], o.box[2], o.box[3], o.box[4], o.box[5]);
+    if (normal) mark_range(0, Nx, 0, Ny, zs_e - 1, zs_e, kMISC);
+    for (auto &o : oscs) mark_range(o.box[0], o.box[1], o.box[2], o.box[3], o.box[4], o.box[5], kOSC);
     for (unsigned m = 0; m < Nmat; m++) {
         HostMat &h = mats[m];
         if (!(h.rc && h.np > 0)) continue;
@@ -894,33 +936,66 @@ void aefdtd_sim::build_work() {
             for (int j = h.y1; j <= h.y2; j++) {
                 const uint32_t *row = &map[size_t(j) * Nx + size_t(k) * Nx * Ny];
                 for (int i = h.x1; i <= h.x2; i++)
-                    if (row[i] == m) special[(size_t(k / kchunk) * nty + j / ty) * ntx + i / tx] = 2;
+                    if (row[i] == m) feat[(size_t(k) * nty + j / ty) * ntx + i / tx] |= kDISP;
             }
     }
-    // AEFDTD_ALL_BOUNDARY=1 routes every item through the full kernels (same results)
+    // AEFDTD_ALL_BOUNDARY=1 routes every item through the general kernels (same results)
     const bool all_boundary = std::getenv("AEFDTD_ALL_BOUNDARY") != nullptr;
-    if (all_boundary) std::fill(special.begin(), special.end(), 1);
-    std::vector<int> vi, vb;
+    // group of a (tile, plane) for the E and the H half-step
+    auto group_e = [&](unsigned f) {
+        if (all_boundary) return (int)kGroupAll;
+        f = (f & ~kOSC) | ((f & kOSC) ? kMISC : 0);
+        if (f == 0) return (int)kGroupInterior;
+        if (f == kPZ) return (int)kGroupPmlZ;
+        if (f == kDISP) return (int)kGroupDisp;
+        return (int)kGroupAll;
+    };
+    auto group_h = [&](unsigned f) {
+        if (all_boundary) return (int)kGroupAll;
+        f &= (kPXY | kPZ | kMISC);
+        if (f == 0) return (int)kGroupInterior;
+        if (f == kPZ) return (int)kGroupPmlZ;
+        return (int)kGroupAll;
+    };
+    // items: within each tile and z-chunk, runs of planes of one group;
+    // dispersive E planes one plane per item (their cells carry the pole state)
+    std::vector<int> v[2][kGroups];
     for (int c = 0; c < nch; c++)
         for (int b = 0; b < nty; b++)
             for (int a = 0; a < ntx; a++) {
-                const char sp = special[(size_t(c) * nty + b) * ntx + a];
-                std::vector<int> &v = sp ? vb : vi;
                 const int z0 = c * kchunk, z1 = std::min(Nz, (c + 1) * kchunk);
-                const int step = (sp == 2) ? 1 : kchunk;   // dispersive items: one plane each
-                for (int z = z0; z < z1; z += step) {
-                    v.push_back(a * tx);
-                    v.push_back(b * ty);
-                    v.push_back(z);
-                    v.push_back(std::min(z1, z + step));
+                for (int half = 0; half < 2; half++) {
+                    int z = z0;
+                    while (z < z1) {
+                        auto grp = [&](int k) {
+                            const unsigned f = feat[(size_t(k) * nty + b) * ntx + a];
+                            return half == 0 ? group_e(f) : group_h(f);
+                        };
+                        const int g = grp(z);
+                        int ze = z + 1;
+                        if (!(half == 0 && g == kGroupDisp))
+                            while (ze < z1 && grp(ze) == g) ze++;
+                        std::vector<int> &dst = v[half][g];
+                        dst.push_back(a * tx);
+                        dst.push_back(b * ty);
+                        dst.push_back(z);
+                        dst.push_back(ze);
+                        z = ze;
+                    }
                 }
             }
-    n_interior = (int)(vi.size() / 4);
-    n_boundary = (int)(vb.size() / 4);
-    items_interior.alloc(std::max<size_t>(vi.size(), 4) * sizeof(int), dev_bytes);
-    items_boundary.alloc(std::max<size_t>(vb.size(), 4) * sizeof(int), dev_bytes);
-    if (!vi.empty()) AE_CUDA(cudaMemcpy(items_interior.p, vi.data(), vi.size() * sizeof(int), cudaMemcpyHostToDevice));
-    if (!vb.empty()) AE_CUDA(cudaMemcpy(items_boundary.p, vb.data(), vb.size() * sizeof(int), cudaMemcpyHostToDevice));
+    std::vector<int> all;
+    for (int half = 0; half < 2; half++) {
+        WorkSplit &w = half == 0 ? wsE : wsH;
+        w.unroll = zunroll;
+        for (int g = 0; g < kGroups; g++) {
+            w.off[g] = (int)(all.size() / 4);
+            w.n[g] = (int)(v[half][g].size() / 4);
+            all.insert(all.end(), v[half][g].begin(), v[half][g].end());
+        }
+    }
+    items.alloc(std::max<size_t>(all.size(), 4) * sizeof(int), dev_bytes);
+    if (!all.empty()) AE_CUDA(cudaMemcpy(items.p, all.data(), all.size() * sizeof(int), cudaMemcpyHostToDevice));
     work_dirty = false;
 }
 

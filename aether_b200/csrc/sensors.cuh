@@ -43,15 +43,34 @@ __device__ __forceinline__ void plane_partial(const SensorStepArgs<T> &a, int b)
     const double Dx2 = a.Dx / 2.0, Dy2 = a.Dy / 2.0, Dz2 = a.Dz / 2.0;
     const double zr = a.kr * a.Dz, zt = a.kt * a.Dz;
     const double tb = a.sc[a.q].tb, tap = a.sc[a.q].taper;
+    // With kx = ky = 0 (normal incidence) the phase kx x + ky y + kz z is
+    // exactly kz z, so the six pulse values are the same at every cell of the
+    // planes: evaluate them once per block.
+    const bool uniform = a.P.kx == 0.0 && a.P.ky == 0.0;
+    __shared__ double pv[6];
+    if (uniform) {
+        const int t = threadIdx.x;
+        if (t < 6) {
+            const double A0 = (t % 3 == 0) ? a.P.Ex0 : (t % 3 == 1) ? a.P.Ey0 : a.P.Ez0;
+            const double z = (t < 3 ? zr : zt) + (t % 3 == 2 ? Dz2 : 0.0);
+            pv[t] = pulse_eval(a.P, A0, (t % 3 == 0) ? Dx2 : 0.0, (t % 3 == 1) ? Dy2 : 0.0, z, tb);
+        }
+        __syncthreads();
+    }
     for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
         const int i = q % a.Nx, j = q / a.Nx;
         const double x = i * a.Dx, y = j * a.Dy;
-        const double bx = pulse_eval(a.P, a.P.Ex0, x + Dx2, y, zr, tb);
-        const double by = pulse_eval(a.P, a.P.Ey0, x, y + Dy2, zr, tb);
-        const double bz = pulse_eval(a.P, a.P.Ez0, x, y, zr + Dz2, tb);
-        const double tx = pulse_eval(a.P, a.P.Ex0, x + Dx2, y, zt, tb);
-        const double ty = pulse_eval(a.P, a.P.Ey0, x, y + Dy2, zt, tb);
-        const double tz = pulse_eval(a.P, a.P.Ez0, x, y, zt + Dz2, tb);
+        double bx, by, bz, tx, ty, tz;
+        if (uniform) {
+            bx = pv[0]; by = pv[1]; bz = pv[2]; tx = pv[3]; ty = pv[4]; tz = pv[5];
+        } else {
+            bx = pulse_eval(a.P, a.P.Ex0, x + Dx2, y, zr, tb);
+            by = pulse_eval(a.P, a.P.Ey0, x, y + Dy2, zr, tb);
+            bz = pulse_eval(a.P, a.P.Ez0, x, y, zr + Dz2, tb);
+            tx = pulse_eval(a.P, a.P.Ex0, x + Dx2, y, zt, tb);
+            ty = pulse_eval(a.P, a.P.Ey0, x, y + Dy2, zt, tb);
+            tz = pulse_eval(a.P, a.P.Ez0, x, y, zt + Dz2, tb);
+        }
         const long long ir = q + a.kr * a.NxNy, it = q + a.kt * a.NxNy;
         acc[0] += bx * tap;
         acc[1] += by * tap;

@@ -17,12 +17,16 @@
 // (i, j) columns times a z-chunk. A CTA of 32 x 4 threads takes one item;
 // each thread owns one column and marches the chunk along z, carrying the z-1
 // (E) or z+1 (H) plane in registers, with x and y neighbours through L1. The
-// host sorts the items into two lists (runtime.cpp, build_work): "interior"
-// items, in which no cell is in a CPML range or PEC plane, dispersive, on the
-// injection plane or inside a source box, run a lean kernel that does only the
-// curl update (few registers, full occupancy); the other items run the full
-// kernel. Both lists are launched for every half-step and cover each cell
-// exactly once.
+// host (runtime.cpp, build_work) tags every item with the features its cells
+// need -- CPML or PEC on x/y, CPML or PEC on z, dispersive poles, plane
+// injection or source boxes -- and sorts the items of each half-step into
+// groups, each run by a kernel compiled for exactly those features:
+//   * interior items (no feature): the curl update only, U z-planes per
+//     iteration with all loads of the U planes issued before any store, so
+//     each thread keeps U planes of reads in flight;
+//   * z-CPML items, dispersive items, and the rest (every phase): the
+//     boundary kernel instantiated for feature sets kFPmlZ, kFDisp and kFAll.
+// All groups of a half-step together cover each cell exactly once.
 //
 // FP64 instantiation (compiled with --fmad=false): operation order equals the
 // reference's expression order, so results are bit-identical to the CPU
@@ -48,10 +52,18 @@ template <typename T> __device__ __forceinline__ T cpml_rec(T b, T psi, T c, T d
     else return psi + (b * psi + c * diff);
 }
 
+// Boundary-item features (bit mask per item; a kernel compiled for set F may
+// run any item whose mask is a subset of F).
+constexpr unsigned kFPmlXY = 1;   // a cell in an x or y CPML range or PEC plane
+constexpr unsigned kFPmlZ = 2;    // a cell in a z CPML range or PEC plane
+constexpr unsigned kFDisp = 4;    // a cell of a dispersive (recursive-convolution) material
+constexpr unsigned kFMisc = 8;    // the injection plane or an oscillator box
+constexpr unsigned kFAll = 15;
+
 // ---- interior items: curl update only -----------------------------------
-template <typename T, typename Tid>
-__global__ void __launch_bounds__(kTileX * kTileY, 12) e_interior(const __grid_constant__ StepArgs<T, Tid> a,
-                                                                  const int4 *__restrict__ items) {
+template <typename T, typename Tid, int U>
+__global__ void __launch_bounds__(kTileX * kTileY, (U == 1 && sizeof(T) == 4) ? 12 : 8)
+e_interior(const __grid_constant__ StepArgs<T, Tid> a, const int4 *__restrict__ items) {
     // coefficients through the read-only path: short-lived CTAs skip a table fill and barrier
     const int4 it = items[blockIdx.x];
     const int i = it.x + threadIdx.x, j = it.y + threadIdx.y;
@@ -70,31 +82,48 @@ __global__ void __launch_bounds__(kTileX * kTileY, 12) e_interior(const __grid_c
     T *__restrict__ Ex = a.Ex;
     T *__restrict__ Ey = a.Ey;
     T *__restrict__ Ez = a.Ez;
-    const T ikx = a.ikx[i], iky = a.iky[j];
+    const Tid *__restrict__ mat = a.mat;
+    const MatCoef<T> *__restrict__ coef = a.coef;
+    const T ikx = __ldg(a.ikx + i), iky = __ldg(a.iky + j);
     const int kmi = (it.z == 0) ? a.Nz - 1 : it.z - 1;
     T hx_km = __ldg(Hx + col + kmi * NxNy);
     T hy_km = __ldg(Hy + col + kmi * NxNy);
-    for (int k = it.z; k < it.w; ++k) {
-        const long long id = col + k * NxNy;
-        const T hx = __ldg(Hx + id), hy = __ldg(Hy + id), hz = __ldg(Hz + id);
-        const T hz_jm = __ldg(Hz + coly + k * NxNy), hx_jm = __ldg(Hx + coly + k * NxNy);
-        const T hz_im = __ldg(Hz + colx + k * NxNy), hy_im = __ldg(Hy + colx + k * NxNy);
-        const T ex = Ex[id], ey = Ey[id], ez = Ez[id];
-        const int m = __ldg(a.mat + colm + k * mNxNy);
-        const MatCoef<T> *cp = a.coef + m;
-        const MatCoef<T> c{__ldg(&cp->C1), __ldg(&cp->C2x), __ldg(&cp->C2y), __ldg(&cp->C2z), T(0), T(0)};
-        const T ikz = a.ikz[k];
-        Ex[id] = (c.C1 * ex + (c.C2y * iky) * (hz - hz_jm)) - (c.C2z * ikz) * (hy - hy_km);
-        Ey[id] = (c.C1 * ey + (c.C2z * ikz) * (hx - hx_km)) - (c.C2x * ikx) * (hz - hz_im);
-        Ez[id] = (c.C1 * ez + (c.C2x * ikx) * (hy - hy_im)) - (c.C2y * iky) * (hx - hx_jm);
-        hx_km = hx;
-        hy_km = hy;
+    for (int k = it.z; k < it.w; k += U) {
+        T hx[U], hy[U], hz[U], hz_jm[U], hx_jm[U], hz_im[U], hy_im[U], ex[U], ey[U], ez[U];
+        int m[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            // planes past the chunk end re-read its last plane (not stored)
+            const long long o = (long long)min(k + u, it.w - 1) * NxNy;
+            hx[u] = __ldg(Hx + col + o); hy[u] = __ldg(Hy + col + o); hz[u] = __ldg(Hz + col + o);
+            hz_jm[u] = __ldg(Hz + coly + o); hx_jm[u] = __ldg(Hx + coly + o);
+            hz_im[u] = __ldg(Hz + colx + o); hy_im[u] = __ldg(Hy + colx + o);
+            ex[u] = Ex[col + o]; ey[u] = Ey[col + o]; ez[u] = Ez[col + o];
+            m[u] = __ldg(mat + colm + (long long)min(k + u, it.w - 1) * mNxNy);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const MatCoef<T> *cp = coef + m[u];
+            const T C1 = __ldg(&cp->C1), C2x = __ldg(&cp->C2x), C2y = __ldg(&cp->C2y), C2z = __ldg(&cp->C2z);
+            const int kk = min(k + u, it.w - 1);
+            const T ikz = __ldg(a.ikz + kk);
+            const T hxm = u ? hx[u - 1] : hx_km, hym = u ? hy[u - 1] : hy_km;
+            const T nex = (C1 * ex[u] + (C2y * iky) * (hz[u] - hz_jm[u])) - (C2z * ikz) * (hy[u] - hym);
+            const T ney = (C1 * ey[u] + (C2z * ikz) * (hx[u] - hxm)) - (C2x * ikx) * (hz[u] - hz_im[u]);
+            const T nez = (C1 * ez[u] + (C2x * ikx) * (hy[u] - hy_im[u])) - (C2y * iky) * (hx[u] - hx_jm[u]);
+            if (k + u < it.w) {
+                const long long id = col + (long long)kk * NxNy;
+                Ex[id] = nex; Ey[id] = ney; Ez[id] = nez;
+            }
+        }
+        hx_km = hx[U - 1];
+        hy_km = hy[U - 1];
     }
 }
 
-template <typename T, typename Tid>
-__global__ void __launch_bounds__(kTileX * kTileY, 12) h_interior(const __grid_constant__ StepArgs<T, Tid> a,
-                                                                  const int4 *__restrict__ items) {
+template <typename T, typename Tid, int U>
+__global__ void __launch_bounds__(kTileX * kTileY, (U == 1 && sizeof(T) == 4) ? 12 : 8)
+h_interior(const __grid_constant__ StepArgs<T, Tid> a, const int4 *__restrict__ items) {
     const int4 it = items[blockIdx.x];
     const int i = it.x + threadIdx.x, j = it.y + threadIdx.y;
     if (i >= a.Nx || j >= a.Ny) return;
@@ -110,29 +139,43 @@ __global__ void __launch_bounds__(kTileX * kTileY, 12) h_interior(const __grid_c
     T *__restrict__ Hx = a.Hx;
     T *__restrict__ Hy = a.Hy;
     T *__restrict__ Hz = a.Hz;
-    const T ax = a.dtdmx * a.ikx[i];
-    const T ay = a.dtdmy * a.iky[j];
+    const T ax = a.dtdmx * __ldg(a.ikx + i);
+    const T ay = a.dtdmy * __ldg(a.iky + j);
     T ex = __ldg(Ex + col + it.z * NxNy);
     T ey = __ldg(Ey + col + it.z * NxNy);
-    for (int k = it.z; k < it.w; ++k) {
-        const long long id = col + k * NxNy;
-        const int kp = (k == a.Nz - 1) ? 0 : k + 1;
-        const T ex_kp = __ldg(Ex + col + kp * NxNy), ey_kp = __ldg(Ey + col + kp * NxNy);
-        const T ez = __ldg(Ez + id);
-        const T ez_jp = __ldg(Ez + coly + k * NxNy), ex_jp = __ldg(Ex + coly + k * NxNy);
-        const T ez_ip = __ldg(Ez + colx + k * NxNy), ey_ip = __ldg(Ey + colx + k * NxNy);
-        const T hx = Hx[id], hy = Hy[id], hz = Hz[id];
-        const T az = a.dtdmz * a.ikz[k];
-        Hx[id] = hx + (az * (ey_kp - ey) - ay * (ez_jp - ez));
-        Hy[id] = hy + (ax * (ez_ip - ez) - az * (ex_kp - ex));
-        Hz[id] = hz + (ay * (ex_jp - ex) - ax * (ey_ip - ey));
-        ex = ex_kp;
-        ey = ey_kp;
+    for (int k = it.z; k < it.w; k += U) {
+        T ex_kp[U], ey_kp[U], ez[U], ez_jp[U], ex_jp[U], ez_ip[U], ey_ip[U], hx[U], hy[U], hz[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int kk = min(k + u, it.w - 1);
+            const int kp = (kk == a.Nz - 1) ? 0 : kk + 1;
+            const long long o = (long long)kk * NxNy, op = (long long)kp * NxNy;
+            ex_kp[u] = __ldg(Ex + col + op); ey_kp[u] = __ldg(Ey + col + op);
+            ez[u] = __ldg(Ez + col + o);
+            ez_jp[u] = __ldg(Ez + coly + o); ex_jp[u] = __ldg(Ex + coly + o);
+            ez_ip[u] = __ldg(Ez + colx + o); ey_ip[u] = __ldg(Ey + colx + o);
+            hx[u] = Hx[col + o]; hy[u] = Hy[col + o]; hz[u] = Hz[col + o];
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int kk = min(k + u, it.w - 1);
+            const T az = a.dtdmz * __ldg(a.ikz + kk);
+            const T exk = u ? ex_kp[u - 1] : ex, eyk = u ? ey_kp[u - 1] : ey;
+            const T nhx = hx[u] + (az * (ey_kp[u] - eyk) - ay * (ez_jp[u] - ez[u]));
+            const T nhy = hy[u] + (ax * (ez_ip[u] - ez[u]) - az * (ex_kp[u] - exk));
+            const T nhz = hz[u] + (ay * (ex_jp[u] - exk) - ax * (ey_ip[u] - eyk));
+            if (k + u < it.w) {
+                const long long id = col + (long long)kk * NxNy;
+                Hx[id] = nhx; Hy[id] = nhy; Hz[id] = nhz;
+            }
+        }
+        ex = ex_kp[U - 1];
+        ey = ey_kp[U - 1];
     }
 }
 
-// ---- boundary items: every phase ------------------------------------------
-template <typename T, typename Tid>
+// ---- boundary items: the phases of feature set F ---------------------------
+template <typename T, typename Tid, unsigned F>
 __global__ void __launch_bounds__(kTileX * kTileY) e_boundary(const __grid_constant__ StepArgs<T, Tid> a,
                                                               const int4 *__restrict__ items) {
     const int4 it = items[blockIdx.x];
@@ -147,62 +190,75 @@ __global__ void __launch_bounds__(kTileX * kTileY) e_boundary(const __grid_const
     const long long coly = i + (long long)jm * a.Nx;
     const long long colm = i + (long long)j * a.mpitch;
     const long long mNxNy = (long long)a.mpitch * a.Ny;
-    const T ikx = a.ikx[i];
-    const T iky = a.iky[j];
+    const T *__restrict__ Hx = a.Hx;
+    const T *__restrict__ Hy = a.Hy;
+    const T *__restrict__ Hz = a.Hz;
+    T *__restrict__ Ex = a.Ex;
+    T *__restrict__ Ey = a.Ey;
+    T *__restrict__ Ez = a.Ez;
+    const T ikx = __ldg(a.ikx + i);
+    const T iky = __ldg(a.iky + j);
 
     // E-side CPML index ranges: [1, pml_m) and [N - pml_p + 1, N) (fdtd_pml.cpp:518,527,547,559)
-    const bool xe = a.px && ((i >= 1 && i < a.pml_xm) || (i >= a.Nx - a.pml_xp + 1));
-    const bool ye = a.py && ((j >= 1 && j < a.pml_ym) || (j >= a.Ny - a.pml_yp + 1));
+    bool xe = false, ye = false;
+    int xn = 0, yn = 0;
     const int nxs = a.pml_xm + a.pml_xp, nys = a.pml_ym + a.pml_yp;
-    const int xn = (i < a.pml_xm) ? i : i - (a.Nx - a.pml_xp) + a.pml_xm;
-    const int yn = (j < a.pml_ym) ? j : j - (a.Ny - a.pml_yp) + a.pml_ym;
     T bxi = 0, cxi = 0, byj = 0, cyj = 0;
-    if (xe) { bxi = a.bx[i]; cxi = a.cx[i]; }
-    if (ye) { byj = a.by[j]; cyj = a.cy[j]; }
+    if constexpr ((F & kFPmlXY) != 0) {
+        xe = a.px && ((i >= 1 && i < a.pml_xm) || (i >= a.Nx - a.pml_xp + 1));
+        ye = a.py && ((j >= 1 && j < a.pml_ym) || (j >= a.Ny - a.pml_yp + 1));
+        xn = (i < a.pml_xm) ? i : i - (a.Nx - a.pml_xp) + a.pml_xm;
+        yn = (j < a.pml_ym) ? j : j - (a.Ny - a.pml_yp) + a.pml_ym;
+        if (xe) { bxi = __ldg(a.bx + i); cxi = __ldg(a.cx + i); }
+        if (ye) { byj = __ldg(a.by + j); cyj = __ldg(a.cy + j); }
+    }
 
     const int kmi = (k0 == 0) ? a.Nz - 1 : k0 - 1;
-    T hx_km = a.Hx[col + kmi * NxNy];
-    T hy_km = a.Hy[col + kmi * NxNy];
+    T hx_km = __ldg(Hx + col + kmi * NxNy);
+    T hy_km = __ldg(Hy + col + kmi * NxNy);
 
     for (int k = k0; k < k1; ++k) {
         const long long id = col + k * NxNy;
-        const T hx = a.Hx[id], hy = a.Hy[id], hz = a.Hz[id];
-        const T hz_jm = a.Hz[coly + k * NxNy], hx_jm = a.Hx[coly + k * NxNy];
-        const T hz_im = a.Hz[colx + k * NxNy], hy_im = a.Hy[colx + k * NxNy];
-        const T ex = a.Ex[id], ey = a.Ey[id], ez = a.Ez[id];
+        const T hx = __ldg(Hx + id), hy = __ldg(Hy + id), hz = __ldg(Hz + id);
+        const T hz_jm = __ldg(Hz + coly + k * NxNy), hx_jm = __ldg(Hx + coly + k * NxNy);
+        const T hz_im = __ldg(Hz + colx + k * NxNy), hy_im = __ldg(Hy + colx + k * NxNy);
+        const T ex = Ex[id], ey = Ey[id], ez = Ez[id];
         const int m = __ldg(a.mat + colm + k * mNxNy);
         const MatCoef<T> c = a.coef[m];
-        const int np_m = a.disp ? __ldg(&a.disp[m].np) : 0;
-        const T ikz = a.ikz[k];
+        const T ikz = __ldg(a.ikz + k);
 
         // Recursive-convolution "ante" with E^n; sums of Re(psi) per component.
         T s0 = 0, s1 = 0, s2 = 0;
-        if (np_m > 0) {
-            const DispInfo d = a.disp[m];
-            const long long q = (i - d.x1) + (long long)(j - d.y1) * d.xs + (long long)(k - d.z1) * d.xs * d.ys;
-            Cplx<T> *P = a.psi + d.psi_off + q;
-            for (int p = 0; p < d.np; ++p) {
-                const Cplx<T> cr = a.crec[d.pole_off + p];
-                const Cplx<T> dc = a.dchi[d.pole_off + p];
-                const T ev[3] = {ex, ey, ez};
+        int np_m = 0;
+        if constexpr ((F & kFDisp) != 0) {
+            np_m = a.disp ? __ldg(&a.disp[m].np) : 0;
+            if (np_m > 0) {
+                const DispInfo d = a.disp[m];
+                const long long q = (i - d.x1) + (long long)(j - d.y1) * d.xs + (long long)(k - d.z1) * d.xs * d.ys;
+                Cplx<T> *__restrict__ P = a.psi + d.psi_off + q;
+                for (int p = 0; p < d.np; ++p) {
+                    const Cplx<T> cr = a.crec[d.pole_off + p];
+                    const Cplx<T> dc = a.dchi[d.pole_off + p];
+                    const T ev[3] = {ex, ey, ez};
 #pragma unroll
-                for (int dd = 0; dd < 3; ++dd) {
-                    Cplx<T> *pp = P + (long long)(3 * p + dd) * d.box;
-                    const Cplx<T> v = *pp;
-                    Cplx<T> r;
-                    if constexpr (Exact<T>::value) {
-                        // Crec*psi + Dchi*E with std::complex<double> rounding order
-                        r.re = (cr.re * v.re - cr.im * v.im) + dc.re * ev[dd];
-                        r.im = (cr.re * v.im + cr.im * v.re) + dc.im * ev[dd];
-                    } else {
-                        // (Crec-1) stored: psi + ((Crec-1)*psi + Dchi*E)
-                        r.re = v.re + ((cr.re * v.re - cr.im * v.im) + dc.re * ev[dd]);
-                        r.im = v.im + ((cr.re * v.im + cr.im * v.re) + dc.im * ev[dd]);
+                    for (int dd = 0; dd < 3; ++dd) {
+                        Cplx<T> *pp = P + (long long)(3 * p + dd) * d.box;
+                        const Cplx<T> v = *pp;
+                        Cplx<T> r;
+                        if constexpr (Exact<T>::value) {
+                            // Crec*psi + Dchi*E with std::complex<double> rounding order
+                            r.re = (cr.re * v.re - cr.im * v.im) + dc.re * ev[dd];
+                            r.im = (cr.re * v.im + cr.im * v.re) + dc.im * ev[dd];
+                        } else {
+                            // (Crec-1) stored: psi + ((Crec-1)*psi + Dchi*E)
+                            r.re = v.re + ((cr.re * v.re - cr.im * v.im) + dc.re * ev[dd]);
+                            r.im = v.im + ((cr.re * v.im + cr.im * v.re) + dc.im * ev[dd]);
+                        }
+                        *pp = r;
+                        if (dd == 0) s0 = s0 + r.re;
+                        else if (dd == 1) s1 = s1 + r.re;
+                        else s2 = s2 + r.re;
                     }
-                    *pp = r;
-                    if (dd == 0) s0 = s0 + r.re;
-                    else if (dd == 1) s1 = s1 + r.re;
-                    else s2 = s2 + r.re;
                 }
             }
         }
@@ -213,88 +269,106 @@ __global__ void __launch_bounds__(kTileX * kTileY) e_boundary(const __grid_const
         T nex = (c.C1 * ex + (c.C2y * iky) * dHz_y) - (c.C2z * ikz) * dHy_z;
         T ney = (c.C1 * ey + (c.C2z * ikz) * dHx_z) - (c.C2x * ikx) * dHz_x;
         T nez = (c.C1 * ez + (c.C2x * ikx) * dHy_x) - (c.C2y * iky) * dHx_y;
-        if (np_m > 0) {
-            nex += c.C3 * s0;
-            ney += c.C3 * s1;
-            nez += c.C3 * s2;
-        }
-
-        // CPML and PEC planes in app_pml_Ex / Ey / Ez order.
-        const bool ze = a.pz && ((k >= 1 && k < a.pml_zm) || (k >= a.Nz - a.pml_zp + 1));
-        const int zn = (k < a.pml_zm) ? k : k - (a.Nz - a.pml_zp) + a.pml_zm;
-        T bzk = 0, czk = 0;
-        if (ze) { bzk = a.bz[k]; czk = a.cz[k]; }
-        // Ex: y block, then z block
-        if (ye) {
-            T *pp = a.psi_y0 + i + (long long)yn * a.Nx + (long long)k * a.Nx * nys;
-            const T ps = cpml_rec(byj, *pp, cyj, dHz_y);
-            *pp = ps;
-            nex += c.C4 * ps;
-        }
-        if (a.py && j == 0) nex = 0;
-        if (ze) {
-            T *pp = a.psi_z0 + col + (long long)zn * NxNy;
-            const T ps = cpml_rec(bzk, *pp, czk, dHy_z);
-            *pp = ps;
-            nex -= c.C4 * ps;
-        }
-        if (a.pz && k == 0) nex = 0;
-        // Ey: x block, then z block
-        if (xe) {
-            T *pp = a.psi_x0 + xn + (long long)j * nxs + (long long)k * nxs * a.Ny;
-            const T ps = cpml_rec(bxi, *pp, cxi, dHz_x);
-            *pp = ps;
-            ney -= c.C4 * ps;
-        }
-        if (a.px && i == 0) ney = 0;
-        if (ze) {
-            T *pp = a.psi_z1 + col + (long long)zn * NxNy;
-            const T ps = cpml_rec(bzk, *pp, czk, dHx_z);
-            *pp = ps;
-            ney += c.C4 * ps;
-        }
-        if (a.pz && k == 0) ney = 0;
-        // Ez: x block, then y block
-        if (xe) {
-            T *pp = a.psi_x1 + xn + (long long)j * nxs + (long long)k * nxs * a.Ny;
-            const T ps = cpml_rec(bxi, *pp, cxi, dHy_x);
-            *pp = ps;
-            nez += c.C4 * ps;
-        }
-        if (a.px && i == 0) nez = 0;
-        if (ye) {
-            T *pp = a.psi_y1 + i + (long long)yn * a.Nx + (long long)k * a.Nx * nys;
-            const T ps = cpml_rec(byj, *pp, cyj, dHx_y);
-            *pp = ps;
-            nez -= c.C4 * ps;
-        }
-        if (a.py && j == 0) nez = 0;
-
-        // Normal-incidence plane injection after update_E (normal_incidence.cpp:338-342)
-        if (k == a.kinj) {
-            nex = nex - (T)a.sc[a.q].inj_eA;
-            ney = ney + (T)a.sc[a.q].inj_eB;
-        }
-        // Oscillator boxes after update_E (sc_oscillator.cpp:43-63)
-        for (int s = 0; s < a.nsrc; ++s) {
-            const int *b = a.src_box[s];
-            if (i >= b[0] && i < b[1] && j >= b[2] && j < b[3] && k >= b[4] && k < b[5]) {
-                const T v = (T)a.sc[a.q].src[s];
-                if (a.src_comp[s] == 0) nex += v;
-                else if (a.src_comp[s] == 1) ney += v;
-                else nez += v;
+        if constexpr ((F & kFDisp) != 0) {
+            if (np_m > 0) {
+                nex += c.C3 * s0;
+                ney += c.C3 * s1;
+                nez += c.C3 * s2;
             }
         }
 
-        a.Ex[id] = nex;
-        a.Ey[id] = ney;
-        a.Ez[id] = nez;
+        // CPML and PEC planes in app_pml_Ex / Ey / Ez order.
+        bool ze = false;
+        int zn = 0;
+        T bzk = 0, czk = 0;
+        if constexpr ((F & kFPmlZ) != 0) {
+            ze = a.pz && ((k >= 1 && k < a.pml_zm) || (k >= a.Nz - a.pml_zp + 1));
+            zn = (k < a.pml_zm) ? k : k - (a.Nz - a.pml_zp) + a.pml_zm;
+            if (ze) { bzk = __ldg(a.bz + k); czk = __ldg(a.cz + k); }
+        }
+        // Ex: y block, then z block
+        if constexpr ((F & kFPmlXY) != 0) {
+            if (ye) {
+                T *pp = a.psi_y0 + i + (long long)yn * a.Nx + (long long)k * a.Nx * nys;
+                const T ps = cpml_rec(byj, *pp, cyj, dHz_y);
+                *pp = ps;
+                nex += c.C4 * ps;
+            }
+            if (a.py && j == 0) nex = 0;
+        }
+        if constexpr ((F & kFPmlZ) != 0) {
+            if (ze) {
+                T *pp = a.psi_z0 + col + (long long)zn * NxNy;
+                const T ps = cpml_rec(bzk, *pp, czk, dHy_z);
+                *pp = ps;
+                nex -= c.C4 * ps;
+            }
+            if (a.pz && k == 0) nex = 0;
+        }
+        // Ey: x block, then z block
+        if constexpr ((F & kFPmlXY) != 0) {
+            if (xe) {
+                T *pp = a.psi_x0 + xn + (long long)j * nxs + (long long)k * nxs * a.Ny;
+                const T ps = cpml_rec(bxi, *pp, cxi, dHz_x);
+                *pp = ps;
+                ney -= c.C4 * ps;
+            }
+            if (a.px && i == 0) ney = 0;
+        }
+        if constexpr ((F & kFPmlZ) != 0) {
+            if (ze) {
+                T *pp = a.psi_z1 + col + (long long)zn * NxNy;
+                const T ps = cpml_rec(bzk, *pp, czk, dHx_z);
+                *pp = ps;
+                ney += c.C4 * ps;
+            }
+            if (a.pz && k == 0) ney = 0;
+        }
+        // Ez: x block, then y block
+        if constexpr ((F & kFPmlXY) != 0) {
+            if (xe) {
+                T *pp = a.psi_x1 + xn + (long long)j * nxs + (long long)k * nxs * a.Ny;
+                const T ps = cpml_rec(bxi, *pp, cxi, dHy_x);
+                *pp = ps;
+                nez += c.C4 * ps;
+            }
+            if (a.px && i == 0) nez = 0;
+            if (ye) {
+                T *pp = a.psi_y1 + i + (long long)yn * a.Nx + (long long)k * a.Nx * nys;
+                const T ps = cpml_rec(byj, *pp, cyj, dHx_y);
+                *pp = ps;
+                nez -= c.C4 * ps;
+            }
+            if (a.py && j == 0) nez = 0;
+        }
+
+        if constexpr ((F & kFMisc) != 0) {
+            // Normal-incidence plane injection after update_E (normal_incidence.cpp:338-342)
+            if (k == a.kinj) {
+                nex = nex - (T)a.sc[a.q].inj_eA;
+                ney = ney + (T)a.sc[a.q].inj_eB;
+            }
+            // Oscillator boxes after update_E (sc_oscillator.cpp:43-63)
+            for (int s = 0; s < a.nsrc; ++s) {
+                const int *b = a.src_box[s];
+                if (i >= b[0] && i < b[1] && j >= b[2] && j < b[3] && k >= b[4] && k < b[5]) {
+                    const T v = (T)a.sc[a.q].src[s];
+                    if (a.src_comp[s] == 0) nex += v;
+                    else if (a.src_comp[s] == 1) ney += v;
+                    else nez += v;
+                }
+            }
+        }
+
+        Ex[id] = nex;
+        Ey[id] = ney;
+        Ez[id] = nez;
         hx_km = hx;
         hy_km = hy;
     }
 }
 
-template <typename T, typename Tid>
+template <typename T, typename Tid, unsigned F>
 __global__ void __launch_bounds__(kTileX * kTileY) h_boundary(const __grid_constant__ StepArgs<T, Tid> a,
                                                               const int4 *__restrict__ items) {
     const int4 it = items[blockIdx.x];
@@ -307,31 +381,41 @@ __global__ void __launch_bounds__(kTileX * kTileY) h_boundary(const __grid_const
     const long long col = i + (long long)j * a.Nx;
     const long long colx = ip + (long long)j * a.Nx;
     const long long coly = i + (long long)jp * a.Nx;
-    const T ax = a.dtdmx * a.ikx[i];
-    const T ay = a.dtdmy * a.iky[j];
+    const T *__restrict__ Ex = a.Ex;
+    const T *__restrict__ Ey = a.Ey;
+    const T *__restrict__ Ez = a.Ez;
+    T *__restrict__ Hx = a.Hx;
+    T *__restrict__ Hy = a.Hy;
+    T *__restrict__ Hz = a.Hz;
+    const T ax = a.dtdmx * __ldg(a.ikx + i);
+    const T ay = a.dtdmy * __ldg(a.iky + j);
 
     // H-side CPML index ranges: [0, pml_m) and [N - pml_p, N - 1) (fdtd_pml.cpp:750,756,775,784)
-    const bool xh = a.px && ((i < a.pml_xm) || (i >= a.Nx - a.pml_xp && i < a.Nx - 1));
-    const bool yh = a.py && ((j < a.pml_ym) || (j >= a.Ny - a.pml_yp && j < a.Ny - 1));
+    bool xh = false, yh = false;
+    int xn = 0, yn = 0;
     const int nxs = a.pml_xm + a.pml_xp, nys = a.pml_ym + a.pml_yp;
-    const int xn = (i < a.pml_xm) ? i : i - (a.Nx - a.pml_xp) + a.pml_xm;
-    const int yn = (j < a.pml_ym) ? j : j - (a.Ny - a.pml_yp) + a.pml_ym;
     T bxi = 0, cxi = 0, byj = 0, cyj = 0;
-    if (xh) { bxi = a.bx[i]; cxi = a.cx[i]; }
-    if (yh) { byj = a.by[j]; cyj = a.cy[j]; }
+    if constexpr ((F & kFPmlXY) != 0) {
+        xh = a.px && ((i < a.pml_xm) || (i >= a.Nx - a.pml_xp && i < a.Nx - 1));
+        yh = a.py && ((j < a.pml_ym) || (j >= a.Ny - a.pml_yp && j < a.Ny - 1));
+        xn = (i < a.pml_xm) ? i : i - (a.Nx - a.pml_xp) + a.pml_xm;
+        yn = (j < a.pml_ym) ? j : j - (a.Ny - a.pml_yp) + a.pml_ym;
+        if (xh) { bxi = __ldg(a.bx + i); cxi = __ldg(a.cx + i); }
+        if (yh) { byj = __ldg(a.by + j); cyj = __ldg(a.cy + j); }
+    }
 
-    T ex = a.Ex[col + k0 * NxNy];
-    T ey = a.Ey[col + k0 * NxNy];
+    T ex = __ldg(Ex + col + k0 * NxNy);
+    T ey = __ldg(Ey + col + k0 * NxNy);
 
     for (int k = k0; k < k1; ++k) {
         const long long id = col + k * NxNy;
         const int kp = (k == a.Nz - 1) ? 0 : k + 1;
-        const T ex_kp = a.Ex[col + kp * NxNy], ey_kp = a.Ey[col + kp * NxNy];
-        const T ez = a.Ez[id];
-        const T ez_jp = a.Ez[coly + k * NxNy], ex_jp = a.Ex[coly + k * NxNy];
-        const T ez_ip = a.Ez[colx + k * NxNy], ey_ip = a.Ey[colx + k * NxNy];
-        const T hx = a.Hx[id], hy = a.Hy[id], hz = a.Hz[id];
-        const T az = a.dtdmz * a.ikz[k];
+        const T ex_kp = __ldg(Ex + col + kp * NxNy), ey_kp = __ldg(Ey + col + kp * NxNy);
+        const T ez = __ldg(Ez + id);
+        const T ez_jp = __ldg(Ez + coly + k * NxNy), ex_jp = __ldg(Ex + coly + k * NxNy);
+        const T ez_ip = __ldg(Ez + colx + k * NxNy), ey_ip = __ldg(Ey + colx + k * NxNy);
+        const T hx = Hx[id], hy = Hy[id], hz = Hz[id];
+        const T az = a.dtdmz * __ldg(a.ikz + k);
 
         const T dEy_z = ey_kp - ey, dEz_y = ez_jp - ez;
         const T dEz_x = ez_ip - ez, dEx_z = ex_kp - ex;
@@ -340,66 +424,116 @@ __global__ void __launch_bounds__(kTileX * kTileY) h_boundary(const __grid_const
         T nhy = hy + (ax * dEz_x - az * dEx_z);
         T nhz = hz + (ay * dEx_y - ax * dEy_x);
 
-        const bool zh = a.pz && ((k < a.pml_zm) || (k >= a.Nz - a.pml_zp && k < a.Nz - 1));
-        const int zn = (k < a.pml_zm) ? k : k - (a.Nz - a.pml_zp) + a.pml_zm;
+        bool zh = false;
+        int zn = 0;
         T bzk = 0, czk = 0;
-        if (zh) { bzk = a.bz[k]; czk = a.cz[k]; }
+        if constexpr ((F & kFPmlZ) != 0) {
+            zh = a.pz && ((k < a.pml_zm) || (k >= a.Nz - a.pml_zp && k < a.Nz - 1));
+            zn = (k < a.pml_zm) ? k : k - (a.Nz - a.pml_zp) + a.pml_zm;
+            if (zh) { bzk = __ldg(a.bz + k); czk = __ldg(a.cz + k); }
+        }
         // Hx: y block, then z block
-        if (yh) {
-            T *pp = a.psi_y0 + i + (long long)yn * a.Nx + (long long)k * a.Nx * nys;
-            const T ps = cpml_rec(byj, *pp, cyj, dEz_y);
-            *pp = ps;
-            nhx -= a.dtm * ps;
+        if constexpr ((F & kFPmlXY) != 0) {
+            if (yh) {
+                T *pp = a.psi_y0 + i + (long long)yn * a.Nx + (long long)k * a.Nx * nys;
+                const T ps = cpml_rec(byj, *pp, cyj, dEz_y);
+                *pp = ps;
+                nhx -= a.dtm * ps;
+            }
+            if (a.py && j == a.Ny - 1) nhx = 0;
         }
-        if (a.py && j == a.Ny - 1) nhx = 0;
-        if (zh) {
-            T *pp = a.psi_z0 + col + (long long)zn * NxNy;
-            const T ps = cpml_rec(bzk, *pp, czk, dEy_z);
-            *pp = ps;
-            nhx += a.dtm * ps;
+        if constexpr ((F & kFPmlZ) != 0) {
+            if (zh) {
+                T *pp = a.psi_z0 + col + (long long)zn * NxNy;
+                const T ps = cpml_rec(bzk, *pp, czk, dEy_z);
+                *pp = ps;
+                nhx += a.dtm * ps;
+            }
+            if (a.pz && k == a.Nz - 1) nhx = 0;
         }
-        if (a.pz && k == a.Nz - 1) nhx = 0;
         // Hy: x block, then z block
-        if (xh) {
-            T *pp = a.psi_x0 + xn + (long long)j * nxs + (long long)k * nxs * a.Ny;
-            const T ps = cpml_rec(bxi, *pp, cxi, dEz_x);
-            *pp = ps;
-            nhy += a.dtm * ps;
+        if constexpr ((F & kFPmlXY) != 0) {
+            if (xh) {
+                T *pp = a.psi_x0 + xn + (long long)j * nxs + (long long)k * nxs * a.Ny;
+                const T ps = cpml_rec(bxi, *pp, cxi, dEz_x);
+                *pp = ps;
+                nhy += a.dtm * ps;
+            }
+            if (a.px && i == a.Nx - 1) nhy = 0;
         }
-        if (a.px && i == a.Nx - 1) nhy = 0;
-        if (zh) {
-            T *pp = a.psi_z1 + col + (long long)zn * NxNy;
-            const T ps = cpml_rec(bzk, *pp, czk, dEx_z);
-            *pp = ps;
-            nhy -= a.dtm * ps;
+        if constexpr ((F & kFPmlZ) != 0) {
+            if (zh) {
+                T *pp = a.psi_z1 + col + (long long)zn * NxNy;
+                const T ps = cpml_rec(bzk, *pp, czk, dEx_z);
+                *pp = ps;
+                nhy -= a.dtm * ps;
+            }
+            if (a.pz && k == a.Nz - 1) nhy = 0;
         }
-        if (a.pz && k == a.Nz - 1) nhy = 0;
         // Hz: x block, then y block
-        if (xh) {
-            T *pp = a.psi_x1 + xn + (long long)j * nxs + (long long)k * nxs * a.Ny;
-            const T ps = cpml_rec(bxi, *pp, cxi, dEy_x);
-            *pp = ps;
-            nhz -= a.dtm * ps;
+        if constexpr ((F & kFPmlXY) != 0) {
+            if (xh) {
+                T *pp = a.psi_x1 + xn + (long long)j * nxs + (long long)k * nxs * a.Ny;
+                const T ps = cpml_rec(bxi, *pp, cxi, dEy_x);
+                *pp = ps;
+                nhz -= a.dtm * ps;
+            }
+            if (a.px && i == a.Nx - 1) nhz = 0;
+            if (yh) {
+                T *pp = a.psi_y1 + i + (long long)yn * a.Nx + (long long)k * a.Nx * nys;
+                const T ps = cpml_rec(byj, *pp, cyj, dEx_y);
+                *pp = ps;
+                nhz += a.dtm * ps;
+            }
+            if (a.py && j == a.Ny - 1) nhz = 0;
         }
-        if (a.px && i == a.Nx - 1) nhz = 0;
-        if (yh) {
-            T *pp = a.psi_y1 + i + (long long)yn * a.Nx + (long long)k * a.Nx * nys;
-            const T ps = cpml_rec(byj, *pp, cyj, dEx_y);
-            *pp = ps;
-            nhz += a.dtm * ps;
-        }
-        if (a.py && j == a.Ny - 1) nhz = 0;
 
-        // H plane injection after update_H (normal_incidence.cpp:353-357)
-        if (k == a.kinj) {
-            nhx = nhx + (T)a.sc[a.q].inj_hA;
-            nhy = nhy - (T)a.sc[a.q].inj_hB;
+        if constexpr ((F & kFMisc) != 0) {
+            // H plane injection after update_H (normal_incidence.cpp:353-357)
+            if (k == a.kinj) {
+                nhx = nhx + (T)a.sc[a.q].inj_hA;
+                nhy = nhy - (T)a.sc[a.q].inj_hB;
+            }
         }
-        a.Hx[id] = nhx;
-        a.Hy[id] = nhy;
-        a.Hz[id] = nhz;
+        Hx[id] = nhx;
+        Hy[id] = nhy;
+        Hz[id] = nhz;
         ex = ex_kp;
         ey = ey_kp;
+    }
+}
+
+// ---- launchers: group g of a half-step's WorkSplit ------------------------
+template <typename T, typename Tid>
+void launch_e_group_impl(const StepArgs<T, Tid> &a, const int4 *items, const WorkSplit &w, int g, cudaStream_t s) {
+    const int n = w.n[g];
+    if (n <= 0) return;
+    const int4 *p = items + w.off[g];
+    const dim3 blk(kTileX, kTileY);
+    switch (g) {
+        case kGroupInterior:
+            if (w.unroll >= 2) e_interior<T, Tid, 2><<<n, blk, 0, s>>>(a, p);
+            else e_interior<T, Tid, 1><<<n, blk, 0, s>>>(a, p);
+            break;
+        case kGroupPmlZ: e_boundary<T, Tid, kFPmlZ><<<n, blk, 0, s>>>(a, p); break;
+        case kGroupDisp: e_boundary<T, Tid, kFDisp><<<n, blk, 0, s>>>(a, p); break;
+        default: e_boundary<T, Tid, kFAll><<<n, blk, 0, s>>>(a, p); break;
+    }
+}
+
+template <typename T, typename Tid>
+void launch_h_group_impl(const StepArgs<T, Tid> &a, const int4 *items, const WorkSplit &w, int g, cudaStream_t s) {
+    const int n = w.n[g];
+    if (n <= 0) return;
+    const int4 *p = items + w.off[g];
+    const dim3 blk(kTileX, kTileY);
+    switch (g) {
+        case kGroupInterior:
+            if (w.unroll >= 2) h_interior<T, Tid, 2><<<n, blk, 0, s>>>(a, p);
+            else h_interior<T, Tid, 1><<<n, blk, 0, s>>>(a, p);
+            break;
+        case kGroupPmlZ: h_boundary<T, Tid, kFPmlZ><<<n, blk, 0, s>>>(a, p); break;
+        default: h_boundary<T, Tid, kFAll><<<n, blk, 0, s>>>(a, p); break;
     }
 }
 

@@ -3,28 +3,16 @@
 #include "yee.cuh"
 
 namespace aefdtd {
-void launch_e_interior(const StepArgs<float, uint8_t> &a, const int4 *items, int n, cudaStream_t s) {
-    if (n > 0) e_interior<float, uint8_t><<<n, dim3(kTileX, kTileY), 0, s>>>(a, items);
+void launch_e_group(const StepArgs<float, uint8_t> &a, const int4 *items, const WorkSplit &w, int g, cudaStream_t s) {
+    launch_e_group_impl(a, items, w, g, s);
 }
-void launch_e_boundary(const StepArgs<float, uint8_t> &a, const int4 *items, int n, cudaStream_t s) {
-    if (n > 0) e_boundary<float, uint8_t><<<n, dim3(kTileX, kTileY), 0, s>>>(a, items);
+void launch_h_group(const StepArgs<float, uint8_t> &a, const int4 *items, const WorkSplit &w, int g, cudaStream_t s) {
+    launch_h_group_impl(a, items, w, g, s);
 }
-void launch_h_interior(const StepArgs<float, uint8_t> &a, const int4 *items, int n, cudaStream_t s) {
-    if (n > 0) h_interior<float, uint8_t><<<n, dim3(kTileX, kTileY), 0, s>>>(a, items);
+void launch_e_group(const StepArgs<float, uint16_t> &a, const int4 *items, const WorkSplit &w, int g, cudaStream_t s) {
+    launch_e_group_impl(a, items, w, g, s);
 }
-void launch_h_boundary(const StepArgs<float, uint8_t> &a, const int4 *items, int n, cudaStream_t s) {
-    if (n > 0) h_boundary<float, uint8_t><<<n, dim3(kTileX, kTileY), 0, s>>>(a, items);
-}
-void launch_e_interior(const StepArgs<float, uint16_t> &a, const int4 *items, int n, cudaStream_t s) {
-    if (n > 0) e_interior<float, uint16_t><<<n, dim3(kTileX, kTileY), 0, s>>>(a, items);
-}
-void launch_e_boundary(const StepArgs<float, uint16_t> &a, const int4 *items, int n, cudaStream_t s) {
-    if (n > 0) e_boundary<float, uint16_t><<<n, dim3(kTileX, kTileY), 0, s>>>(a, items);
-}
-void launch_h_interior(const StepArgs<float, uint16_t> &a, const int4 *items, int n, cudaStream_t s) {
-    if (n > 0) h_interior<float, uint16_t><<<n, dim3(kTileX, kTileY), 0, s>>>(a, items);
-}
-void launch_h_boundary(const StepArgs<float, uint16_t> &a, const int4 *items, int n, cudaStream_t s) {
-    if (n > 0) h_boundary<float, uint16_t><<<n, dim3(kTileX, kTileY), 0, s>>>(a, items);
+void launch_h_group(const StepArgs<float, uint16_t> &a, const int4 *items, const WorkSplit &w, int g, cudaStream_t s) {
+    launch_h_group_impl(a, items, w, g, s);
 }
 }  // namespace aefdtd

@@ -4,28 +4,16 @@
 #include "yee.cuh"
 
 namespace aefdtd {
-void launch_e_interior(const StepArgs<double, uint8_t> &a, const int4 *items, int n, cudaStream_t s) {
-    if (n > 0) e_interior<double, uint8_t><<<n, dim3(kTileX, kTileY), 0, s>>>(a, items);
+void launch_e_group(const StepArgs<double, uint8_t> &a, const int4 *items, const WorkSplit &w, int g, cudaStream_t s) {
+    launch_e_group_impl(a, items, w, g, s);
 }
-void launch_e_boundary(const StepArgs<double, uint8_t> &a, const int4 *items, int n, cudaStream_t s) {
-    if (n > 0) e_boundary<double, uint8_t><<<n, dim3(kTileX, kTileY), 0, s>>>(a, items);
+void launch_h_group(const StepArgs<double, uint8_t> &a, const int4 *items, const WorkSplit &w, int g, cudaStream_t s) {
+    launch_h_group_impl(a, items, w, g, s);
 }
-void launch_h_interior(const StepArgs<double, uint8_t> &a, const int4 *items, int n, cudaStream_t s) {
-    if (n > 0) h_interior<double, uint8_t><<<n, dim3(kTileX, kTileY), 0, s>>>(a, items);
+void launch_e_group(const StepArgs<double, uint16_t> &a, const int4 *items, const WorkSplit &w, int g, cudaStream_t s) {
+    launch_e_group_impl(a, items, w, g, s);
 }
-void launch_h_boundary(const StepArgs<double, uint8_t> &a, const int4 *items, int n, cudaStream_t s) {
-    if (n > 0) h_boundary<double, uint8_t><<<n, dim3(kTileX, kTileY), 0, s>>>(a, items);
-}
-void launch_e_interior(const StepArgs<double, uint16_t> &a, const int4 *items, int n, cudaStream_t s) {
-    if (n > 0) e_interior<double, uint16_t><<<n, dim3(kTileX, kTileY), 0, s>>>(a, items);
-}
-void launch_e_boundary(const StepArgs<double, uint16_t> &a, const int4 *items, int n, cudaStream_t s) {
-    if (n > 0) e_boundary<double, uint16_t><<<n, dim3(kTileX, kTileY), 0, s>>>(a, items);
-}
-void launch_h_interior(const StepArgs<double, uint16_t> &a, const int4 *items, int n, cudaStream_t s) {
-    if (n > 0) h_interior<double, uint16_t><<<n, dim3(kTileX, kTileY), 0, s>>>(a, items);
-}
-void launch_h_boundary(const StepArgs<double, uint16_t> &a, const int4 *items, int n, cudaStream_t s) {
-    if (n > 0) h_boundary<double, uint16_t><<<n, dim3(kTileX, kTileY), 0, s>>>(a, items);
+void launch_h_group(const StepArgs<double, uint16_t> &a, const int4 *items, const WorkSplit &w, int g, cudaStream_t s) {
+    launch_h_group_impl(a, items, w, g, s);
 }
 }  // namespace aefdtd

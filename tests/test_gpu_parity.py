@@ -136,11 +136,27 @@ def test_interior_and_boundary_kernels_agree(prec, monkeypatch):
         assert rel(a["fields"], b["fields"]) < 1e-6
 
 
-@pytest.mark.parametrize("kchunk", ["1", "3", "1000"])
-def test_z_chunking_does_not_change_results(kchunk, monkeypatch):
+@pytest.mark.parametrize("name", ["gold_sphere", "custom_box"])
+def test_concurrent_groups_match_serial_groups(name, monkeypatch):
+    """Boundary groups on side streams (parallel graph branches) against all
+    groups launched in order on one stream: bit-identical."""
+    sc = getattr(scenes, name)(nsteps=90)
+    a = fdtd.run(sc)
+    monkeypatch.setenv("AEFDTD_SERIAL_GROUPS", "1")
+    b = fdtd.run(sc)
+    assert np.array_equal(a["fields"], b["fields"])
+    for fa, fb in zip(a["flux"], b["flux"]):
+        assert np.array_equal(fa, fb)
+
+
+@pytest.mark.parametrize("kchunk,zunroll", [("1", "2"), ("3", "2"), ("3", "1"), ("1000", "1"), ("1000", "2")])
+def test_z_chunking_does_not_change_results(kchunk, zunroll, monkeypatch):
+    """Planes per work item and planes per interior-kernel iteration (odd
+    chunks leave a one-plane tail in the two-plane loop) change no bit."""
     sc = scenes.custom_box(nsteps=40)
     a = fdtd.run(sc)
     monkeypatch.setenv("AEFDTD_KCHUNK", kchunk)
+    monkeypatch.setenv("AEFDTD_ZUNROLL", zunroll)
     b = fdtd.run(sc)
     assert np.array_equal(a["fields"], b["fields"])
 
