@@ -127,6 +127,7 @@ template <typename T> struct SensorStepArgs {
     double *partial;         // [nbp][12] of this step
     int ng;
     GatherDesc g[kMaxGather];
+    int part;                // 0: plane sums + E gathers (reads E only); 1: H gathers (reads H only)
 };
 
 struct PhasorArgs {

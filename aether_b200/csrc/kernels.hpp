@@ -24,8 +24,9 @@ AEFDTD_DECL_YEE(float, uint16_t)
 #undef AEFDTD_DECL_YEE
 
 // sensors.cu (compiled with --fmad=false)
-void launch_sensor_step(const SensorStepArgs<double> &a, cudaStream_t s);
-void launch_sensor_step(const SensorStepArgs<float> &a, cudaStream_t s);
+// one part (a.part) of a step's sensor work; returns the launches issued
+int launch_sensor_step(const SensorStepArgs<double> &a, cudaStream_t s);
+int launch_sensor_step(const SensorStepArgs<float> &a, cudaStream_t s);
 void launch_plane_reduce(const double *partial, int nbp, const StepScalars *sc, double *out, int steps,
                          cudaStream_t s);
 void launch_phasors(const PhasorArgs &a, cudaStream_t s);

@@ -13,6 +13,7 @@
 #include <cstring>
 #include <numbers>
 #include <string>
+#include <map>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -122,8 +123,14 @@ struct PlaneSensor {
     int type, x1, x2, y1, y2, z1, z2, span1, span2, P, nl;
     std::vector<double> lambda, w;
     int step = 0;          // steps fed
-    int nbuf = 0;          // filled slots of the sample buffer
+    int nbuf = 0;          // filled slots of the sample buffer half being written
     int buf_step0 = 0;     // step of slot 0
+    int half = 0;          // sample-buffer half the gathers write (S holds two halves of K steps)
+    // a filled half whose DFT block is still to be accumulated: launched at the
+    // start of the next segment beside its steps, or when results are read
+    bool pending = false;
+    int pend_half = 0, pend_n = 0, pend_step0 = 0;
+    const StepScalars *pend_tbl = nullptr;   // step of slot 0 read from this table, else pend_step0
     DBuf S, acc, wdev, WE, WH, flux;
     DBuf Btc;              // tensor-core phasor image (FP32 path)
     int N0 = 0, N1 = 0;
@@ -151,7 +158,11 @@ struct aefdtd_sim {
     // joined back into `stream` by events (parallel branches in the graphs)
     cudaStream_t side[kGroups - 1] = {};
     cudaEvent_t ev_fork = nullptr, ev_join[kGroups - 1] = {};
+    // side streams of the two sensor parts (part 0 beside H, part 1 beside the next E)
+    cudaStream_t side_s[2] = {};
+    cudaEvent_t ev_s_fork[2] = {}, ev_s_join[2] = {};
     bool concurrent_groups = true;
+    bool serial_now = false;        // timing mode: every launch in order on `stream`
     template <typename Launch> void run_groups(const WorkSplit &w, Launch &&launch);
     size_t dev_bytes = 0;
     uint64_t launches = 0;
@@ -216,7 +227,12 @@ struct aefdtd_sim {
     void finalize_tables();
     template <typename T, typename Tid> void fill_args(StepArgs<T, Tid> &a, bool e_side);
     template <typename T, typename Tid> void run_steps(int n);
-    template <typename T> void flush_sensor(PlaneSensor &s, const StepScalars *step0_ptr = nullptr);
+    template <typename T>
+    void flush_block(PlaneSensor &s, int half, int n, const StepScalars *step0_ptr, int step0, cudaStream_t st);
+    template <typename T> void launch_pending(PlaneSensor &s, cudaStream_t st);
+    void drain_sensors();
+    cudaStream_t side_f = nullptr;
+    cudaEvent_t ev_f_fork = nullptr, ev_f_join = nullptr;
     template <typename T, typename Tid> void enqueue_segment(int L, StepScalars *tbl, bool record);
     void fill_scalars(int t, int osc_offset, StepScalars &s) const;
     void drop_graphs();
@@ -232,7 +248,9 @@ struct aefdtd_sim {
     DBuf tables;
     bool use_graphs = true;
     bool graphs_dirty = true;
-    cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
+    // captured segments, keyed by table slot, pending-flush state and the
+    // sensors' buffer halves (the pointers a segment's launches bake in)
+    std::map<uint64_t, cudaGraphExec_t> graph_exec;
     uint64_t graph_launches = 0;
     void step(int n);
     void zero_state();
@@ -254,7 +272,7 @@ aefdtd_sim::~aefdtd_sim() {
     psum_partial.release(t);
     err.release(t);
     tables.release(t);
-    for (auto &gx : graph_exec) if (gx) cudaGraphExecDestroy(gx);
+    for (auto &gx : graph_exec) if (gx.second) cudaGraphExecDestroy(gx.second);
     items.release(t);
     for (auto *s : sensors) {
         s->S.release(t); s->acc.release(t); s->wdev.release(t); s->WE.release(t); s->WH.release(t); s->flux.release(t);
@@ -265,6 +283,14 @@ aefdtd_sim::~aefdtd_sim() {
     for (auto &e : ev_join) if (e) cudaEventDestroy(e);
     if (ev_fork) cudaEventDestroy(ev_fork);
     for (auto &x : side) if (x) cudaStreamDestroy(x);
+    for (int k = 0; k < 2; k++) {
+        if (ev_s_fork[k]) cudaEventDestroy(ev_s_fork[k]);
+        if (ev_s_join[k]) cudaEventDestroy(ev_s_join[k]);
+        if (side_s[k]) cudaStreamDestroy(side_s[k]);
+    }
+    if (ev_f_fork) cudaEventDestroy(ev_f_fork);
+    if (ev_f_join) cudaEventDestroy(ev_f_join);
+    if (side_f) cudaStreamDestroy(side_f);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -287,6 +313,14 @@ void aefdtd_sim::construct(const aefdtd_grid_desc *d) {
     for (auto &x : side) AE_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
     AE_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
     for (auto &e : ev_join) AE_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    AE_CUDA(cudaStreamCreateWithFlags(&side_f, cudaStreamNonBlocking));
+    AE_CUDA(cudaEventCreateWithFlags(&ev_f_fork, cudaEventDisableTiming));
+    AE_CUDA(cudaEventCreateWithFlags(&ev_f_join, cudaEventDisableTiming));
+    for (int k = 0; k < 2; k++) {
+        AE_CUDA(cudaStreamCreateWithFlags(&side_s[k], cudaStreamNonBlocking));
+        AE_CUDA(cudaEventCreateWithFlags(&ev_s_fork[k], cudaEventDisableTiming));
+        AE_CUDA(cudaEventCreateWithFlags(&ev_s_join[k], cudaEventDisableTiming));
+    }
     concurrent_groups = std::getenv("AEFDTD_SERIAL_GROUPS") == nullptr;
 
     Dx = g.dx; Dy = g.dy; Dz = g.dz;
@@ -642,29 +676,49 @@ void aefdtd_sim::fill_args(StepArgs<T, Tid> &a, bool e_side) {
     a.err = err.as<int>();
 }
 
+// Accumulates one DFT block of a sensor: n buffered steps in sample-buffer
+// half `half`, slot 0 being step *step0_ptr (a step table entry) or step0.
 template <typename T>
-void aefdtd_sim::flush_sensor(PlaneSensor &s, const StepScalars *step0_ptr) {
-    if (s.nbuf == 0) return;
+void aefdtd_sim::flush_block(PlaneSensor &s, int half, int n, const StepScalars *step0_ptr, int step0, cudaStream_t st) {
+    if (n == 0) return;
+    const size_t hoff = size_t(half) * dft_k * 6 * s.P;
     if (!fp64 && s.Btc.p) {
         // tensor-core DFT: phasors split into TF32 hi/lo in the B image, then the GEMM
-        DftTcPhasorArgs pa{dft_k, s.nbuf, s.nl, s.N0, s.N1, Nt, Ntap, step0_ptr ? &step0_ptr->step : nullptr,
-                           step0_ptr ? 0 : s.buf_step0, Dt, s.wdev.as<double>(), s.Btc.as<float>(),
+        DftTcPhasorArgs pa{dft_k, n, s.nl, s.N0, s.N1, Nt, Ntap, step0_ptr ? &step0_ptr->step : nullptr,
+                           step0_ptr ? 0 : step0, Dt, s.wdev.as<double>(), s.Btc.as<float>(),
                            size_t(4) * 256 * dft_k};
-        launch_phasors_tc(pa, stream);
-        DftTcArgs aa{dft_k, s.nbuf, s.nl, s.P, s.N0, s.N1, s.S.as<float>(), s.Btc.as<float>(),
+        launch_phasors_tc(pa, st);
+        DftTcArgs aa{dft_k, n, s.nl, s.P, s.N0, s.N1, s.S.as<float>() + hoff, s.Btc.as<float>(),
                      size_t(4) * 256 * dft_k, s.acc.as<double2>(), err.as<int>()};
-        launch_accumulate_tc(aa, stream);
+        launch_accumulate_tc(aa, st);
         launches += 2;
-        s.nbuf = 0;
         return;
     }
-    PhasorArgs pa{s.nbuf, s.nl, Nt, Ntap, step0_ptr ? &step0_ptr->step : nullptr, step0_ptr ? 0 : s.buf_step0, Dt,
+    PhasorArgs pa{n, s.nl, Nt, Ntap, step0_ptr ? &step0_ptr->step : nullptr, step0_ptr ? 0 : step0, Dt,
                   s.wdev.as<double>(), s.WE.as<double2>(), s.WH.as<double2>()};
-    launch_phasors(pa, stream);
-    AccumArgs<T> aa{s.P, s.nl, s.nbuf, s.S.as<T>(), s.WE.as<double2>(), s.WH.as<double2>(), s.acc.as<double2>()};
-    launch_accumulate(aa, stream);
+    launch_phasors(pa, st);
+    AccumArgs<T> aa{s.P, s.nl, n, s.S.as<T>() + hoff, s.WE.as<double2>(), s.WH.as<double2>(), s.acc.as<double2>()};
+    launch_accumulate(aa, st);
     launches += 2;
-    s.nbuf = 0;
+}
+
+template <typename T> void aefdtd_sim::launch_pending(PlaneSensor &s, cudaStream_t st) {
+    if (!s.pending) return;
+    flush_block<T>(s, s.pend_half, s.pend_n, s.pend_tbl, s.pend_step0, st);
+    s.pending = false;
+}
+
+// Accumulates every buffered sample of every sensor on the main stream:
+// pending blocks first, then the partly filled halves (all sensors stay
+// aligned on block boundaries).
+void aefdtd_sim::drain_sensors() {
+    for (auto *p : sensors) { if (fp64) launch_pending<double>(*p, stream); else launch_pending<float>(*p, stream); }
+    for (auto *p : sensors) {
+        if (p->nbuf == 0) continue;
+        if (fp64) flush_block<double>(*p, p->half, p->nbuf, nullptr, p->buf_step0, stream);
+        else flush_block<float>(*p, p->half, p->nbuf, nullptr, p->buf_step0, stream);
+        p->nbuf = 0;
+    }
 }
 
 // Host values of one step's scalars (excitation, sensors), FP64.
@@ -707,7 +761,7 @@ void aefdtd_sim::fill_scalars(int t, int osc_offset, StepScalars &s) const {
 template <typename Launch> void aefdtd_sim::run_groups(const WorkSplit &w, Launch &&launch) {
     int nside = 0;
     for (int g = 1; g < kGroups; g++) nside += w.n[g] > 0;
-    if (!concurrent_groups || nside == 0) {
+    if (!concurrent_groups || serial_now || nside == 0) {
         for (int g = 0; g < kGroups; g++) launch(g, stream);
         return;
     }
@@ -758,14 +812,44 @@ void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
         sa.P = PulseDev{pulse.k, pulse.omega, pulse.kx, pulse.ky, pulse.kz, pulse.n_ind, pulse.dz, pulse.C1,
                         pulse.Ex0, pulse.Ey0, pulse.Ez0};
     }
+    // Sensor work of step q runs in two parts (sensors.cuh, sensor_step): part 0
+    // (plane sums, E samples) reads E only and runs beside H(q); part 1 (H
+    // samples) reads H only and runs beside E(q+1). H(q+1) and any DFT flush
+    // wait for part 1. In timing mode everything runs in order on `stream`.
+    serial_now = record;
+    const bool conc = concurrent_groups && !record;
+    bool h_pending = false;
+    // DFT blocks filled in the previous segment accumulate beside this one's
+    // steps: they read the other sample-buffer half and only touch acc
+    bool f_pending = false;
+    bool any_pending = false;
+    for (PlaneSensor *ps : sensors) any_pending |= ps->pending;
+    if (any_pending) {
+        if (conc) {
+            AE_CUDA(cudaEventRecord(ev_f_fork, stream));
+            AE_CUDA(cudaStreamWaitEvent(side_f, ev_f_fork, 0));
+            for (PlaneSensor *ps : sensors) launch_pending<T>(*ps, side_f);
+            AE_CUDA(cudaEventRecord(ev_f_join, side_f));
+            f_pending = true;
+        } else {
+            for (PlaneSensor *ps : sensors) launch_pending<T>(*ps, stream);
+        }
+    }
+    auto join_h = [&] {
+        if (h_pending) AE_CUDA(cudaStreamWaitEvent(stream, ev_s_join[1], 0));
+        h_pending = false;
+    };
+    auto fork = [&](int k, auto &&launch) {
+        AE_CUDA(cudaEventRecord(ev_s_fork[k], stream));
+        AE_CUDA(cudaStreamWaitEvent(side_s[k], ev_s_fork[k], 0));
+        launch(side_s[k]);
+        AE_CUDA(cudaEventRecord(ev_s_join[k], side_s[k]));
+    };
     for (int q = 0; q < L; q++) {
         if (record) AE_CUDA(cudaEventRecord(tev[4 * q + 0], stream));
         ea.q = ha.q = q;
         run_groups(wsE, [&](int g, cudaStream_t st) { launch_e_group(ea, wi, wsE, g, st); });
         if (record) AE_CUDA(cudaEventRecord(tev[4 * q + 1], stream));
-        run_groups(wsH, [&](int g, cudaStream_t st) { launch_h_group(ha, wi, wsH, g, st); });
-        launches += groups;
-        if (record) AE_CUDA(cudaEventRecord(tev[4 * q + 2], stream));
         // sensors: fed after H in both drivers; plane sums read E of this step
         sa.q = q;
         sa.partial = psum_partial.as<double>() + size_t(q) * std::max(sa.nbp, 1) * 12;
@@ -780,19 +864,49 @@ void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
             g.block0 = blk;
             g.nblocks = (s.P + kPlaneThreads - 1) / kPlaneThreads;
             blk += g.nblocks;
-            g.S = s.S.as<T>() + (size_t)s.nbuf * 6 * s.P;
+            g.S = s.S.as<T>() + ((size_t)s.half * dft_k + s.nbuf) * 6 * s.P;
         }
-        if (sa.nbp > 0 || sa.ng > 0) {
-            launch_sensor_step(sa, stream);
-            launches++;
+        const bool part0 = sa.nbp > 0 || sa.ng > 0;
+        sa.part = 0;
+        if (part0 && conc) fork(0, [&](cudaStream_t st) { launches += launch_sensor_step(sa, st); });
+        join_h();
+        run_groups(wsH, [&](int g, cudaStream_t st) { launch_h_group(ha, wi, wsH, g, st); });
+        launches += groups;
+        if (record) AE_CUDA(cudaEventRecord(tev[4 * q + 2], stream));
+        if (part0) {
+            if (conc) AE_CUDA(cudaStreamWaitEvent(stream, ev_s_join[0], 0));
+            else launches += launch_sensor_step(sa, stream);
+        }
+        if (sa.ng > 0) {
+            sa.part = 1;
+            if (conc) {
+                fork(1, [&](cudaStream_t st) { launches += launch_sensor_step(sa, st); });
+                h_pending = true;
+            } else {
+                launches += launch_sensor_step(sa, stream);
+            }
         }
         for (PlaneSensor *ps : sensors) {
             ps->nbuf++;
             ps->step++;
-            if (ps->nbuf == dft_k) flush_sensor<T>(*ps, ps->buf_step0 == tstep + q + 1 - dft_k && q + 1 == dft_k ? tbl : nullptr);
+            if (ps->nbuf == dft_k) {
+                // a filled half: accumulated at the next segment's start (or on a read)
+                PlaneSensor &s = *ps;
+                if (s.pending) launch_pending<T>(s, stream);
+                s.pending = true;
+                s.pend_half = s.half;
+                s.pend_n = s.nbuf;
+                s.pend_step0 = s.buf_step0;
+                s.pend_tbl = (s.buf_step0 == tstep + q + 1 - dft_k && q + 1 == dft_k) ? tbl : nullptr;
+                s.half ^= 1;
+                s.nbuf = 0;
+            }
         }
         if (record) AE_CUDA(cudaEventRecord(tev[4 * q + 3], stream));
     }
+    join_h();
+    if (f_pending) AE_CUDA(cudaStreamWaitEvent(stream, ev_f_join, 0));
+    serial_now = false;
     if (normal) {
         launch_plane_reduce(psum_partial.as<double>(), sa.nbp, tbl, psums.as<double>(), L, stream);
         launches++;
@@ -828,37 +942,74 @@ void aefdtd_sim::run_steps(int n) {
     std::vector<StepScalars> host(seg_len);
     int done = 0;
     while (done < n) {
-        // a segment ends where the DFT buffers fill, so captured segments start empty
+        // a segment ends where a DFT buffer half fills, so captured segments start empty
         int L = std::min(n - done, seg_len);
-        if (!sensors.empty()) L = std::min(L, dft_k - sensors[0]->nbuf);
+        bool empty = true;
+        for (auto *s : sensors) { L = std::min(L, dft_k - s->nbuf); empty &= s->nbuf == 0; }
         const int slot = seg_slot;
         seg_slot ^= 1;
         StepScalars *tbl = tables.as<StepScalars>() + size_t(slot) * seg_len;
+        const StepScalars *other = tables.as<StepScalars>() + size_t(slot ^ 1) * seg_len;
+        // pending blocks a graph may carry: each one filled by the previous
+        // (full, other-slot) segment; any other pending block is accumulated now
+        bool canon = true, anyp = false;
+        for (auto *s : sensors)
+            if (s->pending) {
+                anyp = true;
+                canon &= s->pend_tbl == other && s->pend_n == dft_k && s->pend_half == (s->half ^ 1);
+            }
+        const bool full = (L == seg_len) && empty && !timing && use_graphs;
+        if (full && anyp && !canon) {
+            for (auto *s : sensors) launch_pending<T>(*s, stream);
+            anyp = false;
+        }
         for (int q = 0; q < L; q++) fill_scalars(tstep + q, q, host[q]);
         AE_CUDA(cudaMemcpyAsync(tbl, host.data(), sizeof(StepScalars) * L, cudaMemcpyHostToDevice, stream));
-        const bool full = (L == seg_len) && (sensors.empty() || sensors[0]->nbuf == 0);
         if (timing) {
             enqueue_segment<T, Tid>(L, tbl, true);
             accumulate_timing(L);
-        } else if (full && use_graphs) {
-            if (!graph_exec[slot]) {
+        } else if (full) {
+            uint64_t key = uint64_t(slot) | (uint64_t(anyp) << 1);
+            for (size_t k = 0; k < sensors.size(); k++) key |= uint64_t(sensors[k]->half) << (2 + k);
+            // host-side effect of a full segment on the sensors (what enqueue_segment does)
+            auto advance = [&] {
+                for (auto *s : sensors) {
+                    s->pending = true;
+                    s->pend_half = s->half;
+                    s->pend_n = dft_k;
+                    s->pend_step0 = s->step;
+                    s->pend_tbl = tbl;
+                    s->half ^= 1;
+                    s->step += L;
+                    s->buf_step0 = s->step;
+                    s->nbuf = 0;
+                }
+            };
+            cudaGraphExec_t &gx = graph_exec[key];
+            if (!gx) {
                 // capture once; the sequence reads every per-step value from the table
-                std::vector<int> nb0, st0;
-                for (auto *s : sensors) { nb0.push_back(s->nbuf); st0.push_back(s->step); }
+                std::vector<PlaneSensor> snap;
+                for (auto *s : sensors) snap.push_back(*s);
                 uint64_t l0 = launches;
                 AE_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
                 enqueue_segment<T, Tid>(L, tbl, false);
                 cudaGraph_t gr = nullptr;
                 AE_CUDA(cudaStreamEndCapture(stream, &gr));
-                AE_CUDA(cudaGraphInstantiate(&graph_exec[slot], gr, 0));
+                AE_CUDA(cudaGraphInstantiate(&gx, gr, 0));
                 cudaGraphDestroy(gr);
                 graph_launches = launches - l0;
                 launches = l0;
-                for (size_t s = 0; s < sensors.size(); s++) { sensors[s]->nbuf = nb0[s]; sensors[s]->step = st0[s]; }
+                for (size_t k = 0; k < sensors.size(); k++) {
+                    PlaneSensor &d = *sensors[k];
+                    const PlaneSensor &o = snap[k];
+                    d.step = o.step; d.nbuf = o.nbuf; d.buf_step0 = o.buf_step0; d.half = o.half;
+                    d.pending = o.pending; d.pend_half = o.pend_half; d.pend_n = o.pend_n;
+                    d.pend_step0 = o.pend_step0; d.pend_tbl = o.pend_tbl;
+                }
             }
-            AE_CUDA(cudaGraphLaunch(graph_exec[slot], stream));
+            AE_CUDA(cudaGraphLaunch(gx, stream));
             launches += graph_launches;
-            for (auto *s : sensors) { s->step += L; s->buf_step0 = s->step; s->nbuf = 0; }
+            advance();
         } else {
             enqueue_segment<T, Tid>(L, tbl, false);
         }
@@ -871,7 +1022,8 @@ void aefdtd_sim::run_steps(int n) {
 
 void aefdtd_sim::drop_graphs() {
     for (auto &g : graph_exec)
-        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        if (g.second) cudaGraphExecDestroy(g.second);
+    graph_exec.clear();
     graphs_dirty = false;
 }
 
@@ -1031,7 +1183,7 @@ void aefdtd_sim::zero_state() {
     if (psi.p) AE_CUDA(cudaMemsetAsync(psi.p, 0, psi.n, stream));
     for (auto *s : sensors) {
         if (s->acc.p) AE_CUDA(cudaMemsetAsync(s->acc.p, 0, s->acc.n, stream));
-        s->step = 0; s->nbuf = 0;
+        s->step = 0; s->nbuf = 0; s->half = 0; s->pending = false;
     }
     for (auto &o : oscs) o.step = 0;
     tstep = 0;
@@ -1203,7 +1355,7 @@ aefdtd_status aefdtd_add_planar_sensor(aefdtd_sim *s, const aefdtd_sensor_desc *
         }
         size_t es = s->fp64 ? 8 : 4;
         try {
-            p->S.alloc(size_t(s->dft_k) * 6 * p->P * es, s->dev_bytes);
+            p->S.alloc(size_t(2) * s->dft_k * 6 * p->P * es, s->dev_bytes);
             p->acc.alloc(size_t(6) * p->nl * p->P * 16, s->dev_bytes);
             p->wdev.alloc(size_t(p->nl) * 8, s->dev_bytes);
             p->WE.alloc(size_t(s->dft_k) * p->nl * 16, s->dev_bytes);
@@ -1237,8 +1389,7 @@ aefdtd_status aefdtd_add_planar_sensor(aefdtd_sim *s, const aefdtd_sensor_desc *
             delete p;
             fail(AEFDTD_BAD_ARG, "at most 8 planar sensors per simulation");
         }
-        if (!s->sensors.empty() && s->sensors[0]->nbuf != 0)
-            for (auto *o : s->sensors) { if (s->fp64) s->flush_sensor<double>(*o); else s->flush_sensor<float>(*o); }
+        s->drain_sensors();
         s->sensors.push_back(p);
         s->graphs_dirty = true;
         if (id) *id = (int32_t)s->sensors.size() - 1;
@@ -1408,8 +1559,7 @@ aefdtd_status aefdtd_get_sensor_flux(aefdtd_sim *s, int32_t id, double *out, int
         PlaneSensor &p = *s->sensors[id];
         if (nl != p.nl) fail(AEFDTD_BAD_ARG, "nl must equal the sensor's spectrum size");
         s->set_device();
-        if (s->fp64) s->flush_sensor<double>(p); else s->flush_sensor<float>(p);
-        s->graphs_dirty = true;
+        s->drain_sensors();
         double af = p.type <= 1 ? s->Dy * s->Dz : (p.type <= 3 ? s->Dx * s->Dz : s->Dx * s->Dy);
         FluxArgs fa{p.P, p.nl, p.type, af, p.acc.as<double2>(), p.flux.as<double>()};
         launch_flux(fa, s->stream);
@@ -1427,8 +1577,7 @@ aefdtd_status aefdtd_get_sensor_dft(aefdtd_sim *s, int32_t id, double *out, size
         PlaneSensor &p = *s->sensors[id];
         if (count != size_t(6) * p.P * p.nl * 2) fail(AEFDTD_BAD_ARG, "count must be 6*span1*span2*nl*2");
         s->set_device();
-        if (s->fp64) s->flush_sensor<double>(p); else s->flush_sensor<float>(p);
-        s->graphs_dirty = true;
+        s->drain_sensors();
         AE_CUDA(cudaMemcpyAsync(out, p.acc.p, count * 8, cudaMemcpyDeviceToHost, s->stream));
         AE_CUDA(cudaStreamSynchronize(s->stream));
     });

@@ -7,13 +7,16 @@
 #include <algorithm>
 
 namespace aefdtd {
-template <typename T> static void step_impl(const SensorStepArgs<T> &a, cudaStream_t s) {
+// Part 0: plane-sum and gather blocks; part 1: gather blocks only.
+template <typename T> static int step_impl(const SensorStepArgs<T> &a, cudaStream_t s) {
     int nb = a.nbp;
     for (int g = 0; g < a.ng; ++g) nb = std::max(nb, a.g[g].block0 + a.g[g].nblocks);
+    if (a.part) nb -= a.nbp;
     if (nb > 0) sensor_step<<<nb, kPlaneThreads, 0, s>>>(a);
+    return nb > 0;
 }
-void launch_sensor_step(const SensorStepArgs<double> &a, cudaStream_t s) { step_impl(a, s); }
-void launch_sensor_step(const SensorStepArgs<float> &a, cudaStream_t s) { step_impl(a, s); }
+int launch_sensor_step(const SensorStepArgs<double> &a, cudaStream_t s) { return step_impl(a, s); }
+int launch_sensor_step(const SensorStepArgs<float> &a, cudaStream_t s) { return step_impl(a, s); }
 void launch_plane_reduce(const double *partial, int nbp, const StepScalars *sc, double *out, int steps,
                          cudaStream_t s) {
     if (steps > 0) plane_sums_reduce<<<steps, 32, 0, s>>>(partial, nbp, sc, out);

@@ -111,24 +111,31 @@ __device__ __forceinline__ void gather_one(const SensorStepArgs<T> &a, const Gat
     const int jp = (j + 1 == a.Ny) ? 0 : j + 1;
     const int kp = (k + 1 == a.Nz) ? 0 : k + 1;
     auto I = [&](int x, int y, int z) { return x + (long long)y * a.Nx + (long long)z * a.NxNy; };
-    const T ex = (a.Ex[I(i, j, k)] + a.Ex[I(i, jp, k)] + a.Ex[I(i, j, kp)] + a.Ex[I(i, jp, kp)]) / T(4.0);
-    const T ey = (a.Ey[I(i, j, k)] + a.Ey[I(ip, j, k)] + a.Ey[I(i, j, kp)] + a.Ey[I(ip, j, kp)]) / T(4.0);
-    const T ez = (a.Ez[I(i, j, k)] + a.Ez[I(ip, j, k)] + a.Ez[I(i, jp, k)] + a.Ez[I(ip, jp, k)]) / T(4.0);
-    const T hx = (a.Hx[I(i, j, k)] + a.Hx[I(ip, j, k)]) / T(2.0);
-    const T hy = (a.Hy[I(i, j, k)] + a.Hy[I(i, jp, k)]) / T(2.0);
-    const T hz = (a.Hz[I(i, j, k)] + a.Hz[I(i, j, kp)]) / T(2.0);
     T *S = static_cast<T *>(g.S);
-    S[0 * (long long)g.P + q] = ex;
-    S[1 * (long long)g.P + q] = ey;
-    S[2 * (long long)g.P + q] = ez;
-    S[3 * (long long)g.P + q] = hx;
-    S[4 * (long long)g.P + q] = hy;
-    S[5 * (long long)g.P + q] = hz;
+    if (a.part == 0) {
+        const T ex = (a.Ex[I(i, j, k)] + a.Ex[I(i, jp, k)] + a.Ex[I(i, j, kp)] + a.Ex[I(i, jp, kp)]) / T(4.0);
+        const T ey = (a.Ey[I(i, j, k)] + a.Ey[I(ip, j, k)] + a.Ey[I(i, j, kp)] + a.Ey[I(ip, j, kp)]) / T(4.0);
+        const T ez = (a.Ez[I(i, j, k)] + a.Ez[I(ip, j, k)] + a.Ez[I(i, jp, k)] + a.Ez[I(ip, jp, k)]) / T(4.0);
+        S[0 * (long long)g.P + q] = ex;
+        S[1 * (long long)g.P + q] = ey;
+        S[2 * (long long)g.P + q] = ez;
+    } else {
+        const T hx = (a.Hx[I(i, j, k)] + a.Hx[I(ip, j, k)]) / T(2.0);
+        const T hy = (a.Hy[I(i, j, k)] + a.Hy[I(i, jp, k)]) / T(2.0);
+        const T hz = (a.Hz[I(i, j, k)] + a.Hz[I(i, j, kp)]) / T(2.0);
+        S[3 * (long long)g.P + q] = hx;
+        S[4 * (long long)g.P + q] = hy;
+        S[5 * (long long)g.P + q] = hz;
+    }
 }
 
+// One step of the sensors, in two launches. Part 0 (blocks [0, nbp) plane-sum
+// partials, then the gather blocks) reads E only and may run beside the H
+// half-step of the same step; part 1 (the gather blocks, block index offset by
+// nbp) reads H only and may run beside the next E half-step.
 template <typename T>
 __global__ void __launch_bounds__(kPlaneThreads) sensor_step(const __grid_constant__ SensorStepArgs<T> a) {
-    const int b = blockIdx.x;
+    const int b = blockIdx.x + (a.part ? a.nbp : 0);
     if (b < a.nbp) {
         plane_partial(a, b);
         return;
