@@ -162,7 +162,6 @@ struct aefdtd_sim {
     cudaStream_t side_s[2] = {};
     cudaEvent_t ev_s_fork[2] = {}, ev_s_join[2] = {};
     bool concurrent_groups = true;
-    bool serial_now = false;        // timing mode: every launch in order on `stream`
     template <typename Launch> void run_groups(const WorkSplit &w, Launch &&launch);
     size_t dev_bytes = 0;
     uint64_t launches = 0;
@@ -761,7 +760,7 @@ void aefdtd_sim::fill_scalars(int t, int osc_offset, StepScalars &s) const {
 template <typename Launch> void aefdtd_sim::run_groups(const WorkSplit &w, Launch &&launch) {
     int nside = 0;
     for (int g = 1; g < kGroups; g++) nside += w.n[g] > 0;
-    if (!concurrent_groups || serial_now || nside == 0) {
+    if (!concurrent_groups || nside == 0) {
         for (int g = 0; g < kGroups; g++) launch(g, stream);
         return;
     }
@@ -815,9 +814,9 @@ void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
     // Sensor work of step q runs in two parts (sensors.cuh, sensor_step): part 0
     // (plane sums, E samples) reads E only and runs beside H(q); part 1 (H
     // samples) reads H only and runs beside E(q+1). H(q+1) and any DFT flush
-    // wait for part 1. In timing mode everything runs in order on `stream`.
-    serial_now = record;
-    const bool conc = concurrent_groups && !record;
+    // wait for part 1. Timing events sit on `stream` between the joins, so a
+    // phase's time covers the branches that run beside it.
+    const bool conc = concurrent_groups;
     bool h_pending = false;
     // DFT blocks filled in the previous segment accumulate beside this one's
     // steps: they read the other sample-buffer half and only touch acc
@@ -906,7 +905,6 @@ void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
     }
     join_h();
     if (f_pending) AE_CUDA(cudaStreamWaitEvent(stream, ev_f_join, 0));
-    serial_now = false;
     if (normal) {
         launch_plane_reduce(psum_partial.as<double>(), sa.nbp, tbl, psums.as<double>(), L, stream);
         launches++;
@@ -919,7 +917,8 @@ void aefdtd_sim::run_steps(int n) {
     if (graphs_dirty) drop_graphs();
     // capacity of the plane-sum history
     if (normal && tstep + n > psums_cap) {
-        int cap = std::max(tstep + n, std::max(2 * psums_cap, 1024));
+        // sized to the run length Nt (the reference's 12 Grid1(Nt) histories), grown past it
+        int cap = std::max(tstep + n, std::max(2 * psums_cap, std::max(Nt, 1024)));
         DBuf nb;
         nb.alloc(size_t(cap) * 12 * 8, dev_bytes);
         if (psums.p) AE_CUDA(cudaMemcpyAsync(nb.p, psums.p, size_t(psums_cap) * 12 * 8, cudaMemcpyDeviceToDevice, stream));

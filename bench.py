@@ -175,7 +175,10 @@ def run_gpu_arm(args):
             if ws > 1:
                 torch.distributed.barrier()
         launches = sim.launch_count() - launches0
-        ms = sum(a.elapsed_time(b) for a, b in times)
+        per = [a.elapsed_time(b) for a, b in times]
+        ms = sum(per)
+        log(f"[{prec_name}] bench-step ms: min {min(per):.3f} median {statistics.median(per):.3f} "
+            f"max {max(per):.3f}")
         # per-kernel split: the same steps launched one by one with CUDA events
         # around each half-step and the sensor launch (timing pass after the
         # timed region)
@@ -288,6 +291,20 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def profile_run(args):
+    """The bench workload with every kernel launched directly (no CUDA graphs),
+    for ncu launch lists and captures: `--segments` DFT blocks of 64 steps at
+    precision `--profile`. Prints nothing on stdout."""
+    os.environ["AEFDTD_NO_GRAPHS"] = "1"
+    from aether_b200 import _abi as A
+    from aether_b200 import fdtd
+    sim = fdtd.build_simulation(workload(A.FP32 if args.profile == "fp32" else A.FP64))
+    sim.step(STEPS_PER_BENCH_STEP * args.segments)
+    sim.synchronize()
+    log(f"profile run: {args.profile}, {STEPS_PER_BENCH_STEP * args.segments} steps, {sim.launch_count()} launches")
+    sim.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -296,7 +313,12 @@ def main():
     ap.add_argument("--impl", default="aefdtd")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile", choices=["fp32", "fp64"], help="direct-launch run for ncu (no timing)")
+    ap.add_argument("--segments", type=int, default=2)
     args = ap.parse_args()
+    if args.profile:
+        profile_run(args)
+        return
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

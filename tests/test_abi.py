@@ -90,3 +90,75 @@ def test_create_without_gpu_reports_no_device():
     h = C.c_void_p()
     g = A.grid_desc(8, 8, 8, 5e-9)
     assert lib.aefdtd_create(C.byref(g), C.byref(h)) == 6
+
+
+SHIM_SRC = r"""
+#include <cstdio>
+#include <vector>
+#include "aefdtd.hpp"
+int main() {
+    try {
+        // 24 x 20 x 40 structure at 5 nm, CPML 8 on z, vacuum with an n = 1.5 block
+        aefdtd::FDTD f(24, 20, 40, 400, 5e-9, 5e-9, 5e-9, 0.0, "NORMAL", 0, 0, 0, 0, 8, 8, 0, 0, 0, 0, 5, 5);
+        f.set_pml_zm(1.0, 1.0, 0.05);
+        f.set_pml_zp(1.0, 1.0, 0.05);
+        f.set_time_mod(0.5 / 0.99);
+        f.bootstrap();
+        std::vector<uint32_t> map(24 * 20 * 40, 0);
+        for (int k = 15; k < 25; k++)
+            for (int j = 0; j < 20; j++)
+                for (int i = 0; i < 24; i++) map[i + 24 * (j + 20 * k)] = 1;
+        f.set_matsgrid(map);
+        aefdtd_material_desc vac{}, diel{};
+        vac.eps_inf = 1.0;
+        diel.eps_inf = 2.25;
+        f.set_material(0, vac);
+        f.set_material(1, diel);
+        aefdtd_normal_desc nd{};
+        nd.polarization = 1; nd.nl = 11; nd.lambda_min = 400e-9; nd.lambda_max = 1000e-9;
+        f.setup_normal(nd);
+        f.update(60);
+        std::vector<double> ex = f.get_field(0);
+        double s = 0;
+        for (double v : ex) s += v * v;
+        std::printf("ok %d %.17g\n", f.tstep(), s);
+    } catch (const aefdtd::Error &e) {
+        std::printf("error %d %s\n", (int)e.status, e.what());
+    }
+    return 0;
+}
+"""
+
+
+def build_shim_program(d):
+    src = os.path.join(d, "shim.cpp")
+    open(src, "w").write(SHIM_SRC)
+    exe = os.path.join(d, "shim")
+    libdir = os.path.dirname(_lib.LIB_PATH)
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.dirname(HEADER), src, "-o", exe, "-L", libdir,
+                    "-laefdtd", f"-Wl,-rpath,{libdir}"], check=True)
+    return exe
+
+
+def shim_scene():
+    """The structure, materials and excitation the shim program builds."""
+    import numpy as np
+    from aether_b200.scene import Scene
+    g = A.grid_desc(24, 20, 40, 5e-9, mode=A.MODE_NORMAL, precision=A.FP64, nt=400, pml=(0, 0, 0, 0, 8, 8),
+                    pad=(0, 0, 0, 0, 5, 5), time_mod=0.5 / 0.99, alpha=(0, 0, 0, 0, 0.05, 0.05))
+    m = np.zeros((40, 20, 24), np.uint32)
+    m[15:25] = 1
+    return Scene(g, m, [A.material_desc(1.0), A.material_desc(2.25)], 60,
+                 normal=A.NormalDesc(1, 11, 400e-9, 1000e-9), sensors=[], name="shim")
+
+
+def test_cpp_shim_compiles_and_reports_no_device_without_gpu():
+    """The FDTD-named C++ shim builds against the C ABI; without a GPU its
+    first use throws AEFDTD_NO_DEVICE (there is no CPU path)."""
+    import torch
+    with tempfile.TemporaryDirectory() as d:
+        exe = build_shim_program(d)
+        if torch.cuda.is_available():
+            pytest.skip("GPU present: covered by the gpu test")
+        out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout
+        assert out.startswith("error 6"), out

@@ -226,3 +226,20 @@ def test_fp32_tensor_core_dft_many_wavelengths():
     b = fdtd.run(sc32, want_fields=False)
     for fa, fb in zip(a["flux"], b["flux"]):
         assert np.max(np.abs(fb - fa)) <= 2e-3 * np.max(np.abs(fa))
+
+
+def test_cpp_shim_matches_python_path():
+    """The FDTD-named C++ shim (include/aefdtd.hpp) and the ctypes path give
+    the same fields bit for bit (sequential sum of Ex^2 after 60 steps)."""
+    import subprocess
+    import tempfile
+    import test_abi
+    with tempfile.TemporaryDirectory() as d:
+        exe = test_abi.build_shim_program(d)
+        out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()
+    assert out[0] == "ok" and int(out[1]) == 60, out
+    r = fdtd.run(test_abi.shim_scene(), 60)
+    s = 0.0
+    for v in r["fields"][0].ravel():
+        s += float(v) * float(v)
+    assert s == float(out[2]) and s > 0
