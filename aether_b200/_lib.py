@@ -49,6 +49,16 @@ _SIGS = {
     "aefdtd_plane_sums_static": (C.c_int, [_P(C.c_void_p), C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                            _P(C.c_int32), C.c_int32, C.c_double, C.c_void_p, C.c_void_p,
                                            C.c_char_p, C.c_size_t]),
+    "aefdtd_batch_create": (C.c_int, [_P(A.BatchOpts), _P(C.c_void_p)]),
+    "aefdtd_batch_destroy": (C.c_int, [C.c_void_p]),
+    "aefdtd_batch_last_error": (C.c_char_p, [C.c_void_p]),
+    "aefdtd_batch_add": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
+    "aefdtd_batch_remove": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "aefdtd_batch_set_budget": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
+    "aefdtd_batch_autotune": (C.c_int, [C.c_void_p]),
+    "aefdtd_batch_advance": (C.c_int, [C.c_void_p, C.c_int32, _P(C.c_int32)]),
+    "aefdtd_batch_finished": (C.c_int, [C.c_void_p, _P(C.c_void_p), C.c_int32, _P(C.c_int32)]),
+    "aefdtd_batch_get_info": (C.c_int, [C.c_void_p, _P(A.BatchInfo)]),
 }
 
 

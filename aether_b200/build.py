@@ -35,8 +35,9 @@ UNITS = [
     ("voxel.cu", ["--fmad=false"]),
     ("plane_static.cu", []),
     ("runtime.cpp", None),
+    ("batch.cpp", None),
 ]
-HEADERS = ["aefdtd_dev.hpp", "kernels.hpp", "sensors.cuh", "yee.cuh"]
+HEADERS = ["aefdtd_dev.hpp", "kernels.hpp", "sensors.cuh", "yee.cuh", "sim.hpp"]
 
 
 def _stale(obj, deps):

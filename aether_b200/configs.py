@@ -152,7 +152,8 @@ def random_spheres_scene(n_total=(1024, 1024, 512), dx=5 * NM, pml=32, n_dielect
 
 
 def metasurface_cell(rng, dx=5 * NM, nz_total=200, pml=16, nsteps=8000, nl=101,
-                     lmin=400 * NM, lmax=1000 * NM, precision=A.FP32, period_range=(200 * NM, 600 * NM)):
+                     lmin=400 * NM, lmax=1000 * NM, precision=A.FP32, period_range=(200 * NM, 600 * NM),
+                     flux_planes=True):
     """One nanodisk metasurface unit cell: period ~ U(period_range) (square),
     disk radius ~ U(0.15, 0.45) x period, height ~ U(20, 100) nm, gold-like
     model or dielectric n ~ U(1.8, 3.5) by coin flip, on an n=1.45 substrate."""
@@ -174,6 +175,8 @@ def metasurface_cell(rng, dx=5 * NM, nz_total=200, pml=16, nsteps=8000, nl=101,
     g = _normal_grid(n, n, nz_s, dx, pml, precision, nsteps)
     top = min(nz_s - 3, sub_top + h_cells + 10)
     sens = [A.SensorDesc(A.NORMAL_Z, (0, n, 0, n, top, top + 1), nl, lmin, lmax),
-            A.SensorDesc(A.NORMAL_ZM, (0, n, 0, n, sub_top - 8, sub_top - 7), nl, lmin, lmax)]
+            A.SensorDesc(A.NORMAL_ZM, (0, n, 0, n, max(0, sub_top - 8), max(1, sub_top - 7)), nl, lmin, lmax)]
+    if not flux_planes:
+        sens = []   # R/T from the normal-mode plane sums only
     return Scene(g, m, [const_n(1.0), mat, const_n(1.45)], nsteps,
                  normal=A.NormalDesc(1, nl, lmin, lmax), sensors=sens, name="metasurface")

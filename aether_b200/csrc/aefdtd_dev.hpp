@@ -94,6 +94,7 @@ struct WorkSplit {
     int off[kGroups];
     int n[kGroups];
     int unroll;                     // z-planes per iteration of the interior kernels (1 or 2)
+    int tile_y;                     // tile height: CTAs of 32 x tile_y threads (2, 4 or 8)
 };
 
 // ---- sensor-path launch arguments (kernels in sensors.cuh)
@@ -128,6 +129,7 @@ template <typename T> struct SensorStepArgs {
     int ng;
     GatherDesc g[kMaxGather];
     int part;                // 0: plane sums + E gathers (reads E only); 1: H gathers (reads H only)
+    double *out;             // batch: plane-sum history [Nt][12]
 };
 
 struct PhasorArgs {

@@ -1,0 +1,654 @@
+// batch.cpp — batched stepping of many simulations on one GPU.
+//
+// A batch advances its member simulations (typically many small periodic unit
+// cells of uneven sizes) together. Members are created and set up as ordinary
+// simulations; the batch then owns their stepping:
+//
+//  * Size classes. Members are grouped by x-y size (16-cell buckets). Each
+//    class has a tile height (CTAs of 32 x 2, 4 or 8 threads) and a z-block
+//    depth (planes per work item), set by hand or by the autotuner, which
+//    times trial segments of the class's members for every candidate.
+//  * Subsets. Within a class, members are packed into subsets whose device
+//    state fits an L2 budget (126 MB of L2 on B200; the budget is tuned too).
+//    A subset runs a whole segment of steps before the next subset starts, so
+//    after its first step most of its state is served from L2.
+//  * Merged launches. Per step, each work-item group of a subset (interior,
+//    z-CPML, dispersive, general) is ONE launch over the items of all its
+//    members: items carry the member index and the kernels read that member's
+//    arguments from a device array. Boundary groups run on side streams beside
+//    the interior group; the plane sums of all normal-mode members are one
+//    launch beside the H half-step. A full segment (64 steps) of a subset is
+//    captured once per table slot as a CUDA graph and replayed.
+//  * Step budgets. Each member has a number of steps still to run; a segment
+//    never passes a member's budget, so members finish exactly and can be
+//    retired and replaced between segments (continuous batching).
+//
+// Results of a member do not depend on the batch: every member advances with
+// exactly the kernels' arithmetic of a single simulation (FP64 fields are
+// bit-identical to stepping it alone).
+#include "sim.hpp"
+
+
+namespace aefdtd {
+
+struct BatchMember {
+    aefdtd_sim *sim = nullptr;
+    int remaining = 0;   // steps still to run
+    int cls = 0;         // size-class key
+};
+
+struct BatchSubset {
+    int cls = 0;
+    std::vector<int> members;      // indices into aefdtd_batch::members
+    size_t bytes = 0;              // device state of the members
+    long long cells = 0;
+    DBuf items;                    // merged items: E groups, then H groups
+    WorkSplit wsE{}, wsH{};
+    DBuf argsE[2], argsH[2], sargs[2];   // per table slot
+    DBuf blkmap;
+    int nblk = 0;
+    int nplane = 0;                // members with plane sums
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    uint64_t graph_launches = 0;
+    bool built = false;
+    void release(size_t &t) {
+        items.release(t);
+        for (int s = 0; s < 2; s++) {
+            argsE[s].release(t); argsH[s].release(t); sargs[s].release(t);
+            if (graph[s]) { cudaGraphExecDestroy(graph[s]); graph[s] = nullptr; }
+        }
+        blkmap.release(t);
+        built = false;
+    }
+};
+
+struct SizeClass {
+    int tile_y = 4;
+    int kchunk = 0;   // 0: the simulation's own heuristic
+};
+
+}  // namespace aefdtd
+
+using namespace aefdtd;
+
+struct aefdtd_batch {
+    std::string last_error;
+    aefdtd_batch_opts opts{};
+    int device = 0;
+    bool typed = false, fp64 = false;
+    int id_bytes = 1, seg_len = 64;
+    cudaStream_t stream = nullptr, side[kGroups - 1] = {}, side_s = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join[kGroups - 1] = {}, ev_sf = nullptr, ev_sj = nullptr;
+    std::vector<BatchMember> members;
+    std::vector<BatchSubset> subsets;
+    std::map<int, SizeClass> classes;
+    bool layout_dirty = true;
+    long long l2_budget = 96LL << 20;
+    int slot = 0;
+    uint64_t launches = 0;
+    size_t dev_bytes = 0;
+
+    void set_device() const { cudaSetDevice(device); }
+    int class_key(const aefdtd_sim *s) const { return ((s->Nx + 15) / 16) * 1000 + (s->Ny + 15) / 16; }
+    int find(const aefdtd_sim *s) const {
+        for (size_t i = 0; i < members.size(); i++)
+            if (members[i].sim == s) return (int)i;
+        return -1;
+    }
+    void drop_layout() {
+        for (auto &u : subsets) u.release(dev_bytes);
+        subsets.clear();
+        layout_dirty = true;
+    }
+    void layout();
+    template <typename T, typename Tid> void build_subset(BatchSubset &u);
+    template <typename T, typename Tid> void enqueue_segment(BatchSubset &u, int L, int sl);
+    template <typename T, typename Tid> void run_segment(BatchSubset &u, int L);
+    template <typename T, typename Tid> int advance(int max_steps);
+    template <typename T, typename Tid> double time_segments(int reps);
+    template <typename T, typename Tid> void autotune();
+    template <typename Launch> void run_groups(const WorkSplit &w, Launch &&launch);
+    ~aefdtd_batch();
+};
+
+aefdtd_batch::~aefdtd_batch() {
+    set_device();
+    if (stream) cudaStreamSynchronize(stream);
+    for (auto &m : members) m.sim->batch = nullptr;
+    for (auto &u : subsets) u.release(dev_bytes);
+    for (auto &e : ev_join) if (e) cudaEventDestroy(e);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_sf) cudaEventDestroy(ev_sf);
+    if (ev_sj) cudaEventDestroy(ev_sj);
+    for (auto &x : side) if (x) cudaStreamDestroy(x);
+    if (side_s) cudaStreamDestroy(side_s);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+// Subsets: active members grouped by size class, packed in member order up to
+// the L2 budget (a member larger than the budget gets a subset of its own).
+void aefdtd_batch::layout() {
+    drop_layout();
+    std::map<int, std::vector<int>> by_class;
+    for (size_t i = 0; i < members.size(); i++)
+        if (members[i].remaining > 0) by_class[members[i].cls].push_back((int)i);
+    for (auto &kv : by_class) {
+        BatchSubset cur;
+        cur.cls = kv.first;
+        for (int i : kv.second) {
+            const size_t b = members[i].sim->dev_bytes;
+            if (!cur.members.empty() && (l2_budget > 0 && (long long)(cur.bytes + b) > l2_budget)) {
+                subsets.push_back(std::move(cur));
+                cur = BatchSubset();
+                cur.cls = kv.first;
+            }
+            cur.members.push_back(i);
+            cur.bytes += b;
+            const aefdtd_sim *s = members[i].sim;
+            cur.cells += (long long)s->Nx * s->Ny * s->Nz;
+        }
+        if (!cur.members.empty()) subsets.push_back(std::move(cur));
+    }
+    layout_dirty = false;
+}
+
+// Work lists and argument arrays of one subset (both table slots).
+template <typename T, typename Tid> void aefdtd_batch::build_subset(BatchSubset &u) {
+    u.release(dev_bytes);
+    const SizeClass &sc = classes[u.cls];
+    std::vector<int> all;
+    for (int half = 0; half < 2; half++) {
+        WorkSplit &w = half == 0 ? u.wsE : u.wsH;
+        w.unroll = 2;
+        w.tile_y = sc.tile_y;
+        for (int g = 0; g < kGroups; g++) {
+            w.off[g] = (int)(all.size() / 4);
+            for (size_t li = 0; li < u.members.size(); li++) {
+                aefdtd_sim *s = members[u.members[li]].sim;
+                const WorkSplit &mw = half == 0 ? s->wsE : s->wsH;
+                w.unroll = mw.unroll;
+                for (int k = 0; k < mw.n[g]; k++) {
+                    const int *it = &s->items_host[size_t(mw.off[g] + k) * 4];
+                    all.push_back(it[0]);
+                    all.push_back(it[1]);
+                    all.push_back(it[2] | (it[3] << 16));
+                    all.push_back((int)li);
+                }
+            }
+            w.n[g] = (int)(all.size() / 4) - w.off[g];
+        }
+    }
+    u.items.alloc(std::max<size_t>(all.size(), 4) * sizeof(int), dev_bytes);
+    if (!all.empty()) AE_CUDA(cudaMemcpy(u.items.p, all.data(), all.size() * sizeof(int), cudaMemcpyHostToDevice));
+    const size_t n = u.members.size();
+    std::vector<int2> blk;
+    u.nplane = 0;
+    for (int sl = 0; sl < 2; sl++) {
+        std::vector<StepArgs<T, Tid>> ea(n), ha(n);
+        std::vector<SensorStepArgs<T>> sa(n);
+        for (size_t li = 0; li < n; li++) {
+            aefdtd_sim *s = members[u.members[li]].sim;
+            const StepScalars *tbl = s->tables.as<StepScalars>() + size_t(sl) * s->seg_len;
+            s->make_step_args(ea[li], ha[li], tbl);
+            s->make_sensor_args(sa[li], tbl);
+            if (sl == 0 && sa[li].nbp > 0) {
+                u.nplane++;
+                for (int b = 0; b < sa[li].nbp; b++) blk.push_back(make_int2((int)li, b));
+            }
+        }
+        u.argsE[sl].alloc(sizeof(StepArgs<T, Tid>) * n, dev_bytes);
+        u.argsH[sl].alloc(sizeof(StepArgs<T, Tid>) * n, dev_bytes);
+        u.sargs[sl].alloc(sizeof(SensorStepArgs<T>) * n, dev_bytes);
+        AE_CUDA(cudaMemcpy(u.argsE[sl].p, ea.data(), sizeof(StepArgs<T, Tid>) * n, cudaMemcpyHostToDevice));
+        AE_CUDA(cudaMemcpy(u.argsH[sl].p, ha.data(), sizeof(StepArgs<T, Tid>) * n, cudaMemcpyHostToDevice));
+        AE_CUDA(cudaMemcpy(u.sargs[sl].p, sa.data(), sizeof(SensorStepArgs<T>) * n, cudaMemcpyHostToDevice));
+    }
+    u.nblk = (int)blk.size();
+    u.blkmap.alloc(std::max<size_t>(blk.size(), 1) * sizeof(int2), dev_bytes);
+    if (!blk.empty()) AE_CUDA(cudaMemcpy(u.blkmap.p, blk.data(), blk.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    u.built = true;
+}
+
+// Same fork/join scheme as a single simulation's half-step (runtime.cpp, run_groups).
+template <typename Launch> void aefdtd_batch::run_groups(const WorkSplit &w, Launch &&launch) {
+    int nside = 0;
+    for (int g = 1; g < kGroups; g++) nside += w.n[g] > 0;
+    if (nside == 0) {
+        launch(kGroupInterior, stream);
+        return;
+    }
+    AE_CUDA(cudaEventRecord(ev_fork, stream));
+    int si = 0;
+    for (int g = 1; g < kGroups; g++) {
+        if (w.n[g] <= 0) continue;
+        AE_CUDA(cudaStreamWaitEvent(side[si], ev_fork, 0));
+        launch(g, side[si]);
+        AE_CUDA(cudaEventRecord(ev_join[si], side[si]));
+        si++;
+    }
+    launch(kGroupInterior, stream);
+    for (int k = 0; k < si; k++) AE_CUDA(cudaStreamWaitEvent(stream, ev_join[k], 0));
+}
+
+template <typename T, typename Tid> void aefdtd_batch::enqueue_segment(BatchSubset &u, int L, int sl) {
+    const auto *ea = u.argsE[sl].as<StepArgs<T, Tid>>();
+    const auto *ha = u.argsH[sl].as<StepArgs<T, Tid>>();
+    const auto *sa = u.sargs[sl].as<SensorStepArgs<T>>();
+    const int4 *it = u.items.as<int4>();
+    const int2 *blk = u.blkmap.as<int2>();
+    int groups = 0;
+    for (int g = 0; g < kGroups; g++) groups += (u.wsE.n[g] > 0) + (u.wsH.n[g] > 0);
+    for (int q = 0; q < L; q++) {
+        run_groups(u.wsE, [&](int g, cudaStream_t st) { launch_e_group_batch(ea, q, it, u.wsE, g, st); });
+        // plane sums read E only: beside the H half-step
+        if (u.nblk > 0) {
+            AE_CUDA(cudaEventRecord(ev_sf, stream));
+            AE_CUDA(cudaStreamWaitEvent(side_s, ev_sf, 0));
+            launch_plane_partial_batch(sa, blk, u.nblk, q, side_s);
+            AE_CUDA(cudaEventRecord(ev_sj, side_s));
+        }
+        run_groups(u.wsH, [&](int g, cudaStream_t st) { launch_h_group_batch(ha, q, it, u.wsH, g, st); });
+        if (u.nblk > 0) AE_CUDA(cudaStreamWaitEvent(stream, ev_sj, 0));
+        launches += groups + (u.nblk > 0);
+    }
+    if (u.nplane > 0) {
+        launch_plane_reduce_batch(sa, (int)u.members.size(), L, stream);
+        launches++;
+    }
+}
+
+// One segment of L steps of a subset: per-member scalar tables, then the
+// captured graph (full segments) or direct launches; then the members' clocks.
+template <typename T, typename Tid> void aefdtd_batch::run_segment(BatchSubset &u, int L) {
+    if (!u.built) build_subset<T, Tid>(u);
+    const int sl = slot;
+    std::vector<StepScalars> host(seg_len);
+    for (int i : u.members) {
+        aefdtd_sim *s = members[i].sim;
+        for (int q = 0; q < L; q++) s->fill_scalars(s->tstep + q, q, host[q]);
+        AE_CUDA(cudaMemcpyAsync(s->tables.as<StepScalars>() + size_t(sl) * s->seg_len, host.data(),
+                                sizeof(StepScalars) * L, cudaMemcpyHostToDevice, stream));
+    }
+    if (L == seg_len && opts.use_graphs >= 0) {
+        if (!u.graph[sl]) {
+            const uint64_t l0 = launches;
+            AE_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            enqueue_segment<T, Tid>(u, L, sl);
+            cudaGraph_t gr = nullptr;
+            AE_CUDA(cudaStreamEndCapture(stream, &gr));
+            AE_CUDA(cudaGraphInstantiate(&u.graph[sl], gr, 0));
+            cudaGraphDestroy(gr);
+            u.graph_launches = launches - l0;
+            launches = l0;
+        }
+        AE_CUDA(cudaGraphLaunch(u.graph[sl], stream));
+        launches += u.graph_launches;
+    } else {
+        enqueue_segment<T, Tid>(u, L, sl);
+    }
+    for (int i : u.members) {
+        aefdtd_sim *s = members[i].sim;
+        s->tstep += L;
+        for (auto &o : s->oscs) o.step += L;
+        members[i].remaining -= L;
+    }
+}
+
+// Runs segments until max_steps steps have passed or no member is active;
+// stops after the segment in which a member finishes. Returns the steps run.
+template <typename T, typename Tid> int aefdtd_batch::advance(int max_steps) {
+    int done = 0;
+    while (done < max_steps) {
+        int L = std::min(seg_len, max_steps - done);
+        bool any = false;
+        for (auto &m : members)
+            if (m.remaining > 0) { L = std::min(L, m.remaining); any = true; }
+        if (!any) break;
+        if (layout_dirty) layout();
+        for (auto &m : members) {
+            if (m.remaining <= 0) continue;
+            aefdtd_sim *s = m.sim;
+            // plane-sum history for the whole budget, so captured graphs keep valid pointers
+            if (s->normal && s->tstep + m.remaining > s->psums_cap) {
+                DBuf nb;
+                const int cap = s->tstep + m.remaining;
+                nb.alloc(size_t(cap) * 12 * 8, s->dev_bytes);
+                if (s->psums.p)
+                    AE_CUDA(cudaMemcpy(nb.p, s->psums.p, size_t(s->psums_cap) * 12 * 8, cudaMemcpyDeviceToDevice));
+                s->psums.release(s->dev_bytes);
+                s->psums = nb;
+                s->psums_cap = cap;
+                s->graphs_dirty = true;
+                for (auto &u : subsets) u.release(dev_bytes);
+            }
+        }
+        for (auto &u : subsets) run_segment<T, Tid>(u, L);
+        slot ^= 1;
+        done += L;
+        bool finished = false;   // a member of the current layout reached its budget
+        for (auto &u : subsets)
+            for (int i : u.members) finished |= members[i].remaining == 0;
+        if (finished) {
+            // members that reached their budget leave the layout
+            layout_dirty = true;
+            break;
+        }
+    }
+    AE_CUDA(cudaStreamSynchronize(stream));
+    AE_CUDA(cudaGetLastError());
+    return done;
+}
+
+// Device seconds of `reps` full segments of every subset, after one warm-up
+// segment (which also captures the graphs of its slot; the timed segments use
+// the same slot).
+template <typename T, typename Tid> double aefdtd_batch::time_segments(int reps) {
+    if (layout_dirty) layout();
+    for (auto &u : subsets) run_segment<T, Tid>(u, seg_len);   // capture + warm
+    cudaEvent_t a, b;
+    AE_CUDA(cudaEventCreate(&a));
+    AE_CUDA(cudaEventCreate(&b));
+    AE_CUDA(cudaEventRecord(a, stream));
+    for (int r = 0; r < reps; r++)
+        for (auto &u : subsets) run_segment<T, Tid>(u, seg_len);
+    AE_CUDA(cudaEventRecord(b, stream));
+    AE_CUDA(cudaEventSynchronize(b));
+    float ms = 0;
+    AE_CUDA(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return ms * 1e-3;
+}
+
+// Per size class: tile height in {2, 4, 8} x z-block depth in {4, 8}, timed
+// on that class's members alone; then the L2 budget in {48 MiB, 96 MiB, no
+// limit} over all members. Members must be at step 0; they are reset to step
+// 0 afterwards.
+template <typename T, typename Tid> void aefdtd_batch::autotune() {
+    std::vector<int> saved(members.size());
+    for (size_t i = 0; i < members.size(); i++) {
+        if (members[i].sim->tstep != 0) fail(AEFDTD_NOT_READY, "autotune needs every member at step 0");
+        saved[i] = members[i].remaining;
+    }
+    const long long budget0 = l2_budget;
+    // every trial restarts the members at step 0 and runs two segments: the
+    // plane-sum history must hold them (three, with margin)
+    for (auto &m : members) {
+        aefdtd_sim *s = m.sim;
+        if (s->normal && s->psums_cap < 3 * seg_len) {
+            s->psums.release(s->dev_bytes);
+            s->psums.alloc(size_t(3 * seg_len) * 12 * 8, s->dev_bytes);
+            s->psums_cap = 3 * seg_len;
+            s->graphs_dirty = true;
+        }
+    }
+    auto restart = [&] {
+        AE_CUDA(cudaStreamSynchronize(stream));
+        for (auto &m : members) m.sim->zero_state();
+    };
+    auto apply = [&](int cls, const SizeClass &c) {
+        classes[cls] = c;
+        for (auto &m : members)
+            if (m.cls == cls) {
+                m.sim->tile_y = c.tile_y;
+                m.sim->kchunk_override = c.kchunk;
+                m.sim->work_dirty = true;
+                m.sim->build_work();
+            }
+    };
+    std::vector<int> keys;
+    for (auto &kv : classes) keys.push_back(kv.first);
+    for (int cls : keys) {
+        // only this class's members take part in its trials
+        for (size_t i = 0; i < members.size(); i++) members[i].remaining = members[i].cls == cls ? (1 << 30) : 0;
+        double best = 1e30;
+        SizeClass pick = classes[cls];
+        for (int ty : {2, 4, 8})
+            for (int kc : {4, 8}) {
+                SizeClass c{ty, kc};
+                apply(cls, c);
+                drop_layout();
+                restart();
+                const double t = time_segments<T, Tid>(1);
+                if (t < best) { best = t; pick = c; }
+            }
+        apply(cls, pick);
+    }
+    // L2 budget over all members
+    for (size_t i = 0; i < members.size(); i++) members[i].remaining = 1 << 30;
+    double best = 1e30;
+    long long pick = budget0;
+    for (long long b : {48LL << 20, 96LL << 20, -1LL}) {
+        l2_budget = b;
+        drop_layout();
+        restart();
+        const double t = time_segments<T, Tid>(1);
+        if (t < best) { best = t; pick = b; }
+    }
+    l2_budget = pick;
+    drop_layout();
+    restart();
+    for (size_t i = 0; i < members.size(); i++) members[i].remaining = saved[i];
+}
+
+// ------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------
+
+namespace aefdtd {
+void batch_detach(void *bp, aefdtd_sim *s) {
+    auto *b = static_cast<aefdtd_batch *>(bp);
+    const int i = b->find(s);
+    if (i < 0) return;
+    b->set_device();
+    cudaStreamSynchronize(b->stream);
+    b->members.erase(b->members.begin() + i);
+    b->drop_layout();
+    s->batch = nullptr;
+}
+}  // namespace aefdtd
+
+template <typename F> static aefdtd_status bguarded(aefdtd_batch *b, F &&f) {
+    try {
+        f();
+        if (b) b->last_error.clear();
+        return AEFDTD_OK;
+    } catch (Error &e) {
+        if (b) b->last_error = e.msg;
+        return e.st;
+    } catch (std::bad_alloc &) {
+        if (b) b->last_error = "host allocation failed";
+        return AEFDTD_OOM;
+    } catch (std::exception &e) {
+        if (b) b->last_error = e.what();
+        return AEFDTD_BAD_ARG;
+    }
+}
+
+#define AEFDTD_BATCH_DISPATCH(b, fn)                                        \
+    do {                                                                    \
+        if ((b)->fp64) {                                                    \
+            if ((b)->id_bytes == 1) fn(double, uint8_t); else fn(double, uint16_t); \
+        } else {                                                            \
+            if ((b)->id_bytes == 1) fn(float, uint8_t); else fn(float, uint16_t);   \
+        }                                                                   \
+    } while (0)
+
+extern "C" {
+
+aefdtd_status aefdtd_batch_create(const aefdtd_batch_opts *opts, aefdtd_batch **out) {
+    if (!out) return AEFDTD_BAD_ARG;
+    *out = nullptr;
+    auto *b = new aefdtd_batch();
+    aefdtd_status st = bguarded(b, [&] {
+        if (opts) {
+            if (opts->abi_version != AEFDTD_ABI_VERSION) fail(AEFDTD_BAD_ARG, "abi_version mismatch");
+            b->opts = *opts;
+        } else {
+            b->opts.abi_version = AEFDTD_ABI_VERSION;
+        }
+        if (b->opts.l2_budget_bytes != 0) b->l2_budget = b->opts.l2_budget_bytes;
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) fail(AEFDTD_NO_DEVICE, "no CUDA device visible");
+        b->device = b->opts.device;
+        if (b->device < 0 || b->device >= ndev) fail(AEFDTD_BAD_ARG, "device ordinal out of range");
+        AE_CUDA(cudaSetDevice(b->device));
+        AE_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+        for (auto &x : b->side) AE_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+        AE_CUDA(cudaStreamCreateWithFlags(&b->side_s, cudaStreamNonBlocking));
+        AE_CUDA(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+        for (auto &e : b->ev_join) AE_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        AE_CUDA(cudaEventCreateWithFlags(&b->ev_sf, cudaEventDisableTiming));
+        AE_CUDA(cudaEventCreateWithFlags(&b->ev_sj, cudaEventDisableTiming));
+    });
+    if (st != AEFDTD_OK) {
+        delete b;
+        return st;
+    }
+    *out = b;
+    return AEFDTD_OK;
+}
+
+aefdtd_status aefdtd_batch_destroy(aefdtd_batch *b) {
+    if (!b) return AEFDTD_BAD_ARG;
+    delete b;
+    return AEFDTD_OK;
+}
+
+const char *aefdtd_batch_last_error(const aefdtd_batch *b) { return b ? b->last_error.c_str() : ""; }
+
+aefdtd_status aefdtd_batch_add(aefdtd_batch *b, aefdtd_sim *s, int32_t steps) {
+    if (!b || !s) return AEFDTD_BAD_ARG;
+    return bguarded(b, [&] {
+        if (steps < 0) fail(AEFDTD_BAD_ARG, "negative step budget");
+        if (s->batch) fail(AEFDTD_BAD_ARG, "the simulation is already in a batch");
+        if (s->device != b->device) fail(AEFDTD_BAD_ARG, "the simulation is on another device");
+        if (!s->map_set) fail(AEFDTD_NOT_READY, "no material map");
+        if (s->g.mode == AEFDTD_MODE_NORMAL && !s->normal) fail(AEFDTD_NOT_READY, "normal mode needs aefdtd_setup_normal");
+        if (!s->sensors.empty()) fail(AEFDTD_BAD_ARG, "batch members carry no planar DFT sensors (normal-mode plane sums only)");
+        if (s->Nz >= 32768) fail(AEFDTD_BAD_ARG, "batch members need Nz < 32768 (k1 << 16 in an int32 item)");
+        s->set_device();
+        s->finalize_tables();
+        if (s->work_dirty) s->build_work();
+        if (!b->typed) {
+            b->typed = true;
+            b->fp64 = s->fp64;
+            b->id_bytes = s->id_bytes;
+            b->seg_len = s->seg_len;
+        } else if (s->fp64 != b->fp64 || s->id_bytes != b->id_bytes || s->seg_len != b->seg_len) {
+            fail(AEFDTD_BAD_ARG, "batch members share precision, material-id width and DFT block");
+        }
+        AE_CUDA(cudaStreamSynchronize(s->stream));
+        BatchMember m;
+        m.sim = s;
+        m.remaining = steps;
+        m.cls = b->class_key(s);
+        auto it = b->classes.find(m.cls);
+        if (it == b->classes.end()) {
+            SizeClass c;
+            c.tile_y = b->opts.tile_y == 2 || b->opts.tile_y == 8 ? b->opts.tile_y : 4;
+            c.kchunk = b->opts.kchunk;
+            b->classes[m.cls] = c;
+            it = b->classes.find(m.cls);
+        }
+        if (s->tile_y != it->second.tile_y || s->kchunk_override != it->second.kchunk) {
+            s->tile_y = it->second.tile_y;
+            s->kchunk_override = it->second.kchunk;
+            s->work_dirty = true;
+            s->build_work();
+        }
+        s->batch = b;
+        b->members.push_back(m);
+        b->layout_dirty = true;
+    });
+}
+
+aefdtd_status aefdtd_batch_remove(aefdtd_batch *b, aefdtd_sim *s) {
+    if (!b || !s) return AEFDTD_BAD_ARG;
+    return bguarded(b, [&] {
+        if (b->find(s) < 0) fail(AEFDTD_BAD_ARG, "not a member of this batch");
+        batch_detach(b, s);
+    });
+}
+
+aefdtd_status aefdtd_batch_set_budget(aefdtd_batch *b, aefdtd_sim *s, int32_t steps) {
+    if (!b || !s) return AEFDTD_BAD_ARG;
+    return bguarded(b, [&] {
+        const int i = b->find(s);
+        if (i < 0) fail(AEFDTD_BAD_ARG, "not a member of this batch");
+        if (steps < 0) fail(AEFDTD_BAD_ARG, "negative step budget");
+        b->members[i].remaining = steps;
+        b->layout_dirty = true;
+    });
+}
+
+aefdtd_status aefdtd_batch_autotune(aefdtd_batch *b) {
+    if (!b) return AEFDTD_BAD_ARG;
+    return bguarded(b, [&] {
+        if (b->members.empty()) fail(AEFDTD_NOT_READY, "empty batch");
+        b->set_device();
+#define AEFDTD_AT(T, Tid) b->autotune<T, Tid>()
+        AEFDTD_BATCH_DISPATCH(b, AEFDTD_AT);
+#undef AEFDTD_AT
+    });
+}
+
+aefdtd_status aefdtd_batch_advance(aefdtd_batch *b, int32_t max_steps, int32_t *steps_done) {
+    if (!b) return AEFDTD_BAD_ARG;
+    return bguarded(b, [&] {
+        if (max_steps < 0) fail(AEFDTD_BAD_ARG, "negative step count");
+        b->set_device();
+        int done = 0;
+        if (!b->members.empty()) {
+#define AEFDTD_ADV(T, Tid) done = b->advance<T, Tid>(max_steps)
+            AEFDTD_BATCH_DISPATCH(b, AEFDTD_ADV);
+#undef AEFDTD_ADV
+        }
+        if (steps_done) *steps_done = done;
+    });
+}
+
+aefdtd_status aefdtd_batch_finished(aefdtd_batch *b, aefdtd_sim **out, int32_t cap, int32_t *n) {
+    if (!b || !n) return AEFDTD_BAD_ARG;
+    return bguarded(b, [&] {
+        int k = 0;
+        for (auto &m : b->members)
+            if (m.remaining == 0) {
+                if (out && k < cap) out[k] = m.sim;
+                k++;
+            }
+        *n = k;
+    });
+}
+
+aefdtd_status aefdtd_batch_get_info(aefdtd_batch *b, aefdtd_batch_info *info) {
+    if (!b || !info) return AEFDTD_BAD_ARG;
+    return bguarded(b, [&] {
+        if (b->layout_dirty && b->typed) b->layout();
+        std::memset(info, 0, sizeof(*info));
+        info->n_members = (int32_t)b->members.size();
+        for (auto &m : b->members) {
+            if (m.remaining > 0) {
+                info->n_active++;
+                info->cells += (int64_t)m.sim->Nx * m.sim->Ny * m.sim->Nz;
+            }
+            info->member_bytes += (int64_t)m.sim->dev_bytes;
+        }
+        info->n_subsets = (int32_t)b->subsets.size();
+        info->l2_budget_bytes = b->l2_budget;
+        info->launches = b->launches;
+        info->batch_bytes = (int64_t)b->dev_bytes;
+        int c = 0;
+        for (auto &kv : b->classes) {
+            if (c < AEFDTD_BATCH_MAX_CLASSES) {
+                info->class_key[c] = kv.first;
+                info->class_tile_y[c] = kv.second.tile_y;
+                info->class_kchunk[c] = kv.second.kchunk;
+            }
+            c++;
+        }
+        info->n_classes = c;
+    });
+}
+
+}  // extern "C"

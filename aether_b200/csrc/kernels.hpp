@@ -11,12 +11,17 @@
 namespace aefdtd {
 
 // yee_f64.cu (compiled with --fmad=false) and yee_f32.cu: group g of an E or
-// H half-step's WorkSplit, one 32 x 4 CTA per item (nothing when empty).
+// H half-step's WorkSplit, one 32 x tile_y CTA per item (nothing when empty);
+// the batch forms take a device array of per-instance arguments.
 #define AEFDTD_DECL_YEE(T, Tid)                                                                          \
     void launch_e_group(const StepArgs<T, Tid> &a, const int4 *items, const WorkSplit &w, int g,        \
                         cudaStream_t s);                                                                  \
     void launch_h_group(const StepArgs<T, Tid> &a, const int4 *items, const WorkSplit &w, int g,        \
-                        cudaStream_t s);
+                        cudaStream_t s);                                                                  \
+    void launch_e_group_batch(const StepArgs<T, Tid> *args, int q, const int4 *items, const WorkSplit &w, \
+                              int g, cudaStream_t s);                                                     \
+    void launch_h_group_batch(const StepArgs<T, Tid> *args, int q, const int4 *items, const WorkSplit &w, \
+                              int g, cudaStream_t s);
 AEFDTD_DECL_YEE(double, uint8_t)
 AEFDTD_DECL_YEE(double, uint16_t)
 AEFDTD_DECL_YEE(float, uint8_t)
@@ -29,6 +34,12 @@ int launch_sensor_step(const SensorStepArgs<double> &a, cudaStream_t s);
 int launch_sensor_step(const SensorStepArgs<float> &a, cudaStream_t s);
 void launch_plane_reduce(const double *partial, int nbp, const StepScalars *sc, double *out, int steps,
                          cudaStream_t s);
+// batch members: plane-sum partials of step q (blk: block -> (instance, block)),
+// and the reduction of `steps` steps of every instance into its history
+void launch_plane_partial_batch(const SensorStepArgs<double> *args, const int2 *blk, int nblk, int q, cudaStream_t s);
+void launch_plane_partial_batch(const SensorStepArgs<float> *args, const int2 *blk, int nblk, int q, cudaStream_t s);
+void launch_plane_reduce_batch(const SensorStepArgs<double> *args, int n_inst, int steps, cudaStream_t s);
+void launch_plane_reduce_batch(const SensorStepArgs<float> *args, int n_inst, int steps, cudaStream_t s);
 void launch_phasors(const PhasorArgs &a, cudaStream_t s);
 void launch_accumulate(const AccumArgs<double> &a, cudaStream_t s);
 void launch_accumulate(const AccumArgs<float> &a, cudaStream_t s);

@@ -5,293 +5,7 @@
 // issues the fused kernels on the handle's stream in the mode driver's order.
 // There is no CPU compute path: without a CUDA device every call that would
 // touch the device returns AEFDTD_NO_DEVICE.
-#include <algorithm>
-#include <cmath>
-#include <complex>
-#include <cstdio>
-#include <cstdlib>
-#include <cstring>
-#include <numbers>
-#include <string>
-#include <map>
-#include <vector>
-
-#include <cuda_runtime.h>
-
-#include "../../include/aefdtd.h"
-#include "kernels.hpp"
-
-namespace aefdtd {
-constexpr int kTileXHost = 32, kTileYHost = 4;   // kTileX, kTileY of yee.cuh
-}
-
-namespace aefdtd {
-
-cudaError_t launch_voxelize(int nx, int ny, int nz, double dx, double dy, double dz, const aefdtd_structure_op *ops,
-                            int nops, int def, const int per[3], const double l[3], uint32_t *d_out, cudaStream_t s);
-
-namespace phys {
-// src/common/phys_constants.h:18-20
-constexpr double e0 = 8.854187817e-12;
-constexpr double mu0 = 12.566370614e-7;
-constexpr double c_light = 299792458.0;
-constexpr double Pi = std::numbers::pi_v<double>;
-}  // namespace phys
-using namespace phys;
-typedef std::complex<double> cplx;
-
-struct Error {
-    aefdtd_status st;
-    std::string msg;
-};
-
-#define AE_CUDA(call)                                                                        \
-    do {                                                                                     \
-        cudaError_t e__ = (call);                                                            \
-        if (e__ != cudaSuccess)                                                              \
-            throw Error{e__ == cudaErrorMemoryAllocation ? AEFDTD_OOM : AEFDTD_CUDA_ERROR,   \
-                        std::string(#call) + ": " + cudaGetErrorString(e__)};                 \
-    } while (0)
-
-static void fail(aefdtd_status st, const std::string &m) { throw Error{st, m}; }
-
-// Device buffer with byte size bookkeeping.
-struct DBuf {
-    void *p = nullptr;
-    size_t n = 0;
-    void alloc(size_t bytes, size_t &total) {
-        release(total);
-        if (bytes == 0) return;
-        AE_CUDA(cudaMalloc(&p, bytes));
-        n = bytes;
-        total += bytes;
-    }
-    void release(size_t &total) {
-        if (p) { cudaFree(p); total -= n; }
-        p = nullptr;
-        n = 0;
-    }
-    template <typename T> T *as() const { return static_cast<T *>(p); }
-};
-
-// Per-material coefficients (FDTD_Material, fdtd_material.h:38-268).
-struct HostMat {
-    bool set = false, rc = false;
-    int np = 0;
-    double C1 = 1, C2x = 0, C2y = 0, C2z = 0, C3 = 0, C4 = 0, ei = 1, sig = 0;
-    std::vector<cplx> crec, dchi, chi;
-    int x1 = 0, x2 = -1, y1 = 0, y2 = -1, z1 = 0, z2 = -1;   // bounding box in the total grid
-};
-
-struct Pulse {
-    // ChpIn (chpin.cpp:44-90, 479-545) at incidence 0, direction 0.
-    double k, omega, kx, ky, kz, n_ind, dz, C1, Ex0, Ey0, Ez0, Hx0, Hy0, Hz0;
-    void init(double li, double lf, double poli, double startz, double n_ind_i) {
-        double wi = 2.0 * Pi * c_light / li, wf = 2.0 * Pi * c_light / lf;
-        double w0 = (wi + wf) / 2.0;
-        double lambda = 2.0 * Pi * c_light / w0;
-        double dw = std::abs(0.5 * (wi - w0));
-        n_ind = n_ind_i;
-        double inc = 0 * Pi / 180.0, pol = poli * Pi / 180.0, dir = 0 * Pi / 180.0;
-        dz = 2.0 * c_light / dw / n_ind;
-        k = 2.0 * Pi / lambda * n_ind;
-        omega = 2.0 * Pi * c_light / lambda;
-        double incr = Pi / 2.0 - inc;
-        double Ca = std::cos(incr), Sa = std::sin(incr), Cb = std::cos(dir), Sb = std::sin(dir);
-        double Cc = std::cos(pol), Sc = std::sin(pol);
-        kx = k * (Ca * Cb); ky = k * (Ca * Sb); kz = k * (-Sa);
-        Ex0 = (Sa * Cb * Sc - Sb * Cc) * 1.0; Ey0 = (Sa * Sb * Sc + Cb * Cc) * 1.0; Ez0 = Ca * Sc * 1.0;
-        double tmp = 1.0 / (c_light * mu0) * 1.0 * n_ind;
-        Hx0 = tmp * (Sa * Cb * Cc + Sb * Sc); Hy0 = tmp * (Sa * Sb * Cc - Cb * Sc); Hz0 = tmp * (Ca * Cc);
-        C1 = -1.0 / k * (kx * 0 + ky * 0 + kz * startz) + dz * std::sqrt(-std::log(1e-4));
-    }
-    double f(double A0, double x, double y, double z, double t) const {
-        double p = kx * x + ky * y + kz * z;
-        double a = p - omega * t;
-        double b = (1.0 / k * p - c_light * t / n_ind + C1) / dz;
-        return A0 * std::exp(-b * b) * std::cos(a);
-    }
-};
-
-struct Osc {
-    int comp, box[6], step = 0, tshift;
-    double w0, dw;
-};
-
-struct PlaneSensor {
-    aefdtd_sensor_desc d;
-    int type, x1, x2, y1, y2, z1, z2, span1, span2, P, nl;
-    std::vector<double> lambda, w;
-    int step = 0;          // steps fed
-    int nbuf = 0;          // filled slots of the sample buffer half being written
-    int buf_step0 = 0;     // step of slot 0
-    int half = 0;          // sample-buffer half the gathers write (S holds two halves of K steps)
-    // a filled half whose DFT block is still to be accumulated: launched at the
-    // start of the next segment beside its steps, or when results are read
-    bool pending = false;
-    int pend_half = 0, pend_n = 0, pend_step0 = 0;
-    const StepScalars *pend_tbl = nullptr;   // step of slot 0 read from this table, else pend_step0
-    DBuf S, acc, wdev, WE, WH, flux;
-    DBuf Btc;              // tensor-core phasor image (FP32 path)
-    int N0 = 0, N1 = 0;
-};
-
-static inline double s_curve(double x, double xmin, double xmax) {
-    // src/common/mathUT.cpp:1186-1193
-    double u = (x - xmin) / (xmax - xmin);
-    if (u <= 0) return 0;
-    else if (u >= 1.0) return 1.0;
-    else return u * u * (3.0 - 2.0 * u);
-}
-
-}  // namespace aefdtd
-
-using namespace aefdtd;
-
-struct aefdtd_sim {
-    aefdtd_grid_desc g{};
-    std::string last_error;
-    bool fp64 = true;
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    // side streams for the boundary groups of a half-step, forked from and
-    // joined back into `stream` by events (parallel branches in the graphs)
-    cudaStream_t side[kGroups - 1] = {};
-    cudaEvent_t ev_fork = nullptr, ev_join[kGroups - 1] = {};
-    // side streams of the two sensor parts (part 0 beside H, part 1 beside the next E)
-    cudaStream_t side_s[2] = {};
-    cudaEvent_t ev_s_fork[2] = {}, ev_s_join[2] = {};
-    bool concurrent_groups = true;
-    template <typename Launch> void run_groups(const WorkSplit &w, Launch &&launch);
-    size_t dev_bytes = 0;
-    uint64_t launches = 0;
-
-    // geometry (FDTD members)
-    int Nx = 0, Ny = 0, Nz = 0, Nx_s = 0, Ny_s = 0, Nz_s = 0;
-    int xs_s = 0, xs_e = 0, ys_s = 0, ys_e = 0, zs_s = 0, zs_e = 0;
-    int pml[6] = {0}, pad[6] = {0};
-    double Dx = 0, Dy = 0, Dz = 0, Dt = 0, dtm = 0, dtdez = 0, dtdmx = 0, dtdmy = 0, dtdmz = 0;
-    double pml_kappa[6], pml_sigma[6], pml_alpha[6];
-    double pml_m = 4, pml_ma = 2;
-    int Nt = 0, Ntap = 0, dft_k = 64;
-    int tstep = 0;
-
-    // fields and state
-    DBuf F[6], mat;
-    int id_bytes = 1;
-    int mpitch = 0;
-    std::vector<uint32_t> map;      // total-grid material ids
-    bool map_set = false;
-    unsigned Nmat = 1;
-    std::vector<HostMat> mats;
-    bool tables_dirty = true;
-    DBuf coef, disp, crec, dchi, psi;
-    bool any_disp = false;
-    // CPML
-    DBuf ik[6], bE[3], cE[3], bH[3], cH[3];
-    DBuf psiE[6], psiH[6];          // x0,x1,y0,y1,z0,z1
-    // normal mode
-    bool normal = false;
-    aefdtd_normal_desc nd{};
-    Pulse pulse{};
-    double eps_sup = 1, eps_sub = 1, index_sup = 1, index_sub = 1;
-    DBuf psums, psum_partial;
-    int psums_cap = 0;
-    std::vector<double> psums_host;
-    // custom mode
-    std::vector<Osc> oscs;
-    std::vector<PlaneSensor *> sensors;
-    // half-step work lists: (x0, y0, k0, k1) items of 32 x 4 columns x a
-    // z-chunk, in one device array: the E groups, then the H groups
-    bool work_dirty = true;
-    int kchunk = 0;
-    WorkSplit wsE{}, wsH{};
-    DBuf items;
-    void build_work();
-    DBuf err;
-    void check_err();
-    // timing: one event quadruple per step of the last aefdtd_step call
-    // (before E, after E, after H, after sensors), summed on query
-    bool timing = false;
-    std::vector<cudaEvent_t> tev;
-    int tev_steps = 0;
-    double t_e = 0, t_h = 0, t_s = 0;
-
-    ~aefdtd_sim();
-    void construct(const aefdtd_grid_desc *d);
-    void set_device() const { cudaSetDevice(device); }
-    void build_pml_tables();
-    void set_map(const uint32_t *m, size_t count);
-    void set_material(uint32_t idx, const aefdtd_material_desc *md);
-    void finalize_tables();
-    template <typename T, typename Tid> void fill_args(StepArgs<T, Tid> &a, bool e_side);
-    template <typename T, typename Tid> void run_steps(int n);
-    template <typename T>
-    void flush_block(PlaneSensor &s, int half, int n, const StepScalars *step0_ptr, int step0, cudaStream_t st);
-    template <typename T> void launch_pending(PlaneSensor &s, cudaStream_t st);
-    void drain_sensors();
-    cudaStream_t side_f = nullptr;
-    cudaEvent_t ev_f_fork = nullptr, ev_f_join = nullptr;
-    template <typename T, typename Tid> void enqueue_segment(int L, StepScalars *tbl, bool record);
-    void fill_scalars(int t, int osc_offset, StepScalars &s) const;
-    void drop_graphs();
-    void accumulate_timing(int L);
-    int plane_blocks() const {
-        const int n = Nx * Ny;
-        return n >= kPlaneBlocks * kPlaneThreads ? kPlaneBlocks : (n + kPlaneThreads - 1) / kPlaneThreads;
-    }
-    // step segments: device tables of per-step scalars (two slots) and the
-    // CUDA graphs of full segments, one per slot
-    int seg_len = 64;
-    int seg_slot = 0;
-    DBuf tables;
-    bool use_graphs = true;
-    bool graphs_dirty = true;
-    // captured segments, keyed by table slot, pending-flush state and the
-    // sensors' buffer halves (the pointers a segment's launches bake in)
-    std::map<uint64_t, cudaGraphExec_t> graph_exec;
-    uint64_t graph_launches = 0;
-    void step(int n);
-    void zero_state();
-    int kchunk_override = 0;
-    int zunroll = 2;
-};
-
-aefdtd_sim::~aefdtd_sim() {
-    set_device();
-    if (stream) cudaStreamSynchronize(stream);
-    size_t t = 0;
-    for (auto &b : F) b.release(t);
-    mat.release(t); coef.release(t); disp.release(t); crec.release(t); dchi.release(t); psi.release(t);
-    for (auto &b : ik) b.release(t);
-    for (int a = 0; a < 3; a++) { bE[a].release(t); cE[a].release(t); bH[a].release(t); cH[a].release(t); }
-    for (auto &b : psiE) b.release(t);
-    for (auto &b : psiH) b.release(t);
-    psums.release(t);
-    psum_partial.release(t);
-    err.release(t);
-    tables.release(t);
-    for (auto &gx : graph_exec) if (gx.second) cudaGraphExecDestroy(gx.second);
-    items.release(t);
-    for (auto *s : sensors) {
-        s->S.release(t); s->acc.release(t); s->wdev.release(t); s->WE.release(t); s->WH.release(t); s->flux.release(t);
-        s->Btc.release(t);
-        delete s;
-    }
-    for (auto &e : tev) if (e) cudaEventDestroy(e);
-    for (auto &e : ev_join) if (e) cudaEventDestroy(e);
-    if (ev_fork) cudaEventDestroy(ev_fork);
-    for (auto &x : side) if (x) cudaStreamDestroy(x);
-    for (int k = 0; k < 2; k++) {
-        if (ev_s_fork[k]) cudaEventDestroy(ev_s_fork[k]);
-        if (ev_s_join[k]) cudaEventDestroy(ev_s_join[k]);
-        if (side_s[k]) cudaStreamDestroy(side_s[k]);
-    }
-    if (ev_f_fork) cudaEventDestroy(ev_f_fork);
-    if (ev_f_join) cudaEventDestroy(ev_f_join);
-    if (side_f) cudaStreamDestroy(side_f);
-    if (stream) cudaStreamDestroy(stream);
-}
+#include "sim.hpp"
 
 // FDTD::FDTD (fdtd_core.cpp:158-285) for modes NORM and CUSTOM, with the
 // normal-incidence driver's own argument choice (normal_incidence.cpp:188-200).
@@ -387,6 +101,10 @@ void aefdtd_sim::construct(const aefdtd_grid_desc *d) {
     mats.assign(1, HostMat());
     if (const char *kc = std::getenv("AEFDTD_KCHUNK")) kchunk_override = std::max(0, atoi(kc));
     if (const char *zu = std::getenv("AEFDTD_ZUNROLL")) zunroll = atoi(zu) >= 2 ? 2 : 1;
+    if (const char *ty = std::getenv("AEFDTD_TILE_Y")) {
+        const int v = atoi(ty);
+        tile_y = (v == 2 || v == 8) ? v : 4;
+    }
     AE_CUDA(cudaStreamSynchronize(stream));
 }
 
@@ -777,14 +495,10 @@ template <typename Launch> void aefdtd_sim::run_groups(const WorkSplit &w, Launc
     for (int k = 0; k < si; k++) AE_CUDA(cudaStreamWaitEvent(stream, ev_join[k], 0));
 }
 
-// Enqueues the kernels of L consecutive steps on the stream: for each step
-// the E half-step (interior + boundary items), the H half-step, and the fused
-// sensor launch; then the plane-sum reduction of the L steps and, when a DFT
-// buffer fills, its accumulation. `tbl` is the device table of the L steps'
-// scalars. With record = true per-step timing events are recorded.
+// Arguments of the E and H half-step kernels for steps whose scalars are in
+// the table `tbl` (shared by single-simulation segments and batches).
 template <typename T, typename Tid>
-void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
-    StepArgs<T, Tid> ea, ha;
+void aefdtd_sim::make_step_args(StepArgs<T, Tid> &ea, StepArgs<T, Tid> &ha, const StepScalars *tbl) {
     fill_args(ea, true);
     fill_args(ha, false);
     ea.kchunk = ha.kchunk = kchunk;
@@ -796,10 +510,11 @@ void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
         ea.src_comp[s] = oscs[s].comp;
         ea.nsrc++;
     }
-    const int4 *wi = items.as<int4>();
-    int groups = 0;
-    for (int g = 0; g < kGroups; g++) groups += (wsE.n[g] > 0) + (wsH.n[g] > 0);
-    SensorStepArgs<T> sa{};
+}
+
+// Sensor-launch arguments without gathers: fields, plane-sum geometry and pulse.
+template <typename T> void aefdtd_sim::make_sensor_args(SensorStepArgs<T> &sa, const StepScalars *tbl) {
+    sa = SensorStepArgs<T>{};
     sa.Nx = Nx; sa.Ny = Ny; sa.Nz = Nz; sa.NxNy = (long long)Nx * Ny;
     sa.Ex = F[0].as<T>(); sa.Ey = F[1].as<T>(); sa.Ez = F[2].as<T>();
     sa.Hx = F[3].as<T>(); sa.Hy = F[4].as<T>(); sa.Hz = F[5].as<T>();
@@ -810,7 +525,36 @@ void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
         sa.Dx = Dx; sa.Dy = Dy; sa.Dz = Dz;
         sa.P = PulseDev{pulse.k, pulse.omega, pulse.kx, pulse.ky, pulse.kz, pulse.n_ind, pulse.dz, pulse.C1,
                         pulse.Ex0, pulse.Ey0, pulse.Ez0};
+        sa.partial = psum_partial.as<double>();
+        sa.out = psums.as<double>();
     }
+}
+
+template void aefdtd_sim::make_step_args<double, uint8_t>(StepArgs<double, uint8_t> &, StepArgs<double, uint8_t> &,
+                                                           const StepScalars *);
+template void aefdtd_sim::make_step_args<double, uint16_t>(StepArgs<double, uint16_t> &, StepArgs<double, uint16_t> &,
+                                                            const StepScalars *);
+template void aefdtd_sim::make_step_args<float, uint8_t>(StepArgs<float, uint8_t> &, StepArgs<float, uint8_t> &,
+                                                          const StepScalars *);
+template void aefdtd_sim::make_step_args<float, uint16_t>(StepArgs<float, uint16_t> &, StepArgs<float, uint16_t> &,
+                                                           const StepScalars *);
+template void aefdtd_sim::make_sensor_args<double>(SensorStepArgs<double> &, const StepScalars *);
+template void aefdtd_sim::make_sensor_args<float>(SensorStepArgs<float> &, const StepScalars *);
+
+// Enqueues the kernels of L consecutive steps on the stream: for each step
+// the E half-step (interior + boundary items), the H half-step, and the fused
+// sensor launch; then the plane-sum reduction of the L steps and, when a DFT
+// buffer fills, its accumulation. `tbl` is the device table of the L steps'
+// scalars. With record = true per-step timing events are recorded.
+template <typename T, typename Tid>
+void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
+    StepArgs<T, Tid> ea, ha;
+    make_step_args(ea, ha, tbl);
+    const int4 *wi = items.as<int4>();
+    int groups = 0;
+    for (int g = 0; g < kGroups; g++) groups += (wsE.n[g] > 0) + (wsH.n[g] > 0);
+    SensorStepArgs<T> sa;
+    make_sensor_args(sa, tbl);
     // Sensor work of step q runs in two parts (sensors.cuh, sensor_step): part 0
     // (plane sums, E samples) reads E only and runs beside H(q); part 1 (H
     // samples) reads H only and runs beside E(q+1). H(q+1) and any DFT flush
@@ -1044,7 +788,7 @@ void aefdtd_sim::accumulate_timing(int L) {
 // an oscillator box, or of a dispersive material; all others are "interior"
 // and run the curl-only kernels.
 void aefdtd_sim::build_work() {
-    const int tx = kTileXHost, ty = kTileYHost;
+    const int tx = kTileXHost, ty = tile_y;
     const int ntx = (Nx + tx - 1) / tx, nty = (Ny + ty - 1) / ty;
     const long long tiles = (long long)ntx * nty;
     if (kchunk_override > 0) kchunk = kchunk_override;
@@ -1139,13 +883,16 @@ void aefdtd_sim::build_work() {
     for (int half = 0; half < 2; half++) {
         WorkSplit &w = half == 0 ? wsE : wsH;
         w.unroll = zunroll;
+        w.tile_y = tile_y;
         for (int g = 0; g < kGroups; g++) {
             w.off[g] = (int)(all.size() / 4);
             w.n[g] = (int)(v[half][g].size() / 4);
             all.insert(all.end(), v[half][g].begin(), v[half][g].end());
         }
     }
+    items_host = all;
     items.alloc(std::max<size_t>(all.size(), 4) * sizeof(int), dev_bytes);
+    graphs_dirty = true;   // captured segments point at the old lists
     if (!all.empty()) AE_CUDA(cudaMemcpy(items.p, all.data(), all.size() * sizeof(int), cudaMemcpyHostToDevice));
     work_dirty = false;
 }
@@ -1193,23 +940,6 @@ void aefdtd_sim::zero_state() {
 // C ABI
 // ------------------------------------------------------------------------
 
-template <typename F> static aefdtd_status guarded(aefdtd_sim *s, F &&f) {
-    try {
-        f();
-        if (s) s->last_error.clear();
-        return AEFDTD_OK;
-    } catch (Error &e) {
-        if (s) s->last_error = e.msg;
-        return e.st;
-    } catch (std::bad_alloc &) {
-        if (s) s->last_error = "host allocation failed";
-        return AEFDTD_OOM;
-    } catch (std::exception &e) {
-        if (s) s->last_error = e.what();
-        return AEFDTD_BAD_ARG;
-    }
-}
-
 static thread_local std::string g_create_error;
 
 extern "C" {
@@ -1231,6 +961,7 @@ aefdtd_status aefdtd_create(const aefdtd_grid_desc *desc, aefdtd_sim **out) {
 
 aefdtd_status aefdtd_destroy(aefdtd_sim *s) {
     if (!s) return AEFDTD_BAD_ARG;
+    if (s->batch) aefdtd::batch_detach(s->batch, s);
     delete s;
     return AEFDTD_OK;
 }
@@ -1397,7 +1128,10 @@ aefdtd_status aefdtd_add_planar_sensor(aefdtd_sim *s, const aefdtd_sensor_desc *
 
 aefdtd_status aefdtd_step(aefdtd_sim *s, int32_t n) {
     if (!s) return AEFDTD_BAD_ARG;
-    return guarded(s, [&] { s->step(n); });
+    return guarded(s, [&] {
+        if (s->batch) fail(AEFDTD_NOT_READY, "the simulation is stepped by its batch (aefdtd_batch_advance)");
+        s->step(n);
+    });
 }
 
 aefdtd_status aefdtd_synchronize(aefdtd_sim *s) {

@@ -32,4 +32,20 @@ template <typename T> static void acc_impl(const AccumArgs<T> &a, cudaStream_t s
 void launch_accumulate(const AccumArgs<double> &a, cudaStream_t s) { acc_impl(a, s); }
 void launch_accumulate(const AccumArgs<float> &a, cudaStream_t s) { acc_impl(a, s); }
 void launch_flux(const FluxArgs &a, cudaStream_t s) { flux_reduce<<<a.nl, 256, 0, s>>>(a); }
+template <typename T> static void plane_batch_impl(const SensorStepArgs<T> *args, const int2 *blk, int nblk, int q,
+                                                   cudaStream_t s) {
+    if (nblk > 0) plane_partial_batch<T><<<nblk, kPlaneThreads, 0, s>>>(args, blk, q);
+}
+void launch_plane_partial_batch(const SensorStepArgs<double> *args, const int2 *blk, int nblk, int q, cudaStream_t s) {
+    plane_batch_impl(args, blk, nblk, q, s);
+}
+void launch_plane_partial_batch(const SensorStepArgs<float> *args, const int2 *blk, int nblk, int q, cudaStream_t s) {
+    plane_batch_impl(args, blk, nblk, q, s);
+}
+void launch_plane_reduce_batch(const SensorStepArgs<double> *args, int n_inst, int steps, cudaStream_t s) {
+    if (n_inst > 0 && steps > 0) plane_sums_reduce_batch<double><<<dim3(steps, n_inst), 32, 0, s>>>(args);
+}
+void launch_plane_reduce_batch(const SensorStepArgs<float> *args, int n_inst, int steps, cudaStream_t s) {
+    if (n_inst > 0 && steps > 0) plane_sums_reduce_batch<float><<<dim3(steps, n_inst), 32, 0, s>>>(args);
+}
 }  // namespace aefdtd

@@ -23,17 +23,24 @@ namespace aefdtd {
 
 
 
+// Plane-sum arithmetic rounds every multiply and add separately (explicit
+// _rn operations), so every kernel that inlines it gives the same bits.
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+
 __device__ __forceinline__ double pulse_eval(const PulseDev &P, double A0, double x, double y, double z, double t) {
-    const double p = P.kx * x + P.ky * y + P.kz * z;
-    const double a = p - P.omega * t;
-    const double b = (1.0 / P.k * p - 299792458.0 * t / P.n_ind + P.C1) / P.dz;
-    return A0 * exp(-b * b) * cos(a);
+    const double p = dadd(dadd(dmul(P.kx, x), dmul(P.ky, y)), dmul(P.kz, z));
+    const double a = dsub(p, dmul(P.omega, t));
+    const double b = dadd(dsub(dmul(1.0 / P.k, p), dmul(299792458.0, t) / P.n_ind), P.C1) / P.dz;
+    return dmul(dmul(A0, exp(-dmul(b, b))), cos(a));
 }
 
 
 
+// Block b of the plane-sum partials of step q (scalars a.sc[q]) into part[b*12 + c].
 template <typename T>
-__device__ __forceinline__ void plane_partial(const SensorStepArgs<T> &a, int b) {
+__device__ __forceinline__ void plane_partial(const SensorStepArgs<T> &a, int b, int q, double *part) {
     double acc[12];
 #pragma unroll
     for (int c = 0; c < 12; ++c) acc[c] = 0;
@@ -42,7 +49,7 @@ __device__ __forceinline__ void plane_partial(const SensorStepArgs<T> &a, int b)
     const int q0 = b * per, q1 = min(n, q0 + per);
     const double Dx2 = a.Dx / 2.0, Dy2 = a.Dy / 2.0, Dz2 = a.Dz / 2.0;
     const double zr = a.kr * a.Dz, zt = a.kt * a.Dz;
-    const double tb = a.sc[a.q].tb, tap = a.sc[a.q].taper;
+    const double tb = a.sc[q].tb, tap = a.sc[q].taper;
     // With kx = ky = 0 (normal incidence) the phase kx x + ky y + kz z is
     // exactly kz z, so the six pulse values are the same at every cell of the
     // planes: evaluate them once per block.
@@ -57,8 +64,8 @@ __device__ __forceinline__ void plane_partial(const SensorStepArgs<T> &a, int b)
         }
         __syncthreads();
     }
-    for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
-        const int i = q % a.Nx, j = q / a.Nx;
+    for (int c = q0 + threadIdx.x; c < q1; c += blockDim.x) {
+        const int i = c % a.Nx, j = c / a.Nx;
         const double x = i * a.Dx, y = j * a.Dy;
         double bx, by, bz, tx, ty, tz;
         if (uniform) {
@@ -71,19 +78,19 @@ __device__ __forceinline__ void plane_partial(const SensorStepArgs<T> &a, int b)
             ty = pulse_eval(a.P, a.P.Ey0, x, y + Dy2, zt, tb);
             tz = pulse_eval(a.P, a.P.Ez0, x, y, zt + Dz2, tb);
         }
-        const long long ir = q + a.kr * a.NxNy, it = q + a.kt * a.NxNy;
-        acc[0] += bx * tap;
-        acc[1] += by * tap;
-        acc[2] += bz * tap;
-        acc[3] += ((double)a.Ex[ir] - bx) * tap;
-        acc[4] += ((double)a.Ey[ir] - by) * tap;
-        acc[5] += ((double)a.Ez[ir] - bz) * tap;
-        acc[6] += tx * tap;
-        acc[7] += ty * tap;
-        acc[8] += tz * tap;
-        acc[9] += (double)a.Ex[it] * tap;
-        acc[10] += (double)a.Ey[it] * tap;
-        acc[11] += (double)a.Ez[it] * tap;
+        const long long ir = c + a.kr * a.NxNy, it = c + a.kt * a.NxNy;
+        acc[0] = dadd(acc[0], dmul(bx, tap));
+        acc[1] = dadd(acc[1], dmul(by, tap));
+        acc[2] = dadd(acc[2], dmul(bz, tap));
+        acc[3] = dadd(acc[3], dmul(dsub((double)a.Ex[ir], bx), tap));
+        acc[4] = dadd(acc[4], dmul(dsub((double)a.Ey[ir], by), tap));
+        acc[5] = dadd(acc[5], dmul(dsub((double)a.Ez[ir], bz), tap));
+        acc[6] = dadd(acc[6], dmul(tx, tap));
+        acc[7] = dadd(acc[7], dmul(ty, tap));
+        acc[8] = dadd(acc[8], dmul(tz, tap));
+        acc[9] = dadd(acc[9], dmul((double)a.Ex[it], tap));
+        acc[10] = dadd(acc[10], dmul((double)a.Ey[it], tap));
+        acc[11] = dadd(acc[11], dmul((double)a.Ez[it], tap));
     }
     __shared__ double red[12][kPlaneThreads];
 #pragma unroll
@@ -95,7 +102,7 @@ __device__ __forceinline__ void plane_partial(const SensorStepArgs<T> &a, int b)
             for (int c = 0; c < 12; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + s];
         __syncthreads();
     }
-    if (threadIdx.x < 12) a.partial[b * 12 + threadIdx.x] = red[threadIdx.x][0];
+    if (threadIdx.x < 12) part[b * 12 + threadIdx.x] = red[threadIdx.x][0];
 }
 
 template <typename T>
@@ -137,7 +144,7 @@ template <typename T>
 __global__ void __launch_bounds__(kPlaneThreads) sensor_step(const __grid_constant__ SensorStepArgs<T> a) {
     const int b = blockIdx.x + (a.part ? a.nbp : 0);
     if (b < a.nbp) {
-        plane_partial(a, b);
+        plane_partial(a, b, a.q, a.partial);
         return;
     }
     for (int s = 0; s < a.ng; ++s)
@@ -156,6 +163,29 @@ __global__ void plane_sums_reduce(const double *partial, int nbp, const StepScal
     const double *p = partial + (long long)q * nbp * 12;
     for (int b = 0; b < nbp; ++b) s += p[b * 12 + c];
     out[((long long)sc[0].step + q) * 12 + c] = s;
+}
+
+// Batched plane sums (normal-mode members of a batch, no sample gathers):
+// block -> (instance, block of that instance) from blk; partials of step q at
+// args[inst].partial + q * nbp * 12.
+template <typename T>
+__global__ void __launch_bounds__(kPlaneThreads)
+plane_partial_batch(const SensorStepArgs<T> *__restrict__ args, const int2 *__restrict__ blk, int q) {
+    const int2 m = blk[blockIdx.x];
+    const SensorStepArgs<T> &a = args[m.x];
+    plane_partial(a, m.y, q, a.partial + (long long)q * a.nbp * 12);
+}
+
+// grid (L, instances): instance x's step q sums into x.out[(sc[0].step + q) * 12 + c]
+template <typename T>
+__global__ void plane_sums_reduce_batch(const SensorStepArgs<T> *__restrict__ args) {
+    const SensorStepArgs<T> &a = args[blockIdx.y];
+    const int q = blockIdx.x, c = threadIdx.x;
+    if (c >= 12 || a.nbp == 0) return;
+    double s = 0;
+    const double *p = a.partial + (long long)q * a.nbp * 12;
+    for (int b = 0; b < a.nbp; ++b) s += p[b * 12 + c];
+    a.out[((long long)a.sc[0].step + q) * 12 + c] = s;
 }
 
 // s_curve (src/common/mathUT.cpp:1186-1193)

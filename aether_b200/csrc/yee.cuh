@@ -44,7 +44,7 @@ namespace aefdtd {
 template <typename T> struct Exact { static constexpr bool value = std::is_same<T, double>::value; };
 
 constexpr int kTileX = 32;
-constexpr int kTileY = 4;
+constexpr int kTileY = 4;   // default tile height (the batch autotuner may choose 2 or 8)
 
 // psi_new = b*psi + c*diff (FP64, reference order) or psi + ((b-1)*psi + c*diff) (FP32)
 template <typename T> __device__ __forceinline__ T cpml_rec(T b, T psi, T c, T diff) {
@@ -61,11 +61,13 @@ constexpr unsigned kFMisc = 8;    // the injection plane or an oscillator box
 constexpr unsigned kFAll = 15;
 
 // ---- interior items: curl update only -----------------------------------
+// Kernel bodies take the arguments by reference (from the parameter bank for
+// one simulation, from a device array for a batch), the step's table index q
+// and the item (x0, y0, k0, k1). A CTA is 32 x TY threads for tiles of 32 x
+// TY columns (TY = 2, 4 or 8, chosen per launch).
 template <typename T, typename Tid, int U>
-__global__ void __launch_bounds__(kTileX * kTileY, (U == 1 && sizeof(T) == 4) ? 12 : 8)
-e_interior(const __grid_constant__ StepArgs<T, Tid> a, const int4 *__restrict__ items) {
+__device__ __forceinline__ void e_interior_body(const StepArgs<T, Tid> &a, int q, int4 it) {
     // coefficients through the read-only path: short-lived CTAs skip a table fill and barrier
-    const int4 it = items[blockIdx.x];
     const int i = it.x + threadIdx.x, j = it.y + threadIdx.y;
     if (i >= a.Nx || j >= a.Ny) return;
     const long long NxNy = a.NxNy;
@@ -122,9 +124,7 @@ e_interior(const __grid_constant__ StepArgs<T, Tid> a, const int4 *__restrict__ 
 }
 
 template <typename T, typename Tid, int U>
-__global__ void __launch_bounds__(kTileX * kTileY, (U == 1 && sizeof(T) == 4) ? 12 : 8)
-h_interior(const __grid_constant__ StepArgs<T, Tid> a, const int4 *__restrict__ items) {
-    const int4 it = items[blockIdx.x];
+__device__ __forceinline__ void h_interior_body(const StepArgs<T, Tid> &a, int q, int4 it) {
     const int i = it.x + threadIdx.x, j = it.y + threadIdx.y;
     if (i >= a.Nx || j >= a.Ny) return;
     const long long NxNy = a.NxNy;
@@ -176,9 +176,7 @@ h_interior(const __grid_constant__ StepArgs<T, Tid> a, const int4 *__restrict__ 
 
 // ---- boundary items: the phases of feature set F ---------------------------
 template <typename T, typename Tid, unsigned F>
-__global__ void __launch_bounds__(kTileX * kTileY) e_boundary(const __grid_constant__ StepArgs<T, Tid> a,
-                                                              const int4 *__restrict__ items) {
-    const int4 it = items[blockIdx.x];
+__device__ __forceinline__ void e_boundary_body(const StepArgs<T, Tid> &a, int q, int4 it) {
     const int i = it.x + threadIdx.x, j = it.y + threadIdx.y;
     if (i >= a.Nx || j >= a.Ny) return;
     const int k0 = it.z, k1 = it.w;
@@ -345,14 +343,14 @@ __global__ void __launch_bounds__(kTileX * kTileY) e_boundary(const __grid_const
         if constexpr ((F & kFMisc) != 0) {
             // Normal-incidence plane injection after update_E (normal_incidence.cpp:338-342)
             if (k == a.kinj) {
-                nex = nex - (T)a.sc[a.q].inj_eA;
-                ney = ney + (T)a.sc[a.q].inj_eB;
+                nex = nex - (T)a.sc[q].inj_eA;
+                ney = ney + (T)a.sc[q].inj_eB;
             }
             // Oscillator boxes after update_E (sc_oscillator.cpp:43-63)
             for (int s = 0; s < a.nsrc; ++s) {
                 const int *b = a.src_box[s];
                 if (i >= b[0] && i < b[1] && j >= b[2] && j < b[3] && k >= b[4] && k < b[5]) {
-                    const T v = (T)a.sc[a.q].src[s];
+                    const T v = (T)a.sc[q].src[s];
                     if (a.src_comp[s] == 0) nex += v;
                     else if (a.src_comp[s] == 1) ney += v;
                     else nez += v;
@@ -369,9 +367,7 @@ __global__ void __launch_bounds__(kTileX * kTileY) e_boundary(const __grid_const
 }
 
 template <typename T, typename Tid, unsigned F>
-__global__ void __launch_bounds__(kTileX * kTileY) h_boundary(const __grid_constant__ StepArgs<T, Tid> a,
-                                                              const int4 *__restrict__ items) {
-    const int4 it = items[blockIdx.x];
+__device__ __forceinline__ void h_boundary_body(const StepArgs<T, Tid> &a, int q, int4 it) {
     const int i = it.x + threadIdx.x, j = it.y + threadIdx.y;
     if (i >= a.Nx || j >= a.Ny) return;
     const int k0 = it.z, k1 = it.w;
@@ -491,8 +487,8 @@ __global__ void __launch_bounds__(kTileX * kTileY) h_boundary(const __grid_const
         if constexpr ((F & kFMisc) != 0) {
             // H plane injection after update_H (normal_incidence.cpp:353-357)
             if (k == a.kinj) {
-                nhx = nhx + (T)a.sc[a.q].inj_hA;
-                nhy = nhy - (T)a.sc[a.q].inj_hB;
+                nhx = nhx + (T)a.sc[q].inj_hA;
+                nhy = nhy - (T)a.sc[q].inj_hB;
             }
         }
         Hx[id] = nhx;
@@ -503,13 +499,71 @@ __global__ void __launch_bounds__(kTileX * kTileY) h_boundary(const __grid_const
     }
 }
 
+// ---- kernels -----------------------------------------------------------------
+// Register caps: at most 256 threads per CTA; the interior kernels keep the
+// register budget of 12 (U = 1, FP32) or 8 resident 128-thread CTAs per SM.
+template <typename T, int U> struct InteriorBounds {
+    static constexpr int kMinBlocks = (U == 1 && sizeof(T) == 4) ? 6 : 4;   // per 256 threads
+};
+constexpr int kMaxTileThreads = 256;
+
+template <typename T, typename Tid, int U>
+__global__ void __launch_bounds__(kMaxTileThreads, InteriorBounds<T, U>::kMinBlocks)
+e_interior(const __grid_constant__ StepArgs<T, Tid> a, const int4 *__restrict__ items) {
+    e_interior_body<T, Tid, U>(a, a.q, items[blockIdx.x]);
+}
+template <typename T, typename Tid, int U>
+__global__ void __launch_bounds__(kMaxTileThreads, InteriorBounds<T, U>::kMinBlocks)
+h_interior(const __grid_constant__ StepArgs<T, Tid> a, const int4 *__restrict__ items) {
+    h_interior_body<T, Tid, U>(a, a.q, items[blockIdx.x]);
+}
+template <typename T, typename Tid, unsigned F>
+__global__ void __launch_bounds__(kMaxTileThreads) e_boundary(const __grid_constant__ StepArgs<T, Tid> a,
+                                                              const int4 *__restrict__ items) {
+    e_boundary_body<T, Tid, F>(a, a.q, items[blockIdx.x]);
+}
+template <typename T, typename Tid, unsigned F>
+__global__ void __launch_bounds__(kMaxTileThreads) h_boundary(const __grid_constant__ StepArgs<T, Tid> a,
+                                                              const int4 *__restrict__ items) {
+    h_boundary_body<T, Tid, F>(a, a.q, items[blockIdx.x]);
+}
+
+// Batched forms: item (x0, y0, k0 | k1 << 16, instance), arguments of the
+// instance from a device array, q the step's index in every member's table.
+__device__ __forceinline__ int4 batch_item(int4 b) { return make_int4(b.x, b.y, b.z & 0xffff, b.z >> 16); }
+
+template <typename T, typename Tid, int U>
+__global__ void __launch_bounds__(kMaxTileThreads, InteriorBounds<T, U>::kMinBlocks)
+e_interior_batch(const StepArgs<T, Tid> *__restrict__ args, int q, const int4 *__restrict__ items) {
+    const int4 b = items[blockIdx.x];
+    e_interior_body<T, Tid, U>(args[b.w], q, batch_item(b));
+}
+template <typename T, typename Tid, int U>
+__global__ void __launch_bounds__(kMaxTileThreads, InteriorBounds<T, U>::kMinBlocks)
+h_interior_batch(const StepArgs<T, Tid> *__restrict__ args, int q, const int4 *__restrict__ items) {
+    const int4 b = items[blockIdx.x];
+    h_interior_body<T, Tid, U>(args[b.w], q, batch_item(b));
+}
+template <typename T, typename Tid, unsigned F>
+__global__ void __launch_bounds__(kMaxTileThreads)
+e_boundary_batch(const StepArgs<T, Tid> *__restrict__ args, int q, const int4 *__restrict__ items) {
+    const int4 b = items[blockIdx.x];
+    e_boundary_body<T, Tid, F>(args[b.w], q, batch_item(b));
+}
+template <typename T, typename Tid, unsigned F>
+__global__ void __launch_bounds__(kMaxTileThreads)
+h_boundary_batch(const StepArgs<T, Tid> *__restrict__ args, int q, const int4 *__restrict__ items) {
+    const int4 b = items[blockIdx.x];
+    h_boundary_body<T, Tid, F>(args[b.w], q, batch_item(b));
+}
+
 // ---- launchers: group g of a half-step's WorkSplit ------------------------
 template <typename T, typename Tid>
 void launch_e_group_impl(const StepArgs<T, Tid> &a, const int4 *items, const WorkSplit &w, int g, cudaStream_t s) {
     const int n = w.n[g];
     if (n <= 0) return;
     const int4 *p = items + w.off[g];
-    const dim3 blk(kTileX, kTileY);
+    const dim3 blk(kTileX, w.tile_y);
     switch (g) {
         case kGroupInterior:
             if (w.unroll >= 2) e_interior<T, Tid, 2><<<n, blk, 0, s>>>(a, p);
@@ -526,7 +580,7 @@ void launch_h_group_impl(const StepArgs<T, Tid> &a, const int4 *items, const Wor
     const int n = w.n[g];
     if (n <= 0) return;
     const int4 *p = items + w.off[g];
-    const dim3 blk(kTileX, kTileY);
+    const dim3 blk(kTileX, w.tile_y);
     switch (g) {
         case kGroupInterior:
             if (w.unroll >= 2) h_interior<T, Tid, 2><<<n, blk, 0, s>>>(a, p);
@@ -534,6 +588,41 @@ void launch_h_group_impl(const StepArgs<T, Tid> &a, const int4 *items, const Wor
             break;
         case kGroupPmlZ: h_boundary<T, Tid, kFPmlZ><<<n, blk, 0, s>>>(a, p); break;
         default: h_boundary<T, Tid, kFAll><<<n, blk, 0, s>>>(a, p); break;
+    }
+}
+
+template <typename T, typename Tid>
+void launch_e_group_batch_impl(const StepArgs<T, Tid> *args, int q, const int4 *items, const WorkSplit &w, int g,
+                               cudaStream_t s) {
+    const int n = w.n[g];
+    if (n <= 0) return;
+    const int4 *p = items + w.off[g];
+    const dim3 blk(kTileX, w.tile_y);
+    switch (g) {
+        case kGroupInterior:
+            if (w.unroll >= 2) e_interior_batch<T, Tid, 2><<<n, blk, 0, s>>>(args, q, p);
+            else e_interior_batch<T, Tid, 1><<<n, blk, 0, s>>>(args, q, p);
+            break;
+        case kGroupPmlZ: e_boundary_batch<T, Tid, kFPmlZ><<<n, blk, 0, s>>>(args, q, p); break;
+        case kGroupDisp: e_boundary_batch<T, Tid, kFDisp><<<n, blk, 0, s>>>(args, q, p); break;
+        default: e_boundary_batch<T, Tid, kFAll><<<n, blk, 0, s>>>(args, q, p); break;
+    }
+}
+
+template <typename T, typename Tid>
+void launch_h_group_batch_impl(const StepArgs<T, Tid> *args, int q, const int4 *items, const WorkSplit &w, int g,
+                               cudaStream_t s) {
+    const int n = w.n[g];
+    if (n <= 0) return;
+    const int4 *p = items + w.off[g];
+    const dim3 blk(kTileX, w.tile_y);
+    switch (g) {
+        case kGroupInterior:
+            if (w.unroll >= 2) h_interior_batch<T, Tid, 2><<<n, blk, 0, s>>>(args, q, p);
+            else h_interior_batch<T, Tid, 1><<<n, blk, 0, s>>>(args, q, p);
+            break;
+        case kGroupPmlZ: h_boundary_batch<T, Tid, kFPmlZ><<<n, blk, 0, s>>>(args, q, p); break;
+        default: h_boundary_batch<T, Tid, kFAll><<<n, blk, 0, s>>>(args, q, p); break;
     }
 }
 

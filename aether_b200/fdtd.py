@@ -10,7 +10,7 @@ import time
 import numpy as np
 
 from . import _abi as A
-from ._lib import check, load
+from ._lib import AefdtdError, check, load
 
 _P = C.POINTER
 
@@ -187,3 +187,95 @@ def run(scene, nsteps=None, want_fields=True):
         out["flux"] = [sim.sensor_flux(i) for i in range(len(scene.sensors))]
         out["launches"] = sim.launch_count()
         return out
+
+
+class Batch:
+    """Many simulations advanced together (include/aefdtd.h, aefdtd_batch_*):
+    merged launches per work-item group over all members of an L2-sized
+    subset, one captured graph per subset and segment. Members are ordinary
+    Simulations; the batch keeps references to them while they are members."""
+
+    def __init__(self, l2_budget_bytes=0, tile_y=0, kchunk=0, use_graphs=True, device=0):
+        self._lib = load()
+        o = A.BatchOpts()
+        o.abi_version = A.ABI_VERSION
+        o.device = device
+        o.l2_budget_bytes = int(l2_budget_bytes)
+        o.tile_y, o.kchunk = int(tile_y), int(kchunk)
+        o.use_graphs = 0 if use_graphs else -1
+        self._h = C.c_void_p()
+        st = self._lib.aefdtd_batch_create(C.byref(o), C.byref(self._h))
+        if st != 0:
+            raise AefdtdError(st, "aefdtd_batch_create failed")
+        self.members = {}
+
+    def _c(self, st):
+        if st != 0:
+            msg = self._lib.aefdtd_batch_last_error(self._h)
+            raise AefdtdError(st, msg.decode() if msg else "")
+
+    def close(self):
+        if self._h:
+            self._lib.aefdtd_batch_destroy(self._h)
+            self._h = C.c_void_p()
+        self.members = {}
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def add(self, sim: Simulation, steps: int):
+        self._c(self._lib.aefdtd_batch_add(self._h, sim._h, int(steps)))
+        self.members[sim._h.value] = sim
+
+    def remove(self, sim: Simulation):
+        self._c(self._lib.aefdtd_batch_remove(self._h, sim._h))
+        self.members.pop(sim._h.value, None)
+
+    def set_budget(self, sim: Simulation, steps: int):
+        self._c(self._lib.aefdtd_batch_set_budget(self._h, sim._h, int(steps)))
+
+    def autotune(self):
+        self._c(self._lib.aefdtd_batch_autotune(self._h))
+
+    def advance(self, max_steps: int) -> int:
+        done = C.c_int32(0)
+        self._c(self._lib.aefdtd_batch_advance(self._h, int(max_steps), C.byref(done)))
+        return done.value
+
+    def run(self, max_steps: int) -> int:
+        """Advances until every member used its budget (or max_steps)."""
+        total = 0
+        while total < max_steps:
+            n = self.advance(max_steps - total)
+            if n == 0:
+                break
+            total += n
+        return total
+
+    def finished(self):
+        n = C.c_int32(0)
+        self._c(self._lib.aefdtd_batch_finished(self._h, None, 0, C.byref(n)))
+        if n.value == 0:
+            return []
+        arr = (C.c_void_p * n.value)()
+        self._c(self._lib.aefdtd_batch_finished(self._h, arr, n.value, C.byref(n)))
+        return [self.members[p] for p in arr[:n.value] if p in self.members]
+
+    def info(self) -> dict:
+        i = A.BatchInfo()
+        self._c(self._lib.aefdtd_batch_get_info(self._h, C.byref(i)))
+        k = min(i.n_classes, A.BATCH_MAX_CLASSES)
+        return {"n_members": i.n_members, "n_active": i.n_active, "n_subsets": i.n_subsets, "cells": i.cells,
+                "member_bytes": i.member_bytes, "batch_bytes": i.batch_bytes,
+                "l2_budget_bytes": i.l2_budget_bytes, "launches": i.launches,
+                "classes": [{"key": i.class_key[c], "tile_y": i.class_tile_y[c], "kchunk": i.class_kchunk[c]}
+                            for c in range(k)]}

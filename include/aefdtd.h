@@ -259,6 +259,64 @@ aefdtd_status aefdtd_get_stream(aefdtd_sim *sim, void **stream);
 /* Number of device kernel launches issued by this handle since creation. */
 aefdtd_status aefdtd_get_launch_count(aefdtd_sim *sim, uint64_t *launches);
 
+/* ---- batches: many simulations advanced together ----------------------
+ *
+ * No single reference counterpart: a batch runs what the reference runs as one
+ * FDTD_normal_incidence/FDTD_Mode per simulation (normal_incidence.cpp:161-436)
+ * for many simulations at once (parameter sweeps of periodic unit cells).
+ * Members are ordinary simulations (created, given map, materials and
+ * excitation as usual) without planar DFT sensors; normal-mode plane sums and
+ * spectra are kept per member. A member is stepped only by its batch
+ * (aefdtd_step on it returns AEFDTD_NOT_READY) and leaves it with
+ * aefdtd_batch_remove or aefdtd_destroy. All members share precision,
+ * material-id width and DFT block size. Member results are the same as
+ * stepping each alone (FP64: bit-identical fields). */
+typedef struct aefdtd_batch aefdtd_batch;
+
+typedef struct aefdtd_batch_opts {
+    int32_t abi_version;      /* = AEFDTD_ABI_VERSION */
+    int32_t device;           /* CUDA device of the batch and its members */
+    int64_t l2_budget_bytes;  /* device state per subset of members stepped together; 0 -> 96 MiB, < 0 -> no limit */
+    int32_t tile_y;           /* tile height 2, 4 or 8 (0 -> 4) until autotuned */
+    int32_t kchunk;           /* planes per work item (0 -> each simulation's heuristic) until autotuned */
+    int32_t use_graphs;       /* < 0: no CUDA graphs (direct launches) */
+    int32_t reserved;
+} aefdtd_batch_opts;
+
+#define AEFDTD_BATCH_MAX_CLASSES 32
+typedef struct aefdtd_batch_info {
+    int32_t n_members, n_active, n_subsets, n_classes;
+    int64_t cells;            /* total cells of the active members */
+    int64_t member_bytes;     /* device memory held by all members */
+    int64_t batch_bytes;      /* device memory held by the batch itself (work lists, argument arrays) */
+    int64_t l2_budget_bytes;
+    uint64_t launches;        /* kernel launches issued by the batch */
+    int32_t class_key[AEFDTD_BATCH_MAX_CLASSES];     /* ceil(Nx/16)*1000 + ceil(Ny/16) */
+    int32_t class_tile_y[AEFDTD_BATCH_MAX_CLASSES];
+    int32_t class_kchunk[AEFDTD_BATCH_MAX_CLASSES];
+} aefdtd_batch_info;
+
+aefdtd_status aefdtd_batch_create(const aefdtd_batch_opts *opts, aefdtd_batch **out);
+aefdtd_status aefdtd_batch_destroy(aefdtd_batch *batch);
+const char *aefdtd_batch_last_error(const aefdtd_batch *batch);
+/* Adds a simulation with a budget of `steps` more time steps. */
+aefdtd_status aefdtd_batch_add(aefdtd_batch *batch, aefdtd_sim *sim, int32_t steps);
+aefdtd_status aefdtd_batch_remove(aefdtd_batch *batch, aefdtd_sim *sim);
+aefdtd_status aefdtd_batch_set_budget(aefdtd_batch *batch, aefdtd_sim *sim, int32_t steps);
+/* Chooses per size class the tile height (2, 4, 8) and planes per work item
+ * (4, 8), then the subset L2 budget (48 MiB, 96 MiB, none), by timing trial
+ * segments on the device. Every member must be at step 0; members are reset
+ * to step 0. */
+aefdtd_status aefdtd_batch_autotune(aefdtd_batch *batch);
+/* Advances the members with budget left, by at most max_steps steps, and
+ * returns after the segment in which a member uses up its budget (so callers
+ * can retire it and admit others). *steps_done: steps run. Waits for the
+ * device before returning. */
+aefdtd_status aefdtd_batch_advance(aefdtd_batch *batch, int32_t max_steps, int32_t *steps_done);
+/* Members whose budget is used up: up to cap handles in out, count in *n. */
+aefdtd_status aefdtd_batch_finished(aefdtd_batch *batch, aefdtd_sim **out, int32_t cap, int32_t *n);
+aefdtd_status aefdtd_batch_get_info(aefdtd_batch *batch, aefdtd_batch_info *info);
+
 /* ---- allocation-free diagnostics -------------------------------------- */
 
 /* No counterpart in the reference: an entry point for callers that must not

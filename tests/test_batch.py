@@ -1,0 +1,158 @@
+"""Batches (aefdtd_batch_*): many simulations advanced together.
+
+A member's results must not depend on the batch. In FP64, fields and plane
+sums of every member are bit-identical to the same simulation stepped alone,
+whatever the subset budget, tile height, planes per item, step budgets or
+autotuning. In FP32 they agree to 1e-5 relative: the batched kernels are
+separate instantiations and may contract multiply-adds differently."""
+import numpy as np
+import pytest
+
+from aether_b200 import _abi as A
+from aether_b200 import configs as CF
+from aether_b200 import fdtd
+from aether_b200._lib import AefdtdError
+
+pytestmark = pytest.mark.gpu
+
+NM = 1e-9
+
+
+def cells(seed, n=4, precision=A.FP64, nsteps=400):
+    """Small nanodisk unit cells of uneven sizes (16-36 cells across)."""
+    rng = np.random.default_rng(seed)
+    return [CF.metasurface_cell(rng, nz_total=64, pml=8, nsteps=nsteps, nl=11, precision=precision,
+                                period_range=(80 * NM, 180 * NM), flux_planes=False) for _ in range(n)]
+
+
+def alone(scene, steps):
+    with fdtd.build_simulation(scene) as s:
+        s.step(steps)
+        return s.fields(), s.plane_sums()
+
+
+def rel(a, b):
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(np.asarray(b)), 1e-300)
+
+
+@pytest.mark.parametrize("opts", [dict(), dict(l2_budget_bytes=1), dict(l2_budget_bytes=-1),
+                                  dict(tile_y=2, kchunk=16), dict(tile_y=8, kchunk=4), dict(use_graphs=False)])
+def test_fp64_batch_members_bit_identical_to_alone(opts):
+    scenes = cells(3)
+    steps = 150
+    want = [alone(sc, steps) for sc in scenes]
+    sims = [fdtd.build_simulation(sc) for sc in scenes]
+    with fdtd.Batch(**opts) as b:
+        for s in sims:
+            b.add(s, steps)
+        assert b.run(10 ** 6) == steps
+        assert len(b.finished()) == len(sims)
+        for s, (f, p) in zip(sims, want):
+            assert np.array_equal(s.fields(), f)
+            assert np.array_equal(s.plane_sums(), p)
+    for s in sims:
+        s.close()
+
+
+def test_uneven_budgets_finish_exactly_and_batch_stops_at_each_finish():
+    scenes = cells(5, n=3)
+    budgets = [70, 130, 200]
+    want = [alone(sc, n) for sc, n in zip(scenes, budgets)]
+    sims = [fdtd.build_simulation(sc) for sc in scenes]
+    with fdtd.Batch() as b:
+        for s, n in zip(sims, budgets):
+            b.add(s, n)
+        stops = []
+        total = 0
+        while True:
+            n = b.advance(10 ** 6)
+            if n == 0:
+                break
+            total += n
+            stops.append(total)
+        assert stops == budgets
+        for s, n, (f, p) in zip(sims, budgets, want):
+            assert s.dims().step == n
+            assert np.array_equal(s.fields(), f)
+            assert np.array_equal(s.plane_sums(), p)
+    for s in sims:
+        s.close()
+
+
+def test_members_join_and_leave_between_segments():
+    """Continuous batching: a member retires when done, another joins later;
+    each result equals its run alone."""
+    scenes = cells(11, n=3)
+    want = [alone(sc, 100) for sc in scenes]
+    s0, s1, s2 = (fdtd.build_simulation(sc) for sc in scenes)
+    with fdtd.Batch() as b:
+        b.add(s0, 100)
+        b.add(s1, 100)
+        assert b.advance(40) == 40
+        b.add(s2, 100)              # joins while the others are mid-run
+        done = []
+        while len(done) < 3:
+            n = b.advance(10 ** 6)
+            assert n > 0
+            for s in b.finished():
+                done.append(s)
+                b.remove(s)
+        for s, (f, p) in zip((s0, s1, s2), want):
+            assert np.array_equal(s.fields(), f)
+            assert np.array_equal(s.plane_sums(), p)
+    for s in (s0, s1, s2):
+        s.close()
+
+
+def test_autotune_then_run_matches_alone():
+    scenes = cells(21, n=4)
+    steps = 128
+    want = [alone(sc, steps) for sc in scenes]
+    sims = [fdtd.build_simulation(sc) for sc in scenes]
+    with fdtd.Batch() as b:
+        for s in sims:
+            b.add(s, steps)
+        b.autotune()
+        info = b.info()
+        assert len(info["classes"]) >= 1
+        for c in info["classes"]:
+            assert c["tile_y"] in (2, 4, 8) and c["kchunk"] in (4, 8)
+        assert all(s.dims().step == 0 for s in sims)
+        assert b.run(10 ** 6) == steps
+        for s, (f, p) in zip(sims, want):
+            assert np.array_equal(s.fields(), f)
+            assert np.array_equal(s.plane_sums(), p)
+    for s in sims:
+        s.close()
+
+
+def test_fp32_batch_close_to_alone():
+    scenes = cells(7, n=3, precision=A.FP32)
+    steps = 200
+    want = [alone(sc, steps) for sc in scenes]
+    sims = [fdtd.build_simulation(sc) for sc in scenes]
+    with fdtd.Batch() as b:
+        for s in sims:
+            b.add(s, steps)
+        b.run(10 ** 6)
+        for s, (f, p) in zip(sims, want):
+            assert rel(s.fields(), f) < 1e-5
+            assert rel(s.plane_sums(), p) < 1e-5
+    for s in sims:
+        s.close()
+
+
+def test_member_refuses_direct_steps_and_leaves_on_destroy():
+    scenes = cells(2, n=2)
+    s0, s1 = (fdtd.build_simulation(sc) for sc in scenes)
+    with fdtd.Batch() as b:
+        b.add(s0, 64)
+        b.add(s1, 64)
+        with pytest.raises(AefdtdError):
+            s0.step(1)
+        h1 = s1._h.value
+        s1.close()                  # destroying a member detaches it
+        b.members.pop(h1, None)
+        assert b.info()["n_members"] == 1
+        assert b.run(10 ** 6) == 64
+    s0.close()
