@@ -98,6 +98,42 @@ class BatchInfo(C.Structure):
     ]
 
 
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED = 0, 1, 2, 3
+
+
+class ServerOpts(C.Structure):
+    _fields_ = [
+        ("abi_version", C.c_int32), ("device", C.c_int32), ("hbm_fraction", C.c_double),
+        ("budget_bytes", C.c_int64), ("max_active", C.c_int32), ("segment_steps", C.c_int32),
+        ("lookahead", C.c_int32), ("reserved", C.c_int32), ("batch", BatchOpts),
+    ]
+
+
+class JobDesc(C.Structure):
+    _fields_ = [
+        ("grid", C.POINTER(GridDesc)), ("map", C.POINTER(C.c_uint32)), ("map_count", C.c_size_t),
+        ("materials", C.POINTER(MaterialDesc)), ("n_materials", C.c_int32),
+        ("normal", C.POINTER(NormalDesc)), ("steps", C.c_int32),
+    ]
+
+
+class JobInfo(C.Structure):
+    _fields_ = [
+        ("state", C.c_int32), ("steps", C.c_int32), ("cells", C.c_int64), ("est_bytes", C.c_int64),
+        ("bytes", C.c_int64), ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double),
+    ]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_int32), ("queued", C.c_int32), ("running", C.c_int32), ("done", C.c_int32),
+        ("failed", C.c_int32), ("reserved", C.c_int32),
+        ("budget_bytes", C.c_int64), ("in_use_bytes", C.c_int64), ("peak_bytes", C.c_int64),
+        ("p50_s", C.c_double), ("p99_s", C.c_double), ("mean_s", C.c_double), ("elapsed_s", C.c_double),
+        ("sims_per_s", C.c_double), ("gcells_per_s", C.c_double),
+    ]
+
+
 class StructureOp(C.Structure):
     _fields_ = [("kind", C.c_int32), ("mat_index", C.c_int32), ("p", C.c_double * 8)]
 

@@ -59,6 +59,14 @@ _SIGS = {
     "aefdtd_batch_advance": (C.c_int, [C.c_void_p, C.c_int32, _P(C.c_int32)]),
     "aefdtd_batch_finished": (C.c_int, [C.c_void_p, _P(C.c_void_p), C.c_int32, _P(C.c_int32)]),
     "aefdtd_batch_get_info": (C.c_int, [C.c_void_p, _P(A.BatchInfo)]),
+    "aefdtd_server_create": (C.c_int, [_P(A.ServerOpts), _P(C.c_void_p)]),
+    "aefdtd_server_destroy": (C.c_int, [C.c_void_p]),
+    "aefdtd_server_last_error": (C.c_char_p, [C.c_void_p]),
+    "aefdtd_server_submit": (C.c_int, [C.c_void_p, _P(A.JobDesc), _P(C.c_int32)]),
+    "aefdtd_server_poll": (C.c_int, [C.c_void_p, _P(C.c_int32)]),
+    "aefdtd_server_job_info": (C.c_int, [C.c_void_p, C.c_int32, _P(A.JobInfo)]),
+    "aefdtd_server_job_spectra": (C.c_int, [C.c_void_p, C.c_int32, _P(C.c_double), C.c_int32]),
+    "aefdtd_server_get_stats": (C.c_int, [C.c_void_p, _P(A.ServerStats)]),
 }
 
 

@@ -36,6 +36,7 @@ UNITS = [
     ("plane_static.cu", []),
     ("runtime.cpp", None),
     ("batch.cpp", None),
+    ("server.cpp", None),
 ]
 HEADERS = ["aefdtd_dev.hpp", "kernels.hpp", "sensors.cuh", "yee.cuh", "sim.hpp"]
 

@@ -35,27 +35,28 @@ struct BatchMember {
     aefdtd_sim *sim = nullptr;
     int remaining = 0;   // steps still to run
     int cls = 0;         // size-class key
+    bool placed = false; // in a subset
 };
 
 struct BatchSubset {
     int cls = 0;
-    std::vector<int> members;      // indices into aefdtd_batch::members
+    std::vector<aefdtd_sim *> members;
     size_t bytes = 0;              // device state of the members
-    long long cells = 0;
     DBuf items;                    // merged items: E groups, then H groups
     WorkSplit wsE{}, wsH{};
     DBuf argsE[2], argsH[2], sargs[2];   // per table slot
     DBuf blkmap;
     int nblk = 0;
     int nplane = 0;                // members with plane sums
+    int slot = 0;                  // table slot of the next segment
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     uint64_t graph_launches = 0;
     bool built = false;
     void release(size_t &t) {
         items.release(t);
-        for (int s = 0; s < 2; s++) {
-            argsE[s].release(t); argsH[s].release(t); sargs[s].release(t);
-            if (graph[s]) { cudaGraphExecDestroy(graph[s]); graph[s] = nullptr; }
+        for (int k = 0; k < 2; k++) {
+            argsE[k].release(t); argsH[k].release(t); sargs[k].release(t);
+            if (graph[k]) { cudaGraphExecDestroy(graph[k]); graph[k] = nullptr; }
         }
         blkmap.release(t);
         built = false;
@@ -84,7 +85,6 @@ struct aefdtd_batch {
     std::map<int, SizeClass> classes;
     bool layout_dirty = true;
     long long l2_budget = 96LL << 20;
-    int slot = 0;
     uint64_t launches = 0;
     size_t dev_bytes = 0;
 
@@ -95,15 +95,22 @@ struct aefdtd_batch {
             if (members[i].sim == s) return (int)i;
         return -1;
     }
+    BatchMember &rec(const aefdtd_sim *s) { return members[find(s)]; }
     void drop_layout() {
         for (auto &u : subsets) u.release(dev_bytes);
         subsets.clear();
+        for (auto &m : members) m.placed = false;
         layout_dirty = true;
     }
-    void layout();
+    bool fits(const BatchSubset &u, size_t b) const {
+        return u.members.empty() || l2_budget < 0 || (long long)(u.bytes + b) <= l2_budget;
+    }
+    void place(BatchMember &m);
+    void update_layout();
     template <typename T, typename Tid> void build_subset(BatchSubset &u);
     template <typename T, typename Tid> void enqueue_segment(BatchSubset &u, int L, int sl);
     template <typename T, typename Tid> void run_segment(BatchSubset &u, int L);
+    template <typename T, typename Tid> void ensure_history();
     template <typename T, typename Tid> int advance(int max_steps);
     template <typename T, typename Tid> double time_segments(int reps);
     template <typename T, typename Tid> void autotune();
@@ -125,31 +132,69 @@ aefdtd_batch::~aefdtd_batch() {
     if (stream) cudaStreamDestroy(stream);
 }
 
-// Subsets: active members grouped by size class, packed in member order up to
-// the L2 budget (a member larger than the budget gets a subset of its own).
-void aefdtd_batch::layout() {
-    drop_layout();
-    std::map<int, std::vector<int>> by_class;
-    for (size_t i = 0; i < members.size(); i++)
-        if (members[i].remaining > 0) by_class[members[i].cls].push_back((int)i);
-    for (auto &kv : by_class) {
-        BatchSubset cur;
-        cur.cls = kv.first;
-        for (int i : kv.second) {
-            const size_t b = members[i].sim->dev_bytes;
-            if (!cur.members.empty() && (l2_budget > 0 && (long long)(cur.bytes + b) > l2_budget)) {
-                subsets.push_back(std::move(cur));
-                cur = BatchSubset();
-                cur.cls = kv.first;
-            }
-            cur.members.push_back(i);
-            cur.bytes += b;
-            const aefdtd_sim *s = members[i].sim;
-            cur.cells += (long long)s->Nx * s->Ny * s->Nz;
+// A member joins the last subset of its class that still fits the L2 budget,
+// else a new subset (a member larger than the budget gets one of its own).
+void aefdtd_batch::place(BatchMember &m) {
+    const size_t b = m.sim->dev_bytes;
+    BatchSubset *dst = nullptr;
+    for (auto it = subsets.rbegin(); it != subsets.rend(); ++it)
+        if (it->cls == m.cls) {
+            if (fits(*it, b)) dst = &*it;
+            break;
         }
-        if (!cur.members.empty()) subsets.push_back(std::move(cur));
+    if (!dst) {
+        subsets.emplace_back();
+        dst = &subsets.back();
+        dst->cls = m.cls;
     }
-    layout_dirty = false;
+    dst->release(dev_bytes);
+    dst->members.push_back(m.sim);
+    dst->bytes += b;
+    m.placed = true;
+}
+
+// Subsets follow membership incrementally: members out of budget (or gone)
+// leave their subset, new members are placed; only touched subsets are
+// rebuilt (and their graphs re-captured). layout_dirty forces a full layout in
+// member order, grouped by size class.
+void aefdtd_batch::update_layout() {
+    if (layout_dirty) {
+        for (auto &u : subsets) u.release(dev_bytes);
+        subsets.clear();
+        for (auto &m : members) m.placed = false;
+        layout_dirty = false;
+    }
+    for (auto &u : subsets) {
+        std::vector<aefdtd_sim *> keep;
+        size_t bytes = 0;
+        for (aefdtd_sim *s : u.members) {
+            const int i = find(s);
+            if (i >= 0 && members[i].remaining > 0) {
+                keep.push_back(s);
+                bytes += s->dev_bytes;
+            } else if (i >= 0) {
+                members[i].placed = false;
+            }
+        }
+        if (keep.size() != u.members.size()) {
+            u.release(dev_bytes);
+            u.members = keep;
+            u.bytes = bytes;
+        }
+    }
+    for (size_t k = 0; k < subsets.size();) {
+        if (subsets[k].members.empty()) {
+            subsets[k].release(dev_bytes);
+            subsets.erase(subsets.begin() + k);
+        } else {
+            k++;
+        }
+    }
+    std::map<int, std::vector<int>> fresh;   // by class, in member order
+    for (size_t i = 0; i < members.size(); i++)
+        if (members[i].remaining > 0 && !members[i].placed) fresh[members[i].cls].push_back((int)i);
+    for (auto &kv : fresh)
+        for (int i : kv.second) place(members[i]);
 }
 
 // Work lists and argument arrays of one subset (both table slots).
@@ -164,7 +209,7 @@ template <typename T, typename Tid> void aefdtd_batch::build_subset(BatchSubset 
         for (int g = 0; g < kGroups; g++) {
             w.off[g] = (int)(all.size() / 4);
             for (size_t li = 0; li < u.members.size(); li++) {
-                aefdtd_sim *s = members[u.members[li]].sim;
+                aefdtd_sim *s = u.members[li];
                 const WorkSplit &mw = half == 0 ? s->wsE : s->wsH;
                 w.unroll = mw.unroll;
                 for (int k = 0; k < mw.n[g]; k++) {
@@ -187,7 +232,7 @@ template <typename T, typename Tid> void aefdtd_batch::build_subset(BatchSubset 
         std::vector<StepArgs<T, Tid>> ea(n), ha(n);
         std::vector<SensorStepArgs<T>> sa(n);
         for (size_t li = 0; li < n; li++) {
-            aefdtd_sim *s = members[u.members[li]].sim;
+            aefdtd_sim *s = u.members[li];
             const StepScalars *tbl = s->tables.as<StepScalars>() + size_t(sl) * s->seg_len;
             s->make_step_args(ea[li], ha[li], tbl);
             s->make_sensor_args(sa[li], tbl);
@@ -261,10 +306,9 @@ template <typename T, typename Tid> void aefdtd_batch::enqueue_segment(BatchSubs
 // captured graph (full segments) or direct launches; then the members' clocks.
 template <typename T, typename Tid> void aefdtd_batch::run_segment(BatchSubset &u, int L) {
     if (!u.built) build_subset<T, Tid>(u);
-    const int sl = slot;
+    const int sl = u.slot;
     std::vector<StepScalars> host(seg_len);
-    for (int i : u.members) {
-        aefdtd_sim *s = members[i].sim;
+    for (aefdtd_sim *s : u.members) {
         for (int q = 0; q < L; q++) s->fill_scalars(s->tstep + q, q, host[q]);
         AE_CUDA(cudaMemcpyAsync(s->tables.as<StepScalars>() + size_t(sl) * s->seg_len, host.data(),
                                 sizeof(StepScalars) * L, cudaMemcpyHostToDevice, stream));
@@ -286,65 +330,66 @@ template <typename T, typename Tid> void aefdtd_batch::run_segment(BatchSubset &
     } else {
         enqueue_segment<T, Tid>(u, L, sl);
     }
-    for (int i : u.members) {
-        aefdtd_sim *s = members[i].sim;
+    u.slot ^= 1;
+    for (aefdtd_sim *s : u.members) {
         s->tstep += L;
         for (auto &o : s->oscs) o.step += L;
-        members[i].remaining -= L;
+        rec(s).remaining -= L;
     }
 }
 
-// Runs segments until max_steps steps have passed or no member is active;
-// stops after the segment in which a member finishes. Returns the steps run.
+// Plane-sum history for every member's whole budget, so that captured graphs
+// keep valid pointers (a reallocation rebuilds the member's subset).
+template <typename T, typename Tid> void aefdtd_batch::ensure_history() {
+    for (auto &u : subsets)
+        for (aefdtd_sim *s : u.members) {
+            const BatchMember &m = rec(s);
+            if (!s->normal || s->tstep + m.remaining <= s->psums_cap) continue;
+            DBuf nb;
+            const int cap = s->tstep + m.remaining;
+            nb.alloc(size_t(cap) * 12 * 8, s->dev_bytes);
+            if (s->psums.p)
+                AE_CUDA(cudaMemcpy(nb.p, s->psums.p, size_t(s->psums_cap) * 12 * 8, cudaMemcpyDeviceToDevice));
+            s->psums.release(s->dev_bytes);
+            s->psums = nb;
+            s->psums_cap = cap;
+            s->graphs_dirty = true;
+            u.release(dev_bytes);
+        }
+}
+
+// Each subset runs up to max_steps steps in segments of at most seg_len, and
+// stops after the segment in which one of its members uses up its budget.
+// Subsets run one after another. Returns the most steps any subset ran.
 template <typename T, typename Tid> int aefdtd_batch::advance(int max_steps) {
-    int done = 0;
-    while (done < max_steps) {
-        int L = std::min(seg_len, max_steps - done);
-        bool any = false;
-        for (auto &m : members)
-            if (m.remaining > 0) { L = std::min(L, m.remaining); any = true; }
-        if (!any) break;
-        if (layout_dirty) layout();
-        for (auto &m : members) {
-            if (m.remaining <= 0) continue;
-            aefdtd_sim *s = m.sim;
-            // plane-sum history for the whole budget, so captured graphs keep valid pointers
-            if (s->normal && s->tstep + m.remaining > s->psums_cap) {
-                DBuf nb;
-                const int cap = s->tstep + m.remaining;
-                nb.alloc(size_t(cap) * 12 * 8, s->dev_bytes);
-                if (s->psums.p)
-                    AE_CUDA(cudaMemcpy(nb.p, s->psums.p, size_t(s->psums_cap) * 12 * 8, cudaMemcpyDeviceToDevice));
-                s->psums.release(s->dev_bytes);
-                s->psums = nb;
-                s->psums_cap = cap;
-                s->graphs_dirty = true;
-                for (auto &u : subsets) u.release(dev_bytes);
-            }
+    update_layout();
+    ensure_history<T, Tid>();
+    int most = 0;
+    for (auto &u : subsets) {
+        int done = 0;
+        while (done < max_steps) {
+            int L = std::min(seg_len, max_steps - done);
+            for (aefdtd_sim *s : u.members) L = std::min(L, rec(s).remaining);
+            if (L <= 0) break;
+            run_segment<T, Tid>(u, L);
+            done += L;
+            bool finished = false;
+            for (aefdtd_sim *s : u.members) finished |= rec(s).remaining == 0;
+            if (finished) break;
         }
-        for (auto &u : subsets) run_segment<T, Tid>(u, L);
-        slot ^= 1;
-        done += L;
-        bool finished = false;   // a member of the current layout reached its budget
-        for (auto &u : subsets)
-            for (int i : u.members) finished |= members[i].remaining == 0;
-        if (finished) {
-            // members that reached their budget leave the layout
-            layout_dirty = true;
-            break;
-        }
+        most = std::max(most, done);
     }
     AE_CUDA(cudaStreamSynchronize(stream));
     AE_CUDA(cudaGetLastError());
-    return done;
+    return most;
 }
 
 // Device seconds of `reps` full segments of every subset, after one warm-up
-// segment (which also captures the graphs of its slot; the timed segments use
-// the same slot).
+// segment per table slot (which captures the graphs).
 template <typename T, typename Tid> double aefdtd_batch::time_segments(int reps) {
-    if (layout_dirty) layout();
-    for (auto &u : subsets) run_segment<T, Tid>(u, seg_len);   // capture + warm
+    update_layout();
+    for (int w = 0; w < 2; w++)
+        for (auto &u : subsets) run_segment<T, Tid>(u, seg_len);
     cudaEvent_t a, b;
     AE_CUDA(cudaEventCreate(&a));
     AE_CUDA(cudaEventCreate(&b));
@@ -371,8 +416,8 @@ template <typename T, typename Tid> void aefdtd_batch::autotune() {
         saved[i] = members[i].remaining;
     }
     const long long budget0 = l2_budget;
-    // every trial restarts the members at step 0 and runs two segments: the
-    // plane-sum history must hold them (three, with margin)
+    // every trial restarts the members at step 0 and runs three segments: the
+    // plane-sum history must hold them
     for (auto &m : members) {
         aefdtd_sim *s = m.sim;
         if (s->normal && s->psums_cap < 3 * seg_len) {
@@ -385,6 +430,7 @@ template <typename T, typename Tid> void aefdtd_batch::autotune() {
     auto restart = [&] {
         AE_CUDA(cudaStreamSynchronize(stream));
         for (auto &m : members) m.sim->zero_state();
+        for (auto &u : subsets) u.slot = 0;
     };
     auto apply = [&](int cls, const SizeClass &c) {
         classes[cls] = c;
@@ -400,7 +446,7 @@ template <typename T, typename Tid> void aefdtd_batch::autotune() {
     for (auto &kv : classes) keys.push_back(kv.first);
     for (int cls : keys) {
         // only this class's members take part in its trials
-        for (size_t i = 0; i < members.size(); i++) members[i].remaining = members[i].cls == cls ? (1 << 30) : 0;
+        for (auto &m : members) m.remaining = m.cls == cls ? (1 << 30) : 0;
         double best = 1e30;
         SizeClass pick = classes[cls];
         for (int ty : {2, 4, 8})
@@ -415,7 +461,7 @@ template <typename T, typename Tid> void aefdtd_batch::autotune() {
         apply(cls, pick);
     }
     // L2 budget over all members
-    for (size_t i = 0; i < members.size(); i++) members[i].remaining = 1 << 30;
+    for (auto &m : members) m.remaining = 1 << 30;
     double best = 1e30;
     long long pick = budget0;
     for (long long b : {48LL << 20, 96LL << 20, -1LL}) {
@@ -431,10 +477,6 @@ template <typename T, typename Tid> void aefdtd_batch::autotune() {
     for (size_t i = 0; i < members.size(); i++) members[i].remaining = saved[i];
 }
 
-// ------------------------------------------------------------------------
-// C ABI
-// ------------------------------------------------------------------------
-
 namespace aefdtd {
 void batch_detach(void *bp, aefdtd_sim *s) {
     auto *b = static_cast<aefdtd_batch *>(bp);
@@ -442,11 +484,23 @@ void batch_detach(void *bp, aefdtd_sim *s) {
     if (i < 0) return;
     b->set_device();
     cudaStreamSynchronize(b->stream);
+    for (auto &u : b->subsets) {
+        auto it = std::find(u.members.begin(), u.members.end(), s);
+        if (it != u.members.end()) {
+            u.release(b->dev_bytes);
+            u.members.erase(it);
+            u.bytes -= s->dev_bytes;
+        }
+    }
     b->members.erase(b->members.begin() + i);
-    b->drop_layout();
     s->batch = nullptr;
 }
 }  // namespace aefdtd
+
+// ------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------
+
 
 template <typename F> static aefdtd_status bguarded(aefdtd_batch *b, F &&f) {
     try {
@@ -559,7 +613,6 @@ aefdtd_status aefdtd_batch_add(aefdtd_batch *b, aefdtd_sim *s, int32_t steps) {
         }
         s->batch = b;
         b->members.push_back(m);
-        b->layout_dirty = true;
     });
 }
 
@@ -578,7 +631,6 @@ aefdtd_status aefdtd_batch_set_budget(aefdtd_batch *b, aefdtd_sim *s, int32_t st
         if (i < 0) fail(AEFDTD_BAD_ARG, "not a member of this batch");
         if (steps < 0) fail(AEFDTD_BAD_ARG, "negative step budget");
         b->members[i].remaining = steps;
-        b->layout_dirty = true;
     });
 }
 
@@ -624,7 +676,7 @@ aefdtd_status aefdtd_batch_finished(aefdtd_batch *b, aefdtd_sim **out, int32_t c
 aefdtd_status aefdtd_batch_get_info(aefdtd_batch *b, aefdtd_batch_info *info) {
     if (!b || !info) return AEFDTD_BAD_ARG;
     return bguarded(b, [&] {
-        if (b->layout_dirty && b->typed) b->layout();
+        if (b->typed) b->update_layout();
         std::memset(info, 0, sizeof(*info));
         info->n_members = (int32_t)b->members.size();
         for (auto &m : b->members) {

@@ -279,3 +279,96 @@ class Batch:
                 "l2_budget_bytes": i.l2_budget_bytes, "launches": i.launches,
                 "classes": [{"key": i.class_key[c], "tile_y": i.class_tile_y[c], "kchunk": i.class_kchunk[c]}
                             for c in range(k)]}
+
+
+class Server:
+    """The serving loop (include/aefdtd.h, aefdtd_server_*): jobs queue on the
+    host, are admitted by device-memory footprint against a budget (80% of
+    HBM by default), run as members of one batch and retire when done."""
+
+    def __init__(self, hbm_fraction=0.0, budget_bytes=0, max_active=0, segment_steps=0, lookahead=0,
+                 l2_budget_bytes=0, tile_y=0, kchunk=0, device=0):
+        self._lib = load()
+        o = A.ServerOpts()
+        o.abi_version = A.ABI_VERSION
+        o.device = device
+        o.hbm_fraction = float(hbm_fraction)
+        o.budget_bytes = int(budget_bytes)
+        o.max_active, o.segment_steps, o.lookahead = int(max_active), int(segment_steps), int(lookahead)
+        o.batch.l2_budget_bytes = int(l2_budget_bytes)
+        o.batch.tile_y, o.batch.kchunk = int(tile_y), int(kchunk)
+        self._h = C.c_void_p()
+        st = self._lib.aefdtd_server_create(C.byref(o), C.byref(self._h))
+        if st != 0:
+            raise AefdtdError(st, "aefdtd_server_create failed")
+        self.nl = {}
+
+    def _c(self, st):
+        if st != 0:
+            msg = self._lib.aefdtd_server_last_error(self._h)
+            raise AefdtdError(st, msg.decode() if msg else "")
+
+    def close(self):
+        if self._h:
+            self._lib.aefdtd_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def submit(self, scene, steps=None) -> int:
+        """Queues a normal-incidence Scene for `steps` steps (default its own)."""
+        m = np.ascontiguousarray(scene.map, dtype=np.uint32).ravel()
+        mats = (A.MaterialDesc * len(scene.materials))(*scene.materials)
+        g = scene.grid
+        nd = scene.normal
+        jd = A.JobDesc()
+        jd.grid = C.pointer(g)
+        jd.map = m.ctypes.data_as(C.POINTER(C.c_uint32))
+        jd.map_count = m.size
+        jd.materials = mats
+        jd.n_materials = len(scene.materials)
+        jd.normal = C.pointer(nd)
+        jd.steps = int(steps if steps is not None else scene.nsteps)
+        jid = C.c_int32(-1)
+        self._c(self._lib.aefdtd_server_submit(self._h, C.byref(jd), C.byref(jid)))
+        self.nl[jid.value] = nd.nl
+        return jid.value
+
+    def poll(self) -> int:
+        n = C.c_int32(0)
+        self._c(self._lib.aefdtd_server_poll(self._h, C.byref(n)))
+        return n.value
+
+    def info(self, job: int) -> dict:
+        i = A.JobInfo()
+        self._c(self._lib.aefdtd_server_job_info(self._h, int(job), C.byref(i)))
+        return {k: getattr(i, k) for k, _ in A.JobInfo._fields_}
+
+    def spectra(self, job: int) -> np.ndarray:
+        nl = self.nl[job]
+        out = np.empty(15 * nl)
+        self._c(self._lib.aefdtd_server_job_spectra(self._h, int(job), out.ctypes.data_as(C.POINTER(C.c_double)), nl))
+        return out.reshape(nl, 15)
+
+    def stats(self) -> dict:
+        s = A.ServerStats()
+        self._c(self._lib.aefdtd_server_get_stats(self._h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in A.ServerStats._fields_}
+
+    def drain(self, max_polls=10 ** 7):
+        """Polls until no job is queued or running."""
+        for _ in range(max_polls):
+            st = self.stats()
+            if st["queued"] == 0 and st["running"] == 0:
+                return
+            self.poll()

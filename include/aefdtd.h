@@ -308,14 +308,80 @@ aefdtd_status aefdtd_batch_set_budget(aefdtd_batch *batch, aefdtd_sim *sim, int3
  * segments on the device. Every member must be at step 0; members are reset
  * to step 0. */
 aefdtd_status aefdtd_batch_autotune(aefdtd_batch *batch);
-/* Advances the members with budget left, by at most max_steps steps, and
- * returns after the segment in which a member uses up its budget (so callers
- * can retire it and admit others). *steps_done: steps run. Waits for the
- * device before returning. */
+/* Advances every member with budget left by up to max_steps steps. Members
+ * run in subsets, one subset after another; a subset stops early, after the
+ * segment in which one of its members uses up its budget, so that callers can
+ * retire it and admit others between calls. *steps_done: the most steps any
+ * subset ran (0 when no member has budget left). Waits for the device before
+ * returning. */
 aefdtd_status aefdtd_batch_advance(aefdtd_batch *batch, int32_t max_steps, int32_t *steps_done);
 /* Members whose budget is used up: up to cap handles in out, count in *n. */
 aefdtd_status aefdtd_batch_finished(aefdtd_batch *batch, aefdtd_sim **out, int32_t cap, int32_t *n);
 aefdtd_status aefdtd_batch_get_info(aefdtd_batch *batch, aefdtd_batch_info *info);
+
+/* ---- serving: a request loop with continuous batching -----------------
+ *
+ * No reference counterpart (the reference runs one script per simulation).
+ * Jobs are normal-incidence cells with a step budget; they queue on the host
+ * and are admitted, in arrival order, while their estimated device footprint
+ * fits the memory budget; admitted jobs run as members of one batch and are
+ * retired (spectra kept, device memory freed) as soon as their budget is
+ * used. A job's spectra are the same alone and in any mix. */
+typedef struct aefdtd_server aefdtd_server;
+
+enum { AEFDTD_JOB_QUEUED = 0, AEFDTD_JOB_RUNNING = 1, AEFDTD_JOB_DONE = 2, AEFDTD_JOB_FAILED = 3 };
+
+typedef struct aefdtd_server_opts {
+    int32_t abi_version;      /* = AEFDTD_ABI_VERSION */
+    int32_t device;
+    double hbm_fraction;      /* memory budget as a fraction of device memory; 0 -> 0.8 */
+    int64_t budget_bytes;     /* > 0: explicit budget instead of hbm_fraction */
+    int32_t max_active;       /* 0: no limit on running jobs */
+    int32_t segment_steps;    /* steps per poll; 0 -> 64 */
+    int32_t lookahead;        /* queued jobs that may pass one that does not fit; 0 -> 16 */
+    int32_t reserved;
+    aefdtd_batch_opts batch;  /* options of the batch (abi_version and device are set by the server) */
+} aefdtd_server_opts;
+
+typedef struct aefdtd_job_desc {
+    const aefdtd_grid_desc *grid;           /* mode must be AEFDTD_MODE_NORMAL */
+    const uint32_t *map;                    /* nx*ny*nz structure map, x fastest */
+    size_t map_count;
+    const aefdtd_material_desc *materials;  /* indexed by the map */
+    int32_t n_materials;
+    const aefdtd_normal_desc *normal;
+    int32_t steps;
+} aefdtd_job_desc;
+
+typedef struct aefdtd_job_info {
+    int32_t state;            /* AEFDTD_JOB_* */
+    int32_t steps;
+    int64_t cells;            /* total grid cells (after admission) */
+    int64_t est_bytes;        /* footprint estimate used for admission */
+    int64_t bytes;            /* device bytes held while running */
+    double t_submit, t_admit, t_done;   /* seconds since server creation; -1 if not yet */
+} aefdtd_job_info;
+
+typedef struct aefdtd_server_stats {
+    int32_t submitted, queued, running, done, failed, reserved;
+    int64_t budget_bytes, in_use_bytes, peak_bytes;
+    double p50_s, p99_s, mean_s;   /* time to spectrum (submit -> done) of done jobs */
+    double elapsed_s;              /* first submit -> last done */
+    double sims_per_s, gcells_per_s;
+} aefdtd_server_stats;
+
+aefdtd_status aefdtd_server_create(const aefdtd_server_opts *opts, aefdtd_server **out);
+aefdtd_status aefdtd_server_destroy(aefdtd_server *server);
+const char *aefdtd_server_last_error(const aefdtd_server *server);
+/* Copies the job description; no device work. */
+aefdtd_status aefdtd_server_submit(aefdtd_server *server, const aefdtd_job_desc *job, int32_t *job_id);
+/* Retires finished jobs, admits queued ones, advances one segment; *n_done:
+ * jobs finished during the call. */
+aefdtd_status aefdtd_server_poll(aefdtd_server *server, int32_t *n_done);
+aefdtd_status aefdtd_server_job_info(aefdtd_server *server, int32_t job, aefdtd_job_info *info);
+/* The 15-column spectra of a done job, as aefdtd_get_normal_spectra. */
+aefdtd_status aefdtd_server_job_spectra(aefdtd_server *server, int32_t job, double *out, int32_t nl);
+aefdtd_status aefdtd_server_get_stats(aefdtd_server *server, aefdtd_server_stats *stats);
 
 /* ---- allocation-free diagnostics -------------------------------------- */
 

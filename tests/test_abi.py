@@ -162,3 +162,30 @@ def test_cpp_shim_compiles_and_reports_no_device_without_gpu():
             pytest.skip("GPU present: covered by the gpu test")
         out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout
         assert out.startswith("error 6"), out
+
+
+def test_batch_and_server_struct_layouts_match_header():
+    src = """
+#include <stdio.h>
+#include <stddef.h>
+#include "aefdtd.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(aefdtd_batch_opts), sizeof(aefdtd_batch_info),
+         sizeof(aefdtd_server_opts), sizeof(aefdtd_job_desc), sizeof(aefdtd_job_info), sizeof(aefdtd_server_stats));
+  printf("%zu %zu %zu %zu\\n", offsetof(aefdtd_batch_info, class_kchunk), offsetof(aefdtd_server_opts, batch),
+         offsetof(aefdtd_job_desc, steps), offsetof(aefdtd_server_stats, gcells_per_s));
+  return 0;
+}
+"""
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "t.c")
+        open(c, "w").write(src)
+        exe = os.path.join(d, "t")
+        subprocess.run(["gcc", "-std=c11", "-I", os.path.dirname(HEADER), c, "-o", exe], check=True)
+        lines = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split("\n")
+    sizes = [int(x) for x in lines[0].split()]
+    offs = [int(x) for x in lines[1].split()]
+    assert sizes == [C.sizeof(A.BatchOpts), C.sizeof(A.BatchInfo), C.sizeof(A.ServerOpts), C.sizeof(A.JobDesc),
+                     C.sizeof(A.JobInfo), C.sizeof(A.ServerStats)]
+    assert offs == [A.BatchInfo.class_kchunk.offset, A.ServerOpts.batch.offset, A.JobDesc.steps.offset,
+                    A.ServerStats.gcells_per_s.offset]

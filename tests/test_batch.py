@@ -54,29 +54,26 @@ def test_fp64_batch_members_bit_identical_to_alone(opts):
         s.close()
 
 
-def test_uneven_budgets_finish_exactly_and_batch_stops_at_each_finish():
+def test_uneven_budgets_finish_exactly():
+    """Members with different budgets (one subset and several): each stops at
+    exactly its budget, and its results equal its run alone."""
     scenes = cells(5, n=3)
     budgets = [70, 130, 200]
     want = [alone(sc, n) for sc, n in zip(scenes, budgets)]
-    sims = [fdtd.build_simulation(sc) for sc in scenes]
-    with fdtd.Batch() as b:
-        for s, n in zip(sims, budgets):
-            b.add(s, n)
-        stops = []
-        total = 0
-        while True:
-            n = b.advance(10 ** 6)
-            if n == 0:
-                break
-            total += n
-            stops.append(total)
-        assert stops == budgets
-        for s, n, (f, p) in zip(sims, budgets, want):
-            assert s.dims().step == n
-            assert np.array_equal(s.fields(), f)
-            assert np.array_equal(s.plane_sums(), p)
-    for s in sims:
-        s.close()
+    for budget in (-1, 1):
+        sims = [fdtd.build_simulation(sc) for sc in scenes]
+        with fdtd.Batch(l2_budget_bytes=budget) as b:
+            for s, n in zip(sims, budgets):
+                b.add(s, n)
+            while b.advance(64) > 0:
+                pass
+            assert len(b.finished()) == 3
+            for s, n, (f, p) in zip(sims, budgets, want):
+                assert s.dims().step == n
+                assert np.array_equal(s.fields(), f)
+                assert np.array_equal(s.plane_sums(), p)
+        for s in sims:
+            s.close()
 
 
 def test_members_join_and_leave_between_segments():
