@@ -9,16 +9,20 @@
 //    depth (planes per work item), set by hand or by the autotuner, which
 //    times trial segments of the class's members for every candidate.
 //  * Subsets. Within a class, members are packed into subsets whose device
-//    state fits an L2 budget (126 MB of L2 on B200; the budget is tuned too).
+//    state fits an L2 budget (126 MB of L2 on B200; default 48 MiB, tuned).
 //    A subset runs a whole segment of steps before the next subset starts, so
-//    after its first step most of its state is served from L2.
+//    after its first step most of its state is served from L2. Lanes run that
+//    many subsets concurrently (default 1: measured on 32 config-4 cells, one
+//    resident cell at a time beats two or more sharing L2, 45.8 vs 42.0
+//    Gcell/s, and beats merged 5-cell subsets, 37.3 Gcell/s).
 //  * Merged launches. Per step, each work-item group of a subset (interior,
 //    z-CPML, dispersive, general) is ONE launch over the items of all its
 //    members: items carry the member index and the kernels read that member's
 //    arguments from a device array. Boundary groups run on side streams beside
 //    the interior group; the plane sums of all normal-mode members are one
-//    launch beside the H half-step. A full segment (64 steps) of a subset is
-//    captured once per table slot as a CUDA graph and replayed.
+//    launch beside the H half-step. A chunk of 16 steps of a subset is
+//    captured once as a CUDA graph and replayed for every full chunk (the
+//    members' scalar tables are uploaded before each replay).
 //  * Step budgets. Each member has a number of steps still to run; a segment
 //    never passes a member's budget, so members finish exactly and can be
 //    retired and replaced between segments (continuous batching).
@@ -27,6 +31,8 @@
 // exactly the kernels' arithmetic of a single simulation (FP64 fields are
 // bit-identical to stepping it alone).
 #include "sim.hpp"
+
+#include <chrono>
 
 
 namespace aefdtd {
@@ -44,20 +50,17 @@ struct BatchSubset {
     size_t bytes = 0;              // device state of the members
     DBuf items;                    // merged items: E groups, then H groups
     WorkSplit wsE{}, wsH{};
-    DBuf argsE[2], argsH[2], sargs[2];   // per table slot
+    DBuf argsE, argsH, sargs;      // per-member arguments (members' table slot 0)
     DBuf blkmap;
     int nblk = 0;
     int nplane = 0;                // members with plane sums
-    int slot = 0;                  // table slot of the next segment
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t graph = nullptr;   // one chunk of graph_steps steps
     uint64_t graph_launches = 0;
     bool built = false;
     void release(size_t &t) {
         items.release(t);
-        for (int k = 0; k < 2; k++) {
-            argsE[k].release(t); argsH[k].release(t); sargs[k].release(t);
-            if (graph[k]) { cudaGraphExecDestroy(graph[k]); graph[k] = nullptr; }
-        }
+        argsE.release(t); argsH.release(t); sargs.release(t);
+        if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
         blkmap.release(t);
         built = false;
     }
@@ -67,6 +70,33 @@ struct SizeClass {
     int tile_y = 4;
     int kchunk = 0;   // 0: the simulation's own heuristic
 };
+
+// A lane: the streams and events one subset at a time runs on. Subsets on
+// different lanes run concurrently.
+struct Lane {
+    cudaStream_t stream = nullptr, side[kGroups - 1] = {}, side_s = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join[kGroups - 1] = {}, ev_sf = nullptr, ev_sj = nullptr;
+    void create() {
+        AE_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        for (auto &x : side) AE_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+        AE_CUDA(cudaStreamCreateWithFlags(&side_s, cudaStreamNonBlocking));
+        AE_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+        for (auto &e : ev_join) AE_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        AE_CUDA(cudaEventCreateWithFlags(&ev_sf, cudaEventDisableTiming));
+        AE_CUDA(cudaEventCreateWithFlags(&ev_sj, cudaEventDisableTiming));
+    }
+    void destroy() {
+        if (stream) cudaStreamSynchronize(stream);
+        for (auto &e : ev_join) if (e) cudaEventDestroy(e);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_sf) cudaEventDestroy(ev_sf);
+        if (ev_sj) cudaEventDestroy(ev_sj);
+        for (auto &x : side) if (x) cudaStreamDestroy(x);
+        if (side_s) cudaStreamDestroy(side_s);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+constexpr int kMaxLanes = 8;
 
 }  // namespace aefdtd
 
@@ -78,13 +108,15 @@ struct aefdtd_batch {
     int device = 0;
     bool typed = false, fp64 = false;
     int id_bytes = 1, seg_len = 64;
-    cudaStream_t stream = nullptr, side[kGroups - 1] = {}, side_s = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join[kGroups - 1] = {}, ev_sf = nullptr, ev_sj = nullptr;
+    Lane lanes[kMaxLanes];
+    int n_lanes = 1;               // subsets running concurrently
+    cudaStream_t stream = nullptr; // lanes[0].stream
     std::vector<BatchMember> members;
     std::vector<BatchSubset> subsets;
     std::map<int, SizeClass> classes;
     bool layout_dirty = true;
-    long long l2_budget = 96LL << 20;
+    long long l2_budget = 48LL << 20;
+    int graph_steps = 16;          // steps per captured chunk (a divisor of seg_len)
     uint64_t launches = 0;
     size_t dev_bytes = 0;
 
@@ -108,28 +140,25 @@ struct aefdtd_batch {
     void place(BatchMember &m);
     void update_layout();
     template <typename T, typename Tid> void build_subset(BatchSubset &u);
-    template <typename T, typename Tid> void enqueue_segment(BatchSubset &u, int L, int sl);
-    template <typename T, typename Tid> void run_segment(BatchSubset &u, int L);
+    template <typename T, typename Tid> void enqueue_steps(BatchSubset &u, int L, Lane &ln);
+    template <typename T, typename Tid> void run_segment(BatchSubset &u, int L, Lane &ln);
+    void sync_lanes() {
+        for (int k = 0; k < n_lanes; k++) AE_CUDA(cudaStreamSynchronize(lanes[k].stream));
+    }
     template <typename T, typename Tid> void ensure_history();
     template <typename T, typename Tid> int advance(int max_steps);
     template <typename T, typename Tid> double time_segments(int reps);
     template <typename T, typename Tid> void autotune();
-    template <typename Launch> void run_groups(const WorkSplit &w, Launch &&launch);
+    template <typename Launch> void run_groups(const WorkSplit &w, Lane &ln, Launch &&launch);
     ~aefdtd_batch();
 };
 
 aefdtd_batch::~aefdtd_batch() {
     set_device();
-    if (stream) cudaStreamSynchronize(stream);
+    for (auto &ln : lanes) if (ln.stream) cudaStreamSynchronize(ln.stream);
     for (auto &m : members) m.sim->batch = nullptr;
     for (auto &u : subsets) u.release(dev_bytes);
-    for (auto &e : ev_join) if (e) cudaEventDestroy(e);
-    if (ev_fork) cudaEventDestroy(ev_fork);
-    if (ev_sf) cudaEventDestroy(ev_sf);
-    if (ev_sj) cudaEventDestroy(ev_sj);
-    for (auto &x : side) if (x) cudaStreamDestroy(x);
-    if (side_s) cudaStreamDestroy(side_s);
-    if (stream) cudaStreamDestroy(stream);
+    for (auto &ln : lanes) ln.destroy();
 }
 
 // A member joins the last subset of its class that still fits the L2 budget,
@@ -197,7 +226,7 @@ void aefdtd_batch::update_layout() {
         for (int i : kv.second) place(members[i]);
 }
 
-// Work lists and argument arrays of one subset (both table slots).
+// Work lists and argument arrays of one subset.
 template <typename T, typename Tid> void aefdtd_batch::build_subset(BatchSubset &u) {
     u.release(dev_bytes);
     const SizeClass &sc = classes[u.cls];
@@ -228,26 +257,24 @@ template <typename T, typename Tid> void aefdtd_batch::build_subset(BatchSubset 
     const size_t n = u.members.size();
     std::vector<int2> blk;
     u.nplane = 0;
-    for (int sl = 0; sl < 2; sl++) {
-        std::vector<StepArgs<T, Tid>> ea(n), ha(n);
-        std::vector<SensorStepArgs<T>> sa(n);
-        for (size_t li = 0; li < n; li++) {
-            aefdtd_sim *s = u.members[li];
-            const StepScalars *tbl = s->tables.as<StepScalars>() + size_t(sl) * s->seg_len;
-            s->make_step_args(ea[li], ha[li], tbl);
-            s->make_sensor_args(sa[li], tbl);
-            if (sl == 0 && sa[li].nbp > 0) {
-                u.nplane++;
-                for (int b = 0; b < sa[li].nbp; b++) blk.push_back(make_int2((int)li, b));
-            }
+    std::vector<StepArgs<T, Tid>> ea(n), ha(n);
+    std::vector<SensorStepArgs<T>> sa(n);
+    for (size_t li = 0; li < n; li++) {
+        aefdtd_sim *s = u.members[li];
+        const StepScalars *tbl = s->tables.as<StepScalars>();
+        s->make_step_args(ea[li], ha[li], tbl);
+        s->make_sensor_args(sa[li], tbl);
+        if (sa[li].nbp > 0) {
+            u.nplane++;
+            for (int b = 0; b < sa[li].nbp; b++) blk.push_back(make_int2((int)li, b));
         }
-        u.argsE[sl].alloc(sizeof(StepArgs<T, Tid>) * n, dev_bytes);
-        u.argsH[sl].alloc(sizeof(StepArgs<T, Tid>) * n, dev_bytes);
-        u.sargs[sl].alloc(sizeof(SensorStepArgs<T>) * n, dev_bytes);
-        AE_CUDA(cudaMemcpy(u.argsE[sl].p, ea.data(), sizeof(StepArgs<T, Tid>) * n, cudaMemcpyHostToDevice));
-        AE_CUDA(cudaMemcpy(u.argsH[sl].p, ha.data(), sizeof(StepArgs<T, Tid>) * n, cudaMemcpyHostToDevice));
-        AE_CUDA(cudaMemcpy(u.sargs[sl].p, sa.data(), sizeof(SensorStepArgs<T>) * n, cudaMemcpyHostToDevice));
     }
+    u.argsE.alloc(sizeof(StepArgs<T, Tid>) * n, dev_bytes);
+    u.argsH.alloc(sizeof(StepArgs<T, Tid>) * n, dev_bytes);
+    u.sargs.alloc(sizeof(SensorStepArgs<T>) * n, dev_bytes);
+    AE_CUDA(cudaMemcpy(u.argsE.p, ea.data(), sizeof(StepArgs<T, Tid>) * n, cudaMemcpyHostToDevice));
+    AE_CUDA(cudaMemcpy(u.argsH.p, ha.data(), sizeof(StepArgs<T, Tid>) * n, cudaMemcpyHostToDevice));
+    AE_CUDA(cudaMemcpy(u.sargs.p, sa.data(), sizeof(SensorStepArgs<T>) * n, cudaMemcpyHostToDevice));
     u.nblk = (int)blk.size();
     u.blkmap.alloc(std::max<size_t>(blk.size(), 1) * sizeof(int2), dev_bytes);
     if (!blk.empty()) AE_CUDA(cudaMemcpy(u.blkmap.p, blk.data(), blk.size() * sizeof(int2), cudaMemcpyHostToDevice));
@@ -255,86 +282,92 @@ template <typename T, typename Tid> void aefdtd_batch::build_subset(BatchSubset 
 }
 
 // Same fork/join scheme as a single simulation's half-step (runtime.cpp, run_groups).
-template <typename Launch> void aefdtd_batch::run_groups(const WorkSplit &w, Launch &&launch) {
+template <typename Launch> void aefdtd_batch::run_groups(const WorkSplit &w, Lane &ln, Launch &&launch) {
     int nside = 0;
     for (int g = 1; g < kGroups; g++) nside += w.n[g] > 0;
     if (nside == 0) {
-        launch(kGroupInterior, stream);
+        launch(kGroupInterior, ln.stream);
         return;
     }
-    AE_CUDA(cudaEventRecord(ev_fork, stream));
+    AE_CUDA(cudaEventRecord(ln.ev_fork, ln.stream));
     int si = 0;
     for (int g = 1; g < kGroups; g++) {
         if (w.n[g] <= 0) continue;
-        AE_CUDA(cudaStreamWaitEvent(side[si], ev_fork, 0));
-        launch(g, side[si]);
-        AE_CUDA(cudaEventRecord(ev_join[si], side[si]));
+        AE_CUDA(cudaStreamWaitEvent(ln.side[si], ln.ev_fork, 0));
+        launch(g, ln.side[si]);
+        AE_CUDA(cudaEventRecord(ln.ev_join[si], ln.side[si]));
         si++;
     }
-    launch(kGroupInterior, stream);
-    for (int k = 0; k < si; k++) AE_CUDA(cudaStreamWaitEvent(stream, ev_join[k], 0));
+    launch(kGroupInterior, ln.stream);
+    for (int k = 0; k < si; k++) AE_CUDA(cudaStreamWaitEvent(ln.stream, ln.ev_join[k], 0));
 }
 
-template <typename T, typename Tid> void aefdtd_batch::enqueue_segment(BatchSubset &u, int L, int sl) {
-    const auto *ea = u.argsE[sl].as<StepArgs<T, Tid>>();
-    const auto *ha = u.argsH[sl].as<StepArgs<T, Tid>>();
-    const auto *sa = u.sargs[sl].as<SensorStepArgs<T>>();
+// L steps whose scalars are in table entries 0..L-1 of every member.
+template <typename T, typename Tid> void aefdtd_batch::enqueue_steps(BatchSubset &u, int L, Lane &ln) {
+    const auto *ea = u.argsE.as<StepArgs<T, Tid>>();
+    const auto *ha = u.argsH.as<StepArgs<T, Tid>>();
+    const auto *sa = u.sargs.as<SensorStepArgs<T>>();
     const int4 *it = u.items.as<int4>();
     const int2 *blk = u.blkmap.as<int2>();
     int groups = 0;
     for (int g = 0; g < kGroups; g++) groups += (u.wsE.n[g] > 0) + (u.wsH.n[g] > 0);
     for (int q = 0; q < L; q++) {
-        run_groups(u.wsE, [&](int g, cudaStream_t st) { launch_e_group_batch(ea, q, it, u.wsE, g, st); });
+        run_groups(u.wsE, ln, [&](int g, cudaStream_t st) { launch_e_group_batch(ea, q, it, u.wsE, g, st); });
         // plane sums read E only: beside the H half-step
         if (u.nblk > 0) {
-            AE_CUDA(cudaEventRecord(ev_sf, stream));
-            AE_CUDA(cudaStreamWaitEvent(side_s, ev_sf, 0));
-            launch_plane_partial_batch(sa, blk, u.nblk, q, side_s);
-            AE_CUDA(cudaEventRecord(ev_sj, side_s));
+            AE_CUDA(cudaEventRecord(ln.ev_sf, ln.stream));
+            AE_CUDA(cudaStreamWaitEvent(ln.side_s, ln.ev_sf, 0));
+            launch_plane_partial_batch(sa, blk, u.nblk, q, ln.side_s);
+            AE_CUDA(cudaEventRecord(ln.ev_sj, ln.side_s));
         }
-        run_groups(u.wsH, [&](int g, cudaStream_t st) { launch_h_group_batch(ha, q, it, u.wsH, g, st); });
-        if (u.nblk > 0) AE_CUDA(cudaStreamWaitEvent(stream, ev_sj, 0));
+        run_groups(u.wsH, ln, [&](int g, cudaStream_t st) { launch_h_group_batch(ha, q, it, u.wsH, g, st); });
+        if (u.nblk > 0) AE_CUDA(cudaStreamWaitEvent(ln.stream, ln.ev_sj, 0));
         launches += groups + (u.nblk > 0);
     }
     if (u.nplane > 0) {
-        launch_plane_reduce_batch(sa, (int)u.members.size(), L, stream);
+        launch_plane_reduce_batch(sa, (int)u.members.size(), L, ln.stream);
         launches++;
     }
 }
 
-// One segment of L steps of a subset: per-member scalar tables, then the
-// captured graph (full segments) or direct launches; then the members' clocks.
-template <typename T, typename Tid> void aefdtd_batch::run_segment(BatchSubset &u, int L) {
+// L steps of a subset, in chunks: per chunk the members' scalar tables
+// (entries 0..), then either the subset's captured graph of graph_steps steps
+// (full chunks) or direct launches; then the members' clocks.
+template <typename T, typename Tid> void aefdtd_batch::run_segment(BatchSubset &u, int L, Lane &ln) {
     if (!u.built) build_subset<T, Tid>(u);
-    const int sl = u.slot;
     std::vector<StepScalars> host(seg_len);
-    for (aefdtd_sim *s : u.members) {
-        for (int q = 0; q < L; q++) s->fill_scalars(s->tstep + q, q, host[q]);
-        AE_CUDA(cudaMemcpyAsync(s->tables.as<StepScalars>() + size_t(sl) * s->seg_len, host.data(),
-                                sizeof(StepScalars) * L, cudaMemcpyHostToDevice, stream));
-    }
-    if (L == seg_len && opts.use_graphs >= 0) {
-        if (!u.graph[sl]) {
-            const uint64_t l0 = launches;
-            AE_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-            enqueue_segment<T, Tid>(u, L, sl);
-            cudaGraph_t gr = nullptr;
-            AE_CUDA(cudaStreamEndCapture(stream, &gr));
-            AE_CUDA(cudaGraphInstantiate(&u.graph[sl], gr, 0));
-            cudaGraphDestroy(gr);
-            u.graph_launches = launches - l0;
-            launches = l0;
+    int done = 0;
+    while (done < L) {
+        const bool graph = opts.use_graphs >= 0 && L - done >= graph_steps;
+        const int C = graph ? graph_steps : L - done;
+        for (aefdtd_sim *s : u.members) {
+            for (int q = 0; q < C; q++) s->fill_scalars(s->tstep + q, q, host[q]);
+            AE_CUDA(cudaMemcpyAsync(s->tables.as<StepScalars>(), host.data(), sizeof(StepScalars) * C,
+                                    cudaMemcpyHostToDevice, ln.stream));
         }
-        AE_CUDA(cudaGraphLaunch(u.graph[sl], stream));
-        launches += u.graph_launches;
-    } else {
-        enqueue_segment<T, Tid>(u, L, sl);
-    }
-    u.slot ^= 1;
-    for (aefdtd_sim *s : u.members) {
-        s->tstep += L;
-        for (auto &o : s->oscs) o.step += L;
-        rec(s).remaining -= L;
+        if (graph) {
+            if (!u.graph) {
+                const uint64_t l0 = launches;
+                AE_CUDA(cudaStreamBeginCapture(ln.stream, cudaStreamCaptureModeThreadLocal));
+                enqueue_steps<T, Tid>(u, C, ln);
+                cudaGraph_t gr = nullptr;
+                AE_CUDA(cudaStreamEndCapture(ln.stream, &gr));
+                AE_CUDA(cudaGraphInstantiate(&u.graph, gr, 0));
+                cudaGraphDestroy(gr);
+                u.graph_launches = launches - l0;
+                launches = l0;
+            }
+            AE_CUDA(cudaGraphLaunch(u.graph, ln.stream));
+            launches += u.graph_launches;
+        } else {
+            enqueue_steps<T, Tid>(u, C, ln);
+        }
+        for (aefdtd_sim *s : u.members) {
+            s->tstep += C;
+            for (auto &o : s->oscs) o.step += C;
+            rec(s).remaining -= C;
+        }
+        done += C;
     }
 }
 
@@ -364,45 +397,46 @@ template <typename T, typename Tid> void aefdtd_batch::ensure_history() {
 template <typename T, typename Tid> int aefdtd_batch::advance(int max_steps) {
     update_layout();
     ensure_history<T, Tid>();
+    // subsets round-robin over the lanes; each subset's segments are queued
+    // in turn (stream order within a lane, concurrency across lanes)
+    std::vector<int> done(subsets.size(), 0);
     int most = 0;
-    for (auto &u : subsets) {
-        int done = 0;
-        while (done < max_steps) {
-            int L = std::min(seg_len, max_steps - done);
+    bool more = true;
+    while (more) {
+        more = false;
+        for (size_t k = 0; k < subsets.size(); k++) {
+            BatchSubset &u = subsets[k];
+            if (done[k] < 0 || done[k] >= max_steps) continue;
+            int L = std::min(seg_len, max_steps - done[k]);
             for (aefdtd_sim *s : u.members) L = std::min(L, rec(s).remaining);
-            if (L <= 0) break;
-            run_segment<T, Tid>(u, L);
-            done += L;
+            if (L <= 0) { done[k] = -done[k] - 1; continue; }
+            run_segment<T, Tid>(u, L, lanes[k % n_lanes]);
+            done[k] += L;
+            most = std::max(most, done[k]);
             bool finished = false;
             for (aefdtd_sim *s : u.members) finished |= rec(s).remaining == 0;
-            if (finished) break;
+            if (finished) done[k] = -done[k] - 1;   // stops after this segment
+            else more = more || done[k] < max_steps;
         }
-        most = std::max(most, done);
     }
-    AE_CUDA(cudaStreamSynchronize(stream));
+    sync_lanes();
     AE_CUDA(cudaGetLastError());
     return most;
 }
 
 // Device seconds of `reps` full segments of every subset, after one warm-up
-// segment per table slot (which captures the graphs).
+// segment (which captures the graphs).
 template <typename T, typename Tid> double aefdtd_batch::time_segments(int reps) {
     update_layout();
-    for (int w = 0; w < 2; w++)
-        for (auto &u : subsets) run_segment<T, Tid>(u, seg_len);
-    cudaEvent_t a, b;
-    AE_CUDA(cudaEventCreate(&a));
-    AE_CUDA(cudaEventCreate(&b));
-    AE_CUDA(cudaEventRecord(a, stream));
+    for (size_t k = 0; k < subsets.size(); k++) run_segment<T, Tid>(subsets[k], seg_len, lanes[k % n_lanes]);
+    sync_lanes();
+    int a = 0, b = 0;   // host clock over all lanes (the device is idle before)
+    const auto t0 = std::chrono::steady_clock::now();
     for (int r = 0; r < reps; r++)
-        for (auto &u : subsets) run_segment<T, Tid>(u, seg_len);
-    AE_CUDA(cudaEventRecord(b, stream));
-    AE_CUDA(cudaEventSynchronize(b));
-    float ms = 0;
-    AE_CUDA(cudaEventElapsedTime(&ms, a, b));
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
-    return ms * 1e-3;
+        for (size_t k = 0; k < subsets.size(); k++) run_segment<T, Tid>(subsets[k], seg_len, lanes[k % n_lanes]);
+    sync_lanes();
+    (void)a; (void)b;
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
 // Per size class: tile height in {2, 4, 8} x z-block depth in {4, 8}, timed
@@ -416,8 +450,8 @@ template <typename T, typename Tid> void aefdtd_batch::autotune() {
         saved[i] = members[i].remaining;
     }
     const long long budget0 = l2_budget;
-    // every trial restarts the members at step 0 and runs three segments: the
-    // plane-sum history must hold them
+    // every trial restarts the members at step 0 and runs two segments: the
+    // plane-sum history must hold them (three, with margin)
     for (auto &m : members) {
         aefdtd_sim *s = m.sim;
         if (s->normal && s->psums_cap < 3 * seg_len) {
@@ -428,10 +462,9 @@ template <typename T, typename Tid> void aefdtd_batch::autotune() {
         }
     }
     auto restart = [&] {
-        AE_CUDA(cudaStreamSynchronize(stream));
+        sync_lanes();
         for (auto &m : members) m.sim->zero_state();
-        for (auto &u : subsets) u.slot = 0;
-    };
+        };
     auto apply = [&](int cls, const SizeClass &c) {
         classes[cls] = c;
         for (auto &m : members)
@@ -460,18 +493,23 @@ template <typename T, typename Tid> void aefdtd_batch::autotune() {
             }
         apply(cls, pick);
     }
-    // L2 budget over all members
+    // L2 budget and lanes over all members
     for (auto &m : members) m.remaining = 1 << 30;
     double best = 1e30;
     long long pick = budget0;
-    for (long long b : {48LL << 20, 96LL << 20, -1LL}) {
-        l2_budget = b;
-        drop_layout();
-        restart();
-        const double t = time_segments<T, Tid>(1);
-        if (t < best) { best = t; pick = b; }
-    }
+    int pick_lanes = n_lanes;
+    for (long long b : {48LL << 20, 96LL << 20, -1LL})
+        for (int nl : {1, 2, 4}) {
+            if (b < 0 && nl > 1) continue;   // one subset per class: lanes only split classes
+            l2_budget = b;
+            n_lanes = nl;
+            drop_layout();
+            restart();
+            const double t = time_segments<T, Tid>(1);
+            if (t < best) { best = t; pick = b; pick_lanes = nl; }
+        }
     l2_budget = pick;
+    n_lanes = pick_lanes;
     drop_layout();
     restart();
     for (size_t i = 0; i < members.size(); i++) members[i].remaining = saved[i];
@@ -483,7 +521,7 @@ void batch_detach(void *bp, aefdtd_sim *s) {
     const int i = b->find(s);
     if (i < 0) return;
     b->set_device();
-    cudaStreamSynchronize(b->stream);
+    for (int k = 0; k < b->n_lanes; k++) cudaStreamSynchronize(b->lanes[k].stream);
     for (auto &u : b->subsets) {
         auto it = std::find(u.members.begin(), u.members.end(), s);
         if (it != u.members.end()) {
@@ -542,18 +580,15 @@ aefdtd_status aefdtd_batch_create(const aefdtd_batch_opts *opts, aefdtd_batch **
             b->opts.abi_version = AEFDTD_ABI_VERSION;
         }
         if (b->opts.l2_budget_bytes != 0) b->l2_budget = b->opts.l2_budget_bytes;
+        if (b->opts.graph_steps > 0) b->graph_steps = b->opts.graph_steps;
         int ndev = 0;
         if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) fail(AEFDTD_NO_DEVICE, "no CUDA device visible");
         b->device = b->opts.device;
         if (b->device < 0 || b->device >= ndev) fail(AEFDTD_BAD_ARG, "device ordinal out of range");
         AE_CUDA(cudaSetDevice(b->device));
-        AE_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
-        for (auto &x : b->side) AE_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
-        AE_CUDA(cudaStreamCreateWithFlags(&b->side_s, cudaStreamNonBlocking));
-        AE_CUDA(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
-        for (auto &e : b->ev_join) AE_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        AE_CUDA(cudaEventCreateWithFlags(&b->ev_sf, cudaEventDisableTiming));
-        AE_CUDA(cudaEventCreateWithFlags(&b->ev_sj, cudaEventDisableTiming));
+        for (auto &ln : b->lanes) ln.create();
+        b->stream = b->lanes[0].stream;
+        if (b->opts.lanes > 0) b->n_lanes = std::min(b->opts.lanes, kMaxLanes);
     });
     if (st != AEFDTD_OK) {
         delete b;
@@ -589,6 +624,7 @@ aefdtd_status aefdtd_batch_add(aefdtd_batch *b, aefdtd_sim *s, int32_t steps) {
             b->fp64 = s->fp64;
             b->id_bytes = s->id_bytes;
             b->seg_len = s->seg_len;
+            b->graph_steps = std::max(1, std::min(b->graph_steps, b->seg_len));
         } else if (s->fp64 != b->fp64 || s->id_bytes != b->id_bytes || s->seg_len != b->seg_len) {
             fail(AEFDTD_BAD_ARG, "batch members share precision, material-id width and DFT block");
         }
@@ -687,6 +723,7 @@ aefdtd_status aefdtd_batch_get_info(aefdtd_batch *b, aefdtd_batch_info *info) {
             info->member_bytes += (int64_t)m.sim->dev_bytes;
         }
         info->n_subsets = (int32_t)b->subsets.size();
+        info->n_lanes = b->n_lanes;
         info->l2_budget_bytes = b->l2_budget;
         info->launches = b->launches;
         info->batch_bytes = (int64_t)b->dev_bytes;

@@ -195,7 +195,7 @@ class Batch:
     subset, one captured graph per subset and segment. Members are ordinary
     Simulations; the batch keeps references to them while they are members."""
 
-    def __init__(self, l2_budget_bytes=0, tile_y=0, kchunk=0, use_graphs=True, device=0):
+    def __init__(self, l2_budget_bytes=0, tile_y=0, kchunk=0, use_graphs=True, device=0, graph_steps=0, lanes=0):
         self._lib = load()
         o = A.BatchOpts()
         o.abi_version = A.ABI_VERSION
@@ -203,6 +203,8 @@ class Batch:
         o.l2_budget_bytes = int(l2_budget_bytes)
         o.tile_y, o.kchunk = int(tile_y), int(kchunk)
         o.use_graphs = 0 if use_graphs else -1
+        o.graph_steps = int(graph_steps)
+        o.lanes = int(lanes)
         self._h = C.c_void_p()
         st = self._lib.aefdtd_batch_create(C.byref(o), C.byref(self._h))
         if st != 0:
@@ -274,7 +276,8 @@ class Batch:
         i = A.BatchInfo()
         self._c(self._lib.aefdtd_batch_get_info(self._h, C.byref(i)))
         k = min(i.n_classes, A.BATCH_MAX_CLASSES)
-        return {"n_members": i.n_members, "n_active": i.n_active, "n_subsets": i.n_subsets, "cells": i.cells,
+        return {"n_members": i.n_members, "n_active": i.n_active, "n_subsets": i.n_subsets, "n_lanes": i.n_lanes,
+                "cells": i.cells,
                 "member_bytes": i.member_bytes, "batch_bytes": i.batch_bytes,
                 "l2_budget_bytes": i.l2_budget_bytes, "launches": i.launches,
                 "classes": [{"key": i.class_key[c], "tile_y": i.class_tile_y[c], "kchunk": i.class_kchunk[c]}

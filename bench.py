@@ -291,6 +291,104 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def batch_sample(n_cells=512, steps=256, seed=2024):
+    """Config 4: n_cells seeded nanodisk unit cells (period U(200, 600) nm at
+    5 nm, z = 200 cells with 16-cell CPML, gold or n U(1.8, 3.5) disk on
+    n = 1.45, 101 wavelengths) advanced as one FP32 batch. Fixed batch settings
+    (tile 32 x 4, 8 planes per item, 48 MiB subsets, one at a time); a bounded sample of
+    `steps` steps after a one-segment warm-up, timed on the host around the
+    synchronous advance calls, extrapolated to the 8000-step job."""
+    import numpy as np
+    from aether_b200 import _abi as A
+    from aether_b200 import configs as CF
+    from aether_b200 import fdtd
+    rng = np.random.default_rng(seed)
+    scenes = [CF.metasurface_cell(rng, precision=A.FP32, nsteps=8000, nl=101, flux_planes=False)
+              for _ in range(n_cells)]
+    t0 = time.perf_counter()
+    sims = [fdtd.build_simulation(sc) for sc in scenes]
+    setup = time.perf_counter() - t0
+    cells = sum(sc.cells for sc in scenes)
+    with fdtd.Batch(l2_budget_bytes=48 << 20, tile_y=4, kchunk=8, lanes=1) as b:
+        for s in sims:
+            b.add(s, steps + STEPS_PER_BENCH_STEP)
+        b.advance(STEPS_PER_BENCH_STEP)            # warm-up: captures every subset's graph
+        t0 = time.perf_counter()
+        done = 0
+        while done < steps:
+            done += b.advance(steps - done)
+        dt = time.perf_counter() - t0
+        info = b.info()
+    for s in sims:
+        s.close()
+    g = cells * done / dt / 1e9
+    return {"workload": f"config 4: {n_cells} nanodisk unit cells, FP32, {cells / 1e6:.1f} M cells in total",
+            "gcells": g, "sims_per_s": n_cells / (dt * 8000.0 / done), "sample_steps": done, "seconds": dt,
+            "subsets": info["n_subsets"], "setup_seconds": setup,
+            "note": "sims/s extrapolated from the timed sample to 8000 steps per cell"}
+
+
+def serving_sample(n_jobs=32, rate=1.5, seed=77, fp64_check=2):
+    """Config 5: a seeded Poisson stream (rate jobs/s) of config-4 unit cells
+    plus 10% large cells (period U(640, 1280) nm -> up to 256 x 256 cells,
+    z = 384), step budgets U(4000, 20000), 101 wavelengths, FP32, served with
+    continuous batching under an 80%-of-HBM budget. Jobs are submitted when
+    their arrival time passes; the loop polls the server in between. A seeded
+    sample of fp64_check jobs is re-run alone in FP64 (the path bit-identical
+    to the reference core) for the R/T error."""
+    import numpy as np
+    from aether_b200 import _abi as A
+    from aether_b200 import configs as CF
+    from aether_b200 import fdtd
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_jobs))
+    reqs = []
+    for _ in range(n_jobs):
+        large = rng.uniform() < 0.1
+        steps = int(rng.integers(4000, 20001))
+        if large:
+            sc = CF.metasurface_cell(rng, precision=A.FP32, nsteps=steps, nl=101, nz_total=384,
+                                     period_range=(640e-9, 1280e-9), flux_planes=False)
+        else:
+            sc = CF.metasurface_cell(rng, precision=A.FP32, nsteps=steps, nl=101, flux_planes=False)
+        reqs.append((sc, steps, large))
+    with fdtd.Server() as v:
+        ids = [None] * n_jobs
+        nxt = 0
+        t0 = time.perf_counter()
+        while True:
+            now = time.perf_counter() - t0
+            while nxt < n_jobs and arrivals[nxt] <= now:
+                ids[nxt] = v.submit(reqs[nxt][0], reqs[nxt][1])
+                nxt += 1
+            st = v.stats()
+            if nxt == n_jobs and st["queued"] == 0 and st["running"] == 0:
+                break
+            if st["queued"] == 0 and st["running"] == 0:
+                time.sleep(max(0.0, min(0.05, arrivals[nxt] - now)))
+                continue
+            v.poll()
+        st = v.stats()
+        spectra = [v.spectra(j) for j in ids]
+    # FP64 check on a seeded sample
+    pick = sorted(np.random.default_rng(seed + 1).choice(n_jobs, size=min(fp64_check, n_jobs), replace=False))
+    err = 0.0
+    for k in pick:
+        sc, steps, _ = reqs[k]
+        sc.grid.precision = A.FP64
+        with fdtd.build_simulation(sc) as s:
+            s.step(steps)
+            ref = s.normal_spectra()
+        err = max(err, float(np.max(np.abs(spectra[k][:, 1:3] - ref[:, 1:3]))))
+    cu = sum(sc.cells * steps for sc, steps, _ in reqs)
+    return {"workload": f"config 5: {n_jobs} Poisson arrivals at {rate}/s, 10% large cells, steps U(4000, 20000), "
+                        "FP32, 80% HBM budget",
+            "p50_s": st["p50_s"], "p99_s": st["p99_s"], "mean_s": st["mean_s"], "sims_per_s": st["sims_per_s"],
+            "gcells": st["gcells_per_s"], "elapsed_s": st["elapsed_s"], "peak_bytes": st["peak_bytes"],
+            "budget_bytes": st["budget_bytes"], "cell_updates": cu, "large_jobs": int(sum(r[2] for r in reqs)),
+            "rt_abs_err_vs_fp64": err, "fp64_sample_jobs": [int(k) for k in pick]}
+
+
 def profile_run(args):
     """The bench workload with every kernel launched directly (no CUDA graphs),
     for ncu launch lists and captures: `--segments` DFT blocks of 64 steps at
@@ -313,6 +411,8 @@ def main():
     ap.add_argument("--impl", default="aefdtd")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the config-4 batch sample")
+    ap.add_argument("--no-serving", action="store_true", help="skip the config-5 serving sample")
     ap.add_argument("--profile", choices=["fp32", "fp64"], help="direct-launch run for ncu (no timing)")
     ap.add_argument("--segments", type=int, default=2)
     args = ap.parse_args()
@@ -365,6 +465,15 @@ def main():
                        "d2h_bytes_per_step": d2h,
                        "step": "one complete 20000-step job from host buffers (geometry upload, "
                                "all steps, spectra read back)", "seconds": dt}
+    if not args.no_batch:
+        line["batch"] = batch_sample()
+        line["batch"]["over_fp64_single"] = line["batch"]["gcells"] / r64["gcells"]
+        log(f"[batch] {line['batch']['gcells']:.2f} Gcell/s, {line['batch']['sims_per_s']:.2f} sims/s")
+    if not args.no_serving:
+        line["serving"] = serving_sample()
+        sv = line["serving"]
+        log(f"[serving] p50 {sv['p50_s']:.2f} s p99 {sv['p99_s']:.2f} s, {sv['sims_per_s']:.2f} sims/s, "
+            f"{sv['gcells']:.1f} Gcell/s, R/T err {sv['rt_abs_err_vs_fp64']:.2e}")
     if not args.no_cpu:
         try:
             line["cpu_baseline"] = cpu_baseline(workload)

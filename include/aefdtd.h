@@ -276,16 +276,18 @@ typedef struct aefdtd_batch aefdtd_batch;
 typedef struct aefdtd_batch_opts {
     int32_t abi_version;      /* = AEFDTD_ABI_VERSION */
     int32_t device;           /* CUDA device of the batch and its members */
-    int64_t l2_budget_bytes;  /* device state per subset of members stepped together; 0 -> 96 MiB, < 0 -> no limit */
+    int64_t l2_budget_bytes;  /* device state per subset of members stepped together; 0 -> 48 MiB, < 0 -> no limit */
     int32_t tile_y;           /* tile height 2, 4 or 8 (0 -> 4) until autotuned */
     int32_t kchunk;           /* planes per work item (0 -> each simulation's heuristic) until autotuned */
     int32_t use_graphs;       /* < 0: no CUDA graphs (direct launches) */
+    int32_t graph_steps;      /* steps per captured graph of a subset; 0 -> 16 */
+    int32_t lanes;            /* subsets running concurrently (1..8); 0 -> 1 until autotuned */
     int32_t reserved;
 } aefdtd_batch_opts;
 
 #define AEFDTD_BATCH_MAX_CLASSES 32
 typedef struct aefdtd_batch_info {
-    int32_t n_members, n_active, n_subsets, n_classes;
+    int32_t n_members, n_active, n_subsets, n_classes, n_lanes, reserved;
     int64_t cells;            /* total cells of the active members */
     int64_t member_bytes;     /* device memory held by all members */
     int64_t batch_bytes;      /* device memory held by the batch itself (work lists, argument arrays) */
@@ -304,9 +306,9 @@ aefdtd_status aefdtd_batch_add(aefdtd_batch *batch, aefdtd_sim *sim, int32_t ste
 aefdtd_status aefdtd_batch_remove(aefdtd_batch *batch, aefdtd_sim *sim);
 aefdtd_status aefdtd_batch_set_budget(aefdtd_batch *batch, aefdtd_sim *sim, int32_t steps);
 /* Chooses per size class the tile height (2, 4, 8) and planes per work item
- * (4, 8), then the subset L2 budget (48 MiB, 96 MiB, none), by timing trial
- * segments on the device. Every member must be at step 0; members are reset
- * to step 0. */
+ * (4, 8), then the subset L2 budget (48 MiB, 96 MiB, none) and the number of
+ * lanes (1, 2, 4), by timing trial segments on the device. Every member must
+ * be at step 0; members are reset to step 0. */
 aefdtd_status aefdtd_batch_autotune(aefdtd_batch *batch);
 /* Advances every member with budget left by up to max_steps steps. Members
  * run in subsets, one subset after another; a subset stops early, after the
