@@ -84,6 +84,7 @@ template <typename T, typename Tid> struct StepArgs {
     const StepScalars *sc;
     int q;
     int kchunk;                     // z planes per thread
+    int prefetch;                   // interior kernels: prefetch the item's planes into L2 at start
     int *err;                       // device error flag (bounded waits)
 };
 

@@ -101,6 +101,7 @@ void aefdtd_sim::construct(const aefdtd_grid_desc *d) {
     mats.assign(1, HostMat());
     if (const char *kc = std::getenv("AEFDTD_KCHUNK")) kchunk_override = std::max(0, atoi(kc));
     if (const char *zu = std::getenv("AEFDTD_ZUNROLL")) zunroll = atoi(zu) >= 2 ? 2 : 1;
+    if (const char *pf = std::getenv("AEFDTD_PREFETCH")) prefetch_l2 = atoi(pf) != 0;
     if (const char *ty = std::getenv("AEFDTD_TILE_Y")) {
         const int v = atoi(ty);
         tile_y = (v == 2 || v == 8) ? v : 4;
@@ -502,6 +503,7 @@ void aefdtd_sim::make_step_args(StepArgs<T, Tid> &ea, StepArgs<T, Tid> &ha, cons
     fill_args(ea, true);
     fill_args(ha, false);
     ea.kchunk = ha.kchunk = kchunk;
+    ea.prefetch = ha.prefetch = prefetch_l2 ? 1 : 0;
     ea.sc = ha.sc = tbl;
     if (normal) ea.kinj = ha.kinj = zs_e - 1;
     ea.nsrc = 0;
@@ -560,7 +562,17 @@ void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
     // samples) reads H only and runs beside E(q+1). H(q+1) and any DFT flush
     // wait for part 1. Timing events sit on `stream` between the joins, so a
     // phase's time covers the branches that run beside it.
-    const bool conc = concurrent_groups;
+    const bool conc = concurrent_groups && !(record && timing_mode == 2);
+    // group timing: each group of a half-step alone on the main stream between two events
+    auto timed_groups = [&](int q, int half, const WorkSplit &w, auto &&launch) {
+        for (int g = 0; g < kGroups; g++) {
+            if (w.n[g] <= 0) continue;
+            const size_t i = ((size_t(q) * 2 + half) * kGroups + g) * 2;
+            AE_CUDA(cudaEventRecord(tge[i], stream));
+            launch(g, stream);
+            AE_CUDA(cudaEventRecord(tge[i + 1], stream));
+        }
+    };
     bool h_pending = false;
     // DFT blocks filled in the previous segment accumulate beside this one's
     // steps: they read the other sample-buffer half and only touch acc
@@ -591,7 +603,8 @@ void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
     for (int q = 0; q < L; q++) {
         if (record) AE_CUDA(cudaEventRecord(tev[4 * q + 0], stream));
         ea.q = ha.q = q;
-        run_groups(wsE, [&](int g, cudaStream_t st) { launch_e_group(ea, wi, wsE, g, st); });
+        if (record && timing_mode == 2) timed_groups(q, 0, wsE, [&](int g, cudaStream_t st) { launch_e_group(ea, wi, wsE, g, st); });
+        else run_groups(wsE, [&](int g, cudaStream_t st) { launch_e_group(ea, wi, wsE, g, st); });
         if (record) AE_CUDA(cudaEventRecord(tev[4 * q + 1], stream));
         // sensors: fed after H in both drivers; plane sums read E of this step
         sa.q = q;
@@ -613,7 +626,8 @@ void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
         sa.part = 0;
         if (part0 && conc) fork(0, [&](cudaStream_t st) { launches += launch_sensor_step(sa, st); });
         join_h();
-        run_groups(wsH, [&](int g, cudaStream_t st) { launch_h_group(ha, wi, wsH, g, st); });
+        if (record && timing_mode == 2) timed_groups(q, 1, wsH, [&](int g, cudaStream_t st) { launch_h_group(ha, wi, wsH, g, st); });
+        else run_groups(wsH, [&](int g, cudaStream_t st) { launch_h_group(ha, wi, wsH, g, st); });
         launches += groups;
         if (record) AE_CUDA(cudaEventRecord(tev[4 * q + 2], stream));
         if (part0) {
@@ -679,7 +693,13 @@ void aefdtd_sim::run_steps(int n) {
             AE_CUDA(cudaEventCreate(&e));
             tev.push_back(e);
         }
+        while (timing_mode == 2 && (int)tge.size() < seg_len * 2 * kGroups * 2) {
+            cudaEvent_t e;
+            AE_CUDA(cudaEventCreate(&e));
+            tge.push_back(e);
+        }
         t_e = t_h = t_s = 0;
+        for (auto &r : t_grp) for (auto &x : r) x = 0;
         tev_steps = 0;
     }
     std::vector<StepScalars> host(seg_len);
@@ -778,6 +798,16 @@ void aefdtd_sim::accumulate_timing(int L) {
         AE_CUDA(cudaEventElapsedTime(&b, tev[4 * q + 1], tev[4 * q + 2]));
         AE_CUDA(cudaEventElapsedTime(&c, tev[4 * q + 2], tev[4 * q + 3]));
         t_e += a; t_h += b; t_s += c;
+        if (timing_mode == 2)
+            for (int half = 0; half < 2; half++)
+                for (int g = 0; g < kGroups; g++) {
+                    const WorkSplit &w = half == 0 ? wsE : wsH;
+                    if (w.n[g] <= 0) continue;
+                    const size_t i = ((size_t(q) * 2 + half) * kGroups + g) * 2;
+                    float d = 0;
+                    AE_CUDA(cudaEventElapsedTime(&d, tge[i], tge[i + 1]));
+                    t_grp[half][g] += d;
+                }
     }
     tev_steps += L;
 }
@@ -888,6 +918,12 @@ void aefdtd_sim::build_work() {
             w.off[g] = (int)(all.size() / 4);
             w.n[g] = (int)(v[half][g].size() / 4);
             all.insert(all.end(), v[half][g].begin(), v[half][g].end());
+            long long c = 0;
+            for (size_t k = 0; k < v[half][g].size(); k += 4) {
+                const int *it = &v[half][g][k];
+                c += (long long)(std::min(it[0] + tx, Nx) - it[0]) * (std::min(it[1] + ty, Ny) - it[1]) * (it[3] - it[2]);
+            }
+            grp_cells[half][g] = c;
         }
     }
     items_host = all;
@@ -1363,8 +1399,22 @@ aefdtd_status aefdtd_get_timings(aefdtd_sim *s, double *e_ms, double *h_ms, doub
 
 aefdtd_status aefdtd_enable_timing(aefdtd_sim *s, int32_t enable) {
     if (!s) return AEFDTD_BAD_ARG;
+    if (enable < 0 || enable > 2) return AEFDTD_BAD_ARG;
     s->timing = enable != 0;
+    if (enable) s->timing_mode = enable;
     return AEFDTD_OK;
+}
+
+aefdtd_status aefdtd_get_group_timings(aefdtd_sim *s, double *ms, int64_t *cells, int32_t n) {
+    if (!s || n != 2 * kGroups) return AEFDTD_BAD_ARG;
+    return guarded(s, [&] {
+        for (int half = 0; half < 2; half++)
+            for (int g = 0; g < kGroups; g++) {
+                const int i = half * kGroups + g;
+                if (ms) ms[i] = s->tev_steps > 0 ? s->t_grp[half][g] / s->tev_steps : 0.0;
+                if (cells) cells[i] = s->grp_cells[half][g];
+            }
+    });
 }
 
 aefdtd_status aefdtd_get_stream(aefdtd_sim *s, void **stream) {

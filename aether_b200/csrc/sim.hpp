@@ -212,6 +212,10 @@ struct aefdtd_sim {
     // timing: one event quadruple per step of the last aefdtd_step call
     // (before E, after E, after H, after sensors), summed on query
     bool timing = false;
+    int timing_mode = 1;            // 1: per phase (concurrent branches); 2: per work-item group, in order
+    std::vector<cudaEvent_t> tge;   // group mode: [step][half][group][start, end]
+    double t_grp[2][kGroups] = {};  // group mode: summed ms per half-step group
+    long long grp_cells[2][kGroups] = {};   // cells each group updates per half-step
     std::vector<cudaEvent_t> tev;
     int tev_steps = 0;
     double t_e = 0, t_h = 0, t_s = 0;
@@ -259,6 +263,7 @@ struct aefdtd_sim {
     int kchunk_override = 0;
     int zunroll = 2;
     int tile_y = kTileYHost;        // tile height of the work items (2, 4 or 8)
+    bool prefetch_l2 = true;        // interior kernels prefetch their item's planes into L2
 };
 
 inline aefdtd_sim::~aefdtd_sim() {

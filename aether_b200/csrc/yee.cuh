@@ -24,8 +24,10 @@
 //   * interior items (no feature): the curl update only, U z-planes per
 //     iteration with all loads of the U planes issued before any store, so
 //     each thread keeps U planes of reads in flight;
-//   * z-CPML items, dispersive items, and the rest (every phase): the
-//     boundary kernel instantiated for feature sets kFPmlZ, kFDisp and kFAll.
+//   * z-CPML items: the same loop with the psi_z recursions and z PEC planes
+//     (PZ instantiation of the interior kernels);
+//   * dispersive items and the rest (every phase): the boundary kernel
+//     instantiated for feature sets kFDisp and kFAll.
 // All groups of a half-step together cover each cell exactly once.
 //
 // FP64 instantiation (compiled with --fmad=false): operation order equals the
@@ -52,6 +54,9 @@ template <typename T> __device__ __forceinline__ T cpml_rec(T b, T psi, T c, T d
     else return psi + (b * psi + c * diff);
 }
 
+// L2 prefetch hint for the line holding p (no register result, no wait).
+__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 // Boundary-item features (bit mask per item; a kernel compiled for set F may
 // run any item whose mask is a subset of F).
 constexpr unsigned kFPmlXY = 1;   // a cell in an x or y CPML range or PEC plane
@@ -65,7 +70,11 @@ constexpr unsigned kFAll = 15;
 // one simulation, from a device array for a batch), the step's table index q
 // and the item (x0, y0, k0, k1). A CTA is 32 x TY threads for tiles of 32 x
 // TY columns (TY = 2, 4 or 8, chosen per launch).
-template <typename T, typename Tid, int U>
+// PZ: the item may also hold z-CPML planes and the z = 0 PEC plane (and no
+// other feature): the psi_z recursions and PEC of app_pml_Ex/Ey
+// (fdtd_pml.cpp:504-735) are applied after the curl update, in the general
+// kernel's order.
+template <typename T, typename Tid, int U, bool PZ = false>
 __device__ __forceinline__ void e_interior_body(const StepArgs<T, Tid> &a, int q, int4 it) {
     // coefficients through the read-only path: short-lived CTAs skip a table fill and barrier
     const int i = it.x + threadIdx.x, j = it.y + threadIdx.y;
@@ -90,9 +99,30 @@ __device__ __forceinline__ void e_interior_body(const StepArgs<T, Tid> &a, int q
     const int kmi = (it.z == 0) ? a.Nz - 1 : it.z - 1;
     T hx_km = __ldg(Hx + col + kmi * NxNy);
     T hy_km = __ldg(Hy + col + kmi * NxNy);
+    if (a.prefetch) {
+        // every plane of the item into L2 up front: only the first iteration
+        // waits on DRAM; the y-1 row lines are fetched by row 0 only
+        for (int k = it.z; k < it.w; ++k) {
+            const long long o = (long long)k * NxNy;
+            prefetch_l2(Hx + col + o); prefetch_l2(Hy + col + o); prefetch_l2(Hz + col + o);
+            prefetch_l2(Hz + colx + o); prefetch_l2(Hy + colx + o);
+            if (threadIdx.y == 0) { prefetch_l2(Hz + coly + o); prefetch_l2(Hx + coly + o); }
+            prefetch_l2(Ex + col + o); prefetch_l2(Ey + col + o); prefetch_l2(Ez + col + o);
+            prefetch_l2(mat + colm + (long long)k * mNxNy);
+            if constexpr (PZ) {
+                if (a.pz && ((k >= 1 && k < a.pml_zm) || (k >= a.Nz - a.pml_zp + 1))) {
+                    const int zn = (k < a.pml_zm) ? k : k - (a.Nz - a.pml_zp) + a.pml_zm;
+                    prefetch_l2(a.psi_z0 + col + (long long)zn * NxNy);
+                    prefetch_l2(a.psi_z1 + col + (long long)zn * NxNy);
+                }
+            }
+        }
+    }
     for (int k = it.z; k < it.w; k += U) {
         T hx[U], hy[U], hz[U], hz_jm[U], hx_jm[U], hz_im[U], hy_im[U], ex[U], ey[U], ez[U];
         int m[U];
+        T p0[U], p1[U], bzv[U], czv[U];
+        bool zeu[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             // planes past the chunk end re-read its last plane (not stored)
@@ -102,6 +132,19 @@ __device__ __forceinline__ void e_interior_body(const StepArgs<T, Tid> &a, int q
             hz_im[u] = __ldg(Hz + colx + o); hy_im[u] = __ldg(Hy + colx + o);
             ex[u] = Ex[col + o]; ey[u] = Ey[col + o]; ez[u] = Ez[col + o];
             m[u] = __ldg(mat + colm + (long long)min(k + u, it.w - 1) * mNxNy);
+            if constexpr (PZ) {
+                // E-side z range [1, pml_zm) and [Nz - pml_zp + 1, Nz) (fdtd_pml.cpp:547,559)
+                const int kk = min(k + u, it.w - 1);
+                zeu[u] = a.pz && ((kk >= 1 && kk < a.pml_zm) || (kk >= a.Nz - a.pml_zp + 1));
+                if (zeu[u]) {
+                    const int zn = (kk < a.pml_zm) ? kk : kk - (a.Nz - a.pml_zp) + a.pml_zm;
+                    const long long pz = col + (long long)zn * NxNy;
+                    p0[u] = a.psi_z0[pz];
+                    p1[u] = a.psi_z1[pz];
+                    bzv[u] = __ldg(a.bz + kk);
+                    czv[u] = __ldg(a.cz + kk);
+                }
+            }
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
@@ -110,9 +153,25 @@ __device__ __forceinline__ void e_interior_body(const StepArgs<T, Tid> &a, int q
             const int kk = min(k + u, it.w - 1);
             const T ikz = __ldg(a.ikz + kk);
             const T hxm = u ? hx[u - 1] : hx_km, hym = u ? hy[u - 1] : hy_km;
-            const T nex = (C1 * ex[u] + (C2y * iky) * (hz[u] - hz_jm[u])) - (C2z * ikz) * (hy[u] - hym);
-            const T ney = (C1 * ey[u] + (C2z * ikz) * (hx[u] - hxm)) - (C2x * ikx) * (hz[u] - hz_im[u]);
+            T nex = (C1 * ex[u] + (C2y * iky) * (hz[u] - hz_jm[u])) - (C2z * ikz) * (hy[u] - hym);
+            T ney = (C1 * ey[u] + (C2z * ikz) * (hx[u] - hxm)) - (C2x * ikx) * (hz[u] - hz_im[u]);
             const T nez = (C1 * ez[u] + (C2x * ikx) * (hy[u] - hy_im[u])) - (C2y * iky) * (hx[u] - hx_jm[u]);
+            if constexpr (PZ) {
+                if (zeu[u]) {
+                    const T C4 = __ldg(&cp->C4);
+                    const T ps0 = cpml_rec(bzv[u], p0[u], czv[u], hy[u] - hym);   // Ex: PsiExz
+                    nex -= C4 * ps0;
+                    const T ps1 = cpml_rec(bzv[u], p1[u], czv[u], hx[u] - hxm);   // Ey: PsiEyz
+                    ney += C4 * ps1;
+                    if (k + u < it.w) {
+                        const int zn = (kk < a.pml_zm) ? kk : kk - (a.Nz - a.pml_zp) + a.pml_zm;
+                        const long long pz = col + (long long)zn * NxNy;
+                        a.psi_z0[pz] = ps0;
+                        a.psi_z1[pz] = ps1;
+                    }
+                }
+                if (a.pz && kk == 0) { nex = 0; ney = 0; }
+            }
             if (k + u < it.w) {
                 const long long id = col + (long long)kk * NxNy;
                 Ex[id] = nex; Ey[id] = ney; Ez[id] = nez;
@@ -123,7 +182,9 @@ __device__ __forceinline__ void e_interior_body(const StepArgs<T, Tid> &a, int q
     }
 }
 
-template <typename T, typename Tid, int U>
+// PZ: as for E, with the H-side z range, psi recursions and z = Nz-1 PEC of
+// app_pml_Hx/Hy (fdtd_pml.cpp:737-929).
+template <typename T, typename Tid, int U, bool PZ = false>
 __device__ __forceinline__ void h_interior_body(const StepArgs<T, Tid> &a, int q, int4 it) {
     const int i = it.x + threadIdx.x, j = it.y + threadIdx.y;
     if (i >= a.Nx || j >= a.Ny) return;
@@ -143,8 +204,29 @@ __device__ __forceinline__ void h_interior_body(const StepArgs<T, Tid> &a, int q
     const T ay = a.dtdmy * __ldg(a.iky + j);
     T ex = __ldg(Ex + col + it.z * NxNy);
     T ey = __ldg(Ey + col + it.z * NxNy);
+    if (a.prefetch) {
+        // every plane of the item (and the E plane above it) into L2 up front;
+        // the y+1 row lines are fetched by the last row only
+        for (int k = it.z; k < it.w; ++k) {
+            const int kp = (k == a.Nz - 1) ? 0 : k + 1;
+            const long long o = (long long)k * NxNy, op = (long long)kp * NxNy;
+            prefetch_l2(Ex + col + op); prefetch_l2(Ey + col + op); prefetch_l2(Ez + col + o);
+            prefetch_l2(Ez + colx + o); prefetch_l2(Ey + colx + o);
+            if (threadIdx.y == blockDim.y - 1) { prefetch_l2(Ez + coly + o); prefetch_l2(Ex + coly + o); }
+            prefetch_l2(Hx + col + o); prefetch_l2(Hy + col + o); prefetch_l2(Hz + col + o);
+            if constexpr (PZ) {
+                if (a.pz && ((k < a.pml_zm) || (k >= a.Nz - a.pml_zp && k < a.Nz - 1))) {
+                    const int zn = (k < a.pml_zm) ? k : k - (a.Nz - a.pml_zp) + a.pml_zm;
+                    prefetch_l2(a.psi_z0 + col + (long long)zn * NxNy);
+                    prefetch_l2(a.psi_z1 + col + (long long)zn * NxNy);
+                }
+            }
+        }
+    }
     for (int k = it.z; k < it.w; k += U) {
         T ex_kp[U], ey_kp[U], ez[U], ez_jp[U], ex_jp[U], ez_ip[U], ey_ip[U], hx[U], hy[U], hz[U];
+        T p0[U], p1[U], bzv[U], czv[U];
+        bool zhu[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const int kk = min(k + u, it.w - 1);
@@ -155,15 +237,42 @@ __device__ __forceinline__ void h_interior_body(const StepArgs<T, Tid> &a, int q
             ez_jp[u] = __ldg(Ez + coly + o); ex_jp[u] = __ldg(Ex + coly + o);
             ez_ip[u] = __ldg(Ez + colx + o); ey_ip[u] = __ldg(Ey + colx + o);
             hx[u] = Hx[col + o]; hy[u] = Hy[col + o]; hz[u] = Hz[col + o];
+            if constexpr (PZ) {
+                // H-side z range [0, pml_zm) and [Nz - pml_zp, Nz - 1) (fdtd_pml.cpp:775,784)
+                zhu[u] = a.pz && ((kk < a.pml_zm) || (kk >= a.Nz - a.pml_zp && kk < a.Nz - 1));
+                if (zhu[u]) {
+                    const int zn = (kk < a.pml_zm) ? kk : kk - (a.Nz - a.pml_zp) + a.pml_zm;
+                    const long long pz = col + (long long)zn * NxNy;
+                    p0[u] = a.psi_z0[pz];
+                    p1[u] = a.psi_z1[pz];
+                    bzv[u] = __ldg(a.bz + kk);
+                    czv[u] = __ldg(a.cz + kk);
+                }
+            }
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const int kk = min(k + u, it.w - 1);
             const T az = a.dtdmz * __ldg(a.ikz + kk);
             const T exk = u ? ex_kp[u - 1] : ex, eyk = u ? ey_kp[u - 1] : ey;
-            const T nhx = hx[u] + (az * (ey_kp[u] - eyk) - ay * (ez_jp[u] - ez[u]));
-            const T nhy = hy[u] + (ax * (ez_ip[u] - ez[u]) - az * (ex_kp[u] - exk));
+            T nhx = hx[u] + (az * (ey_kp[u] - eyk) - ay * (ez_jp[u] - ez[u]));
+            T nhy = hy[u] + (ax * (ez_ip[u] - ez[u]) - az * (ex_kp[u] - exk));
             const T nhz = hz[u] + (ay * (ex_jp[u] - exk) - ax * (ey_ip[u] - eyk));
+            if constexpr (PZ) {
+                if (zhu[u]) {
+                    const T ps0 = cpml_rec(bzv[u], p0[u], czv[u], ey_kp[u] - eyk);   // Hx: PsiHxz
+                    nhx += a.dtm * ps0;
+                    const T ps1 = cpml_rec(bzv[u], p1[u], czv[u], ex_kp[u] - exk);   // Hy: PsiHyz
+                    nhy -= a.dtm * ps1;
+                    if (k + u < it.w) {
+                        const int zn = (kk < a.pml_zm) ? kk : kk - (a.Nz - a.pml_zp) + a.pml_zm;
+                        const long long pz = col + (long long)zn * NxNy;
+                        a.psi_z0[pz] = ps0;
+                        a.psi_z1[pz] = ps1;
+                    }
+                }
+                if (a.pz && kk == a.Nz - 1) { nhx = 0; nhy = 0; }
+            }
             if (k + u < it.w) {
                 const long long id = col + (long long)kk * NxNy;
                 Hx[id] = nhx; Hy[id] = nhy; Hz[id] = nhz;
@@ -502,20 +611,22 @@ __device__ __forceinline__ void h_boundary_body(const StepArgs<T, Tid> &a, int q
 // ---- kernels -----------------------------------------------------------------
 // Register caps: at most 256 threads per CTA; the interior kernels keep the
 // register budget of 12 (U = 1, FP32) or 8 resident 128-thread CTAs per SM.
-template <typename T, int U> struct InteriorBounds {
-    static constexpr int kMinBlocks = (U == 1 && sizeof(T) == 4) ? 6 : 4;   // per 256 threads
+template <typename T, int U, bool PZ = false> struct InteriorBounds {
+    static constexpr int kMinBlocks = PZ ? (sizeof(T) == 8 ? 2 : 3) : ((U == 1 && sizeof(T) == 4) ? 6 : 4);   // per 256 threads
+    // batched forms keep the member's arguments in registers too
+    static constexpr int kMinBlocksBatch = sizeof(T) == 8 ? 2 : 3;
 };
 constexpr int kMaxTileThreads = 256;
 
-template <typename T, typename Tid, int U>
-__global__ void __launch_bounds__(kMaxTileThreads, InteriorBounds<T, U>::kMinBlocks)
+template <typename T, typename Tid, int U, bool PZ = false>
+__global__ void __launch_bounds__(kMaxTileThreads, InteriorBounds<T, U, PZ>::kMinBlocks)
 e_interior(const __grid_constant__ StepArgs<T, Tid> a, const int4 *__restrict__ items) {
-    e_interior_body<T, Tid, U>(a, a.q, items[blockIdx.x]);
+    e_interior_body<T, Tid, U, PZ>(a, a.q, items[blockIdx.x]);
 }
-template <typename T, typename Tid, int U>
-__global__ void __launch_bounds__(kMaxTileThreads, InteriorBounds<T, U>::kMinBlocks)
+template <typename T, typename Tid, int U, bool PZ = false>
+__global__ void __launch_bounds__(kMaxTileThreads, InteriorBounds<T, U, PZ>::kMinBlocks)
 h_interior(const __grid_constant__ StepArgs<T, Tid> a, const int4 *__restrict__ items) {
-    h_interior_body<T, Tid, U>(a, a.q, items[blockIdx.x]);
+    h_interior_body<T, Tid, U, PZ>(a, a.q, items[blockIdx.x]);
 }
 template <typename T, typename Tid, unsigned F>
 __global__ void __launch_bounds__(kMaxTileThreads) e_boundary(const __grid_constant__ StepArgs<T, Tid> a,
@@ -532,17 +643,17 @@ __global__ void __launch_bounds__(kMaxTileThreads) h_boundary(const __grid_const
 // instance from a device array, q the step's index in every member's table.
 __device__ __forceinline__ int4 batch_item(int4 b) { return make_int4(b.x, b.y, b.z & 0xffff, b.z >> 16); }
 
-template <typename T, typename Tid, int U>
-__global__ void __launch_bounds__(kMaxTileThreads, InteriorBounds<T, U>::kMinBlocks)
+template <typename T, typename Tid, int U, bool PZ = false>
+__global__ void __launch_bounds__(kMaxTileThreads, InteriorBounds<T, U, PZ>::kMinBlocksBatch)
 e_interior_batch(const StepArgs<T, Tid> *__restrict__ args, int q, const int4 *__restrict__ items) {
     const int4 b = items[blockIdx.x];
-    e_interior_body<T, Tid, U>(args[b.w], q, batch_item(b));
+    e_interior_body<T, Tid, U, PZ>(args[b.w], q, batch_item(b));
 }
-template <typename T, typename Tid, int U>
-__global__ void __launch_bounds__(kMaxTileThreads, InteriorBounds<T, U>::kMinBlocks)
+template <typename T, typename Tid, int U, bool PZ = false>
+__global__ void __launch_bounds__(kMaxTileThreads, InteriorBounds<T, U, PZ>::kMinBlocksBatch)
 h_interior_batch(const StepArgs<T, Tid> *__restrict__ args, int q, const int4 *__restrict__ items) {
     const int4 b = items[blockIdx.x];
-    h_interior_body<T, Tid, U>(args[b.w], q, batch_item(b));
+    h_interior_body<T, Tid, U, PZ>(args[b.w], q, batch_item(b));
 }
 template <typename T, typename Tid, unsigned F>
 __global__ void __launch_bounds__(kMaxTileThreads)
@@ -569,7 +680,10 @@ void launch_e_group_impl(const StepArgs<T, Tid> &a, const int4 *items, const Wor
             if (w.unroll >= 2) e_interior<T, Tid, 2><<<n, blk, 0, s>>>(a, p);
             else e_interior<T, Tid, 1><<<n, blk, 0, s>>>(a, p);
             break;
-        case kGroupPmlZ: e_boundary<T, Tid, kFPmlZ><<<n, blk, 0, s>>>(a, p); break;
+        case kGroupPmlZ:
+            if (w.unroll >= 2) e_interior<T, Tid, 2, true><<<n, blk, 0, s>>>(a, p);
+            else e_interior<T, Tid, 1, true><<<n, blk, 0, s>>>(a, p);
+            break;
         case kGroupDisp: e_boundary<T, Tid, kFDisp><<<n, blk, 0, s>>>(a, p); break;
         default: e_boundary<T, Tid, kFAll><<<n, blk, 0, s>>>(a, p); break;
     }
@@ -586,7 +700,10 @@ void launch_h_group_impl(const StepArgs<T, Tid> &a, const int4 *items, const Wor
             if (w.unroll >= 2) h_interior<T, Tid, 2><<<n, blk, 0, s>>>(a, p);
             else h_interior<T, Tid, 1><<<n, blk, 0, s>>>(a, p);
             break;
-        case kGroupPmlZ: h_boundary<T, Tid, kFPmlZ><<<n, blk, 0, s>>>(a, p); break;
+        case kGroupPmlZ:
+            if (w.unroll >= 2) h_interior<T, Tid, 2, true><<<n, blk, 0, s>>>(a, p);
+            else h_interior<T, Tid, 1, true><<<n, blk, 0, s>>>(a, p);
+            break;
         default: h_boundary<T, Tid, kFAll><<<n, blk, 0, s>>>(a, p); break;
     }
 }
@@ -603,7 +720,10 @@ void launch_e_group_batch_impl(const StepArgs<T, Tid> *args, int q, const int4 *
             if (w.unroll >= 2) e_interior_batch<T, Tid, 2><<<n, blk, 0, s>>>(args, q, p);
             else e_interior_batch<T, Tid, 1><<<n, blk, 0, s>>>(args, q, p);
             break;
-        case kGroupPmlZ: e_boundary_batch<T, Tid, kFPmlZ><<<n, blk, 0, s>>>(args, q, p); break;
+        case kGroupPmlZ:
+            if (w.unroll >= 2) e_interior_batch<T, Tid, 2, true><<<n, blk, 0, s>>>(args, q, p);
+            else e_interior_batch<T, Tid, 1, true><<<n, blk, 0, s>>>(args, q, p);
+            break;
         case kGroupDisp: e_boundary_batch<T, Tid, kFDisp><<<n, blk, 0, s>>>(args, q, p); break;
         default: e_boundary_batch<T, Tid, kFAll><<<n, blk, 0, s>>>(args, q, p); break;
     }
@@ -621,7 +741,10 @@ void launch_h_group_batch_impl(const StepArgs<T, Tid> *args, int q, const int4 *
             if (w.unroll >= 2) h_interior_batch<T, Tid, 2><<<n, blk, 0, s>>>(args, q, p);
             else h_interior_batch<T, Tid, 1><<<n, blk, 0, s>>>(args, q, p);
             break;
-        case kGroupPmlZ: h_boundary_batch<T, Tid, kFPmlZ><<<n, blk, 0, s>>>(args, q, p); break;
+        case kGroupPmlZ:
+            if (w.unroll >= 2) h_interior_batch<T, Tid, 2, true><<<n, blk, 0, s>>>(args, q, p);
+            else h_interior_batch<T, Tid, 1, true><<<n, blk, 0, s>>>(args, q, p);
+            break;
         default: h_boundary_batch<T, Tid, kFAll><<<n, blk, 0, s>>>(args, q, p); break;
     }
 }

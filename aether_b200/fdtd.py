@@ -86,8 +86,18 @@ class Simulation:
     def reset(self):
         self._c(self._lib.aefdtd_reset(self._h))
 
-    def enable_timing(self, on=True):
-        self._c(self._lib.aefdtd_enable_timing(self._h, 1 if on else 0))
+    def group_timings(self):
+        """Mode-2 timing: {(half, group): (ms per step, cells)}; half 'E'/'H',
+        group 'interior'/'pml_z'/'dispersive'/'general'."""
+        ms = (C.c_double * 8)()
+        cells = (C.c_int64 * 8)()
+        self._c(self._lib.aefdtd_get_group_timings(self._h, ms, cells, 8))
+        names = ["interior", "pml_z", "dispersive", "general"]
+        return {(h, names[g]): (ms[i * 4 + g], cells[i * 4 + g]) for i, h in enumerate("EH") for g in range(4)}
+
+    def enable_timing(self, on=True, mode=1):
+        """mode 1: per phase; mode 2: per work-item group (groups in order)."""
+        self._c(self._lib.aefdtd_enable_timing(self._h, int(mode) if on else 0))
 
     def timings(self):
         e, h, s = C.c_double(), C.c_double(), C.c_double()

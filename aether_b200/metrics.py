@@ -70,3 +70,21 @@ def kernel_bytes(scene, precision=None):
 
 def gcells(cells, steps, seconds):
     return cells * steps / seconds / 1e9
+
+
+def step_bytes(scene, precision=None, dft_block=64):
+    """Algorithmic bytes of one whole time step: the E and H half-steps, the
+    sensor samples (per point: 18 field reads, 6 sample writes) and, per
+    step, 1/K of each DFT block (samples read once, FP64 complex accumulators
+    read and written for every wavelength)."""
+    kb = kernel_bytes(scene, precision)
+    s = kb["elem_bytes"]
+    total = kb["E"] + kb["H"]
+    for sd in scene.sensors:
+        x1, x2, y1, y2, z1, z2 = sd.box
+        span = [max(1, x2 - x1), max(1, y2 - y1), max(1, z2 - z1)]
+        span.sort()
+        P = span[1] * span[2]
+        total += P * (18 + 6) * s
+        total += (P * 6 * s * dft_block + 2 * 6 * sd.nl * P * 16) / dft_block
+    return int(total)

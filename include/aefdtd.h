@@ -252,7 +252,14 @@ aefdtd_status aefdtd_get_sensor_shape(aefdtd_sim *sim, int32_t sensor_id, int32_
  * with CUDA events on the handle's stream: milliseconds spent in the E
  * half-step kernels, the H half-step kernels and the sensor kernels. */
 aefdtd_status aefdtd_get_timings(aefdtd_sim *sim, double *e_ms, double *h_ms, double *sensor_ms);
+/* enable: 0 off; 1 per phase (E, H, sensors; concurrent branches inside
+ * each phase); 2 per work-item group: the groups of each half-step run one
+ * after another on the handle's stream, each between two events. */
 aefdtd_status aefdtd_enable_timing(aefdtd_sim *sim, int32_t enable);
+/* After a timed aefdtd_step in mode 2: mean milliseconds per step of each
+ * group (index half*4 + group; half 0 = E, 1 = H; groups interior, z-CPML,
+ * dispersive, general) and the cells it updates per half-step. n must be 8. */
+aefdtd_status aefdtd_get_group_timings(aefdtd_sim *sim, double *ms, int64_t *cells, int32_t n);
 /* The handle's CUDA stream (a cudaStream_t), for callers that order their
  * own device work or timing events with the simulation's kernels. */
 aefdtd_status aefdtd_get_stream(aefdtd_sim *sim, void **stream);

@@ -205,6 +205,23 @@ def test_timing_mode_does_not_change_results():
         assert np.array_equal(s1.fields(), s2.fields())
 
 
+def test_group_timing_mode_covers_every_cell_once():
+    """Mode-2 timing runs each group alone between events: same fields, and
+    the groups of each half-step cover every cell of the grid once."""
+    sc = scenes.gold_sphere(nsteps=70)
+    with fdtd.build_simulation(sc) as s1, fdtd.build_simulation(sc) as s2:
+        s1.step(70)
+        s2.enable_timing(True, mode=2)
+        s2.step(70)
+        assert np.array_equal(s1.fields(), s2.fields())
+        g = s2.group_timings()
+        d = s2.dims()
+        for half in "EH":
+            cells = sum(c for (h, _), (ms, c) in g.items() if h == half)
+            assert cells == d.nx * d.ny * d.nz
+        assert g[("E", "interior")][0] > 0 and g[("E", "dispersive")][1] > 0
+
+
 def test_fp32_tensor_core_dft_matches_simt_dft(monkeypatch):
     """FP32 path: the DFT blocks on the tensor cores (tcgen05, 3xTF32) against
     the FP64 SIMT accumulation of the same samples."""
