@@ -343,29 +343,42 @@ __device__ __forceinline__ void e_boundary_body(const StepArgs<T, Tid> &a, int q
                 const DispInfo d = a.disp[m];
                 const long long q = (i - d.x1) + (long long)(j - d.y1) * d.xs + (long long)(k - d.z1) * d.xs * d.ys;
                 Cplx<T> *__restrict__ P = a.psi + d.psi_off + q;
-                for (int p = 0; p < d.np; ++p) {
-                    const Cplx<T> cr = a.crec[d.pole_off + p];
-                    const Cplx<T> dc = a.dchi[d.pole_off + p];
-                    const T ev[3] = {ex, ey, ez};
+                const T ev[3] = {ex, ey, ez};
+                // up to four poles at a time: every psi load issued before any
+                // store, then the updates in pole order (the sums keep the
+                // reference's order over poles)
+                for (int p0 = 0; p0 < d.np; p0 += 4) {
+                    const int pn = min(4, d.np - p0);
+                    Cplx<T> v[4][3], cr[4], dc[4];
 #pragma unroll
-                    for (int dd = 0; dd < 3; ++dd) {
-                        Cplx<T> *pp = P + (long long)(3 * p + dd) * d.box;
-                        const Cplx<T> v = *pp;
-                        Cplx<T> r;
-                        if constexpr (Exact<T>::value) {
-                            // Crec*psi + Dchi*E with std::complex<double> rounding order
-                            r.re = (cr.re * v.re - cr.im * v.im) + dc.re * ev[dd];
-                            r.im = (cr.re * v.im + cr.im * v.re) + dc.im * ev[dd];
-                        } else {
-                            // (Crec-1) stored: psi + ((Crec-1)*psi + Dchi*E)
-                            r.re = v.re + ((cr.re * v.re - cr.im * v.im) + dc.re * ev[dd]);
-                            r.im = v.im + ((cr.re * v.im + cr.im * v.re) + dc.im * ev[dd]);
+                    for (int p = 0; p < 4; ++p)
+                        if (p < pn) {
+                            cr[p] = a.crec[d.pole_off + p0 + p];
+                            dc[p] = a.dchi[d.pole_off + p0 + p];
+#pragma unroll
+                            for (int dd = 0; dd < 3; ++dd) v[p][dd] = P[(long long)(3 * (p0 + p) + dd) * d.box];
                         }
-                        *pp = r;
-                        if (dd == 0) s0 = s0 + r.re;
-                        else if (dd == 1) s1 = s1 + r.re;
-                        else s2 = s2 + r.re;
-                    }
+#pragma unroll
+                    for (int p = 0; p < 4; ++p)
+                        if (p < pn) {
+#pragma unroll
+                            for (int dd = 0; dd < 3; ++dd) {
+                                Cplx<T> r;
+                                if constexpr (Exact<T>::value) {
+                                    // Crec*psi + Dchi*E with std::complex<double> rounding order
+                                    r.re = (cr[p].re * v[p][dd].re - cr[p].im * v[p][dd].im) + dc[p].re * ev[dd];
+                                    r.im = (cr[p].re * v[p][dd].im + cr[p].im * v[p][dd].re) + dc[p].im * ev[dd];
+                                } else {
+                                    // (Crec-1) stored: psi + ((Crec-1)*psi + Dchi*E)
+                                    r.re = v[p][dd].re + ((cr[p].re * v[p][dd].re - cr[p].im * v[p][dd].im) + dc[p].re * ev[dd]);
+                                    r.im = v[p][dd].im + ((cr[p].re * v[p][dd].im + cr[p].im * v[p][dd].re) + dc[p].im * ev[dd]);
+                                }
+                                P[(long long)(3 * (p0 + p) + dd) * d.box] = r;
+                                if (dd == 0) s0 = s0 + r.re;
+                                else if (dd == 1) s1 = s1 + r.re;
+                                else s2 = s2 + r.re;
+                            }
+                        }
                 }
             }
         }
