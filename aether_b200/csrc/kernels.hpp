@@ -40,6 +40,13 @@ void launch_plane_partial_batch(const SensorStepArgs<double> *args, const int2 *
 void launch_plane_partial_batch(const SensorStepArgs<float> *args, const int2 *blk, int nblk, int q, cudaStream_t s);
 void launch_plane_reduce_batch(const SensorStepArgs<double> *args, int n_inst, int steps, cudaStream_t s);
 void launch_plane_reduce_batch(const SensorStepArgs<float> *args, int n_inst, int steps, cudaStream_t s);
+// completion sensor (energy mode): per-step grid energy partials, and their
+// reduction for `steps` steps into hist[sc[0].step + q]
+void launch_energy_partial(const double *Ex, const double *Ey, const double *Ez, long long N, int nb, double *part,
+                           cudaStream_t s);
+void launch_energy_partial(const float *Ex, const float *Ey, const float *Ez, long long N, int nb, double *part,
+                           cudaStream_t s);
+void launch_energy_reduce(const double *part, int nb, const StepScalars *sc, double *hist, int steps, cudaStream_t s);
 void launch_phasors(const PhasorArgs &a, cudaStream_t s);
 void launch_accumulate(const AccumArgs<double> &a, cudaStream_t s);
 void launch_accumulate(const AccumArgs<float> &a, cudaStream_t s);

@@ -622,17 +622,29 @@ void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
             blk += g.nblocks;
             g.S = s.S.as<T>() + ((size_t)s.half * dft_k + s.nbuf) * 6 * s.P;
         }
-        const bool part0 = sa.nbp > 0 || sa.ng > 0;
+        const bool cc = cc_coeff > 0;
+        const bool part0 = sa.nbp > 0 || sa.ng > 0 || cc;
         sa.part = 0;
-        if (part0 && conc) fork(0, [&](cudaStream_t st) { launches += launch_sensor_step(sa, st); });
+        // completion energy of this step reads E only: with part 0, beside H
+        auto energy = [&](cudaStream_t st) {
+            if (!cc) return;
+            launch_energy_partial(F[0].as<T>(), F[1].as<T>(), F[2].as<T>(), (long long)Nx * Ny * Nz, cc_nb,
+                                  cc_partial.as<double>() + size_t(q) * cc_nb, st);
+            launches++;
+        };
+        if (part0 && conc) fork(0, [&](cudaStream_t st) { launches += launch_sensor_step(sa, st); energy(st); });
         join_h();
         if (record && timing_mode == 2) timed_groups(q, 1, wsH, [&](int g, cudaStream_t st) { launch_h_group(ha, wi, wsH, g, st); });
         else run_groups(wsH, [&](int g, cudaStream_t st) { launch_h_group(ha, wi, wsH, g, st); });
         launches += groups;
         if (record) AE_CUDA(cudaEventRecord(tev[4 * q + 2], stream));
         if (part0) {
-            if (conc) AE_CUDA(cudaStreamWaitEvent(stream, ev_s_join[0], 0));
-            else launches += launch_sensor_step(sa, stream);
+            if (conc) {
+                AE_CUDA(cudaStreamWaitEvent(stream, ev_s_join[0], 0));
+            } else {
+                launches += launch_sensor_step(sa, stream);
+                energy(stream);
+            }
         }
         if (sa.ng > 0) {
             sa.part = 1;
@@ -667,6 +679,32 @@ void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
         launch_plane_reduce(psum_partial.as<double>(), sa.nbp, tbl, psums.as<double>(), L, stream);
         launches++;
     }
+    if (cc_coeff > 0) {
+        launch_energy_reduce(cc_partial.as<double>(), cc_nb, tbl, cc_hist.as<double>(), L, stream);
+        launches++;
+    }
+}
+
+// CompletionSensor::completion_check in energy mode (s_completion.cpp:39-43,
+// 121-130) after check step t = tstep - 1: the energies since the last check
+// update the running maximum; the run completes when the last energy is below
+// coeff times the maximum, once tstep >= 2 max(Nx, Ny, Nz).
+void aefdtd_sim::completion_check() {
+    const int n = tstep - cc_read;
+    if (n > 0) {
+        std::vector<double> e(n);
+        AE_CUDA(cudaMemcpyAsync(e.data(), cc_hist.as<double>() + cc_read, n * sizeof(double), cudaMemcpyDeviceToHost,
+                                stream));
+        AE_CUDA(cudaStreamSynchronize(stream));
+        for (double x : e) cc_max = std::max(cc_max, x);
+        cc_last = e.back();
+        cc_read = tstep;
+    }
+    if (tstep < 2 * std::max(Nx, std::max(Ny, Nz))) return;
+    if (cc_last / cc_max < cc_coeff) {
+        cc_done = true;
+        cc_stop = tstep - 1;
+    }
 }
 
 template <typename T, typename Tid>
@@ -686,6 +724,25 @@ void aefdtd_sim::run_steps(int n) {
         psums_cap = cap;
         graphs_dirty = true;
         drop_graphs();
+    }
+    if (cc_coeff > 0) {
+        if (cc_done) return;   // completed: the driver's loop has ended
+        if (tstep + n > cc_cap) {
+            const int cap = std::max(tstep + n, std::max(2 * cc_cap, std::max(Nt, 1024)));
+            DBuf nb;
+            nb.alloc(size_t(cap) * 8, dev_bytes);
+            if (cc_hist.p) AE_CUDA(cudaMemcpyAsync(nb.p, cc_hist.p, size_t(cc_cap) * 8, cudaMemcpyDeviceToDevice, stream));
+            AE_CUDA(cudaStreamSynchronize(stream));
+            cc_hist.release(dev_bytes);
+            cc_hist = nb;
+            cc_cap = cap;
+            graphs_dirty = true;
+            drop_graphs();
+        }
+        if (!cc_partial.p) {
+            cc_nb = std::max(1, std::min(2 * 148, (int)(((long long)Nx * Ny * Nz + 4095) / 4096)));
+            cc_partial.alloc(size_t(seg_len) * cc_nb * 8, dev_bytes);
+        }
     }
     if (timing) {
         while ((int)tev.size() < 4 * seg_len) {
@@ -709,6 +766,11 @@ void aefdtd_sim::run_steps(int n) {
         int L = std::min(n - done, seg_len);
         bool empty = true;
         for (auto *s : sensors) { L = std::min(L, dft_k - s->nbuf); empty &= s->nbuf == 0; }
+        if (cc_coeff > 0) {
+            // a segment ends right after each check step t (t % cc_step == 0)
+            const int tchk = (tstep + cc_step - 1) / cc_step * cc_step;
+            L = std::min(L, tchk + 1 - tstep);
+        }
         const int slot = seg_slot;
         seg_slot ^= 1;
         StepScalars *tbl = tables.as<StepScalars>() + size_t(slot) * seg_len;
@@ -779,6 +841,10 @@ void aefdtd_sim::run_steps(int n) {
         for (auto &o : oscs) o.step += L;
         tstep += L;
         done += L;
+        if (cc_coeff > 0 && (tstep - 1) % cc_step == 0) {
+            completion_check();
+            if (cc_done) break;
+        }
     }
     AE_CUDA(cudaGetLastError());
 }
@@ -959,6 +1025,10 @@ void aefdtd_sim::step(int n) {
 
 void aefdtd_sim::zero_state() {
     set_device();
+    cc_done = false;
+    cc_stop = -1;
+    cc_read = 0;
+    cc_last = cc_max = 0;
     for (auto &b : F) if (b.p) AE_CUDA(cudaMemsetAsync(b.p, 0, b.n, stream));
     for (auto &b : psiE) if (b.p) AE_CUDA(cudaMemsetAsync(b.p, 0, b.n, stream));
     for (auto &b : psiH) if (b.p) AE_CUDA(cudaMemsetAsync(b.p, 0, b.n, stream));
@@ -1249,10 +1319,12 @@ aefdtd_status aefdtd_get_normal_spectra(aefdtd_sim *s, double *out, int32_t nl) 
     return guarded(s, [&] {
         if (!s->normal) fail(AEFDTD_NOT_READY, "spectra exist in normal mode only");
         if (nl != s->nd.nl) fail(AEFDTD_BAD_ARG, "nl must equal the normal-mode spectrum size");
-        int NtP = s->tstep;
+        const int Ntot = s->tstep;
+        // after a completion at step t the driver analyses Nt = t steps (normal_incidence.cpp:417-427)
+        const int NtP = s->cc_done ? s->cc_stop : Ntot;
         if (NtP < 2) fail(AEFDTD_NOT_READY, "run at least two steps");
-        std::vector<double> S(size_t(NtP) * 12);
-        aefdtd_status st = aefdtd_get_plane_sums(s, S.data(), NtP);
+        std::vector<double> S(size_t(Ntot) * 12);
+        aefdtd_status st = aefdtd_get_plane_sums(s, S.data(), Ntot);
         if (st != AEFDTD_OK) fail(st, s->last_error);
         auto M = [&](int i, int j, int k) { return s->map[i + size_t(j) * s->Nx + size_t(k) * s->Nx * s->Ny]; };
         // FDTD::find_slab (fdtd_utils.cpp:347-392)
@@ -1278,7 +1350,7 @@ aefdtd_status aefdtd_get_normal_spectra(aefdtd_sim *s, double *out, int32_t nl) 
         hsub -= Dz / 2.0;
         const cplx Im(0, 1);
         const double *SS[12];
-        for (int c = 0; c < 12; c++) SS[c] = S.data() + size_t(c) * NtP;
+        for (int c = 0; c < 12; c++) SS[c] = S.data() + size_t(c) * Ntot;
         for (int l = 0; l < nl; l++) {
             double lam = s->nd.lambda_min + (s->nd.lambda_max - s->nd.lambda_min) * l / (nl - 1.0);
             double w = 2.0 * Pi * c_light / lam;
@@ -1402,6 +1474,29 @@ aefdtd_status aefdtd_enable_timing(aefdtd_sim *s, int32_t enable) {
     if (enable < 0 || enable > 2) return AEFDTD_BAD_ARG;
     s->timing = enable != 0;
     if (enable) s->timing_mode = enable;
+    return AEFDTD_OK;
+}
+
+aefdtd_status aefdtd_set_completion(aefdtd_sim *s, double coeff, int32_t check_every) {
+    if (!s) return AEFDTD_BAD_ARG;
+    return guarded(s, [&] {
+        if (check_every < 0) fail(AEFDTD_BAD_ARG, "negative check interval");
+        if (s->batch) fail(AEFDTD_NOT_READY, "batch members run without a completion sensor");
+        s->cc_coeff = coeff > 0 ? coeff : 0;
+        s->cc_step = check_every > 0 ? check_every : 500;
+        s->cc_done = false;
+        s->cc_stop = -1;
+        s->cc_read = s->tstep;
+        s->cc_last = s->cc_max = 0;
+        s->graphs_dirty = true;
+    });
+}
+
+aefdtd_status aefdtd_get_completion(aefdtd_sim *s, int32_t *done, int32_t *stop_step, double *ratio) {
+    if (!s) return AEFDTD_BAD_ARG;
+    if (done) *done = s->cc_done ? 1 : 0;
+    if (stop_step) *stop_step = s->cc_stop;
+    if (ratio) *ratio = s->cc_max > 0 ? s->cc_last / s->cc_max : 0.0;
     return AEFDTD_OK;
 }
 

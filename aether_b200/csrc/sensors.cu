@@ -48,4 +48,15 @@ void launch_plane_reduce_batch(const SensorStepArgs<double> *args, int n_inst, i
 void launch_plane_reduce_batch(const SensorStepArgs<float> *args, int n_inst, int steps, cudaStream_t s) {
     if (n_inst > 0 && steps > 0) plane_sums_reduce_batch<float><<<dim3(steps, n_inst), 32, 0, s>>>(args);
 }
+void launch_energy_partial(const double *Ex, const double *Ey, const double *Ez, long long N, int nb, double *part,
+                           cudaStream_t s) {
+    energy_partial<double><<<nb, kPlaneThreads, 0, s>>>(Ex, Ey, Ez, N, nb, part);
+}
+void launch_energy_partial(const float *Ex, const float *Ey, const float *Ez, long long N, int nb, double *part,
+                           cudaStream_t s) {
+    energy_partial<float><<<nb, kPlaneThreads, 0, s>>>(Ex, Ey, Ez, N, nb, part);
+}
+void launch_energy_reduce(const double *part, int nb, const StepScalars *sc, double *hist, int steps, cudaStream_t s) {
+    if (steps > 0) energy_reduce<<<steps, 32, 0, s>>>(part, nb, sc, hist);
+}
 }  // namespace aefdtd

@@ -188,6 +188,41 @@ __global__ void plane_sums_reduce_batch(const SensorStepArgs<T> *__restrict__ ar
     a.out[((long long)a.sc[0].step + q) * 12 + c] = s;
 }
 
+// Completion sensor, energy mode (CompletionSensor::deep_feed,
+// s_completion.cpp:177-190): sum of Ex^2 + Ey^2 + Ez^2 over the grid after a
+// step. Block b of nb sums a contiguous chunk (threads strided, then a tree);
+// the partials of step q go to part[q * nb + b] and are added in block order.
+template <typename T>
+__global__ void __launch_bounds__(kPlaneThreads)
+energy_partial(const T *__restrict__ Ex, const T *__restrict__ Ey, const T *__restrict__ Ez, long long N, int nb,
+               double *part) {
+    const int b = blockIdx.x;
+    const long long per = (N + nb - 1) / nb;
+    const long long q0 = b * per, q1 = min(N, q0 + per);
+    double s = 0;
+    for (long long c = q0 + threadIdx.x; c < q1; c += blockDim.x) {
+        const double ex = (double)Ex[c], ey = (double)Ey[c], ez = (double)Ez[c];
+        s = dadd(s, dadd(dadd(dmul(ex, ex), dmul(ey, ey)), dmul(ez, ez)));
+    }
+    __shared__ double red[kPlaneThreads];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] = dadd(red[threadIdx.x], red[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[b] = red[0];
+}
+
+// grid L: step q's energy into hist[sc[0].step + q]
+__global__ void energy_reduce(const double *part, int nb, const StepScalars *sc, double *hist) {
+    if (threadIdx.x != 0) return;
+    const int q = blockIdx.x;
+    double s = 0;
+    for (int b = 0; b < nb; ++b) s = dadd(s, part[(long long)q * nb + b]);
+    hist[(long long)sc[0].step + q] = s;
+}
+
 // s_curve (src/common/mathUT.cpp:1186-1193)
 __device__ __forceinline__ double s_curve_dev(double x, double xmin, double xmax) {
     const double u = (x - xmin) / (xmax - xmin);

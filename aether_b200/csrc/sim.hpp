@@ -264,6 +264,16 @@ struct aefdtd_sim {
     int zunroll = 2;
     int tile_y = kTileYHost;        // tile height of the work items (2, 4 or 8)
     bool prefetch_l2 = true;        // interior kernels prefetch their item's planes into L2
+    // completion sensor, energy mode (CompletionSensor(coeff), s_completion.cpp)
+    double cc_coeff = 0;            // > 0: enabled
+    int cc_step = 500;              // checked after steps t with t % cc_step == 0
+    bool cc_done = false;
+    int cc_stop = -1;               // completion step t: the driver's Nt = t
+    int cc_read = 0;                // energies read back so far
+    double cc_last = 0, cc_max = 0;
+    int cc_nb = 0, cc_cap = 0;      // energy blocks per step; history capacity
+    DBuf cc_partial, cc_hist;
+    void completion_check();
 };
 
 inline aefdtd_sim::~aefdtd_sim() {
@@ -278,6 +288,8 @@ inline aefdtd_sim::~aefdtd_sim() {
     for (auto &b : psiH) b.release(t);
     psums.release(t);
     psum_partial.release(t);
+    cc_partial.release(t);
+    cc_hist.release(t);
     err.release(t);
     tables.release(t);
     for (auto &gx : graph_exec) if (gx.second) cudaGraphExecDestroy(gx.second);

@@ -86,6 +86,16 @@ class Simulation:
     def reset(self):
         self._c(self._lib.aefdtd_reset(self._h))
 
+    def set_completion(self, coeff=1e-3, check_every=500):
+        """Energy-mode completion sensor (coeff <= 0: off)."""
+        self._c(self._lib.aefdtd_set_completion(self._h, float(coeff), int(check_every)))
+
+    def completion(self):
+        """(done, stop step t or -1, last/max energy at the last check)."""
+        d, t, r = C.c_int32(), C.c_int32(), C.c_double()
+        self._c(self._lib.aefdtd_get_completion(self._h, C.byref(d), C.byref(t), C.byref(r)))
+        return bool(d.value), t.value, r.value
+
     def group_timings(self):
         """Mode-2 timing: {(half, group): (ms per step, cells)}; half 'E'/'H',
         group 'interior'/'pml_z'/'dispersive'/'general'."""

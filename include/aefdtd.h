@@ -248,6 +248,20 @@ aefdtd_status aefdtd_get_sensor_flux(aefdtd_sim *sim, int32_t sensor_id, double 
 aefdtd_status aefdtd_get_sensor_dft(aefdtd_sim *sim, int32_t sensor_id, double *out, size_t count);
 aefdtd_status aefdtd_get_sensor_shape(aefdtd_sim *sim, int32_t sensor_id, int32_t *span1, int32_t *span2, int32_t *nl);
 
+/* Completion sensor in energy mode (CompletionSensor(coeff),
+ * s_completion.cpp:20-24, 39-43, 121-130, 177-190; checked by the drivers at
+ * normal_incidence.cpp:417-427 and default_fdtd.cpp:193-203). After every
+ * step the sum of Ex^2 + Ey^2 + Ez^2 over the grid is kept. After each step t
+ * with t % check_every == 0, once t + 1 >= 2 max(Nx, Ny, Nz), the run
+ * completes when that sum is below coeff times its maximum so far; aefdtd_step
+ * then returns after step t, later calls run no step, and the normal-mode
+ * spectra use Nt = t steps (the driver's rule). coeff <= 0 turns it off;
+ * check_every 0 -> 500 (the reference default, with coeff 1e-3). Not for batch
+ * members. */
+aefdtd_status aefdtd_set_completion(aefdtd_sim *sim, double coeff, int32_t check_every);
+/* done: 1 after completion; stop_step: t (or -1); ratio: last / largest energy at the last check. */
+aefdtd_status aefdtd_get_completion(aefdtd_sim *sim, int32_t *done, int32_t *stop_step, double *ratio);
+
 /* Per-launch device timings of the most recent aefdtd_step call, measured
  * with CUDA events on the handle's stream: milliseconds spent in the E
  * half-step kernels, the H half-step kernels and the sensor kernels. */

@@ -21,6 +21,7 @@
 #include <chrono>
 #include <cmath>
 #include <complex>
+#include <filesystem>
 #include <fstream>
 #include <iostream>
 #include <sstream>
@@ -31,6 +32,15 @@
 extern const Imdouble Im;
 
 namespace {
+
+// Completion sensor in energy mode (normal mode only), set by
+// aeref_set_completion: CompletionSensor(coeff) fed after the planar sensors,
+// checked after step t's plane sums when t % every == 0
+// (normal_incidence.cpp:284-297, 417-427).
+double g_cc_coeff = 0;
+int g_cc_every = 500;
+int g_cc_stop = -1;
+double g_cc_last = 0, g_cc_max = 0;
 
 int ref_orientation(int o) {
     static const int tbl[6] = {NORMAL_X, NORMAL_XM, NORMAL_Y, NORMAL_YM, NORMAL_Z, NORMAL_ZM};
@@ -183,6 +193,14 @@ int aeref_run(const aefdtd_grid_desc *g, const uint32_t *map,
         int NtR = nsteps;
         std::vector<double> S[12];
         for (auto &v : S) v.assign(NtR, 0.0);
+        CompletionSensor *cpl = nullptr;
+        g_cc_stop = -1;
+        g_cc_last = g_cc_max = 0;
+        if (g_cc_coeff > 0) {
+            cpl = new CompletionSensor(g_cc_coeff);
+            cpl->link(fdtd, std::filesystem::path("."));
+        }
+        int NtSpec = NtR;
         double tb = 0;
         for (int t = 0; t < NtR; t++) {
             fdtd.update_E();
@@ -204,6 +222,7 @@ int aeref_run(const aefdtd_grid_desc *g, const uint32_t *map,
                     fdtd.Hy(i, j, zs_e - 1) -= fdtd.dtdmz * inj_Ex;
                 }
             for (auto *s : sensors) s->feed(fdtd);
+            if (cpl) cpl->feed(fdtd);   // fed with the sensors, after the planar ones
 
             tb = (t + 0.5) * Dt;
             double Dx2 = Dx / 2.0, Dy2 = Dy / 2.0, Dz2 = Dz / 2.0;
@@ -229,15 +248,26 @@ int aeref_run(const aefdtd_grid_desc *g, const uint32_t *map,
                     S[11][t] += fdtd.Ez(i, j, zs_s) * tapering;
                 }
             }
+            if (cpl && t % g_cc_every == 0 && cpl->completion_check()) {
+                // the driver's Nt = t: spectra from the first t samples
+                g_cc_stop = t;
+                g_cc_last = cpl->energy_last;
+                g_cc_max = cpl->energy_max;
+                NtSpec = t;
+                break;
+            }
+            if (cpl) { g_cc_last = cpl->energy_last; g_cc_max = cpl->energy_max; }
         }
+        delete cpl;
         if (loop_seconds) loop_seconds[0] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         if (plane_sums_out)
             for (int c = 0; c < 12; c++)
                 for (int t = 0; t < NtR; t++) plane_sums_out[size_t(c) * NtR + t] = S[c][t];
 
         if (spectra_out) {
-            // normal_incidence.cpp:442-570 with Nt = number of steps run.
-            int NtP = NtR;
+            // normal_incidence.cpp:442-570 with Nt = number of steps run
+            // (or the completion step).
+            int NtP = NtSpec;
             double hsup, hsub, hstruc;
             fdtd.find_slab(zs_s, zs_e - 1, hsub, hstruc, hsup);
             hsup -= Dz / 2.0;
@@ -305,5 +335,20 @@ int aeref_run(const aefdtd_grid_desc *g, const uint32_t *map,
 
 /* Number of worker threads the reference core uses per FDTD object. */
 int aeref_threads(void) { return max_threads_number(); }
+
+/* Completion sensor for the following aeref_run calls (normal mode):
+ * coeff <= 0 disables; every = the driver's cc_step. */
+void aeref_set_completion(double coeff, int32_t every) {
+    g_cc_coeff = coeff;
+    g_cc_every = every > 0 ? every : 500;
+}
+
+/* Result of the last aeref_run with completion: stop step t (-1 if it ran
+ * to the end) and the last and largest grid energies. */
+void aeref_completion_result(int32_t *stop, double *last, double *max) {
+    if (stop) *stop = g_cc_stop;
+    if (last) *last = g_cc_last;
+    if (max) *max = g_cc_max;
+}
 
 }  // extern "C"

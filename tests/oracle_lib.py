@@ -90,3 +90,21 @@ def run(scene, which="port", nsteps=None, want_fields=True):
         off += s.nl
     out["flux"] = fl
     return out
+
+
+def run_ref_completion(scene, coeff, every, nsteps=None):
+    """The reference core with its energy-mode CompletionSensor(coeff), checked
+    every `every` steps (normal mode): the run dict of `run` plus 'stop' (the
+    completion step t, or -1) and the last and largest grid energies."""
+    lib = C.CDLL(REF_PATH)
+    lib.aeref_set_completion.argtypes = [C.c_double, C.c_int32]
+    lib.aeref_completion_result.argtypes = [_P(C.c_int32), _P(C.c_double), _P(C.c_double)]
+    lib.aeref_set_completion(coeff, every)
+    try:
+        out = run(scene, "ref", nsteps=nsteps, want_fields=True)
+        stop, last, mx = C.c_int32(), C.c_double(), C.c_double()
+        lib.aeref_completion_result(C.byref(stop), C.byref(last), C.byref(mx))
+    finally:
+        lib.aeref_set_completion(0.0, 500)
+    out.update(stop=stop.value, energy_last=last.value, energy_max=mx.value)
+    return out
