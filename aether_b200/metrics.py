@@ -41,9 +41,18 @@ def cell_counts(scene):
     poles = np.zeros(len(scene.materials), np.int64)
     for i, m in enumerate(scene.materials):
         poles[i] = m.n_debye + m.n_drude + m.n_lorentz + m.n_critpoint
-    total_map = expand_map(scene)
-    out["disp_pole_cells"] = int(poles[np.minimum(total_map, len(poles) - 1)].sum())
-    out["id_bytes"] = 1 if total_map.max() < 256 else 2
+    # plane by plane over the total grid (no full-size temporaries)
+    nx_, ny_, nz_ = scene.total_dims()
+    xs, ys, zs = pml[0] + pad[0], pml[2] + pad[2], pml[4] + pad[4]
+    m = scene.map
+    xi = np.clip(np.arange(nx_) - xs, 0, m.shape[2] - 1)
+    yi = np.clip(np.arange(ny_) - ys, 0, m.shape[1] - 1)
+    counts = np.zeros(len(poles), np.int64)
+    for k in range(nz_):
+        plane = m[min(max(k - zs, 0), m.shape[0] - 1)][np.ix_(yi, xi)]
+        counts += np.bincount(np.minimum(plane.ravel(), len(poles) - 1), minlength=len(poles))[:len(poles)]
+    out["disp_pole_cells"] = int((counts * poles).sum())
+    out["id_bytes"] = 1 if int(m.max()) < 256 else 2
     return out
 
 

@@ -397,6 +397,47 @@ def serving_sample(n_jobs=32, rate=1.5, seed=77, fp64_check=2):
             "rt_abs_err_vs_fp64": err, "fp64_sample_jobs": [int(k) for k in pick]}
 
 
+def large_grid_sample(steps=128, seed=1234):
+    """Config 3: 1024 x 1024 x 512 cells at 5 nm, 32-cell CPML on all six
+    faces, 500 seeded dielectric spheres (r U(20, 80) nm, eps U(2, 12)) plus 50
+    Lorentz spheres sharing one material, an oscillator at the centre (600 nm,
+    300 nm band), custom mode. FP32 and FP64: `steps` steps after a 64-step
+    warm-up, timed with CUDA events on the simulation's stream (inputs far
+    larger than L2)."""
+    import torch
+    from aether_b200 import _abi as A
+    from aether_b200 import configs as CF
+    from aether_b200 import fdtd
+    from aether_b200 import metrics as MT
+    peak, _ = measured_peaks()
+    sc = CF.random_spheres_scene(seed=seed, precision=A.FP32)
+    out = {"workload": "config 3: 1024x1024x512 @5nm, 32-cell CPML x6, 500 dielectric + 50 Lorentz spheres, "
+                       "oscillator source"}
+    for name, prec in (("fp32", A.FP32), ("fp64", A.FP64)):
+        sc.grid.precision = prec
+        t0 = time.perf_counter()
+        sim = fdtd.build_simulation(sc)
+        setup = time.perf_counter() - t0
+        sim.step(STEPS_PER_BENCH_STEP)
+        sim.synchronize()
+        ext = torch.cuda.ExternalStream(sim.stream_ptr())
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        sim.step(steps)
+        e1.record(ext)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        sb = MT.step_bytes(sc, prec)
+        out[name] = {"gcells": sc.cells / (ms * 1e-3) / 1e9, "ms_per_step": ms,
+                     "step_frac": sb / (ms * 1e-3) / 1e9 / peak, "bytes_per_step": sb,
+                     "device_gb": sim.dims().device_bytes / 1e9, "setup_seconds": setup}
+        sim.close()
+        log(f"[large {name}] {out[name]['gcells']:.1f} Gcell/s, {out[name]['step_frac']:.2f} of HBM peak, "
+            f"{out[name]['device_gb']:.1f} GB on the device")
+    return out
+
+
 def profile_run(args):
     """The bench workload with every kernel launched directly (no CUDA graphs),
     for ncu launch lists and captures: `--segments` DFT blocks of 64 steps at
@@ -420,6 +461,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the config-4 batch sample")
+    ap.add_argument("--no-large", action="store_true", help="skip the config-3 large-grid sample")
     ap.add_argument("--no-serving", action="store_true", help="skip the config-5 serving sample")
     ap.add_argument("--profile", choices=["fp32", "fp64"], help="direct-launch run for ncu (no timing)")
     ap.add_argument("--segments", type=int, default=2)
@@ -486,6 +528,8 @@ def main():
                        "d2h_bytes_per_step": d2h,
                        "step": "one complete 20000-step job from host buffers (geometry upload, "
                                "all steps, spectra read back)", "seconds": dt}
+    if not args.no_large:
+        line["large_grid"] = large_grid_sample()
     if not args.no_batch:
         line["batch"] = batch_sample()
         line["batch"]["over_fp64_single"] = line["batch"]["gcells"] / r64["gcells"]
