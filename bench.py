@@ -336,7 +336,7 @@ def batch_sample(n_cells=512, steps=256, seed=2024):
             "note": "sims/s extrapolated from the timed sample to 8000 steps per cell"}
 
 
-def serving_sample(n_jobs=32, rate=1.5, seed=77, fp64_check=2):
+def serving_sample(n_jobs=32, rate=1.5, seed=77, fp64_check=2, **server_opts):
     """Config 5: a seeded Poisson stream (rate jobs/s) of config-4 unit cells
     plus 10% large cells (period U(640, 1280) nm -> up to 256 x 256 cells,
     z = 384), step budgets U(4000, 20000), 101 wavelengths, FP32, served with
@@ -360,7 +360,7 @@ def serving_sample(n_jobs=32, rate=1.5, seed=77, fp64_check=2):
         else:
             sc = CF.metasurface_cell(rng, precision=A.FP32, nsteps=steps, nl=101, flux_planes=False)
         reqs.append((sc, steps, large))
-    with fdtd.Server() as v:
+    with fdtd.Server(**server_opts) as v:
         ids = [None] * n_jobs
         nxt = 0
         t0 = time.perf_counter()

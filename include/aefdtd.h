@@ -360,10 +360,11 @@ typedef struct aefdtd_server_opts {
     double hbm_fraction;      /* memory budget as a fraction of device memory; 0 -> 0.8 */
     int64_t budget_bytes;     /* > 0: explicit budget instead of hbm_fraction */
     int32_t max_active;       /* 0: no limit on running jobs */
-    int32_t segment_steps;    /* steps per poll; 0 -> 64 */
+    int32_t segment_steps;    /* steps per poll; 0 -> 256 */
     int32_t lookahead;        /* queued jobs that may pass one that does not fit; 0 -> 16 */
     int32_t reserved;
-    aefdtd_batch_opts batch;  /* options of the batch (abi_version and device are set by the server) */
+    aefdtd_batch_opts batch;  /* options of the batch (abi_version and device are set by the server;
+                                 l2_budget_bytes 0 -> no limit: one merged subset per size class) */
 } aefdtd_server_opts;
 
 typedef struct aefdtd_job_desc {
