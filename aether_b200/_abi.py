@@ -136,6 +136,11 @@ class ServerStats(C.Structure):
     ]
 
 
+class BoxSensorDesc(C.Structure):
+    _fields_ = [("box", C.c_int32 * 6), ("nl", C.c_int32), ("disabled", C.c_int32),
+                ("lambda_min", C.c_double), ("lambda_max", C.c_double)]
+
+
 class StructureOp(C.Structure):
     _fields_ = [("kind", C.c_int32), ("mat_index", C.c_int32), ("p", C.c_double * 8)]
 

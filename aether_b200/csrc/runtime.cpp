@@ -1385,6 +1385,63 @@ aefdtd_status aefdtd_get_normal_spectra(aefdtd_sim *s, double *out, int32_t nl) 
     });
 }
 
+// Box_Spect_Poynting (s_spec_power.cpp:124-232): six planar spectral Poynting
+// faces, xm, xp, ym, yp, zm, zp, on the faces of the box; flux = their sum in
+// that order.
+aefdtd_status aefdtd_add_box_sensor(aefdtd_sim *s, const aefdtd_box_sensor_desc *d, int32_t *id) {
+    if (!s || !d) return AEFDTD_BAD_ARG;
+    const int x1 = d->box[0], x2 = d->box[1], y1 = d->box[2], y2 = d->box[3], z1 = d->box[4], z2 = d->box[5];
+    const int fb[6][7] = {{AEFDTD_NORMAL_XM, x1, x1 + 1, y1, y2, z1, z2}, {AEFDTD_NORMAL_X, x2 - 1, x2, y1, y2, z1, z2},
+                          {AEFDTD_NORMAL_YM, x1, x2, y1, y1 + 1, z1, z2}, {AEFDTD_NORMAL_Y, x1, x2, y2 - 1, y2, z1, z2},
+                          {AEFDTD_NORMAL_ZM, x1, x2, y1, y2, z1, z1 + 1}, {AEFDTD_NORMAL_Z, x1, x2, y1, y2, z2 - 1, z2}};
+    int n = 0;
+    for (int f = 0; f < 6; f++) n += !(d->disabled & (1 << f));
+    if (n == 0 || x2 <= x1 || y2 <= y1 || z2 <= z1 || d->nl < 1) {
+        s->last_error = "a box needs positive extents, nl >= 1 and at least one face";
+        return AEFDTD_BAD_ARG;
+    }
+    if (s->sensors.size() + n > (size_t)kMaxGather) {
+        s->last_error = "a box takes one planar sensor per face; at most 8 per simulation";
+        return AEFDTD_BAD_ARG;
+    }
+    std::array<int, 6> ids;
+    ids.fill(-1);
+    for (int f = 0; f < 6; f++) {
+        if (d->disabled & (1 << f)) continue;
+        aefdtd_sensor_desc sd{};
+        sd.orientation = fb[f][0];
+        for (int k = 0; k < 6; k++) sd.box[k] = fb[f][1 + k];
+        sd.nl = d->nl;
+        sd.lambda_min = d->lambda_min;
+        sd.lambda_max = d->lambda_max;
+        int32_t sid = -1;
+        const aefdtd_status st = aefdtd_add_planar_sensor(s, &sd, &sid);
+        if (st != AEFDTD_OK) return st;
+        ids[f] = sid;
+    }
+    s->boxes.push_back(ids);
+    if (id) *id = (int32_t)s->boxes.size() - 1;
+    return AEFDTD_OK;
+}
+
+aefdtd_status aefdtd_get_box_flux(aefdtd_sim *s, int32_t id, double *out, int32_t nl) {
+    if (!s || !out) return AEFDTD_BAD_ARG;
+    if (id < 0 || id >= (int)s->boxes.size()) {
+        s->last_error = "unknown box sensor";
+        return AEFDTD_BAD_ARG;
+    }
+    std::vector<double> face(std::max(nl, 1));
+    for (int l = 0; l < nl; l++) out[l] = 0;
+    for (int f = 0; f < 6; f++) {
+        const int sid = s->boxes[id][f];
+        if (sid < 0) continue;
+        const aefdtd_status st = aefdtd_get_sensor_flux(s, sid, face.data(), nl);
+        if (st != AEFDTD_OK) return st;
+        for (int l = 0; l < nl; l++) out[l] += face[l];
+    }
+    return AEFDTD_OK;
+}
+
 aefdtd_status aefdtd_get_sensor_shape(aefdtd_sim *s, int32_t id, int32_t *span1, int32_t *span2, int32_t *nl) {
     if (!s || id < 0 || id >= (int)s->sensors.size()) return AEFDTD_BAD_ARG;
     if (span1) *span1 = s->sensors[id]->span1;

@@ -11,6 +11,7 @@
 #include <cstring>
 #include <numbers>
 #include <string>
+#include <array>
 #include <map>
 #include <vector>
 
@@ -199,6 +200,7 @@ struct aefdtd_sim {
     // custom mode
     std::vector<Osc> oscs;
     std::vector<PlaneSensor *> sensors;
+    std::vector<std::array<int, 6>> boxes;   // box sensors: planar sensor per face (-1: disabled)
     // half-step work lists: (x0, y0, k0, k1) items of 32 x 4 columns x a
     // z-chunk, in one device array: the E groups, then the H groups
     bool work_dirty = true;

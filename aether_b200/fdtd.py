@@ -86,6 +86,26 @@ class Simulation:
     def reset(self):
         self._c(self._lib.aefdtd_reset(self._h))
 
+    def add_box_sensor(self, box, nl, lambda_min, lambda_max, disabled=0) -> int:
+        """Box spectral Poynting sensor: six planar faces (bits of `disabled`:
+        xm, xp, ym, yp, zm, zp); returns the box id."""
+        d = A.BoxSensorDesc()
+        for k in range(6):
+            d.box[k] = int(box[k])
+        d.nl, d.disabled = int(nl), int(disabled)
+        d.lambda_min, d.lambda_max = float(lambda_min), float(lambda_max)
+        bid = C.c_int32(-1)
+        self._c(self._lib.aefdtd_add_box_sensor(self._h, C.byref(d), C.byref(bid)))
+        self.box_nl = getattr(self, "box_nl", {})
+        self.box_nl[bid.value] = int(nl)
+        return bid.value
+
+    def box_flux(self, bid: int) -> np.ndarray:
+        nl = self.box_nl[bid]
+        out = np.empty(nl)
+        self._c(self._lib.aefdtd_get_box_flux(self._h, int(bid), out.ctypes.data_as(C.POINTER(C.c_double)), nl))
+        return out
+
     def set_completion(self, coeff=1e-3, check_every=500):
         """Energy-mode completion sensor (coeff <= 0: off)."""
         self._c(self._lib.aefdtd_set_completion(self._h, float(coeff), int(check_every)))

@@ -248,6 +248,22 @@ aefdtd_status aefdtd_get_sensor_flux(aefdtd_sim *sim, int32_t sensor_id, double 
 aefdtd_status aefdtd_get_sensor_dft(aefdtd_sim *sim, int32_t sensor_id, double *out, size_t count);
 aefdtd_status aefdtd_get_sensor_shape(aefdtd_sim *sim, int32_t sensor_id, int32_t *span1, int32_t *span2, int32_t *nl);
 
+/* Box spectral Poynting sensor (Box_Spect_Poynting, s_spec_power.cpp:124-232):
+ * planar spectral Poynting sensors on the six faces of the box (structure
+ * cells x1,x2,y1,y2,z1,z2): xm on x1, xp on x2-1, ym, yp, zm, zp likewise,
+ * each face created as by aefdtd_add_planar_sensor (one of the 8 planar
+ * sensors per simulation per face). disabled: bits 0..5 = xm, xp, ym, yp, zm,
+ * zp (Sensor::disable_*). The flux is the sum of the face fluxes in that
+ * order (Box_Spect_Poynting::treat). */
+typedef struct aefdtd_box_sensor_desc {
+    int32_t box[6];
+    int32_t nl;
+    int32_t disabled;
+    double lambda_min, lambda_max;
+} aefdtd_box_sensor_desc;
+aefdtd_status aefdtd_add_box_sensor(aefdtd_sim *sim, const aefdtd_box_sensor_desc *desc, int32_t *box_id);
+aefdtd_status aefdtd_get_box_flux(aefdtd_sim *sim, int32_t box_id, double *out, int32_t nl);
+
 /* Completion sensor in energy mode (CompletionSensor(coeff),
  * s_completion.cpp:20-24, 39-43, 121-130, 177-190; checked by the drivers at
  * normal_incidence.cpp:417-427 and default_fdtd.cpp:193-203). After every

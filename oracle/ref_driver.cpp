@@ -42,6 +42,15 @@ int g_cc_every = 500;
 int g_cc_stop = -1;
 double g_cc_last = 0, g_cc_max = 0;
 
+// One box spectral Poynting sensor (Box_Spect_Poynting, s_spec_power.cpp:
+// 124-232), set by aeref_set_box: fed after the planar sensors; its
+// rsp_result is kept for aeref_box_result.
+bool g_box_on = false;
+int g_box[6] = {0, 0, 0, 0, 0, 0};
+int g_box_nl = 0, g_box_mask = 0;
+double g_box_lmin = 0, g_box_lmax = 0;
+std::vector<double> g_box_result;
+
 int ref_orientation(int o) {
     static const int tbl[6] = {NORMAL_X, NORMAL_XM, NORMAL_Y, NORMAL_YM, NORMAL_Z, NORMAL_ZM};
     return (o >= 0 && o < 6) ? tbl[o] : NORMAL_UNDEF;
@@ -162,6 +171,17 @@ int aeref_run(const aefdtd_grid_desc *g, const uint32_t *map,
         sp->set_silent(true);
         sensors.push_back(sp);
     }
+    Box_Spect_Poynting *bx = nullptr;
+    if (g_box_on) {
+        bx = new Box_Spect_Poynting(g_box[0], g_box[1], g_box[2], g_box[3], g_box[4], g_box[5]);
+        bx->disable_xm = g_box_mask & 1; bx->disable_xp = g_box_mask & 2;
+        bx->disable_ym = g_box_mask & 4; bx->disable_yp = g_box_mask & 8;
+        bx->disable_zm = g_box_mask & 16; bx->disable_zp = g_box_mask & 32;
+        bx->set_spectrum(g_box_nl, g_box_lmin, g_box_lmax);
+        bx->name = "aeref_box";
+        bx->set_silent(true);
+        bx->link(fdtd, std::filesystem::path("."));
+    }
     std::vector<Source *> sources;
     if (g->mode == AEFDTD_MODE_CUSTOM) {
         for (int s = 0; s < nsrc; s++) {
@@ -222,6 +242,7 @@ int aeref_run(const aefdtd_grid_desc *g, const uint32_t *map,
                     fdtd.Hy(i, j, zs_e - 1) -= fdtd.dtdmz * inj_Ex;
                 }
             for (auto *s : sensors) s->feed(fdtd);
+            if (bx) bx->feed(fdtd);
             if (cpl) cpl->feed(fdtd);   // fed with the sensors, after the planar ones
 
             tb = (t + 0.5) * Dt;
@@ -313,6 +334,7 @@ int aeref_run(const aefdtd_grid_desc *g, const uint32_t *map,
             for (auto *s : sources) s->inject_E(fdtd);
             fdtd.update_H();
             for (auto *s : sensors) s->feed(fdtd);
+            if (bx) bx->feed(fdtd);
             for (auto *s : sources) s->inject_H(fdtd);
         }
         if (loop_seconds) loop_seconds[0] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -326,6 +348,12 @@ int aeref_run(const aefdtd_grid_desc *g, const uint32_t *map,
             for (int l = 0; l < sensors[s]->Nl; l++) flux_out[off + l] = sensors[s]->rsp_result[l];
         off += sensors[s]->Nl;
     }
+    if (bx) {
+        bx->treat();
+        g_box_result.assign(bx->Nl, 0.0);
+        for (int l = 0; l < bx->Nl; l++) g_box_result[l] = bx->rsp_result[l];
+        delete bx;
+    }
     for (auto *s : sensors) delete s;
     for (auto *s : sources) delete s;
     delete fp;
@@ -335,6 +363,25 @@ int aeref_run(const aefdtd_grid_desc *g, const uint32_t *map,
 
 /* Number of worker threads the reference core uses per FDTD object. */
 int aeref_threads(void) { return max_threads_number(); }
+
+/* Box spectral Poynting sensor for the following aeref_run calls: box in
+ * structure cells, disabled_mask bits xm, xp, ym, yp, zm, zp; nl <= 0 turns
+ * it off. */
+void aeref_set_box(const int32_t box[6], int32_t nl, double lmin, double lmax, int32_t disabled_mask) {
+    g_box_on = nl > 0;
+    for (int i = 0; i < 6; i++) g_box[i] = box ? box[i] : 0;
+    g_box_nl = nl;
+    g_box_lmin = lmin;
+    g_box_lmax = lmax;
+    g_box_mask = disabled_mask;
+}
+
+/* rsp_result of the box after the last aeref_run (nl values). */
+int aeref_box_result(double *out, int32_t nl) {
+    if ((int)g_box_result.size() != nl) return 1;
+    for (int l = 0; l < nl; l++) out[l] = g_box_result[l];
+    return 0;
+}
 
 /* Completion sensor for the following aeref_run calls (normal mode):
  * coeff <= 0 disables; every = the driver's cc_step. */

@@ -108,3 +108,21 @@ def run_ref_completion(scene, coeff, every, nsteps=None):
         lib.aeref_set_completion(0.0, 500)
     out.update(stop=stop.value, energy_last=last.value, energy_max=mx.value)
     return out
+
+
+def run_ref_box(scene, box, nl, lambda_min, lambda_max, disabled=0, nsteps=None):
+    """The reference core with one Box_Spect_Poynting sensor: the run dict of
+    `run` plus 'box_flux' (its rsp_result, nl values)."""
+    lib = C.CDLL(REF_PATH)
+    lib.aeref_set_box.argtypes = [_P(C.c_int32), C.c_int32, C.c_double, C.c_double, C.c_int32]
+    lib.aeref_box_result.argtypes = [_P(C.c_double), C.c_int32]
+    b = (C.c_int32 * 6)(*box)
+    lib.aeref_set_box(b, nl, lambda_min, lambda_max, disabled)
+    try:
+        out = run(scene, "ref", nsteps=nsteps, want_fields=False)
+        res = np.zeros(nl)
+        assert lib.aeref_box_result(res.ctypes.data_as(_P(C.c_double)), nl) == 0
+    finally:
+        lib.aeref_set_box(None, 0, 0.0, 0.0, 0)
+    out["box_flux"] = res
+    return out

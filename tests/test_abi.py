@@ -174,6 +174,7 @@ int main(void) {
          sizeof(aefdtd_server_opts), sizeof(aefdtd_job_desc), sizeof(aefdtd_job_info), sizeof(aefdtd_server_stats));
   printf("%zu %zu %zu %zu\\n", offsetof(aefdtd_batch_info, class_kchunk), offsetof(aefdtd_server_opts, batch),
          offsetof(aefdtd_job_desc, steps), offsetof(aefdtd_server_stats, gcells_per_s));
+  printf("%zu %zu\\n", sizeof(aefdtd_box_sensor_desc), offsetof(aefdtd_box_sensor_desc, lambda_min));
   return 0;
 }
 """
@@ -189,3 +190,4 @@ int main(void) {
                      C.sizeof(A.JobInfo), C.sizeof(A.ServerStats)]
     assert offs == [A.BatchInfo.class_kchunk.offset, A.ServerOpts.batch.offset, A.JobDesc.steps.offset,
                     A.ServerStats.gcells_per_s.offset]
+    assert [int(x) for x in lines[2].split()] == [C.sizeof(A.BoxSensorDesc), A.BoxSensorDesc.lambda_min.offset]
