@@ -235,6 +235,7 @@ template <typename T, typename Tid> void aefdtd_batch::build_subset(BatchSubset 
         WorkSplit &w = half == 0 ? u.wsE : u.wsH;
         w.unroll = 2;
         w.tile_y = sc.tile_y;
+        w.pair_mask = 0;
         for (int g = 0; g < kGroups; g++) {
             w.off[g] = (int)(all.size() / 4);
             for (size_t li = 0; li < u.members.size(); li++) {
@@ -619,7 +620,8 @@ aefdtd_status aefdtd_batch_add(aefdtd_batch *b, aefdtd_sim *s, int32_t steps) {
         if (s->Nz >= 32768) fail(AEFDTD_BAD_ARG, "batch members need Nz < 32768 (k1 << 16 in an int32 item)");
         s->set_device();
         s->finalize_tables();
-        if (s->work_dirty) s->build_work();
+        s->pair_mask = 0;            // the batched kernels take 32-column items
+        if (s->work_dirty || s->wsE.pair_mask || s->wsH.pair_mask) s->build_work();
         if (!b->typed) {
             b->typed = true;
             b->fp64 = s->fp64;

@@ -102,6 +102,9 @@ void aefdtd_sim::construct(const aefdtd_grid_desc *d) {
     if (const char *kc = std::getenv("AEFDTD_KCHUNK")) kchunk_override = std::max(0, atoi(kc));
     if (const char *zu = std::getenv("AEFDTD_ZUNROLL")) zunroll = atoi(zu) >= 2 ? 2 : 1;
     if (const char *pf = std::getenv("AEFDTD_PREFETCH")) prefetch_l2 = atoi(pf) != 0;
+    // two cells per thread: FP32 interior and z-CPML items, FP64 z-CPML items
+    pair_mask = fp64 ? (1u << kGroupPmlZ) : (1u << kGroupInterior) | (1u << kGroupPmlZ);
+    if (const char *pm = std::getenv("AEFDTD_PAIR")) pair_mask = unsigned(atoi(pm)) & 3u;
     if (const char *ty = std::getenv("AEFDTD_TILE_Y")) {
         const int v = atoi(ty);
         tile_y = (v == 2 || v == 8) ? v : 4;
@@ -882,8 +885,11 @@ void aefdtd_sim::accumulate_timing(int L) {
 // columns by kchunk planes; an item is "boundary" when any of its cells is in
 // a CPML range or PEC plane of either half-step, on the injection plane, in
 // an oscillator box, or of a dispersive material; all others are "interior"
-// and run the curl-only kernels.
+// and run the curl-only kernels. Groups in pair_mask (two cells per thread,
+// even Nx only) take 64-column items where both 32-column tiles of a pair
+// fall in the group, and 32-column items flagged kHalfItem elsewhere.
 void aefdtd_sim::build_work() {
+    const unsigned pmask = (Nx % 2 == 0) ? pair_mask & ((1u << kGroupInterior) | (1u << kGroupPmlZ)) : 0u;
     const int tx = kTileXHost, ty = tile_y;
     const int ntx = (Nx + tx - 1) / tx, nty = (Ny + ty - 1) / ty;
     const long long tiles = (long long)ntx * nty;
@@ -948,29 +954,61 @@ void aefdtd_sim::build_work() {
         if (f == kPZ) return (int)kGroupPmlZ;
         return (int)kGroupAll;
     };
-    // items: within each tile and z-chunk, runs of planes of one group;
-    // dispersive E planes one plane per item (their cells carry the pole state)
+    // items: within each tile (or pair of tiles) and z-chunk, runs of planes
+    // of one group; dispersive E planes one plane per item (their cells carry
+    // the pole state)
     std::vector<int> v[2][kGroups];
+    const int step_a = pmask ? 2 : 1;
     for (int c = 0; c < nch; c++)
         for (int b = 0; b < nty; b++)
-            for (int a = 0; a < ntx; a++) {
+            for (int a = 0; a < ntx; a += step_a) {
                 const int z0 = c * kchunk, z1 = std::min(Nz, (c + 1) * kchunk);
                 for (int half = 0; half < 2; half++) {
+                    auto grp = [&](int t, int k) {
+                        const unsigned f = feat[(size_t(k) * nty + b) * ntx + t];
+                        return half == 0 ? group_e(f) : group_h(f);
+                    };
+                    auto emit = [&](int g, int x0, int za, int zb) {
+                        std::vector<int> &dst = v[half][g];
+                        dst.push_back(x0);
+                        dst.push_back(b * ty);
+                        dst.push_back(za);
+                        dst.push_back(zb);
+                    };
+                    // runs of one group within [za, zb) of tile t
+                    auto runs = [&](int t, int za, int zb) {
+                        int z = za;
+                        while (z < zb) {
+                            const int g = grp(t, z);
+                            int ze = z + 1;
+                            if (!(half == 0 && g == kGroupDisp))
+                                while (ze < zb && grp(t, ze) == g) ze++;
+                            emit(g, t * tx | ((pmask >> g) & 1u ? kHalfItem : 0), z, ze);
+                            z = ze;
+                        }
+                    };
+                    if (!pmask) {
+                        runs(a, z0, z1);
+                        continue;
+                    }
+                    const bool right = a + 1 < ntx;
+                    // plane k pairs when both tiles (or the last, lone tile) are in one pair group
+                    auto paired = [&](int k) {
+                        const int g = grp(a, k);
+                        return ((pmask >> g) & 1u) && (!right || grp(a + 1, k) == g);
+                    };
                     int z = z0;
                     while (z < z1) {
-                        auto grp = [&](int k) {
-                            const unsigned f = feat[(size_t(k) * nty + b) * ntx + a];
-                            return half == 0 ? group_e(f) : group_h(f);
-                        };
-                        const int g = grp(z);
                         int ze = z + 1;
-                        if (!(half == 0 && g == kGroupDisp))
-                            while (ze < z1 && grp(ze) == g) ze++;
-                        std::vector<int> &dst = v[half][g];
-                        dst.push_back(a * tx);
-                        dst.push_back(b * ty);
-                        dst.push_back(z);
-                        dst.push_back(ze);
+                        if (paired(z)) {
+                            const int g = grp(a, z);
+                            while (ze < z1 && paired(ze) && grp(a, ze) == g) ze++;
+                            emit(g, a * tx, z, ze);
+                        } else {
+                            while (ze < z1 && !paired(ze)) ze++;
+                            runs(a, z, ze);
+                            if (right) runs(a + 1, z, ze);
+                        }
                         z = ze;
                     }
                 }
@@ -980,6 +1018,7 @@ void aefdtd_sim::build_work() {
         WorkSplit &w = half == 0 ? wsE : wsH;
         w.unroll = zunroll;
         w.tile_y = tile_y;
+        w.pair_mask = pmask;
         for (int g = 0; g < kGroups; g++) {
             w.off[g] = (int)(all.size() / 4);
             w.n[g] = (int)(v[half][g].size() / 4);
@@ -987,7 +1026,8 @@ void aefdtd_sim::build_work() {
             long long c = 0;
             for (size_t k = 0; k < v[half][g].size(); k += 4) {
                 const int *it = &v[half][g][k];
-                c += (long long)(std::min(it[0] + tx, Nx) - it[0]) * (std::min(it[1] + ty, Ny) - it[1]) * (it[3] - it[2]);
+                const int x0 = it[0] & ~kHalfItem, gw = ((pmask >> g) & 1u) && !(it[0] & kHalfItem) ? 2 * tx : tx;
+                c += (long long)(std::min(x0 + gw, Nx) - x0) * (std::min(it[1] + ty, Ny) - it[1]) * (it[3] - it[2]);
             }
             grp_cells[half][g] = c;
         }

@@ -265,6 +265,7 @@ struct aefdtd_sim {
     int kchunk_override = 0;
     int zunroll = 2;
     int tile_y = kTileYHost;        // tile height of the work items (2, 4 or 8)
+    unsigned pair_mask = 0;         // groups run two cells per thread (WorkSplit::pair_mask; even Nx only)
     bool prefetch_l2 = true;        // interior kernels prefetch their item's planes into L2
     // completion sensor, energy mode (CompletionSensor(coeff), s_completion.cpp)
     double cc_coeff = 0;            // > 0: enabled

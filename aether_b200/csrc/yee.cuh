@@ -621,6 +621,256 @@ __device__ __forceinline__ void h_boundary_body(const StepArgs<T, Tid> &a, int q
     }
 }
 
+// ---- interior items, two cells per thread along x ------------------------
+// The same curl updates (and PZ phases) on items of 64 x TY columns: each
+// thread owns columns i0 = x0 + 2 lane and i0 + 1 and moves both with 8-byte
+// (FP32) or 16-byte (FP64) loads. The x-1 (E) or x+1 (H) neighbour of the
+// pair comes from the adjacent lane by a warp shuffle; the lane at the tile
+// edge loads it, with the periodic wrap. Needs Nx even (vector alignment).
+// An item whose x0 carries kHalfItem covers 32 columns (the other half of its
+// 64-column tile belongs to another group). Per cell the arithmetic and its
+// order are those of the one-cell bodies.
+template <typename T> struct Vec2;
+template <> struct Vec2<float> { using type = float2; };
+template <> struct Vec2<double> { using type = double2; };
+template <typename Tid> struct IdPair;
+template <> struct IdPair<uint8_t> { using type = uchar2; };
+template <> struct IdPair<uint16_t> { using type = ushort2; };
+constexpr unsigned kFullMask = 0xffffffffu;
+
+template <typename V, typename P> __device__ __forceinline__ V ldg2(const P *p) {
+    return __ldg(reinterpret_cast<const V *>(p));
+}
+template <typename V, typename P> __device__ __forceinline__ V ld2(const P *p) { return *reinterpret_cast<const V *>(p); }
+template <typename V, typename P> __device__ __forceinline__ void st2(P *p, V v) { *reinterpret_cast<V *>(p) = v; }
+
+template <typename T, typename Tid, bool PZ>
+__device__ __forceinline__ void e_interior_v2_body(const StepArgs<T, Tid> &a, int q, int4 it) {
+    using T2 = typename Vec2<T>::type;
+    using I2 = typename IdPair<Tid>::type;
+    const int lane = threadIdx.x;
+    const int j = it.y + threadIdx.y;
+    if (j >= a.Ny) return;                          // a whole warp: one row
+    // lanes past the item (kHalfItem: 32 columns) or the grid read valid
+    // memory, feed the shuffles and store nothing
+    const int i0 = (it.x & ~kHalfItem) + 2 * lane;
+    const bool act = i0 < a.Nx && ((it.x & kHalfItem) == 0 || lane < 16);
+    const int ic = i0 < a.Nx ? i0 : a.Nx - 2;
+    const long long NxNy = a.NxNy;
+    const int jm = (j == 0) ? a.Ny - 1 : j - 1;
+    const int im = (ic == 0) ? a.Nx - 1 : ic - 1;   // used by lane 0 only
+    const long long col = ic + (long long)j * a.Nx;
+    const long long coly = ic + (long long)jm * a.Nx;
+    const long long colx = im + (long long)j * a.Nx;
+    const long long colm = ic + (long long)j * a.mpitch;
+    const long long mNxNy = (long long)a.mpitch * a.Ny;
+    const T *__restrict__ Hx = a.Hx;
+    const T *__restrict__ Hy = a.Hy;
+    const T *__restrict__ Hz = a.Hz;
+    T *__restrict__ Ex = a.Ex;
+    T *__restrict__ Ey = a.Ey;
+    T *__restrict__ Ez = a.Ez;
+    const MatCoef<T> *__restrict__ coef = a.coef;
+    const T2 ikx = ldg2<T2>(a.ikx + ic);
+    const T iky = __ldg(a.iky + j);
+    const int kmi = (it.z == 0) ? a.Nz - 1 : it.z - 1;
+    T2 hx_km = ldg2<T2>(Hx + col + kmi * NxNy);
+    T2 hy_km = ldg2<T2>(Hy + col + kmi * NxNy);
+    if (a.prefetch) {
+        for (int k = it.z; k < it.w; ++k) {
+            const long long o = (long long)k * NxNy;
+            prefetch_l2(Hx + col + o); prefetch_l2(Hy + col + o); prefetch_l2(Hz + col + o);
+            if (lane == 0) { prefetch_l2(Hz + colx + o); prefetch_l2(Hy + colx + o); }
+            if (threadIdx.y == 0) { prefetch_l2(Hz + coly + o); prefetch_l2(Hx + coly + o); }
+            prefetch_l2(Ex + col + o); prefetch_l2(Ey + col + o); prefetch_l2(Ez + col + o);
+            prefetch_l2(a.mat + colm + (long long)k * mNxNy);
+            if constexpr (PZ) {
+                if (a.pz && ((k >= 1 && k < a.pml_zm) || (k >= a.Nz - a.pml_zp + 1))) {
+                    const int zn = (k < a.pml_zm) ? k : k - (a.Nz - a.pml_zp) + a.pml_zm;
+                    prefetch_l2(a.psi_z0 + col + (long long)zn * NxNy);
+                    prefetch_l2(a.psi_z1 + col + (long long)zn * NxNy);
+                }
+            }
+        }
+    }
+    for (int k = it.z; k < it.w; ++k) {
+        const long long o = (long long)k * NxNy;
+        const T2 hx = ldg2<T2>(Hx + col + o), hy = ldg2<T2>(Hy + col + o), hz = ldg2<T2>(Hz + col + o);
+        const T2 hz_jm = ldg2<T2>(Hz + coly + o), hx_jm = ldg2<T2>(Hx + coly + o);
+        T hz_edge = 0, hy_edge = 0;
+        if (lane == 0) { hz_edge = __ldg(Hz + colx + o); hy_edge = __ldg(Hy + colx + o); }
+        const T2 ex = ld2<T2>(Ex + col + o), ey = ld2<T2>(Ey + col + o), ez = ld2<T2>(Ez + col + o);
+        const I2 mm = ldg2<I2>(a.mat + colm + (long long)k * mNxNy);
+        T2 p0, p1;
+        T bzk = 0, czk = 0;
+        bool ze = false;
+        long long pzi = 0;
+        if constexpr (PZ) {
+            // E-side z range [1, pml_zm) and [Nz - pml_zp + 1, Nz) (fdtd_pml.cpp:547,559)
+            ze = a.pz && ((k >= 1 && k < a.pml_zm) || (k >= a.Nz - a.pml_zp + 1));
+            if (ze) {
+                const int zn = (k < a.pml_zm) ? k : k - (a.Nz - a.pml_zp) + a.pml_zm;
+                pzi = col + (long long)zn * NxNy;
+                p0 = ld2<T2>(a.psi_z0 + pzi);
+                p1 = ld2<T2>(a.psi_z1 + pzi);
+                bzk = __ldg(a.bz + k);
+                czk = __ldg(a.cz + k);
+            }
+        }
+        // x-1 neighbours: column i0 - 1 from the previous lane, or loaded at the edge
+        const T hz_up = __shfl_up_sync(kFullMask, hz.y, 1), hy_up = __shfl_up_sync(kFullMask, hy.y, 1);
+        const T hz_im0 = lane == 0 ? hz_edge : hz_up, hy_im0 = lane == 0 ? hy_edge : hy_up;
+        const MatCoef<T> *ca = coef + mm.x, *cb = coef + mm.y;
+        const T C1a = __ldg(&ca->C1), C2xa = __ldg(&ca->C2x), C2ya = __ldg(&ca->C2y), C2za = __ldg(&ca->C2z);
+        const T C1b = __ldg(&cb->C1), C2xb = __ldg(&cb->C2x), C2yb = __ldg(&cb->C2y), C2zb = __ldg(&cb->C2z);
+        const T ikz = __ldg(a.ikz + k);
+        T2 ne, nf, ng;   // Ex, Ey, Ez of the pair
+        ne.x = (C1a * ex.x + (C2ya * iky) * (hz.x - hz_jm.x)) - (C2za * ikz) * (hy.x - hy_km.x);
+        nf.x = (C1a * ey.x + (C2za * ikz) * (hx.x - hx_km.x)) - (C2xa * ikx.x) * (hz.x - hz_im0);
+        ng.x = (C1a * ez.x + (C2xa * ikx.x) * (hy.x - hy_im0)) - (C2ya * iky) * (hx.x - hx_jm.x);
+        ne.y = (C1b * ex.y + (C2yb * iky) * (hz.y - hz_jm.y)) - (C2zb * ikz) * (hy.y - hy_km.y);
+        nf.y = (C1b * ey.y + (C2zb * ikz) * (hx.y - hx_km.y)) - (C2xb * ikx.y) * (hz.y - hz.x);
+        ng.y = (C1b * ez.y + (C2xb * ikx.y) * (hy.y - hy.x)) - (C2yb * iky) * (hx.y - hx_jm.y);
+        if constexpr (PZ) {
+            if (ze) {
+                const T C4a = __ldg(&ca->C4), C4b = __ldg(&cb->C4);
+                T2 ps0, ps1;
+                ps0.x = cpml_rec(bzk, p0.x, czk, hy.x - hy_km.x);   // Ex: PsiExz
+                ps0.y = cpml_rec(bzk, p0.y, czk, hy.y - hy_km.y);
+                ne.x -= C4a * ps0.x;
+                ne.y -= C4b * ps0.y;
+                ps1.x = cpml_rec(bzk, p1.x, czk, hx.x - hx_km.x);   // Ey: PsiEyz
+                ps1.y = cpml_rec(bzk, p1.y, czk, hx.y - hx_km.y);
+                nf.x += C4a * ps1.x;
+                nf.y += C4b * ps1.y;
+                if (act) {
+                    st2<T2>(a.psi_z0 + pzi, ps0);
+                    st2<T2>(a.psi_z1 + pzi, ps1);
+                }
+            }
+            if (a.pz && k == 0) { ne.x = 0; ne.y = 0; nf.x = 0; nf.y = 0; }
+        }
+        if (act) {
+            st2<T2>(Ex + col + o, ne);
+            st2<T2>(Ey + col + o, nf);
+            st2<T2>(Ez + col + o, ng);
+        }
+        hx_km = hx;
+        hy_km = hy;
+    }
+}
+
+template <typename T, typename Tid, bool PZ>
+__device__ __forceinline__ void h_interior_v2_body(const StepArgs<T, Tid> &a, int q, int4 it) {
+    using T2 = typename Vec2<T>::type;
+    const int lane = threadIdx.x;
+    const int j = it.y + threadIdx.y;
+    if (j >= a.Ny) return;
+    const int i0 = (it.x & ~kHalfItem) + 2 * lane;
+    const bool act = i0 < a.Nx && ((it.x & kHalfItem) == 0 || lane < 16);
+    const int ic = i0 < a.Nx ? i0 : a.Nx - 2;
+    // x+1 neighbour of the pair's second cell: the next lane's first, or loaded
+    // (last lane, or the grid end with its periodic wrap)
+    const bool edge = lane == 31 || ic + 2 >= a.Nx;
+    const int ipn = (ic + 2 >= a.Nx) ? ic + 2 - a.Nx : ic + 2;
+    const long long NxNy = a.NxNy;
+    const int jp = (j == a.Ny - 1) ? 0 : j + 1;
+    const long long col = ic + (long long)j * a.Nx;
+    const long long colx = ipn + (long long)j * a.Nx;
+    const long long coly = ic + (long long)jp * a.Nx;
+    const T *__restrict__ Ex = a.Ex;
+    const T *__restrict__ Ey = a.Ey;
+    const T *__restrict__ Ez = a.Ez;
+    T *__restrict__ Hx = a.Hx;
+    T *__restrict__ Hy = a.Hy;
+    T *__restrict__ Hz = a.Hz;
+    const T2 ikx = ldg2<T2>(a.ikx + ic);
+    T2 ax;
+    ax.x = a.dtdmx * ikx.x;
+    ax.y = a.dtdmx * ikx.y;
+    const T ay = a.dtdmy * __ldg(a.iky + j);
+    T2 ex = ldg2<T2>(Ex + col + it.z * NxNy);
+    T2 ey = ldg2<T2>(Ey + col + it.z * NxNy);
+    if (a.prefetch) {
+        for (int k = it.z; k < it.w; ++k) {
+            const int kp = (k == a.Nz - 1) ? 0 : k + 1;
+            const long long o = (long long)k * NxNy, op = (long long)kp * NxNy;
+            prefetch_l2(Ex + col + op); prefetch_l2(Ey + col + op); prefetch_l2(Ez + col + o);
+            if (edge) { prefetch_l2(Ez + colx + o); prefetch_l2(Ey + colx + o); }
+            if (threadIdx.y == blockDim.y - 1) { prefetch_l2(Ez + coly + o); prefetch_l2(Ex + coly + o); }
+            prefetch_l2(Hx + col + o); prefetch_l2(Hy + col + o); prefetch_l2(Hz + col + o);
+            if constexpr (PZ) {
+                if (a.pz && ((k < a.pml_zm) || (k >= a.Nz - a.pml_zp && k < a.Nz - 1))) {
+                    const int zn = (k < a.pml_zm) ? k : k - (a.Nz - a.pml_zp) + a.pml_zm;
+                    prefetch_l2(a.psi_z0 + col + (long long)zn * NxNy);
+                    prefetch_l2(a.psi_z1 + col + (long long)zn * NxNy);
+                }
+            }
+        }
+    }
+    for (int k = it.z; k < it.w; ++k) {
+        const int kp = (k == a.Nz - 1) ? 0 : k + 1;
+        const long long o = (long long)k * NxNy, op = (long long)kp * NxNy;
+        const T2 ex_kp = ldg2<T2>(Ex + col + op), ey_kp = ldg2<T2>(Ey + col + op);
+        const T2 ez = ldg2<T2>(Ez + col + o);
+        const T2 ez_jp = ldg2<T2>(Ez + coly + o), ex_jp = ldg2<T2>(Ex + coly + o);
+        T ez_edge = 0, ey_edge = 0;
+        if (edge) { ez_edge = __ldg(Ez + colx + o); ey_edge = __ldg(Ey + colx + o); }
+        const T2 hx = ld2<T2>(Hx + col + o), hy = ld2<T2>(Hy + col + o), hz = ld2<T2>(Hz + col + o);
+        T2 p0, p1;
+        T bzk = 0, czk = 0;
+        bool zh = false;
+        long long pzi = 0;
+        if constexpr (PZ) {
+            // H-side z range [0, pml_zm) and [Nz - pml_zp, Nz - 1) (fdtd_pml.cpp:775,784)
+            zh = a.pz && ((k < a.pml_zm) || (k >= a.Nz - a.pml_zp && k < a.Nz - 1));
+            if (zh) {
+                const int zn = (k < a.pml_zm) ? k : k - (a.Nz - a.pml_zp) + a.pml_zm;
+                pzi = col + (long long)zn * NxNy;
+                p0 = ld2<T2>(a.psi_z0 + pzi);
+                p1 = ld2<T2>(a.psi_z1 + pzi);
+                bzk = __ldg(a.bz + k);
+                czk = __ldg(a.cz + k);
+            }
+        }
+        const T ez_dn = __shfl_down_sync(kFullMask, ez.x, 1), ey_dn = __shfl_down_sync(kFullMask, ey.x, 1);
+        const T ez_ip1 = edge ? ez_edge : ez_dn, ey_ip1 = edge ? ey_edge : ey_dn;
+        const T az = a.dtdmz * __ldg(a.ikz + k);
+        T2 nh, ni, nk;   // Hx, Hy, Hz of the pair
+        nh.x = hx.x + (az * (ey_kp.x - ey.x) - ay * (ez_jp.x - ez.x));
+        ni.x = hy.x + (ax.x * (ez.y - ez.x) - az * (ex_kp.x - ex.x));
+        nk.x = hz.x + (ay * (ex_jp.x - ex.x) - ax.x * (ey.y - ey.x));
+        nh.y = hx.y + (az * (ey_kp.y - ey.y) - ay * (ez_jp.y - ez.y));
+        ni.y = hy.y + (ax.y * (ez_ip1 - ez.y) - az * (ex_kp.y - ex.y));
+        nk.y = hz.y + (ay * (ex_jp.y - ex.y) - ax.y * (ey_ip1 - ey.y));
+        if constexpr (PZ) {
+            if (zh) {
+                T2 ps0, ps1;
+                ps0.x = cpml_rec(bzk, p0.x, czk, ey_kp.x - ey.x);   // Hx: PsiHxz
+                ps0.y = cpml_rec(bzk, p0.y, czk, ey_kp.y - ey.y);
+                nh.x += a.dtm * ps0.x;
+                nh.y += a.dtm * ps0.y;
+                ps1.x = cpml_rec(bzk, p1.x, czk, ex_kp.x - ex.x);   // Hy: PsiHyz
+                ps1.y = cpml_rec(bzk, p1.y, czk, ex_kp.y - ex.y);
+                ni.x -= a.dtm * ps1.x;
+                ni.y -= a.dtm * ps1.y;
+                if (act) {
+                    st2<T2>(a.psi_z0 + pzi, ps0);
+                    st2<T2>(a.psi_z1 + pzi, ps1);
+                }
+            }
+            if (a.pz && k == a.Nz - 1) { nh.x = 0; nh.y = 0; ni.x = 0; ni.y = 0; }
+        }
+        if (act) {
+            st2<T2>(Hx + col + o, nh);
+            st2<T2>(Hy + col + o, ni);
+            st2<T2>(Hz + col + o, nk);
+        }
+        ex = ex_kp;
+        ey = ey_kp;
+    }
+}
+
 // ---- kernels -----------------------------------------------------------------
 // Register caps: at most 256 threads per CTA; the interior kernels keep the
 // register budget of 12 (U = 1, FP32) or 8 resident 128-thread CTAs per SM.
@@ -628,6 +878,8 @@ template <typename T, int U, bool PZ = false> struct InteriorBounds {
     static constexpr int kMinBlocks = PZ ? (sizeof(T) == 8 ? 2 : 3) : ((U == 1 && sizeof(T) == 4) ? 6 : 4);   // per 256 threads
     // batched forms keep the member's arguments in registers too
     static constexpr int kMinBlocksBatch = sizeof(T) == 8 ? 2 : 3;
+    // two cells per thread: FP64 pairs need about 80 registers
+    static constexpr int kMinBlocksVec2 = PZ ? (sizeof(T) == 8 ? 2 : 3) : (sizeof(T) == 8 ? 3 : 4);
 };
 constexpr int kMaxTileThreads = 256;
 
@@ -650,6 +902,17 @@ template <typename T, typename Tid, unsigned F>
 __global__ void __launch_bounds__(kMaxTileThreads) h_boundary(const __grid_constant__ StepArgs<T, Tid> a,
                                                               const int4 *__restrict__ items) {
     h_boundary_body<T, Tid, F>(a, a.q, items[blockIdx.x]);
+}
+
+template <typename T, typename Tid, bool PZ>
+__global__ void __launch_bounds__(kMaxTileThreads, InteriorBounds<T, 2, PZ>::kMinBlocksVec2)
+e_interior_v2(const __grid_constant__ StepArgs<T, Tid> a, const int4 *__restrict__ items) {
+    e_interior_v2_body<T, Tid, PZ>(a, a.q, items[blockIdx.x]);
+}
+template <typename T, typename Tid, bool PZ>
+__global__ void __launch_bounds__(kMaxTileThreads, InteriorBounds<T, 2, PZ>::kMinBlocksVec2)
+h_interior_v2(const __grid_constant__ StepArgs<T, Tid> a, const int4 *__restrict__ items) {
+    h_interior_v2_body<T, Tid, PZ>(a, a.q, items[blockIdx.x]);
 }
 
 // Batched forms: item (x0, y0, k0 | k1 << 16, instance), arguments of the
@@ -690,11 +953,13 @@ void launch_e_group_impl(const StepArgs<T, Tid> &a, const int4 *items, const Wor
     const dim3 blk(kTileX, w.tile_y);
     switch (g) {
         case kGroupInterior:
-            if (w.unroll >= 2) e_interior<T, Tid, 2><<<n, blk, 0, s>>>(a, p);
+            if (w.pair_mask & (1u << kGroupInterior)) e_interior_v2<T, Tid, false><<<n, blk, 0, s>>>(a, p);
+            else if (w.unroll >= 2) e_interior<T, Tid, 2><<<n, blk, 0, s>>>(a, p);
             else e_interior<T, Tid, 1><<<n, blk, 0, s>>>(a, p);
             break;
         case kGroupPmlZ:
-            if (w.unroll >= 2) e_interior<T, Tid, 2, true><<<n, blk, 0, s>>>(a, p);
+            if (w.pair_mask & (1u << kGroupPmlZ)) e_interior_v2<T, Tid, true><<<n, blk, 0, s>>>(a, p);
+            else if (w.unroll >= 2) e_interior<T, Tid, 2, true><<<n, blk, 0, s>>>(a, p);
             else e_interior<T, Tid, 1, true><<<n, blk, 0, s>>>(a, p);
             break;
         case kGroupDisp: e_boundary<T, Tid, kFDisp><<<n, blk, 0, s>>>(a, p); break;
@@ -710,11 +975,13 @@ void launch_h_group_impl(const StepArgs<T, Tid> &a, const int4 *items, const Wor
     const dim3 blk(kTileX, w.tile_y);
     switch (g) {
         case kGroupInterior:
-            if (w.unroll >= 2) h_interior<T, Tid, 2><<<n, blk, 0, s>>>(a, p);
+            if (w.pair_mask & (1u << kGroupInterior)) h_interior_v2<T, Tid, false><<<n, blk, 0, s>>>(a, p);
+            else if (w.unroll >= 2) h_interior<T, Tid, 2><<<n, blk, 0, s>>>(a, p);
             else h_interior<T, Tid, 1><<<n, blk, 0, s>>>(a, p);
             break;
         case kGroupPmlZ:
-            if (w.unroll >= 2) h_interior<T, Tid, 2, true><<<n, blk, 0, s>>>(a, p);
+            if (w.pair_mask & (1u << kGroupPmlZ)) h_interior_v2<T, Tid, true><<<n, blk, 0, s>>>(a, p);
+            else if (w.unroll >= 2) h_interior<T, Tid, 2, true><<<n, blk, 0, s>>>(a, p);
             else h_interior<T, Tid, 1, true><<<n, blk, 0, s>>>(a, p);
             break;
         default: h_boundary<T, Tid, kFAll><<<n, blk, 0, s>>>(a, p); break;

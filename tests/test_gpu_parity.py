@@ -15,6 +15,7 @@ import pytest
 import oracle_lib
 import scenes
 from aether_b200 import _abi as A
+from aether_b200 import configs as CF
 from aether_b200 import fdtd
 
 pytestmark = pytest.mark.gpu
@@ -178,6 +179,52 @@ def test_z_chunking_does_not_change_results(kchunk, zunroll, monkeypatch):
     monkeypatch.setenv("AEFDTD_ZUNROLL", zunroll)
     b = fdtd.run(sc)
     assert np.array_equal(a["fields"], b["fields"])
+
+
+def _wide_cell(n, precision, nsteps=120):
+    """A periodic nanodisk cell n x n (ragged against 64-column items when n
+    is not a multiple of 64) with z CPML and, by the seed, a Drude-Lorentz disk."""
+    rng = np.random.default_rng(5)
+    return CF.metasurface_cell(rng, nz_total=64, pml=8, nsteps=nsteps, nl=9, precision=precision,
+                               period_range=(n * 5e-9, n * 5e-9))
+
+
+@pytest.mark.parametrize("name,mask", [("slab_tm", "3"), ("gold_sphere", "3"), ("custom_box", "3"),
+                                       ("wide130", "3"), ("wide130", "1"), ("wide130", "2"), ("wide192", "3"),
+                                       ("wide129", "3")])
+def test_two_cells_per_thread_bit_identical(name, mask, monkeypatch):
+    """Interior and z-CPML kernels moving two x cells per thread (64-column
+    items, pair loads, lane shuffles for the x neighbour, 32-column half items
+    beside other groups) against one cell per thread: FP64 fields, plane sums
+    and flux bit-identical, including the periodic x wrap, ragged last items
+    and odd Nx (which keeps one cell per thread)."""
+    sc = _wide_cell(int(name[4:]), A.FP64) if name.startswith("wide") else getattr(scenes, name)(nsteps=120)
+    monkeypatch.setenv("AEFDTD_PAIR", "0")
+    a = fdtd.run(sc)
+    monkeypatch.setenv("AEFDTD_PAIR", mask)
+    b = fdtd.run(sc)
+    assert np.array_equal(a["fields"], b["fields"])
+    assert np.array_equal(a["plane_sums"], b["plane_sums"])
+    for fa, fb in zip(a["flux"], b["flux"]):
+        assert np.array_equal(fa, fb)
+
+
+def test_two_cells_per_thread_fp32_and_cell_cover(monkeypatch):
+    """FP32 pair kernels within 1e-6 relative of one cell per thread, and the
+    64- and 32-column items of each half-step still cover every cell once."""
+    sc = _wide_cell(130, A.FP32, nsteps=100)
+    monkeypatch.setenv("AEFDTD_PAIR", "0")
+    a = fdtd.run(sc)
+    monkeypatch.setenv("AEFDTD_PAIR", "3")
+    with fdtd.build_simulation(sc) as s:
+        s.enable_timing(True, mode=2)
+        s.step(100)
+        assert rel(s.fields(), a["fields"]) < 1e-6
+        g = s.group_timings()
+        d = s.dims()
+        for half in "EH":
+            assert sum(c for (h, _), (ms, c) in g.items() if h == half) == d.nx * d.ny * d.nz
+        assert g[("E", "interior")][1] > 0 and g[("E", "pml_z")][1] > 0
 
 
 def test_graph_replay_matches_direct_launches(monkeypatch):
