@@ -141,6 +141,14 @@ class BoxSensorDesc(C.Structure):
                 ("lambda_min", C.c_double), ("lambda_max", C.c_double)]
 
 
+MAP_PLANE, MAP_BLOCK, MAP_POINT = range(3)
+
+
+class FieldMapDesc(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("orientation", C.c_int32), ("box", C.c_int32 * 6),
+                ("cumulative", C.c_int32), ("magnetic", C.c_int32), ("lambda_", C.c_double)]
+
+
 class StructureOp(C.Structure):
     _fields_ = [("kind", C.c_int32), ("mat_index", C.c_int32), ("p", C.c_double * 8)]
 

@@ -136,6 +136,36 @@ template <typename T> struct SensorStepArgs {
     double *out;             // batch: plane-sum history [Nt][12]
 };
 
+// Single-wavelength field sensors (s_fieldmap.cpp): one launch per sensor
+// part of a step over every map of that part. Part 0 reads E (E plane maps,
+// the E half of blocks, points) beside H; part 1 reads H (H plane maps, the
+// H half of blocks) beside the next E.
+struct MapDesc {
+    int kind;                // AEFDTD_MAP_PLANE / BLOCK / POINT
+    int type;                // plane maps: 0 x-, 1 y-, 2 z-normal
+    int x1, y1, z1;          // first cell, total grid
+    int span1, span2, span3; // plane: map span1 x span2, span3 planes summed (1 unless cumulative); block: x, y, z
+    int mag;                 // plane maps: H components
+    int P;                   // threads' cells: span1*span2 (plane), span1*span2*span3 (block), 1 (point)
+    int block0, nblocks;     // blocks of the launch serving this map
+    int slot;                // this map's entry in the coefficient table rows
+    int cap, step0;          // points: history rows, and the step of row 0
+    double *acc;             // plane/block: complex [components][span3 x span2 x span1]; point: [cap][3]
+};
+
+constexpr int kMaxMaps = 8;
+enum { kMapPlane = 0, kMapBlock = 1, kMapPoint = 2 };   // AEFDTD_MAP_* of aefdtd.h
+
+template <typename T> struct MapStepArgs {
+    int Nx, Ny, Nz;
+    long long NxNy;
+    const T *Ex, *Ey, *Ez, *Hx, *Hy, *Hz;
+    const double *coef;      // this segment's phases: [step q][kMaxMaps][E re, E im, H re, H im]
+    const StepScalars *sc;   // per-step scalars (global step index)
+    int q, part, nm;
+    MapDesc m[kMaxMaps];
+};
+
 struct PhasorArgs {
     int nk, nl, Nt, Ntap;
     const int *step_ptr;     // step of buffer slot 0 = (*step_ptr if set) + step_add

@@ -34,6 +34,9 @@ int launch_sensor_step(const SensorStepArgs<double> &a, cudaStream_t s);
 int launch_sensor_step(const SensorStepArgs<float> &a, cudaStream_t s);
 void launch_plane_reduce(const double *partial, int nbp, const StepScalars *sc, double *out, int steps,
                          cudaStream_t s);
+// single-wavelength field sensors: one part (a.part) of step a.q; returns the launches issued
+int launch_fieldmap_step(const MapStepArgs<double> &a, cudaStream_t s);
+int launch_fieldmap_step(const MapStepArgs<float> &a, cudaStream_t s);
 // batch members: plane-sum partials of step q (blk: block -> (instance, block)),
 // and the reduction of `steps` steps of every instance into its history
 void launch_plane_partial_batch(const SensorStepArgs<double> *args, const int2 *blk, int nblk, int q, cudaStream_t s);

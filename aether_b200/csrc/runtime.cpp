@@ -474,6 +474,55 @@ void aefdtd_sim::fill_scalars(int t, int osc_offset, StepScalars &s) const {
     }
 }
 
+static_assert(kMapPlane == AEFDTD_MAP_PLANE && kMapBlock == AEFDTD_MAP_BLOCK && kMapPoint == AEFDTD_MAP_POINT,
+              "field-sensor kinds");
+
+// Phases of the field sensors for steps t0 .. t0+L-1, row q = step t0+q:
+// per map E then H phase as (re, im). The expressions are those of
+// FieldMap::FT_compute (s_fieldmap.cpp:356-358) and
+// FieldBlock::threaded_computation (:197-202), evaluated on the host in FP64.
+void aefdtd_sim::fill_map_phases(int t0, int L, double *rows) const {
+    const cplx Im(0, 1);
+    for (int q = 0; q < L; q++) {
+        const int step = t0 + q;
+        for (size_t m = 0; m < fmaps.size(); m++) {
+            const double w = fmaps[m]->w;
+            const cplx ce = std::exp(w * step * Dt * Im);
+            const cplx ch = std::exp(w * (step + 0.5) * Dt * Im);
+            double *r = rows + (size_t(q) * kMaxMaps + m) * 4;
+            r[0] = ce.real(); r[1] = ce.imag(); r[2] = ch.real(); r[3] = ch.imag();
+        }
+    }
+}
+
+// One part of step q's field sensors in one launch: part 0 the maps that read
+// E (E plane maps, blocks' E half, points), part 1 those that read H.
+template <typename T>
+int aefdtd_sim::launch_maps(int part, int q, const double *coef, const StepScalars *tbl, cudaStream_t st) {
+    MapStepArgs<T> a{};
+    a.Nx = Nx; a.Ny = Ny; a.Nz = Nz; a.NxNy = (long long)Nx * Ny;
+    a.Ex = F[0].as<T>(); a.Ey = F[1].as<T>(); a.Ez = F[2].as<T>();
+    a.Hx = F[3].as<T>(); a.Hy = F[4].as<T>(); a.Hz = F[5].as<T>();
+    a.coef = coef;
+    a.sc = tbl;
+    a.q = q;
+    a.part = part;
+    int blk = 0;
+    for (size_t m = 0; m < fmaps.size(); m++) {
+        const MapDesc &d = fmaps[m]->dev;
+        const bool reads_h = d.kind == kMapBlock || (d.kind == kMapPlane && d.mag);
+        const bool reads_e = d.kind != kMapPlane || !d.mag;
+        if (!(part ? reads_h : reads_e)) continue;
+        MapDesc &o = a.m[a.nm++];
+        o = d;
+        o.slot = (int)m;
+        o.block0 = blk;
+        o.nblocks = (d.P + kPlaneThreads - 1) / kPlaneThreads;
+        blk += o.nblocks;
+    }
+    return a.nm ? launch_fieldmap_step(a, st) : 0;
+}
+
 // Launches the groups of one half-step. The groups update disjoint cells and
 // read only the other field family, so the boundary groups run on side
 // streams forked from the main stream, concurrently with the interior group,
@@ -560,6 +609,15 @@ void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
     for (int g = 0; g < kGroups; g++) groups += (wsE.n[g] > 0) + (wsH.n[g] > 0);
     SensorStepArgs<T> sa;
     make_sensor_args(sa, tbl);
+    // field sensors: this segment's phase rows (same table slot as tbl)
+    bool maps_e = false, maps_h = false;
+    for (auto *m : fmaps) {
+        maps_e |= m->dev.kind != kMapPlane || !m->dev.mag;
+        maps_h |= m->dev.kind == kMapBlock || (m->dev.kind == kMapPlane && m->dev.mag);
+    }
+    const double *fm_coef =
+        fmaps.empty() ? nullptr
+                      : fm_tbl.as<double>() + size_t(tbl - tables.as<StepScalars>()) * kMaxMaps * 4;
     // Sensor work of step q runs in two parts (sensors.cuh, sensor_step): part 0
     // (plane sums, E samples) reads E only and runs beside H(q); part 1 (H
     // samples) reads H only and runs beside E(q+1). H(q+1) and any DFT flush
@@ -626,7 +684,7 @@ void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
             g.S = s.S.as<T>() + ((size_t)s.half * dft_k + s.nbuf) * 6 * s.P;
         }
         const bool cc = cc_coeff > 0;
-        const bool part0 = sa.nbp > 0 || sa.ng > 0 || cc;
+        const bool part0 = sa.nbp > 0 || sa.ng > 0 || cc || maps_e;
         sa.part = 0;
         // completion energy of this step reads E only: with part 0, beside H
         auto energy = [&](cudaStream_t st) {
@@ -635,7 +693,15 @@ void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
                                   cc_partial.as<double>() + size_t(q) * cc_nb, st);
             launches++;
         };
-        if (part0 && conc) fork(0, [&](cudaStream_t st) { launches += launch_sensor_step(sa, st); energy(st); });
+        auto maps = [&](int part, cudaStream_t st) {
+            if (part ? maps_h : maps_e) launches += launch_maps<T>(part, q, fm_coef, tbl, st);
+        };
+        if (part0 && conc)
+            fork(0, [&](cudaStream_t st) {
+                launches += launch_sensor_step(sa, st);
+                energy(st);
+                maps(0, st);
+            });
         join_h();
         if (record && timing_mode == 2) timed_groups(q, 1, wsH, [&](int g, cudaStream_t st) { launch_h_group(ha, wi, wsH, g, st); });
         else run_groups(wsH, [&](int g, cudaStream_t st) { launch_h_group(ha, wi, wsH, g, st); });
@@ -647,15 +713,20 @@ void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
             } else {
                 launches += launch_sensor_step(sa, stream);
                 energy(stream);
+                maps(0, stream);
             }
         }
-        if (sa.ng > 0) {
+        if (sa.ng > 0 || maps_h) {
             sa.part = 1;
             if (conc) {
-                fork(1, [&](cudaStream_t st) { launches += launch_sensor_step(sa, st); });
+                fork(1, [&](cudaStream_t st) {
+                    launches += launch_sensor_step(sa, st);
+                    maps(1, st);
+                });
                 h_pending = true;
             } else {
                 launches += launch_sensor_step(sa, stream);
+                maps(1, stream);
             }
         }
         for (PlaneSensor *ps : sensors) {
@@ -793,6 +864,12 @@ void aefdtd_sim::run_steps(int n) {
         }
         for (int q = 0; q < L; q++) fill_scalars(tstep + q, q, host[q]);
         AE_CUDA(cudaMemcpyAsync(tbl, host.data(), sizeof(StepScalars) * L, cudaMemcpyHostToDevice, stream));
+        if (!fmaps.empty()) {
+            map_rows.assign(size_t(L) * kMaxMaps * 4, 0.0);
+            fill_map_phases(tstep, L, map_rows.data());
+            AE_CUDA(cudaMemcpyAsync(fm_tbl.as<double>() + size_t(slot) * seg_len * kMaxMaps * 4, map_rows.data(),
+                                    map_rows.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+        }
         if (timing) {
             enqueue_segment<T, Tid>(L, tbl, true);
             accumulate_timing(L);
@@ -1078,6 +1155,11 @@ void aefdtd_sim::zero_state() {
         s->step = 0; s->nbuf = 0; s->half = 0; s->pending = false;
     }
     for (auto &o : oscs) o.step = 0;
+    for (auto *m : fmaps) {
+        if (m->acc.p) AE_CUDA(cudaMemsetAsync(m->acc.p, 0, m->acc.n, stream));
+        m->step0 = 0;
+        m->dev.step0 = 0;
+    }
     tstep = 0;
     AE_CUDA(cudaStreamSynchronize(stream));
 }
@@ -1480,6 +1562,108 @@ aefdtd_status aefdtd_get_box_flux(aefdtd_sim *s, int32_t id, double *out, int32_
         for (int l = 0; l < nl; l++) out[l] += face[l];
     }
     return AEFDTD_OK;
+}
+
+aefdtd_status aefdtd_add_fieldmap(aefdtd_sim *s, const aefdtd_fieldmap_desc *d, int32_t *id) {
+    if (!s || !d) return AEFDTD_BAD_ARG;
+    return guarded(s, [&] {
+        if (s->batch) fail(AEFDTD_NOT_READY, "batch members carry no field sensors");
+        if (d->kind < AEFDTD_MAP_PLANE || d->kind > AEFDTD_MAP_POINT) fail(AEFDTD_BAD_ARG, "bad field-sensor kind");
+        if (d->kind == AEFDTD_MAP_PLANE && (d->orientation < 0 || d->orientation > 5))
+            fail(AEFDTD_BAD_ARG, "bad orientation");
+        if (d->kind != AEFDTD_MAP_POINT && !(d->lambda > 0)) fail(AEFDTD_BAD_ARG, "lambda must be positive");
+        if (s->fmaps.size() >= (size_t)kMaxMaps) fail(AEFDTD_BAD_ARG, "at most 8 field sensors per simulation");
+        s->set_device();
+        // Sensor::link (sensors.cpp:196-230): structure cells -> total grid, clamped
+        int b[6] = {d->box[0], d->box[1], d->box[2], d->box[3], d->box[4], d->box[5]};
+        if (d->kind == AEFDTD_MAP_POINT) { b[1] = b[0] + 1; b[3] = b[2] + 1; b[5] = b[4] + 1; }   // FieldPoint ctor
+        const int x1 = std::clamp(b[0] + s->xs_s, 0, s->Nx), x2 = std::clamp(b[1] + s->xs_s, 0, s->Nx);
+        const int y1 = std::clamp(b[2] + s->ys_s, 0, s->Ny), y2 = std::clamp(b[3] + s->ys_s, 0, s->Ny);
+        const int z1 = std::clamp(b[4] + s->zs_s, 0, s->Nz), z2 = std::clamp(b[5] + s->zs_s, 0, s->Nz);
+        if (x2 <= x1 || y2 <= y1 || z2 <= z1 || x1 >= s->Nx || y1 >= s->Ny || z1 >= s->Nz)
+            fail(AEFDTD_BAD_ARG, "field-sensor box is empty or outside the grid");
+        auto *m = new FieldMapHost();
+        m->d = *d;
+        MapDesc &v = m->dev;
+        v.kind = d->kind;
+        v.x1 = x1; v.y1 = y1; v.z1 = z1;
+        size_t n = 0;
+        if (d->kind == AEFDTD_MAP_PLANE) {
+            // FieldMap::initialize (s_fieldmap.cpp:425-440): -M orientations map to the plus ones
+            v.type = d->orientation / 2;
+            v.mag = d->magnetic != 0;
+            if (v.type == 0) { v.span1 = y2 - y1; v.span2 = z2 - z1; v.span3 = x2 - x1; }
+            else if (v.type == 1) { v.span1 = x2 - x1; v.span2 = z2 - z1; v.span3 = y2 - y1; }
+            else { v.span1 = x2 - x1; v.span2 = y2 - y1; v.span3 = z2 - z1; }
+            if (!d->cumulative) v.span3 = 1;
+            v.P = v.span1 * v.span2;
+            m->ncomp = 3;
+            n = size_t(3) * v.P * 16;
+        } else if (d->kind == AEFDTD_MAP_BLOCK) {
+            // FieldBlock::initialize (s_fieldmap.cpp:177-190)
+            v.span1 = x2 - x1; v.span2 = y2 - y1; v.span3 = z2 - z1;
+            v.P = v.span1 * v.span2 * v.span3;
+            m->ncomp = 6;
+            n = size_t(6) * v.P * 16;
+        } else {
+            v.span1 = v.span2 = v.span3 = 1;
+            v.P = 1;
+            v.cap = std::max(1, s->Nt);
+            m->ncomp = 3;
+            n = size_t(v.cap) * 3 * 8;
+        }
+        if (d->kind != AEFDTD_MAP_POINT) m->w = 2.0 * Pi * c_light / d->lambda;
+        m->step0 = s->tstep;
+        v.step0 = s->tstep;
+        try {
+            m->acc.alloc(n, s->dev_bytes);
+            AE_CUDA(cudaMemsetAsync(m->acc.p, 0, m->acc.n, s->stream));
+            if (!s->fm_tbl.p) s->fm_tbl.alloc(size_t(2) * s->seg_len * kMaxMaps * 4 * sizeof(double), s->dev_bytes);
+            AE_CUDA(cudaStreamSynchronize(s->stream));
+        } catch (...) {
+            m->acc.release(s->dev_bytes);
+            delete m;
+            throw;
+        }
+        v.acc = m->acc.as<double>();
+        s->fmaps.push_back(m);
+        s->graphs_dirty = true;
+        if (id) *id = (int32_t)s->fmaps.size() - 1;
+    });
+}
+
+aefdtd_status aefdtd_get_fieldmap_shape(aefdtd_sim *s, int32_t id, int32_t shape[4]) {
+    if (!s || !shape) return AEFDTD_BAD_ARG;
+    if (id < 0 || id >= (int)s->fmaps.size()) {
+        s->last_error = "unknown field sensor";
+        return AEFDTD_BAD_ARG;
+    }
+    const FieldMapHost &m = *s->fmaps[id];
+    if (m.dev.kind == kMapPoint) {
+        shape[0] = std::clamp(s->tstep - m.step0, 0, m.dev.cap);
+        shape[1] = shape[2] = 1;
+    } else {
+        shape[0] = m.dev.span1;
+        shape[1] = m.dev.span2;
+        shape[2] = m.dev.kind == kMapBlock ? m.dev.span3 : 1;
+    }
+    shape[3] = m.ncomp;
+    return AEFDTD_OK;
+}
+
+aefdtd_status aefdtd_get_fieldmap(aefdtd_sim *s, int32_t id, double *out, size_t count) {
+    if (!s || !out) return AEFDTD_BAD_ARG;
+    return guarded(s, [&] {
+        if (id < 0 || id >= (int)s->fmaps.size()) fail(AEFDTD_BAD_ARG, "unknown field sensor");
+        const FieldMapHost &m = *s->fmaps[id];
+        size_t want;
+        if (m.dev.kind == kMapPoint) want = size_t(std::clamp(s->tstep - m.step0, 0, m.dev.cap)) * 3;
+        else want = size_t(m.ncomp) * m.dev.P * 2;
+        if (count != want) fail(AEFDTD_BAD_ARG, "count must be " + std::to_string(want));
+        s->set_device();
+        AE_CUDA(cudaStreamSynchronize(s->stream));
+        if (want) AE_CUDA(cudaMemcpy(out, m.acc.p, want * sizeof(double), cudaMemcpyDeviceToHost));
+    });
 }
 
 aefdtd_status aefdtd_get_sensor_shape(aefdtd_sim *s, int32_t id, int32_t *span1, int32_t *span2, int32_t *nl) {

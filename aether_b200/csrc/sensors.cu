@@ -17,6 +17,14 @@ template <typename T> static int step_impl(const SensorStepArgs<T> &a, cudaStrea
 }
 int launch_sensor_step(const SensorStepArgs<double> &a, cudaStream_t s) { return step_impl(a, s); }
 int launch_sensor_step(const SensorStepArgs<float> &a, cudaStream_t s) { return step_impl(a, s); }
+template <typename T> static int map_impl(const MapStepArgs<T> &a, cudaStream_t s) {
+    int nb = 0;
+    for (int m = 0; m < a.nm; ++m) nb = std::max(nb, a.m[m].block0 + a.m[m].nblocks);
+    if (nb > 0) fieldmap_step<<<nb, kPlaneThreads, 0, s>>>(a);
+    return nb > 0;
+}
+int launch_fieldmap_step(const MapStepArgs<double> &a, cudaStream_t s) { return map_impl(a, s); }
+int launch_fieldmap_step(const MapStepArgs<float> &a, cudaStream_t s) { return map_impl(a, s); }
 void launch_plane_reduce(const double *partial, int nbp, const StepScalars *sc, double *out, int steps,
                          cudaStream_t s) {
     if (steps > 0) plane_sums_reduce<<<steps, 32, 0, s>>>(partial, nbp, sc, out);

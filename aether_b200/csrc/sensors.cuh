@@ -105,6 +105,30 @@ __device__ __forceinline__ void plane_partial(const SensorStepArgs<T> &a, int b,
     if (threadIdx.x < 12) part[b * 12 + threadIdx.x] = red[threadIdx.x][0];
 }
 
+// Fields interpolated to the node of cell (i, j, k): FDTD::local_E*/local_H*
+// (fdtd_utils.cpp:457-507), periodic wrap at the upper faces. A: any argument
+// struct with the grid sizes and the six field pointers.
+template <typename T, typename A>
+__device__ __forceinline__ void local_e(const A &a, int i, int j, int k, T f[3]) {
+    const int ip = (i + 1 == a.Nx) ? 0 : i + 1;
+    const int jp = (j + 1 == a.Ny) ? 0 : j + 1;
+    const int kp = (k + 1 == a.Nz) ? 0 : k + 1;
+    auto I = [&](int x, int y, int z) { return x + (long long)y * a.Nx + (long long)z * a.NxNy; };
+    f[0] = (a.Ex[I(i, j, k)] + a.Ex[I(i, jp, k)] + a.Ex[I(i, j, kp)] + a.Ex[I(i, jp, kp)]) / T(4.0);
+    f[1] = (a.Ey[I(i, j, k)] + a.Ey[I(ip, j, k)] + a.Ey[I(i, j, kp)] + a.Ey[I(ip, j, kp)]) / T(4.0);
+    f[2] = (a.Ez[I(i, j, k)] + a.Ez[I(ip, j, k)] + a.Ez[I(i, jp, k)] + a.Ez[I(ip, jp, k)]) / T(4.0);
+}
+template <typename T, typename A>
+__device__ __forceinline__ void local_h(const A &a, int i, int j, int k, T f[3]) {
+    const int ip = (i + 1 == a.Nx) ? 0 : i + 1;
+    const int jp = (j + 1 == a.Ny) ? 0 : j + 1;
+    const int kp = (k + 1 == a.Nz) ? 0 : k + 1;
+    auto I = [&](int x, int y, int z) { return x + (long long)y * a.Nx + (long long)z * a.NxNy; };
+    f[0] = (a.Hx[I(i, j, k)] + a.Hx[I(ip, j, k)]) / T(2.0);
+    f[1] = (a.Hy[I(i, j, k)] + a.Hy[I(i, jp, k)]) / T(2.0);
+    f[2] = (a.Hz[I(i, j, k)] + a.Hz[I(i, j, kp)]) / T(2.0);
+}
+
 template <typename T>
 __device__ __forceinline__ void gather_one(const SensorStepArgs<T> &a, const GatherDesc &g, int b) {
     const int q = (b - g.block0) * blockDim.x + threadIdx.x;
@@ -114,26 +138,84 @@ __device__ __forceinline__ void gather_one(const SensorStepArgs<T> &a, const Gat
     if (g.type <= 1) { i = g.x1; j = g.y1 + u; k = g.z1 + v; }
     else if (g.type <= 3) { i = g.x1 + u; j = g.y1; k = g.z1 + v; }
     else { i = g.x1 + u; j = g.y1 + v; k = g.z1; }
-    const int ip = (i + 1 == a.Nx) ? 0 : i + 1;
-    const int jp = (j + 1 == a.Ny) ? 0 : j + 1;
-    const int kp = (k + 1 == a.Nz) ? 0 : k + 1;
-    auto I = [&](int x, int y, int z) { return x + (long long)y * a.Nx + (long long)z * a.NxNy; };
     T *S = static_cast<T *>(g.S);
-    if (a.part == 0) {
-        const T ex = (a.Ex[I(i, j, k)] + a.Ex[I(i, jp, k)] + a.Ex[I(i, j, kp)] + a.Ex[I(i, jp, kp)]) / T(4.0);
-        const T ey = (a.Ey[I(i, j, k)] + a.Ey[I(ip, j, k)] + a.Ey[I(i, j, kp)] + a.Ey[I(ip, j, kp)]) / T(4.0);
-        const T ez = (a.Ez[I(i, j, k)] + a.Ez[I(ip, j, k)] + a.Ez[I(i, jp, k)] + a.Ez[I(ip, jp, k)]) / T(4.0);
-        S[0 * (long long)g.P + q] = ex;
-        S[1 * (long long)g.P + q] = ey;
-        S[2 * (long long)g.P + q] = ez;
-    } else {
-        const T hx = (a.Hx[I(i, j, k)] + a.Hx[I(ip, j, k)]) / T(2.0);
-        const T hy = (a.Hy[I(i, j, k)] + a.Hy[I(i, jp, k)]) / T(2.0);
-        const T hz = (a.Hz[I(i, j, k)] + a.Hz[I(i, j, kp)]) / T(2.0);
-        S[3 * (long long)g.P + q] = hx;
-        S[4 * (long long)g.P + q] = hy;
-        S[5 * (long long)g.P + q] = hz;
+    T f[3];
+    if (a.part == 0) local_e(a, i, j, k, f);
+    else local_h(a, i, j, k, f);
+    const int c0 = a.part ? 3 : 0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) S[(c0 + c) * (long long)g.P + q] = f[c];
+}
+
+// One cell (or map point) of a single-wavelength field sensor for step q.
+// Plane maps (FieldMap::FT_compute, s_fieldmap.cpp:352-423): F at the plane,
+// or summed along the normal over span3 planes in order (cumulative), then
+// acc += e^{i w t Dt} F per component. Blocks (FieldBlock::FT_E*/FT_H*,
+// :113-173, 191-228): acc += F e^{i w t Dt} (E, part 0) or e^{i w (t+1/2) Dt}
+// (H, part 1). Points (FieldPoint::deep_feed, :711-719): E into row t - step0.
+// Products and sums in FP64 with round-to-nearest intrinsics: the reference's
+// complex x real product is two real products, the += two real sums.
+template <typename T>
+__device__ __forceinline__ void map_one(const MapStepArgs<T> &a, const MapDesc &m, int b) {
+    const int p = (b - m.block0) * blockDim.x + threadIdx.x;
+    if (p >= m.P) return;
+    const double *cf = a.coef + ((size_t)a.q * kMaxMaps + m.slot) * 4;
+    T f[3];
+    if (m.kind == kMapPoint) {
+        const int row = a.sc[a.q].step - m.step0;
+        if (row < 0 || row >= m.cap) return;
+        local_e(a, m.x1, m.y1, m.z1, f);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) m.acc[(size_t)row * 3 + c] = (double)f[c];
+        return;
     }
+    double2 *acc = reinterpret_cast<double2 *>(m.acc);
+    if (m.kind == kMapBlock) {
+        const int i = m.x1 + p % m.span1, j = m.y1 + (p / m.span1) % m.span2, k = m.z1 + p / (m.span1 * m.span2);
+        if (a.part == 0) local_e(a, i, j, k, f);
+        else local_h(a, i, j, k, f);
+        const double cr = cf[2 * a.part], ci = cf[2 * a.part + 1];
+        acc += (size_t)(3 * a.part) * m.P + p;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            double2 v = acc[(size_t)c * m.P];
+            v.x = dadd(v.x, dmul(cr, (double)f[c]));
+            v.y = dadd(v.y, dmul(ci, (double)f[c]));
+            acc[(size_t)c * m.P] = v;
+        }
+        return;
+    }
+    const int u = p % m.span1, v = p / m.span1;
+    double S[3] = {0.0, 0.0, 0.0};
+    for (int kk = 0; kk < m.span3; ++kk) {
+        int i, j, k;
+        if (m.type == 0) { i = m.x1 + kk; j = m.y1 + u; k = m.z1 + v; }
+        else if (m.type == 1) { i = m.x1 + u; j = m.y1 + kk; k = m.z1 + v; }
+        else { i = m.x1 + u; j = m.y1 + v; k = m.z1 + kk; }
+        if (m.mag) local_h(a, i, j, k, f);
+        else local_e(a, i, j, k, f);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) S[c] = dadd(S[c], (double)f[c]);
+    }
+    const double cr = cf[0], ci = cf[1];
+    acc += p;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        double2 w = acc[(size_t)c * m.P];
+        w.x = dadd(w.x, dmul(cr, S[c]));
+        w.y = dadd(w.y, dmul(ci, S[c]));
+        acc[(size_t)c * m.P] = w;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kPlaneThreads) fieldmap_step(const __grid_constant__ MapStepArgs<T> a) {
+    const int b = blockIdx.x;
+    for (int s = 0; s < a.nm; ++s)
+        if (b >= a.m[s].block0 && b < a.m[s].block0 + a.m[s].nblocks) {
+            map_one(a, a.m[s], b);
+            return;
+        }
 }
 
 // One step of the sensors, in two launches. Part 0 (blocks [0, nbp) plane-sum

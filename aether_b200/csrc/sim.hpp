@@ -135,6 +135,17 @@ struct PlaneSensor {
     int N0 = 0, N1 = 0;
 };
 
+// Single-wavelength field sensor (FieldMap, FieldBlock, FieldPoint of
+// s_fieldmap.cpp); dev.acc holds the device accumulators or point history.
+struct FieldMapHost {
+    aefdtd_fieldmap_desc d;
+    MapDesc dev{};           // block0/nblocks/slot set per launch
+    int ncomp = 3;
+    double w = 0;            // 2 pi c / lambda
+    int step0 = 0;           // tstep when added (points: step of history row 0)
+    DBuf acc;
+};
+
 static inline double s_curve(double x, double xmin, double xmax) {
     // src/common/mathUT.cpp:1186-1193
     double u = (x - xmin) / (xmax - xmin);
@@ -201,6 +212,11 @@ struct aefdtd_sim {
     std::vector<Osc> oscs;
     std::vector<PlaneSensor *> sensors;
     std::vector<std::array<int, 6>> boxes;   // box sensors: planar sensor per face (-1: disabled)
+    std::vector<FieldMapHost *> fmaps;       // single-wavelength field sensors
+    DBuf fm_tbl;                             // their phases: [slot][seg_len][kMaxMaps][4] doubles
+    std::vector<double> map_rows;            // host staging of one segment's phase rows
+    void fill_map_phases(int t0, int L, double *rows) const;
+    template <typename T> int launch_maps(int part, int q, const double *coef, const StepScalars *tbl, cudaStream_t st);
     // half-step work lists: (x0, y0, k0, k1) items of 32 x 4 columns x a
     // z-chunk, in one device array: the E groups, then the H groups
     bool work_dirty = true;
@@ -297,6 +313,8 @@ inline aefdtd_sim::~aefdtd_sim() {
     tables.release(t);
     for (auto &gx : graph_exec) if (gx.second) cudaGraphExecDestroy(gx.second);
     items.release(t);
+    fm_tbl.release(t);
+    for (auto *m : fmaps) { m->acc.release(t); delete m; }
     for (auto *s : sensors) {
         s->S.release(t); s->acc.release(t); s->wdev.release(t); s->WE.release(t); s->WH.release(t); s->flux.release(t);
         s->Btc.release(t);

@@ -106,6 +106,38 @@ class Simulation:
         self._c(self._lib.aefdtd_get_box_flux(self._h, int(bid), out.ctypes.data_as(C.POINTER(C.c_double)), nl))
         return out
 
+    def add_fieldmap(self, kind, box, lambda_=0.0, orientation=A.NORMAL_Z, cumulative=False,
+                     magnetic=False) -> int:
+        """Single-wavelength field sensor (include/aefdtd.h, aefdtd_add_fieldmap):
+        kind MAP_PLANE (FieldMap), MAP_BLOCK (FieldBlock) or MAP_POINT
+        (FieldPoint); box in structure cells; returns the map id."""
+        d = A.FieldMapDesc()
+        d.kind, d.orientation = int(kind), int(orientation)
+        for k in range(6):
+            d.box[k] = int(box[k])
+        d.cumulative, d.magnetic, d.lambda_ = int(bool(cumulative)), int(bool(magnetic)), float(lambda_)
+        mid = C.c_int32(-1)
+        self._c(self._lib.aefdtd_add_fieldmap(self._h, C.byref(d), C.byref(mid)))
+        self._map_kinds = getattr(self, "_map_kinds", {})
+        self._map_kinds[mid.value] = int(kind)
+        return mid.value
+
+    def fieldmap(self, mid: int) -> np.ndarray:
+        """Plane maps: complex (3, span2, span1); blocks: complex (6, span3,
+        span2, span1); points: (steps, 3) real E."""
+        sh = (C.c_int32 * 4)()
+        self._c(self._lib.aefdtd_get_fieldmap_shape(self._h, int(mid), sh))
+        s1, s2, s3, nc = sh[0], sh[1], sh[2], sh[3]
+        kind = getattr(self, "_map_kinds", {}).get(int(mid), A.MAP_PLANE)
+        shape = (s1, 3) if kind == A.MAP_POINT else (nc, s3, s2, s1, 2)
+        out = np.empty(shape)
+        self._c(self._lib.aefdtd_get_fieldmap(self._h, int(mid), out.ctypes.data_as(C.POINTER(C.c_double)),
+                                              out.size))
+        if kind == A.MAP_POINT:
+            return out
+        z = out[..., 0] + 1j * out[..., 1]
+        return z[:, 0] if kind == A.MAP_PLANE else z
+
     def set_completion(self, coeff=1e-3, check_every=500):
         """Energy-mode completion sensor (coeff <= 0: off)."""
         self._c(self._lib.aefdtd_set_completion(self._h, float(coeff), int(check_every)))

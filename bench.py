@@ -485,7 +485,7 @@ def main():
     ei_ms, ei_cells = r32["groups"][("E", "interior")]
     ei_bytes = ei_cells * (9 * 4 + r32["bytes"]["detail"]["id_bytes"])
     achieved = ei_bytes / (ei_ms * 1e-3) / 1e9
-    traffic = profiled_traffic("e_interior", "fp32")
+    traffic = profiled_traffic("e_interior_v2", "fp32")
     step_achieved = r32["step_bytes"] / (r32["ms_per_step"] * 1e-3 / STEPS_PER_BENCH_STEP) / 1e9
     line = {
         "metric": METRIC, "value": r32["gcells"], "unit": METRIC, "n_gpus": ws, "steps": args.steps,
@@ -503,7 +503,7 @@ def main():
                  / (r64["groups"][("E", "interior")][0] * 1e-3) / 1e9 / peak,
                  "step_frac": r64["step_bytes"] / (r64["ms_per_step"] * 1e-3 / STEPS_PER_BENCH_STEP) / 1e9 / peak},
         "fp32_over_fp64": r32["gcells"] / r64["gcells"],
-        "roofline": {"bound": "hbm", "kernel": "e_interior<float, uint8, 2>", "achieved": achieved, "peak": peak,
+        "roofline": {"bound": "hbm", "kernel": "e_interior_v2<float, uint8, false>", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": traffic, "algorithmic_bytes_per_launch": ei_bytes, "launch_us": ei_ms * 1e3,
                      "cells_per_launch": ei_cells,

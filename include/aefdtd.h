@@ -264,6 +264,46 @@ typedef struct aefdtd_box_sensor_desc {
 aefdtd_status aefdtd_add_box_sensor(aefdtd_sim *sim, const aefdtd_box_sensor_desc *desc, int32_t *box_id);
 aefdtd_status aefdtd_get_box_flux(aefdtd_sim *sim, int32_t box_id, double *out, int32_t nl);
 
+/* Single-wavelength field sensors (s_fieldmap.cpp), fed after every step
+ * like the planar sensors, with the step index t of the simulation:
+ *   AEFDTD_MAP_PLANE (FieldMap, :289-461): a plane normal to X, Y or Z
+ *     (the -M orientations give the same map) at the box's first index along
+ *     the normal; acc(i,j) += e^{i w t Dt} F(i,j) for the three E components,
+ *     or the H components when magnetic is set (FieldMap::set_mag_map; the H
+ *     phase is also e^{i w t Dt}); with cumulative set
+ *     (FieldMap::set_cumulative) F is first summed along the normal over the
+ *     box. Output 3 x span2 x span1 complex.
+ *   AEFDTD_MAP_BLOCK (FieldBlock, :28-228): every cell of the box,
+ *     E with e^{i w t Dt}, H with e^{i w (t + 1/2) Dt}. Output 6 x span3 x
+ *     span2 x span1 complex.
+ *   AEFDTD_MAP_POINT (FieldPoint, :702-732): E at one cell (the box's first
+ *     corner) after each step, as a time series: steps x 3 doubles (Ex, Ey,
+ *     Ez) for the steps fed, at most the grid's nt.
+ * F is the field interpolated to the cell node as for the planar sensors
+ * (FDTD::local_E*, local_H*, fdtd_utils.cpp:457-507); w = 2 pi c / lambda.
+ * The box is in structure cells and clamped to the grid as by Sensor::link
+ * (sensors.cpp:196-230). Accumulation is FP64 in both precisions. At most 8
+ * field sensors per simulation; not for batch members. */
+enum {
+    AEFDTD_MAP_PLANE = 0, AEFDTD_MAP_BLOCK = 1, AEFDTD_MAP_POINT = 2
+};
+typedef struct aefdtd_fieldmap_desc {
+    int32_t kind;          /* AEFDTD_MAP_* */
+    int32_t orientation;   /* AEFDTD_MAP_PLANE: AEFDTD_NORMAL_* */
+    int32_t box[6];        /* x1, x2, y1, y2, z1, z2, structure cells */
+    int32_t cumulative;    /* AEFDTD_MAP_PLANE: sum along the normal first */
+    int32_t magnetic;      /* AEFDTD_MAP_PLANE: H instead of E */
+    double lambda;         /* analysis wavelength (m); unused by AEFDTD_MAP_POINT */
+} aefdtd_fieldmap_desc;
+aefdtd_status aefdtd_add_fieldmap(aefdtd_sim *sim, const aefdtd_fieldmap_desc *desc, int32_t *map_id);
+/* shape[4]: span1, span2, span3 (1 for plane maps and points), components
+ * (3 or 6; for points 3 and span1 = the number of steps recorded so far). */
+aefdtd_status aefdtd_get_fieldmap_shape(aefdtd_sim *sim, int32_t map_id, int32_t shape[4]);
+/* Plane maps and blocks: components x span3 x span2 x span1 complex values
+ * as interleaved double (re, im), i fastest; count = 2 x that product.
+ * Points: steps x 3 doubles; count = 3 x steps. */
+aefdtd_status aefdtd_get_fieldmap(aefdtd_sim *sim, int32_t map_id, double *out, size_t count);
+
 /* Completion sensor in energy mode (CompletionSensor(coeff),
  * s_completion.cpp:20-24, 39-43, 121-130, 177-190; checked by the drivers at
  * normal_incidence.cpp:417-427 and default_fdtd.cpp:193-203). After every

@@ -51,6 +51,13 @@ int g_box_nl = 0, g_box_mask = 0;
 double g_box_lmin = 0, g_box_lmax = 0;
 std::vector<double> g_box_result;
 
+// Single-wavelength field sensors (FieldMap, FieldBlock, FieldPoint of
+// s_fieldmap.cpp), set by aeref_set_fieldmaps: fed after the planar sensors;
+// their accumulators (or, for points, FDTD::local_E* at the linked point
+// after each feed) are kept for aeref_fieldmap_result.
+std::vector<aefdtd_fieldmap_desc> g_maps;
+std::vector<std::vector<double>> g_map_results;
+
 int ref_orientation(int o) {
     static const int tbl[6] = {NORMAL_X, NORMAL_XM, NORMAL_Y, NORMAL_YM, NORMAL_Z, NORMAL_ZM};
     return (o >= 0 && o < 6) ? tbl[o] : NORMAL_UNDEF;
@@ -182,6 +189,41 @@ int aeref_run(const aefdtd_grid_desc *g, const uint32_t *map,
         bx->set_silent(true);
         bx->link(fdtd, std::filesystem::path("."));
     }
+    std::vector<Sensor *> maps;
+    g_map_results.assign(g_maps.size(), {});
+    for (const aefdtd_fieldmap_desc &d : g_maps) {
+        Sensor *m = nullptr;
+        if (d.kind == AEFDTD_MAP_PLANE) {
+            FieldMap *fm = new FieldMap(ref_orientation(d.orientation), d.box[0], d.box[1], d.box[2], d.box[3],
+                                        d.box[4], d.box[5]);
+            fm->set_cumulative(d.cumulative != 0);
+            fm->set_mag_map(d.magnetic != 0);
+            fm->set_spectrum(d.lambda);
+            m = fm;
+        } else if (d.kind == AEFDTD_MAP_BLOCK) {
+            m = new FieldBlock(d.box[0], d.box[1], d.box[2], d.box[3], d.box[4], d.box[5]);
+            m->set_spectrum(d.lambda);
+        } else {
+            m = new FieldPoint(d.box[0], d.box[2], d.box[4]);
+            m->set_spectrum(d.lambda > 0 ? d.lambda : 500e-9);
+        }
+        m->name = "aeref_map";
+        m->set_silent(true);
+        // FieldPoint::initialize opens its text output under the working directory
+        m->link(fdtd, std::filesystem::temp_directory_path());
+        maps.push_back(m);
+    }
+    auto feed_maps = [&] {
+        for (size_t i = 0; i < maps.size(); i++) {
+            maps[i]->feed(fdtd);
+            if (g_maps[i].kind == AEFDTD_MAP_POINT) {
+                const Sensor &p = *maps[i];
+                g_map_results[i].push_back(fdtd.local_Ex(p.x1, p.y1, p.z1));
+                g_map_results[i].push_back(fdtd.local_Ey(p.x1, p.y1, p.z1));
+                g_map_results[i].push_back(fdtd.local_Ez(p.x1, p.y1, p.z1));
+            }
+        }
+    };
     std::vector<Source *> sources;
     if (g->mode == AEFDTD_MODE_CUSTOM) {
         for (int s = 0; s < nsrc; s++) {
@@ -243,6 +285,7 @@ int aeref_run(const aefdtd_grid_desc *g, const uint32_t *map,
                 }
             for (auto *s : sensors) s->feed(fdtd);
             if (bx) bx->feed(fdtd);
+            feed_maps();
             if (cpl) cpl->feed(fdtd);   // fed with the sensors, after the planar ones
 
             tb = (t + 0.5) * Dt;
@@ -335,6 +378,7 @@ int aeref_run(const aefdtd_grid_desc *g, const uint32_t *map,
             fdtd.update_H();
             for (auto *s : sensors) s->feed(fdtd);
             if (bx) bx->feed(fdtd);
+            feed_maps();
             for (auto *s : sources) s->inject_H(fdtd);
         }
         if (loop_seconds) loop_seconds[0] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -353,6 +397,30 @@ int aeref_run(const aefdtd_grid_desc *g, const uint32_t *map,
         g_box_result.assign(bx->Nl, 0.0);
         for (int l = 0; l < bx->Nl; l++) g_box_result[l] = bx->rsp_result[l];
         delete bx;
+    }
+    for (size_t i = 0; i < maps.size(); i++) {
+        std::vector<double> &o = g_map_results[i];
+        if (g_maps[i].kind == AEFDTD_MAP_PLANE) {
+            FieldMap &fm = *static_cast<FieldMap *>(maps[i]);
+            Grid2<Imdouble> *acc[3] = {&fm.acc_Ex, &fm.acc_Ey, &fm.acc_Ez};
+            for (int c = 0; c < 3; c++)
+                for (int j = 0; j < fm.span2; j++)
+                    for (int i = 0; i < fm.span1; i++) {
+                        o.push_back((*acc[c])(i, j).real());
+                        o.push_back((*acc[c])(i, j).imag());
+                    }
+        } else if (g_maps[i].kind == AEFDTD_MAP_BLOCK) {
+            FieldBlock &fb = *static_cast<FieldBlock *>(maps[i]);
+            Grid3<Imdouble> *acc[6] = {&fb.Ex, &fb.Ey, &fb.Ez, &fb.Hx, &fb.Hy, &fb.Hz};
+            for (int c = 0; c < 6; c++)
+                for (int k = 0; k < fb.span3; k++)
+                    for (int j = 0; j < fb.span2; j++)
+                        for (int i = 0; i < fb.span1; i++) {
+                            o.push_back((*acc[c])(i, j, k).real());
+                            o.push_back((*acc[c])(i, j, k).imag());
+                        }
+        }
+        delete maps[i];
     }
     for (auto *s : sensors) delete s;
     for (auto *s : sources) delete s;
@@ -374,6 +442,21 @@ void aeref_set_box(const int32_t box[6], int32_t nl, double lmin, double lmax, i
     g_box_lmin = lmin;
     g_box_lmax = lmax;
     g_box_mask = disabled_mask;
+}
+
+/* Field sensors for the following aeref_run calls (n = 0: none). */
+void aeref_set_fieldmaps(const aefdtd_fieldmap_desc *d, int32_t n) {
+    g_maps.assign(d, d + (n > 0 ? n : 0));
+}
+
+/* Results of field sensor idx after the last aeref_run: plane maps 3 x span2
+ * x span1 and blocks 6 x span3 x span2 x span1 complex as (re, im), i fastest;
+ * points steps x 3. Returns the number of doubles, copying at most count. */
+int64_t aeref_fieldmap_result(int32_t idx, double *out, int64_t count) {
+    if (idx < 0 || idx >= (int)g_map_results.size()) return -1;
+    const std::vector<double> &v = g_map_results[idx];
+    for (int64_t i = 0; i < count && i < (int64_t)v.size(); i++) out[i] = v[i];
+    return (int64_t)v.size();
 }
 
 /* rsp_result of the box after the last aeref_run (nl values). */

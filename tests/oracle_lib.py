@@ -126,3 +126,34 @@ def run_ref_box(scene, box, nl, lambda_min, lambda_max, disabled=0, nsteps=None)
         lib.aeref_set_box(None, 0, 0.0, 0.0, 0)
     out["box_flux"] = res
     return out
+
+
+def run_ref_fieldmaps(scene, maps, nsteps=None):
+    """The reference core with FieldMap / FieldBlock / FieldPoint sensors
+    (maps: list of aefdtd FieldMapDesc): the run dict of `run` plus 'maps',
+    one flat float64 array per sensor in the aefdtd_get_fieldmap layout."""
+    lib = C.CDLL(REF_PATH)
+    lib.aeref_set_fieldmaps.argtypes = [_P(A.FieldMapDesc), C.c_int32]
+    lib.aeref_fieldmap_result.argtypes = [C.c_int32, _P(C.c_double), C.c_int64]
+    lib.aeref_fieldmap_result.restype = C.c_int64
+    arr = (A.FieldMapDesc * max(1, len(maps)))(*maps)
+    lib.aeref_set_fieldmaps(arr, len(maps))
+    try:
+        out = run(scene, "ref", nsteps=nsteps, want_fields=False)
+        res = []
+        for i in range(len(maps)):
+            n = lib.aeref_fieldmap_result(i, None, 0)
+            v = np.zeros(max(n, 0))
+            lib.aeref_fieldmap_result(i, v.ctypes.data_as(_P(C.c_double)), n)
+            res.append(v)
+    finally:
+        lib.aeref_set_fieldmaps(arr, 0)
+    out["maps"] = res
+    return out
+
+
+def ref_threads():
+    """Worker threads per sensor and FDTD object in the reference core."""
+    lib = C.CDLL(REF_PATH)
+    lib.aeref_threads.restype = C.c_int
+    return int(lib.aeref_threads())

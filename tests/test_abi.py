@@ -175,6 +175,8 @@ int main(void) {
   printf("%zu %zu %zu %zu\\n", offsetof(aefdtd_batch_info, class_kchunk), offsetof(aefdtd_server_opts, batch),
          offsetof(aefdtd_job_desc, steps), offsetof(aefdtd_server_stats, gcells_per_s));
   printf("%zu %zu\\n", sizeof(aefdtd_box_sensor_desc), offsetof(aefdtd_box_sensor_desc, lambda_min));
+  printf("%zu %zu %zu\\n", sizeof(aefdtd_fieldmap_desc), offsetof(aefdtd_fieldmap_desc, magnetic),
+         offsetof(aefdtd_fieldmap_desc, lambda));
   return 0;
 }
 """
@@ -191,3 +193,5 @@ int main(void) {
     assert offs == [A.BatchInfo.class_kchunk.offset, A.ServerOpts.batch.offset, A.JobDesc.steps.offset,
                     A.ServerStats.gcells_per_s.offset]
     assert [int(x) for x in lines[2].split()] == [C.sizeof(A.BoxSensorDesc), A.BoxSensorDesc.lambda_min.offset]
+    assert [int(x) for x in lines[3].split()] == [C.sizeof(A.FieldMapDesc), A.FieldMapDesc.magnetic.offset,
+                                                  A.FieldMapDesc.lambda_.offset]
