@@ -7,7 +7,7 @@ import ctypes as C
 ABI_VERSION = 1
 MAX_TERMS = 4
 
-MODE_NORMAL, MODE_CUSTOM = 0, 1
+MODE_NORMAL, MODE_CUSTOM, MODE_OBLIQUE = 0, 1, 2
 FP64, FP32 = 0, 1
 EX, EY, EZ, HX, HY, HZ = range(6)
 NORMAL_X, NORMAL_XM, NORMAL_Y, NORMAL_YM, NORMAL_Z, NORMAL_ZM = range(6)
@@ -139,6 +139,11 @@ class ServerStats(C.Structure):
 class BoxSensorDesc(C.Structure):
     _fields_ = [("box", C.c_int32 * 6), ("nl", C.c_int32), ("disabled", C.c_int32),
                 ("lambda_min", C.c_double), ("lambda_max", C.c_double)]
+
+
+class ObliqueDesc(C.Structure):
+    _fields_ = [("polarization", C.c_int32), ("nl", C.c_int32), ("lambda_min", C.c_double),
+                ("lambda_max", C.c_double), ("kx_in", C.c_double), ("ky_in", C.c_double)]
 
 
 MAP_PLANE, MAP_BLOCK, MAP_POINT = range(3)

@@ -34,7 +34,9 @@ UNITS = [
     ("dft_tc.cu", []),
     ("voxel.cu", ["--fmad=false"]),
     ("plane_static.cu", []),
+    ("oblique.cu", ["--fmad=false"]),
     ("runtime.cpp", None),
+    ("oblique_driver.cpp", None),
     ("batch.cpp", None),
     ("server.cpp", None),
 ]

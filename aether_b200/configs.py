@@ -67,6 +67,32 @@ def slab_scene(nx=64, ny=64, nz_total=128, dx=5 * NM, pml=16, slab=20, n_slab=1.
                  normal=A.NormalDesc(polarization, nl, lmin, lmax), sensors=sens, name="slab")
 
 
+def oblique_scene(nx=24, ny=20, nz_total=96, dx=5 * NM, pml=12, kx_in=0.4, ky_in=0.0, slab=10, disk=True,
+                  nsteps=600, nl=31, lmin=400 * NM, lmax=1000 * NM, polarization=0, precision=A.FP64):
+    """Oblique incidence ("fdtd_oblique_ARS", one in-plane wavevector): a
+    periodic cell with a dielectric slab on an n=1.45 substrate, optionally a
+    gold-like disk (Drude + critical points) on the slab, CPML on +/-z. kx_in,
+    ky_in are fractions of 2 pi / lmax (the driver's k_in, rad/m in vacuum)."""
+    nz_s = nz_total - 2 * pml - 10
+    m = np.zeros((nz_s, ny, nx), np.uint32)
+    sub_top = nz_s // 3
+    m[:sub_top] = 2
+    m[sub_top:sub_top + slab] = 3
+    if disk:
+        x = (np.arange(nx) - nx / 2 + 0.5) * dx
+        y = (np.arange(ny) - ny / 2 + 0.5) * dx
+        r = 0.3 * min(nx, ny) * dx
+        inside = (x[None, :] ** 2 + y[:, None] ** 2) <= r * r
+        m[sub_top + slab:sub_top + slab + 4][:, inside] = 1
+    g = A.grid_desc(nx, ny, nz_s, dx, mode=A.MODE_OBLIQUE, precision=precision, nt=nsteps,
+                    time_mod=0.5 / 0.99, pml=(0, 0, 0, 0, pml, pml), pad=(0, 0, 0, 0, 5, 5),
+                    kappa=(1.0,) * 6, sigma=(1.0,) * 6, alpha=(0.05,) * 6)
+    k0 = 2 * math.pi / lmax
+    od = A.ObliqueDesc(polarization, nl, lmin, lmax, kx_in * k0, ky_in * k0)
+    return Scene(g, m, [const_n(1.0), gold_cp_model(), const_n(1.45), const_n(1.9)], nsteps, oblique=od,
+                 name="oblique")
+
+
 def sphere_scene(nx=128, ny=128, nz_total=256, dx=2.5 * NM, pml=24, radius=40 * NM, n_sub=1.45,
                  nsteps=20000, nl=201, lmin=400 * NM, lmax=1000 * NM, polarization=1,
                  precision=A.FP64, material=None, sensor_gap=12):

@@ -86,6 +86,15 @@ template <typename T, typename Tid> struct StepArgs {
     int kchunk;                     // z planes per thread
     int prefetch;                   // interior kernels: prefetch the item's planes into L2 at start
     int *err;                       // device error flag (bounded waits)
+    // oblique driver: two grids hold the real and imaginary parts of a
+    // Bloch-periodic field; their wrap cells run in the general kernels
+    int bloch;                      // 0: periodic wraps; 1: this is the real grid; 2: the imaginary grid
+    const T *oEx, *oEy, *oEz, *oHx, *oHy, *oHz;   // the other grid's fields
+    double bxr, bxi, byr, byi;      // Bloch phase of the x and y wraps (E side e^{-ikL}, H side e^{+ikL})
+    int kobl;                       // Bloch_Wideband injection plane (-1: none)
+    double obl_coef;                // E side: C2z of the injection plane's material; H side: dtdmz
+    const double2 *obl_px, *obl_py; // per-column phases at the x- and y-staggered points
+    const double *obl_inc;          // per-step incident sums [step][14] (E side 0..3, H side 4..7)
 };
 
 // Item groups of one half-step: a device array of int4 items (x0, y0, k0,
@@ -164,6 +173,37 @@ template <typename T> struct MapStepArgs {
     const StepScalars *sc;   // per-step scalars (global step index)
     int q, part, nm;
     MapDesc m[kMaxMaps];
+};
+
+// R/T sums of the oblique driver (oblique_biphase.cpp:300-327): per step, the
+// complex sums over the plane of incident (BR), reflected-plane (R, z =
+// zs_e+2) and transmitted-plane (T, z = zs_s) E times e^{-i k.r}.
+template <typename T> struct OblSumArgs {
+    int Nx, Ny;
+    long long NxNy;
+    const T *Ex, *Ey, *Ez;          // the real grid
+    int kr, kt;                     // zs_e + 2, zs_s
+    const double2 *mk;              // [3][Nx*Ny] mk_x, mk_y, mk_z
+    const double2 *ph;              // [3][Nx*Ny] phases of the incident field at the Ex, Ey, Ez points
+    const double *inc;              // per-step incident sums [step][14] (8..13: E at zs_s)
+    const StepScalars *sc;
+    int q;
+    double *partial;                // [blocks][18] of this step
+};
+
+// Per-step sums of the wideband Bloch source (Bloch_Wideband::inject_E,
+// inject_H and get_E, sc_bloch.cpp:43-83, 216-285) for steps t0 .. t0+n-1:
+// out[t][0..3] H_x, H_y at (z2 - 1/2, t - 1/2), [4..7] E_x, E_y at (z2, t),
+// [8..13] E_x, E_y, E_z at zs_s, time (t + 1/2) Dt, as complex (re, im).
+struct OblIncArgs {
+    int nl;                  // spectral lines
+    const double *w, *kz;    // [nl]
+    const double *eb;        // [nl][3] E_base
+    const double *hb;        // [nl][2] H_base x, y
+    double Dt, Dz;
+    int z2, zs_s, t_offset;
+    int t0, n;
+    double *out;             // [t0 + n][14]
 };
 
 struct PhasorArgs {

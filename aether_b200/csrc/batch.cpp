@@ -618,6 +618,7 @@ aefdtd_status aefdtd_batch_add(aefdtd_batch *b, aefdtd_sim *s, int32_t steps) {
         if (!s->sensors.empty()) fail(AEFDTD_BAD_ARG, "batch members carry no planar DFT sensors (normal-mode plane sums only)");
         if (s->cc_coeff > 0) fail(AEFDTD_BAD_ARG, "batch members run without a completion sensor (fixed step budgets)");
         if (!s->fmaps.empty()) fail(AEFDTD_BAD_ARG, "batch members carry no field sensors");
+        if (s->g.mode == AEFDTD_MODE_OBLIQUE) fail(AEFDTD_BAD_ARG, "batch members run normal or custom mode only");
         if (s->Nz >= 32768) fail(AEFDTD_BAD_ARG, "batch members need Nz < 32768 (k1 << 16 in an int32 item)");
         s->set_device();
         s->finalize_tables();

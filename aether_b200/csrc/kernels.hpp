@@ -55,6 +55,14 @@ void launch_accumulate(const AccumArgs<double> &a, cudaStream_t s);
 void launch_accumulate(const AccumArgs<float> &a, cudaStream_t s);
 void launch_flux(const FluxArgs &a, cudaStream_t s);
 
+// oblique.cu (compiled with --fmad=false): the oblique driver's incident sums
+// and its per-step R/T sums (block partials of step a.q, then the reduction
+// of `steps` steps into hist[sc[0].step + q][18]); the sums return launches issued
+void launch_obl_incident(const OblIncArgs &a, cudaStream_t s);
+int launch_obl_sums(const OblSumArgs<double> &a, int nb, cudaStream_t s);
+int launch_obl_sums(const OblSumArgs<float> &a, int nb, cudaStream_t s);
+void launch_obl_reduce(const double *partial, int nb, const StepScalars *sc, double *hist, int steps, cudaStream_t s);
+
 // dft_tc.cu: FP32 DFT blocks on the tensor cores (tcgen05, 3xTF32)
 void launch_phasors_tc(const DftTcPhasorArgs &a, cudaStream_t s);
 void launch_accumulate_tc(const DftTcArgs &a, cudaStream_t s);

@@ -12,7 +12,8 @@
 void aefdtd_sim::construct(const aefdtd_grid_desc *d) {
     g = *d;
     if (g.abi_version != AEFDTD_ABI_VERSION) fail(AEFDTD_BAD_ARG, "abi_version mismatch");
-    if (g.mode != AEFDTD_MODE_NORMAL && g.mode != AEFDTD_MODE_CUSTOM) fail(AEFDTD_BAD_ARG, "unknown mode");
+    if (g.mode != AEFDTD_MODE_NORMAL && g.mode != AEFDTD_MODE_CUSTOM && g.mode != AEFDTD_MODE_OBLIQUE)
+        fail(AEFDTD_BAD_ARG, "unknown mode");
     if (g.precision != AEFDTD_FP64 && g.precision != AEFDTD_FP32) fail(AEFDTD_BAD_ARG, "unknown precision");
     if (g.nx < 1 || g.ny < 1 || g.nz < 1) fail(AEFDTD_BAD_ARG, "grid sizes must be positive");
     if (!(g.dx > 0 && g.dy > 0 && g.dz > 0)) fail(AEFDTD_BAD_ARG, "cell sizes must be positive");
@@ -46,7 +47,8 @@ void aefdtd_sim::construct(const aefdtd_grid_desc *d) {
     if (g.pml_ma > 0) pml_ma = g.pml_ma;
     for (int f = 0; f < 6; f++) { pml[f] = g.pml[f]; pad[f] = g.pad[f]; }
     for (int f = 0; f < 6; f++) if (pml[f] < 0 || pad[f] < 0) fail(AEFDTD_BAD_ARG, "negative PML or pad");
-    if (g.mode == AEFDTD_MODE_NORMAL) {
+    if (g.mode == AEFDTD_MODE_NORMAL || g.mode == AEFDTD_MODE_OBLIQUE) {
+        // normal_incidence.cpp:195-200 (FDTD ctor pad rule) and oblique_biphase.cpp:55-60
         for (int f = 0; f < 4; f++) { pml[f] = 0; pad[f] = 0; }
         pad[4] = std::max(5, pad[4]);
         pad[5] = std::max(5, pad[5]);
@@ -363,17 +365,22 @@ void aefdtd_sim::finalize_tables() {
         psi.alloc(size_t(off) * es, dev_bytes);
         if (psi.p) AE_CUDA(cudaMemsetAsync(psi.p, 0, psi.n, stream));
     }
+    if (obl && obl->psi_i.n != psi.n) {
+        obl->psi_i.alloc(psi.n, dev_bytes);
+        if (obl->psi_i.p) AE_CUDA(cudaMemsetAsync(obl->psi_i.p, 0, obl->psi_i.n, stream));
+    }
     AE_CUDA(cudaStreamSynchronize(stream));
     tables_dirty = false;
 }
 
 template <typename T, typename Tid>
-void aefdtd_sim::fill_args(StepArgs<T, Tid> &a, bool e_side) {
+void aefdtd_sim::fill_args(StepArgs<T, Tid> &a, bool e_side, int grid) {
     std::memset(&a, 0, sizeof(a));
     a.Nx = Nx; a.Ny = Ny; a.Nz = Nz;
     a.NxNy = (long long)Nx * Ny;
-    a.Ex = F[0].as<T>(); a.Ey = F[1].as<T>(); a.Ez = F[2].as<T>();
-    a.Hx = F[3].as<T>(); a.Hy = F[4].as<T>(); a.Hz = F[5].as<T>();
+    DBuf *G = grid_fields(grid);
+    a.Ex = G[0].as<T>(); a.Ey = G[1].as<T>(); a.Ez = G[2].as<T>();
+    a.Hx = G[3].as<T>(); a.Hy = G[4].as<T>(); a.Hz = G[5].as<T>();
     a.mat = mat.as<Tid>();
     a.mpitch = mpitch;
     a.coef = coef.as<MatCoef<T>>();
@@ -381,12 +388,13 @@ void aefdtd_sim::fill_args(StepArgs<T, Tid> &a, bool e_side) {
     a.disp = any_disp ? disp.as<DispInfo>() : nullptr;
     a.crec = crec.as<Cplx<T>>();
     a.dchi = dchi.as<Cplx<T>>();
-    a.psi = psi.as<Cplx<T>>();
+    a.psi = (grid && obl ? obl->psi_i : psi).as<Cplx<T>>();
     a.pml_xm = pml[0]; a.pml_xp = pml[1]; a.pml_ym = pml[2]; a.pml_yp = pml[3]; a.pml_zm = pml[4]; a.pml_zp = pml[5];
     a.px = pml[0] || pml[1]; a.py = pml[2] || pml[3]; a.pz = pml[4] || pml[5];
     int o = e_side ? 0 : 3;
     a.ikx = ik[o + 0].as<T>(); a.iky = ik[o + 1].as<T>(); a.ikz = ik[o + 2].as<T>();
     DBuf *B = e_side ? bE : bH, *Cc = e_side ? cE : cH, *P = e_side ? psiE : psiH;
+    if (grid && obl) P = e_side ? obl->psiEi : obl->psiHi;
     a.bx = B[0].as<T>(); a.by = B[1].as<T>(); a.bz = B[2].as<T>();
     a.cx = Cc[0].as<T>(); a.cy = Cc[1].as<T>(); a.cz = Cc[2].as<T>();
     a.psi_x0 = P[0].as<T>(); a.psi_x1 = P[1].as<T>();
@@ -394,7 +402,22 @@ void aefdtd_sim::fill_args(StepArgs<T, Tid> &a, bool e_side) {
     a.psi_z0 = P[4].as<T>(); a.psi_z1 = P[5].as<T>();
     a.dtdmx = (T)dtdmx; a.dtdmy = (T)dtdmy; a.dtdmz = (T)dtdmz; a.dtm = (T)dtm;
     a.kinj = -1;
+    a.kobl = -1;
     a.err = err.as<int>();
+    if (obl) {
+        // the other grid's fields and the Bloch phases of this half-step's wraps
+        DBuf *O = grid_fields(grid ^ 1);
+        a.oEx = O[0].as<T>(); a.oEy = O[1].as<T>(); a.oEz = O[2].as<T>();
+        a.oHx = O[3].as<T>(); a.oHy = O[4].as<T>(); a.oHz = O[5].as<T>();
+        a.bloch = grid + 1;
+        const cplx bx = e_side ? obl->dH_x : obl->dE_x, by = e_side ? obl->dH_y : obl->dE_y;
+        a.bxr = bx.real(); a.bxi = bx.imag(); a.byr = by.real(); a.byi = by.imag();
+        a.kobl = e_side ? obl->z2 : obl->z2 - 1;
+        a.obl_coef = e_side ? obl->c2z : dtdmz;
+        a.obl_px = obl->ph.as<double2>();
+        a.obl_py = obl->ph.as<double2>() + size_t(Nx) * Ny;
+        a.obl_inc = obl->inc.as<double>();
+    }
 }
 
 // Accumulates one DFT block of a sensor: n buffered steps in sample-buffer
@@ -551,9 +574,9 @@ template <typename Launch> void aefdtd_sim::run_groups(const WorkSplit &w, Launc
 // Arguments of the E and H half-step kernels for steps whose scalars are in
 // the table `tbl` (shared by single-simulation segments and batches).
 template <typename T, typename Tid>
-void aefdtd_sim::make_step_args(StepArgs<T, Tid> &ea, StepArgs<T, Tid> &ha, const StepScalars *tbl) {
-    fill_args(ea, true);
-    fill_args(ha, false);
+void aefdtd_sim::make_step_args(StepArgs<T, Tid> &ea, StepArgs<T, Tid> &ha, const StepScalars *tbl, int grid) {
+    fill_args(ea, true, grid);
+    fill_args(ha, false, grid);
     ea.kchunk = ha.kchunk = kchunk;
     ea.prefetch = ha.prefetch = prefetch_l2 ? 1 : 0;
     ea.sc = ha.sc = tbl;
@@ -585,13 +608,13 @@ template <typename T> void aefdtd_sim::make_sensor_args(SensorStepArgs<T> &sa, c
 }
 
 template void aefdtd_sim::make_step_args<double, uint8_t>(StepArgs<double, uint8_t> &, StepArgs<double, uint8_t> &,
-                                                           const StepScalars *);
+                                                           const StepScalars *, int);
 template void aefdtd_sim::make_step_args<double, uint16_t>(StepArgs<double, uint16_t> &, StepArgs<double, uint16_t> &,
-                                                            const StepScalars *);
+                                                            const StepScalars *, int);
 template void aefdtd_sim::make_step_args<float, uint8_t>(StepArgs<float, uint8_t> &, StepArgs<float, uint8_t> &,
-                                                          const StepScalars *);
+                                                          const StepScalars *, int);
 template void aefdtd_sim::make_step_args<float, uint16_t>(StepArgs<float, uint16_t> &, StepArgs<float, uint16_t> &,
-                                                           const StepScalars *);
+                                                           const StepScalars *, int);
 template void aefdtd_sim::make_sensor_args<double>(SensorStepArgs<double> &, const StepScalars *);
 template void aefdtd_sim::make_sensor_args<float>(SensorStepArgs<float> &, const StepScalars *);
 
@@ -602,11 +625,13 @@ template void aefdtd_sim::make_sensor_args<float>(SensorStepArgs<float> &, const
 // scalars. With record = true per-step timing events are recorded.
 template <typename T, typename Tid>
 void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
-    StepArgs<T, Tid> ea, ha;
+    StepArgs<T, Tid> ea, ha, ea_i, ha_i;
     make_step_args(ea, ha, tbl);
+    if (obl) make_step_args(ea_i, ha_i, tbl, 1);   // the oblique driver's imaginary grid
     const int4 *wi = items.as<int4>();
     int groups = 0;
     for (int g = 0; g < kGroups; g++) groups += (wsE.n[g] > 0) + (wsH.n[g] > 0);
+    if (obl) groups *= 2;
     SensorStepArgs<T> sa;
     make_sensor_args(sa, tbl);
     // field sensors: this segment's phase rows (same table slot as tbl)
@@ -663,9 +688,11 @@ void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
     };
     for (int q = 0; q < L; q++) {
         if (record) AE_CUDA(cudaEventRecord(tev[4 * q + 0], stream));
-        ea.q = ha.q = q;
+        ea.q = ha.q = ea_i.q = ha_i.q = q;
         if (record && timing_mode == 2) timed_groups(q, 0, wsE, [&](int g, cudaStream_t st) { launch_e_group(ea, wi, wsE, g, st); });
         else run_groups(wsE, [&](int g, cudaStream_t st) { launch_e_group(ea, wi, wsE, g, st); });
+        // both grids' E read only H: the imaginary grid follows on the same phase
+        if (obl) run_groups(wsE, [&](int g, cudaStream_t st) { launch_e_group(ea_i, wi, wsE, g, st); });
         if (record) AE_CUDA(cudaEventRecord(tev[4 * q + 1], stream));
         // sensors: fed after H in both drivers; plane sums read E of this step
         sa.q = q;
@@ -684,7 +711,7 @@ void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
             g.S = s.S.as<T>() + ((size_t)s.half * dft_k + s.nbuf) * 6 * s.P;
         }
         const bool cc = cc_coeff > 0;
-        const bool part0 = sa.nbp > 0 || sa.ng > 0 || cc || maps_e;
+        const bool part0 = sa.nbp > 0 || sa.ng > 0 || cc || maps_e || obl;
         sa.part = 0;
         // completion energy of this step reads E only: with part 0, beside H
         auto energy = [&](cudaStream_t st) {
@@ -701,10 +728,12 @@ void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
                 launches += launch_sensor_step(sa, st);
                 energy(st);
                 maps(0, st);
+                if (obl) launches += launch_obl_sums<T>(q, tbl, st);
             });
         join_h();
         if (record && timing_mode == 2) timed_groups(q, 1, wsH, [&](int g, cudaStream_t st) { launch_h_group(ha, wi, wsH, g, st); });
         else run_groups(wsH, [&](int g, cudaStream_t st) { launch_h_group(ha, wi, wsH, g, st); });
+        if (obl) run_groups(wsH, [&](int g, cudaStream_t st) { launch_h_group(ha_i, wi, wsH, g, st); });
         launches += groups;
         if (record) AE_CUDA(cudaEventRecord(tev[4 * q + 2], stream));
         if (part0) {
@@ -714,6 +743,7 @@ void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
                 launches += launch_sensor_step(sa, stream);
                 energy(stream);
                 maps(0, stream);
+                if (obl) launches += launch_obl_sums<T>(q, tbl, stream);
             }
         }
         if (sa.ng > 0 || maps_h) {
@@ -757,6 +787,10 @@ void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
         launch_energy_reduce(cc_partial.as<double>(), cc_nb, tbl, cc_hist.as<double>(), L, stream);
         launches++;
     }
+    if (obl) {
+        launch_obl_reduce(obl->part.as<double>(), obl->nb, tbl, obl->hist.as<double>(), L, stream);
+        launches++;
+    }
 }
 
 // CompletionSensor::completion_check in energy mode (s_completion.cpp:39-43,
@@ -796,6 +830,11 @@ void aefdtd_sim::run_steps(int n) {
         psums.release(dev_bytes);
         psums = nb;
         psums_cap = cap;
+        graphs_dirty = true;
+        drop_graphs();
+    }
+    if (obl && tstep + n > obl->cap) {
+        obl_ensure(tstep + n);   // incident sums and R/T history (pointers the graphs bake in)
         graphs_dirty = true;
         drop_graphs();
     }
@@ -1002,6 +1041,15 @@ void aefdtd_sim::build_work() {
         mark_range(0, Nx, 0, Ny, Nz - std::max(pml[5], 1), Nz, kPZ);
     }
     if (normal) mark_range(0, Nx, 0, Ny, zs_e - 1, zs_e, kMISC);
+    if (obl) {
+        // oblique driver: Bloch wrap columns and rows (both half-steps) and the
+        // Bloch_Wideband planes z2 - 1 (H) and z2 (E)
+        mark_range(0, 1, 0, Ny, 0, Nz, kMISC);
+        mark_range(Nx - 1, Nx, 0, Ny, 0, Nz, kMISC);
+        mark_range(0, Nx, 0, 1, 0, Nz, kMISC);
+        mark_range(0, Nx, Ny - 1, Ny, 0, Nz, kMISC);
+        mark_range(0, Nx, 0, Ny, obl->z2 - 1, obl->z2 + 1, kMISC);
+    }
     for (auto &o : oscs) mark_range(o.box[0], o.box[1], o.box[2], o.box[3], o.box[4], o.box[5], kOSC);
     for (unsigned m = 0; m < Nmat; m++) {
         HostMat &h = mats[m];
@@ -1131,6 +1179,7 @@ void aefdtd_sim::step(int n) {
     if (n < 0) fail(AEFDTD_BAD_ARG, "negative step count");
     if (!map_set) fail(AEFDTD_NOT_READY, "no material map");
     if (g.mode == AEFDTD_MODE_NORMAL && !normal) fail(AEFDTD_NOT_READY, "normal mode needs aefdtd_setup_normal");
+    if (g.mode == AEFDTD_MODE_OBLIQUE && !obl) fail(AEFDTD_NOT_READY, "oblique mode needs aefdtd_setup_oblique");
     set_device();
     finalize_tables();
     if (fp64) {
@@ -1150,6 +1199,13 @@ void aefdtd_sim::zero_state() {
     for (auto &b : psiE) if (b.p) AE_CUDA(cudaMemsetAsync(b.p, 0, b.n, stream));
     for (auto &b : psiH) if (b.p) AE_CUDA(cudaMemsetAsync(b.p, 0, b.n, stream));
     if (psi.p) AE_CUDA(cudaMemsetAsync(psi.p, 0, psi.n, stream));
+    if (obl) {
+        for (int c = 0; c < 6; c++) {
+            DBuf *b[3] = {&obl->Fi[c], &obl->psiEi[c], &obl->psiHi[c]};
+            for (DBuf *x : b) if (x->p) AE_CUDA(cudaMemsetAsync(x->p, 0, x->n, stream));
+        }
+        if (obl->psi_i.p) AE_CUDA(cudaMemsetAsync(obl->psi_i.p, 0, obl->psi_i.n, stream));
+    }
     for (auto *s : sensors) {
         if (s->acc.p) AE_CUDA(cudaMemsetAsync(s->acc.p, 0, s->acc.n, stream));
         s->step = 0; s->nbuf = 0; s->half = 0; s->pending = false;
@@ -1379,16 +1435,17 @@ aefdtd_status aefdtd_reset(aefdtd_sim *s) {
 aefdtd_status aefdtd_get_field(aefdtd_sim *s, int32_t c, double *out, size_t count) {
     if (!s || !out) return AEFDTD_BAD_ARG;
     return guarded(s, [&] {
-        if (c < 0 || c > 5) fail(AEFDTD_BAD_ARG, "component out of range");
+        if (c < 0 || c > (s->obl ? 11 : 5)) fail(AEFDTD_BAD_ARG, "component out of range");
         size_t N = size_t(s->Nx) * s->Ny * s->Nz;
         if (count != N) fail(AEFDTD_BAD_ARG, "count must be Nx*Ny*Nz of the total grid");
         s->set_device();
+        const void *src = s->grid_fields(c / 6)[c % 6].p;
         if (s->fp64) {
-            AE_CUDA(cudaMemcpyAsync(out, s->F[c].p, N * 8, cudaMemcpyDeviceToHost, s->stream));
+            AE_CUDA(cudaMemcpyAsync(out, src, N * 8, cudaMemcpyDeviceToHost, s->stream));
             AE_CUDA(cudaStreamSynchronize(s->stream));
         } else {
             std::vector<float> tmp(N);
-            AE_CUDA(cudaMemcpyAsync(tmp.data(), s->F[c].p, N * 4, cudaMemcpyDeviceToHost, s->stream));
+            AE_CUDA(cudaMemcpyAsync(tmp.data(), src, N * 4, cudaMemcpyDeviceToHost, s->stream));
             AE_CUDA(cudaStreamSynchronize(s->stream));
             for (size_t q = 0; q < N; q++) out[q] = tmp[q];
         }
@@ -1398,23 +1455,24 @@ aefdtd_status aefdtd_get_field(aefdtd_sim *s, int32_t c, double *out, size_t cou
 aefdtd_status aefdtd_set_field(aefdtd_sim *s, int32_t c, const double *in, size_t count) {
     if (!s || !in) return AEFDTD_BAD_ARG;
     return guarded(s, [&] {
-        if (c < 0 || c > 5) fail(AEFDTD_BAD_ARG, "component out of range");
+        if (c < 0 || c > (s->obl ? 11 : 5)) fail(AEFDTD_BAD_ARG, "component out of range");
         size_t N = size_t(s->Nx) * s->Ny * s->Nz;
         if (count != N) fail(AEFDTD_BAD_ARG, "count must be Nx*Ny*Nz of the total grid");
         s->set_device();
+        void *dst = s->grid_fields(c / 6)[c % 6].p;
         if (s->fp64) {
-            AE_CUDA(cudaMemcpyAsync(s->F[c].p, in, N * 8, cudaMemcpyHostToDevice, s->stream));
+            AE_CUDA(cudaMemcpyAsync(dst, in, N * 8, cudaMemcpyHostToDevice, s->stream));
         } else {
             std::vector<float> tmp(in, in + N);
-            AE_CUDA(cudaMemcpyAsync(s->F[c].p, tmp.data(), N * 4, cudaMemcpyHostToDevice, s->stream));
+            AE_CUDA(cudaMemcpyAsync(dst, tmp.data(), N * 4, cudaMemcpyHostToDevice, s->stream));
         }
         AE_CUDA(cudaStreamSynchronize(s->stream));
     });
 }
 
 aefdtd_status aefdtd_field_device_ptr(aefdtd_sim *s, int32_t c, void **ptr) {
-    if (!s || !ptr || c < 0 || c > 5) return AEFDTD_BAD_ARG;
-    *ptr = s->F[c].p;
+    if (!s || !ptr || c < 0 || c > (s->obl ? 11 : 5)) return AEFDTD_BAD_ARG;
+    *ptr = s->grid_fields(c / 6)[c % 6].p;
     return AEFDTD_OK;
 }
 

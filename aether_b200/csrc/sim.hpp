@@ -146,6 +146,27 @@ struct FieldMapHost {
     DBuf acc;
 };
 
+// Oblique driver state (FDTD_oblique_biphase_comp, oblique_biphase.cpp:29-330):
+// the imaginary grid's fields and CPML / dispersive state, the wideband Bloch
+// source (Bloch_Wideband, sc_bloch.cpp), phases and the R/T sum history.
+struct Oblique {
+    aefdtd_oblique_desc d{};
+    double kx = 0, ky = 0, kxy = 0;     // k_in * n_sup
+    double eps_sup = 1, eps_sub = 1, index_sup = 1, index_sub = 1;
+    cplx dE_x, dE_y, dH_x, dH_y;        // Bloch phases of the wraps: e^{+-i k N D}
+    // Bloch_Wideband (sc_bloch.cpp:85-214)
+    int z2 = 0, t_offset = 0, nlines = 0;
+    double eps_inf = 1, c2z = 0;
+    std::vector<double> w, kz, eb, hb;  // eb: [l][3], hb: [l][2]
+    DBuf dw, dkz, deb, dhb;
+    DBuf Fi[6], psiEi[6], psiHi[6], psi_i;   // imaginary grid
+    DBuf ph;                            // [3][Nx*Ny] complex e^{+i k.r} at the Ex, Ey, Ez points
+    DBuf mk;                            // [3][Nx*Ny] complex mk_x, mk_y, mk_z = e^{-i k.r}
+    DBuf inc;                           // [cap][14] per-step incident sums
+    DBuf part, hist;                    // R/T sums: per-step block partials, [cap][18] history
+    int cap = 0, nb = 0;
+};
+
 static inline double s_curve(double x, double xmin, double xmax) {
     // src/common/mathUT.cpp:1186-1193
     double u = (x - xmin) / (xmax - xmin);
@@ -212,6 +233,11 @@ struct aefdtd_sim {
     std::vector<Osc> oscs;
     std::vector<PlaneSensor *> sensors;
     std::vector<std::array<int, 6>> boxes;   // box sensors: planar sensor per face (-1: disabled)
+    Oblique *obl = nullptr;                  // mode OBLIQUE after aefdtd_setup_oblique
+    void obl_ensure(int steps);              // incident table and history for `steps` steps
+    template <typename T> int launch_obl_sums(int q, const StepScalars *tbl, cudaStream_t st);
+    void find_slab(int sub_ref, int sup_ref, double &hsub, double &hstruc, double &hsup) const;
+    DBuf *grid_fields(int grid) { return grid && obl ? obl->Fi : F; }
     std::vector<FieldMapHost *> fmaps;       // single-wavelength field sensors
     DBuf fm_tbl;                             // their phases: [slot][seg_len][kMaxMaps][4] doubles
     std::vector<double> map_rows;            // host staging of one segment's phase rows
@@ -245,7 +271,7 @@ struct aefdtd_sim {
     void set_map(const uint32_t *m, size_t count);
     void set_material(uint32_t idx, const aefdtd_material_desc *md);
     void finalize_tables();
-    template <typename T, typename Tid> void fill_args(StepArgs<T, Tid> &a, bool e_side);
+    template <typename T, typename Tid> void fill_args(StepArgs<T, Tid> &a, bool e_side, int grid = 0);
     template <typename T, typename Tid> void run_steps(int n);
     template <typename T>
     void flush_block(PlaneSensor &s, int half, int n, const StepScalars *step0_ptr, int step0, cudaStream_t st);
@@ -255,7 +281,7 @@ struct aefdtd_sim {
     cudaEvent_t ev_f_fork = nullptr, ev_f_join = nullptr;
     template <typename T, typename Tid> void enqueue_segment(int L, StepScalars *tbl, bool record);
     template <typename T, typename Tid>
-    void make_step_args(StepArgs<T, Tid> &ea, StepArgs<T, Tid> &ha, const StepScalars *tbl);
+    void make_step_args(StepArgs<T, Tid> &ea, StepArgs<T, Tid> &ha, const StepScalars *tbl, int grid = 0);
     template <typename T> void make_sensor_args(SensorStepArgs<T> &sa, const StepScalars *tbl);
     void *batch = nullptr;          // the batch this simulation is a member of (it steps it)
     void fill_scalars(int t, int osc_offset, StepScalars &s) const;
@@ -314,6 +340,13 @@ inline aefdtd_sim::~aefdtd_sim() {
     for (auto &gx : graph_exec) if (gx.second) cudaGraphExecDestroy(gx.second);
     items.release(t);
     fm_tbl.release(t);
+    if (obl) {
+        for (int c = 0; c < 6; c++) { obl->Fi[c].release(t); obl->psiEi[c].release(t); obl->psiHi[c].release(t); }
+        DBuf *b[] = {&obl->psi_i, &obl->ph, &obl->mk, &obl->inc, &obl->part, &obl->hist,
+                     &obl->dw, &obl->dkz, &obl->deb, &obl->dhb};
+        for (DBuf *x : b) x->release(t);
+        delete obl;
+    }
     for (auto *m : fmaps) { m->acc.release(t); delete m; }
     for (auto *s : sensors) {
         s->S.release(t); s->acc.release(t); s->wdev.release(t); s->WE.release(t); s->WH.release(t); s->flux.release(t);

@@ -283,6 +283,16 @@ __device__ __forceinline__ void h_interior_body(const StepArgs<T, Tid> &a, int q
     }
 }
 
+// Bloch wrap of the oblique driver (oblique_biphase.cpp:211-290): the value
+// past the x or y edge is the wrapped cell's complex field (real grid +
+// i imaginary grid) times the Bloch phase c + i d; the real grid takes the
+// real part, the imaginary grid the imaginary part, in std::complex order.
+template <typename T>
+__device__ __forceinline__ T bloch_ghost(int bloch, T own, T other, double c, double d) {
+    const T tc = (T)c, td = (T)d;
+    return bloch == 1 ? own * tc - other * td : other * td + own * tc;
+}
+
 // ---- boundary items: the phases of feature set F ---------------------------
 template <typename T, typename Tid, unsigned F>
 __device__ __forceinline__ void e_boundary_body(const StepArgs<T, Tid> &a, int q, int4 it) {
@@ -327,8 +337,21 @@ __device__ __forceinline__ void e_boundary_body(const StepArgs<T, Tid> &a, int q
     for (int k = k0; k < k1; ++k) {
         const long long id = col + k * NxNy;
         const T hx = __ldg(Hx + id), hy = __ldg(Hy + id), hz = __ldg(Hz + id);
-        const T hz_jm = __ldg(Hz + coly + k * NxNy), hx_jm = __ldg(Hx + coly + k * NxNy);
-        const T hz_im = __ldg(Hz + colx + k * NxNy), hy_im = __ldg(Hy + colx + k * NxNy);
+        T hz_jm = __ldg(Hz + coly + k * NxNy), hx_jm = __ldg(Hx + coly + k * NxNy);
+        T hz_im = __ldg(Hz + colx + k * NxNy), hy_im = __ldg(Hy + colx + k * NxNy);
+        if constexpr ((F & kFMisc) != 0) {
+            // oblique driver: H ghosts past the y = 0 and x = 0 edges (set before update_E)
+            if (a.bloch) {
+                if (j == 0) {
+                    hz_jm = bloch_ghost(a.bloch, hz_jm, __ldg(a.oHz + coly + k * NxNy), a.byr, a.byi);
+                    hx_jm = bloch_ghost(a.bloch, hx_jm, __ldg(a.oHx + coly + k * NxNy), a.byr, a.byi);
+                }
+                if (i == 0) {
+                    hz_im = bloch_ghost(a.bloch, hz_im, __ldg(a.oHz + colx + k * NxNy), a.bxr, a.bxi);
+                    hy_im = bloch_ghost(a.bloch, hy_im, __ldg(a.oHy + colx + k * NxNy), a.bxr, a.bxi);
+                }
+            }
+        }
         const T ex = Ex[id], ey = Ey[id], ez = Ez[id];
         const int m = __ldg(a.mat + colm + k * mNxNy);
         const MatCoef<T> c = a.coef[m];
@@ -468,6 +491,16 @@ __device__ __forceinline__ void e_boundary_body(const StepArgs<T, Tid> &a, int q
                 nex = nex - (T)a.sc[q].inj_eA;
                 ney = ney + (T)a.sc[q].inj_eB;
             }
+            // Bloch_Wideband::inject_E after update_E (sc_bloch.cpp:216-250): the
+            // step's complex H sums times the column's phase, real or imaginary part
+            if (k == a.kobl) {
+                const double *v = a.obl_inc + (size_t)a.sc[q].step * 14;
+                const double2 px = a.obl_px[col], py = a.obl_py[col];
+                const double hyr = v[2] * px.x - v[3] * px.y, hyi = v[2] * px.y + v[3] * px.x;
+                const double hxr = v[0] * py.x - v[1] * py.y, hxi = v[0] * py.y + v[1] * py.x;
+                nex = nex - (T)(a.obl_coef * (a.bloch == 1 ? hyr : hyi));
+                ney = ney + (T)(a.obl_coef * (a.bloch == 1 ? hxr : hxi));
+            }
             // Oscillator boxes after update_E (sc_oscillator.cpp:43-63)
             for (int s = 0; s < a.nsrc; ++s) {
                 const int *b = a.src_box[s];
@@ -530,8 +563,21 @@ __device__ __forceinline__ void h_boundary_body(const StepArgs<T, Tid> &a, int q
         const int kp = (k == a.Nz - 1) ? 0 : k + 1;
         const T ex_kp = __ldg(Ex + col + kp * NxNy), ey_kp = __ldg(Ey + col + kp * NxNy);
         const T ez = __ldg(Ez + id);
-        const T ez_jp = __ldg(Ez + coly + k * NxNy), ex_jp = __ldg(Ex + coly + k * NxNy);
-        const T ez_ip = __ldg(Ez + colx + k * NxNy), ey_ip = __ldg(Ey + colx + k * NxNy);
+        T ez_jp = __ldg(Ez + coly + k * NxNy), ex_jp = __ldg(Ex + coly + k * NxNy);
+        T ez_ip = __ldg(Ez + colx + k * NxNy), ey_ip = __ldg(Ey + colx + k * NxNy);
+        if constexpr ((F & kFMisc) != 0) {
+            // oblique driver: E ghosts past the y = Ny-1 and x = Nx-1 edges (set after inject_E)
+            if (a.bloch) {
+                if (j == a.Ny - 1) {
+                    ez_jp = bloch_ghost(a.bloch, ez_jp, __ldg(a.oEz + coly + k * NxNy), a.byr, a.byi);
+                    ex_jp = bloch_ghost(a.bloch, ex_jp, __ldg(a.oEx + coly + k * NxNy), a.byr, a.byi);
+                }
+                if (i == a.Nx - 1) {
+                    ez_ip = bloch_ghost(a.bloch, ez_ip, __ldg(a.oEz + colx + k * NxNy), a.bxr, a.bxi);
+                    ey_ip = bloch_ghost(a.bloch, ey_ip, __ldg(a.oEy + colx + k * NxNy), a.bxr, a.bxi);
+                }
+            }
+        }
         const T hx = Hx[id], hy = Hy[id], hz = Hz[id];
         const T az = a.dtdmz * __ldg(a.ikz + k);
 
@@ -611,6 +657,16 @@ __device__ __forceinline__ void h_boundary_body(const StepArgs<T, Tid> &a, int q
             if (k == a.kinj) {
                 nhx = nhx + (T)a.sc[q].inj_hA;
                 nhy = nhy - (T)a.sc[q].inj_hB;
+            }
+            // Bloch_Wideband::inject_H (sc_bloch.cpp:252-285): dtdmz times the
+            // step's complex E sums times the column's phase
+            if (k == a.kobl) {
+                const double *v = a.obl_inc + (size_t)a.sc[q].step * 14 + 4;
+                const double2 px = a.obl_px[col], py = a.obl_py[col];
+                const double exr = v[0] * px.x - v[1] * px.y, exi = v[0] * px.y + v[1] * px.x;
+                const double eyr = v[2] * py.x - v[3] * py.y, eyi = v[2] * py.y + v[3] * py.x;
+                nhx = nhx + (T)(a.obl_coef * (a.bloch == 1 ? eyr : eyi));
+                nhy = nhy - (T)(a.obl_coef * (a.bloch == 1 ? exr : exi));
             }
         }
         Hx[id] = nhx;

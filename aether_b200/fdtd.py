@@ -183,8 +183,28 @@ class Simulation:
         self._c(self._lib.aefdtd_get_field(self._h, comp, out.ctypes.data_as(_P(C.c_double)), out.size))
         return out.reshape(d.nz, d.ny, d.nx)
 
-    def fields(self) -> np.ndarray:
-        return np.stack([self.field(c) for c in range(6)])
+    def fields(self, grid: int = 0) -> np.ndarray:
+        """Ex..Hz; grid 1: the imaginary grid of the oblique driver."""
+        return np.stack([self.field(6 * grid + c) for c in range(6)])
+
+    def setup_oblique(self, od):
+        self._c(self._lib.aefdtd_setup_oblique(self._h, C.byref(od)))
+        self._obl_nl = int(od.nl)
+
+    def oblique_spectra(self) -> np.ndarray:
+        """(nl', 10): lambda, angle (deg), |r_TE|, arg, |r_TM|, arg, |t_TE|, arg, |t_TM|, arg."""
+        out = np.empty((self._obl_nl, 10))
+        n = C.c_int32(0)
+        self._c(self._lib.aefdtd_get_oblique_spectra(self._h, out.ctypes.data_as(_P(C.c_double)), self._obl_nl,
+                                                     C.byref(n)))
+        return out[:n.value]
+
+    def oblique_series(self) -> np.ndarray:
+        """(steps, 18): BR, R, T sums (x, y, z as re, im) per step."""
+        n = self.dims().step
+        out = np.empty((n, 18))
+        self._c(self._lib.aefdtd_get_oblique_series(self._h, out.ctypes.data_as(_P(C.c_double)), out.size))
+        return out
 
     def set_field(self, comp: int, values: np.ndarray):
         v = np.ascontiguousarray(values, dtype=np.float64).ravel()
@@ -226,6 +246,8 @@ def build_simulation(scene) -> Simulation:
             sim.set_material(i, m)
         if scene.grid.mode == A.MODE_NORMAL:
             sim.setup_normal(scene.normal)
+        if scene.grid.mode == A.MODE_OBLIQUE:
+            sim.setup_oblique(scene.oblique)
         for s in scene.sources:
             sim.add_oscillator(s)
         for s in scene.sensors:
@@ -253,6 +275,10 @@ def run(scene, nsteps=None, want_fields=True):
         if scene.grid.mode == A.MODE_NORMAL:
             out["plane_sums"] = sim.plane_sums()
             out["spectra"] = sim.normal_spectra() if nsteps >= 2 else None
+        elif scene.grid.mode == A.MODE_OBLIQUE:
+            out["fields_imag"] = sim.fields(1) if want_fields else None
+            out["plane_sums"] = sim.oblique_series()
+            out["spectra"] = sim.oblique_spectra() if nsteps >= 2 else None
         else:
             out["plane_sums"] = None
             out["spectra"] = None

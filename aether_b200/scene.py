@@ -26,6 +26,7 @@ class Scene:
     materials: List[A.MaterialDesc]
     nsteps: int
     normal: Optional[A.NormalDesc] = None
+    oblique: Optional[A.ObliqueDesc] = None   # mode OBLIQUE: polarization, spectrum, in-plane k
     sensors: List[A.SensorDesc] = dataclasses.field(default_factory=list)
     sources: List[A.SourceDesc] = dataclasses.field(default_factory=list)
     name: str = "scene"
@@ -41,7 +42,7 @@ class Scene:
         g = self.grid
         pml = list(g.pml)
         pad = list(g.pad)
-        if g.mode == A.MODE_NORMAL:
+        if g.mode in (A.MODE_NORMAL, A.MODE_OBLIQUE):
             pml[:4] = [0, 0, 0, 0]
             pad[:4] = [0, 0, 0, 0]
             pad[4] = max(5, pad[4])

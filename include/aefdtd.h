@@ -45,9 +45,14 @@ typedef enum aefdtd_status {
 /* Driver orderings. NORMAL = "fdtd_normal" (normal_incidence.cpp:325-436):
  * E, E-plane injection, H, H-plane injection, sensor feed, R/T plane sums.
  * CUSTOM = "fdtd" (default_fdtd.cpp:156-204): E, source inject_E, H, sensor
- * feed, source inject_H. The grid padding rules follow the FDTD constructor
- * (fdtd_core.cpp:158-251) for modes "NORM" and "CUSTOM". */
-typedef enum aefdtd_mode { AEFDTD_MODE_NORMAL = 0, AEFDTD_MODE_CUSTOM = 1 } aefdtd_mode;
+ * feed, source inject_H. OBLIQUE = "fdtd_oblique_ARS", one in-plane
+ * wavevector (FDTD_oblique_biphase_comp, oblique_biphase.cpp:29-330): two grids hold
+ * the real and imaginary parts of a Bloch-periodic field; per step E of both
+ * grids, Bloch_Wideband inject_E, H of both, inject_H, sensor feed (real
+ * grid), R/T sums. The grid padding rules follow the FDTD constructor
+ * (fdtd_core.cpp:158-251) for modes "NORM", "CUSTOM" and "OBL_PHASE" (no x/y
+ * PML or pads; z pads raised to 5 by the oblique driver). */
+typedef enum aefdtd_mode { AEFDTD_MODE_NORMAL = 0, AEFDTD_MODE_CUSTOM = 1, AEFDTD_MODE_OBLIQUE = 2 } aefdtd_mode;
 
 /* FP64: bit-compatible operation order with the reference CPU core.
  * FP32: fields, CPML and dispersive state in FP32; coefficients generated in
@@ -202,6 +207,29 @@ aefdtd_status aefdtd_voxelize(aefdtd_sim *sim, int32_t nx, int32_t ny, int32_t n
  * plane-sum R/T sensors and their spectrum (normal_incidence.cpp:228-262).
  * Requires mode NORMAL and a material map with materials set. */
 aefdtd_status aefdtd_setup_normal(aefdtd_sim *sim, const aefdtd_normal_desc *nd);
+/* Oblique incidence at a fixed in-plane wavevector (FDTD_oblique_biphase_comp,
+ * oblique_biphase.cpp:29-330): kx_in, ky_in are the driver's kx_in, ky_in
+ * (rad/m in vacuum; the grids use k = k_in * n_sup). Sets up the wideband
+ * Bloch plane wave (Bloch_Wideband, sc_bloch.cpp:23-285, 30001 spectral
+ * lines, injected at the structure top z = zs_e), the Bloch phases of the
+ * x/y wraps and the R/T sums. polarization: 0 = "TE", 1 = "TM". Requires
+ * mode OBLIQUE and a material map with materials set. */
+typedef struct aefdtd_oblique_desc {
+    int32_t polarization;
+    int32_t nl;
+    double lambda_min, lambda_max;
+    double kx_in, ky_in;
+} aefdtd_oblique_desc;
+aefdtd_status aefdtd_setup_oblique(aefdtd_sim *sim, const aefdtd_oblique_desc *od);
+/* Spectra of the steps run so far (oblique_biphase.cpp:334-480): after the
+ * driver's resizing of the wavelength range to the 89-degree limit, nl_out
+ * wavelengths of 10 columns: lambda, incidence angle (degrees), |r_TE|,
+ * arg r_TE, |r_TM|, arg r_TM, |t_TE|, arg t_TE, |t_TM|, arg t_TM (the columns
+ * of the driver's obl_ file). out holds at most nl_max rows. */
+aefdtd_status aefdtd_get_oblique_spectra(aefdtd_sim *sim, double *out, int32_t nl_max, int32_t *nl_out);
+/* Per-step R/T sums of the steps run (steps x 18 doubles: the complex
+ * BRsensorX..Z, RsensorX..Z, TsensorX..Z of the driver; BT equals BR). */
+aefdtd_status aefdtd_get_oblique_series(aefdtd_sim *sim, double *out, size_t count);
 /* Replaces generate_fdtd_source(...Oscillator) + Source::link (sources.cpp:252-283). */
 aefdtd_status aefdtd_add_oscillator(aefdtd_sim *sim, const aefdtd_source_desc *src, int32_t *source_id);
 /* Replaces generate_fdtd_sensor(...PLANAR_SPECTRAL_POYNTING) (sensors.cpp:402-417). */
@@ -223,7 +251,9 @@ aefdtd_status aefdtd_reset(aefdtd_sim *sim);
 /* ---- results ---------------------------------------------------------- */
 
 /* Copies one field component of the total grid (Nx*Ny*Nz values) into host
- * memory as double regardless of precision (replaces reading FDTD::Ex..Hz). */
+ * memory as double regardless of precision (replaces reading FDTD::Ex..Hz).
+ * In mode OBLIQUE components 6..11 are Ex..Hz of the imaginary grid (the
+ * reference's fdtd_i; its x/y ghost layers are not stored). */
 aefdtd_status aefdtd_get_field(aefdtd_sim *sim, int32_t component, double *out, size_t count);
 /* Overwrites one field component from host memory (checkpoint restore). */
 aefdtd_status aefdtd_set_field(aefdtd_sim *sim, int32_t component, const double *in, size_t count);

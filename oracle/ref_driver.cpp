@@ -429,6 +429,220 @@ int aeref_run(const aefdtd_grid_desc *g, const uint32_t *map,
     return 0;
 }
 
+/* Oblique incidence at one in-plane wavevector through the reference core:
+ * FDTD_oblique_biphase_comp (oblique_biphase.cpp:29-480) minus the
+ * structure discretisation (map is the structure-size material map), the
+ * previews, sensors and files. Outputs (each may be NULL): fields_out 12 *
+ * Ntot doubles (Ex..Hz of fdtd_r, then of fdtd_i, without the ghost layers);
+ * series_out nsteps * 18 (BRsensorX..Z, RsensorX..Z, TsensorX..Z as re, im);
+ * spectra_out nl_max * 10 (the obl_ file columns), nl_out the resized Nl;
+ * dims_out as for aeref_run. */
+int aeref_run_oblique(const aefdtd_grid_desc *g, const uint32_t *map, const aefdtd_material_desc *mats, int32_t nmat,
+                      const aefdtd_oblique_desc *od, int32_t nsteps, int32_t quiet, double *fields_out,
+                      double *series_out, double *spectra_out, int32_t nl_max, int32_t *nl_out, int32_t *dims_out,
+                      double *loop_seconds) {
+    if (!g || !map || !mats || nmat <= 0 || nsteps < 0 || !od) return 1;
+    CoutSilencer *silence = quiet ? new CoutSilencer() : nullptr;
+    int Nx = g->nx, Ny = g->ny, Nz = g->nz, Nt = nsteps;
+    double Dx = g->dx, Dy = g->dy, Dz = g->dz;
+    Grid3<unsigned int> matsgrid(Nx, Ny, Nz, 0);
+    for (int k = 0; k < Nz; k++)
+        for (int j = 0; j < Ny; j++)
+            for (int i = 0; i < Nx; i++) matsgrid(i, j, k) = map[i + size_t(j) * Nx + size_t(k) * Nx * Ny];
+    double Dt = g->dt;
+    if (Dt <= 0) Dt = std::min(std::min(Dx, Dy), Dz) / (std::sqrt(3.0) * c_light) * 0.99 * g->time_mod;
+    const int pad_zm = std::max(5, g->pad[AEFDTD_ZM]), pad_zp = std::max(5, g->pad[AEFDTD_ZP]);
+    FDTD fdtd_r(Nx, Ny, Nz, Nt, Dx, Dy, Dz, Dt, "OBL_PHASE", 0, 0, 0, 0, g->pml[AEFDTD_ZM], g->pml[AEFDTD_ZP],
+                0, 0, 0, 0, pad_zm, pad_zp);
+    FDTD fdtd_i(Nx, Ny, Nz, Nt, Dx, Dy, Dz, Dt, "OBL_PHASE", 0, 0, 0, 0, g->pml[AEFDTD_ZM], g->pml[AEFDTD_ZP],
+                0, 0, 0, 0, pad_zm, pad_zp);
+    for (FDTD *f : {&fdtd_r, &fdtd_i}) {
+        f->set_pml_zm(g->pml_kappa[AEFDTD_ZM], g->pml_sigma[AEFDTD_ZM], g->pml_alpha[AEFDTD_ZM]);
+        f->set_pml_zp(g->pml_kappa[AEFDTD_ZP], g->pml_sigma[AEFDTD_ZP], g->pml_alpha[AEFDTD_ZP]);
+        f->set_tapering(g->tapering);
+        f->set_matsgrid(matsgrid);
+        for (int m = 0; m < nmat; m++) f->set_material(m, make_material(mats[m]));
+        f->bootstrap();
+    }
+    Nx = fdtd_r.Nx; Ny = fdtd_r.Ny; Nz = fdtd_r.Nz;
+    const int zs_s = fdtd_r.zs_s, zs_e = fdtd_r.zs_e;
+    if (dims_out) {
+        int d[10] = {fdtd_r.Nx, fdtd_r.Ny, fdtd_r.Nz, fdtd_r.xs_s, fdtd_r.xs_e, fdtd_r.ys_s, fdtd_r.ys_e,
+                     fdtd_r.zs_s, fdtd_r.zs_e, int(fdtd_r.Nmat)};
+        for (int i = 0; i < 10; i++) dims_out[i] = d[i];
+    }
+    double eps_sub = fdtd_r.mats[fdtd_r.matsgrid(0, 0, zs_s)].ei;
+    double eps_sup = fdtd_r.mats[fdtd_r.matsgrid(0, 0, zs_e)].ei;
+    double index_sub = std::sqrt(eps_sub), index_sup = std::sqrt(eps_sup);
+    double kx = od->kx_in * index_sup, ky = od->ky_in * index_sup, kxy = std::sqrt(kx * kx + ky * ky);
+    AngleRad pol;
+    pol.degree(0);
+    if (od->polarization == 1) pol.degree(90);
+    Bloch_Wideband inc_field(0, Nx, 0, Ny, 0, fdtd_r.Nz_s, kx, ky, pol);
+    inc_field.set_spectrum(od->lambda_min, od->lambda_max);
+    inc_field.link(fdtd_r);
+    Imdouble dephasE_x = std::exp(kx * Nx * Dx * Im), dephasE_y = std::exp(ky * Ny * Dy * Im);
+    Imdouble dephasH_x = std::exp(-kx * Nx * Dx * Im), dephasH_y = std::exp(-ky * Ny * Dy * Im);
+    fdtd_r.set_kx(kx); fdtd_r.set_ky(ky);
+    fdtd_i.set_kx(kx); fdtd_i.set_ky(ky);
+    Grid2<double> inc_Ex(Nx, Ny, 0), inc_Ey(Nx, Ny, 0), inc_Ez(Nx, Ny, 0);
+    Grid2<Imdouble> mk_x(Nx, Ny, 0), mk_y(Nx, Ny, 0), mk_z(Nx, Ny, 0);
+    for (int i = 0; i < Nx; i++)
+        for (int j = 0; j < Ny; j++) {
+            mk_x(i, j) = std::exp(-(kx * (i + 0.5) * Dx + ky * j * Dy) * Im);
+            mk_y(i, j) = std::exp(-(kx * i * Dx + ky * (j + 0.5) * Dy) * Im);
+            mk_z(i, j) = std::exp(-(kx * i * Dx + ky * j * Dy) * Im);
+        }
+    std::vector<Imdouble> BR[3], R[3], T[3];
+    for (int d = 0; d < 3; d++) { BR[d].assign(Nt, 0); R[d].assign(Nt, 0); T[d].assign(Nt, 0); }
+    fdtd_r.reset_fields();
+    fdtd_i.reset_fields();
+    fdtd_r.tstep = 0;
+    fdtd_i.tstep = 0;
+    auto t0 = std::chrono::steady_clock::now();
+    Imdouble i_E, i_H;
+    for (int t = 0; t < Nt; t++) {
+        for (int k = 0; k < Nz; k++) {   // Bloch conditions, H (:211-240)
+            for (int i = 0; i < Nx; i++) {
+                i_H = fdtd_r.Hx(i, Ny - 1, k) + fdtd_i.Hx(i, Ny - 1, k) * Im;
+                fdtd_r.Hx(i, Ny, k) = std::real(i_H * dephasH_y);
+                fdtd_i.Hx(i, Ny, k) = std::imag(i_H * dephasH_y);
+                i_H = fdtd_r.Hz(i, Ny - 1, k) + fdtd_i.Hz(i, Ny - 1, k) * Im;
+                fdtd_r.Hz(i, Ny, k) = std::real(i_H * dephasH_y);
+                fdtd_i.Hz(i, Ny, k) = std::imag(i_H * dephasH_y);
+            }
+            for (int j = 0; j < Ny; j++) {
+                i_H = fdtd_r.Hy(Nx - 1, j, k) + fdtd_i.Hy(Nx - 1, j, k) * Im;
+                fdtd_r.Hy(Nx, j, k) = std::real(i_H * dephasH_x);
+                fdtd_i.Hy(Nx, j, k) = std::imag(i_H * dephasH_x);
+                i_H = fdtd_r.Hz(Nx - 1, j, k) + fdtd_i.Hz(Nx - 1, j, k) * Im;
+                fdtd_r.Hz(Nx, j, k) = std::real(i_H * dephasH_x);
+                fdtd_i.Hz(Nx, j, k) = std::imag(i_H * dephasH_x);
+            }
+        }
+        fdtd_r.update_E();
+        fdtd_i.update_E();
+        inc_field.inject_E(fdtd_r, fdtd_i);
+        for (int k = 0; k < Nz; k++) {   // Bloch conditions, E (:252-282)
+            for (int i = 0; i < Nx; i++) {
+                i_E = fdtd_r.Ex(i, 0, k) + fdtd_i.Ex(i, 0, k) * Im;
+                fdtd_r.Ex(i, Ny, k) = std::real(i_E * dephasE_y);
+                fdtd_i.Ex(i, Ny, k) = std::imag(i_E * dephasE_y);
+                i_E = fdtd_r.Ez(i, 0, k) + fdtd_i.Ez(i, 0, k) * Im;
+                fdtd_r.Ez(i, Ny, k) = std::real(i_E * dephasE_y);
+                fdtd_i.Ez(i, Ny, k) = std::imag(i_E * dephasE_y);
+            }
+            for (int j = 0; j < Ny; j++) {
+                i_E = fdtd_r.Ey(0, j, k) + fdtd_i.Ey(0, j, k) * Im;
+                fdtd_r.Ey(Nx, j, k) = std::real(i_E * dephasE_x);
+                fdtd_i.Ey(Nx, j, k) = std::imag(i_E * dephasE_x);
+                i_E = fdtd_r.Ez(0, j, k) + fdtd_i.Ez(0, j, k) * Im;
+                fdtd_r.Ez(Nx, j, k) = std::real(i_E * dephasE_x);
+                fdtd_i.Ez(Nx, j, k) = std::imag(i_E * dephasE_x);
+            }
+        }
+        fdtd_r.update_H();
+        fdtd_i.update_H();
+        inc_field.inject_H(fdtd_r, fdtd_i);
+        double tb = (t + 0.5) * Dt;   // R/T sums (:300-327)
+        double z = zs_s * Dz;
+        inc_field.get_E(inc_Ex, inc_Ey, inc_Ez, z, tb);
+        for (int i = 0; i < Nx; i++)
+            for (int j = 0; j < Ny; j++) {
+                BR[0][t] += inc_Ex(i, j) * mk_x(i, j);
+                BR[1][t] += inc_Ey(i, j) * mk_y(i, j);
+                BR[2][t] += inc_Ez(i, j) * mk_z(i, j);
+                R[0][t] += fdtd_r.Ex(i, j, zs_e + 2) * mk_x(i, j);
+                R[1][t] += fdtd_r.Ey(i, j, zs_e + 2) * mk_y(i, j);
+                R[2][t] += 0.5 * (fdtd_r.Ez(i, j, zs_e + 1) + fdtd_r.Ez(i, j, zs_e + 2)) * mk_z(i, j);
+                T[0][t] += fdtd_r.Ex(i, j, zs_s) * mk_x(i, j);
+                T[1][t] += fdtd_r.Ey(i, j, zs_s) * mk_y(i, j);
+                T[2][t] += 0.5 * (fdtd_r.Ez(i, j, zs_s) + fdtd_r.Ez(i, j, zs_s - 1)) * mk_z(i, j);
+            }
+    }
+    if (loop_seconds) loop_seconds[0] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (fields_out) {
+        const size_t n = size_t(Nx) * Ny * Nz;
+        copy_fields(fdtd_r, fields_out);
+        copy_fields(fdtd_i, fields_out + 6 * n);
+    }
+    if (series_out)
+        for (int t = 0; t < Nt; t++)
+            for (int d = 0; d < 3; d++) {
+                double *o = series_out + size_t(t) * 18;
+                o[2 * d] = BR[d][t].real(); o[2 * d + 1] = BR[d][t].imag();
+                o[6 + 2 * d] = R[d][t].real(); o[7 + 2 * d] = R[d][t].imag();
+                o[12 + 2 * d] = T[d][t].real(); o[13 + 2 * d] = T[d][t].imag();
+            }
+    if (spectra_out && Nt >= 2) {
+        // :334-480
+        int Nl = od->nl;
+        double lambda_min = od->lambda_min, lambda_max = od->lambda_max;
+        double lambda_limit_max = lambda_max;
+        if (kx != 0 || ky != 0) lambda_limit_max = 2 * Pi * std::sin(89.0 * Pi / 180.0) * index_sup / kxy;
+        if (lambda_limit_max < lambda_max) {
+            double D_lambda = (lambda_max - lambda_min) / (Nl - 1.0);
+            Nl = static_cast<int>((lambda_limit_max - lambda_min) / D_lambda);
+            if (Nl < 2) Nl = 2;
+            lambda_max = lambda_min + (Nl - 1.0) * D_lambda;
+        }
+        if (nl_out) *nl_out = Nl;
+        double hsup, hsub, hstruc;
+        fdtd_r.find_slab(zs_s, zs_e + 2, hsub, hstruc, hsup);
+        AngleRad inc_ang, ref_ang, phi(std::atan2(ky, kx));
+        phi = std::atan2(ky, kx);
+        double cp = std::cos(phi), sp = std::sin(phi);
+        for (int l = 0; l < Nl && l < nl_max; l++) {
+            double lambda = lambda_min + (lambda_max - lambda_min) * l / (Nl - 1.0);
+            double w = 2.0 * Pi * c_light / lambda;
+            double kn = 2.0 * Pi * index_sup / lambda;
+            inc_ang = std::asin(kxy / kn);
+            ref_ang = std::asin(index_sup / index_sub * std::sin(inc_ang));
+            double s_k0 = -w / c_light, s_k1 = s_k0 * index_sup, s_k3 = s_k0 * index_sub;
+            Imdouble BRS[3] = {0, 0, 0}, RS[3] = {0, 0, 0}, BTS[3] = {0, 0, 0}, TS[3] = {0, 0, 0};
+            for (int t = 0; t < Nt; t++) {
+                Imdouble coeff = std::exp(w * t * Dt * Im);
+                for (int d = 0; d < 3; d++) {
+                    BRS[d] += BR[d][t] * coeff;
+                    RS[d] += R[d][t] * coeff;
+                    BTS[d] += BR[d][t] * coeff;
+                    TS[d] += T[d][t] * coeff;
+                }
+            }
+            Imdouble *rot[4] = {BRS, RS, BTS, TS};
+            for (Imdouble *v : rot) {
+                Imdouble tmp_x = v[0], tmp_y = v[1];
+                v[0] = cp * tmp_x + sp * tmp_y;
+                v[1] = -sp * tmp_x + cp * tmp_y;
+            }
+            double s_k1z = s_k1 * std::cos(inc_ang);
+            Imdouble tmp_sup = im_exp((2.0 * hsup + 2 * Dz) * s_k1z);
+            Imdouble tmp_sub = im_exp(s_k3 * (hsub - Dz / 2.0) * std::cos(ref_ang) + s_k0 * (hsup + Dz / 2.0) * std::cos(inc_ang));
+            bool tm = od->polarization == 1;
+            Imdouble Rbase = tm ? BRS[0] : BRS[1], Tbase = tm ? BTS[0] : BTS[1];
+            double base_norm_ref = std::abs(BRS[1]), base_norm_trans = std::abs(BTS[1]);
+            if (tm) {
+                base_norm_ref = std::sqrt(std::norm(BRS[0]) + std::norm(BRS[2]));
+                base_norm_trans = std::sqrt(std::norm(BTS[0]) + std::norm(BTS[2]));
+            }
+            double TE_norm_ref = std::abs(RS[1]), TM_norm_ref = std::sqrt(std::norm(RS[0]) + std::norm(RS[2]));
+            double TE_norm_trans = std::abs(TS[1]), TM_norm_trans = std::sqrt(std::norm(TS[0]) + std::norm(TS[2]));
+            double TE_arg_ref = std::arg(RS[1] / Rbase * tmp_sup), TM_arg_ref = std::arg(RS[0] / Rbase * tmp_sup);
+            double TE_arg_trans = std::arg(TS[1] / Tbase * tmp_sub), TM_arg_trans = std::arg(TS[0] / Tbase * tmp_sub);
+            Imdouble sp4[4] = {TE_norm_ref / base_norm_ref * std::exp(TE_arg_ref * Im),
+                               TM_norm_ref / base_norm_ref * std::exp(TM_arg_ref * Im),
+                               TE_norm_trans / base_norm_trans * std::exp(TE_arg_trans * Im),
+                               TM_norm_trans / base_norm_trans * std::exp(TM_arg_trans * Im)};
+            double *o = spectra_out + size_t(l) * 10;
+            o[0] = lambda;
+            o[1] = inc_ang.degree();
+            for (int q = 0; q < 4; q++) { o[2 + 2 * q] = std::abs(sp4[q]); o[3 + 2 * q] = std::arg(sp4[q]); }
+        }
+    }
+    delete silence;
+    return 0;
+}
+
 /* Number of worker threads the reference core uses per FDTD object. */
 int aeref_threads(void) { return max_threads_number(); }
 

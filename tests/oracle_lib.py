@@ -157,3 +157,38 @@ def ref_threads():
     lib = C.CDLL(REF_PATH)
     lib.aeref_threads.restype = C.c_int
     return int(lib.aeref_threads())
+
+
+def run_ref_oblique(scene, nsteps=None, want_fields=True):
+    """The reference's oblique driver (two OBL_PHASE grids, Bloch_Wideband)
+    on an oblique Scene: dict with fields (6, nz, ny, nx) of the real grid,
+    fields_imag, series (nsteps, 18), spectra (nl', 10), dims, seconds."""
+    lib = C.CDLL(REF_PATH)
+    fn = lib.aeref_run_oblique
+    fn.argtypes = [_P(A.GridDesc), _P(C.c_uint32), _P(A.MaterialDesc), C.c_int32, _P(A.ObliqueDesc), C.c_int32,
+                   C.c_int32, _P(C.c_double), _P(C.c_double), _P(C.c_double), C.c_int32, _P(C.c_int32),
+                   _P(C.c_int32), _P(C.c_double)]
+    fn.restype = C.c_int
+    nsteps = scene.nsteps if nsteps is None else nsteps
+    nx, ny, nz = scene.total_dims()
+    ntot = nx * ny * nz
+    fields = np.zeros(12 * ntot) if want_fields else None
+    series = np.zeros(18 * max(nsteps, 1))
+    nl = scene.oblique.nl
+    spectra = np.zeros(10 * nl)
+    nl_out = C.c_int32(0)
+    dims = (C.c_int32 * 10)()
+    secs = C.c_double(0)
+    mats = (A.MaterialDesc * len(scene.materials))(*scene.materials)
+    rc = fn(C.byref(scene.grid), scene.map.ctypes.data_as(_P(C.c_uint32)), mats, len(scene.materials),
+            C.byref(scene.oblique), nsteps, 1, _dptr(fields), _dptr(series), _dptr(spectra), nl, C.byref(nl_out),
+            dims, C.byref(secs))
+    if rc != 0:
+        raise RuntimeError(f"reference oblique run failed with code {rc}")
+    out = {"dims": np.array(list(dims)), "seconds": secs.value}
+    if want_fields:
+        f = fields.reshape(2, 6, nz, ny, nx)
+        out["fields"], out["fields_imag"] = f[0], f[1]
+    out["series"] = series[:18 * nsteps].reshape(nsteps, 18)
+    out["spectra"] = spectra.reshape(nl, 10)[:nl_out.value]
+    return out

@@ -177,6 +177,7 @@ int main(void) {
   printf("%zu %zu\\n", sizeof(aefdtd_box_sensor_desc), offsetof(aefdtd_box_sensor_desc, lambda_min));
   printf("%zu %zu %zu\\n", sizeof(aefdtd_fieldmap_desc), offsetof(aefdtd_fieldmap_desc, magnetic),
          offsetof(aefdtd_fieldmap_desc, lambda));
+  printf("%zu %zu\\n", sizeof(aefdtd_oblique_desc), offsetof(aefdtd_oblique_desc, kx_in));
   return 0;
 }
 """
@@ -195,3 +196,4 @@ int main(void) {
     assert [int(x) for x in lines[2].split()] == [C.sizeof(A.BoxSensorDesc), A.BoxSensorDesc.lambda_min.offset]
     assert [int(x) for x in lines[3].split()] == [C.sizeof(A.FieldMapDesc), A.FieldMapDesc.magnetic.offset,
                                                   A.FieldMapDesc.lambda_.offset]
+    assert [int(x) for x in lines[4].split()] == [C.sizeof(A.ObliqueDesc), A.ObliqueDesc.kx_in.offset]
