@@ -108,3 +108,19 @@ def test_setup_checks():
             s.setup_oblique(sc.oblique)                 # once
         s.step(3)
         assert s.oblique_series().shape == (3, 18)
+
+
+def test_kp_sweep_runs_each_wavevector():
+    """aether_b200.oblique.sweep: one run per kp at the incident-plane angle,
+    each equal to the single run at that kx, ky."""
+    from aether_b200 import oblique
+    import math
+    sc = CF.oblique_scene(nsteps=150, disk=False)
+    kps = oblique.kp_list("fixed_lambda", nkp=2, lmin=700e-9, amin_deg=10, amax_deg=30)
+    res = oblique.sweep(sc, kps, phi_deg=30, nsteps=150)
+    assert len(res) == 2
+    for kp, r in zip(kps, res):
+        sc1 = CF.oblique_scene(nsteps=150, disk=False)
+        phi = 30 * (math.pi / 180.0)
+        sc1.oblique.kx_in, sc1.oblique.ky_in = kp * math.cos(phi), kp * math.sin(phi)
+        assert np.array_equal(fdtd.run(sc1, nsteps=150)["spectra"], r)
