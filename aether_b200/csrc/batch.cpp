@@ -117,6 +117,7 @@ struct aefdtd_batch {
     bool layout_dirty = true;
     long long l2_budget = 48LL << 20;
     int graph_steps = 16;          // steps per captured chunk (a divisor of seg_len)
+    bool h_reverse = false;        // H pass over the members in reverse order (measured slower on L2-sized subsets)
     uint64_t launches = 0;
     size_t dev_bytes = 0;
 
@@ -238,7 +239,10 @@ template <typename T, typename Tid> void aefdtd_batch::build_subset(BatchSubset 
         w.pair_mask = 0;
         for (int g = 0; g < kGroups; g++) {
             w.off[g] = (int)(all.size() / 4);
-            for (size_t li = 0; li < u.members.size(); li++) {
+            // H: members in reverse order (each member's H list is top plane
+            // first): the half-step starts on the data the E pass touched last
+            for (size_t mi = 0; mi < u.members.size(); mi++) {
+                const size_t li = (half == 1 && h_reverse) ? u.members.size() - 1 - mi : mi;
                 aefdtd_sim *s = u.members[li];
                 const WorkSplit &mw = half == 0 ? s->wsE : s->wsH;
                 w.unroll = mw.unroll;
@@ -623,7 +627,8 @@ aefdtd_status aefdtd_batch_add(aefdtd_batch *b, aefdtd_sim *s, int32_t steps) {
         s->set_device();
         s->finalize_tables();
         s->pair_mask = 0;            // the batched kernels take 32-column items
-        if (s->work_dirty || s->wsE.pair_mask || s->wsH.pair_mask) s->build_work();
+        s->h_reverse = 0;            // L2-sized subsets: forward H lists
+        s->build_work();
         if (!b->typed) {
             b->typed = true;
             b->fp64 = s->fp64;

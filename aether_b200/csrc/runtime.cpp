@@ -104,6 +104,8 @@ void aefdtd_sim::construct(const aefdtd_grid_desc *d) {
     if (const char *kc = std::getenv("AEFDTD_KCHUNK")) kchunk_override = std::max(0, atoi(kc));
     if (const char *zu = std::getenv("AEFDTD_ZUNROLL")) zunroll = atoi(zu) >= 2 ? 2 : 1;
     if (const char *pf = std::getenv("AEFDTD_PREFETCH")) prefetch_l2 = atoi(pf) != 0;
+    if (const char *hr = std::getenv("AEFDTD_HREV")) h_reverse = atoi(hr) != 0 ? 1 : 0;
+    if (const char *pe = std::getenv("AEFDTD_PERSIST")) persist = atoi(pe) != 0 ? 1 : 0;
     // two cells per thread: FP32 interior and z-CPML items, FP64 z-CPML items
     pair_mask = fp64 ? (1u << kGroupPmlZ) : (1u << kGroupInterior) | (1u << kGroupPmlZ);
     if (const char *pm = std::getenv("AEFDTD_PAIR")) pair_mask = unsigned(atoi(pm)) & 3u;
@@ -1138,12 +1140,24 @@ void aefdtd_sim::build_work() {
                     }
                 }
             }
+    // The H lists run in reverse (top plane first): each half-step starts on
+    // the planes the previous one touched last, which are still in L2. Pays
+    // when the fields are about the size of L2 (126 MB) or smaller.
+    const size_t field_bytes = size_t(6) * Nx * Ny * Nz * (fp64 ? 8 : 4);
+    if (h_reverse > 0 || (h_reverse < 0 && field_bytes <= (size_t(128) << 20)))
+        for (int g = 0; g < kGroups; g++) {
+            std::vector<int> &h = v[1][g];
+            const size_t n = h.size() / 4;
+            for (size_t a = 0, b = n ? n - 1 : 0; a < b; a++, b--)
+                for (int c = 0; c < 4; c++) std::swap(h[4 * a + c], h[4 * b + c]);
+        }
     std::vector<int> all;
     for (int half = 0; half < 2; half++) {
         WorkSplit &w = half == 0 ? wsE : wsH;
         w.unroll = zunroll;
         w.tile_y = tile_y;
         w.pair_mask = pmask;
+        w.persist = persist;
         for (int g = 0; g < kGroups; g++) {
             w.off[g] = (int)(all.size() / 4);
             w.n[g] = (int)(v[half][g].size() / 4);
