@@ -106,7 +106,6 @@ struct WorkSplit {
     int unroll;                     // z-planes per iteration of the interior kernels (1 or 2)
     int tile_y;                     // tile height: CTAs of 32 x tile_y threads (2, 4 or 8)
     unsigned pair_mask;             // bit g: group g runs the two-cells-per-thread kernels on 64-column items
-    int persist;                    // pair kernels: resident CTAs stride over the items (else one CTA per item)
 };
 // x0 flag of a 32-column item in a group of 64-column (pair) items
 constexpr int kHalfItem = 1 << 30;

@@ -105,7 +105,6 @@ void aefdtd_sim::construct(const aefdtd_grid_desc *d) {
     if (const char *zu = std::getenv("AEFDTD_ZUNROLL")) zunroll = atoi(zu) >= 2 ? 2 : 1;
     if (const char *pf = std::getenv("AEFDTD_PREFETCH")) prefetch_l2 = atoi(pf) != 0;
     if (const char *hr = std::getenv("AEFDTD_HREV")) h_reverse = atoi(hr) != 0 ? 1 : 0;
-    if (const char *pe = std::getenv("AEFDTD_PERSIST")) persist = atoi(pe) != 0 ? 1 : 0;
     // two cells per thread: FP32 interior and z-CPML items, FP64 z-CPML items
     pair_mask = fp64 ? (1u << kGroupPmlZ) : (1u << kGroupInterior) | (1u << kGroupPmlZ);
     if (const char *pm = std::getenv("AEFDTD_PAIR")) pair_mask = unsigned(atoi(pm)) & 3u;
@@ -1157,7 +1156,6 @@ void aefdtd_sim::build_work() {
         w.unroll = zunroll;
         w.tile_y = tile_y;
         w.pair_mask = pmask;
-        w.persist = persist;
         for (int g = 0; g < kGroups; g++) {
             w.off[g] = (int)(all.size() / 4);
             w.n[g] = (int)(v[half][g].size() / 4);

@@ -37,11 +37,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
-#include <algorithm>
-#include <map>
-#include <mutex>
 #include <type_traits>
-#include <utility>
 
 #include "aefdtd_dev.hpp"
 
@@ -966,14 +962,13 @@ __global__ void __launch_bounds__(kMaxTileThreads) h_boundary(const __grid_const
 
 template <typename T, typename Tid, bool PZ>
 __global__ void __launch_bounds__(kMaxTileThreads, InteriorBounds<T, 2, PZ>::kMinBlocksVec2)
-e_interior_v2(const __grid_constant__ StepArgs<T, Tid> a, const int4 *__restrict__ items, int n) {
-    // one item per CTA, or a persistent grid striding over the items
-    for (int b = blockIdx.x; b < n; b += gridDim.x) e_interior_v2_body<T, Tid, PZ>(a, a.q, items[b]);
+e_interior_v2(const __grid_constant__ StepArgs<T, Tid> a, const int4 *__restrict__ items) {
+    e_interior_v2_body<T, Tid, PZ>(a, a.q, items[blockIdx.x]);
 }
 template <typename T, typename Tid, bool PZ>
 __global__ void __launch_bounds__(kMaxTileThreads, InteriorBounds<T, 2, PZ>::kMinBlocksVec2)
-h_interior_v2(const __grid_constant__ StepArgs<T, Tid> a, const int4 *__restrict__ items, int n) {
-    for (int b = blockIdx.x; b < n; b += gridDim.x) h_interior_v2_body<T, Tid, PZ>(a, a.q, items[b]);
+h_interior_v2(const __grid_constant__ StepArgs<T, Tid> a, const int4 *__restrict__ items) {
+    h_interior_v2_body<T, Tid, PZ>(a, a.q, items[blockIdx.x]);
 }
 
 // Batched forms: item (x0, y0, k0 | k1 << 16, instance), arguments of the
@@ -1006,25 +1001,6 @@ h_boundary_batch(const StepArgs<T, Tid> *__restrict__ args, int q, const int4 *_
 }
 
 // ---- launchers: group g of a half-step's WorkSplit ------------------------
-// Grid of a pair-kernel launch over n items: one CTA per item, or (persist
-// set) the resident CTAs of every SM striding over the items.
-template <typename K> int pair_grid(K kernel, int n, dim3 blk, int persist) {
-    if (!persist) return n;
-    static std::mutex mu;
-    static std::map<std::pair<const void *, int>, int> resident;   // (kernel, CTA threads) -> CTAs on the device
-    std::lock_guard<std::mutex> lock(mu);
-    const auto key = std::make_pair(reinterpret_cast<const void *>(kernel), int(blk.x * blk.y));
-    auto it = resident.find(key);
-    if (it == resident.end()) {
-        int per_sm = 0, sms = 0, dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, key.second, 0);
-        it = resident.emplace(key, std::max(1, per_sm * sms)).first;
-    }
-    return std::min(n, it->second);
-}
-
 template <typename T, typename Tid>
 void launch_e_group_impl(const StepArgs<T, Tid> &a, const int4 *items, const WorkSplit &w, int g, cudaStream_t s) {
     const int n = w.n[g];
@@ -1033,14 +1009,12 @@ void launch_e_group_impl(const StepArgs<T, Tid> &a, const int4 *items, const Wor
     const dim3 blk(kTileX, w.tile_y);
     switch (g) {
         case kGroupInterior:
-            if (w.pair_mask & (1u << kGroupInterior))
-                e_interior_v2<T, Tid, false><<<pair_grid(e_interior_v2<T, Tid, false>, n, blk, w.persist), blk, 0, s>>>(a, p, n);
+            if (w.pair_mask & (1u << kGroupInterior)) e_interior_v2<T, Tid, false><<<n, blk, 0, s>>>(a, p);
             else if (w.unroll >= 2) e_interior<T, Tid, 2><<<n, blk, 0, s>>>(a, p);
             else e_interior<T, Tid, 1><<<n, blk, 0, s>>>(a, p);
             break;
         case kGroupPmlZ:
-            if (w.pair_mask & (1u << kGroupPmlZ))
-                e_interior_v2<T, Tid, true><<<pair_grid(e_interior_v2<T, Tid, true>, n, blk, w.persist), blk, 0, s>>>(a, p, n);
+            if (w.pair_mask & (1u << kGroupPmlZ)) e_interior_v2<T, Tid, true><<<n, blk, 0, s>>>(a, p);
             else if (w.unroll >= 2) e_interior<T, Tid, 2, true><<<n, blk, 0, s>>>(a, p);
             else e_interior<T, Tid, 1, true><<<n, blk, 0, s>>>(a, p);
             break;
@@ -1057,14 +1031,12 @@ void launch_h_group_impl(const StepArgs<T, Tid> &a, const int4 *items, const Wor
     const dim3 blk(kTileX, w.tile_y);
     switch (g) {
         case kGroupInterior:
-            if (w.pair_mask & (1u << kGroupInterior))
-                h_interior_v2<T, Tid, false><<<pair_grid(h_interior_v2<T, Tid, false>, n, blk, w.persist), blk, 0, s>>>(a, p, n);
+            if (w.pair_mask & (1u << kGroupInterior)) h_interior_v2<T, Tid, false><<<n, blk, 0, s>>>(a, p);
             else if (w.unroll >= 2) h_interior<T, Tid, 2><<<n, blk, 0, s>>>(a, p);
             else h_interior<T, Tid, 1><<<n, blk, 0, s>>>(a, p);
             break;
         case kGroupPmlZ:
-            if (w.pair_mask & (1u << kGroupPmlZ))
-                h_interior_v2<T, Tid, true><<<pair_grid(h_interior_v2<T, Tid, true>, n, blk, w.persist), blk, 0, s>>>(a, p, n);
+            if (w.pair_mask & (1u << kGroupPmlZ)) h_interior_v2<T, Tid, true><<<n, blk, 0, s>>>(a, p);
             else if (w.unroll >= 2) h_interior<T, Tid, 2, true><<<n, blk, 0, s>>>(a, p);
             else h_interior<T, Tid, 1, true><<<n, blk, 0, s>>>(a, p);
             break;

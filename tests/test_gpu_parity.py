@@ -209,19 +209,6 @@ def test_two_cells_per_thread_bit_identical(name, mask, monkeypatch):
         assert np.array_equal(fa, fb)
 
 
-@pytest.mark.parametrize("name", ["wide130", "wide192"])
-def test_persistent_pair_grid_bit_identical(name, monkeypatch):
-    """Pair kernels on a persistent grid (resident CTAs striding over the
-    items) against one CTA per item: FP64 bit-identical."""
-    sc = _wide_cell(int(name[4:]), A.FP64)
-    monkeypatch.setenv("AEFDTD_PAIR", "3")
-    a = fdtd.run(sc)
-    monkeypatch.setenv("AEFDTD_PERSIST", "1")
-    b = fdtd.run(sc)
-    assert np.array_equal(a["fields"], b["fields"])
-    assert np.array_equal(a["plane_sums"], b["plane_sums"])
-
-
 def test_two_cells_per_thread_fp32_and_cell_cover(monkeypatch):
     """FP32 pair kernels within 1e-6 relative of one cell per thread, and the
     64- and 32-column items of each half-step still cover every cell once."""
