@@ -329,7 +329,8 @@ aefdtd_status aefdtd_get_oblique_spectra(aefdtd_sim *s, double *out, int32_t nl_
         const double phi = std::atan2(ky, kx);
         const double cp = std::cos(phi), sp = std::sin(phi);
         auto series = [&](int c, int t) { return cplx(S[size_t(t) * 18 + c], S[size_t(t) * 18 + c + 1]); };
-        for (int l = 0; l < Nl && l < nl_max; l++) {
+        // wavelengths are independent; each one's sums run in the driver's order
+        parallel_for(std::min(Nl, nl_max), [&](int l) {
             const double lambda = lambda_min + (lambda_max - lambda_min) * l / (Nl - 1.0);
             const double w = 2.0 * Pi * c_light / lambda;
             const double kn = 2.0 * Pi * o.index_sup / lambda;
@@ -380,7 +381,7 @@ aefdtd_status aefdtd_get_oblique_spectra(aefdtd_sim *s, double *out, int32_t nl_
             r[4] = std::abs(tm_r); r[5] = std::arg(tm_r);
             r[6] = std::abs(te_t); r[7] = std::arg(te_t);
             r[8] = std::abs(tm_t); r[9] = std::arg(tm_t);
-        }
+        });
     });
 }
 

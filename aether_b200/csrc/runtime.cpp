@@ -7,6 +7,13 @@
 // touch the device returns AEFDTD_NO_DEVICE.
 #include "sim.hpp"
 
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
+
+
+
 // FDTD::FDTD (fdtd_core.cpp:158-285) for modes NORM and CUSTOM, with the
 // normal-incidence driver's own argument choice (normal_incidence.cpp:188-200).
 void aefdtd_sim::construct(const aefdtd_grid_desc *d) {
@@ -198,14 +205,18 @@ void aefdtd_sim::set_map(const uint32_t *m, size_t count) {
     if (mx >= 65535u) fail(AEFDTD_BAD_ARG, "at most 65535 material indices");
     Nmat = mx + 1;
     mats.assign(Nmat, HostMat());
-    // bounding boxes for every index in one pass (FDTD_Material::link_grid, mats.cpp:394-443)
+    // bounding boxes for every index in one pass (FDTD_Material::link_grid,
+    // mats.cpp:394-443), one update per run of equal indices along x
     for (int k = 0; k < Nz; k++)
         for (int j = 0; j < Ny; j++) {
             const uint32_t *row = &M(0, j, k);
-            for (int i = 0; i < Nx; i++) {
-                HostMat &h = mats[row[i]];
-                if (h.x2 < h.x1) { h.x1 = h.x2 = i; h.y1 = h.y2 = j; h.z1 = h.z2 = k; continue; }
-                h.x1 = std::min(h.x1, i); h.x2 = std::max(h.x2, i);
+            for (int i = 0; i < Nx;) {
+                const uint32_t v = row[i];
+                const int i0 = i;
+                while (i < Nx && row[i] == v) i++;
+                HostMat &h = mats[v];
+                if (h.x2 < h.x1) { h.x1 = i0; h.x2 = i - 1; h.y1 = h.y2 = j; h.z1 = h.z2 = k; continue; }
+                h.x1 = std::min(h.x1, i0); h.x2 = std::max(h.x2, i - 1);
                 h.y1 = std::min(h.y1, j); h.y2 = std::max(h.y2, j);
                 h.z1 = std::min(h.z1, k); h.z2 = std::max(h.z2, k);
             }
@@ -897,7 +908,9 @@ void aefdtd_sim::run_steps(int n) {
                 anyp = true;
                 canon &= s->pend_tbl == other && s->pend_n == dft_k && s->pend_half == (s->half ^ 1);
             }
-        const bool full = (L == seg_len) && empty && !timing && use_graphs;
+        // with DFT sensors only the first segment after a drain has no pending
+        // block: it runs as direct launches instead of a graph used once
+        const bool full = (L == seg_len) && empty && !timing && use_graphs && !(sensors.size() && !anyp);
         if (full && anyp && !canon) {
             for (auto *s : sensors) launch_pending<T>(*s, stream);
             anyp = false;
@@ -971,10 +984,57 @@ void aefdtd_sim::run_steps(int n) {
 
 void aefdtd_sim::drop_graphs() {
     for (auto &g : graph_exec)
-        if (g.second) cudaGraphExecDestroy(g.second);
+        if (g.second) reap_graph(g.second, device);
     graph_exec.clear();
     graphs_dirty = false;
 }
+
+namespace aefdtd {
+namespace {
+// The reaper: one detached thread and a queue. At process exit (an atexit
+// handler registered after the CUDA runtime's, so it runs first) it stops
+// between two destroys and leaves the rest to the driver's teardown.
+struct Reaper {
+    std::mutex mu;
+    std::condition_variable cv;
+    std::deque<std::pair<cudaGraphExec_t, int>> q;
+    bool exiting = false;
+};
+Reaper &reaper() {
+    static Reaper *r = [] {
+        auto *x = new Reaper();   // never deleted: outlives static destruction
+        std::atexit([] {
+            Reaper &R = reaper();
+            std::lock_guard<std::mutex> lock(R.mu);
+            R.exiting = true;
+            R.q.clear();
+            R.cv.notify_all();
+        });
+        std::thread([x] {
+            std::unique_lock<std::mutex> lock(x->mu);
+            for (;;) {
+                x->cv.wait(lock, [x] { return x->exiting || !x->q.empty(); });
+                if (x->exiting) return;
+                const auto item = x->q.front();
+                x->q.pop_front();
+                cudaSetDevice(item.second);
+                cudaGraphExecDestroy(item.first);
+            }
+        }).detach();
+        return x;
+    }();
+    return *r;
+}
+}  // namespace
+
+void reap_graph(cudaGraphExec_t g, int device) {
+    Reaper &R = reaper();
+    std::lock_guard<std::mutex> lock(R.mu);
+    if (R.exiting) return;
+    R.q.emplace_back(g, device);
+    R.cv.notify_one();
+}
+}  // namespace aefdtd
 
 void aefdtd_sim::accumulate_timing(int L) {
     AE_CUDA(cudaEventSynchronize(tev[4 * L - 1]));
@@ -1543,7 +1603,8 @@ aefdtd_status aefdtd_get_normal_spectra(aefdtd_sim *s, double *out, int32_t nl) 
         const cplx Im(0, 1);
         const double *SS[12];
         for (int c = 0; c < 12; c++) SS[c] = S.data() + size_t(c) * Ntot;
-        for (int l = 0; l < nl; l++) {
+        // wavelengths are independent; each one's sums run in the driver's order
+        auto one = [&](int l) {
             double lam = s->nd.lambda_min + (s->nd.lambda_max - s->nd.lambda_min) * l / (nl - 1.0);
             double w = 2.0 * Pi * c_light / lam;
             cplx r1x = 0, r1y = 0, r1z = 0, r2x = 0, r2y = 0, r2z = 0, t1x = 0, t1y = 0, t1z = 0, t2x = 0, t2y = 0, t2z = 0;
@@ -1573,7 +1634,8 @@ aefdtd_status aefdtd_get_normal_spectra(aefdtd_sim *s, double *out, int32_t nl) 
             o[6] = std::abs(refy); o[7] = std::arg(refy); o[8] = std::norm(refy);
             o[9] = std::abs(transx); o[10] = std::arg(transx); o[11] = std::norm(transx) * s->index_sub / s->index_sup;
             o[12] = std::abs(transy); o[13] = std::arg(transy); o[14] = std::norm(transy) * s->index_sub / s->index_sup;
-        }
+        };
+        parallel_for(nl, one);
     });
 }
 

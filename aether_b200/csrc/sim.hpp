@@ -13,6 +13,7 @@
 #include <string>
 #include <array>
 #include <map>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -25,6 +26,28 @@ constexpr int kTileXHost = 32, kTileYHost = 4;   // kTileX, kTileY of yee.cuh
 }
 
 namespace aefdtd {
+
+// f(0) .. f(n-1) on up to hardware_concurrency host threads (static blocks);
+// f must only write state of its own index.
+template <typename F> void parallel_for(int n, F &&f) {
+    const int nt = std::max(1, std::min<int>(n, std::min(32u, std::max(1u, std::thread::hardware_concurrency()))));
+    if (nt <= 1 || n < 8) {
+        for (int i = 0; i < n; i++) f(i);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (int w = 0; w < nt; w++)
+        th.emplace_back([&, w] {
+            for (int i = w * n / nt; i < (w + 1) * n / nt; i++) f(i);
+        });
+    for (auto &x : th) x.join();
+}
+
+// Hands a graph executable to a background thread that destroys it: with a
+// few thousand nodes each destroy takes ~20 ms, which would otherwise land in
+// aefdtd_destroy and in work-list rebuilds. In-flight graphs are freed by the
+// driver on completion, as for a direct destroy.
+void reap_graph(cudaGraphExec_t g, int device);
 
 cudaError_t launch_voxelize(int nx, int ny, int nz, double dx, double dy, double dz, const aefdtd_structure_op *ops,
                             int nops, int def, const int per[3], const double l[3], uint32_t *d_out, cudaStream_t s);
@@ -338,7 +361,7 @@ inline aefdtd_sim::~aefdtd_sim() {
     cc_hist.release(t);
     err.release(t);
     tables.release(t);
-    for (auto &gx : graph_exec) if (gx.second) cudaGraphExecDestroy(gx.second);
+    for (auto &gx : graph_exec) if (gx.second) reap_graph(gx.second, device);
     items.release(t);
     fm_tbl.release(t);
     if (obl) {
@@ -355,6 +378,7 @@ inline aefdtd_sim::~aefdtd_sim() {
         delete s;
     }
     for (auto &e : tev) if (e) cudaEventDestroy(e);
+    for (auto &e : tge) if (e) cudaEventDestroy(e);
     for (auto &e : ev_join) if (e) cudaEventDestroy(e);
     if (ev_fork) cudaEventDestroy(ev_fork);
     for (auto &x : side) if (x) cudaStreamDestroy(x);
