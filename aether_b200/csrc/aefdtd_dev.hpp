@@ -84,7 +84,7 @@ template <typename T, typename Tid> struct StepArgs {
     const StepScalars *sc;
     int q;
     int kchunk;                     // z planes per thread
-    int prefetch;                   // interior kernels: prefetch the item's planes into L2 at start
+    int prefetch;                   // prefetch the item's planes into L2 at start: bit 0 interior, bit 1 CPML kernels
     int *err;                       // device error flag (bounded waits)
     // oblique driver: two grids hold the real and imaginary parts of a
     // Bloch-periodic field; their wrap cells run in the general kernels
@@ -99,7 +99,7 @@ template <typename T, typename Tid> struct StepArgs {
 
 // Item groups of one half-step: a device array of int4 items (x0, y0, k0,
 // k1) sorted by group; group g is items [off[g], off[g] + n[g]).
-enum { kGroupInterior = 0, kGroupPmlZ = 1, kGroupDisp = 2, kGroupAll = 3, kGroups = 4 };
+enum { kGroupInterior = 0, kGroupPmlZ = 1, kGroupDisp = 2, kGroupAll = 3, kGroupPmlXY = 4, kGroups = 5 };
 struct WorkSplit {
     int off[kGroups];
     int n[kGroups];

@@ -16,7 +16,7 @@
 //    resident cell at a time beats two or more sharing L2, 45.8 vs 42.0
 //    Gcell/s, and beats merged 5-cell subsets, 37.3 Gcell/s).
 //  * Merged launches. Per step, each work-item group of a subset (interior,
-//    z-CPML, dispersive, general) is ONE launch over the items of all its
+//    z-CPML, dispersive, general, x/y-CPML) is ONE launch over the items of all its
 //    members: items carry the member index and the kernels read that member's
 //    arguments from a device array. Boundary groups run on side streams beside
 //    the interior group; the plane sums of all normal-mode members are one

@@ -110,7 +110,7 @@ void aefdtd_sim::construct(const aefdtd_grid_desc *d) {
     mats.assign(1, HostMat());
     if (const char *kc = std::getenv("AEFDTD_KCHUNK")) kchunk_override = std::max(0, atoi(kc));
     if (const char *zu = std::getenv("AEFDTD_ZUNROLL")) zunroll = atoi(zu) >= 2 ? 2 : 1;
-    if (const char *pf = std::getenv("AEFDTD_PREFETCH")) prefetch_l2 = atoi(pf) != 0;
+    if (const char *pf = std::getenv("AEFDTD_PREFETCH")) prefetch_l2 = std::clamp(atoi(pf), 0, 3);
     if (const char *hr = std::getenv("AEFDTD_HREV")) h_reverse = atoi(hr) != 0 ? 1 : 0;
     // two cells per thread: FP32 interior and z-CPML items, FP64 z-CPML items
     pair_mask = fp64 ? (1u << kGroupPmlZ) : (1u << kGroupInterior) | (1u << kGroupPmlZ);
@@ -590,7 +590,7 @@ void aefdtd_sim::make_step_args(StepArgs<T, Tid> &ea, StepArgs<T, Tid> &ha, cons
     fill_args(ea, true, grid);
     fill_args(ha, false, grid);
     ea.kchunk = ha.kchunk = kchunk;
-    ea.prefetch = ha.prefetch = prefetch_l2 ? 1 : 0;
+    ea.prefetch = ha.prefetch = prefetch_l2;
     ea.sc = ha.sc = tbl;
     if (normal) ea.kinj = ha.kinj = zs_e - 1;
     ea.nsrc = 0;
@@ -1131,6 +1131,7 @@ void aefdtd_sim::build_work() {
         if (f == 0) return (int)kGroupInterior;
         if (f == kPZ) return (int)kGroupPmlZ;
         if (f == kDISP) return (int)kGroupDisp;
+        if (f == kPXY || f == (kPXY | kPZ)) return (int)kGroupPmlXY;
         return (int)kGroupAll;
     };
     auto group_h = [&](unsigned f) {
@@ -1138,6 +1139,7 @@ void aefdtd_sim::build_work() {
         f &= (kPXY | kPZ | kMISC);
         if (f == 0) return (int)kGroupInterior;
         if (f == kPZ) return (int)kGroupPmlZ;
+        if (f == kPXY || f == (kPXY | kPZ)) return (int)kGroupPmlXY;
         return (int)kGroupAll;
     };
     // items: within each tile (or pair of tiles) and z-chunk, runs of planes

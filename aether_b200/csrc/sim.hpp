@@ -331,7 +331,7 @@ struct aefdtd_sim {
     int zunroll = 2;
     int tile_y = kTileYHost;        // tile height of the work items (2, 4 or 8)
     unsigned pair_mask = 0;         // groups run two cells per thread (WorkSplit::pair_mask; even Nx only)
-    bool prefetch_l2 = true;        // interior kernels prefetch their item's planes into L2
+    int prefetch_l2 = 3;            // L2 prefetch of each item's planes: bit 0 interior kernels, bit 1 CPML kernels
     int h_reverse = -1;             // H work lists top plane first (L2 reuse between half-steps); -1: by size
     // completion sensor, energy mode (CompletionSensor(coeff), s_completion.cpp)
     double cc_coeff = 0;            // > 0: enabled

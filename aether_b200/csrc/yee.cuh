@@ -26,6 +26,8 @@
 //     each thread keeps U planes of reads in flight;
 //   * z-CPML items: the same loop with the psi_z recursions and z PEC planes
 //     (PZ instantiation of the interior kernels);
+//   * x/y-CPML items (with or without z-CPML): the boundary kernel for
+//     kFPmlXY | kFPmlZ (about 50 registers instead of 120);
 //   * dispersive items and the rest (every phase): the boundary kernel
 //     instantiated for feature sets kFDisp and kFAll.
 // All groups of a half-step together cover each cell exactly once.
@@ -99,7 +101,7 @@ __device__ __forceinline__ void e_interior_body(const StepArgs<T, Tid> &a, int q
     const int kmi = (it.z == 0) ? a.Nz - 1 : it.z - 1;
     T hx_km = __ldg(Hx + col + kmi * NxNy);
     T hy_km = __ldg(Hy + col + kmi * NxNy);
-    if (a.prefetch) {
+    if (a.prefetch & 1) {
         // every plane of the item into L2 up front: only the first iteration
         // waits on DRAM; the y-1 row lines are fetched by row 0 only
         for (int k = it.z; k < it.w; ++k) {
@@ -204,7 +206,7 @@ __device__ __forceinline__ void h_interior_body(const StepArgs<T, Tid> &a, int q
     const T ay = a.dtdmy * __ldg(a.iky + j);
     T ex = __ldg(Ex + col + it.z * NxNy);
     T ey = __ldg(Ey + col + it.z * NxNy);
-    if (a.prefetch) {
+    if (a.prefetch & 1) {
         // every plane of the item (and the E plane above it) into L2 up front;
         // the y+1 row lines are fetched by the last row only
         for (int k = it.z; k < it.w; ++k) {
@@ -330,6 +332,31 @@ __device__ __forceinline__ void e_boundary_body(const StepArgs<T, Tid> &a, int q
         if (ye) { byj = __ldg(a.by + j); cyj = __ldg(a.cy + j); }
     }
 
+    if constexpr (F == (kFPmlXY | kFPmlZ)) {
+        // CPML items: every plane of the item (fields, ids, psi slabs) into L2 up front
+        if (a.prefetch & 2)
+            for (int k = k0; k < k1; ++k) {
+                const long long o = (long long)k * NxNy;
+                prefetch_l2(Hx + col + o); prefetch_l2(Hy + col + o); prefetch_l2(Hz + col + o);
+                prefetch_l2(Hz + colx + o); prefetch_l2(Hy + colx + o);
+                if (threadIdx.y == 0) { prefetch_l2(Hz + coly + o); prefetch_l2(Hx + coly + o); }
+                prefetch_l2(Ex + col + o); prefetch_l2(Ey + col + o); prefetch_l2(Ez + col + o);
+                prefetch_l2(a.mat + colm + (long long)k * mNxNy);
+                if (xe) {
+                    const long long px = xn + (long long)j * nxs + (long long)k * nxs * a.Ny;
+                    prefetch_l2(a.psi_x0 + px); prefetch_l2(a.psi_x1 + px);
+                }
+                if (ye) {
+                    const long long py = i + (long long)yn * a.Nx + (long long)k * a.Nx * nys;
+                    prefetch_l2(a.psi_y0 + py); prefetch_l2(a.psi_y1 + py);
+                }
+                if (a.pz && ((k >= 1 && k < a.pml_zm) || (k >= a.Nz - a.pml_zp + 1))) {
+                    const int zn = (k < a.pml_zm) ? k : k - (a.Nz - a.pml_zp) + a.pml_zm;
+                    prefetch_l2(a.psi_z0 + col + (long long)zn * NxNy);
+                    prefetch_l2(a.psi_z1 + col + (long long)zn * NxNy);
+                }
+            }
+    }
     const int kmi = (k0 == 0) ? a.Nz - 1 : k0 - 1;
     T hx_km = __ldg(Hx + col + kmi * NxNy);
     T hy_km = __ldg(Hy + col + kmi * NxNy);
@@ -555,6 +582,30 @@ __device__ __forceinline__ void h_boundary_body(const StepArgs<T, Tid> &a, int q
         if (yh) { byj = __ldg(a.by + j); cyj = __ldg(a.cy + j); }
     }
 
+    if constexpr (F == (kFPmlXY | kFPmlZ)) {
+        if (a.prefetch & 2)
+            for (int k = k0; k < k1; ++k) {
+                const int kp = (k == a.Nz - 1) ? 0 : k + 1;
+                const long long o = (long long)k * NxNy, op = (long long)kp * NxNy;
+                prefetch_l2(Ex + col + op); prefetch_l2(Ey + col + op); prefetch_l2(Ez + col + o);
+                prefetch_l2(Ez + colx + o); prefetch_l2(Ey + colx + o);
+                if (threadIdx.y == blockDim.y - 1) { prefetch_l2(Ez + coly + o); prefetch_l2(Ex + coly + o); }
+                prefetch_l2(Hx + col + o); prefetch_l2(Hy + col + o); prefetch_l2(Hz + col + o);
+                if (xh) {
+                    const long long px = xn + (long long)j * nxs + (long long)k * nxs * a.Ny;
+                    prefetch_l2(a.psi_x0 + px); prefetch_l2(a.psi_x1 + px);
+                }
+                if (yh) {
+                    const long long py = i + (long long)yn * a.Nx + (long long)k * a.Nx * nys;
+                    prefetch_l2(a.psi_y0 + py); prefetch_l2(a.psi_y1 + py);
+                }
+                if (a.pz && ((k < a.pml_zm) || (k >= a.Nz - a.pml_zp && k < a.Nz - 1))) {
+                    const int zn = (k < a.pml_zm) ? k : k - (a.Nz - a.pml_zp) + a.pml_zm;
+                    prefetch_l2(a.psi_z0 + col + (long long)zn * NxNy);
+                    prefetch_l2(a.psi_z1 + col + (long long)zn * NxNy);
+                }
+            }
+    }
     T ex = __ldg(Ex + col + k0 * NxNy);
     T ey = __ldg(Ey + col + k0 * NxNy);
 
@@ -732,7 +783,7 @@ __device__ __forceinline__ void e_interior_v2_body(const StepArgs<T, Tid> &a, in
     const int kmi = (it.z == 0) ? a.Nz - 1 : it.z - 1;
     T2 hx_km = ldg2<T2>(Hx + col + kmi * NxNy);
     T2 hy_km = ldg2<T2>(Hy + col + kmi * NxNy);
-    if (a.prefetch) {
+    if (a.prefetch & 1) {
         for (int k = it.z; k < it.w; ++k) {
             const long long o = (long long)k * NxNy;
             prefetch_l2(Hx + col + o); prefetch_l2(Hy + col + o); prefetch_l2(Hz + col + o);
@@ -847,7 +898,7 @@ __device__ __forceinline__ void h_interior_v2_body(const StepArgs<T, Tid> &a, in
     const T ay = a.dtdmy * __ldg(a.iky + j);
     T2 ex = ldg2<T2>(Ex + col + it.z * NxNy);
     T2 ey = ldg2<T2>(Ey + col + it.z * NxNy);
-    if (a.prefetch) {
+    if (a.prefetch & 1) {
         for (int k = it.z; k < it.w; ++k) {
             const int kp = (k == a.Nz - 1) ? 0 : k + 1;
             const long long o = (long long)k * NxNy, op = (long long)kp * NxNy;
@@ -1019,6 +1070,7 @@ void launch_e_group_impl(const StepArgs<T, Tid> &a, const int4 *items, const Wor
             else e_interior<T, Tid, 1, true><<<n, blk, 0, s>>>(a, p);
             break;
         case kGroupDisp: e_boundary<T, Tid, kFDisp><<<n, blk, 0, s>>>(a, p); break;
+        case kGroupPmlXY: e_boundary<T, Tid, kFPmlXY | kFPmlZ><<<n, blk, 0, s>>>(a, p); break;
         default: e_boundary<T, Tid, kFAll><<<n, blk, 0, s>>>(a, p); break;
     }
 }
@@ -1040,6 +1092,7 @@ void launch_h_group_impl(const StepArgs<T, Tid> &a, const int4 *items, const Wor
             else if (w.unroll >= 2) h_interior<T, Tid, 2, true><<<n, blk, 0, s>>>(a, p);
             else h_interior<T, Tid, 1, true><<<n, blk, 0, s>>>(a, p);
             break;
+        case kGroupPmlXY: h_boundary<T, Tid, kFPmlXY | kFPmlZ><<<n, blk, 0, s>>>(a, p); break;
         default: h_boundary<T, Tid, kFAll><<<n, blk, 0, s>>>(a, p); break;
     }
 }

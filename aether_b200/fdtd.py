@@ -150,12 +150,13 @@ class Simulation:
 
     def group_timings(self):
         """Mode-2 timing: {(half, group): (ms per step, cells)}; half 'E'/'H',
-        group 'interior'/'pml_z'/'dispersive'/'general'."""
-        ms = (C.c_double * 8)()
-        cells = (C.c_int64 * 8)()
-        self._c(self._lib.aefdtd_get_group_timings(self._h, ms, cells, 8))
-        names = ["interior", "pml_z", "dispersive", "general"]
-        return {(h, names[g]): (ms[i * 4 + g], cells[i * 4 + g]) for i, h in enumerate("EH") for g in range(4)}
+        group 'interior'/'pml_z'/'dispersive'/'general'/'pml_xy'."""
+        names = ["interior", "pml_z", "dispersive", "general", "pml_xy"]
+        G = len(names)
+        ms = (C.c_double * (2 * G))()
+        cells = (C.c_int64 * (2 * G))()
+        self._c(self._lib.aefdtd_get_group_timings(self._h, ms, cells, 2 * G))
+        return {(h, names[g]): (ms[i * G + g], cells[i * G + g]) for i, h in enumerate("EH") for g in range(G)}
 
     def enable_timing(self, on=True, mode=1):
         """mode 1: per phase; mode 2: per work-item group (groups in order)."""

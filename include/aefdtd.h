@@ -357,8 +357,9 @@ aefdtd_status aefdtd_get_timings(aefdtd_sim *sim, double *e_ms, double *h_ms, do
  * after another on the handle's stream, each between two events. */
 aefdtd_status aefdtd_enable_timing(aefdtd_sim *sim, int32_t enable);
 /* After a timed aefdtd_step in mode 2: mean milliseconds per step of each
- * group (index half*4 + group; half 0 = E, 1 = H; groups interior, z-CPML,
- * dispersive, general) and the cells it updates per half-step. n must be 8. */
+ * group (index half*5 + group; half 0 = E, 1 = H; groups interior, z-CPML,
+ * dispersive, general, x/y-CPML) and the cells it updates per half-step.
+ * n must be 10. */
 aefdtd_status aefdtd_get_group_timings(aefdtd_sim *sim, double *ms, int64_t *cells, int32_t n);
 /* The handle's CUDA stream (a cudaStream_t), for callers that order their
  * own device work or timing events with the simulation's kernels. */
