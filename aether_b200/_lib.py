@@ -51,6 +51,8 @@ _SIGS = {
     "aefdtd_get_box_flux": (C.c_int, [C.c_void_p, C.c_int32, _P(C.c_double), C.c_int32]),
     "aefdtd_add_fieldmap": (C.c_int, [C.c_void_p, _P(A.FieldMapDesc), _P(C.c_int32)]),
     "aefdtd_setup_oblique": (C.c_int, [C.c_void_p, _P(A.ObliqueDesc)]),
+    "aefdtd_set_completion_ft": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int32, C.c_char_p,
+                                           C.c_uint32, C.c_int32]),
     "aefdtd_get_oblique_spectra": (C.c_int, [C.c_void_p, _P(C.c_double), C.c_int32, _P(C.c_int32)]),
     "aefdtd_get_oblique_series": (C.c_int, [C.c_void_p, _P(C.c_double), C.c_size_t]),
     "aefdtd_get_fieldmap_shape": (C.c_int, [C.c_void_p, C.c_int32, _P(C.c_int32)]),

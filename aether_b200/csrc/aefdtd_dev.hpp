@@ -206,6 +206,22 @@ struct OblIncArgs {
     double *out;             // [t0 + n][14]
 };
 
+// Completion sensor, FT mode (CompletionSensor::deep_feed, s_completion.cpp:
+// 137-160): per probe, acc += local E x e^{i w step Dt}, then the running sums
+// into slot step % n_avg of the ring [Ex re, Ey re, Ez re, Ex im, Ey im, Ez im][np][n_avg].
+template <typename T> struct CcFtArgs {
+    int Nx, Ny, Nz;
+    long long NxNy;
+    const T *Ex, *Ey, *Ez;
+    int np, n_avg, step0;
+    const int *pts;                 // [np][3] probe cells
+    const double2 *coef;            // this segment's phases [q][np]
+    const StepScalars *sc;
+    int q;
+    double2 *acc;                   // [np][3]
+    double *ring;
+};
+
 struct PhasorArgs {
     int nk, nl, Nt, Ntap;
     const int *step_ptr;     // step of buffer slot 0 = (*step_ptr if set) + step_add

@@ -34,6 +34,9 @@ int launch_sensor_step(const SensorStepArgs<double> &a, cudaStream_t s);
 int launch_sensor_step(const SensorStepArgs<float> &a, cudaStream_t s);
 void launch_plane_reduce(const double *partial, int nbp, const StepScalars *sc, double *out, int steps,
                          cudaStream_t s);
+// completion sensor, FT mode: step a.q of every probe
+void launch_completion_ft(const CcFtArgs<double> &a, cudaStream_t s);
+void launch_completion_ft(const CcFtArgs<float> &a, cudaStream_t s);
 // single-wavelength field sensors: one part (a.part) of step a.q; returns the launches issued
 int launch_fieldmap_step(const MapStepArgs<double> &a, cudaStream_t s);
 int launch_fieldmap_step(const MapStepArgs<float> &a, cudaStream_t s);

@@ -10,6 +10,7 @@
 #include <condition_variable>
 #include <deque>
 #include <mutex>
+#include <random>
 #include <thread>
 
 
@@ -728,8 +729,22 @@ void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
         // completion energy of this step reads E only: with part 0, beside H
         auto energy = [&](cudaStream_t st) {
             if (!cc) return;
-            launch_energy_partial(F[0].as<T>(), F[1].as<T>(), F[2].as<T>(), (long long)Nx * Ny * Nz, cc_nb,
-                                  cc_partial.as<double>() + size_t(q) * cc_nb, st);
+            if (ccft) {
+                // FT mode: the probes' running transforms (CompletionSensor::deep_feed)
+                CcFtArgs<T> fa{};
+                fa.Nx = Nx; fa.Ny = Ny; fa.Nz = Nz; fa.NxNy = (long long)Nx * Ny;
+                fa.Ex = F[0].as<T>(); fa.Ey = F[1].as<T>(); fa.Ez = F[2].as<T>();
+                fa.np = ccft->np; fa.n_avg = ccft->n_avg; fa.step0 = ccft->step0;
+                fa.pts = ccft->dpts.as<int>();
+                fa.coef = ccft->ctab.as<double2>() + size_t(tbl - tables.as<StepScalars>()) * ccft->np;
+                fa.sc = tbl; fa.q = q;
+                fa.acc = ccft->acc.as<double2>();
+                fa.ring = ccft->ring.as<double>();
+                launch_completion_ft(fa, st);
+            } else {
+                launch_energy_partial(F[0].as<T>(), F[1].as<T>(), F[2].as<T>(), (long long)Nx * Ny * Nz, cc_nb,
+                                      cc_partial.as<double>() + size_t(q) * cc_nb, st);
+            }
             launches++;
         };
         auto maps = [&](int part, cudaStream_t st) {
@@ -795,7 +810,7 @@ void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
         launch_plane_reduce(psum_partial.as<double>(), sa.nbp, tbl, psums.as<double>(), L, stream);
         launches++;
     }
-    if (cc_coeff > 0) {
+    if (cc_coeff > 0 && !ccft) {
         launch_energy_reduce(cc_partial.as<double>(), cc_nb, tbl, cc_hist.as<double>(), L, stream);
         launches++;
     }
@@ -809,7 +824,51 @@ void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
 // 121-130) after check step t = tstep - 1: the energies since the last check
 // update the running maximum; the run completes when the last energy is below
 // coeff times the maximum, once tstep >= 2 max(Nx, Ny, Nz).
+// CompletionSensor::completion_check in FT mode (s_completion.cpp:45-121),
+// FP64 on the host over the device ring, in the reference's order (its six
+// averages carry over from one probe to the next, as there).
+bool aefdtd_sim::ft_check() {
+    CompletionFT &c = *ccft;
+    const int step = tstep - c.step0;   // the sensor's step after this step's feed
+    if (step < 2 * std::max(Nx, std::max(Ny, Nz))) return false;
+    const size_t n = size_t(6) * c.np * c.n_avg;
+    c.ring_host.resize(n);
+    AE_CUDA(cudaMemcpyAsync(c.ring_host.data(), c.ring.p, n * 8, cudaMemcpyDeviceToHost, stream));
+    AE_CUDA(cudaStreamSynchronize(stream));
+    auto R = [&](int comp, int i, int j) { return c.ring_host[(size_t(comp) * c.np + i) * c.n_avg + j]; };
+    double av[6] = {0, 0, 0, 0, 0, 0};
+    int N_ok = 0;
+    for (int i = 0; i < c.np; i++) {
+        for (int j = 0; j < c.n_avg; j++)
+            for (int d = 0; d < 6; d++) av[d] += R(d, i, j);
+        for (int d = 0; d < 6; d++) av[d] = std::abs(av[d] / (c.n_avg + 0.0));
+        // var_max(Ex_r, Ey_r, Ez_r, Ex_i, Ey_i, Ez_i): max(a, max(b, ...))
+        double avg_max = av[5];
+        for (int d = 4; d >= 0; d--) avg_max = std::max(av[d], avg_max);
+        int g = 0;
+        for (int d = 0; d < 6; d++)
+            if (avg_max == av[d]) { g = d; break; }
+        double t_min = R(g, i, 0), t_max = R(g, i, 0);
+        for (int k = 0; k < c.n_avg; k++) {
+            t_min = std::min(t_min, R(g, i, k));
+            t_max = std::max(t_max, R(g, i, k));
+        }
+        const double span = std::abs(t_max - t_min);
+        if (span <= avg_max * cc_coeff) N_ok++;
+    }
+    const double ok_rat = N_ok / (c.np + 0.0);
+    c.open_ratio = 1.0 - ok_rat;
+    return ok_rat >= 0.9;
+}
+
 void aefdtd_sim::completion_check() {
+    if (ccft) {
+        if (ft_check()) {
+            cc_done = true;
+            cc_stop = tstep - 1;
+        }
+        return;
+    }
     const int n = tstep - cc_read;
     if (n > 0) {
         std::vector<double> e(n);
@@ -852,7 +911,7 @@ void aefdtd_sim::run_steps(int n) {
     }
     if (cc_coeff > 0) {
         if (cc_done) return;   // completed: the driver's loop has ended
-        if (tstep + n > cc_cap) {
+        if (!ccft && tstep + n > cc_cap) {
             const int cap = std::max(tstep + n, std::max(2 * cc_cap, std::max(Nt, 1024)));
             DBuf nb;
             nb.alloc(size_t(cap) * 8, dev_bytes);
@@ -864,7 +923,7 @@ void aefdtd_sim::run_steps(int n) {
             graphs_dirty = true;
             drop_graphs();
         }
-        if (!cc_partial.p) {
+        if (!ccft && !cc_partial.p) {
             cc_nb = std::max(1, std::min(2 * 148, (int)(((long long)Nx * Ny * Nz + 4095) / 4096)));
             cc_partial.alloc(size_t(seg_len) * cc_nb * 8, dev_bytes);
         }
@@ -917,6 +976,22 @@ void aefdtd_sim::run_steps(int n) {
         }
         for (int q = 0; q < L; q++) fill_scalars(tstep + q, q, host[q]);
         AE_CUDA(cudaMemcpyAsync(tbl, host.data(), sizeof(StepScalars) * L, cudaMemcpyHostToDevice, stream));
+        if (ccft && cc_coeff > 0) {
+            // CompletionSensor::deep_feed's phases e^{i w step Dt} (s_completion.cpp:149)
+            CompletionFT &c = *ccft;
+            c.rows.resize(size_t(L) * c.np * 2);
+            const cplx Im(0, 1);
+            for (int q = 0; q < L; q++) {
+                const int step = tstep + q - c.step0;
+                for (int p = 0; p < c.np; p++) {
+                    const cplx coeff = std::exp(c.w[p] * step * Dt * Im);
+                    c.rows[(size_t(q) * c.np + p) * 2] = coeff.real();
+                    c.rows[(size_t(q) * c.np + p) * 2 + 1] = coeff.imag();
+                }
+            }
+            AE_CUDA(cudaMemcpyAsync(c.ctab.as<double>() + size_t(slot) * seg_len * c.np * 2, c.rows.data(),
+                                    c.rows.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+        }
         if (!fmaps.empty()) {
             map_rows.assign(size_t(L) * kMaxMaps * 4, 0.0);
             fill_map_phases(tstep, L, map_rows.data());
@@ -1285,6 +1360,11 @@ void aefdtd_sim::zero_state() {
         s->step = 0; s->nbuf = 0; s->half = 0; s->pending = false;
     }
     for (auto &o : oscs) o.step = 0;
+    if (ccft) {
+        AE_CUDA(cudaMemsetAsync(ccft->acc.p, 0, ccft->acc.n, stream));
+        AE_CUDA(cudaMemsetAsync(ccft->ring.p, 0, ccft->ring.n, stream));
+        ccft->step0 = 0;
+    }
     for (auto *m : fmaps) {
         if (m->acc.p) AE_CUDA(cudaMemsetAsync(m->acc.p, 0, m->acc.n, stream));
         m->step0 = 0;
@@ -1897,6 +1977,13 @@ aefdtd_status aefdtd_set_completion(aefdtd_sim *s, double coeff, int32_t check_e
     return guarded(s, [&] {
         if (check_every < 0) fail(AEFDTD_BAD_ARG, "negative check interval");
         if (s->batch) fail(AEFDTD_NOT_READY, "batch members run without a completion sensor");
+        if (s->ccft) {
+            size_t t = 0;
+            s->ccft->dpts.release(t); s->ccft->acc.release(t); s->ccft->ring.release(t); s->ccft->ctab.release(t);
+            s->dev_bytes -= std::min(s->dev_bytes, t);
+            delete s->ccft;
+            s->ccft = nullptr;
+        }
         s->cc_coeff = coeff > 0 ? coeff : 0;
         s->cc_step = check_every > 0 ? check_every : 500;
         s->cc_done = false;
@@ -1907,11 +1994,95 @@ aefdtd_status aefdtd_set_completion(aefdtd_sim *s, double coeff, int32_t check_e
     });
 }
 
+// CompletionSensor(lmin, lmax, coeff, Np, layout) and its initialize()
+// (s_completion.cpp:26-37, 246-361): probe cells on the named faces and their
+// wavelengths, drawn with randp (mathUT.cpp:65-68) from a std::mt19937.
+aefdtd_status aefdtd_set_completion_ft(aefdtd_sim *s, double lambda_min, double lambda_max, double coeff,
+                                       int32_t n_points, const char *layout, uint32_t seed, int32_t check_every) {
+    if (!s) return AEFDTD_BAD_ARG;
+    aefdtd_status st = aefdtd_set_completion(s, coeff, check_every);   // clears either mode
+    if (st != AEFDTD_OK || !(coeff > 0)) return st;
+    return guarded(s, [&] {
+        if (n_points < 1) fail(AEFDTD_BAD_ARG, "n_points must be positive");
+        if (!(lambda_min > 0) || !(lambda_max > 0)) fail(AEFDTD_BAD_ARG, "bad probe wavelengths");
+        s->set_device();
+        auto *c = new CompletionFT();
+        c->lmin = lambda_min; c->lmax = lambda_max; c->np = n_points;
+        std::string lay = layout ? layout : "";
+        bool known = lay == "v";
+        const char combi[4] = {'n', 'd', 'u', 'b'};
+        for (int a = 0; a < 4; a++) for (int b = 0; b < 4; b++) for (int d = 0; d < 4; d++)
+            if (lay.size() == 3 && lay[0] == combi[a] && lay[1] == combi[b] && lay[2] == combi[d]) known = true;
+        if (lay == "nnn" || !known) lay = "nnb";
+        c->layout = lay;
+        std::mt19937 mte(seed);
+        auto randp = [&](double A, double B) { return A + (B - A) * mte() / (mte.max() - mte.min()); };
+        const int Np = n_points;
+        c->pts.assign(size_t(Np) * 3, 0);
+        auto P = [&](int i, int d) -> int & { return c->pts[size_t(i) * 3 + d]; };
+        if (lay == "v") {
+            for (int i = 0; i < Np; i++) {
+                P(i, 0) = static_cast<int>(randp(s->xs_s, s->xs_e - 1) + 0.5);
+                P(i, 1) = static_cast<int>(randp(s->ys_s, s->ys_e - 1) + 0.5);
+                P(i, 2) = static_cast<int>(randp(s->zs_s, s->zs_e - 1) + 0.5);
+            }
+        } else {
+            const int Nx = s->Nx, Ny = s->Ny, Nz = s->Nz;
+            int n_face[6] = {0, 0, 0, 0, 0, 0};   // xd, xu, yd, yu, zd, zu
+            const int area[3] = {Ny * Nz, Nx * Nz, Nx * Ny};
+            for (int a = 0; a < 3; a++) {
+                if (lay[a] == 'd' || lay[a] == 'b') n_face[2 * a] = area[a];
+                if (lay[a] == 'u' || lay[a] == 'b') n_face[2 * a + 1] = area[a];
+            }
+            const double tot_area = n_face[0] + n_face[1] + n_face[2] + n_face[3] + n_face[4] + n_face[5];
+            int N_left = Np;
+            for (int f = 0; f < 6; f++) {
+                int N_alloc = static_cast<int>(Np * n_face[f] / tot_area + 0.5);
+                N_alloc = N_alloc < N_left ? N_alloc : N_left;
+                N_left -= N_alloc;
+                n_face[f] = N_alloc;
+            }
+            int off = 0;
+            const int lo[3] = {s->xs_s, s->ys_s, s->zs_s}, hi[3] = {s->xs_e - 1, s->ys_e - 1, s->zs_e - 1};
+            for (int f = 0; f < 6; f++) {
+                const int axis = f / 2;
+                for (int i = off; i < off + n_face[f]; i++)
+                    for (int d = 0; d < 3; d++)
+                        P(i, d) = d == axis ? (f % 2 ? hi[d] : lo[d]) : static_cast<int>(randp(lo[d], hi[d]) + 0.5);
+                off += n_face[f];
+            }
+        }
+        c->w.resize(Np);
+        for (int i = 0; i < Np; i++) c->w[i] = 2.0 * Pi * c_light / randp(lambda_min, lambda_max);
+        const double T = std::max(lambda_min, lambda_max) / c_light;
+        c->n_avg = std::max(1, static_cast<int>(T / s->Dt));
+        c->step0 = s->tstep;
+        try {
+            c->dpts.alloc(c->pts.size() * sizeof(int), s->dev_bytes);
+            AE_CUDA(cudaMemcpy(c->dpts.p, c->pts.data(), c->pts.size() * sizeof(int), cudaMemcpyHostToDevice));
+            c->acc.alloc(size_t(Np) * 3 * 16, s->dev_bytes);
+            c->ring.alloc(size_t(6) * Np * c->n_avg * 8, s->dev_bytes);
+            c->ctab.alloc(size_t(2) * s->seg_len * Np * 16, s->dev_bytes);
+            AE_CUDA(cudaMemsetAsync(c->acc.p, 0, c->acc.n, s->stream));
+            AE_CUDA(cudaMemsetAsync(c->ring.p, 0, c->ring.n, s->stream));
+            AE_CUDA(cudaStreamSynchronize(s->stream));
+        } catch (...) {
+            size_t t = 0;
+            c->dpts.release(t); c->acc.release(t); c->ring.release(t); c->ctab.release(t);
+            s->dev_bytes -= std::min(s->dev_bytes, t);
+            delete c;
+            throw;
+        }
+        s->ccft = c;
+        s->graphs_dirty = true;
+    });
+}
+
 aefdtd_status aefdtd_get_completion(aefdtd_sim *s, int32_t *done, int32_t *stop_step, double *ratio) {
     if (!s) return AEFDTD_BAD_ARG;
     if (done) *done = s->cc_done ? 1 : 0;
     if (stop_step) *stop_step = s->cc_stop;
-    if (ratio) *ratio = s->cc_max > 0 ? s->cc_last / s->cc_max : 0.0;
+    if (ratio) *ratio = s->ccft ? s->ccft->open_ratio : (s->cc_max > 0 ? s->cc_last / s->cc_max : 0.0);
     return AEFDTD_OK;
 }
 

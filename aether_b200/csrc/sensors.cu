@@ -24,6 +24,11 @@ template <typename T> static int map_impl(const MapStepArgs<T> &a, cudaStream_t 
     return nb > 0;
 }
 int launch_fieldmap_step(const MapStepArgs<double> &a, cudaStream_t s) { return map_impl(a, s); }
+template <typename T> static void ccft_impl(const CcFtArgs<T> &a, cudaStream_t s) {
+    if (a.np > 0) completion_ft_step<<<(a.np + kPlaneThreads - 1) / kPlaneThreads, kPlaneThreads, 0, s>>>(a);
+}
+void launch_completion_ft(const CcFtArgs<double> &a, cudaStream_t s) { ccft_impl(a, s); }
+void launch_completion_ft(const CcFtArgs<float> &a, cudaStream_t s) { ccft_impl(a, s); }
 int launch_fieldmap_step(const MapStepArgs<float> &a, cudaStream_t s) { return map_impl(a, s); }
 void launch_plane_reduce(const double *partial, int nbp, const StepScalars *sc, double *out, int steps,
                          cudaStream_t s) {

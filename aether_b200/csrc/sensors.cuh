@@ -208,6 +208,26 @@ __device__ __forceinline__ void map_one(const MapStepArgs<T> &a, const MapDesc &
     }
 }
 
+// One step of the FT-mode completion sensor: one thread per probe.
+template <typename T>
+__global__ void __launch_bounds__(kPlaneThreads) completion_ft_step(const __grid_constant__ CcFtArgs<T> a) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.np) return;
+    T f[3];
+    local_e(a, a.pts[3 * p], a.pts[3 * p + 1], a.pts[3 * p + 2], f);
+    const double2 c = a.coef[(size_t)a.q * a.np + p];
+    const int offset = (a.sc[a.q].step - a.step0) % a.n_avg;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        double2 v = a.acc[3 * p + d];
+        v.x = dadd(v.x, dmul((double)f[d], c.x));
+        v.y = dadd(v.y, dmul((double)f[d], c.y));
+        a.acc[3 * p + d] = v;
+        a.ring[((size_t)d * a.np + p) * a.n_avg + offset] = v.x;
+        a.ring[((size_t)(3 + d) * a.np + p) * a.n_avg + offset] = v.y;
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kPlaneThreads) fieldmap_step(const __grid_constant__ MapStepArgs<T> a) {
     const int b = blockIdx.x;

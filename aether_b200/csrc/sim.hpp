@@ -158,6 +158,19 @@ struct PlaneSensor {
     int N0 = 0, N1 = 0;
 };
 
+// Completion sensor in FT mode (CompletionSensor, s_completion.cpp): probe
+// cells and wavelengths, the transform ring on the device and its host copy.
+struct CompletionFT {
+    double lmin = 0, lmax = 0;
+    int np = 0, n_avg = 1, step0 = 0;
+    std::string layout;
+    std::vector<int> pts;          // [np][3]
+    std::vector<double> w;         // [np] angular frequencies
+    std::vector<double> ring_host, rows;
+    DBuf dpts, acc, ring, ctab;    // ctab: [2 slots][seg_len][np] complex phases
+    double open_ratio = 0;         // fraction of probes not settled at the last check
+};
+
 // Single-wavelength field sensor (FieldMap, FieldBlock, FieldPoint of
 // s_fieldmap.cpp); dev.acc holds the device accumulators or point history.
 struct FieldMapHost {
@@ -342,7 +355,9 @@ struct aefdtd_sim {
     double cc_last = 0, cc_max = 0;
     int cc_nb = 0, cc_cap = 0;      // energy blocks per step; history capacity
     DBuf cc_partial, cc_hist;
+    CompletionFT *ccft = nullptr;   // FT mode (else energy mode)
     void completion_check();
+    bool ft_check();
 };
 
 inline aefdtd_sim::~aefdtd_sim() {
@@ -372,6 +387,10 @@ inline aefdtd_sim::~aefdtd_sim() {
         delete obl;
     }
     for (auto *m : fmaps) { m->acc.release(t); delete m; }
+    if (ccft) {
+        ccft->dpts.release(t); ccft->acc.release(t); ccft->ring.release(t); ccft->ctab.release(t);
+        delete ccft;
+    }
     for (auto *s : sensors) {
         s->S.release(t); s->acc.release(t); s->wdev.release(t); s->WE.release(t); s->WH.release(t); s->flux.release(t);
         s->Btc.release(t);

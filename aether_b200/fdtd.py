@@ -142,6 +142,12 @@ class Simulation:
         """Energy-mode completion sensor (coeff <= 0: off)."""
         self._c(self._lib.aefdtd_set_completion(self._h, float(coeff), int(check_every)))
 
+    def set_completion_ft(self, lambda_min, lambda_max, coeff=1e-3, n_points=500, layout="nnb", seed=0,
+                          check_every=500):
+        """FT-mode completion sensor: probes on the faces named by layout, std::mt19937(seed) draws."""
+        self._c(self._lib.aefdtd_set_completion_ft(self._h, float(lambda_min), float(lambda_max), float(coeff),
+                                                   int(n_points), layout.encode(), int(seed), int(check_every)))
+
     def completion(self):
         """(done, stop step t or -1, last/max energy at the last check)."""
         d, t, r = C.c_int32(), C.c_int32(), C.c_double()

@@ -345,7 +345,22 @@ aefdtd_status aefdtd_get_fieldmap(aefdtd_sim *sim, int32_t map_id, double *out, 
  * check_every 0 -> 500 (the reference default, with coeff 1e-3). Not for batch
  * members. */
 aefdtd_status aefdtd_set_completion(aefdtd_sim *sim, double coeff, int32_t check_every);
-/* done: 1 after completion; stop_step: t (or -1); ratio: last / largest energy at the last check. */
+/* Completion sensor in FT mode (CompletionSensor(lmin, lmax, coeff, Np,
+ * layout), s_completion.cpp:26-37, 45-121, 137-166, 246-361): n_points probe
+ * cells on the structure faces named by layout (three letters, per axis x y z:
+ * n none, d lower face, u upper face, b both; or "v" for the volume; unknown
+ * layouts and "nnn" become "nnb"), each with a wavelength drawn in
+ * [lambda_min, lambda_max]. Every step the probe's E is accumulated into a
+ * running single-frequency transform; at a check the run completes when 90% of
+ * the probes vary by at most coeff of their mean over the last
+ * max(lambda)/c/Dt steps. The draws come from a std::mt19937 seeded with
+ * seed (the reference draws from its global generator, seeded with the start
+ * time or by seedp). check_every 0 -> 500. coeff <= 0 turns the sensor off. */
+aefdtd_status aefdtd_set_completion_ft(aefdtd_sim *sim, double lambda_min, double lambda_max, double coeff,
+                                       int32_t n_points, const char *layout, uint32_t seed, int32_t check_every);
+/* done: 1 after completion; stop_step: t (or -1); ratio: energy mode, last /
+ * largest energy at the last check; FT mode, the fraction of probes not yet
+ * settled at the last check. */
 aefdtd_status aefdtd_get_completion(aefdtd_sim *sim, int32_t *done, int32_t *stop_step, double *ratio);
 
 /* Per-launch device timings of the most recent aefdtd_step call, measured

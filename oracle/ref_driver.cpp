@@ -39,6 +39,13 @@ namespace {
 // (normal_incidence.cpp:284-297, 417-427).
 double g_cc_coeff = 0;
 int g_cc_every = 500;
+// FT mode (CompletionSensor(lmin, lmax, coeff, Np, layout)) when g_cc_np > 0;
+// the global generator is reseeded with g_cc_seed (seedp) before the sensor
+// draws its probes
+int g_cc_np = 0;
+double g_cc_lmin = 0, g_cc_lmax = 0;
+std::string g_cc_layout;
+int g_cc_seed = 0;
 int g_cc_stop = -1;
 double g_cc_last = 0, g_cc_max = 0;
 
@@ -258,7 +265,11 @@ int aeref_run(const aefdtd_grid_desc *g, const uint32_t *map,
         CompletionSensor *cpl = nullptr;
         g_cc_stop = -1;
         g_cc_last = g_cc_max = 0;
-        if (g_cc_coeff > 0) {
+        if (g_cc_coeff > 0 && g_cc_np > 0) {
+            seedp(g_cc_seed);
+            cpl = new CompletionSensor(g_cc_lmin, g_cc_lmax, g_cc_coeff, g_cc_np, g_cc_layout);
+            cpl->link(fdtd, std::filesystem::path("."));
+        } else if (g_cc_coeff > 0) {
             cpl = new CompletionSensor(g_cc_coeff);
             cpl->link(fdtd, std::filesystem::path("."));
         }
@@ -685,6 +696,18 @@ int aeref_box_result(double *out, int32_t nl) {
 void aeref_set_completion(double coeff, int32_t every) {
     g_cc_coeff = coeff;
     g_cc_every = every > 0 ? every : 500;
+    g_cc_np = 0;
+}
+
+/* FT-mode completion sensor for the following aeref_run calls (normal mode). */
+void aeref_set_completion_ft(double lmin, double lmax, double coeff, int32_t np, const char *layout, int32_t seed,
+                             int32_t every) {
+    aeref_set_completion(coeff, every);
+    g_cc_np = np;
+    g_cc_lmin = lmin;
+    g_cc_lmax = lmax;
+    g_cc_layout = layout ? layout : "";
+    g_cc_seed = seed;
 }
 
 /* Result of the last aeref_run with completion: stop step t (-1 if it ran

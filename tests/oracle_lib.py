@@ -110,6 +110,25 @@ def run_ref_completion(scene, coeff, every, nsteps=None):
     return out
 
 
+def run_ref_completion_ft(scene, lmin, lmax, coeff, n_points, layout, seed, every, nsteps=None):
+    """As run_ref_completion with the FT-mode CompletionSensor(lmin, lmax,
+    coeff, n_points, layout), the reference's generator reseeded with seed."""
+    lib = C.CDLL(REF_PATH)
+    lib.aeref_set_completion_ft.argtypes = [C.c_double, C.c_double, C.c_double, C.c_int32, C.c_char_p, C.c_int32,
+                                            C.c_int32]
+    lib.aeref_set_completion.argtypes = [C.c_double, C.c_int32]
+    lib.aeref_completion_result.argtypes = [_P(C.c_int32), _P(C.c_double), _P(C.c_double)]
+    lib.aeref_set_completion_ft(lmin, lmax, coeff, n_points, layout.encode(), seed, every)
+    try:
+        out = run(scene, "ref", nsteps=nsteps, want_fields=True)
+        stop, last, mx = C.c_int32(), C.c_double(), C.c_double()
+        lib.aeref_completion_result(C.byref(stop), C.byref(last), C.byref(mx))
+    finally:
+        lib.aeref_set_completion(0.0, 500)
+    out.update(stop=stop.value)
+    return out
+
+
 def run_ref_box(scene, box, nl, lambda_min, lambda_max, disabled=0, nsteps=None):
     """The reference core with one Box_Spect_Poynting sensor: the run dict of
     `run` plus 'box_flux' (its rsp_result, nl values)."""
