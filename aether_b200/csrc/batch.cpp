@@ -57,6 +57,7 @@ struct BatchSubset {
     cudaGraphExec_t graph = nullptr;   // one chunk of graph_steps steps
     uint64_t graph_launches = 0;
     bool built = false;
+    bool solo = false;             // one member: its own single-simulation kernels and work lists
     void release(size_t &t) {
         items.release(t);
         argsE.release(t); argsH.release(t); sargs.release(t);
@@ -109,14 +110,14 @@ struct aefdtd_batch {
     bool typed = false, fp64 = false;
     int id_bytes = 1, seg_len = 64;
     Lane lanes[kMaxLanes];
-    int n_lanes = 1;               // subsets running concurrently
+    int n_lanes = 2;               // subsets running concurrently
     cudaStream_t stream = nullptr; // lanes[0].stream
     std::vector<BatchMember> members;
     std::vector<BatchSubset> subsets;
     std::map<int, SizeClass> classes;
     bool layout_dirty = true;
     long long l2_budget = 48LL << 20;
-    int graph_steps = 16;          // steps per captured chunk (a divisor of seg_len)
+    int graph_steps = 32;          // steps per captured chunk (a divisor of seg_len)
     bool h_reverse = false;        // H pass over the members in reverse order (measured slower on L2-sized subsets)
     uint64_t launches = 0;
     size_t dev_bytes = 0;
@@ -231,6 +232,18 @@ void aefdtd_batch::update_layout() {
 template <typename T, typename Tid> void aefdtd_batch::build_subset(BatchSubset &u) {
     u.release(dev_bytes);
     const SizeClass &sc = classes[u.cls];
+    // A lone member keeps its own work lists (two-cell items, L2-ordered H
+    // lists) and kernels; merged members take one-cell, forward lists.
+    u.solo = u.members.size() == 1;
+    for (aefdtd_sim *s : u.members) {
+        const unsigned pm = u.solo ? s->pair_mask0 : 0u;
+        const int hr = u.solo ? s->h_reverse0 : 0;
+        if (s->pair_mask != pm || s->h_reverse != hr || s->work_dirty) {
+            s->pair_mask = pm;
+            s->h_reverse = hr;
+            s->build_work();
+        }
+    }
     std::vector<int> all;
     for (int half = 0; half < 2; half++) {
         WorkSplit &w = half == 0 ? u.wsE : u.wsH;
@@ -316,8 +329,15 @@ template <typename T, typename Tid> void aefdtd_batch::enqueue_steps(BatchSubset
     const int2 *blk = u.blkmap.as<int2>();
     int groups = 0;
     for (int g = 0; g < kGroups; g++) groups += (u.wsE.n[g] > 0) + (u.wsH.n[g] > 0);
+    // a lone member: its own arguments as launch parameters, its own lists
+    aefdtd_sim *m0 = u.members[0];
+    StepArgs<T, Tid> se, sh;
+    if (u.solo) m0->make_step_args(se, sh, m0->tables.as<StepScalars>());
+    const int4 *mit = m0->items.as<int4>();
     for (int q = 0; q < L; q++) {
-        run_groups(u.wsE, ln, [&](int g, cudaStream_t st) { launch_e_group_batch(ea, q, it, u.wsE, g, st); });
+        se.q = sh.q = q;
+        if (u.solo) run_groups(m0->wsE, ln, [&](int g, cudaStream_t st) { launch_e_group(se, mit, m0->wsE, g, st); });
+        else run_groups(u.wsE, ln, [&](int g, cudaStream_t st) { launch_e_group_batch(ea, q, it, u.wsE, g, st); });
         // plane sums read E only: beside the H half-step
         if (u.nblk > 0) {
             AE_CUDA(cudaEventRecord(ln.ev_sf, ln.stream));
@@ -325,7 +345,8 @@ template <typename T, typename Tid> void aefdtd_batch::enqueue_steps(BatchSubset
             launch_plane_partial_batch(sa, blk, u.nblk, q, ln.side_s);
             AE_CUDA(cudaEventRecord(ln.ev_sj, ln.side_s));
         }
-        run_groups(u.wsH, ln, [&](int g, cudaStream_t st) { launch_h_group_batch(ha, q, it, u.wsH, g, st); });
+        if (u.solo) run_groups(m0->wsH, ln, [&](int g, cudaStream_t st) { launch_h_group(sh, mit, m0->wsH, g, st); });
+        else run_groups(u.wsH, ln, [&](int g, cudaStream_t st) { launch_h_group_batch(ha, q, it, u.wsH, g, st); });
         if (u.nblk > 0) AE_CUDA(cudaStreamWaitEvent(ln.stream, ln.ev_sj, 0));
         launches += groups + (u.nblk > 0);
     }
@@ -626,9 +647,7 @@ aefdtd_status aefdtd_batch_add(aefdtd_batch *b, aefdtd_sim *s, int32_t steps) {
         if (s->Nz >= 32768) fail(AEFDTD_BAD_ARG, "batch members need Nz < 32768 (k1 << 16 in an int32 item)");
         s->set_device();
         s->finalize_tables();
-        s->pair_mask = 0;            // the batched kernels take 32-column items
-        s->h_reverse = 0;            // L2-sized subsets: forward H lists
-        s->build_work();
+        s->build_work();             // lists for its subset follow in build_subset
         if (!b->typed) {
             b->typed = true;
             b->fp64 = s->fp64;

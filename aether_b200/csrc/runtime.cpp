@@ -116,6 +116,8 @@ void aefdtd_sim::construct(const aefdtd_grid_desc *d) {
     // two cells per thread: FP32 interior and z-CPML items, FP64 z-CPML items
     pair_mask = fp64 ? (1u << kGroupPmlZ) : (1u << kGroupInterior) | (1u << kGroupPmlZ);
     if (const char *pm = std::getenv("AEFDTD_PAIR")) pair_mask = unsigned(atoi(pm)) & 3u;
+    pair_mask0 = pair_mask;
+    h_reverse0 = h_reverse;
     if (const char *ty = std::getenv("AEFDTD_TILE_Y")) {
         const int v = atoi(ty);
         tile_y = (v == 2 || v == 8) ? v : 4;

@@ -345,6 +345,8 @@ struct aefdtd_sim {
     int tile_y = kTileYHost;        // tile height of the work items (2, 4 or 8)
     unsigned pair_mask = 0;         // groups run two cells per thread (WorkSplit::pair_mask; even Nx only)
     int prefetch_l2 = 3;            // L2 prefetch of each item's planes: bit 0 interior kernels, bit 1 CPML kernels
+    unsigned pair_mask0 = 0;        // the simulation's own choices (restored when it runs alone)
+    int h_reverse0 = -1;
     int h_reverse = -1;             // H work lists top plane first (L2 reuse between half-steps); -1: by size
     // completion sensor, energy mode (CompletionSensor(coeff), s_completion.cpp)
     double cc_coeff = 0;            // > 0: enabled

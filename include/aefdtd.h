@@ -403,8 +403,8 @@ typedef struct aefdtd_batch_opts {
     int32_t tile_y;           /* tile height 2, 4 or 8 (0 -> 4) until autotuned */
     int32_t kchunk;           /* planes per work item (0 -> each simulation's heuristic) until autotuned */
     int32_t use_graphs;       /* < 0: no CUDA graphs (direct launches) */
-    int32_t graph_steps;      /* steps per captured graph of a subset; 0 -> 16 */
-    int32_t lanes;            /* subsets running concurrently (1..8); 0 -> 1 until autotuned */
+    int32_t graph_steps;      /* steps per captured graph of a subset; 0 -> 32 */
+    int32_t lanes;            /* subsets running concurrently (1..8); 0 -> 2 until autotuned */
     int32_t reserved;
 } aefdtd_batch_opts;
 
