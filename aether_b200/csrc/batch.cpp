@@ -12,17 +12,21 @@
 //    state fits an L2 budget (126 MB of L2 on B200; default 48 MiB, tuned).
 //    A subset runs a whole segment of steps before the next subset starts, so
 //    after its first step most of its state is served from L2. Lanes run that
-//    many subsets concurrently (default 1: measured on 32 config-4 cells, one
-//    resident cell at a time beats two or more sharing L2, 45.8 vs 42.0
-//    Gcell/s, and beats merged 5-cell subsets, 37.3 Gcell/s).
-//  * Merged launches. Per step, each work-item group of a subset (interior,
-//    z-CPML, dispersive, general, x/y-CPML) is ONE launch over the items of all its
-//    members: items carry the member index and the kernels read that member's
-//    arguments from a device array. Boundary groups run on side streams beside
-//    the interior group; the plane sums of all normal-mode members are one
-//    launch beside the H half-step. A chunk of 16 steps of a subset is
-//    captured once as a CUDA graph and replayed for every full chunk (the
-//    members' scalar tables are uploaded before each replay).
+//    many subsets concurrently (default 2: measured on 96 config-4 cells, two
+//    resident cells at a time 57.8 Gcell/s, one 47.0, three 55.4).
+//  * Lone members. A subset of one member (one config-4 cell fills the
+//    default budget) runs the member's own single-simulation kernels and work
+//    lists (two-cell items, L2-ordered H lists, arguments as launch
+//    parameters).
+//  * Merged launches. Otherwise, per step, each work-item group of a subset
+//    (interior, z-CPML, dispersive, general, x/y-CPML) is ONE launch over the
+//    items of all its members: items carry the member index and the kernels
+//    read that member's arguments from a device array.
+//  * Either way boundary groups run on side streams beside the interior group;
+//    the plane sums of all normal-mode members are one launch beside the H
+//    half-step. A chunk of 32 steps of a subset is captured once as a CUDA
+//    graph and replayed for every full chunk (the members' scalar tables are
+//    uploaded before each replay).
 //  * Step budgets. Each member has a number of steps still to run; a segment
 //    never passes a member's budget, so members finish exactly and can be
 //    retired and replaced between segments (continuous batching).
