@@ -466,8 +466,16 @@ def profile_run(args):
     precision `--profile`. Prints nothing on stdout."""
     os.environ["AEFDTD_NO_GRAPHS"] = "1"
     from aether_b200 import _abi as A
+    from aether_b200 import configs as CF
     from aether_b200 import fdtd
-    sim = fdtd.build_simulation(workload(A.FP32 if args.profile == "fp32" else A.FP64))
+    prec = A.FP32 if args.profile == "fp32" else A.FP64
+    if args.profile_grid == "large":
+        # config 3's scene at 384 x 384 x 192 (CPML on six faces, spheres, oscillator)
+        sc = CF.random_spheres_scene(n_total=(384, 384, 192), n_dielectric=60, n_lorentz=6, seed=1234,
+                                     precision=prec)
+    else:
+        sc = workload(prec)
+    sim = fdtd.build_simulation(sc)
     sim.step(STEPS_PER_BENCH_STEP * args.segments)
     sim.synchronize()
     log(f"profile run: {args.profile}, {STEPS_PER_BENCH_STEP * args.segments} steps, {sim.launch_count()} launches")
@@ -487,6 +495,8 @@ def main():
     ap.add_argument("--no-serving", action="store_true", help="skip the config-5 serving sample")
     ap.add_argument("--profile", choices=["fp32", "fp64"], help="direct-launch run for ncu (no timing)")
     ap.add_argument("--segments", type=int, default=2)
+    ap.add_argument("--profile-grid", choices=["bench", "large"], default="bench",
+                    help="--profile on the bench grid or on config 3's scene at 384 x 384 x 192")
     args = ap.parse_args()
     if args.profile:
         profile_run(args)
