@@ -12,7 +12,8 @@ FP64, FP32 = 0, 1
 EX, EY, EZ, HX, HY, HZ = range(6)
 NORMAL_X, NORMAL_XM, NORMAL_Y, NORMAL_YM, NORMAL_Z, NORMAL_ZM = range(6)
 XM, XP, YM, YP, ZM, ZP = range(6)
-OP_BLOCK, OP_LAYER, OP_SPHERE, OP_CYLINDER = range(4)
+(OP_BLOCK, OP_LAYER, OP_SPHERE, OP_CYLINDER, OP_CONE, OP_ELLIPSOID, OP_SIN_LAYER, OP_VECT_BLOCK, OP_VECT_TRI,
+ OP_COATING, OP_CONF_COATING) = range(11)
 
 STATUS = {
     0: "OK", 1: "BAD_ARG", 2: "OOM", 3: "TIMEOUT", 4: "CUDA_ERROR",
@@ -155,7 +156,28 @@ class FieldMapDesc(C.Structure):
 
 
 class StructureOp(C.Structure):
-    _fields_ = [("kind", C.c_int32), ("mat_index", C.c_int32), ("p", C.c_double * 8)]
+    _fields_ = [("kind", C.c_int32), ("mat_index", C.c_int32), ("p", C.c_double * 16)]
+
+
+class StructureDesc(C.Structure):
+    _fields_ = [("default_material", C.c_int32), ("periodic", C.c_int32 * 3), ("flip", C.c_int32 * 3),
+                ("reserved", C.c_int32), ("lengths", C.c_double * 3)]
+
+
+def structure_op(kind, mat, *p):
+    o = StructureOp()
+    o.kind, o.mat_index = int(kind), int(mat)
+    for i, v in enumerate(p):
+        o.p[i] = float(v)
+    return o
+
+
+def structure_desc(default=0, periodic=(0, 0, 0), flip=(0, 0, 0), lengths=(0.0, 0.0, 0.0)):
+    d = StructureDesc()
+    d.default_material = int(default)
+    for a in range(3):
+        d.periodic[a], d.flip[a], d.lengths[a] = int(periodic[a]), int(flip[a]), float(lengths[a])
+    return d
 
 
 def material_desc(eps_inf=1.0, debye=(), drude=(), lorentz=(), critpoint=()):

@@ -28,6 +28,9 @@ _SIGS = {
     "aefdtd_voxelize": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
                                   C.c_double, _P(A.StructureOp), C.c_int32, C.c_int32, _P(C.c_int32),
                                   _P(C.c_double), _P(C.c_uint32), C.c_int32]),
+    "aefdtd_discretize": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
+                                    C.c_double, _P(A.StructureOp), C.c_int32, _P(A.StructureDesc),
+                                    _P(C.c_uint32), C.c_int32]),
     "aefdtd_setup_normal": (C.c_int, [C.c_void_p, _P(A.NormalDesc)]),
     "aefdtd_add_oscillator": (C.c_int, [C.c_void_p, _P(A.SourceDesc), _P(C.c_int32)]),
     "aefdtd_add_planar_sensor": (C.c_int, [C.c_void_p, _P(A.SensorDesc), _P(C.c_int32)]),

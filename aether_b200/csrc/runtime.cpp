@@ -1921,41 +1921,88 @@ aefdtd_status aefdtd_get_sensor_dft(aefdtd_sim *s, int32_t id, double *out, size
     });
 }
 
-aefdtd_status aefdtd_voxelize(aefdtd_sim *sim, int32_t nx, int32_t ny, int32_t nz, double dx, double dy, double dz,
-                              const aefdtd_structure_op *ops, int32_t n_ops, int32_t default_material,
-                              const int32_t periodic[3], const double lengths[3], uint32_t *out_map, int32_t device) {
-    if (nx < 1 || ny < 1 || nz < 1 || n_ops < 0 || n_ops > 256 || (n_ops > 0 && !ops) || !out_map) return AEFDTD_BAD_ARG;
+aefdtd_status aefdtd_discretize(aefdtd_sim *sim, int32_t nx, int32_t ny, int32_t nz, double dx, double dy, double dz,
+                                const aefdtd_structure_op *ops, int32_t n_ops, const aefdtd_structure_desc *desc,
+                                uint32_t *out_map, int32_t device) {
+    if (nx < 1 || ny < 1 || nz < 1 || n_ops < 0 || n_ops > 256 || (n_ops > 0 && !ops) || !out_map || !desc)
+        return AEFDTD_BAD_ARG;
     return guarded(sim, [&] {
         int ndev = 0;
         if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) fail(AEFDTD_NO_DEVICE, "no CUDA device visible");
         int dev = sim ? sim->device : device;
         AE_CUDA(cudaSetDevice(dev));
-        for (int q = 0; q < n_ops; q++)
-            if (ops[q].kind < AEFDTD_OP_BLOCK || ops[q].kind > AEFDTD_OP_CYLINDER || ops[q].mat_index < 0)
-                fail(AEFDTD_BAD_ARG, "bad structure operation");
-        int per[3] = {0, 0, 0};
-        double L[3] = {0, 0, 0};
+        aefdtd_structure_desc d = *desc;
         for (int a = 0; a < 3; a++) {
-            per[a] = periodic ? (periodic[a] ? 1 : 0) : 0;
-            L[a] = lengths ? lengths[a] : 0;
-            if (per[a] && !(L[a] > 0)) fail(AEFDTD_BAD_ARG, "periodic axis needs a positive length");
+            if (d.periodic[a] && !(d.lengths[a] > 0)) fail(AEFDTD_BAD_ARG, "periodic axis needs a positive length");
+            if (!std::isfinite(d.lengths[a])) fail(AEFDTD_BAD_ARG, "structure lengths must be finite");
+        }
+        // coatings evaluate the structure below them; the device follows at most 3 nested coatings
+        std::vector<int> depth(n_ops, 0);
+        long long lattice = 0;
+        for (int q = 0; q < n_ops; q++) {
+            const aefdtd_structure_op &o = ops[q];
+            if (o.kind < AEFDTD_OP_BLOCK || o.kind > AEFDTD_OP_CONF_COATING || o.mat_index < 0)
+                fail(AEFDTD_BAD_ARG, "bad structure operation " + std::to_string(q));
+            for (int t = 0; t < 16; t++)
+                if (!std::isfinite(o.p[t])) fail(AEFDTD_BAD_ARG, "structure operation parameters must be finite");
+            if (o.kind == AEFDTD_OP_COATING || o.kind == AEFDTD_OP_CONF_COATING) {
+                int below = 0;
+                for (int p = 0; p < q; p++) below = std::max(below, depth[p]);
+                depth[q] = below + 1;
+                if (depth[q] > 3) fail(AEFDTD_BAD_ARG, "coatings nest more than 3 deep");
+            }
+            if (o.kind == AEFDTD_OP_COATING) {
+                const double delta = o.p[3], cz = std::cos(o.p[0] * (3.141592653589793 / 180.0));
+                if (!(delta > 0)) fail(AEFDTD_BAD_ARG, "a coating needs delta > 0");
+                if (!(cz > 0) || !(d.lengths[2] > 0) || 3.0 * d.lengths[2] / (delta * cz) > 1e6)
+                    fail(AEFDTD_BAD_ARG, "coating direction too shallow for its delta (the march through z would not end)");
+                if (!(o.p[2] >= 0)) fail(AEFDTD_BAD_ARG, "coating thickness must be >= 0");
+            }
+            if (o.kind == AEFDTD_OP_CONF_COATING) {
+                const double delta = o.p[1] > 0 ? o.p[1] : 5e-9;
+                long long n = 1;
+                for (int a = 0; a < 3; a++) n *= std::max(0LL, (long long)(d.lengths[a] / delta));
+                lattice += n;
+                if (lattice > (1LL << 31)) fail(AEFDTD_BAD_ARG, "conformal-coating seed lattice too large");
+            }
+            if ((o.kind == AEFDTD_OP_ELLIPSOID) && !(o.p[3] > 0 && o.p[4] > 0 && o.p[5] > 0))
+                fail(AEFDTD_BAD_ARG, "ellipsoid radii must be positive");
         }
         size_t n = size_t(nx) * ny * nz;
         cudaStream_t st = sim ? sim->stream : nullptr;
-        uint32_t *d = nullptr;
-        AE_CUDA(cudaMallocAsync((void **)&d, n * 4, st));
-        cudaError_t e = launch_voxelize(nx, ny, nz, dx, dy, dz, ops, n_ops, default_material, per, L, d, st);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(out_map, d, n * 4, cudaMemcpyDeviceToHost, st);
-        cudaFreeAsync(d, st);
+        uint32_t *dmap = nullptr;
+        int *derr = nullptr;
+        AE_CUDA(cudaMallocAsync((void **)&dmap, n * 4 + 16, st));
+        derr = reinterpret_cast<int *>(reinterpret_cast<char *>(dmap) + (n * 4 + 15) / 16 * 16);
+        cudaError_t e = cudaMemsetAsync(derr, 0, sizeof(int), st);
+        if (e == cudaSuccess) e = launch_discretize(nx, ny, nz, dx, dy, dz, ops, n_ops, d, dmap, derr, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(out_map, dmap, n * 4, cudaMemcpyDeviceToHost, st);
+        int herr = 0;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, st);
+        cudaFreeAsync(dmap, st);
         cudaError_t e2 = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) fail(AEFDTD_CUDA_ERROR, std::string("voxelize: ") + cudaGetErrorString(e));
-        if (e2 != cudaSuccess) fail(AEFDTD_CUDA_ERROR, std::string("voxelize: ") + cudaGetErrorString(e2));
+        if (e != cudaSuccess) fail(AEFDTD_CUDA_ERROR, std::string("discretize: ") + cudaGetErrorString(e));
+        if (e2 != cudaSuccess) fail(AEFDTD_CUDA_ERROR, std::string("discretize: ") + cudaGetErrorString(e2));
+        if (herr == 1) fail(AEFDTD_TIMEOUT, "discretize: a walk through the structure exceeded its bound");
+        if (herr) fail(AEFDTD_BAD_ARG, "discretize: coatings nest too deep");
         if (sim) {
             sim->launches++;
             if (nx != sim->Nx_s || ny != sim->Ny_s || nz != sim->Nz_s) fail(AEFDTD_BAD_ARG, "map size differs from the structure grid");
             sim->set_map(out_map, n);
         }
     });
+}
+
+aefdtd_status aefdtd_voxelize(aefdtd_sim *sim, int32_t nx, int32_t ny, int32_t nz, double dx, double dy, double dz,
+                              const aefdtd_structure_op *ops, int32_t n_ops, int32_t default_material,
+                              const int32_t periodic[3], const double lengths[3], uint32_t *out_map, int32_t device) {
+    aefdtd_structure_desc d{};
+    d.default_material = default_material;
+    for (int a = 0; a < 3; a++) {
+        d.periodic[a] = periodic ? (periodic[a] ? 1 : 0) : 0;
+        d.lengths[a] = lengths ? lengths[a] : 0;
+    }
+    return aefdtd_discretize(sim, nx, ny, nz, dx, dy, dz, ops, n_ops, &d, out_map, device);
 }
 
 aefdtd_status aefdtd_get_timings(aefdtd_sim *s, double *e_ms, double *h_ms, double *sensor_ms) {

@@ -49,8 +49,8 @@ template <typename F> void parallel_for(int n, F &&f) {
 // driver on completion, as for a direct destroy.
 void reap_graph(cudaGraphExec_t g, int device);
 
-cudaError_t launch_voxelize(int nx, int ny, int nz, double dx, double dy, double dz, const aefdtd_structure_op *ops,
-                            int nops, int def, const int per[3], const double l[3], uint32_t *d_out, cudaStream_t s);
+cudaError_t launch_discretize(int nx, int ny, int nz, double dx, double dy, double dz, const aefdtd_structure_op *ops,
+                              int nops, const aefdtd_structure_desc &d, uint32_t *d_out, int *d_err, cudaStream_t s);
 
 namespace phys {
 // src/common/phys_constants.h:18-20

@@ -33,8 +33,8 @@ wavevector, and every registered sensor's flux, DFT or map in registration
 order.
 
 Not available: Lua material files (Material.load_script, material(i, "file");
-describe the model with the add_* terms), structure flips, and the primitives
-outside the device voxeliser (cones, ellipsoids, meshes, coatings)."""
+describe the model with the add_* terms), and the structure operations that
+need the Lua host or files (add_lua_def, add_mesh)."""
 from __future__ import annotations
 
 import ctypes as C
@@ -123,6 +123,7 @@ class Structure:
         self.lx = self.ly = self.lz = 0.0
         self.default = 0
         self.periodic = [0, 0, 0]
+        self.flips = [0, 0, 0]
         self.ops: List[A.StructureOp] = []
         self.script(self)
 
@@ -147,12 +148,12 @@ class Structure:
         """Structure::set_loop (structure.cpp:338-348): periodic images."""
         self.periodic = [int(px != 0), int(py != 0), int(pz != 0)]
 
+    def flip(self, fx, fy, fz):
+        """Structure::set_flip (structure.cpp:326-336): mirrored axes."""
+        self.flips = [int(fx != 0), int(fy != 0), int(fz != 0)]
+
     def _op(self, kind, mat, *p):
-        o = A.StructureOp()
-        o.kind, o.mat_index = kind, int(mat)
-        for i, v in enumerate(p):
-            o.p[i] = float(v)
-        self.ops.append(o)
+        self.ops.append(A.structure_op(kind, mat, *p))
 
     def add_block(self, x1, x2, y1, y2, z1, z2, index):
         self._op(A.OP_BLOCK, index, x1, x2, y1, y2, z1, z2)
@@ -168,18 +169,49 @@ class Structure:
         # lua_structure.cpp:376-397: from (x, y, z) along (dx, dy, dz)
         self._op(A.OP_CYLINDER, index, x, y, z, x + dx, y + dy, z + dz, r)
 
+    def add_cone(self, x, y, z, dx, dy, dz, r, index):
+        """Base centre (x, y, z), apex at (x+dx, y+dy, z+dz), base radius r
+        (structure_add_cone)."""
+        self._op(A.OP_CONE, index, x, y, z, x + dx, y + dy, z + dz, r)
+
+    def add_ellipsoid(self, x, y, z, rx, ry, rz, index):
+        self._op(A.OP_ELLIPSOID, index, x, y, z, rx, ry, rz)
+
+    def add_sin_layer(self, z1, a1, z2, a2, px, phi_x, py, phi_y, index):
+        """Layer between z1 + a1 t and z2 + a2 t, t = (sin 2pi(x/px + phi_x)
+        + sin 2pi(y/py + phi_y)) / 2 (a period of 0 drops its term)."""
+        self._op(A.OP_SIN_LAYER, index, z1, a1, z2, a2, px, phi_x, py, phi_y)
+
+    def add_vect_block(self, xO, yO, zO, xA, yA, zA, xB, yB, zB, xC, yC, zC, index):
+        """Parallelepiped at O spanned by the edges A, B, C."""
+        self._op(A.OP_VECT_BLOCK, index, xO, yO, zO, xA, yA, zA, xB, yB, zB, xC, yC, zC)
+
+    def add_vect_tri(self, xO, yO, zO, xA, yA, zA, xB, yB, zB, xC, yC, zC, alp, index):
+        """Prism at O over the edges A, B, C, slanted by alp along C."""
+        self._op(A.OP_VECT_TRI, index, xO, yO, zO, xA, yA, zA, xB, yB, zB, xC, yC, zC, alp)
+
+    def add_coating(self, theta, phi, thickness, delta, origin_index, index):
+        """Coats, with material `index`, the cells of `origin_index` that lie
+        within `thickness` along the direction (theta, phi) (degrees) above a
+        different material, and see only `origin_index` up to the top."""
+        self._op(A.OP_COATING, index, theta, phi, thickness, delta, origin_index)
+
+    def add_conformal_coating(self, thickness, delta, origin_index, index):
+        """Coats, with material `index`, the cells of `origin_index` closer
+        than `thickness` to its surface, sampled every `delta` (0: 5 nm)."""
+        self._op(A.OP_CONF_COATING, index, thickness, delta, origin_index)
+
     def retrieve_nominal_size(self):
         return self.lx, self.ly, self.lz
 
     def discretize(self, nx, ny, nz, dx, dy, dz, device=0) -> np.ndarray:
-        """Structure::discretize on the GPU (aefdtd_voxelize): (nz, ny, nx) map."""
+        """Structure::discretize on the GPU (aefdtd_discretize): (nz, ny, nx) map."""
         lib = load()
         out = np.zeros(nx * ny * nz, np.uint32)
         arr = (A.StructureOp * max(1, len(self.ops)))(*self.ops)
-        per = (C.c_int32 * 3)(*self.periodic)
-        lens = (C.c_double * 3)(self.lx, self.ly, self.lz)
-        check(lib.aefdtd_voxelize(None, nx, ny, nz, dx, dy, dz, arr, len(self.ops), self.default, per, lens,
-                                  out.ctypes.data_as(C.POINTER(C.c_uint32)), device), None)
+        desc = A.structure_desc(self.default, self.periodic, self.flips, (self.lx, self.ly, self.lz))
+        check(lib.aefdtd_discretize(None, nx, ny, nz, dx, dy, dz, arr, len(self.ops), C.byref(desc),
+                                    out.ctypes.data_as(C.POINTER(C.c_uint32)), device), None)
         return out.reshape(nz, ny, nx)
 
 

@@ -174,26 +174,51 @@ aefdtd_status aefdtd_set_material_map(aefdtd_sim *sim, const uint32_t *map, size
 aefdtd_status aefdtd_set_material(aefdtd_sim *sim, uint32_t index, const aefdtd_material_desc *mat);
 
 /* Structure discretisation on the device (Structure::discretize,
- * structure.cpp:94-113, with Add_Block/Add_Layer/Add_Sphere/Add_Cylinder
- * ::index, structure_primitives.cpp:34-39,266-284,323-339,490-499). Operation
- * kinds and parameter layouts are listed with aefdtd_voxelize. */
+ * structure.cpp:94-113, and Structure::index, structure.cpp:223-258, with the
+ * primitives' index tests of structure_primitives.cpp). Operation kinds and
+ * their parameters (p[]) follow the reference's structure-script functions
+ * (lua_structure.cpp:292-548) after their argument conversions: */
 enum {
-    AEFDTD_OP_BLOCK = 0,    /* x1,x2,y1,y2,z1,z2 */
-    AEFDTD_OP_LAYER = 1,    /* axis(0/1/2 as double), z1, z2 */
-    AEFDTD_OP_SPHERE = 2,   /* x, y, z, r */
-    AEFDTD_OP_CYLINDER = 3  /* x1,y1,z1,x2,y2,z2,r */
+    AEFDTD_OP_BLOCK = 0,        /* x1,x2,y1,y2,z1,z2 (Add_Block, :24-39) */
+    AEFDTD_OP_LAYER = 1,        /* axis (0/1/2 as double), z1, z2 (Add_Layer, :317-339) */
+    AEFDTD_OP_SPHERE = 2,       /* x, y, z, r (Add_Sphere, :484-499) */
+    AEFDTD_OP_CYLINDER = 3,     /* x1,y1,z1,x2,y2,z2,r: axis end points (Add_Cylinder, :255-285) */
+    AEFDTD_OP_CONE = 4,         /* x1,y1,z1 (base centre), x2,y2,z2 (apex), r (Add_Cone, :101-134) */
+    AEFDTD_OP_ELLIPSOID = 5,    /* x, y, z, rx, ry, rz (Add_Ellipsoid, :291-312) */
+    AEFDTD_OP_SIN_LAYER = 6,    /* z1, a1, z2, a2, px, phi_x, py, phi_y (Add_Sin_Layer, :449-478) */
+    AEFDTD_OP_VECT_BLOCK = 7,   /* xO,yO,zO, xA,yA,zA, xB,yB,zB, xC,yC,zC (Add_Vect_Block, :505-566) */
+    AEFDTD_OP_VECT_TRI = 8,     /* the twelve of VECT_BLOCK, then alp (Add_Vect_Tri, :572-601) */
+    AEFDTD_OP_COATING = 9,      /* theta, phi (degrees), thickness, delta, origin material (Add_Coating, :45-95) */
+    AEFDTD_OP_CONF_COATING = 10 /* thickness, delta (<= 0: 5 nm), origin material (Add_Conf_Coating, :140-248) */
 };
 typedef struct aefdtd_structure_op {
     int32_t kind;
     int32_t mat_index;
-    double p[8];
+    double p[16];
 } aefdtd_structure_op;
+/* Structure-wide settings: default material, periodic images (loop) and
+ * mirror flips (flip) per axis, and the nominal lengths lx, ly, lz that both
+ * use and that the coatings read. */
+typedef struct aefdtd_structure_desc {
+    int32_t default_material;
+    int32_t periodic[3];
+    int32_t flip[3];
+    int32_t reserved;
+    double lengths[3];
+} aefdtd_structure_desc;
 /* Tags every cell corner (i*dx, j*dy, k*dz) of an nx*ny*nz structure grid
- * with the material of the last operation containing it, else
- * default_material; writes the map to host memory (out_map, nx*ny*nz) and,
- * when sim is not NULL, also installs it as aefdtd_set_material_map does.
- * periodic[3] and lengths l[3] reproduce Structure::index's periodic images
- * (structure.cpp:228-258). */
+ * with the material of the last operation containing it, else the default
+ * material; writes the map to host memory (out_map, nx*ny*nz, x fastest)
+ * and, when sim is not NULL, also installs it as aefdtd_set_material_map
+ * does. At most 256 operations; coatings may nest 3 deep. A directional
+ * coating needs delta > 0 and theta below 90 degrees (the reference's marches
+ * would not end otherwise). */
+aefdtd_status aefdtd_discretize(aefdtd_sim *sim, int32_t nx, int32_t ny, int32_t nz,
+                                double dx, double dy, double dz,
+                                const aefdtd_structure_op *ops, int32_t n_ops,
+                                const aefdtd_structure_desc *desc, uint32_t *out_map, int32_t device);
+/* aefdtd_discretize without flips: periodic[3] and lengths l[3] as in
+ * aefdtd_structure_desc. */
 aefdtd_status aefdtd_voxelize(aefdtd_sim *sim, int32_t nx, int32_t ny, int32_t nz,
                               double dx, double dy, double dz,
                               const aefdtd_structure_op *ops, int32_t n_ops,

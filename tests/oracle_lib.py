@@ -211,3 +211,18 @@ def run_ref_oblique(scene, nsteps=None, want_fields=True):
     out["series"] = series[:18 * nsteps].reshape(nsteps, 18)
     out["spectra"] = spectra.reshape(nl, 10)[:nl_out.value]
     return out
+
+
+def ref_discretize(nx, ny, nz, d, ops, desc):
+    """The reference's own Structure::discretize (oracle/_ref) on the given
+    operations and structure settings; (nz, ny, nx) uint32 map."""
+    lib = C.CDLL(REF_PATH)
+    fn = lib.aeref_discretize
+    fn.argtypes = [C.c_int32] * 3 + [C.c_double] * 3 + [_P(A.StructureOp), C.c_int32, _P(A.StructureDesc),
+                                                      _P(C.c_uint32)]
+    out = np.zeros(nx * ny * nz, np.uint32)
+    arr = (A.StructureOp * max(len(ops), 1))(*ops)
+    rc = fn(nx, ny, nz, d[0], d[1], d[2], arr, len(ops), C.byref(desc), out.ctypes.data_as(_P(C.c_uint32)))
+    if rc != 0:
+        raise RuntimeError(f"reference discretize failed with code {rc}")
+    return out.reshape(nz, ny, nx)

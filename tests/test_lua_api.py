@@ -276,3 +276,29 @@ def test_oblique_mode_compute_runs_the_kp_sweep():
     assert np.isclose(out["kp"][0], kp, rtol=1e-15)
     direct = OBL.sweep(f.scene(), [kp], phi_deg=30)
     assert np.array_equal(out["obl"][0], direct[0])
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not oracle_lib.available("ref"), reason="reference build absent")
+def test_structure_script_with_every_kind_matches_reference():
+    """A structure script using the primitives, coatings, loop and flip
+    through the front end, against the reference's own Structure."""
+    def script(st):
+        st.size(80e-9, 60e-9, 70e-9)
+        st.default_material(0)
+        st.loop(1, 0, 0)
+        st.flip(0, 1, 0)
+        st.add_layer("Z", 0, 15e-9, 1)
+        st.add_cone(40e-9, 30e-9, 15e-9, 0, 0, 40e-9, 20e-9, 2)
+        st.add_ellipsoid(10e-9, 45e-9, 30e-9, 12e-9, 8e-9, 10e-9, 3)
+        st.add_sin_layer(50e-9, 4e-9, 58e-9, -3e-9, 40e-9, 0.1, 0, 0, 4)
+        st.add_vect_tri(55e-9, 5e-9, 20e-9, 20e-9, 0, 0, 0, 20e-9, 0, 0, 0, 25e-9, 0.3, 5)
+        st.add_conformal_coating(5e-9, 2.5e-9, 0, 6)
+
+    st = L.Structure(script)
+    d = (2.5e-9,) * 3
+    gpu = st.discretize(32, 24, 28, *d)
+    desc = A.structure_desc(st.default, st.periodic, st.flips, (st.lx, st.ly, st.lz))
+    ref = oracle_lib.ref_discretize(32, 24, 28, d, st.ops, desc)
+    assert np.array_equal(gpu, ref)
+    assert set(np.unique(ref)) >= {0, 1, 2, 3, 6}
