@@ -4,6 +4,8 @@ Kept field-for-field identical to the header; tests check the struct sizes
 against the compiled library (aefdtd_abi_sizes)."""
 import ctypes as C
 
+import numpy as np
+
 ABI_VERSION = 1
 MAX_TERMS = 4
 
@@ -13,7 +15,7 @@ EX, EY, EZ, HX, HY, HZ = range(6)
 NORMAL_X, NORMAL_XM, NORMAL_Y, NORMAL_YM, NORMAL_Z, NORMAL_ZM = range(6)
 XM, XP, YM, YP, ZM, ZP = range(6)
 (OP_BLOCK, OP_LAYER, OP_SPHERE, OP_CYLINDER, OP_CONE, OP_ELLIPSOID, OP_SIN_LAYER, OP_VECT_BLOCK, OP_VECT_TRI,
- OP_COATING, OP_CONF_COATING) = range(11)
+ OP_COATING, OP_CONF_COATING, OP_MESH) = range(12)
 
 STATUS = {
     0: "OK", 1: "BAD_ARG", 2: "OOM", 3: "TIMEOUT", 4: "CUDA_ERROR",
@@ -159,9 +161,14 @@ class StructureOp(C.Structure):
     _fields_ = [("kind", C.c_int32), ("mat_index", C.c_int32), ("p", C.c_double * 16)]
 
 
+class Mesh(C.Structure):
+    _fields_ = [("vertices", C.POINTER(C.c_double)), ("faces", C.POINTER(C.c_int32)), ("n_vertices", C.c_int32),
+                ("n_faces", C.c_int32)]
+
+
 class StructureDesc(C.Structure):
     _fields_ = [("default_material", C.c_int32), ("periodic", C.c_int32 * 3), ("flip", C.c_int32 * 3),
-                ("reserved", C.c_int32), ("lengths", C.c_double * 3)]
+                ("n_meshes", C.c_int32), ("lengths", C.c_double * 3), ("meshes", C.POINTER(Mesh))]
 
 
 def structure_op(kind, mat, *p):
@@ -172,11 +179,27 @@ def structure_op(kind, mat, *p):
     return o
 
 
-def structure_desc(default=0, periodic=(0, 0, 0), flip=(0, 0, 0), lengths=(0.0, 0.0, 0.0)):
+def structure_desc(default=0, periodic=(0, 0, 0), flip=(0, 0, 0), lengths=(0.0, 0.0, 0.0), meshes=()):
+    """meshes: (vertices (nv, 3) float64, faces (nf, 3) int32) pairs; the
+    returned struct keeps them alive."""
     d = StructureDesc()
     d.default_material = int(default)
     for a in range(3):
         d.periodic[a], d.flip[a], d.lengths[a] = int(periodic[a]), int(flip[a]), float(lengths[a])
+    keep = []
+    if meshes:
+        arr = (Mesh * len(meshes))()
+        for i, (v, f) in enumerate(meshes):
+            v = np.ascontiguousarray(v, dtype=np.float64).reshape(-1, 3)
+            f = np.ascontiguousarray(f, dtype=np.int32).reshape(-1, 3)
+            keep += [v, f]
+            arr[i].vertices = v.ctypes.data_as(C.POINTER(C.c_double))
+            arr[i].faces = f.ctypes.data_as(C.POINTER(C.c_int32))
+            arr[i].n_vertices, arr[i].n_faces = len(v), len(f)
+        d.meshes = arr
+        d.n_meshes = len(meshes)
+        keep.append(arr)
+    d._keep = keep
     return d
 
 

@@ -1941,8 +1941,19 @@ aefdtd_status aefdtd_discretize(aefdtd_sim *sim, int32_t nx, int32_t ny, int32_t
         long long lattice = 0;
         for (int q = 0; q < n_ops; q++) {
             const aefdtd_structure_op &o = ops[q];
-            if (o.kind < AEFDTD_OP_BLOCK || o.kind > AEFDTD_OP_CONF_COATING || o.mat_index < 0)
+            if (o.kind < AEFDTD_OP_BLOCK || o.kind > AEFDTD_OP_MESH || o.mat_index < 0)
                 fail(AEFDTD_BAD_ARG, "bad structure operation " + std::to_string(q));
+            if (o.kind == AEFDTD_OP_MESH) {
+                const int mi = (int)o.p[4];
+                if (o.p[4] != mi || mi < 0 || mi >= d.n_meshes || !d.meshes) fail(AEFDTD_BAD_ARG, "mesh number out of range");
+                const aefdtd_mesh &m = d.meshes[mi];
+                if (m.n_vertices < 1 || m.n_faces < 0 || !m.vertices || (m.n_faces > 0 && !m.faces))
+                    fail(AEFDTD_BAD_ARG, "empty mesh");
+                for (long long t = 0; t < 3LL * m.n_faces; t++)
+                    if (m.faces[t] < 0 || m.faces[t] >= m.n_vertices) fail(AEFDTD_BAD_ARG, "mesh face refers to a missing vertex");
+                for (long long t = 0; t < 3LL * m.n_vertices; t++)
+                    if (!std::isfinite(m.vertices[t])) fail(AEFDTD_BAD_ARG, "mesh vertices must be finite");
+            }
             for (int t = 0; t < 16; t++)
                 if (!std::isfinite(o.p[t])) fail(AEFDTD_BAD_ARG, "structure operation parameters must be finite");
             if (o.kind == AEFDTD_OP_COATING || o.kind == AEFDTD_OP_CONF_COATING) {

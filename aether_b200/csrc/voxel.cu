@@ -18,6 +18,11 @@
 // grid corners (std::sin), the coating direction (std::cos/std::sin of the
 // angles), the unit axis of cylinders and cones, and the pivoted LU factors of
 // the vector-block edge matrix.
+//
+// A mesh point counts ray crossings over all triangles with the reference's
+// Moller-Trumbore test. The reference draws the ray direction at random for
+// every point; here it is a hash of the point. The crossing parity agrees
+// except for rays through a triangle's edge or vertex.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -47,6 +52,8 @@ struct VoxOp {
     long long sin_off;                       // sine layer: offset of its x then y tables
     int nl[3];                               // conformal coating: seed lattice size
     long long lat_off;                       // conformal coating: offset of its lattice masks
+    long long tri_off;                       // mesh: offset of its triangles (V1, E1, E2: 9 doubles each)
+    int n_tri;
 };
 
 struct VoxArgs {
@@ -55,6 +62,7 @@ struct VoxArgs {
     const VoxOp *ops;
     const uint8_t *lattice;
     const double *sintab;
+    const double *tris;
     uint32_t *out;
     int *err;
 };
@@ -245,6 +253,42 @@ __device__ int op_index(const VoxArgs &a, const VoxOp &o, double x, double y, do
                 return -1;
             }
         }
+        case AEFDTD_OP_MESH: {  // Add_Mesh::index (:428-440)
+            if (x < o.vmin[0] || x > o.vmax[0] || y < o.vmin[1] || y > o.vmax[1] || z < o.vmin[2] || z > o.vmax[2])
+                return -1;
+            // The reference casts one ray in a random direction (Vector3::rand_sph); the crossing
+            // parity does not depend on it away from rays through edges and vertices. Here the
+            // direction is a hash of the point, uniform on the sphere.
+            unsigned long long h = __double_as_longlong(x) * 0x9E3779B97F4A7C15ull;
+            h ^= __double_as_longlong(y) + 0x632BE59BD9B4E019ull + (h << 6) + (h >> 2);
+            h ^= __double_as_longlong(z) + 0x85EBCA77C2B2AE63ull + (h << 6) + (h >> 2);
+            h ^= h >> 33; h *= 0xFF51AFD7ED558CCDull; h ^= h >> 33; h *= 0xC4CEB9FE1A85EC53ull; h ^= h >> 33;
+            const double u1 = (double)(h >> 11) * (1.0 / 9007199254740992.0);
+            const double u2 = (double)((h * 0x2545F4914F6CDD1Dull) >> 11) * (1.0 / 9007199254740992.0);
+            const double dz = 1.0 - 2.0 * u1, rr = sqrt(fmax(0.0, 1.0 - dz * dz));
+            double sphi, cphi;
+            sincos(2.0 * kPi * u2, &sphi, &cphi);
+            const double dxr = rr * cphi, dyr = rr * sphi;
+            int n = 0;
+            const double *t = a.tris + o.tri_off;
+            for (int f = 0; f < o.n_tri; f++, t += 9) {
+                // ray_N_inter (ray_intersect.h:121-166): T = O - V1, P = D x E2, Q = T x E1
+                const double e1x = t[3], e1y = t[4], e1z = t[5], e2x = t[6], e2y = t[7], e2z = t[8];
+                const double tx = x - t[0], ty = y - t[1], tz = z - t[2];
+                const double px = dyr * e2z - dz * e2y, py = dz * e2x - dxr * e2z, pz = dxr * e2y - dyr * e2x;
+                const double qx = ty * e1z - tz * e1y, qy = tz * e1x - tx * e1z, qz = tx * e1y - ty * e1x;
+                const double det = px * e1x + py * e1y + pz * e1z;
+                const double invdet = 1.0 / det;
+                const double u = (px * tx + py * ty + pz * tz) * invdet;
+                if (u >= 0 && u <= 1.0) {
+                    const double v = (qx * dxr + qy * dyr + qz * dz) * invdet;
+                    if (v >= 0 && u + v <= 1.0) {
+                        if ((qx * e2x + qy * e2y + qz * e2z) * invdet >= 0) n += 1;
+                    }
+                }
+            }
+            return (n % 2 != 0) ? o.mat : -1;
+        }
     }
     return -1;
 }
@@ -355,7 +399,7 @@ cudaError_t launch_discretize(int nx, int ny, int nz, double dx, double dy, doub
                               int nops, const aefdtd_structure_desc &d, uint32_t *d_out, int *d_err, cudaStream_t s) {
     if (nops > 256) return cudaErrorInvalidValue;
     std::vector<VoxOp> h(nops);
-    std::vector<double> sintab;
+    std::vector<double> sintab, tris;
     long long lat_total = 0;
     const double L[3] = {d.lengths[0], d.lengths[1], d.lengths[2]};
     const int per[3] = {d.periodic[0] ? 1 : 0, d.periodic[1] ? 1 : 0, d.periodic[2] ? 1 : 0};
@@ -434,14 +478,38 @@ cudaError_t launch_discretize(int nx, int ny, int nz, double dx, double dy, doub
             o.lat_off = lat_total;
             lat_total += (long long)o.nl[0] * o.nl[1] * o.nl[2];
         }
+        if (o.kind == AEFDTD_OP_MESH) {
+            // Add_Mesh ctor (:396-425): vertices scaled in place; the box starts from the first
+            // vertex before scaling, as the reference's does
+            const aefdtd_mesh &m = d.meshes[(int)o.p[4]];
+            const double sc = o.p[3];
+            for (int a = 0; a < 3; a++) o.vmin[a] = o.vmax[a] = m.vertices[a];
+            std::vector<double> v(3 * (size_t)m.n_vertices);
+            for (int i = 0; i < m.n_vertices; i++)
+                for (int a = 0; a < 3; a++) {
+                    v[3 * i + a] = m.vertices[3 * i + a] * sc;
+                    o.vmin[a] = std::min(o.vmin[a], v[3 * i + a]);
+                    o.vmax[a] = std::max(o.vmax[a], v[3 * i + a]);
+                }
+            o.tri_off = (long long)tris.size();
+            o.n_tri = m.n_faces;
+            for (int f = 0; f < m.n_faces; f++) {
+                const double *v1 = &v[3 * (size_t)m.faces[3 * f]], *v2 = &v[3 * (size_t)m.faces[3 * f + 1]],
+                             *v3 = &v[3 * (size_t)m.faces[3 * f + 2]];
+                for (int a = 0; a < 3; a++) tris.push_back(v1[a]);
+                for (int a = 0; a < 3; a++) tris.push_back(v2[a] - v1[a]);
+                for (int a = 0; a < 3; a++) tris.push_back(v3[a] - v1[a]);
+            }
+        }
     }
     VoxOp *d_ops = nullptr;
-    double *d_sin = nullptr;
+    double *d_sin = nullptr, *d_tri = nullptr;
     uint8_t *d_lat = nullptr;
     cudaError_t e = cudaSuccess;
     auto release = [&] {
         if (d_ops) cudaFreeAsync(d_ops, s);
         if (d_sin) cudaFreeAsync(d_sin, s);
+        if (d_tri) cudaFreeAsync(d_tri, s);
         if (d_lat) cudaFreeAsync(d_lat, s);
     };
     if (nops > 0) {
@@ -452,6 +520,11 @@ cudaError_t launch_discretize(int nx, int ny, int nz, double dx, double dy, doub
         e = cudaMallocAsync((void **)&d_sin, sizeof(double) * sintab.size(), s);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(d_sin, sintab.data(), sizeof(double) * sintab.size(), cudaMemcpyHostToDevice, s);
+    }
+    if (e == cudaSuccess && !tris.empty()) {
+        e = cudaMallocAsync((void **)&d_tri, sizeof(double) * tris.size(), s);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d_tri, tris.data(), sizeof(double) * tris.size(), cudaMemcpyHostToDevice, s);
     }
     if (e == cudaSuccess && lat_total > 0) e = cudaMallocAsync((void **)&d_lat, (size_t)lat_total, s);
     if (e != cudaSuccess) {
@@ -469,6 +542,7 @@ cudaError_t launch_discretize(int nx, int ny, int nz, double dx, double dy, doub
     a.ops = d_ops;
     a.lattice = d_lat;
     a.sintab = d_sin;
+    a.tris = d_tri;
     a.out = d_out;
     a.err = d_err;
     // conformal-coating seed lattices, lowest operation first: each depends on the ones below it

@@ -33,8 +33,8 @@ wavevector, and every registered sensor's flux, DFT or map in registration
 order.
 
 Not available: Lua material files (Material.load_script, material(i, "file");
-describe the model with the add_* terms), and the structure operations that
-need the Lua host or files (add_lua_def, add_mesh)."""
+describe the model with the add_* terms), add_lua_def (a Lua function per
+point) and random_packing."""
 from __future__ import annotations
 
 import ctypes as C
@@ -108,6 +108,28 @@ def const_material(n: float) -> Material:
 
 # ---- structures -------------------------------------------------------------
 
+def load_obj(fname):
+    """obj_file_load (mesh_tools.h:103-152): "v x y z" vertices and "f" faces
+    of three or four vertex numbers (1-based, anything after a '/' ignored);
+    a quad becomes the triangles (0, 1, 2) and (0, 2, 3). Returns (vertices
+    (nv, 3) float64, faces (nf, 3) int32, 0-based)."""
+    verts, faces = [], []
+    with open(fname) as f:
+        for line in f:
+            t = line.split()
+            if not t:
+                continue
+            if t[0] == "v":
+                verts.append((float(t[1]), float(t[2]), float(t[3])))
+            elif t[0] == "f":
+                ids = [int(w.split("/")[0]) - 1 for w in t[1:]]
+                if len(ids) == 3:
+                    faces.append(ids)
+                elif len(ids) == 4:
+                    faces += [[ids[0], ids[1], ids[2]], [ids[0], ids[2], ids[3]]]
+    return np.array(verts, np.float64).reshape(-1, 3), np.array(faces, np.int32).reshape(-1, 3)
+
+
 class Structure:
     """Structure(script) (structure.cpp, lua_structure.cpp): `script` is a
     callable taking this object; it calls size / default_material / add_* /
@@ -124,6 +146,7 @@ class Structure:
         self.default = 0
         self.periodic = [0, 0, 0]
         self.flips = [0, 0, 0]
+        self.meshes: List[tuple] = []
         self.ops: List[A.StructureOp] = []
         self.script(self)
 
@@ -196,6 +219,13 @@ class Structure:
         different material, and see only `origin_index` up to the top."""
         self._op(A.OP_COATING, index, theta, phi, thickness, delta, origin_index)
 
+    def add_mesh(self, x, y, z, scale, fname, index):
+        """Closed triangle mesh from an OBJ file, vertices multiplied by
+        `scale` (structure_add_mesh; the reference records x, y, z but does
+        not move the mesh)."""
+        self.meshes.append(load_obj(fname))
+        self._op(A.OP_MESH, index, x, y, z, scale, len(self.meshes) - 1)
+
     def add_conformal_coating(self, thickness, delta, origin_index, index):
         """Coats, with material `index`, the cells of `origin_index` closer
         than `thickness` to its surface, sampled every `delta` (0: 5 nm)."""
@@ -209,7 +239,7 @@ class Structure:
         lib = load()
         out = np.zeros(nx * ny * nz, np.uint32)
         arr = (A.StructureOp * max(1, len(self.ops)))(*self.ops)
-        desc = A.structure_desc(self.default, self.periodic, self.flips, (self.lx, self.ly, self.lz))
+        desc = A.structure_desc(self.default, self.periodic, self.flips, (self.lx, self.ly, self.lz), self.meshes)
         check(lib.aefdtd_discretize(None, nx, ny, nz, dx, dy, dz, arr, len(self.ops), C.byref(desc),
                                     out.ctypes.data_as(C.POINTER(C.c_uint32)), device), None)
         return out.reshape(nz, ny, nx)

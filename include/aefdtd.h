@@ -189,22 +189,36 @@ enum {
     AEFDTD_OP_VECT_BLOCK = 7,   /* xO,yO,zO, xA,yA,zA, xB,yB,zB, xC,yC,zC (Add_Vect_Block, :505-566) */
     AEFDTD_OP_VECT_TRI = 8,     /* the twelve of VECT_BLOCK, then alp (Add_Vect_Tri, :572-601) */
     AEFDTD_OP_COATING = 9,      /* theta, phi (degrees), thickness, delta, origin material (Add_Coating, :45-95) */
-    AEFDTD_OP_CONF_COATING = 10 /* thickness, delta (<= 0: 5 nm), origin material (Add_Conf_Coating, :140-248) */
+    AEFDTD_OP_CONF_COATING = 10, /* thickness, delta (<= 0: 5 nm), origin material (Add_Conf_Coating, :140-248) */
+    AEFDTD_OP_MESH = 11         /* x, y, z (recorded, unused as in the reference), scale, mesh number in
+                                   aefdtd_structure_desc.meshes (Add_Mesh, :396-440) */
 };
+/* A triangle mesh as Add_Mesh reads it from an OBJ file (obj_file_load,
+ * mesh_tools.h:103-152: quads split into (0,1,2) and (0,2,3)): vertex
+ * coordinates before scaling, three 0-based vertex numbers per triangle. A
+ * point inside the scaled vertices' box is inside the mesh when a ray from
+ * it crosses the triangles an odd number of times (Moller-Trumbore,
+ * ray_intersect.h:121-166). */
+typedef struct aefdtd_mesh {
+    const double *vertices;
+    const int32_t *faces;
+    int32_t n_vertices, n_faces;
+} aefdtd_mesh;
 typedef struct aefdtd_structure_op {
     int32_t kind;
     int32_t mat_index;
     double p[16];
 } aefdtd_structure_op;
 /* Structure-wide settings: default material, periodic images (loop) and
- * mirror flips (flip) per axis, and the nominal lengths lx, ly, lz that both
- * use and that the coatings read. */
+ * mirror flips (flip) per axis, the nominal lengths lx, ly, lz that both use
+ * and that the coatings read, and the meshes that AEFDTD_OP_MESH refers to. */
 typedef struct aefdtd_structure_desc {
     int32_t default_material;
     int32_t periodic[3];
     int32_t flip[3];
-    int32_t reserved;
+    int32_t n_meshes;
     double lengths[3];
+    const aefdtd_mesh *meshes;
 } aefdtd_structure_desc;
 /* Tags every cell corner (i*dx, j*dy, k*dz) of an nx*ny*nz structure grid
  * with the material of the last operation containing it, else the default

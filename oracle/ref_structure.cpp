@@ -9,14 +9,18 @@
  * Structure::finalize's closing loop (structure.cpp:215-220) links and
  * precomputes them, and Structure::discretize (structure.cpp:94-113) tags the
  * grid. The nominal lengths, which a script sets as Lua globals, are written
- * into the object directly. */
+ * into the object directly. A mesh is written to a temporary OBJ file with
+ * round-trip precision and read back by Add_Mesh's own loader. */
 #include <lua_base.h>
 #include <mesh_base.h>
 #include <octree.h>
 #include <Eigen/Eigen>
 
 #include <cstdint>
+#include <cstdio>
 #include <filesystem>
+#include <string>
+#include <unistd.h>
 #include <vector>
 
 #define private public
@@ -62,6 +66,30 @@ extern "C" int aeref_discretize(int32_t nx, int32_t ny, int32_t nz, double dx, d
                 o = new Add_Coating(Degree(p[0]), Degree(p[1]), p[2], p[3], int(p[4]), m);
                 break;
             case AEFDTD_OP_CONF_COATING: o = new Add_Conf_Coating(p[0], p[1], int(p[2]), m); break;
+            case AEFDTD_OP_MESH: {
+                const int mi = int(p[4]);
+                if (mi < 0 || mi >= d->n_meshes) {
+                    for (Structure_OP *x : made) delete x;
+                    return 3;
+                }
+                const aefdtd_mesh &mesh = d->meshes[mi];
+                char path[] = "/tmp/aeref_meshXXXXXX";
+                const int fd = mkstemp(path);
+                if (fd < 0) {
+                    for (Structure_OP *x : made) delete x;
+                    return 4;
+                }
+                FILE *f = fdopen(fd, "w");
+                for (int v = 0; v < mesh.n_vertices; v++)
+                    std::fprintf(f, "v %.17g %.17g %.17g\n", mesh.vertices[3 * v], mesh.vertices[3 * v + 1],
+                                 mesh.vertices[3 * v + 2]);
+                for (int t = 0; t < mesh.n_faces; t++)
+                    std::fprintf(f, "f %d %d %d\n", mesh.faces[3 * t] + 1, mesh.faces[3 * t + 1] + 1, mesh.faces[3 * t + 2] + 1);
+                std::fclose(f);
+                o = new Add_Mesh(p[0], p[1], p[2], p[3], std::filesystem::path(path), m);
+                std::remove(path);
+                break;
+            }
             default:
                 for (Structure_OP *x : made) delete x;
                 return 2;
