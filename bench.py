@@ -40,6 +40,36 @@ def workload(precision):
                            nl=201, precision=precision)
 
 
+def rta(spec):
+    """R, T, A per wavelength from the spectdata_norm2 columns: |r|^2 and
+    |t|^2 n_sub/n_sup of both polarisation components."""
+    r = spec[:, 5] + spec[:, 8]
+    t = spec[:, 11] + spec[:, 14]
+    return r, t, 1.0 - r - t
+
+
+def spectrum_error_sample():
+    """FP32 against FP64 (the FP64 path is bit-identical to the reference
+    core) on complete runs of the n=1.5 slab (64x64x128, 4000 steps, 61
+    wavelengths) and of the bench's gold-sphere cell (20000 steps, 201
+    wavelengths): the largest absolute R, T and A differences."""
+    import numpy as np
+    from aether_b200 import _abi as A
+    from aether_b200 import configs as CF
+    from aether_b200 import fdtd
+    out = {}
+    for name, make in (("slab_64x64x128_4000_steps", lambda p: CF.slab_scene(precision=p)),
+                       ("gold_sphere_128x128x256_20000_steps", workload)):
+        res = {}
+        for prec in (A.FP32, A.FP64):
+            res[prec] = rta(fdtd.run(make(prec), want_fields=False)["spectra"])
+        d = [float(np.max(np.abs(res[A.FP32][q] - res[A.FP64][q]))) for q in range(3)]
+        out[name] = {"max_abs_dR": d[0], "max_abs_dT": d[1], "max_abs_dA": d[2]}
+        log(f"[accuracy] {name}: |dR| {d[0]:.2e} |dT| {d[1]:.2e} |dA| {d[2]:.2e}")
+    out["source"] = "FP32 vs FP64 spectra of complete runs; FP64 fields are bit-identical to the reference core"
+    return out
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -493,6 +523,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the config-4 batch sample")
     ap.add_argument("--no-large", action="store_true", help="skip the config-3 large-grid sample")
     ap.add_argument("--no-serving", action="store_true", help="skip the config-5 serving sample")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the FP32-vs-FP64 spectrum error runs")
     ap.add_argument("--profile", choices=["fp32", "fp64"], help="direct-launch run for ncu (no timing)")
     ap.add_argument("--segments", type=int, default=2)
     ap.add_argument("--profile-grid", choices=["bench", "large"], default="bench",
@@ -560,6 +591,8 @@ def main():
                        "d2h_bytes_per_step": d2h,
                        "step": "one complete 20000-step job from host buffers (geometry upload, "
                                "all steps, spectra read back)", "seconds": dt}
+    if not args.no_accuracy:
+        line["spectrum_error"] = spectrum_error_sample()
     if not args.no_large:
         line["large_grid"] = large_grid_sample()
     if not args.no_batch:
