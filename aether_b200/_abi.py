@@ -118,7 +118,7 @@ class JobDesc(C.Structure):
     _fields_ = [
         ("grid", C.POINTER(GridDesc)), ("map", C.POINTER(C.c_uint32)), ("map_count", C.c_size_t),
         ("materials", C.POINTER(MaterialDesc)), ("n_materials", C.c_int32),
-        ("normal", C.POINTER(NormalDesc)), ("steps", C.c_int32),
+        ("normal", C.POINTER(NormalDesc)), ("steps", C.c_int32), ("cc_step", C.c_int32), ("cc_coeff", C.c_double),
     ]
 
 
@@ -126,6 +126,7 @@ class JobInfo(C.Structure):
     _fields_ = [
         ("state", C.c_int32), ("steps", C.c_int32), ("cells", C.c_int64), ("est_bytes", C.c_int64),
         ("bytes", C.c_int64), ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double),
+        ("stop_step", C.c_int32), ("reserved", C.c_int32),
     ]
 
 

@@ -338,24 +338,39 @@ template <typename T, typename Tid> void aefdtd_batch::enqueue_steps(BatchSubset
     StepArgs<T, Tid> se, sh;
     if (u.solo) m0->make_step_args(se, sh, m0->tables.as<StepScalars>());
     const int4 *mit = m0->items.as<int4>();
+    // members with the energy-mode completion sensor: the energy of every step
+    std::vector<aefdtd_sim *> cc;
+    for (aefdtd_sim *s : u.members)
+        if (s->cc_coeff > 0) cc.push_back(s);
+    const bool side = u.nblk > 0 || !cc.empty();
     for (int q = 0; q < L; q++) {
         se.q = sh.q = q;
         if (u.solo) run_groups(m0->wsE, ln, [&](int g, cudaStream_t st) { launch_e_group(se, mit, m0->wsE, g, st); });
         else run_groups(u.wsE, ln, [&](int g, cudaStream_t st) { launch_e_group_batch(ea, q, it, u.wsE, g, st); });
-        // plane sums read E only: beside the H half-step
-        if (u.nblk > 0) {
+        // plane sums and completion energies read E only: beside the H half-step
+        if (side) {
             AE_CUDA(cudaEventRecord(ln.ev_sf, ln.stream));
             AE_CUDA(cudaStreamWaitEvent(ln.side_s, ln.ev_sf, 0));
-            launch_plane_partial_batch(sa, blk, u.nblk, q, ln.side_s);
+            if (u.nblk > 0) launch_plane_partial_batch(sa, blk, u.nblk, q, ln.side_s);
+            for (aefdtd_sim *s : cc)
+                launch_energy_partial(s->F[0].as<T>(), s->F[1].as<T>(), s->F[2].as<T>(),
+                                      (long long)s->Nx * s->Ny * s->Nz, s->cc_nb,
+                                      s->cc_partial.as<double>() + size_t(q) * s->cc_nb, ln.side_s);
             AE_CUDA(cudaEventRecord(ln.ev_sj, ln.side_s));
         }
         if (u.solo) run_groups(m0->wsH, ln, [&](int g, cudaStream_t st) { launch_h_group(sh, mit, m0->wsH, g, st); });
         else run_groups(u.wsH, ln, [&](int g, cudaStream_t st) { launch_h_group_batch(ha, q, it, u.wsH, g, st); });
-        if (u.nblk > 0) AE_CUDA(cudaStreamWaitEvent(ln.stream, ln.ev_sj, 0));
-        launches += groups + (u.nblk > 0);
+        if (side) AE_CUDA(cudaStreamWaitEvent(ln.stream, ln.ev_sj, 0));
+        launches += groups + (u.nblk > 0) + cc.size();
     }
     if (u.nplane > 0) {
         launch_plane_reduce_batch(sa, (int)u.members.size(), L, ln.stream);
+        launches++;
+    }
+    for (aefdtd_sim *s : cc) {
+        // hist[t] for the chunk's steps (the member's table holds the chunk's first step)
+        launch_energy_reduce(s->cc_partial.as<double>(), s->cc_nb, s->tables.as<StepScalars>(), s->cc_hist.as<double>(), L,
+                             ln.stream);
         launches++;
     }
 }
@@ -419,6 +434,58 @@ template <typename T, typename Tid> void aefdtd_batch::ensure_history() {
             s->graphs_dirty = true;
             u.release(dev_bytes);
         }
+    // completion energies: a history for the whole budget and one chunk of partials
+    for (auto &u : subsets)
+        for (aefdtd_sim *s : u.members) {
+            const BatchMember &m = rec(s);
+            if (s->cc_coeff <= 0) continue;
+            if (!s->cc_partial.p) {
+                s->cc_nb = std::max(1, std::min(2 * 148, (int)(((long long)s->Nx * s->Ny * s->Nz + 4095) / 4096)));
+                s->cc_partial.alloc(size_t(s->seg_len) * s->cc_nb * 8, s->dev_bytes);
+                u.release(dev_bytes);
+            }
+            if (s->tstep + m.remaining > s->cc_cap) {
+                DBuf nb;
+                const int cap = s->tstep + m.remaining;
+                nb.alloc(size_t(cap) * 8, s->dev_bytes);
+                if (s->cc_hist.p)
+                    AE_CUDA(cudaMemcpy(nb.p, s->cc_hist.p, size_t(s->cc_cap) * 8, cudaMemcpyDeviceToDevice));
+                s->cc_hist.release(s->dev_bytes);
+                s->cc_hist = nb;
+                s->cc_cap = cap;
+                s->graphs_dirty = true;
+                u.release(dev_bytes);
+            }
+        }
+}
+
+// CompletionSensor::completion_check (energy mode, s_completion.cpp:39-43,
+// 121-130) at every check step t (t % cc_step == 0) that the member passed in
+// its last segment, in order, as aefdtd_sim::completion_check does after each
+// check step of a single run. A member that completes at t has its budget
+// set to zero; the steps it ran past t (at most one segment) do not enter its
+// results, which are read up to t (aefdtd_get_normal_spectra uses cc_stop).
+static bool batch_completion_check(aefdtd_sim *s, int t0, int t1, cudaStream_t st) {
+    const int first = (t0 + s->cc_step - 1) / s->cc_step * s->cc_step;
+    if (first >= t1) return false;
+    AE_CUDA(cudaStreamSynchronize(st));
+    for (int t = first; t < t1; t += s->cc_step) {
+        const int n = t + 1 - s->cc_read;
+        if (n > 0) {
+            std::vector<double> e(n);
+            AE_CUDA(cudaMemcpy(e.data(), s->cc_hist.as<double>() + s->cc_read, n * sizeof(double), cudaMemcpyDeviceToHost));
+            for (double x : e) s->cc_max = std::max(s->cc_max, x);
+            s->cc_last = e.back();
+            s->cc_read = t + 1;
+        }
+        if (t + 1 < 2 * std::max(s->Nx, std::max(s->Ny, s->Nz))) continue;
+        if (s->cc_last / s->cc_max < s->cc_coeff) {
+            s->cc_done = true;
+            s->cc_stop = t;
+            return true;
+        }
+    }
+    return false;
 }
 
 // Each subset runs up to max_steps steps in segments of at most seg_len, and
@@ -440,7 +507,15 @@ template <typename T, typename Tid> int aefdtd_batch::advance(int max_steps) {
             int L = std::min(seg_len, max_steps - done[k]);
             for (aefdtd_sim *s : u.members) L = std::min(L, rec(s).remaining);
             if (L <= 0) { done[k] = -done[k] - 1; continue; }
+            std::vector<int> t0;
+            for (aefdtd_sim *s : u.members) t0.push_back(s->tstep);
             run_segment<T, Tid>(u, L, lanes[k % n_lanes]);
+            for (size_t i = 0; i < u.members.size(); i++) {
+                aefdtd_sim *s = u.members[i];
+                if (s->cc_coeff > 0 && !s->cc_done &&
+                    batch_completion_check(s, t0[i], s->tstep, lanes[k % n_lanes].stream))
+                    rec(s).remaining = 0;
+            }
             done[k] += L;
             most = std::max(most, done[k]);
             bool finished = false;
@@ -645,7 +720,7 @@ aefdtd_status aefdtd_batch_add(aefdtd_batch *b, aefdtd_sim *s, int32_t steps) {
         if (!s->map_set) fail(AEFDTD_NOT_READY, "no material map");
         if (s->g.mode == AEFDTD_MODE_NORMAL && !s->normal) fail(AEFDTD_NOT_READY, "normal mode needs aefdtd_setup_normal");
         if (!s->sensors.empty()) fail(AEFDTD_BAD_ARG, "batch members carry no planar DFT sensors (normal-mode plane sums only)");
-        if (s->cc_coeff > 0) fail(AEFDTD_BAD_ARG, "batch members run without a completion sensor (fixed step budgets)");
+        if (s->cc_coeff > 0 && s->ccft) fail(AEFDTD_BAD_ARG, "batch members take the energy-mode completion sensor only");
         if (!s->fmaps.empty()) fail(AEFDTD_BAD_ARG, "batch members carry no field sensors");
         if (s->g.mode == AEFDTD_MODE_OBLIQUE) fail(AEFDTD_BAD_ARG, "batch members run normal or custom mode only");
         if (s->Nz >= 32768) fail(AEFDTD_BAD_ARG, "batch members need Nz < 32768 (k1 << 16 in an int32 item)");
@@ -664,7 +739,7 @@ aefdtd_status aefdtd_batch_add(aefdtd_batch *b, aefdtd_sim *s, int32_t steps) {
         AE_CUDA(cudaStreamSynchronize(s->stream));
         BatchMember m;
         m.sim = s;
-        m.remaining = steps;
+        m.remaining = (s->cc_coeff > 0 && s->cc_done) ? 0 : steps;
         m.cls = b->class_key(s);
         auto it = b->classes.find(m.cls);
         if (it == b->classes.end()) {

@@ -36,6 +36,8 @@ struct Job {
     std::vector<aefdtd_material_desc> mats;
     aefdtd_normal_desc nd{};
     int steps = 0;
+    double cc_coeff = 0;
+    int cc_step = 500, stop = -1;
     size_t est = 0, bytes = 0;
     long long cells = 0;
     aefdtd_sim *sim = nullptr;
@@ -96,6 +98,7 @@ size_t estimate_job_bytes(const Job &j) {
     const int seg = g.dft_block > 0 ? g.dft_block : 64;
     b += size_t(std::max(std::max(g.nt, j.steps), 1024)) * 12 * 8;        // plane-sum history
     b += size_t(seg) * kPlaneBlocks * 12 * 8;                               // plane-sum partials
+    if (j.cc_coeff > 0) b += size_t(j.steps) * 8 + size_t(seg) * 2 * 148 * 8;  // completion energies
     b += N / 16 + 2 * sizeof(StepScalars) * seg + (1 << 16);                // work lists, tables, small
     return b + b / 10;
 }
@@ -133,6 +136,12 @@ int aefdtd_server::retire() {
         j.spectra.assign(size_t(15) * j.nd.nl, 0.0);
         aefdtd_status st = aefdtd_get_normal_spectra(s, j.spectra.data(), j.nd.nl);
         j.t_done = now();
+        if (j.cc_coeff > 0) {
+            int32_t cdone = 0, cstop = -1;
+            double ratio = 0;
+            aefdtd_get_completion(s, &cdone, &cstop, &ratio);
+            j.stop = cdone ? cstop : -1;
+        }
         if (st == AEFDTD_OK) {
             j.state = AEFDTD_JOB_DONE;
         } else {
@@ -173,6 +182,7 @@ void aefdtd_server::admit() {
         if (st == AEFDTD_OK) st = aefdtd_set_material_map(s, j.map.data(), j.map.size());
         for (size_t m = 0; st == AEFDTD_OK && m < j.mats.size(); m++) st = aefdtd_set_material(s, (uint32_t)m, &j.mats[m]);
         if (st == AEFDTD_OK) st = aefdtd_setup_normal(s, &j.nd);
+        if (st == AEFDTD_OK && j.cc_coeff > 0) st = aefdtd_set_completion(s, j.cc_coeff, j.cc_step);
         if (st == AEFDTD_OK && aefdtd_batch_add(batch, s, j.steps) != AEFDTD_OK) {
             st = AEFDTD_BAD_ARG;
             j.error = aefdtd_batch_last_error(batch);
@@ -291,6 +301,9 @@ aefdtd_status aefdtd_server_submit(aefdtd_server *v, const aefdtd_job_desc *jd, 
         j.mats.assign(jd->materials, jd->materials + jd->n_materials);
         j.nd = *jd->normal;
         j.steps = jd->steps;
+        if (!(jd->cc_coeff >= 0) || jd->cc_step < 0) fail(AEFDTD_BAD_ARG, "bad completion settings");
+        j.cc_coeff = jd->cc_coeff;
+        j.cc_step = jd->cc_step > 0 ? jd->cc_step : 500;
         j.est = estimate_job_bytes(j);
         j.t_submit = v->now();
         v->jobs.push_back(std::move(j));
@@ -328,6 +341,7 @@ aefdtd_status aefdtd_server_job_info(aefdtd_server *v, int32_t job, aefdtd_job_i
         info->t_admit = j.t_admit;
         info->t_done = j.t_done;
         info->steps = j.steps;
+        info->stop_step = j.stop;
     });
 }
 

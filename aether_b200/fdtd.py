@@ -433,8 +433,10 @@ class Server:
     def __exit__(self, *a):
         self.close()
 
-    def submit(self, scene, steps=None) -> int:
-        """Queues a normal-incidence Scene for `steps` steps (default its own)."""
+    def submit(self, scene, steps=None, completion=None) -> int:
+        """Queues a normal-incidence Scene for `steps` steps (default its own).
+        completion=(coeff, check_every): energy-mode completion sensor; the
+        job then ends at its completion step (info()['stop_step'])."""
         m = np.ascontiguousarray(scene.map, dtype=np.uint32).ravel()
         mats = (A.MaterialDesc * len(scene.materials))(*scene.materials)
         g = scene.grid
@@ -447,6 +449,8 @@ class Server:
         jd.n_materials = len(scene.materials)
         jd.normal = C.pointer(nd)
         jd.steps = int(steps if steps is not None else scene.nsteps)
+        if completion is not None:
+            jd.cc_coeff, jd.cc_step = float(completion[0]), int(completion[1])
         jid = C.c_int32(-1)
         self._c(self._lib.aefdtd_server_submit(self._h, C.byref(jd), C.byref(jid)))
         self.nl[jid.value] = nd.nl

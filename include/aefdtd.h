@@ -515,7 +515,10 @@ typedef struct aefdtd_job_desc {
     const aefdtd_material_desc *materials;  /* indexed by the map */
     int32_t n_materials;
     const aefdtd_normal_desc *normal;
-    int32_t steps;
+    int32_t steps;                          /* step budget (the driver's Nt) */
+    int32_t cc_step;                        /* completion check period (0 -> 500) */
+    double cc_coeff;                        /* > 0: energy-mode completion sensor (auto_tsteps(Nt, cc_step,
+                                               cc_coeff)); the job ends at its completion step */
 } aefdtd_job_desc;
 
 typedef struct aefdtd_job_info {
@@ -525,6 +528,8 @@ typedef struct aefdtd_job_info {
     int64_t est_bytes;        /* footprint estimate used for admission */
     int64_t bytes;            /* device bytes held while running */
     double t_submit, t_admit, t_done;   /* seconds since server creation; -1 if not yet */
+    int32_t stop_step;        /* completion step t of a job with a completion sensor, else -1 */
+    int32_t reserved;
 } aefdtd_job_info;
 
 typedef struct aefdtd_server_stats {

@@ -154,3 +154,42 @@ def test_member_refuses_direct_steps_and_leaves_on_destroy():
         assert b.info()["n_members"] == 1
         assert b.run(10 ** 6) == 64
     s0.close()
+
+
+def alone_completion(scene, budget, coeff, every):
+    with fdtd.build_simulation(scene) as s:
+        s.set_completion(coeff, every)
+        s.step(budget)
+        return s.completion(), s.normal_spectra()
+
+
+@pytest.mark.parametrize("opts", [dict(), dict(l2_budget_bytes=-1), dict(graph_steps=7)])
+def test_completion_inside_a_batch_stops_where_alone_stops(opts):
+    """Members with the energy-mode completion sensor: each completes at the
+    same step as alone (checks every 40 steps, not aligned with the batch's
+    segments) and its spectra, read up to that step, are bit-identical; a
+    member without the sensor runs its whole budget beside them."""
+    scenes = cells(11, n=3, nsteps=3000)
+    budget, coeff, every = 3000, 5e-2, 40
+    want = [alone_completion(sc, budget, coeff, every) for sc in scenes]
+    assert all(w[0][0] for w in want), "the cells must complete inside the budget"
+    plain = cells(12, n=1, nsteps=700)[0]
+    sims = [fdtd.build_simulation(sc) for sc in scenes]
+    for s in sims:
+        s.set_completion(coeff, every)
+    ps = fdtd.build_simulation(plain)
+    with fdtd.Batch(**opts) as b:
+        for s in sims:
+            b.add(s, budget)
+        b.add(ps, 700)
+        b.run(10 ** 6)
+        assert len(b.finished()) == len(sims) + 1
+        for s, ((done, stop, ratio), spec) in zip(sims, want):
+            got = s.completion()
+            assert got[0] and got[1] == stop and got[2] == ratio
+            assert s.dims().step > stop and s.dims().step <= stop + 1 + 64
+            assert np.array_equal(s.normal_spectra(), spec)
+        assert ps.dims().step == 700
+        assert np.array_equal(ps.plane_sums(), alone(plain, 700)[1])
+    for s in sims + [ps]:
+        s.close()

@@ -95,3 +95,24 @@ def test_job_above_budget_fails_alone():
         assert all(v.info(j)["state"] == A.JOB_FAILED for j in ids)
         with pytest.raises(Exception):
             v.spectra(ids[0])
+
+
+def test_jobs_with_completion_end_at_their_completion_step():
+    """auto_tsteps for served jobs: each job stops at the step its completion
+    sensor gives alone, and its spectra are the ones of that run."""
+    rng = np.random.default_rng(21)
+    scs = [CF.metasurface_cell(rng, nz_total=64, pml=8, nsteps=3000, nl=21, precision=A.FP64,
+                               period_range=(80 * NM, 180 * NM), flux_planes=False) for _ in range(3)]
+    budget, coeff, every = 3000, 5e-2, 40
+    with fdtd.Server() as v:
+        ids = [v.submit(sc, budget, completion=(coeff, every)) for sc in scs]
+        v.drain()
+        got = [(v.info(j), v.spectra(j)) for j in ids]
+    for sc, (info, spec) in zip(scs, got):
+        assert info["state"] == A.JOB_DONE
+        with fdtd.build_simulation(sc) as s:
+            s.set_completion(coeff, every)
+            s.step(budget)
+            done, stop, _ = s.completion()
+            assert done and info["stop_step"] == stop
+            assert np.array_equal(spec, s.normal_spectra())
