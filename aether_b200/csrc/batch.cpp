@@ -12,9 +12,10 @@
 //    state fits an L2 budget (126 MB of L2 on B200; default 48 MiB, tuned).
 //    A subset runs a whole segment of steps before the next subset starts, so
 //    after its first step most of its state is served from L2. Lanes run that
-//    many subsets concurrently (default 2: measured on 96 config-4 cells, two
+//    many subsets concurrently (default 2: measured on 96 nanodisk unit cells of up to
+//    120 x 120 x 200, two
 //    resident cells at a time 57.8 Gcell/s, one 47.0, three 55.4).
-//  * Lone members. A subset of one member (one config-4 cell fills the
+//  * Lone members. A subset of one member (one such unit cell fills the
 //    default budget) runs the member's own single-simulation kernels and work
 //    lists (two-cell items, L2-ordered H lists, arguments as launch
 //    parameters).

@@ -248,7 +248,7 @@ aefdtd_status aefdtd_server_create(const aefdtd_server_opts *opts, aefdtd_server
         } else {
             v->opts.abi_version = AEFDTD_ABI_VERSION;
         }
-        // defaults measured on the config-5 stream (32 jobs, 10% large cells):
+        // defaults measured on a Poisson stream of 32 unit-cell jobs, 10% large cells:
         // 256 steps per poll and one merged subset per size class gave p50 5.2 s,
         // p99 16.4 s, 36.5 Gcell/s, against 7.5 s, 19.6 s, 33.5 Gcell/s for 64 steps
         // and 48 MiB subsets

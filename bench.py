@@ -330,7 +330,7 @@ def reference_arm(args):
 
 
 def batch_sample(n_cells=512, steps=256, seed=2024):
-    """Config 4: n_cells seeded nanodisk unit cells (period U(200, 600) nm at
+    """Batch: n_cells seeded nanodisk unit cells (period U(200, 600) nm at
     5 nm, z = 200 cells with 16-cell CPML, gold or n U(1.8, 3.5) disk on
     n = 1.45, 101 wavelengths) advanced as one FP32 batch. Fixed batch settings
     (tile 32 x 4, 8 planes per item, 48 MiB subsets, two at a time, 32-step graphs); a bounded sample of
@@ -380,7 +380,7 @@ def batch_sample(n_cells=512, steps=256, seed=2024):
             single_cells += sc.cells * steps
         sc.grid.precision = A.FP32
     g64 = single_cells / single_s / 1e9
-    return {"workload": f"config 4: {n_cells} nanodisk unit cells, FP32, {cells / 1e6:.1f} M cells in total",
+    return {"workload": f"batch: {n_cells} nanodisk unit cells, FP32, {cells / 1e6:.1f} M cells in total",
             "gcells": g, "sims_per_s": n_cells / (dt * 8000.0 / done), "sample_steps": done, "seconds": dt,
             "subsets": info["n_subsets"], "setup_seconds": setup,
             "fp64_single_gcells": g64, "over_fp64_single_same_cells": g / g64,
@@ -389,7 +389,7 @@ def batch_sample(n_cells=512, steps=256, seed=2024):
 
 
 def serving_sample(n_jobs=32, rate=1.5, seed=77, fp64_check=2, **server_opts):
-    """Config 5: a seeded Poisson stream (rate jobs/s) of config-4 unit cells
+    """Serving: a seeded Poisson stream (rate jobs/s) of the batch sample's unit cells
     plus 10% large cells (period U(640, 1280) nm -> up to 256 x 256 cells,
     z = 384), step budgets U(4000, 20000), 101 wavelengths, FP32, served with
     continuous batching under an 80%-of-HBM budget. Jobs are submitted when
@@ -441,7 +441,7 @@ def serving_sample(n_jobs=32, rate=1.5, seed=77, fp64_check=2, **server_opts):
             ref = s.normal_spectra()
         err = max(err, float(np.max(np.abs(spectra[k][:, 1:3] - ref[:, 1:3]))))
     cu = sum(sc.cells * steps for sc, steps, _ in reqs)
-    return {"workload": f"config 5: {n_jobs} Poisson arrivals at {rate}/s, 10% large cells, steps U(4000, 20000), "
+    return {"workload": f"serving: {n_jobs} Poisson arrivals at {rate}/s, 10% large cells, steps U(4000, 20000), "
                         "FP32, 80% HBM budget",
             "p50_s": st["p50_s"], "p99_s": st["p99_s"], "mean_s": st["mean_s"], "sims_per_s": st["sims_per_s"],
             "gcells": st["gcells_per_s"], "elapsed_s": st["elapsed_s"], "peak_bytes": st["peak_bytes"],
@@ -450,7 +450,7 @@ def serving_sample(n_jobs=32, rate=1.5, seed=77, fp64_check=2, **server_opts):
 
 
 def large_grid_sample(steps=128, seed=1234):
-    """Config 3: 1024 x 1024 x 512 cells at 5 nm, 32-cell CPML on all six
+    """Large grid: 1024 x 1024 x 512 cells at 5 nm, 32-cell CPML on all six
     faces, 500 seeded dielectric spheres (r U(20, 80) nm, eps U(2, 12)) plus 50
     Lorentz spheres sharing one material, an oscillator at the centre (600 nm,
     300 nm band), custom mode. FP32 and FP64: `steps` steps after a 64-step
@@ -463,7 +463,7 @@ def large_grid_sample(steps=128, seed=1234):
     from aether_b200 import metrics as MT
     peak, _ = measured_peaks()
     sc = CF.random_spheres_scene(seed=seed, precision=A.FP32)
-    out = {"workload": "config 3: 1024x1024x512 @5nm, 32-cell CPML x6, 500 dielectric + 50 Lorentz spheres, "
+    out = {"workload": "large grid: 1024x1024x512 @5nm, 32-cell CPML x6, 500 dielectric + 50 Lorentz spheres, "
                        "oscillator source"}
     for name, prec in (("fp32", A.FP32), ("fp64", A.FP64)):
         sc.grid.precision = prec
@@ -500,7 +500,7 @@ def profile_run(args):
     from aether_b200 import fdtd
     prec = A.FP32 if args.profile == "fp32" else A.FP64
     if args.profile_grid == "large":
-        # config 3's scene at 384 x 384 x 192 (CPML on six faces, spheres, oscillator)
+        # the large grid's scene at 384 x 384 x 192 (CPML on six faces, spheres, oscillator)
         sc = CF.random_spheres_scene(n_total=(384, 384, 192), n_dielectric=60, n_lorentz=6, seed=1234,
                                      precision=prec)
     else:
@@ -520,14 +520,14 @@ def main():
     ap.add_argument("--impl", default="aefdtd")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--no-batch", action="store_true", help="skip the config-4 batch sample")
-    ap.add_argument("--no-large", action="store_true", help="skip the config-3 large-grid sample")
-    ap.add_argument("--no-serving", action="store_true", help="skip the config-5 serving sample")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batch sample (512 nanodisk unit cells)")
+    ap.add_argument("--no-large", action="store_true", help="skip the 1024x1024x512 large-grid sample")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving sample (Poisson stream of unit cells)")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the FP32-vs-FP64 spectrum error runs")
     ap.add_argument("--profile", choices=["fp32", "fp64"], help="direct-launch run for ncu (no timing)")
     ap.add_argument("--segments", type=int, default=2)
     ap.add_argument("--profile-grid", choices=["bench", "large"], default="bench",
-                    help="--profile on the bench grid or on config 3's scene at 384 x 384 x 192")
+                    help="--profile on the bench grid or on the large grid's scene at 384 x 384 x 192")
     args = ap.parse_args()
     if args.profile:
         profile_run(args)

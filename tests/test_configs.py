@@ -1,12 +1,12 @@
-"""BASELINE configurations at full size.
+"""The benchmark workloads at full size.
 
-Config 1 (64x64x128 at 5 nm, n = 1.5 slab, 16-cell CPML on z, 4000 steps, 61
+The slab (64x64x128 at 5 nm, n = 1.5 slab, 16-cell CPML on z, 4000 steps, 61
 wavelengths, flux planes above and below): the FP64 GPU path against the
 reference core compiled from source, fields bit-identical, spectra and flux
-to 1e-10 relative. The CPML grading is the reference's (order 4); BASELINE's
+to 1e-10 relative. The CPML grading is the reference's (order 4); grading
 order 3 is the grid descriptor's pml_m, outside what the reference can run.
 
-Configs 1 and 2 (the 128x128x256 dispersive unit cell, 20000 steps, 201
+The slab and the 128x128x256 dispersive unit cell (gold sphere, 20000 steps, 201
 wavelengths): the FP32 path's R/T spectra against the FP64 path (itself
 bit-identical to the reference on every golden scene) within 1e-4 absolute,
 flux within 1e-3 relative. The measured errors are printed."""
@@ -36,7 +36,7 @@ def rel(a, b):
     return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
 
 
-def test_config1_fp64_full_size_matches_reference():
+def test_slab_fp64_full_size_matches_reference():
     if not oracle_lib.available("ref"):
         pytest.skip("reference core not built")
     sc = CF.slab_scene(precision=A.FP64)
@@ -56,9 +56,9 @@ def rt_error(scene_fn):
     return d, fl
 
 
-@pytest.mark.parametrize("name", ["config1", "config2"])
+@pytest.mark.parametrize("name", ["slab", "gold_sphere"])
 def test_fp32_rt_error_against_fp64(name):
-    if name == "config1":
+    if name == "slab":
         fn = lambda p: CF.slab_scene(precision=p)
     else:
         fn = lambda p: CF.sphere_scene(nx=128, ny=128, nz_total=256, dx=2.5e-9, pml=24, radius=40e-9,
