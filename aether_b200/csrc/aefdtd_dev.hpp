@@ -47,7 +47,8 @@ struct StepScalars {
     double inj_hA, inj_hB;   // H plane injection: added to Hx / subtracted from Hy
     double src[4];           // oscillator values
     double tb, taper;        // plane-sum sample time (t + 1/2) Dt and tapering
-    int step, pad;           // global step index
+    int step;                // global step index
+    int snap;                // FT-mode completion: ring snapshot slot after this step (-1: none)
 };
 
 // Parameters of one fused half-step launch. Pointers are device pointers.
@@ -220,6 +221,7 @@ template <typename T> struct CcFtArgs {
     int q;
     double2 *acc;                   // [np][3]
     double *ring;
+    double *snap;                   // ring snapshots [slot][6][np][n_avg] (batch members), or null
 };
 
 struct PhasorArgs {

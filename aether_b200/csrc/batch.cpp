@@ -353,10 +353,28 @@ template <typename T, typename Tid> void aefdtd_batch::enqueue_steps(BatchSubset
             AE_CUDA(cudaEventRecord(ln.ev_sf, ln.stream));
             AE_CUDA(cudaStreamWaitEvent(ln.side_s, ln.ev_sf, 0));
             if (u.nblk > 0) launch_plane_partial_batch(sa, blk, u.nblk, q, ln.side_s);
-            for (aefdtd_sim *s : cc)
-                launch_energy_partial(s->F[0].as<T>(), s->F[1].as<T>(), s->F[2].as<T>(),
-                                      (long long)s->Nx * s->Ny * s->Nz, s->cc_nb,
-                                      s->cc_partial.as<double>() + size_t(q) * s->cc_nb, ln.side_s);
+            for (aefdtd_sim *s : cc) {
+                if (s->ccft) {
+                    // FT mode: the probes' running transforms, with a ring snapshot at check steps
+                    const CompletionFT &c = *s->ccft;
+                    CcFtArgs<T> fa{};
+                    fa.Nx = s->Nx; fa.Ny = s->Ny; fa.Nz = s->Nz; fa.NxNy = (long long)s->Nx * s->Ny;
+                    fa.Ex = s->F[0].as<T>(); fa.Ey = s->F[1].as<T>(); fa.Ez = s->F[2].as<T>();
+                    fa.np = c.np; fa.n_avg = c.n_avg; fa.step0 = c.step0;
+                    fa.pts = c.dpts.as<int>();
+                    fa.coef = c.ctab.as<double2>();
+                    fa.sc = s->tables.as<StepScalars>();
+                    fa.q = q;
+                    fa.acc = c.acc.as<double2>();
+                    fa.ring = c.ring.as<double>();
+                    fa.snap = c.snap.as<double>();
+                    launch_completion_ft(fa, ln.side_s);
+                } else {
+                    launch_energy_partial(s->F[0].as<T>(), s->F[1].as<T>(), s->F[2].as<T>(),
+                                          (long long)s->Nx * s->Ny * s->Nz, s->cc_nb,
+                                          s->cc_partial.as<double>() + size_t(q) * s->cc_nb, ln.side_s);
+                }
+            }
             AE_CUDA(cudaEventRecord(ln.ev_sj, ln.side_s));
         }
         if (u.solo) run_groups(m0->wsH, ln, [&](int g, cudaStream_t st) { launch_h_group(sh, mit, m0->wsH, g, st); });
@@ -369,6 +387,7 @@ template <typename T, typename Tid> void aefdtd_batch::enqueue_steps(BatchSubset
         launches++;
     }
     for (aefdtd_sim *s : cc) {
+        if (s->ccft) continue;
         // hist[t] for the chunk's steps (the member's table holds the chunk's first step)
         launch_energy_reduce(s->cc_partial.as<double>(), s->cc_nb, s->tables.as<StepScalars>(), s->cc_hist.as<double>(), L,
                              ln.stream);
@@ -388,6 +407,24 @@ template <typename T, typename Tid> void aefdtd_batch::run_segment(BatchSubset &
         const int C = graph ? graph_steps : L - done;
         for (aefdtd_sim *s : u.members) {
             for (int q = 0; q < C; q++) s->fill_scalars(s->tstep + q, q, host[q]);
+            if (s->ccft && s->cc_coeff > 0) {
+                CompletionFT &c = *s->ccft;
+                for (int q = 0; q < C; q++)
+                    if ((s->tstep + q) % s->cc_step == 0) host[q].snap = ((s->tstep + q) / s->cc_step) % c.nsnap;
+                // CompletionSensor::deep_feed's phases e^{i w step Dt} (s_completion.cpp:149)
+                c.rows.resize(size_t(C) * c.np * 2);
+                const std::complex<double> Im(0, 1);
+                for (int q = 0; q < C; q++) {
+                    const int step = s->tstep + q - c.step0;
+                    for (int p = 0; p < c.np; p++) {
+                        const std::complex<double> e = std::exp(c.w[p] * step * s->Dt * Im);
+                        c.rows[(size_t(q) * c.np + p) * 2] = e.real();
+                        c.rows[(size_t(q) * c.np + p) * 2 + 1] = e.imag();
+                    }
+                }
+                AE_CUDA(cudaMemcpyAsync(c.ctab.p, c.rows.data(), c.rows.size() * sizeof(double), cudaMemcpyHostToDevice,
+                                        ln.stream));
+            }
             AE_CUDA(cudaMemcpyAsync(s->tables.as<StepScalars>(), host.data(), sizeof(StepScalars) * C,
                                     cudaMemcpyHostToDevice, ln.stream));
         }
@@ -440,6 +477,16 @@ template <typename T, typename Tid> void aefdtd_batch::ensure_history() {
         for (aefdtd_sim *s : u.members) {
             const BatchMember &m = rec(s);
             if (s->cc_coeff <= 0) continue;
+            if (s->ccft) {
+                CompletionFT &c = *s->ccft;
+                if (!c.snap.p) {
+                    // check steps one segment can pass, and one more
+                    c.nsnap = s->seg_len / s->cc_step + 2;
+                    c.snap.alloc(size_t(c.nsnap) * 6 * c.np * c.n_avg * 8, s->dev_bytes);
+                    u.release(dev_bytes);
+                }
+                continue;
+            }
             if (!s->cc_partial.p) {
                 s->cc_nb = std::max(1, std::min(2 * 148, (int)(((long long)s->Nx * s->Ny * s->Nz + 4095) / 4096)));
                 s->cc_partial.alloc(size_t(s->seg_len) * s->cc_nb * 8, s->dev_bytes);
@@ -461,15 +508,33 @@ template <typename T, typename Tid> void aefdtd_batch::ensure_history() {
 }
 
 // CompletionSensor::completion_check (energy mode, s_completion.cpp:39-43,
-// 121-130) at every check step t (t % cc_step == 0) that the member passed in
-// its last segment, in order, as aefdtd_sim::completion_check does after each
-// check step of a single run. A member that completes at t has its budget
+// 121-130; FT mode on the ring snapshot taken after the check step) at every
+// check step t (t % cc_step == 0) that the member passed in its last segment,
+// in order, as aefdtd_sim::completion_check does after each check step of a
+// single run. A member that completes at t has its budget
 // set to zero; the steps it ran past t (at most one segment) do not enter its
 // results, which are read up to t (aefdtd_get_normal_spectra uses cc_stop).
 static bool batch_completion_check(aefdtd_sim *s, int t0, int t1, cudaStream_t st) {
     const int first = (t0 + s->cc_step - 1) / s->cc_step * s->cc_step;
     if (first >= t1) return false;
     AE_CUDA(cudaStreamSynchronize(st));
+    if (s->ccft) {
+        // FT mode (CompletionSensor::completion_check, s_completion.cpp:45-121) on the ring as it
+        // stood after each check step
+        CompletionFT &c = *s->ccft;
+        const size_t n = size_t(6) * c.np * c.n_avg;
+        c.ring_host.resize(n);
+        for (int t = first; t < t1; t += s->cc_step) {
+            const int slot = (t / s->cc_step) % c.nsnap;
+            AE_CUDA(cudaMemcpy(c.ring_host.data(), c.snap.as<double>() + size_t(slot) * n, n * 8, cudaMemcpyDeviceToHost));
+            if (s->ft_eval(c.ring_host.data(), t + 1 - c.step0)) {
+                s->cc_done = true;
+                s->cc_stop = t;
+                return true;
+            }
+        }
+        return false;
+    }
     for (int t = first; t < t1; t += s->cc_step) {
         const int n = t + 1 - s->cc_read;
         if (n > 0) {
@@ -721,7 +786,6 @@ aefdtd_status aefdtd_batch_add(aefdtd_batch *b, aefdtd_sim *s, int32_t steps) {
         if (!s->map_set) fail(AEFDTD_NOT_READY, "no material map");
         if (s->g.mode == AEFDTD_MODE_NORMAL && !s->normal) fail(AEFDTD_NOT_READY, "normal mode needs aefdtd_setup_normal");
         if (!s->sensors.empty()) fail(AEFDTD_BAD_ARG, "batch members carry no planar DFT sensors (normal-mode plane sums only)");
-        if (s->cc_coeff > 0 && s->ccft) fail(AEFDTD_BAD_ARG, "batch members take the energy-mode completion sensor only");
         if (!s->fmaps.empty()) fail(AEFDTD_BAD_ARG, "batch members carry no field sensors");
         if (s->g.mode == AEFDTD_MODE_OBLIQUE) fail(AEFDTD_BAD_ARG, "batch members run normal or custom mode only");
         if (s->Nz >= 32768) fail(AEFDTD_BAD_ARG, "batch members need Nz < 32768 (k1 << 16 in an int32 item)");

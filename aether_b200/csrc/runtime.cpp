@@ -484,6 +484,7 @@ void aefdtd_sim::drain_sensors() {
 void aefdtd_sim::fill_scalars(int t, int osc_offset, StepScalars &s) const {
     std::memset(&s, 0, sizeof(s));
     s.step = t;
+    s.snap = -1;
     if (normal) {
         // normal_incidence.cpp:334-357
         double tb = t * Dt;
@@ -837,7 +838,15 @@ bool aefdtd_sim::ft_check() {
     c.ring_host.resize(n);
     AE_CUDA(cudaMemcpyAsync(c.ring_host.data(), c.ring.p, n * 8, cudaMemcpyDeviceToHost, stream));
     AE_CUDA(cudaStreamSynchronize(stream));
-    auto R = [&](int comp, int i, int j) { return c.ring_host[(size_t(comp) * c.np + i) * c.n_avg + j]; };
+    return ft_eval(c.ring_host.data(), step);
+}
+
+// The FT-mode decision over a host copy of the ring (layout [6][np][n_avg]),
+// `step` the sensor's step after the checked step's feed.
+bool aefdtd_sim::ft_eval(const double *ring, int step) {
+    CompletionFT &c = *ccft;
+    if (step < 2 * std::max(Nx, std::max(Ny, Nz))) return false;
+    auto R = [&](int comp, int i, int j) { return ring[(size_t(comp) * c.np + i) * c.n_avg + j]; };
     double av[6] = {0, 0, 0, 0, 0, 0};
     int N_ok = 0;
     for (int i = 0; i < c.np; i++) {
@@ -2036,10 +2045,10 @@ aefdtd_status aefdtd_set_completion(aefdtd_sim *s, double coeff, int32_t check_e
     if (!s) return AEFDTD_BAD_ARG;
     return guarded(s, [&] {
         if (check_every < 0) fail(AEFDTD_BAD_ARG, "negative check interval");
-        if (s->batch) fail(AEFDTD_NOT_READY, "batch members run without a completion sensor");
+        if (s->batch) fail(AEFDTD_NOT_READY, "set the completion sensor before the simulation joins a batch");
         if (s->ccft) {
             size_t t = 0;
-            s->ccft->dpts.release(t); s->ccft->acc.release(t); s->ccft->ring.release(t); s->ccft->ctab.release(t);
+            s->ccft->dpts.release(t); s->ccft->acc.release(t); s->ccft->ring.release(t); s->ccft->ctab.release(t); s->ccft->snap.release(t);
             s->dev_bytes -= std::min(s->dev_bytes, t);
             delete s->ccft;
             s->ccft = nullptr;

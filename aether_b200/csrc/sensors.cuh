@@ -226,6 +226,14 @@ __global__ void __launch_bounds__(kPlaneThreads) completion_ft_step(const __grid
         a.ring[((size_t)d * a.np + p) * a.n_avg + offset] = v.x;
         a.ring[((size_t)(3 + d) * a.np + p) * a.n_avg + offset] = v.y;
     }
+    // a batch member's check step: this probe's ring as the check will read it
+    const int slot = a.sc[a.q].snap;
+    if (a.snap && slot >= 0) {
+        const size_t per = (size_t)a.np * a.n_avg;
+        for (int d = 0; d < 6; ++d)
+            for (int j = 0; j < a.n_avg; ++j)
+                a.snap[((size_t)slot * 6 + d) * per + (size_t)p * a.n_avg + j] = a.ring[((size_t)d * a.np + p) * a.n_avg + j];
+    }
 }
 
 template <typename T>

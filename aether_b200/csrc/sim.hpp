@@ -168,6 +168,8 @@ struct CompletionFT {
     std::vector<double> w;         // [np] angular frequencies
     std::vector<double> ring_host, rows;
     DBuf dpts, acc, ring, ctab;    // ctab: [2 slots][seg_len][np] complex phases
+    DBuf snap;                     // batch members: ring snapshots at check steps
+    int nsnap = 0;
     double open_ratio = 0;         // fraction of probes not settled at the last check
 };
 
@@ -360,6 +362,7 @@ struct aefdtd_sim {
     CompletionFT *ccft = nullptr;   // FT mode (else energy mode)
     void completion_check();
     bool ft_check();
+    bool ft_eval(const double *ring, int step);
 };
 
 inline aefdtd_sim::~aefdtd_sim() {
@@ -390,7 +393,7 @@ inline aefdtd_sim::~aefdtd_sim() {
     }
     for (auto *m : fmaps) { m->acc.release(t); delete m; }
     if (ccft) {
-        ccft->dpts.release(t); ccft->acc.release(t); ccft->ring.release(t); ccft->ctab.release(t);
+        ccft->dpts.release(t); ccft->acc.release(t); ccft->ring.release(t); ccft->ctab.release(t); ccft->snap.release(t);
         delete ccft;
     }
     for (auto *s : sensors) {

@@ -193,3 +193,35 @@ def test_completion_inside_a_batch_stops_where_alone_stops(opts):
         assert np.array_equal(ps.plane_sums(), alone(plain, 700)[1])
     for s in sims + [ps]:
         s.close()
+
+
+@pytest.mark.parametrize("coeff,layout,npts,seed", [(2e-2, "nnb", 40, 7), (5e-2, "bnn", 24, 11)])
+def test_ft_completion_inside_a_batch_stops_where_alone_stops(coeff, layout, npts, seed):
+    """FT-mode completion sensor (probes drawn from the seeded generator) on
+    batch members: the check reads the probe ring as it stood after each
+    check step, so a member completes at the step it completes alone, with
+    bit-identical spectra, although it runs on past it within its segment."""
+    import scenes
+    scs = [scenes.slab_tm(nsteps=6000), scenes.slab_tm(nsteps=6000, n_slab=2.0)]
+    for sc in scs:
+        sc.sensors = []            # batch members carry plane sums only
+    want = []
+    for sc in scs:
+        with fdtd.build_simulation(sc) as s:
+            s.set_completion_ft(400e-9, 1000e-9, coeff, npts, layout, seed, 50)
+            s.step(6000)
+            want.append((s.completion(), s.normal_spectra()))
+    assert all(w[0][0] for w in want), "the runs must complete inside the budget"
+    sims = [fdtd.build_simulation(sc) for sc in scs]
+    for s in sims:
+        s.set_completion_ft(400e-9, 1000e-9, coeff, npts, layout, seed, 50)
+    with fdtd.Batch(graph_steps=16) as b:
+        for s in sims:
+            b.add(s, 6000)
+        b.run(10 ** 6)
+        for s, ((done, stop, ratio), spec) in zip(sims, want):
+            got = s.completion()
+            assert got[0] and got[1] == stop and got[2] == ratio
+            assert np.array_equal(s.normal_spectra(), spec)
+    for s in sims:
+        s.close()
