@@ -122,6 +122,7 @@ struct aefdtd_batch {
     std::map<int, SizeClass> classes;
     bool layout_dirty = true;
     long long l2_budget = 48LL << 20;
+    int next_solo_class = -1;   // size-class keys below zero: members that never share a subset
     int graph_steps = 32;          // steps per captured chunk (a divisor of seg_len)
     bool h_reverse = false;        // H pass over the members in reverse order (measured slower on L2-sized subsets)
     uint64_t launches = 0;
@@ -336,23 +337,31 @@ template <typename T, typename Tid> void aefdtd_batch::enqueue_steps(BatchSubset
     for (int g = 0; g < kGroups; g++) groups += (u.wsE.n[g] > 0) + (u.wsH.n[g] > 0);
     // a lone member: its own arguments as launch parameters, its own lists
     aefdtd_sim *m0 = u.members[0];
-    StepArgs<T, Tid> se, sh;
+    StepArgs<T, Tid> se, sh, se_i, sh_i;
     if (u.solo) m0->make_step_args(se, sh, m0->tables.as<StepScalars>());
+    // an oblique member (always alone): its imaginary grid on the same lists, and its R/T sums
+    const bool obl = u.solo && m0->obl;
+    if (obl) {
+        m0->make_step_args(se_i, sh_i, m0->tables.as<StepScalars>(), 1);
+        groups *= 2;
+    }
     const int4 *mit = m0->items.as<int4>();
     // members with the energy-mode completion sensor: the energy of every step
     std::vector<aefdtd_sim *> cc;
     for (aefdtd_sim *s : u.members)
         if (s->cc_coeff > 0) cc.push_back(s);
-    const bool side = u.nblk > 0 || !cc.empty();
+    const bool side = u.nblk > 0 || !cc.empty() || obl;
     for (int q = 0; q < L; q++) {
-        se.q = sh.q = q;
+        se.q = sh.q = se_i.q = sh_i.q = q;
         if (u.solo) run_groups(m0->wsE, ln, [&](int g, cudaStream_t st) { launch_e_group(se, mit, m0->wsE, g, st); });
         else run_groups(u.wsE, ln, [&](int g, cudaStream_t st) { launch_e_group_batch(ea, q, it, u.wsE, g, st); });
+        if (obl) run_groups(m0->wsE, ln, [&](int g, cudaStream_t st) { launch_e_group(se_i, mit, m0->wsE, g, st); });
         // plane sums and completion energies read E only: beside the H half-step
         if (side) {
             AE_CUDA(cudaEventRecord(ln.ev_sf, ln.stream));
             AE_CUDA(cudaStreamWaitEvent(ln.side_s, ln.ev_sf, 0));
             if (u.nblk > 0) launch_plane_partial_batch(sa, blk, u.nblk, q, ln.side_s);
+            if (obl) launches += m0->launch_obl_sums<T>(q, m0->tables.as<StepScalars>(), ln.side_s);
             for (aefdtd_sim *s : cc) {
                 if (s->ccft) {
                     // FT mode: the probes' running transforms, with a ring snapshot at check steps
@@ -379,11 +388,17 @@ template <typename T, typename Tid> void aefdtd_batch::enqueue_steps(BatchSubset
         }
         if (u.solo) run_groups(m0->wsH, ln, [&](int g, cudaStream_t st) { launch_h_group(sh, mit, m0->wsH, g, st); });
         else run_groups(u.wsH, ln, [&](int g, cudaStream_t st) { launch_h_group_batch(ha, q, it, u.wsH, g, st); });
+        if (obl) run_groups(m0->wsH, ln, [&](int g, cudaStream_t st) { launch_h_group(sh_i, mit, m0->wsH, g, st); });
         if (side) AE_CUDA(cudaStreamWaitEvent(ln.stream, ln.ev_sj, 0));
         launches += groups + (u.nblk > 0) + cc.size();
     }
     if (u.nplane > 0) {
         launch_plane_reduce_batch(sa, (int)u.members.size(), L, ln.stream);
+        launches++;
+    }
+    if (obl) {
+        launch_obl_reduce(m0->obl->part.as<double>(), m0->obl->nb, m0->tables.as<StepScalars>(),
+                          m0->obl->hist.as<double>(), L, ln.stream);
         launches++;
     }
     for (aefdtd_sim *s : cc) {
@@ -471,6 +486,14 @@ template <typename T, typename Tid> void aefdtd_batch::ensure_history() {
             s->psums_cap = cap;
             s->graphs_dirty = true;
             u.release(dev_bytes);
+        }
+    // oblique members: incident sums and R/T history for the whole budget
+    for (auto &u : subsets)
+        for (aefdtd_sim *s : u.members) {
+            if (!s->obl) continue;
+            const int cap0 = s->obl->cap;
+            s->obl_ensure(s->tstep + rec(s).remaining);
+            if (s->obl->cap != cap0) u.release(dev_bytes);
         }
     // completion energies: a history for the whole budget and one chunk of partials
     for (auto &u : subsets)
@@ -785,9 +808,9 @@ aefdtd_status aefdtd_batch_add(aefdtd_batch *b, aefdtd_sim *s, int32_t steps) {
         if (s->device != b->device) fail(AEFDTD_BAD_ARG, "the simulation is on another device");
         if (!s->map_set) fail(AEFDTD_NOT_READY, "no material map");
         if (s->g.mode == AEFDTD_MODE_NORMAL && !s->normal) fail(AEFDTD_NOT_READY, "normal mode needs aefdtd_setup_normal");
+        if (s->g.mode == AEFDTD_MODE_OBLIQUE && !s->obl) fail(AEFDTD_NOT_READY, "oblique mode needs aefdtd_setup_oblique");
         if (!s->sensors.empty()) fail(AEFDTD_BAD_ARG, "batch members carry no planar DFT sensors (normal-mode plane sums only)");
         if (!s->fmaps.empty()) fail(AEFDTD_BAD_ARG, "batch members carry no field sensors");
-        if (s->g.mode == AEFDTD_MODE_OBLIQUE) fail(AEFDTD_BAD_ARG, "batch members run normal or custom mode only");
         if (s->Nz >= 32768) fail(AEFDTD_BAD_ARG, "batch members need Nz < 32768 (k1 << 16 in an int32 item)");
         s->set_device();
         s->finalize_tables();
@@ -805,7 +828,8 @@ aefdtd_status aefdtd_batch_add(aefdtd_batch *b, aefdtd_sim *s, int32_t steps) {
         BatchMember m;
         m.sim = s;
         m.remaining = (s->cc_coeff > 0 && s->cc_done) ? 0 : steps;
-        m.cls = b->class_key(s);
+        // an oblique member (two coupled grids) always runs as a subset of its own
+        m.cls = s->obl ? b->next_solo_class-- : b->class_key(s);
         auto it = b->classes.find(m.cls);
         if (it == b->classes.end()) {
             SizeClass c;

@@ -62,13 +62,33 @@ def kp_list(kind: str, *, lambda_min=None, lambda_max=None, amin_deg=0.0, amax_d
     raise ValueError(f"unknown kp sweep kind {kind!r}")
 
 
-def sweep(scene, kps, phi_deg=0.0, nsteps=None):
+def sweep(scene, kps, phi_deg=0.0, nsteps=None, batch=False):
     """Runs `scene` (mode OBLIQUE) once per kp at kx = kp cos(phi), ky = kp
     sin(phi) (incident_plane(phi), stored as Degree(phi)); returns one
     (nl', 10) array per kp: lambda, angle, |r_TE|, arg, |r_TM|, arg, |t_TE|,
-    arg, |t_TM|, arg."""
+    arg, |t_TM|, arg. batch=True advances all wavevectors together in one
+    batch (each as a subset of its own, two at a time on the GPU) with the
+    same results."""
     phi = phi_deg * (math.pi / 180.0)
     base = scene.oblique
+    steps = scene.nsteps if nsteps is None else nsteps
+    if batch:
+        sims = []
+        try:
+            for kp in kps:
+                scene.oblique = A.ObliqueDesc(base.polarization, base.nl, base.lambda_min, base.lambda_max,
+                                              kp * math.cos(phi), kp * math.sin(phi))
+                sims.append(fdtd.build_simulation(scene))
+            scene.oblique = base
+            with fdtd.Batch() as b:
+                for s in sims:
+                    b.add(s, steps)
+                b.run(10 ** 9)
+                return [s.oblique_spectra() for s in sims]
+        finally:
+            scene.oblique = base
+            for s in sims:
+                s.close()
     out = []
     for kp in kps:
         od = A.ObliqueDesc(base.polarization, base.nl, base.lambda_min, base.lambda_max,
@@ -76,7 +96,7 @@ def sweep(scene, kps, phi_deg=0.0, nsteps=None):
         scene.oblique = od
         try:
             with fdtd.build_simulation(scene) as s:
-                s.step(scene.nsteps if nsteps is None else nsteps)
+                s.step(steps)
                 out.append(s.oblique_spectra())
         finally:
             scene.oblique = base

@@ -124,3 +124,17 @@ def test_kp_sweep_runs_each_wavevector():
         phi = 30 * (math.pi / 180.0)
         sc1.oblique.kx_in, sc1.oblique.ky_in = kp * math.cos(phi), kp * math.sin(phi)
         assert np.array_equal(fdtd.run(sc1, nsteps=150)["spectra"], r)
+
+
+def test_kp_sweep_in_one_batch_matches_sequential_runs():
+    """The oblique driver's wavevector sweep advanced as one batch (each
+    wavevector a subset of its own) gives the sequential runs' spectra and
+    R/T sums bit for bit (FP64)."""
+    from aether_b200 import oblique as OBL
+    from aether_b200 import configs as CF
+    sc = CF.oblique_scene(nsteps=300)
+    kps = OBL.kp_list("fixed_lambda", nkp=3, lmin=600e-9, amin_deg=10, amax_deg=40)
+    seq = OBL.sweep(sc, kps, phi_deg=20)
+    bat = OBL.sweep(sc, kps, phi_deg=20, batch=True)
+    for a, b in zip(seq, bat):
+        assert np.array_equal(a, b)
