@@ -560,7 +560,8 @@ class Mode:
             if kind in ("auto", "full"):
                 kw.update(lambda_min=self.lmin, lambda_max=self.lmax)
             kps = OBL.kp_list(kind, **kw)
-            return {"kp": kps, "obl": OBL.sweep(sc, kps, phi_deg=self.phi)}
+            # several wavevectors advance together as one batch (same results as one by one)
+            return {"kp": kps, "obl": OBL.sweep(sc, kps, phi_deg=self.phi, batch=len(kps) > 1)}
         out: dict = {}
         with fdtd.build_simulation(sc) as sim:
             ids = self._add_extra_sensors(sim)
