@@ -298,7 +298,9 @@ class Batch:
     """Many simulations advanced together (include/aefdtd.h, aefdtd_batch_*):
     merged launches per work-item group over all members of an L2-sized
     subset, one captured graph per subset and segment. Members are ordinary
-    Simulations; the batch keeps references to them while they are members."""
+    Simulations (normal, custom or oblique mode; a completion sensor, set
+    before they join, ends them at their completion step); the batch keeps
+    references to them while they are members."""
 
     def __init__(self, l2_budget_bytes=0, tile_y=0, kchunk=0, use_graphs=True, device=0, graph_steps=0, lanes=0):
         self._lib = load()

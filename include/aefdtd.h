@@ -455,7 +455,7 @@ typedef struct aefdtd_batch_info {
     int64_t batch_bytes;      /* device memory held by the batch itself (work lists, argument arrays) */
     int64_t l2_budget_bytes;
     uint64_t launches;        /* kernel launches issued by the batch */
-    int32_t class_key[AEFDTD_BATCH_MAX_CLASSES];     /* ceil(Nx/16)*1000 + ceil(Ny/16) */
+    int32_t class_key[AEFDTD_BATCH_MAX_CLASSES];     /* ceil(Nx/16)*1000 + ceil(Ny/16); < 0: one oblique member */
     int32_t class_tile_y[AEFDTD_BATCH_MAX_CLASSES];
     int32_t class_kchunk[AEFDTD_BATCH_MAX_CLASSES];
 } aefdtd_batch_info;
@@ -463,7 +463,10 @@ typedef struct aefdtd_batch_info {
 aefdtd_status aefdtd_batch_create(const aefdtd_batch_opts *opts, aefdtd_batch **out);
 aefdtd_status aefdtd_batch_destroy(aefdtd_batch *batch);
 const char *aefdtd_batch_last_error(const aefdtd_batch *batch);
-/* Adds a simulation with a budget of `steps` more time steps. */
+/* Adds a simulation with a budget of `steps` more time steps. Members carry
+ * no planar DFT sensors or field maps. A member with a completion sensor
+ * (set before it joins, either mode) finishes at its completion step; one in
+ * oblique mode runs as a subset of its own (class key below zero). */
 aefdtd_status aefdtd_batch_add(aefdtd_batch *batch, aefdtd_sim *sim, int32_t steps);
 aefdtd_status aefdtd_batch_remove(aefdtd_batch *batch, aefdtd_sim *sim);
 aefdtd_status aefdtd_batch_set_budget(aefdtd_batch *batch, aefdtd_sim *sim, int32_t steps);
