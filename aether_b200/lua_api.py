@@ -33,11 +33,12 @@ wavevector, and every registered sensor's flux, DFT or map in registration
 order.
 
 Not available: Lua material files (Material.load_script, material(i, "file");
-describe the model with the add_* terms), add_lua_def (a Lua function per
-point) and random_packing."""
+describe the model with the add_* terms) and add_lua_def (a Lua function per
+point)."""
 from __future__ import annotations
 
 import ctypes as C
+import math
 import time
 from typing import Callable, Dict, List, Optional
 
@@ -108,6 +109,101 @@ def const_material(n: float) -> Material:
 
 # ---- structures -------------------------------------------------------------
 
+class _MT19937:
+    """The 32-bit Mersenne Twister (Matsumoto and Nishimura, 1998) with the
+    standard integer seeding, i.e. std::mt19937(seed)."""
+
+    def __init__(self, seed):
+        self.mt = [0] * 624
+        self.mt[0] = seed & 0xFFFFFFFF
+        for i in range(1, 624):
+            self.mt[i] = (1812433253 * (self.mt[i - 1] ^ (self.mt[i - 1] >> 30)) + i) & 0xFFFFFFFF
+        self.i = 624
+
+    def __call__(self):
+        if self.i >= 624:
+            mt = self.mt
+            for k in range(624):
+                y = (mt[k] & 0x80000000) | (mt[(k + 1) % 624] & 0x7FFFFFFF)
+                mt[k] = mt[(k + 397) % 624] ^ (y >> 1) ^ (0x9908B0DF if y & 1 else 0)
+            self.i = 0
+        y = self.mt[self.i]
+        self.i += 1
+        y ^= y >> 11
+        y ^= (y << 7) & 0x9D2C5680
+        y ^= (y << 15) & 0xEFC60000
+        return y ^ (y >> 18)
+
+
+def random_packing(x_max, y_max, r, n_part, seed=None, max_iterations=1000000):
+    """random_packing(x_max, y_max, r, N[, seed]) of the structure scripts
+    (lua_structure.cpp, random_packing; phys_tools.cpp:244-426): N discs of
+    radius r in a periodic x_max x y_max cell, particle 0 fixed at the origin,
+    the others drawn from std::mt19937(seed) and pushed apart by soft
+    repulsion until no particle moves (the reference's loop has no bound; here
+    it stops with an error after max_iterations). Returns the x and y lists."""
+    import time as _time
+    gen = _MT19937(int(_time.time()) if seed is None or seed < 0 else int(seed))
+    span = 4294967295.0   # gen.max() - gen.min()
+    px, py = [0.0] * n_part, [0.0] * n_part
+    for i in range(1, n_part):
+        # set(randp(x_max, gen), randp(y_max, gen), r): the reference's x86-64
+        # GCC build evaluates these arguments right to left, so y is drawn first
+        py[i] = y_max * gen() / span
+        px[i] = x_max * gen() / span
+    stable = [False] * n_part
+    fx, fy = [0.0] * n_part, [0.0] * n_part
+    cx = (0, 1, 1, 0, -1, -1, -1, 0, 1)
+    cy = (0, 0, 1, 1, 1, 0, -1, -1, -1)
+    nx, ny = int(x_max / (2.0 * r)), int(y_max / (2.0 * r))
+    if nx < 1 or ny < 1:
+        raise ValueError("the cell must hold at least one particle diameter per side")
+    dx, dy = x_max / nx, y_max / ny
+    unstable, it = True, 0
+    while unstable:
+        if it >= max_iterations:
+            raise RuntimeError("random_packing did not settle")
+        unstable = False
+        grid = [[[] for _ in range(ny)] for _ in range(nx)]
+        for l in range(n_part):
+            grid[int(px[l] / dx) % nx][int(py[l] / dy) % ny].append(l)
+        for i in range(nx):
+            for j in range(ny):
+                for p in grid[i][j]:
+                    for l in range(9):
+                        for q in grid[(i + cx[l] + nx) % nx][(j + cy[l] + ny) % ny]:
+                            for n in range(9):
+                                if p != q and p != 0:
+                                    # SeedParticle::add_force
+                                    xd = px[p] - (px[q] + cx[n] * x_max)
+                                    yd = py[p] - (py[q] + cy[n] * y_max)
+                                    d = math.sqrt(xd * xd + yd * yd)
+                                    if d <= r + r:
+                                        c = max(1.0 - 0.99 * d / (r + r), 0.0)
+                                        fx[p] += r / 10.0 * c * xd / d
+                                        fy[p] += r / 10.0 * c * yd / d
+        for i in range(n_part):   # SeedParticle::clamp_force(0.01)
+            if fx[i] * fx[i] + fy[i] * fy[i] > 0.01 * 0.01:
+                fn = math.sqrt(fx[i] * fx[i] + fy[i] * fy[i])
+                fx[i], fy[i] = 0.01 * fx[i] / fn, 0.01 * fy[i] / fn
+        unstable = not all(stable)
+        for i in range(n_part):   # SeedParticle::advance
+            px[i] += fx[i]
+            py[i] += fy[i]
+            while px[i] < 0:
+                px[i] += x_max
+            while py[i] < 0:
+                py[i] += y_max
+            while px[i] > x_max:
+                px[i] -= x_max
+            while py[i] > y_max:
+                py[i] -= y_max
+            stable[i] = not ((fx[i] * fx[i] + fy[i] * fy[i]) / (r * r) >= 1e-9)
+            fx[i] = fy[i] = 0.0
+        it += 1
+    return px, py
+
+
 def load_obj(fname):
     """obj_file_load (mesh_tools.h:103-152): "v x y z" vertices and "f" faces
     of three or four vertex numbers (1-based, anything after a '/' ignored);
@@ -166,6 +262,10 @@ class Structure:
 
     def default_material(self, index: int):
         self.default = int(index)
+
+    def random_packing(self, x_max, y_max, r, n_part, seed=None):
+        """The structure scripts' random_packing (see the module function)."""
+        return random_packing(x_max, y_max, r, n_part, seed)
 
     def loop(self, px, py, pz):
         """Structure::set_loop (structure.cpp:338-348): periodic images."""

@@ -26,6 +26,7 @@
 #define private public
 #include <structure.h>
 #undef private
+#include <phys_tools.h>
 
 #include "../include/aefdtd.h"
 
@@ -109,5 +110,19 @@ extern "C" int aeref_discretize(int32_t nx, int32_t ny, int32_t nz, double dx, d
             for (int i = 0; i < nx; i++) out[i + std::size_t(j) * nx + std::size_t(k) * nx * ny] = g(i, j, k);
     S.operations.clear();
     for (Structure_OP *x : made) delete x;
+    return 0;
+}
+
+// The structure scripts' random_packing helper (phys_tools.cpp:302-426),
+// called as the Lua binding does (lua_structure.cpp, random_packing).
+extern "C" int aeref_random_packing(double x_max, double y_max, double r, int32_t n_part, int32_t seed, double *x,
+                                    double *y) {
+    if (n_part < 1 || !x || !y) return 1;
+    std::vector<SeedParticle> particles(n_part);
+    random_packing(particles, x_max, y_max, r, n_part, seed);
+    for (int i = 0; i < n_part; i++) {
+        x[i] = particles[i].x;
+        y[i] = particles[i].y;
+    }
     return 0;
 }

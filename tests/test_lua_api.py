@@ -302,3 +302,35 @@ def test_structure_script_with_every_kind_matches_reference():
     ref = oracle_lib.ref_discretize(32, 24, 28, d, st.ops, desc)
     assert np.array_equal(gpu, ref)
     assert set(np.unique(ref)) >= {0, 1, 2, 3, 6}
+
+
+@pytest.mark.skipif(not oracle_lib.available("ref"), reason="reference build absent")
+@pytest.mark.parametrize("case", [(200e-9, 200e-9, 20e-9, 12, 5), (300e-9, 250e-9, 15e-9, 30, 9)])
+def test_random_packing_matches_reference(case):
+    """The structure scripts' random_packing against the reference's own
+    (phys_tools.cpp) compiled in the oracle build: same seeded draws, same
+    relaxation, bit-identical positions."""
+    import ctypes as C
+    x_max, y_max, r, n, seed = case
+    lib = C.CDLL(oracle_lib.REF_PATH)
+    f = lib.aeref_random_packing
+    f.argtypes = [C.c_double] * 3 + [C.c_int32] * 2 + [C.POINTER(C.c_double)] * 2
+    x, y = np.zeros(n), np.zeros(n)
+    assert f(x_max, y_max, r, n, seed, x.ctypes.data_as(C.POINTER(C.c_double)),
+             y.ctypes.data_as(C.POINTER(C.c_double))) == 0
+    px, py = L.random_packing(x_max, y_max, r, n, seed)
+    assert np.array_equal(x, px) and np.array_equal(y, py)
+    # the discs end up apart: no pair (with periodic images) closer than 1.5 r
+    for i in range(n):
+        for j in range(i + 1, n):
+            ddx = min(abs(px[i] - px[j]), x_max - abs(px[i] - px[j]))
+            ddy = min(abs(py[i] - py[j]), y_max - abs(py[i] - py[j]))
+            assert (ddx * ddx + ddy * ddy) ** 0.5 > 1.5 * r
+
+
+def test_mersenne_twister_known_answer():
+    # std::mt19937 with the default seed 5489: its 10000th output is 4123659995 (C++ [rand.predef])
+    g = L._MT19937(5489)
+    for _ in range(9999):
+        g()
+    assert g() == 4123659995
