@@ -77,6 +77,27 @@ def dist_env():
     return ws, rank, local
 
 
+def max_over_ranks(ms, device="cuda"):
+    """The slowest rank's timed duration: the job ends when its last replica
+    ends. `device` is where the reduction tensor lives: "cuda" under NCCL,
+    "cpu" under gloo. Without an initialised group of two or more ranks, `ms`
+    comes back as given."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() < 2:
+        return ms
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_gcells(cells, steps, ms, ws):
+    """Whole-job Gcell-updates/s of `ws` replicas that each advance `cells`
+    cells by `steps` time steps, over the slowest rank's `ms`."""
+    from aether_b200 import metrics as MT
+    return MT.gcells(cells, steps, ms / 1e3) * ws
+
+
 class ClockSampler:
     """nvidia-smi samples during the timed region."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -230,13 +251,10 @@ def run_gpu_arm(args):
         groups = sim.group_timings()
         sim.enable_timing(False)
         sim.synchronize()
-        if ws > 1:
-            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(ms, device="cuda")
         nsteps = args.steps * STEPS_PER_BENCH_STEP
         results[prec_name] = {
-            "gcells": MT.gcells(cells, nsteps, ms / 1e3) * ws,
+            "gcells": whole_job_gcells(cells, nsteps, ms, ws),
             "ms_per_step": ms / args.steps,
             "e_ms": e_ms / tsteps, "h_ms": h_ms / tsteps, "s_ms": s_ms / tsteps,
             "bytes": kb, "launches": launches, "clocks": cs.summary(), "cells": cells,
