@@ -263,6 +263,11 @@ def run_gpu_arm(args):
         sim.close()
         log(f"[{prec_name}] {results[prec_name]['gcells']:.2f} Gcell/s  E {e_ms / tsteps * 1e3:.1f} us  "
             f"H {h_ms / tsteps * 1e3:.1f} us  sensors {s_ms / tsteps * 1e3:.1f} us per time step (timing pass)")
+    if ws > 1:
+        # the run's last collective is done: all ranks leave the group together
+        # (no CUDA graph holds an NCCL call); rank 0's later samples are local
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
     return results, ws, rank
 
 
