@@ -6,8 +6,8 @@ import ctypes as C
 
 import numpy as np
 
-ABI_VERSION = 1
-MAX_TERMS = 4
+ABI_VERSION = 2
+MAX_TERMS = 8
 
 MODE_NORMAL, MODE_CUSTOM, MODE_OBLIQUE = 0, 1, 2
 FP64, FP32 = 0, 1

@@ -62,6 +62,8 @@ _SIGS = {
     "aefdtd_get_fieldmap": (C.c_int, [C.c_void_p, C.c_int32, _P(C.c_double), C.c_size_t]),
     "aefdtd_get_completion": (C.c_int, [C.c_void_p, _P(C.c_int32), _P(C.c_int32), _P(C.c_double)]),
     "aefdtd_get_launch_count": (C.c_int, [C.c_void_p, _P(C.c_uint64)]),
+    "aefdtd_device_memory": (C.c_int, [C.c_int32, _P(C.c_size_t), _P(C.c_size_t)]),
+    "aefdtd_test_hook": (C.c_int, [C.c_void_p, C.c_int32, C.c_int64]),
     "aefdtd_plane_sums_static": (C.c_int, [_P(C.c_void_p), C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                            _P(C.c_int32), C.c_int32, C.c_double, C.c_void_p, C.c_void_p,
                                            C.c_char_p, C.c_size_t]),

@@ -265,6 +265,8 @@ struct DftTcArgs {
     size_t tile_stride;
     double2 *acc;            // [6][nl][P]
     int *err;
+    long long wait_cycles;   // bound of each mbarrier wait (SM cycles)
+    int withhold_copy;       // test hook: 1 = issue no phasor copy, so the first wait runs out
 };
 constexpr int kDftTcMaxK = 64;
 constexpr int kDftTcThreads = 512;   // 16 warps: 4 per TMEM lane quarter

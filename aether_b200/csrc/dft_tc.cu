@@ -50,12 +50,12 @@ __device__ __forceinline__ bool bar_try(uint64_t *b, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// about 2^32 SM cycles (~2 s) before giving up
-__device__ __forceinline__ bool bar_wait(uint64_t *b, uint32_t parity) {
+// gives up after `limit` SM cycles (2^32 by default, about 2 s)
+__device__ __forceinline__ bool bar_wait(uint64_t *b, uint32_t parity, long long limit) {
     if (bar_try(b, parity)) return true;
     const long long t0 = clock64();
     while (!bar_try(b, parity))
-        if (clock64() - t0 > (1LL << 32)) return false;
+        if (clock64() - t0 > limit) return false;
     return true;
 }
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *b) {
@@ -217,13 +217,15 @@ __global__ void __launch_bounds__(kDftTcThreads, 1) dft_accumulate_tc(const __gr
     for (int t = 0; t < ntiles && ok; ++t) {
         const int Nt = t ? a.N1 : a.N0;
         const uint32_t part = (uint32_t)(Nt * K * 4);
-        if (tid == 0) {
+        if (tid == 0 && !a.withhold_copy) {
             const float *src = a.B + (size_t)t * a.tile_stride + (size_t)fam * Nt * K;
             bar_expect_tx(&bars[0], 2 * part);
             bulk_g2s(Bhi, src, part, &bars[0]);
             bulk_g2s(Blo, src + (size_t)Nt * K, part, &bars[0]);
         }
-        if (!bar_wait(&bars[0], t & 1)) ok = false;
+        // withheld (test hook): no arrive and no copy in flight, so this wait
+        // runs out and the CTA takes the error path below
+        if (!bar_wait(&bars[0], t & 1, a.wait_cycles)) ok = false;
         if (tid == 0 && ok) {
             tc_fence_after();
             const uint32_t idesc = instr_desc(Nt);
@@ -239,7 +241,7 @@ __global__ void __launch_bounds__(kDftTcThreads, 1) dft_accumulate_tc(const __gr
             }
             mma_commit(&bars[1]);
         }
-        if (ok && !bar_wait(&bars[1], t & 1)) ok = false;
+        if (ok && !bar_wait(&bars[1], t & 1, a.wait_cycles)) ok = false;
         // every thread leaves the tile loop together: a failed wait on any
         // thread stops all of them before the next tile's copies
         ok = __syncthreads_and(ok);

@@ -25,15 +25,15 @@
 // calls whose kernels overlap on one device (different streams, or different
 // host threads) race on it and may return each other's sums: serialise them.
 //
-// Set-up: the first call on a device resolves the array's address on that
-// device with cudaGetSymbolAddress (with the device current) and caches it;
-// make that first call before any stream capture on the device.
+// Set-up: every call resolves the array's address on the current device with
+// cudaGetSymbolAddress and checks the result. The first call on a device also
+// loads this library's device code there; make that first call before any
+// stream capture on the device.
 #include <cuda_runtime.h>
 
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
-#include <mutex>
 
 #include "../../include/aefdtd.h"
 #include "aefdtd_dev.hpp"
@@ -42,7 +42,6 @@ namespace aefdtd {
 namespace {
 
 constexpr int kStaticPlanes = AEFDTD_STATIC_MAX_PLANES;
-constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) double g_plane_scratch[kStaticPlanes * kPlaneBlocks * 3];
 
@@ -64,11 +63,14 @@ plane_sums_static_partial(const __grid_constant__ StaticPlaneArgs a, double *par
     const long long base = (long long)a.planes[p] * a.NxNy;
     const int per = (a.n + a.nbp - 1) / a.nbp;
     const int q0 = b * per, q1 = min(a.n, q0 + per);
+    // every multiply and add rounded separately, as in the stepping path's
+    // plane_partial, so that no contraction into a fused multiply-add can
+    // change the last bit for weights other than 1
     double s0 = 0, s1 = 0, s2 = 0;
     for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
-        s0 += (double)f0[base + q] * a.w;
-        s1 += (double)f1[base + q] * a.w;
-        s2 += (double)f2[base + q] * a.w;
+        s0 = __dadd_rn(s0, __dmul_rn((double)f0[base + q], a.w));
+        s1 = __dadd_rn(s1, __dmul_rn((double)f1[base + q], a.w));
+        s2 = __dadd_rn(s2, __dmul_rn((double)f2[base + q], a.w));
     }
     __shared__ double red[3][kPlaneThreads];
     red[0][threadIdx.x] = s0;
@@ -95,19 +97,17 @@ __global__ void plane_sums_static_reduce(const double *partial, int nbp, double 
     out[p * 3 + c] = s;
 }
 
-std::mutex g_scratch_mu;
-void *g_scratch_ptr[kMaxDevices] = {};
-
-// Address of g_plane_scratch on the current device `dev`, resolved once.
-cudaError_t scratch_address(int dev, double **out) {
-    std::lock_guard<std::mutex> lk(g_scratch_mu);
-    if (!g_scratch_ptr[dev]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_plane_scratch);
-        if (e != cudaSuccess) return e;
-        g_scratch_ptr[dev] = p;
-    }
-    *out = static_cast<double *>(g_scratch_ptr[dev]);
+// Address of g_plane_scratch on the current device, resolved on every call:
+// after a cudaDeviceReset (or a new primary context) the module is loaded
+// again at another address, so a cached pointer would go stale. Once the
+// module is loaded on the device the lookup is cheap; the first lookup loads
+// it, which is why the first call on a device should come before any stream
+// capture there.
+cudaError_t scratch_address(double **out) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_plane_scratch);
+    if (e != cudaSuccess) return e;
+    *out = static_cast<double *>(p);
     return cudaSuccess;
 }
 
@@ -166,8 +166,6 @@ extern "C" aefdtd_status aefdtd_plane_sums_static(const void *const *fields, int
         cudaGetLastError();
         return report(errbuf, errbuf_len, AEFDTD_NO_DEVICE, "cudaGetDevice: %s", cudaGetErrorString(e));
     }
-    if (dev < 0 || dev >= kMaxDevices)
-        return report(errbuf, errbuf_len, AEFDTD_BAD_ARG, "device %d beyond the %d devices supported", dev, kMaxDevices);
     const size_t elem = precision == AEFDTD_FP64 ? 8 : 4;
     for (int c = 0; c < 3; ++c) {
         if (const char *why = check_device_ptr(fields[c], dev, elem))
@@ -177,7 +175,7 @@ extern "C" aefdtd_status aefdtd_plane_sums_static(const void *const *fields, int
     if (const char *why = check_device_ptr(out, dev, 8))
         return report(errbuf, errbuf_len, AEFDTD_BAD_ARG, "out %s", why);
     double *scratch = nullptr;
-    e = scratch_address(dev, &scratch);
+    e = scratch_address(&scratch);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return report(errbuf, errbuf_len, AEFDTD_CUDA_ERROR, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));

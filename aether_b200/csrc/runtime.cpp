@@ -448,7 +448,8 @@ void aefdtd_sim::flush_block(PlaneSensor &s, int half, int n, const StepScalars 
                            size_t(4) * 256 * dft_k};
         launch_phasors_tc(pa, st);
         DftTcArgs aa{dft_k, n, s.nl, s.P, s.N0, s.N1, s.S.as<float>() + hoff, s.Btc.as<float>(),
-                     size_t(4) * 256 * dft_k, s.acc.as<double2>(), err.as<int>()};
+                     size_t(4) * 256 * dft_k, s.acc.as<double2>(), err.as<int>(), tc_wait_cycles,
+                     tc_withhold_copy};
         launch_accumulate_tc(aa, st);
         launches += 2;
         return;
@@ -2176,6 +2177,43 @@ aefdtd_status aefdtd_get_stream(aefdtd_sim *s, void **stream) {
 aefdtd_status aefdtd_get_launch_count(aefdtd_sim *s, uint64_t *launches) {
     if (!s || !launches) return AEFDTD_BAD_ARG;
     *launches = s->launches;
+    return AEFDTD_OK;
+}
+
+aefdtd_status aefdtd_test_hook(aefdtd_sim *s, int32_t what, int64_t value) {
+    if (!s) return AEFDTD_BAD_ARG;
+    return guarded(s, [&] {
+        if (what == AEFDTD_TEST_DFT_WAIT_CYCLES) {
+            if (value < 1) fail(AEFDTD_BAD_ARG, "wait bound must be at least 1 cycle");
+            s->tc_wait_cycles = value;
+        } else if (what == AEFDTD_TEST_DFT_WITHHOLD_COPY) {
+            s->tc_withhold_copy = value ? 1 : 0;
+        } else {
+            fail(AEFDTD_BAD_ARG, "unknown test hook");
+        }
+        s->graphs_dirty = true;   // captured segments hold the old arguments
+    });
+}
+
+aefdtd_status aefdtd_device_memory(int32_t device, size_t *free_bytes, size_t *total_bytes) {
+    if (!free_bytes || !total_bytes) return AEFDTD_BAD_ARG;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return AEFDTD_NO_DEVICE;
+    }
+    if (device < 0 || device >= n) return AEFDTD_BAD_ARG;
+    int prev = 0;
+    if (cudaGetDevice(&prev) != cudaSuccess || cudaSetDevice(device) != cudaSuccess) {
+        cudaGetLastError();
+        return AEFDTD_CUDA_ERROR;
+    }
+    const cudaError_t e = cudaMemGetInfo(free_bytes, total_bytes);
+    cudaSetDevice(prev);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return AEFDTD_CUDA_ERROR;
+    }
     return AEFDTD_OK;
 }
 

@@ -336,6 +336,9 @@ struct aefdtd_sim {
     DBuf tables;
     bool use_graphs = true;
     bool graphs_dirty = true;
+    // tensor-core DFT wait bound and the withheld-copy test hook (aefdtd_test_hook)
+    long long tc_wait_cycles = 1LL << 32;
+    int tc_withhold_copy = 0;
     // captured segments, keyed by table slot, pending-flush state and the
     // sensors' buffer halves (the pointers a segment's launches bake in)
     std::map<uint64_t, cudaGraphExec_t> graph_exec;

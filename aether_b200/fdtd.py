@@ -243,6 +243,14 @@ class Simulation:
         return z.reshape(6, nl.value, s2.value, s1.value)
 
 
+def device_memory(device: int = 0):
+    """(free, total) bytes of a device (aefdtd_device_memory)."""
+    lib = load()
+    fr, tot = C.c_size_t(), C.c_size_t()
+    check(lib.aefdtd_device_memory(device, C.byref(fr), C.byref(tot)))
+    return fr.value, tot.value
+
+
 def build_simulation(scene) -> Simulation:
     """Creates the device simulation of a Scene (grid, map, materials,
     excitation, sensors), in the order of the reference drivers."""

@@ -91,14 +91,43 @@ class Material:
 
     description = name
 
-    def load_script(self, path: str):
-        raise NotImplementedError("Lua material files need the Lua host; describe the model with "
-                                  "epsilon_infinity / add_debye / add_drude / add_lorentz / add_crit_point")
+    def load_script(self, path: str, search=()):
+        """Material:load_script (lua_material.cpp:365-373, Loader::load
+        :466-497): resets the material and runs a material file of the
+        reference's library format (mat_lib/*.lua) with aether_b200.matlib's
+        reader. `path` is found as written, else in each directory of
+        `search` (PathManager::locate_file's order, filehdl.cpp:292-340:
+        working directory, then the calling script's directory, ...)."""
+        from . import matlib
+        m = matlib.load_file(locate_file(path, search))
+        self.eps_inf = m.eps_inf
+        self.terms = {k: list(v) for k, v in m.terms.items()}
+        self._name = m.name
+        self._refusal = m.refusal()
 
     def desc(self) -> A.MaterialDesc:
+        why = getattr(self, "_refusal", None)
+        if why:
+            raise ValueError(f"material {self._name!r} cannot be used by the FDTD: {why}")
         t = self.terms
         return A.material_desc(self.eps_inf, debye=t["debye"], drude=t["drude"], lorentz=t["lorentz"],
                                critpoint=t["critpoint"])
+
+
+def locate_file(path: str, search=()) -> str:
+    """PathManager::locate_file (filehdl.cpp:292-340) over the given
+    directories: an absolute path must exist; a relative one is tried from
+    the working directory, then from each directory of `search`."""
+    import os
+    if os.path.isabs(path):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"couldn't locate absolute path {path!r}")
+        return path
+    for d in (os.getcwd(),) + tuple(search):
+        cand = os.path.normpath(os.path.join(d, path))
+        if os.path.exists(cand):
+            return cand
+    raise FileNotFoundError(f"couldn't locate {path!r}")
 
 
 def const_material(n: float) -> Material:
@@ -575,9 +604,16 @@ class Mode:
         if nl is not None:
             self.Nl = int(nl)
 
-    def material(self, index: int, mat: Material):
+    def material(self, index: int, mat):
+        """FD_mode_set_material (lua_fd.cpp:576-604): a Material, or the path
+        of a material file (located from the working directory, then from the
+        directories in `self.search_path`, like locate_file)."""
+        if isinstance(mat, str):
+            m = Material()
+            m.load_script(mat, getattr(self, "search_path", ()))
+            mat = m
         if not isinstance(mat, Material):
-            raise NotImplementedError("material files need the Lua host; pass a Material")
+            raise TypeError("material: a Material or the path of a material file")
         self.mats[int(index)] = mat
 
     def register_sensor(self, s: SensorGen): self.sensors.append(s)

@@ -62,33 +62,50 @@ def kp_list(kind: str, *, lambda_min=None, lambda_max=None, amin_deg=0.0, amax_d
     raise ValueError(f"unknown kp sweep kind {kind!r}")
 
 
-def sweep(scene, kps, phi_deg=0.0, nsteps=None, batch=False):
+def sweep(scene, kps, phi_deg=0.0, nsteps=None, batch=False, hbm_fraction=0.8, max_chunk=0):
     """Runs `scene` (mode OBLIQUE) once per kp at kx = kp cos(phi), ky = kp
     sin(phi) (incident_plane(phi), stored as Degree(phi)); returns one
     (nl', 10) array per kp: lambda, angle, |r_TE|, arg, |r_TM|, arg, |t_TE|,
-    arg, |t_TM|, arg. batch=True advances all wavevectors together in one
-    batch (each as a subset of its own, two at a time on the GPU) with the
-    same results."""
+    arg, |t_TM|, arg. batch=True advances the wavevectors together in batches
+    (each as a subset of its own, two at a time on the GPU) with the same
+    results. A batch holds as many wavevectors as fit: members are built one
+    by one while the device's used memory stays within hbm_fraction of its
+    total with room for one more member of the first member's footprint
+    (max_chunk > 0 caps the count too); the rest run in the next batch. A
+    first member that does not fit fails like a single run would."""
     phi = phi_deg * (math.pi / 180.0)
     base = scene.oblique
     steps = scene.nsteps if nsteps is None else nsteps
-    if batch:
-        sims = []
+
+    def member(kp):
+        scene.oblique = A.ObliqueDesc(base.polarization, base.nl, base.lambda_min, base.lambda_max,
+                                      kp * math.cos(phi), kp * math.sin(phi))
         try:
-            for kp in kps:
-                scene.oblique = A.ObliqueDesc(base.polarization, base.nl, base.lambda_min, base.lambda_max,
-                                              kp * math.cos(phi), kp * math.sin(phi))
-                sims.append(fdtd.build_simulation(scene))
-            scene.oblique = base
-            with fdtd.Batch() as b:
-                for s in sims:
-                    b.add(s, steps)
-                b.run(10 ** 9)
-                return [s.oblique_spectra() for s in sims]
+            return fdtd.build_simulation(scene)
         finally:
             scene.oblique = base
-            for s in sims:
-                s.close()
+
+    if batch:
+        out = []
+        while len(out) < len(kps):
+            sims = []
+            try:
+                while len(out) + len(sims) < len(kps) and (max_chunk <= 0 or len(sims) < max_chunk):
+                    if sims:
+                        free, total = fdtd.device_memory(scene.grid.device)
+                        per = sims[0].dims().device_bytes
+                        if (total - free) + per > hbm_fraction * total:
+                            break
+                    sims.append(member(kps[len(out) + len(sims)]))
+                with fdtd.Batch() as b:
+                    for s in sims:
+                        b.add(s, steps)
+                    b.run(10 ** 9)
+                    out.extend(s.oblique_spectra() for s in sims)
+            finally:
+                for s in sims:
+                    s.close()
+        return out
     out = []
     for kp in kps:
         od = A.ObliqueDesc(base.polarization, base.nl, base.lambda_min, base.lambda_max,

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define AEFDTD_ABI_VERSION 1
+#define AEFDTD_ABI_VERSION 2
 
 typedef enum aefdtd_status {
     AEFDTD_OK = 0,
@@ -72,7 +72,7 @@ enum {
 /* Faces in descriptor arrays: xm, xp, ym, yp, zm, zp. */
 enum { AEFDTD_XM = 0, AEFDTD_XP, AEFDTD_YM, AEFDTD_YP, AEFDTD_ZM, AEFDTD_ZP };
 
-#define AEFDTD_MAX_TERMS 4 /* per model family, per material */
+#define AEFDTD_MAX_TERMS 8 /* per model family, per material (mat_lib files hold up to 6) */
 
 /* Grid and boundary description: the FDTD constructor arguments
  * (fdtd_core.h:86-94) plus set_pml_* (fdtd_pml.cpp:457-497) and
@@ -420,6 +420,21 @@ aefdtd_status aefdtd_get_group_timings(aefdtd_sim *sim, double *ms, int64_t *cel
 aefdtd_status aefdtd_get_stream(aefdtd_sim *sim, void **stream);
 /* Number of device kernel launches issued by this handle since creation. */
 aefdtd_status aefdtd_get_launch_count(aefdtd_sim *sim, uint64_t *launches);
+/* Free and total memory of device `device` (cudaMemGetInfo with that device
+ * current), for callers that size groups of simulations by footprint (the
+ * oblique driver's wavevector sweep, batches). No reference counterpart. */
+aefdtd_status aefdtd_device_memory(int32_t device, size_t *free_bytes, size_t *total_bytes);
+/* Test hooks of the bounded device waits (no reference counterpart; tests
+ * only). AEFDTD_TEST_DFT_WAIT_CYCLES sets the bound, in SM cycles, of each
+ * mbarrier wait in the FP32 tensor-core DFT (default 2^32, about 2 s);
+ * AEFDTD_TEST_DFT_WITHHOLD_COPY (value 1) makes that kernel issue no phasor
+ * copy, so its first wait runs out: each CTA then flags the error, frees its
+ * tensor memory and returns, and the next synchronising call returns
+ * AEFDTD_TIMEOUT. Value 0 restores normal operation; the handle stays usable
+ * (aefdtd_reset, then step again). */
+#define AEFDTD_TEST_DFT_WAIT_CYCLES 1
+#define AEFDTD_TEST_DFT_WITHHOLD_COPY 2
+aefdtd_status aefdtd_test_hook(aefdtd_sim *sim, int32_t what, int64_t value);
 
 /* ---- batches: many simulations advanced together ----------------------
  *
@@ -573,8 +588,9 @@ aefdtd_status aefdtd_server_get_stats(aefdtd_server *server, aefdtd_server_stats
  * Calls no allocating routine. Its scratch is a fixed 96 KiB device array
  * held by every device that loads the library until exit, which caps a call
  * at AEFDTD_STATIC_MAX_PLANES planes: more returns AEFDTD_BAD_ARG with the
- * reason in errbuf (may be NULL). The first call on a device resolves that
- * array's address there; make it before any stream capture on the device.
+ * reason in errbuf (may be NULL). Every call resolves that array's address
+ * on the current device; the first call on a device also loads the library's
+ * device code there, so make it before any stream capture on the device.
  * All calls share the array, so calls that overlap on the device race. */
 #define AEFDTD_STATIC_MAX_PLANES 64
 aefdtd_status aefdtd_plane_sums_static(const void *const *fields, int32_t precision, int32_t nx, int32_t ny,

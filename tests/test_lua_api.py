@@ -139,8 +139,8 @@ def test_mode_settings():
     m.add_lorentz(1.0, 3e15, 1e14)
     d = m.desc()
     assert d.eps_inf == 4.0 and d.n_lorentz == 1 and d.lorentz[0][1] == 3e15
-    with pytest.raises(NotImplementedError):
-        f.material(1, "gold.lua")
+    with pytest.raises(FileNotFoundError):   # a material file is located, then read (tests/test_matlib.py)
+        f.material(1, "no_such_material_file.lua")
     with pytest.raises(ValueError):
         L.MODE("fdtd_lab")
 

@@ -7,7 +7,16 @@ aefdtd_get_plane_sums (slots 9..11 at plane zs_s) and against FP64 sums of the
 fields read back with aefdtd_get_field. Tolerance: the plane-sum tolerance of
 the parity tests (relative 1e-12 of the summed magnitudes; only the summation
 order may differ). This file sorts last so that it also runs after every other
-test has used the device; it passes alone in a fresh process too."""
+test has used the device; it passes alone in a fresh process too.
+
+Free device memory is recorded before the first call as well: the first call
+on a device may load the library's device code there (module data, a few
+KiB to MiB, taken once per process), so that growth is bounded; the second
+call must leave free memory unchanged.
+
+A tapered step checks the weight path: inside the taper window the stepping
+path weights each plane sum by s_curve (mathUT.cpp:1186-1193); the static
+call given the same weight must equal slots 9..11 bit for bit."""
 import ctypes as C
 
 import numpy as np
@@ -70,7 +79,9 @@ def test_static_plane_sums_match_stepping_path_twice(precision):
         d = sim.dims()
         planes = [d.zs_s, 0, d.zs_s + 3, d.zs_e - 1, d.nz - 1]
         sim.step(40)
+        free_first = torch.cuda.mem_get_info()[0]
         first = _static_sums(sim, planes, precision)
+        assert free_first - torch.cuda.mem_get_info()[0] <= 8 << 20   # module load at most
         _check(sim, planes, first)
         assert np.any(first != 0)
         sim.step(37)
@@ -92,3 +103,25 @@ def test_static_plane_sums_reject_sizes_beyond_scratch():
     planes[0] = 8
     st = lib.aefdtd_plane_sums_static(ptrs, A.FP64, 8, 8, 8, planes, 1, 1.0, None, None, err, 256)
     assert st == 1 and b"outside" in err.value
+
+
+def _s_curve(x, xmin, xmax):
+    u = (x - xmin) / (xmax - xmin)
+    return 0.0 if u <= 0 else (1.0 if u >= 1.0 else u * u * (3.0 - 2.0 * u))
+
+
+@pytest.mark.parametrize("precision", [A.FP64, A.FP32])
+def test_static_plane_sums_tapered_weight_bit_identical(precision):
+    scene = scenes.slab_tm(precision=precision, nsteps=300)
+    scene.grid.tapering = 100
+    nt, ntap = scene.grid.nt, scene.grid.tapering
+    with fdtd.build_simulation(scene) as sim:
+        d = sim.dims()
+        sim.step(250)
+        t = 249                                   # the last step's index
+        w = _s_curve(float(t), nt - 1.0, float(nt - ntap))
+        assert 0.0 < w < 1.0
+        got = _static_sums(sim, [d.zs_s], precision, weight=w)
+        want = sim.plane_sums()[9:12, t]
+        assert np.any(want != 0)
+        assert np.array_equal(got[0], want), (got[0], want)
