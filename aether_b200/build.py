@@ -30,17 +30,20 @@ CXXFLAGS = ["-std=c++20", "-O2", "-fPIC", "-ffp-contract=off", "-Wall", "-Wno-un
 UNITS = [
     ("yee_f64.cu", ["--fmad=false"]),
     ("yee_f32.cu", []),
+    ("leapfrog_f64.cu", ["--fmad=false"]),
+    ("leapfrog_f32.cu", []),
     ("sensors.cu", []),
     ("dft_tc.cu", []),
     ("voxel.cu", ["--fmad=false"]),
     ("plane_static.cu", []),
     ("oblique.cu", ["--fmad=false"]),
     ("runtime.cpp", None),
+    ("fused.cpp", None),
     ("oblique_driver.cpp", None),
     ("batch.cpp", None),
     ("server.cpp", None),
 ]
-HEADERS = ["aefdtd_dev.hpp", "kernels.hpp", "sensors.cuh", "yee.cuh", "sim.hpp"]
+HEADERS = ["aefdtd_dev.hpp", "kernels.hpp", "sensors.cuh", "yee.cuh", "leapfrog.cuh", "sim.hpp"]
 
 
 def _stale(obj, deps):

@@ -98,6 +98,20 @@ template <typename T, typename Tid> struct StepArgs {
     const double *obl_inc;          // per-step incident sums [step][14] (E side 0..3, H side 4..7)
 };
 
+// One fused time step (leapfrog.cuh): the E and the H half-step in one pass,
+// reading the old fields and E-side state and writing new ones (ping-pong).
+template <typename T, typename Tid> struct FusedArgs {
+    StepArgs<T, Tid> e;      // E side: old fields (all six), E tables, old E-side CPML psi, old RC psi
+    StepArgs<T, Tid> h;      // H side: H tables and H-side CPML psi (updated in place)
+    T *nEx, *nEy, *nEz, *nHx, *nHy, *nHz;          // new fields
+    T *npx0, *npx1, *npy0, *npy1, *npz0, *npz1;    // new E-side CPML psi
+    Cplx<T> *npsi;                                 // new RC psi
+};
+constexpr int kFusedTileX = 64;   // columns per fused tile (32 lanes x 2)
+constexpr int kFusedMaxTY = 8;    // owned rows per fused tile (warps), plus one recomputed row
+// Fused item groups: curl only, z-CPML planes, every phase.
+enum { kFusedInterior = 0, kFusedPmlZ = 1, kFusedAll = 2, kFusedGroups = 3 };
+
 // Item groups of one half-step: a device array of int4 items (x0, y0, k0,
 // k1) sorted by group; group g is items [off[g], off[g] + n[g]).
 enum { kGroupInterior = 0, kGroupPmlZ = 1, kGroupDisp = 2, kGroupAll = 3, kGroupPmlXY = 4, kGroups = 5 };

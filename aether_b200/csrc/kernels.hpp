@@ -22,6 +22,16 @@ namespace aefdtd {
                               int g, cudaStream_t s);                                                     \
     void launch_h_group_batch(const StepArgs<T, Tid> *args, int q, const int4 *items, const WorkSplit &w, \
                               int g, cudaStream_t s);
+// leapfrog_f64.cu (--fmad=false) and leapfrog_f32.cu: fused group g
+// (kFused*) of one time step, items [off, off + n), CTAs of 32 x (ty + 2) threads
+#define AEFDTD_DECL_FUSED(T, Tid)                                                                      \
+    void launch_fused_group(const FusedArgs<T, Tid> &a, const int4 *items, int off, int n, int g, int ty, \
+                            cudaStream_t s);
+AEFDTD_DECL_FUSED(double, uint8_t)
+AEFDTD_DECL_FUSED(double, uint16_t)
+AEFDTD_DECL_FUSED(float, uint8_t)
+AEFDTD_DECL_FUSED(float, uint16_t)
+#undef AEFDTD_DECL_FUSED
 AEFDTD_DECL_YEE(double, uint8_t)
 AEFDTD_DECL_YEE(double, uint16_t)
 AEFDTD_DECL_YEE(float, uint8_t)

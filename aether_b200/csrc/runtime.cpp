@@ -118,6 +118,10 @@ void aefdtd_sim::construct(const aefdtd_grid_desc *d) {
     if (const char *pm = std::getenv("AEFDTD_PAIR")) pair_mask = unsigned(atoi(pm)) & 3u;
     pair_mask0 = pair_mask;
     h_reverse0 = h_reverse;
+    // fused time steps (AEFDTD_NO_FUSED=1: the split half-step kernels, same results in FP64)
+    if (std::getenv("AEFDTD_NO_FUSED")) use_fused = false;
+    if (const char *fy = std::getenv("AEFDTD_FUSED_TY")) fused_ty = std::clamp(atoi(fy), 1, kFusedMaxTY);
+    if (const char *fk = std::getenv("AEFDTD_FUSED_KCHUNK")) fused_kchunk = std::max(0, atoi(fk));
     if (const char *ty = std::getenv("AEFDTD_TILE_Y")) {
         const int v = atoi(ty);
         tile_y = (v == 2 || v == 8) ? v : 4;
@@ -634,6 +638,11 @@ template void aefdtd_sim::make_step_args<float, uint16_t>(StepArgs<float, uint16
                                                            const StepScalars *, int);
 template void aefdtd_sim::make_sensor_args<double>(SensorStepArgs<double> &, const StepScalars *);
 template void aefdtd_sim::make_sensor_args<float>(SensorStepArgs<float> &, const StepScalars *);
+// used by the fused segments (fused.cpp)
+template void aefdtd_sim::launch_pending<double>(PlaneSensor &, cudaStream_t);
+template void aefdtd_sim::launch_pending<float>(PlaneSensor &, cudaStream_t);
+template int aefdtd_sim::launch_maps<double>(int, int, const double *, const StepScalars *, cudaStream_t);
+template int aefdtd_sim::launch_maps<float>(int, int, const double *, const StepScalars *, cudaStream_t);
 
 // Enqueues the kernels of L consecutive steps on the stream: for each step
 // the E half-step (interior + boundary items), the H half-step, and the fused
@@ -900,7 +909,12 @@ void aefdtd_sim::completion_check() {
 
 template <typename T, typename Tid>
 void aefdtd_sim::run_steps(int n) {
-    if (work_dirty) { build_work(); graphs_dirty = true; }
+    if (work_dirty) { build_work(); graphs_dirty = true; fwork_dirty = true; }
+    const bool fused = fused_eligible();
+    if (fused) {
+        if (fwork_dirty) build_fused_work();
+        ensure_other_set();
+    }
     if (graphs_dirty) drop_graphs();
     // capacity of the plane-sum history
     if (normal && tstep + n > psums_cap) {
@@ -1010,11 +1024,23 @@ void aefdtd_sim::run_steps(int n) {
             AE_CUDA(cudaMemcpyAsync(fm_tbl.as<double>() + size_t(slot) * seg_len * kMaxMaps * 4, map_rows.data(),
                                     map_rows.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
         }
+        auto enqueue = [&](bool record) {
+            if (fused) enqueue_segment_fused<T, Tid>(L, tbl, record);
+            else enqueue_segment<T, Tid>(L, tbl, record);
+        };
         if (timing) {
-            enqueue_segment<T, Tid>(L, tbl, true);
+            enqueue(true);
+            timed_fused = fused;
+            if (fused) {
+                // cells per fused group, in the slots the timings use
+                for (auto &r : grp_cells) for (auto &x : r) x = 0;
+                for (int g = 0; g < kFusedGroups; g++) grp_cells[0][g == kFusedAll ? kGroupAll : g] = fcells[g];
+            }
             accumulate_timing(L);
         } else if (full) {
             uint64_t key = uint64_t(slot) | (uint64_t(anyp) << 1);
+            // fused segments bake in which buffers hold the current set
+            key |= (uint64_t(fused) << 62) | (uint64_t(fused && set_b) << 61);
             for (size_t k = 0; k < sensors.size(); k++) key |= uint64_t(sensors[k]->half) << (2 + k);
             // host-side effect of a full segment on the sensors (what enqueue_segment does)
             auto advance = [&] {
@@ -1037,7 +1063,7 @@ void aefdtd_sim::run_steps(int n) {
                 for (auto *s : sensors) snap.push_back(*s);
                 uint64_t l0 = launches;
                 AE_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-                enqueue_segment<T, Tid>(L, tbl, false);
+                enqueue(false);
                 cudaGraph_t gr = nullptr;
                 AE_CUDA(cudaStreamEndCapture(stream, &gr));
                 AE_CUDA(cudaGraphInstantiate(&gx, gr, 0));
@@ -1056,7 +1082,7 @@ void aefdtd_sim::run_steps(int n) {
             launches += graph_launches;
             advance();
         } else {
-            enqueue_segment<T, Tid>(L, tbl, false);
+            enqueue(false);
         }
         for (auto &o : oscs) o.step += L;
         tstep += L;
@@ -1135,7 +1161,13 @@ void aefdtd_sim::accumulate_timing(int L) {
             for (int half = 0; half < 2; half++)
                 for (int g = 0; g < kGroups; g++) {
                     const WorkSplit &w = half == 0 ? wsE : wsH;
-                    if (w.n[g] <= 0) continue;
+                    if (timed_fused) {
+                        // fused groups are reported in the E-side slots (kFusedAll as kGroupAll)
+                        const int fg = g == kGroupAll ? kFusedAll : g;
+                        if (half == 1 || g == kGroupDisp || g == kGroupPmlXY || fnum[fg] <= 0) continue;
+                    } else if (w.n[g] <= 0) {
+                        continue;
+                    }
                     const size_t i = ((size_t(q) * 2 + half) * kGroups + g) * 2;
                     float d = 0;
                     AE_CUDA(cudaEventElapsedTime(&d, tge[i], tge[i + 1]));

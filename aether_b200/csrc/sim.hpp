@@ -353,6 +353,25 @@ struct aefdtd_sim {
     unsigned pair_mask0 = 0;        // the simulation's own choices (restored when it runs alone)
     int h_reverse0 = -1;
     int h_reverse = -1;             // H work lists top plane first (L2 reuse between half-steps); -1: by size
+    // fused time steps (leapfrog.cuh): one launch per step and feature group,
+    // reading the current field / E-side state set and writing the other one
+    bool use_fused = true;           // when the simulation allows it (fused_eligible)
+    int fused_ty = kFusedMaxTY;      // owned rows per fused tile
+    int fused_kchunk = 0;            // planes per fused item (0: chosen by build_fused_work)
+    int fused_chunk = 0;             // the chunk depth in use
+    DBuf F2[6], psiE2[6], psi2;      // the other set: fields, E-side CPML psi, RC psi
+    bool set_b = false;              // the current set sits in the buffers allocated second
+    bool fwork_dirty = true;
+    DBuf fitems;
+    int foff[kFusedGroups] = {}, fnum[kFusedGroups] = {};
+    long long fcells[kFusedGroups] = {};   // owned cells per group (all chunks)
+    bool timed_fused = false;        // the timed segments ran fused (group timings in fused slots)
+    bool fused_eligible() const;
+    void build_fused_work();
+    void ensure_other_set();
+    void swap_sets();
+    template <typename T, typename Tid> void make_fused_args(FusedArgs<T, Tid> &A, const StepScalars *tbl, bool other);
+    template <typename T, typename Tid> void enqueue_segment_fused(int L, StepScalars *tbl, bool record);
     // completion sensor, energy mode (CompletionSensor(coeff), s_completion.cpp)
     double cc_coeff = 0;            // > 0: enabled
     int cc_step = 500;              // checked after steps t with t % cc_step == 0
@@ -373,6 +392,10 @@ inline aefdtd_sim::~aefdtd_sim() {
     if (stream) cudaStreamSynchronize(stream);
     size_t t = 0;
     for (auto &b : F) b.release(t);
+    for (auto &b : F2) b.release(t);
+    for (auto &b : psiE2) b.release(t);
+    psi2.release(t);
+    fitems.release(t);
     mat.release(t); coef.release(t); disp.release(t); crec.release(t); dchi.release(t); psi.release(t);
     for (auto &b : ik) b.release(t);
     for (int a = 0; a < 3; a++) { bE[a].release(t); cE[a].release(t); bH[a].release(t); cH[a].release(t); }

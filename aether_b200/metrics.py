@@ -1,6 +1,11 @@
-"""Algorithmic byte counts of the fused half-step kernels (the roofline
-numerator) and the Gcell-updates/s metric.
+"""Algorithmic byte counts of the stepping kernels (the roofline numerator)
+and the Gcell-updates/s metric.
 
+Fused time step (one pass per step, leapfrog.cuh): per interior cell-update
+12*s + b_id bytes -- the six old field values read once, the six new ones
+written once, the material id read once. CPML and dispersive add-ons as below.
+
+Split half-steps:
 Per interior cell-update the E and H half-steps together move 18*s + b_id
 bytes (s = 8 for FP64, 4 for FP32; b_id = 1 or 2): each kernel reads its own
 3 components and the other family's 3 components once and writes its 3
@@ -77,18 +82,26 @@ def kernel_bytes(scene, precision=None):
     return {"E": int(e), "H": int(h), "cells": c["cells"], "detail": c, "elem_bytes": s}
 
 
+def fused_bytes(scene, precision=None):
+    """Algorithmic bytes of one fused time step over the whole grid."""
+    s = 8 if (scene.grid.precision if precision is None else precision) == A.FP64 else 4
+    c = cell_counts(scene)
+    return int(c["cells"] * (12 * s + c["id_bytes"]) + (c["pml_E"] + c["pml_H"]) * 4 * s
+               + c["disp_pole_cells"] * 12 * s)
+
+
 def gcells(cells, steps, seconds):
     return cells * steps / seconds / 1e9
 
 
-def step_bytes(scene, precision=None, dft_block=64):
-    """Algorithmic bytes of one whole time step: the E and H half-steps, the
-    sensor samples (per point: 18 field reads, 6 sample writes) and, per
-    step, 1/K of each DFT block (samples read once, FP64 complex accumulators
-    read and written for every wavelength)."""
+def step_bytes(scene, precision=None, dft_block=64, fused=False):
+    """Algorithmic bytes of one whole time step: the E and H half-steps (or
+    the fused step), the sensor samples (per point: 18 field reads, 6 sample
+    writes) and, per step, 1/K of each DFT block (samples read once, FP64
+    complex accumulators read and written for every wavelength)."""
     kb = kernel_bytes(scene, precision)
     s = kb["elem_bytes"]
-    total = kb["E"] + kb["H"]
+    total = fused_bytes(scene, precision) if fused else kb["E"] + kb["H"]
     for sd in scene.sensors:
         x1, x2, y1, y2, z1, z2 = sd.box
         span = [max(1, x2 - x1), max(1, y2 - y1), max(1, z2 - z1)]

@@ -1,12 +1,14 @@
 """Benchmark of the FDTD time-stepping core on one B200.
 
-Workload: the dispersive unit cell — 128x128x256 total cells at 2.5 nm,
-periodic x/y, 24-cell CPML on z, a 40 nm gold-like sphere (Drude + 2 critical
-points) on an n=1.45 substrate, normal-incidence 400-1000 nm pulse, two planar
-flux sensors at 201 wavelengths with K=64 buffered steps per DFT block
-(seeded synthetic geometry; no dataset). One bench step = 64 FDTD time steps
-(one DFT block), inputs resident in HBM. The FP32 path is the headline value;
-the FP64 path is measured alongside.
+Workload (the headline): the dispersive unit cell -- 128x128x256 total cells
+at 2.5 nm, periodic x/y, 24-cell CPML on z, a 40 nm gold-like sphere (Drude +
+2 critical points) on an n=1.45 substrate, normal-incidence 400-1000 nm pulse,
+two planar flux sensors at 201 wavelengths with K=64 buffered steps per DFT
+block (seeded synthetic geometry; no dataset). The headline value is the FP64
+path, the reference's own arithmetic (fields bit-identical to the reference
+core); the FP32 path, the large random grid (1024x1024x512), the batch of
+nanodisk cells and the serving loop are reported in sub-objects. One bench
+step = 64 FDTD time steps (one DFT block), inputs resident in HBM.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -32,6 +34,18 @@ METRIC = "Gcell-updates/s"
 
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
+
+
+WORKLOAD = ("dispersive unit cell 128x128x256 @2.5nm, gold Drude+2CP sphere r=40nm on n=1.45 substrate, "
+            "24-cell CPML z, normal incidence 400-1000nm, 2 DFT planes x 201 lambda, K=64")
+
+
+def config_dict(ws):
+    """The workload description both arms print, identical by construction."""
+    return {"workload": WORKLOAD, "precision": "FP64 (the reference's arithmetic)",
+            "l2": "inputs exceed L2 (201 MB of FP64 fields, 632 MB of DFT accumulators); a 256 MiB buffer "
+                  "is also written between timed GPU steps",
+            "parallelism": f"replicas x{ws}"}
 
 
 def workload(precision):
@@ -253,12 +267,14 @@ def run_gpu_arm(args):
         sim.synchronize()
         ms = max_over_ranks(ms, device="cuda")
         nsteps = args.steps * STEPS_PER_BENCH_STEP
+        # the fused path reports its groups in the E-side slots and none in the H side
+        fused = groups.get(("H", "interior"), (0.0, 0))[1] == 0
         results[prec_name] = {
             "gcells": whole_job_gcells(cells, nsteps, ms, ws),
             "ms_per_step": ms / args.steps,
             "e_ms": e_ms / tsteps, "h_ms": h_ms / tsteps, "s_ms": s_ms / tsteps,
             "bytes": kb, "launches": launches, "clocks": cs.summary(), "cells": cells,
-            "groups": groups, "step_bytes": MT.step_bytes(scene),
+            "groups": groups, "step_bytes": MT.step_bytes(scene, fused=fused), "fused": fused,
         }
         sim.close()
         log(f"[{prec_name}] {results[prec_name]['gcells']:.2f} Gcell/s  E {e_ms / tsteps * 1e3:.1f} us  "
@@ -342,9 +358,8 @@ def reference_arm(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": "dispersive unit cell 128x128x256 @2.5nm, gold Drude+2CP sphere r=40nm on "
-                               "n=1.45 substrate, 24-cell CPML z, 2 DFT planes x 201 lambda",
-                   "step": f"{sample_steps} FDTD time steps per bench step (bounded CPU sample)"},
+        "config": config_dict(ws),
+        "step": f"{sample_steps} FDTD time steps per bench step (bounded CPU sample of the same workload)",
         "cpu_baseline": {"value": val, "unit": METRIC, "cores": cores, "kind": kind,
                          "sample": f"{sample_steps} time steps per bench step, reference time loop"},
         "e2e": {"value": val, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -503,7 +518,7 @@ def large_grid_sample(steps=128, seed=1234):
         e1.record(ext)
         e1.synchronize()
         ms = e0.elapsed_time(e1) / steps
-        sb = MT.step_bytes(sc, prec)
+        sb = MT.step_bytes(sc, prec, fused=os.environ.get("AEFDTD_NO_FUSED") is None)
         out[name] = {"gcells": sc.cells / (ms * 1e-3) / 1e9, "ms_per_step": ms,
                      "step_frac": sb / (ms * 1e-3) / 1e9 / peak, "bytes_per_step": sb,
                      "device_gb": sim.dims().device_bytes / 1e9, "setup_seconds": setup}
@@ -511,6 +526,30 @@ def large_grid_sample(steps=128, seed=1234):
         log(f"[large {name}] {out[name]['gcells']:.1f} Gcell/s, {out[name]['step_frac']:.2f} of HBM peak, "
             f"{out[name]['device_gb']:.1f} GB on the device")
     return out
+
+
+def large_grid_cpu_crop(steps=8, seed=1234):
+    """The reference core on a 256 x 256 x 128 crop of the large grid's scene
+    (the same densities scaled to a 64x smaller grid: 12 dielectric spheres
+    with their own indices, 3 Lorentz spheres sharing one, an oscillator,
+    32-cell CPML on all six faces), FP64, `steps` steps timed on the host
+    cores. The full 1024 x 1024 x 512 grid is out of reach for the reference:
+    its setup scans the whole grid once per material index
+    (FDTD_Material::link_grid, mats.cpp:394-443), 552 scans of 537 M cells."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import ctypes as C
+    import oracle_lib
+    from aether_b200 import _abi as A
+    from aether_b200 import configs as CF
+    which = "ref" if oracle_lib.available("ref") else "port"
+    sc = CF.random_spheres_scene(n_total=(256, 256, 128), n_dielectric=12, n_lorentz=3, nsteps=5000, seed=seed,
+                                 precision=A.FP64)
+    r = oracle_lib.run(sc, which, nsteps=steps, want_fields=False)
+    cores = int(C.CDLL(oracle_lib.REF_PATH).aeref_threads()) if which == "ref" else 1
+    return {"value": sc.cells * steps / r["seconds"] / 1e9, "unit": METRIC, "cores": cores,
+            "kind": "reference" if which == "ref" else "port",
+            "sample": f"{steps} time steps of a 256x256x128 crop of the large grid's scene (same densities), "
+                      f"time loop only, {r['seconds']:.2f} s"}
 
 
 def profile_run(args):
@@ -567,57 +606,73 @@ def main():
     from aether_b200 import _abi as A
     r32, r64 = res["fp32"], res["fp64"]
     peak, peak_kind = measured_peaks()
-    # dominant kernel: the E interior group (curl update of the interior items)
-    ei_ms, ei_cells = r32["groups"][("E", "interior")]
-    ei_bytes = ei_cells * (9 * 4 + r32["bytes"]["detail"]["id_bytes"])
-    achieved = ei_bytes / (ei_ms * 1e-3) / 1e9
-    traffic = profiled_traffic("e_interior_v2", "fp32")
-    step_achieved = r32["step_bytes"] / (r32["ms_per_step"] * 1e-3 / STEPS_PER_BENCH_STEP) / 1e9
+
+    def interior_roofline(r, s, kernel, traffic_key):
+        # dominant kernel: the interior group (fused step, or the E half-step's curl update)
+        ms, cells = r["groups"][("E", "interior")]
+        per = (12 if r["fused"] else 9) * s + r["bytes"]["detail"]["id_bytes"]
+        b = cells * per
+        ach = b / (ms * 1e-3) / 1e9
+        if r["fused"]:
+            kernel = f"yee_fused<{'double' if s == 8 else 'float'}, uint8, 0>"
+            traffic_key = ("yee_fused", "fp64" if s == 8 else "fp32")
+        return {"bound": "hbm", "kernel": kernel, "achieved": ach, "peak": peak, "unit": "GB/s",
+                "frac": ach / peak, "peak_source": peak_kind, "traffic": profiled_traffic(*traffic_key),
+                "algorithmic_bytes_per_launch": b, "launch_us": ms * 1e3, "cells_per_launch": cells,
+                "source": "CUDA events around each launch on the simulation's stream in a 64-step "
+                          f"group-timing pass after the timed region; bytes = cells x "
+                          + (f"(12 x {s} + id bytes): six fields read and six written once per fused step"
+                             if r["fused"] else f"(9 x {s} + id bytes)")}
+
+    def step_roofline(r):
+        a = r["step_bytes"] / (r["ms_per_step"] * 1e-3 / STEPS_PER_BENCH_STEP) / 1e9
+        return {"achieved": a, "peak": peak, "unit": "GB/s", "frac": a / peak, "bytes_per_step": r["step_bytes"],
+                "note": "algorithmic bytes of a whole time step (E, H, sensor samples, 1/64 of each DFT block) "
+                        "over the graph-replay step time of the timed region"}
+
+    def kernel_split(r):
+        return {"e": r["e_ms"] * 1e3, "h": r["h_ms"] * 1e3, "sensors": r["s_ms"] * 1e3,
+                "groups": {f"{h}/{g}": round(v[0] * 1e3, 2) for (h, g), v in r["groups"].items() if v[1] > 0},
+                "source": "phases: CUDA events between the joined branches of each phase in a 128-step timing "
+                          "pass; groups: each group alone between events in a 64-step pass"}
+
     line = {
-        "metric": METRIC, "value": r32["gcells"], "unit": METRIC, "n_gpus": ws, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": r32["ms_per_step"], "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "dispersive unit cell 128x128x256 @2.5nm, gold Drude+2CP sphere r=40nm on "
-                               "n=1.45 substrate, 24-cell CPML z, normal incidence 400-1000nm, "
-                               "2 DFT planes x 201 lambda, K=64",
-                   "step": f"{STEPS_PER_BENCH_STEP} FDTD time steps (one DFT block)",
-                   "l2": "256 MiB buffer written between timed steps",
-                   "parallelism": f"replicas x{ws}"},
-        "fp64": {"value": r64["gcells"], "ms_per_step": r64["ms_per_step"],
-                 "e_us": r64["e_ms"] * 1e3, "h_us": r64["h_ms"] * 1e3,
-                 "e_interior_frac": r64["groups"][("E", "interior")][1] * (9 * 8 + 1)
-                 / (r64["groups"][("E", "interior")][0] * 1e-3) / 1e9 / peak,
-                 "step_frac": r64["step_bytes"] / (r64["ms_per_step"] * 1e-3 / STEPS_PER_BENCH_STEP) / 1e9 / peak},
-        "fp32_over_fp64": r32["gcells"] / r64["gcells"],
-        "roofline": {"bound": "hbm", "kernel": "e_interior_v2<float, uint8, false>", "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                     "traffic": traffic, "algorithmic_bytes_per_launch": ei_bytes, "launch_us": ei_ms * 1e3,
-                     "cells_per_launch": ei_cells,
-                     "source": "CUDA events around each launch on the simulation's stream in a 64-step "
-                               "group-timing pass after the timed region; bytes = cells x (9 x 4 + 1)"},
-        "step_roofline": {"achieved": step_achieved, "peak": peak, "unit": "GB/s", "frac": step_achieved / peak,
-                          "bytes_per_step": r32["step_bytes"],
-                          "note": "algorithmic bytes of a whole time step (E, H, sensor samples, 1/64 of "
-                                  "each DFT block) over the graph-replay step time of the timed region"},
-        "kernel_us_per_time_step": {
-            "e": r32["e_ms"] * 1e3, "h": r32["h_ms"] * 1e3, "sensors": r32["s_ms"] * 1e3,
-            "groups": {f"{h}/{g}": round(v[0] * 1e3, 2) for (h, g), v in r32["groups"].items() if v[1] > 0},
-            "source": "phases: CUDA events between the joined branches of each phase in a 128-step timing pass; "
-                      "groups: each group alone between events in a 64-step pass"},
-        "gpu_launches": r32["launches"],
-        "clocks": r32["clocks"],
+        "metric": METRIC, "value": r64["gcells"], "unit": METRIC, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r64["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_dict(ws),
+        "step": f"{STEPS_PER_BENCH_STEP} FDTD time steps (one DFT block) per bench step",
+        "roofline": interior_roofline(r64, 8, "e_interior<double, uint8, 2>", ("e_interior", "fp64")),
+        "step_roofline": step_roofline(r64),
+        "kernel_us_per_time_step": kernel_split(r64),
+        "gpu_launches": r64["launches"],
+        "clocks": r64["clocks"],
+        "fp32": {"value": r32["gcells"], "unit": METRIC, "ms_per_step": r32["ms_per_step"], "dtype": "f32",
+                 "over_fp64": r32["gcells"] / r64["gcells"],
+                 "roofline": interior_roofline(r32, 4, "e_interior_v2<float, uint8, false>", ("e_interior_v2", "fp32")),
+                 "step_roofline": step_roofline(r32), "kernel_us_per_time_step": kernel_split(r32),
+                 "gpu_launches": r32["launches"], "clocks": r32["clocks"]},
     }
     if not args.no_e2e:
-        e2e_job(A.FP32, 2 * STEPS_PER_BENCH_STEP)
-        dt, h2d, d2h, cells = e2e_job(A.FP32, 20000)
-        line["e2e"] = {"value": cells * 20000 / dt / 1e9, "unit": METRIC, "h2d_bytes_per_step": h2d,
-                       "d2h_bytes_per_step": d2h,
-                       "step": "one complete 20000-step job from host buffers (geometry upload, "
-                               "all steps, spectra read back)", "seconds": dt}
+        for prec, where in ((A.FP64, line), (A.FP32, line["fp32"])):
+            e2e_job(prec, 2 * STEPS_PER_BENCH_STEP)        # warm-up: module load, first captures
+            dt, h2d, d2h, cells = e2e_job(prec, 20000)
+            where["e2e"] = {"value": cells * 20000 / dt / 1e9, "unit": METRIC, "h2d_bytes_per_step": h2d,
+                            "d2h_bytes_per_step": d2h,
+                            "step": "one complete 20000-step job through the public API from host buffers "
+                                    "(geometry and materials uploaded, all steps, spectra and flux read back)",
+                            "seconds": dt}
     if not args.no_accuracy:
-        line["spectrum_error"] = spectrum_error_sample()
+        line["fp32"]["spectrum_error"] = spectrum_error_sample()
     if not args.no_large:
         line["large_grid"] = large_grid_sample()
+        if not args.no_cpu:
+            try:
+                line["large_grid"]["cpu_reference_crop"] = large_grid_cpu_crop()
+                c = line["large_grid"]["cpu_reference_crop"]
+                line["large_grid"]["fp64"]["over_cpu_reference"] = line["large_grid"]["fp64"]["gcells"] / c["value"]
+            except Exception as e:  # pragma: no cover
+                line["large_grid"]["cpu_reference_crop"] = {"value": None, "error": str(e)}
     if not args.no_batch:
         line["batch"] = batch_sample()
         line["batch"]["over_fp64_single"] = line["batch"]["gcells"] / r64["gcells"]
