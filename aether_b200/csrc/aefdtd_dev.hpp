@@ -109,8 +109,10 @@ template <typename T, typename Tid> struct FusedArgs {
 };
 constexpr int kFusedTileX = 64;   // columns per fused tile (32 lanes x 2)
 constexpr int kFusedMaxTY = 8;    // owned rows per fused tile (warps), plus one recomputed row
-// Fused item groups: curl only, z-CPML planes, every phase.
-enum { kFusedInterior = 0, kFusedPmlZ = 1, kFusedAll = 2, kFusedGroups = 3 };
+// Fused item groups, numbered like the split groups below (the timing slots
+// are shared): curl only, z-CPML planes, dispersive cells only, every phase,
+// x/y (and z) CPML.
+enum { kFusedInterior = 0, kFusedPmlZ = 1, kFusedDisp = 2, kFusedAll = 3, kFusedPmlXY = 4, kFusedGroups = 5 };
 
 // Item groups of one half-step: a device array of int4 items (x0, y0, k0,
 // k1) sorted by group; group g is items [off[g], off[g] + n[g]).
@@ -288,7 +290,5 @@ constexpr int kDftTcSmem = (128 * kDftTcMaxK * 2 + 256 * kDftTcMaxK * 2) * 4 + 6
 
 constexpr int kPlaneBlocks = 64;    // plane-sum stage-1 blocks
 constexpr int kPlaneThreads = 256;
-constexpr int kDftFTile = 8;
-constexpr int kDftKTile = 16;
 
 }  // namespace aefdtd

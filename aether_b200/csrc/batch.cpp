@@ -60,13 +60,16 @@ struct BatchSubset {
     int nblk = 0;
     int nplane = 0;                // members with plane sums
     cudaGraphExec_t graph = nullptr;   // one chunk of graph_steps steps
+    cudaGraphExec_t graph_b = nullptr; // the same with a fused lone member's state in its second buffer set
     uint64_t graph_launches = 0;
+    bool fused = false;            // a lone member that takes the fused time step
     bool built = false;
     bool solo = false;             // one member: its own single-simulation kernels and work lists
     void release(size_t &t) {
         items.release(t);
         argsE.release(t); argsH.release(t); sargs.release(t);
         if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+        if (graph_b) { cudaGraphExecDestroy(graph_b); graph_b = nullptr; }
         blkmap.release(t);
         built = false;
     }
@@ -248,7 +251,18 @@ template <typename T, typename Tid> void aefdtd_batch::build_subset(BatchSubset 
             s->pair_mask = pm;
             s->h_reverse = hr;
             s->build_work();
+            s->fwork_dirty = true;
         }
+    }
+    // a lone member takes its own fused time step when it can (not with the
+    // FT-mode completion sensor, whose check steps need the ring snapshots of
+    // the batched path)
+    aefdtd_sim *m0 = u.members[0];
+    u.fused = u.solo && m0->fused_eligible() && !m0->ccft;
+    if (u.fused) {
+        if (m0->fwork_dirty) m0->build_fused_work();
+        m0->ensure_other_set();
+        AE_CUDA(cudaStreamSynchronize(m0->stream));
     }
     std::vector<int> all;
     for (int half = 0; half < 2; half++) {
@@ -328,6 +342,21 @@ template <typename Launch> void aefdtd_batch::run_groups(const WorkSplit &w, Lan
 
 // L steps whose scalars are in table entries 0..L-1 of every member.
 template <typename T, typename Tid> void aefdtd_batch::enqueue_steps(BatchSubset &u, int L, Lane &ln) {
+    if (u.fused) {
+        // the lone member's own fused segment (fused.cpp) on this lane's stream;
+        // its side streams and events serve only this member
+        aefdtd_sim *m0 = u.members[0];
+        struct OnLane {
+            aefdtd_sim *s;
+            cudaStream_t own;
+            ~OnLane() { s->stream = own; }
+        } on{m0, m0->stream};
+        m0->stream = ln.stream;
+        const uint64_t l0 = m0->launches;
+        m0->enqueue_segment_fused<T, Tid>(L, m0->tables.as<StepScalars>(), false);
+        launches += m0->launches - l0;
+        return;
+    }
     const auto *ea = u.argsE.as<StepArgs<T, Tid>>();
     const auto *ha = u.argsH.as<StepArgs<T, Tid>>();
     const auto *sa = u.sargs.as<SensorStepArgs<T>>();
@@ -444,22 +473,25 @@ template <typename T, typename Tid> void aefdtd_batch::run_segment(BatchSubset &
                                     cudaMemcpyHostToDevice, ln.stream));
         }
         if (graph) {
-            if (!u.graph) {
+            // a fused member's captured chunk reads and writes the buffer sets it was captured with
+            cudaGraphExec_t &gx = (u.fused && u.members[0]->set_b) ? u.graph_b : u.graph;
+            if (!gx) {
                 const uint64_t l0 = launches;
                 AE_CUDA(cudaStreamBeginCapture(ln.stream, cudaStreamCaptureModeThreadLocal));
                 enqueue_steps<T, Tid>(u, C, ln);
                 cudaGraph_t gr = nullptr;
                 AE_CUDA(cudaStreamEndCapture(ln.stream, &gr));
-                AE_CUDA(cudaGraphInstantiate(&u.graph, gr, 0));
+                AE_CUDA(cudaGraphInstantiate(&gx, gr, 0));
                 cudaGraphDestroy(gr);
                 u.graph_launches = launches - l0;
                 launches = l0;
             }
-            AE_CUDA(cudaGraphLaunch(u.graph, ln.stream));
+            AE_CUDA(cudaGraphLaunch(gx, ln.stream));
             launches += u.graph_launches;
         } else {
             enqueue_steps<T, Tid>(u, C, ln);
         }
+        if (u.fused && C % 2) u.members[0]->swap_sets();   // its current state moved to the other set
         for (aefdtd_sim *s : u.members) {
             s->tstep += C;
             for (auto &o : s->oscs) o.step += C;

@@ -64,7 +64,7 @@ void aefdtd_sim::build_fused_work() {
     const int TX = kFusedTileX, TY = std::max(1, std::min(fused_ty, kFusedMaxTY));
     const int ntx = (Nx + TX - 1) / TX, nty = (Ny + TY - 1) / TY;
     const long long tiles = (long long)ntx * nty;
-    constexpr unsigned kPXY = 1, kPZ = 2, kOTHER = 4;
+    constexpr unsigned kPXY = 1, kPZ = 2, kDISP = 4, kOTHER = 8;
     std::vector<unsigned char> feat(size_t(tiles) * Nz, 0);
     // tiles whose updated or recomputed columns include column c (rows: likewise)
     auto tiles_x = [&](int c, int out[2]) {
@@ -120,13 +120,15 @@ void aefdtd_sim::build_fused_work() {
                     if (row[i] == m)
                         for (int n = tiles_x(i, o), a = 0; a < n; a++)
                             for (int nn = tiles_y(j, p), b = 0; b < nn; b++)
-                                feat[(size_t(k) * nty + p[b]) * ntx + o[a]] |= kOTHER;
+                                feat[(size_t(k) * nty + p[b]) * ntx + o[a]] |= kDISP;
             }
     }
     // a plane's group also covers the plane after it (recomputed by the item ending there)
     auto group_of = [&](unsigned f) {
         if (f == 0) return (int)kFusedInterior;
         if (f == kPZ) return (int)kFusedPmlZ;
+        if (f == kDISP) return (int)kFusedDisp;
+        if ((f & ~(kPXY | kPZ)) == 0) return (int)kFusedPmlXY;
         return (int)kFusedAll;
     };
     // chunk depth: fewest waves of resident CTAs (2 per SM in FP64, 3 in FP32), times the planes an item walks
@@ -201,7 +203,9 @@ void aefdtd_sim::make_fused_args(FusedArgs<T, Tid> &A, const StepScalars *tbl, b
 
 // The kernels of L consecutive fused steps (see the file comment), then the
 // plane-sum reduction of the L steps. With record = true per-step timing
-// events are recorded and everything runs in order on the main stream.
+// events are recorded and everything runs in order on the main stream. Step
+// 0 reads the current set; with L odd the caller calls swap_sets() after
+// enqueueing (or after launching the captured graph).
 template <typename T, typename Tid>
 void aefdtd_sim::enqueue_segment_fused(int L, StepScalars *tbl, bool record) {
     FusedArgs<T, Tid> A[2];
@@ -244,7 +248,7 @@ void aefdtd_sim::enqueue_segment_fused(int L, StepScalars *tbl, bool record) {
         if (record && timing_mode == 2) {
             for (int g = 0; g < kFusedGroups; g++) {
                 if (fnum[g] <= 0) continue;
-                const int slot = g == kFusedAll ? kGroupAll : g;   // fused groups reported as E-side groups
+                const int slot = g;   // fused groups are reported in the E-side group slots of the same number
                 const size_t i = ((size_t(q) * 2 + 0) * kGroups + slot) * 2;
                 AE_CUDA(cudaEventRecord(tge[i], stream));
                 launch_fused_group(a, fi, foff[g], fnum[g], g, ty, stream);
@@ -380,7 +384,8 @@ void aefdtd_sim::enqueue_segment_fused(int L, StepScalars *tbl, bool record) {
         launch_energy_reduce(cc_partial.as<double>(), cc_nb, tbl, cc_hist.as<double>(), L, stream);
         launches++;
     }
-    if (L % 2) swap_sets();   // the current set is the one the last step wrote
+    // after an odd L the current set is the other one: the caller swaps the
+    // sets once these launches are enqueued (or their captured graph is)
 }
 
 template void aefdtd_sim::enqueue_segment_fused<double, uint8_t>(int, StepScalars *, bool);

@@ -297,6 +297,8 @@ __device__ __forceinline__ void h_cell(const FusedArgs<T, Tid> &A, int q, int i,
     }
 }
 
+constexpr int kFusedPrefetch = 6;   // planes of L2 prefetch ahead of the march
+
 template <typename T> struct FusedSmem {
     using T2 = typename Vec2<T>::type;
     T2 hz[2][kFusedMaxTY][32], hx[2][kFusedMaxTY][32];       // H(k) of the owned rows, by plane parity
@@ -382,15 +384,18 @@ __device__ __forceinline__ void fused_body(const FusedArgs<T, Tid> &A, int q, in
     const long long colm = ic + (long long)j * a.mpitch;
     const long long colym = ic + (long long)jm * Nx;
 
-    if (active && (a.prefetch & 1)) {
-        for (int kk0 = k0; kk0 <= k1; ++kk0) {
-            const long long o = (long long)(kk0 % Nz) * NxNy;
-            prefetch_l2(Hx + col + o); prefetch_l2(Hy + col + o); prefetch_l2(Hz + col + o);
-            prefetch_l2(Ex + col + o); prefetch_l2(Ey + col + o); prefetch_l2(Ez + col + o);
-            prefetch_l2(mat + colm + (long long)(kk0 % Nz) * mNxNy);
-            if (r == 0) { prefetch_l2(Hz + colym + o); prefetch_l2(Hx + colym + o); }
-        }
-    }
+    // L2 prefetch kFusedPrefetch planes ahead of the march (the first ones up front)
+    const bool pf = active && (a.prefetch & 1);
+    auto prefetch_plane = [&](int kq) {
+        const int kk = kq % Nz;
+        const long long o = (long long)kk * NxNy;
+        prefetch_l2(Hx + col + o); prefetch_l2(Hy + col + o); prefetch_l2(Hz + col + o);
+        prefetch_l2(Ex + col + o); prefetch_l2(Ey + col + o); prefetch_l2(Ez + col + o);
+        prefetch_l2(mat + colm + (long long)kk * mNxNy);
+        if (r == 0) { prefetch_l2(Hz + colym + o); prefetch_l2(Hx + colym + o); }
+    };
+    if (pf)
+        for (int kq = k0; kq <= min(k1, k0 + kFusedPrefetch - 1); ++kq) prefetch_plane(kq);
     // H(k0 - 1): the z-1 neighbours of E(k0)
     const int kb = (k0 == 0) ? Nz - 1 : k0 - 1;
     T2 hxp, hyp, hzp;
@@ -406,6 +411,7 @@ __device__ __forceinline__ void fused_body(const FusedArgs<T, Tid> &A, int q, in
         T2 hx, hy, hz, ex, ey, ez, hzy, hxy;
         I2 mm;
         T hz_e = 0, hy_e = 0;                            // x-1 of lane 0
+        if (pf && kq + kFusedPrefetch <= k1) prefetch_plane(kq + kFusedPrefetch);
         if (active) {
             hx = ldg2<T2>(Hx + col + o); hy = ldg2<T2>(Hy + col + o); hz = ldg2<T2>(Hz + col + o);
             ex = ldg2<T2>(Ex + col + o); ey = ldg2<T2>(Ey + col + o); ez = ldg2<T2>(Ez + col + o);
@@ -466,7 +472,11 @@ __device__ __forceinline__ void fused_body(const FusedArgs<T, Tid> &A, int q, in
 
 template <typename T, typename Tid, unsigned F> struct FusedBounds {
     static constexpr int kThreads = 32 * (kFusedMaxTY + 2);
-    static constexpr int kMinBlocks = sizeof(T) == 8 ? 2 : 3;
+    // the curl-only and z-CPML variants keep two (FP64) or three (FP32) CTAs per
+    // SM; the variants with x/y CPML, poles or sources trade occupancy for
+    // fewer spills (they cover a small share of the cells)
+    static constexpr bool kHeavy = (F & (kFPmlXY | kFDisp | kFMisc)) != 0;
+    static constexpr int kMinBlocks = sizeof(T) == 8 ? (kHeavy ? 1 : 2) : (kHeavy ? 2 : 3);
 };
 
 template <typename T, typename Tid, unsigned F>
@@ -484,6 +494,8 @@ void launch_fused_group_impl(const FusedArgs<T, Tid> &A, const int4 *items, int 
     switch (g) {
         case kFusedInterior: yee_fused<T, Tid, 0><<<n, blk, 0, s>>>(A, p); break;
         case kFusedPmlZ: yee_fused<T, Tid, kFPmlZ><<<n, blk, 0, s>>>(A, p); break;
+        case kFusedDisp: yee_fused<T, Tid, kFDisp><<<n, blk, 0, s>>>(A, p); break;
+        case kFusedPmlXY: yee_fused<T, Tid, kFPmlXY | kFPmlZ><<<n, blk, 0, s>>>(A, p); break;
         default: yee_fused<T, Tid, kFPmlXY | kFPmlZ | kFDisp | kFMisc><<<n, blk, 0, s>>>(A, p); break;
     }
 }

@@ -1028,13 +1028,18 @@ void aefdtd_sim::run_steps(int n) {
             if (fused) enqueue_segment_fused<T, Tid>(L, tbl, record);
             else enqueue_segment<T, Tid>(L, tbl, record);
         };
+        // an odd fused segment leaves the current state in the other set (graphs hold even segments)
+        auto settle = [&] {
+            if (fused && L % 2) swap_sets();
+        };
         if (timing) {
             enqueue(true);
+            settle();
             timed_fused = fused;
             if (fused) {
                 // cells per fused group, in the slots the timings use
                 for (auto &r : grp_cells) for (auto &x : r) x = 0;
-                for (int g = 0; g < kFusedGroups; g++) grp_cells[0][g == kFusedAll ? kGroupAll : g] = fcells[g];
+                for (int g = 0; g < kFusedGroups; g++) grp_cells[0][g] = fcells[g];
             }
             accumulate_timing(L);
         } else if (full) {
@@ -1081,8 +1086,10 @@ void aefdtd_sim::run_steps(int n) {
             AE_CUDA(cudaGraphLaunch(gx, stream));
             launches += graph_launches;
             advance();
+            settle();
         } else {
             enqueue(false);
+            settle();
         }
         for (auto &o : oscs) o.step += L;
         tstep += L;
@@ -1162,9 +1169,8 @@ void aefdtd_sim::accumulate_timing(int L) {
                 for (int g = 0; g < kGroups; g++) {
                     const WorkSplit &w = half == 0 ? wsE : wsH;
                     if (timed_fused) {
-                        // fused groups are reported in the E-side slots (kFusedAll as kGroupAll)
-                        const int fg = g == kGroupAll ? kFusedAll : g;
-                        if (half == 1 || g == kGroupDisp || g == kGroupPmlXY || fnum[fg] <= 0) continue;
+                        // fused group g is reported in E-side slot g
+                        if (half == 1 || fnum[g] <= 0) continue;
                     } else if (w.n[g] <= 0) {
                         continue;
                     }

@@ -39,8 +39,8 @@ void launch_phasors(const PhasorArgs &a, cudaStream_t s) {
     dft_phasors<<<(n + 255) / 256, 256, 0, s>>>(a);
 }
 template <typename T> static void acc_impl(const AccumArgs<T> &a, cudaStream_t s) {
-    dim3 g((a.P + 127) / 128, (a.nl + kDftFTile - 1) / kDftFTile, 6);
-    dft_accumulate<<<g, 128, 0, s>>>(a);
+    dim3 g((a.P + 63) / 64, (a.nl + 63) / 64, 6);
+    dft_accumulate<<<g, 256, 0, s>>>(a);
 }
 void launch_accumulate(const AccumArgs<double> &a, cudaStream_t s) { acc_impl(a, s); }
 void launch_accumulate(const AccumArgs<float> &a, cudaStream_t s) { acc_impl(a, s); }

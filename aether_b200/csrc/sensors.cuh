@@ -363,51 +363,72 @@ __global__ void dft_phasors(PhasorArgs a) {
 
 
 
-// grid: (ceil(P/128), ceil(nl/kDftFTile), 6); block 128
+// One DFT block of one component: acc[c][l][p] += sum_k S[k][c][p] W_c[k][l],
+// as a tiled FP64 product. A CTA of 256 threads takes 64 points x 64
+// wavelengths and walks the K steps in slices of kDftKSlice: each slice of
+// samples (as FP64) and phasors is staged in shared memory, and each thread
+// keeps a 4-point x 4-wavelength block of complex partial sums in registers
+// (32 FMA per 6 shared-memory loads). Partial sums start from zero and add the
+// steps in order with FMA, then are added to the accumulators once, so a
+// one-step block is the reference's acc + round(coeff * t) exactly.
+// grid: (ceil(P / 64), ceil(nl / 64), 6)
+constexpr int kDftKSlice = 32;
 template <typename T>
-__global__ void __launch_bounds__(128) dft_accumulate(AccumArgs<T> a) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    const int l0 = blockIdx.y * kDftFTile;
-    const int c = blockIdx.z;
+__global__ void __launch_bounds__(256, 2) dft_accumulate(AccumArgs<T> a) {
+    __shared__ __align__(16) double sS[kDftKSlice][64];
+    __shared__ __align__(16) double2 sW[kDftKSlice][64];
+    const int tid = threadIdx.x;
+    const int p0 = blockIdx.x * 64, l0 = blockIdx.y * 64, c = blockIdx.z;
     const double2 *W = (c < 3) ? a.WE : a.WH;
-    __shared__ double2 sw[kDftKTile][kDftFTile];
-    double re[kDftFTile], im[kDftFTile];
+    const int tp = tid & 15, tl = tid >> 4;   // points p0 + 4 tp .. +3, wavelengths l0 + 4 tl .. +3
+    double re[4][4], im[4][4];
 #pragma unroll
-    for (int f = 0; f < kDftFTile; ++f) { re[f] = 0; im[f] = 0; }
-    for (int kt = 0; kt < a.nk; kt += kDftKTile) {
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int f = 0; f < 4; ++f) { re[i][f] = 0; im[i][f] = 0; }
+    for (int kt = 0; kt < a.nk; kt += kDftKSlice) {
+        const int kn = min(kDftKSlice, a.nk - kt);
         __syncthreads();
-        for (int t = threadIdx.x; t < kDftKTile * kDftFTile; t += blockDim.x) {
-            const int kk = kt + t / kDftFTile, l = l0 + t % kDftFTile;
-            sw[t / kDftFTile][t % kDftFTile] = (kk < a.nk && l < a.nl) ? W[kk * a.nl + l] : make_double2(0, 0);
+        for (int t = tid; t < kDftKSlice * 64; t += 256) {
+            const int kk = t >> 6, x = t & 63;
+            const bool kin = kk < kn;
+            sS[kk][x] = (kin && p0 + x < a.P) ? (double)a.S[((long long)(kt + kk) * 6 + c) * a.P + p0 + x] : 0.0;
+            sW[kk][x] = (kin && l0 + x < a.nl) ? W[(long long)(kt + kk) * a.nl + l0 + x] : make_double2(0, 0);
         }
         __syncthreads();
-        if (p < a.P) {
-            const int kend = min(kDftKTile, a.nk - kt);
-            for (int kk = 0; kk < kend; ++kk) {
-                const double s = (double)a.S[((long long)(kt + kk) * 6 + c) * a.P + p];
+        for (int kk = 0; kk < kn; ++kk) {
+            const double2 s01 = *reinterpret_cast<const double2 *>(&sS[kk][4 * tp]);
+            const double2 s23 = *reinterpret_cast<const double2 *>(&sS[kk][4 * tp + 2]);
+            const double sv[4] = {s01.x, s01.y, s23.x, s23.y};
+            double2 wv[4];
 #pragma unroll
-                for (int f = 0; f < kDftFTile; ++f) {
-                    re[f] = re[f] + s * sw[kk][f].x;
-                    im[f] = im[f] + s * sw[kk][f].y;
+            for (int f = 0; f < 4; ++f) wv[f] = sW[kk][4 * tl + f];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int f = 0; f < 4; ++f) {
+                    re[i][f] = fma(sv[i], wv[f].x, re[i][f]);
+                    im[i][f] = fma(sv[i], wv[f].y, im[i][f]);
                 }
+        }
+    }
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+        const int l = l0 + 4 * tl + f;
+        if (l >= a.nl) continue;
+        double2 *q = a.acc + ((long long)c * a.nl + l) * a.P;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int p = p0 + 4 * tp + i;
+            if (p < a.P) {
+                double2 v = q[p];
+                v.x = v.x + re[i][f];
+                v.y = v.y + im[i][f];
+                q[p] = v;
             }
         }
     }
-    if (p >= a.P) return;
-#pragma unroll
-    for (int f = 0; f < kDftFTile; ++f) {
-        const int l = l0 + f;
-        if (l < a.nl) {
-            double2 *q = a.acc + ((long long)c * a.nl + l) * a.P + p;
-            double2 v = *q;
-            v.x = v.x + re[f];
-            v.y = v.y + im[f];
-            *q = v;
-        }
-    }
 }
-
-
 
 // One block per wavelength; deterministic reduction.
 __global__ void __launch_bounds__(256) flux_reduce(FluxArgs a) {

@@ -76,6 +76,7 @@ size_t estimate_job_bytes(const Job &j) {
     // recursive-convolution psi: bounding box of each dispersive material in
     // the structure map, extended to the grid edge where the map touches it
     // (edge slices are replicated into pads and PML)
+    size_t rc = 0;   // recursive-convolution psi
     for (size_t m = 0; m < j.mats.size(); m++) {
         const aefdtd_material_desc &md = j.mats[m];
         const int np = md.n_debye + md.n_drude + md.n_lorentz + md.n_critpoint;
@@ -94,7 +95,12 @@ size_t estimate_job_bytes(const Job &j) {
         const size_t by = (y1 == 0 ? pml[2] + pad[2] : 0) + (y2 == g.ny - 1 ? pml[3] + pad[3] : 0) + (y2 - y1 + 1);
         const size_t bz = (z1 == 0 ? pml[4] + pad[4] : 0) + (z2 == g.nz - 1 ? pml[5] + pad[5] : 0) + (z2 - z1 + 1);
         b += bx * by * bz * 3 * size_t(np) * 2 * es;
+        rc += bx * by * bz * 3 * size_t(np) * 2 * es;
     }
+    // a job that runs alone in its subset takes the fused time step when its x
+    // size is even: a second set of fields, E-side CPML psi and RC psi
+    if (Nx % 2 == 0 && g.mode != AEFDTD_MODE_OBLIQUE && !std::getenv("AEFDTD_NO_FUSED"))
+        b += 6 * N * es + 2 * (nxs * Ny * Nz + Nx * nys * Nz + Nx * Ny * nzs) * es + rc;
     const int seg = g.dft_block > 0 ? g.dft_block : 64;
     b += size_t(std::max(std::max(g.nt, j.steps), 1024)) * 12 * 8;        // plane-sum history
     b += size_t(seg) * kPlaneBlocks * 12 * 8;                               // plane-sum partials
