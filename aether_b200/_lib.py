@@ -64,6 +64,7 @@ _SIGS = {
     "aefdtd_get_launch_count": (C.c_int, [C.c_void_p, _P(C.c_uint64)]),
     "aefdtd_device_memory": (C.c_int, [C.c_int32, _P(C.c_size_t), _P(C.c_size_t)]),
     "aefdtd_test_hook": (C.c_int, [C.c_void_p, C.c_int32, C.c_int64]),
+    "aefdtd_probe_copy_bandwidth": (C.c_int, [C.c_int32, C.c_size_t, C.c_int32, _P(C.c_double)]),
     "aefdtd_plane_sums_static": (C.c_int, [_P(C.c_void_p), C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                            _P(C.c_int32), C.c_int32, C.c_double, C.c_void_p, C.c_void_p,
                                            C.c_char_p, C.c_size_t]),

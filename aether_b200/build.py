@@ -36,6 +36,7 @@ UNITS = [
     ("dft_tc.cu", []),
     ("voxel.cu", ["--fmad=false"]),
     ("plane_static.cu", []),
+    ("probe.cu", []),
     ("oblique.cu", ["--fmad=false"]),
     ("runtime.cpp", None),
     ("fused.cpp", None),

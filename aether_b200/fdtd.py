@@ -251,6 +251,15 @@ def device_memory(device: int = 0):
     return fr.value, tot.value
 
 
+def copy_bandwidth(nbytes=64 << 20, reps=50, device=0) -> float:
+    """Copy bandwidth (read + written GB/s) of a device over an nbytes buffer
+    (aefdtd_probe_copy_bandwidth): below the L2 size, the L2 ceiling."""
+    lib = load()
+    v = C.c_double()
+    check(lib.aefdtd_probe_copy_bandwidth(device, nbytes, reps, C.byref(v)))
+    return v.value
+
+
 def build_simulation(scene) -> Simulation:
     """Creates the device simulation of a Scene (grid, map, materials,
     excitation, sensors), in the order of the reference drivers."""

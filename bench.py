@@ -398,6 +398,14 @@ def batch_sample(n_cells=512, steps=256, seed=2024):
     for s in sims:
         s.close()
     g = cells * done / dt / 1e9
+    # algorithmic bytes per step over all members (fused step where the x size is
+    # even, split half-steps elsewhere) against the L2 copy ceiling: the subsets
+    # are sized to stay in L2
+    from aether_b200 import metrics as MT
+    fused_ok = os.environ.get("AEFDTD_NO_FUSED") is None
+    step_b = sum(MT.step_bytes(sc, A.FP32, fused=fused_ok and sc.total_dims()[0] % 2 == 0) for sc in scenes)
+    l2 = fdtd.copy_bandwidth(64 << 20, 50)
+    l2_frac = step_b * done / dt / 1e9 / l2
     # the plain FP64 single-simulation path on the same cells: a seeded sample
     # of 8 cells, each stepped alone (its own graphs), timed on the device
     import torch
@@ -422,6 +430,8 @@ def batch_sample(n_cells=512, steps=256, seed=2024):
             "gcells": g, "sims_per_s": n_cells / (dt * 8000.0 / done), "sample_steps": done, "seconds": dt,
             "subsets": info["n_subsets"], "setup_seconds": setup,
             "fp64_single_gcells": g64, "over_fp64_single_same_cells": g / g64,
+            "bytes_per_step": step_b, "l2_copy_gbs": l2, "l2_frac": l2_frac,
+            "l2_source": "aefdtd_probe_copy_bandwidth over a 64 MiB buffer (read + written bytes), this run",
             "note": "sims/s extrapolated from the timed sample to 8000 steps per cell; fp64_single_gcells: "
                     "8 of the cells stepped one at a time as plain FP64 simulations, device-timed"}
 

@@ -424,6 +424,11 @@ aefdtd_status aefdtd_get_launch_count(aefdtd_sim *sim, uint64_t *launches);
  * current), for callers that size groups of simulations by footprint (the
  * oblique driver's wavevector sweep, batches). No reference counterpart. */
 aefdtd_status aefdtd_device_memory(int32_t device, size_t *free_bytes, size_t *total_bytes);
+/* Copy bandwidth of a device over a buffer of `bytes` (half copied into the
+ * other half `reps` times): read plus written bytes per second in GB/s. Over a
+ * buffer smaller than the L2 it measures the L2 ceiling the batches are sized
+ * for. No reference counterpart (a measurement aid). */
+aefdtd_status aefdtd_probe_copy_bandwidth(int32_t device, size_t bytes, int32_t reps, double *gbs);
 /* Test hooks of the bounded device waits (no reference counterpart; tests
  * only). AEFDTD_TEST_DFT_WAIT_CYCLES sets the bound, in SM cycles, of each
  * mbarrier wait in the FP32 tensor-core DFT (default 2^32, about 2 s);
