@@ -124,7 +124,10 @@ void aefdtd_sim::build_fused_work() {
             }
     }
     // a plane's group also covers the plane after it (recomputed by the item ending there)
+    // AEFDTD_ALL_BOUNDARY=1 routes every item through the kernel with every phase (same results)
+    const bool all_features = std::getenv("AEFDTD_ALL_BOUNDARY") != nullptr;
     auto group_of = [&](unsigned f) {
+        if (all_features) return (int)kFusedAll;
         if (f == 0) return (int)kFusedInterior;
         if (f == kPZ) return (int)kFusedPmlZ;
         if (f == kDISP) return (int)kFusedDisp;

@@ -87,3 +87,44 @@ def test_fused_fp64_matches_reference_core():
     ref = oracle_lib.run(sc, "ref")
     got = run(sc, [sc.nsteps], fused=True)
     assert sha(got["fields"]) == sha(ref["fields"])
+
+
+def _env_run(scene, env):
+    saved = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
+    try:
+        return run(scene, [scene.nsteps], fused=True)
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+
+
+@pytest.mark.parametrize("env", [{"AEFDTD_ALL_BOUNDARY": "1"}, {"AEFDTD_FUSED_KCHUNK": "5"},
+                                 {"AEFDTD_FUSED_KCHUNK": "1000"}, {"AEFDTD_FUSED_TY": "3"},
+                                 {"AEFDTD_FUSED_TY": "1"}, {"AEFDTD_SERIAL_GROUPS": "1"}])
+def test_fused_layout_changes_no_bit(env):
+    """Every item on the kernel with every phase, other z-chunk depths and tile
+    heights, serial groups: FP64 fields and flux bit-identical to the default."""
+    sc = SCENES["debye_lorentz_sphere"](A.FP64)
+    a = run(sc, [sc.nsteps], fused=True)
+    b = _env_run(sc, env)
+    assert sha(a["fields"]) == sha(b["fields"])
+    for x, y in zip(a["flux"], b["flux"]):
+        assert np.array_equal(x, y)
+
+
+def test_fused_group_timings_cover_every_cell_once():
+    """With group timing on, the fused groups report their owned cells in the
+    E-side slots: together every cell once per step, nothing on the H side."""
+    sc = SCENES["wide_sphere"](A.FP32)
+    with fdtd.build_simulation(sc) as s:
+        s.enable_timing(True, mode=2)
+        s.step(20)
+        g = s.group_timings()
+        d = s.dims()
+        assert sum(c for (h, _), (ms, c) in g.items() if h == "E") == d.nx * d.ny * d.nz
+        assert sum(c for (h, _), (ms, c) in g.items() if h == "H") == 0
+        assert g[("E", "interior")][1] > 0 and g[("E", "interior")][0] > 0
