@@ -256,9 +256,11 @@ def test_timing_mode_does_not_change_results():
         assert np.array_equal(s1.fields(), s2.fields())
 
 
-def test_group_timing_mode_covers_every_cell_once():
+def test_group_timing_mode_covers_every_cell_once(monkeypatch):
     """Mode-2 timing runs each group alone between events: same fields, and
-    the groups of each half-step cover every cell of the grid once."""
+    the groups of each half-step cover every cell of the grid once (split
+    half-step kernels; the fused groups: test_fused.py)."""
+    monkeypatch.setenv("AEFDTD_NO_FUSED", "1")
     sc = scenes.gold_sphere(nsteps=70)
     with fdtd.build_simulation(sc) as s1, fdtd.build_simulation(sc) as s2:
         s1.step(70)
