@@ -28,9 +28,8 @@ struct FieldSwap {
 }  // namespace
 
 bool aefdtd_sim::fused_eligible() const {
-    // two cells per lane need an even Nx; the oblique driver's Bloch-coupled
-    // grids run on the split kernels
-    return use_fused && !obl && Nx % 2 == 0 && Nx >= 2;
+    // the oblique driver's Bloch-coupled grids run on the split kernels
+    return use_fused && !obl && Nx >= 1;
 }
 
 void aefdtd_sim::ensure_other_set() {

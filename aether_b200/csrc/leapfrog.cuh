@@ -18,7 +18,7 @@
 //
 // Tile. A CTA of 32 x (TY + 1) threads owns 64 x TY columns (x0, y0) and a
 // z-chunk [k0, k1). Warp w < TY owns row y0 + w; lane L its columns
-// x0 + 2L, x0 + 2L + 1 (8/16-byte pair loads; Nx must be even). The H update
+// x0 + 2L, x0 + 2L + 1 (8/16-byte pair loads; per-cell loads when Nx is odd). The H update
 // of the tile's last column and last row needs the new E one cell beyond the
 // tile, so that E is computed again here (the owner computes the same value
 // from the same old state): the extra warp TY computes E of row y0 + TY (mod
@@ -310,7 +310,11 @@ template <typename T> struct FusedSmem {
 // One step over item (x0, y0, k0, k1): blockDim (32, TY + 2), TY <= kFusedMaxTY.
 // Warps 0 .. TY-1 own the rows, warp TY recomputes E of the row after them,
 // warp TY+1 (lane r for row r) recomputes E of the column after them.
-template <typename T, typename Tid, unsigned F>
+// ODD: Nx is odd. Each cell is then loaded and stored on its own (rows are not
+// pair-aligned), and on a tile of odd width the last lane's second cell is the
+// column after the tile (mod Nx): its E is recomputed there, not stored, and
+// serves as the x+1 neighbour of the tile's last column.
+template <typename T, typename Tid, unsigned F, bool ODD>
 __device__ __forceinline__ void fused_body(const FusedArgs<T, Tid> &A, int q, int4 it) {
     using T2 = typename Vec2<T>::type;
     using I2 = typename IdPair<Tid>::type;
@@ -322,8 +326,8 @@ __device__ __forceinline__ void fused_body(const FusedArgs<T, Tid> &A, int q, in
     const int w = threadIdx.y, lane = threadIdx.x;
     const int x0 = it.x, y0 = it.y, k0 = it.z, k1 = it.w;
     const int hrows = min(TY, Ny - y0);
-    const int wcols = min(kFusedTileX, Nx - x0);         // even
-    const int llast = wcols / 2 - 1;                     // lane of the last owned pair
+    const int wcols = min(kFusedTileX, Nx - x0);         // even unless ODD on the last tile
+    const int llast = wcols / 2 - 1;                     // lane of the last owned pair (even width)
     const int ie = (x0 + wcols) % Nx;                    // the column after the tile (mod Nx)
     const long long mNxNy = (long long)a.mpitch * Ny;
     const T *__restrict__ Ex = a.Ex;
@@ -375,14 +379,41 @@ __device__ __forceinline__ void fused_body(const FusedArgs<T, Tid> &A, int q, in
     const int r = xw ? hrows : w;
     const int j = (y0 + r) % Ny;
     const int jm = (j == 0) ? Ny - 1 : j - 1;            // row y-1 (loaded by r == 0)
-    const bool lown = 2 * lane < wcols;                  // the pair holds owned columns
-    const int ic = lown ? x0 + 2 * lane : x0 + wcols - 2;
+    const bool lown = 2 * lane < wcols;                  // the pair's first column is owned
+    const bool lown1 = 2 * lane + 1 < wcols;             // ... and its second
+    const int ic = lown ? x0 + 2 * lane : (ODD ? x0 : x0 + wcols - 2);
+    // the pair's second column: ic + 1, or the column after the tile (mod Nx)
+    // when it lies past the grid (ODD)
+    const int ic1 = ODD ? ((ic + 1 < Nx) ? ic + 1 : ic + 1 - Nx) : ic + 1;
     const int im0 = (x0 == 0) ? Nx - 1 : x0 - 1;         // x-1 of lane 0's first cell
     const bool hrow = !xw && w < hrows;                  // owns H (and E) of its row
-    const bool xl = hrow && lane == llast;
+    // the lane whose second cell is the tile's last column takes the x+1
+    // neighbour of H from the column warp (an odd-width tile recomputes it itself)
+    const bool xl = hrow && (wcols % 2 == 0) && lane == llast;
     const long long col = ic + (long long)j * Nx;
+    const long long colb = ic1 + (long long)j * Nx;      // ODD: the second cell's offset
     const long long colm = ic + (long long)j * a.mpitch;
+    const long long colmb = ic1 + (long long)j * a.mpitch;
     const long long colym = ic + (long long)jm * Nx;
+    const long long colymb = ic1 + (long long)jm * Nx;
+    auto ld = [&](const T *p, long long a0, long long b0) {
+        if constexpr (ODD) {
+            T2 v;
+            v.x = __ldg(p + a0);
+            v.y = __ldg(p + b0);
+            return v;
+        } else {
+            return ldg2<T2>(p + a0);
+        }
+    };
+    auto st = [&](T *p, long long a0, long long b0, T2 v, bool s0, bool s1) {
+        if constexpr (ODD) {
+            if (s0) p[a0] = v.x;
+            if (s1) p[b0] = v.y;
+        } else {
+            st2<T2>(p + a0, v);
+        }
+    };
 
     // L2 prefetch kFusedPrefetch planes ahead of the march (the first ones up front)
     const bool pf = active && (a.prefetch & 1);
@@ -400,7 +431,10 @@ __device__ __forceinline__ void fused_body(const FusedArgs<T, Tid> &A, int q, in
     const int kb = (k0 == 0) ? Nz - 1 : k0 - 1;
     T2 hxp, hyp, hzp;
     hxp.x = hxp.y = hyp.x = hyp.y = hzp.x = hzp.y = 0;
-    if (active) { hxp = ldg2<T2>(Hx + col + kb * NxNy); hyp = ldg2<T2>(Hy + col + kb * NxNy); }
+    if (active) {
+        hxp = ld(Hx, col + kb * NxNy, colb + kb * NxNy);
+        hyp = ld(Hy, col + kb * NxNy, colb + kb * NxNy);
+    }
     T2 exp_, eyp, ezp;                                   // new E(k - 1), own pair
     exp_.x = exp_.y = eyp.x = eyp.y = ezp.x = ezp.y = 0;
 
@@ -413,11 +447,16 @@ __device__ __forceinline__ void fused_body(const FusedArgs<T, Tid> &A, int q, in
         T hz_e = 0, hy_e = 0;                            // x-1 of lane 0
         if (pf && kq + kFusedPrefetch <= k1) prefetch_plane(kq + kFusedPrefetch);
         if (active) {
-            hx = ldg2<T2>(Hx + col + o); hy = ldg2<T2>(Hy + col + o); hz = ldg2<T2>(Hz + col + o);
-            ex = ldg2<T2>(Ex + col + o); ey = ldg2<T2>(Ey + col + o); ez = ldg2<T2>(Ez + col + o);
-            mm = ldg2<I2>(mat + colm + (long long)k * mNxNy);
+            hx = ld(Hx, col + o, colb + o); hy = ld(Hy, col + o, colb + o); hz = ld(Hz, col + o, colb + o);
+            ex = ld(Ex, col + o, colb + o); ey = ld(Ey, col + o, colb + o); ez = ld(Ez, col + o, colb + o);
+            if constexpr (ODD) {
+                mm.x = __ldg(mat + colm + (long long)k * mNxNy);
+                mm.y = __ldg(mat + colmb + (long long)k * mNxNy);
+            } else {
+                mm = ldg2<I2>(mat + colm + (long long)k * mNxNy);
+            }
             if (lane == 0) { hz_e = __ldg(Hz + im0 + (long long)j * Nx + o); hy_e = __ldg(Hy + im0 + (long long)j * Nx + o); }
-            if (r == 0) { hzy = ldg2<T2>(Hz + colym + o); hxy = ldg2<T2>(Hx + colym + o); }
+            if (r == 0) { hzy = ld(Hz, colym + o, colymb + o); hxy = ld(Hx, colym + o, colymb + o); }
             if (hrow) {   // rows read by the row above, and the column warp's x-1
                 sm.hz[buf][r][lane] = hz;
                 sm.hx[buf][r][lane] = hx;
@@ -430,15 +469,16 @@ __device__ __forceinline__ void fused_body(const FusedArgs<T, Tid> &A, int q, in
             if (r > 0) { hzy = sm.hz[buf][r - 1][lane]; hxy = sm.hx[buf][r - 1][lane]; }
             const T hz_up = __shfl_up_sync(kFullMask, hz.y, 1), hy_up = __shfl_up_sync(kFullMask, hy.y, 1);
             const T hz_im0 = lane == 0 ? hz_e : hz_up, hy_im0 = lane == 0 ? hy_e : hy_up;
-            const bool st = hrow && lown && kq < k1;     // owned cells of owned planes
-            e_cell<T, Tid, F>(A, q, ic, j, k, st, mm.x, ex.x, ey.x, ez.x, hx.x, hy.x, hz.x, hxp.x, hyp.x, hzy.x, hxy.x,
+            const bool sx = hrow && lown && kq < k1;     // owned cells of owned planes
+            const bool sy = ODD ? (hrow && lown1 && kq < k1) : sx;
+            e_cell<T, Tid, F>(A, q, ic, j, k, sx, mm.x, ex.x, ey.x, ez.x, hx.x, hy.x, hz.x, hxp.x, hyp.x, hzy.x, hxy.x,
                               hz_im0, hy_im0, nex.x, ney.x, nez.x);
-            e_cell<T, Tid, F>(A, q, ic + 1, j, k, st, mm.y, ex.y, ey.y, ez.y, hx.y, hy.y, hz.y, hxp.y, hyp.y, hzy.y,
+            e_cell<T, Tid, F>(A, q, ic1, j, k, sy, mm.y, ex.y, ey.y, ez.y, hx.y, hy.y, hz.y, hxp.y, hyp.y, hzy.y,
                               hxy.y, hz.x, hy.x, nex.y, ney.y, nez.y);
-            if (st) {
-                st2<T2>(A.nEx + col + o, nex);
-                st2<T2>(A.nEy + col + o, ney);
-                st2<T2>(A.nEz + col + o, nez);
+            if (sx) {
+                st(A.nEx, col + o, colb + o, nex, true, sy);
+                st(A.nEy, col + o, colb + o, ney, true, sy);
+                st(A.nEz, col + o, colb + o, nez, true, sy);
             }
             if (r > 0) {   // rows read by the row below
                 sm.ez[buf][r][lane] = nez;
@@ -456,12 +496,14 @@ __device__ __forceinline__ void fused_body(const FusedArgs<T, Tid> &A, int q, in
             T2 nhx, nhy, nhz;
             h_cell<T, Tid, F>(A, q, ic, j, kh, hxp.x, hyp.x, hzp.x, exp_.x, eyp.x, ezp.x, nex.x, ney.x, ezj.x, exj.x,
                               ezp.y, eyp.y, nhx.x, nhy.x, nhz.x);
-            h_cell<T, Tid, F>(A, q, ic + 1, j, kh, hxp.y, hyp.y, hzp.y, exp_.y, eyp.y, ezp.y, nex.y, ney.y, ezj.y,
-                              exj.y, ez_ip1, ey_ip1, nhx.y, nhy.y, nhz.y);
+            const bool sy = ODD ? lown1 : true;
+            if (sy)
+                h_cell<T, Tid, F>(A, q, ic1, j, kh, hxp.y, hyp.y, hzp.y, exp_.y, eyp.y, ezp.y, nex.y, ney.y, ezj.y,
+                                  exj.y, ez_ip1, ey_ip1, nhx.y, nhy.y, nhz.y);
             const long long oh = (long long)kh * NxNy;
-            st2<T2>(A.nHx + col + oh, nhx);
-            st2<T2>(A.nHy + col + oh, nhy);
-            st2<T2>(A.nHz + col + oh, nhz);
+            st(A.nHx, col + oh, colb + oh, nhx, true, sy);
+            st(A.nHy, col + oh, colb + oh, nhy, true, sy);
+            st(A.nHz, col + oh, colb + oh, nhz, true, sy);
         }
         if (active) {
             hxp = hx; hyp = hy; hzp = hz;
@@ -479,10 +521,10 @@ template <typename T, typename Tid, unsigned F> struct FusedBounds {
     static constexpr int kMinBlocks = sizeof(T) == 8 ? (kHeavy ? 1 : 2) : (kHeavy ? 2 : 3);
 };
 
-template <typename T, typename Tid, unsigned F>
+template <typename T, typename Tid, unsigned F, bool ODD>
 __global__ void __launch_bounds__(FusedBounds<T, Tid, F>::kThreads, FusedBounds<T, Tid, F>::kMinBlocks)
 yee_fused(const __grid_constant__ FusedArgs<T, Tid> A, const int4 *__restrict__ items) {
-    fused_body<T, Tid, F>(A, A.e.q, items[blockIdx.x]);
+    fused_body<T, Tid, F, ODD>(A, A.e.q, items[blockIdx.x]);
 }
 
 template <typename T, typename Tid>
@@ -491,13 +533,18 @@ void launch_fused_group_impl(const FusedArgs<T, Tid> &A, const int4 *items, int 
     if (n <= 0) return;
     const dim3 blk(32, ty + 2);
     const int4 *p = items + off;
-    switch (g) {
-        case kFusedInterior: yee_fused<T, Tid, 0><<<n, blk, 0, s>>>(A, p); break;
-        case kFusedPmlZ: yee_fused<T, Tid, kFPmlZ><<<n, blk, 0, s>>>(A, p); break;
-        case kFusedDisp: yee_fused<T, Tid, kFDisp><<<n, blk, 0, s>>>(A, p); break;
-        case kFusedPmlXY: yee_fused<T, Tid, kFPmlXY | kFPmlZ><<<n, blk, 0, s>>>(A, p); break;
-        default: yee_fused<T, Tid, kFPmlXY | kFPmlZ | kFDisp | kFMisc><<<n, blk, 0, s>>>(A, p); break;
-    }
+    auto go = [&](auto odd) {
+        constexpr bool O = decltype(odd)::value;
+        switch (g) {
+            case kFusedInterior: yee_fused<T, Tid, 0, O><<<n, blk, 0, s>>>(A, p); break;
+            case kFusedPmlZ: yee_fused<T, Tid, kFPmlZ, O><<<n, blk, 0, s>>>(A, p); break;
+            case kFusedDisp: yee_fused<T, Tid, kFDisp, O><<<n, blk, 0, s>>>(A, p); break;
+            case kFusedPmlXY: yee_fused<T, Tid, kFPmlXY | kFPmlZ, O><<<n, blk, 0, s>>>(A, p); break;
+            default: yee_fused<T, Tid, kFPmlXY | kFPmlZ | kFDisp | kFMisc, O><<<n, blk, 0, s>>>(A, p); break;
+        }
+    };
+    if (A.e.Nx % 2) go(std::true_type{});
+    else go(std::false_type{});
 }
 
 }  // namespace aefdtd

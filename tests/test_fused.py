@@ -3,9 +3,9 @@ buffers) against the split half-step kernels and the reference.
 
 FP64: fields, plane sums and flux bit-identical to the split path on every
 scene shape (normal and custom mode, CPML on z or on all faces, dispersive
-spheres, 16-bit material ids, grids narrower than a fused tile, odd step
-counts that leave the current state in the second buffer set, steps in
-pieces); and fields SHA-identical to the reference core compiled from source.
+spheres, 16-bit material ids, grids narrower than a fused tile, odd Nx down
+to a single column, odd step counts that leave the current state in the
+second buffer set, steps in pieces); and fields SHA-identical to the reference core compiled from source.
 FP32: fields within 1e-5 relative of the split path (contraction may differ)."""
 import hashlib
 import os
@@ -54,6 +54,12 @@ SCENES = {
     "custom_many_materials": lambda p: scenes.custom_many_materials(precision=p, nsteps=60),
     "wide_sphere": lambda p: CF.sphere_scene(nx=130, ny=70, nz_total=96, dx=2.5e-9, pml=8, radius=30e-9, nsteps=120,
                                              nl=5, sensor_gap=4, precision=p),
+    # odd Nx: per-cell loads, and the last tile's odd width (recomputed next column in its last lane)
+    "odd_sphere": lambda p: CF.sphere_scene(nx=67, ny=21, nz_total=80, dx=2.5e-9, pml=8, radius=20e-9, nsteps=100,
+                                            nl=5, sensor_gap=4, precision=p),
+    "odd_custom": lambda p: CF.random_spheres_scene(n_total=(71, 40, 44), pml=6, n_dielectric=8, n_lorentz=3,
+                                                    r_range=(10e-9, 30e-9), nsteps=70, nl=5, precision=p, seed=9),
+    "thin_column": lambda p: scenes.thin_column(precision=p, nsteps=120),
 }
 
 
@@ -70,7 +76,7 @@ def test_fused_fp64_bit_identical_to_split(name):
         assert np.array_equal(x, y)
 
 
-@pytest.mark.parametrize("name", ["gold_sphere", "custom_box"])
+@pytest.mark.parametrize("name", ["gold_sphere", "custom_box", "odd_custom"])
 def test_fused_fp32_close_to_split(name):
     sc = SCENES[name](A.FP32)
     a = run(sc, [sc.nsteps], fused=True)
