@@ -398,12 +398,11 @@ def batch_sample(n_cells=512, steps=256, seed=2024):
     for s in sims:
         s.close()
     g = cells * done / dt / 1e9
-    # algorithmic bytes per step over all members (fused step where the x size is
-    # even, split half-steps elsewhere) against the L2 copy ceiling: the subsets
-    # are sized to stay in L2
+    # algorithmic bytes per step over all members (fused steps) against the L2
+    # copy ceiling: the subsets are sized to stay in L2
     from aether_b200 import metrics as MT
     fused_ok = os.environ.get("AEFDTD_NO_FUSED") is None
-    step_b = sum(MT.step_bytes(sc, A.FP32, fused=fused_ok and sc.total_dims()[0] % 2 == 0) for sc in scenes)
+    step_b = sum(MT.step_bytes(sc, A.FP32, fused=fused_ok) for sc in scenes)
     l2 = fdtd.copy_bandwidth(64 << 20, 50)
     l2_frac = step_b * done / dt / 1e9 / l2
     # the plain FP64 single-simulation path on the same cells: a seeded sample
