@@ -93,7 +93,7 @@ def test_static_plane_sums_match_stepping_path_twice(precision):
         sim.synchronize()
         free_first = torch.cuda.mem_get_info()[0]
         first = _static_sums(sim, planes, precision, out=outs[0])
-        assert free_first - torch.cuda.mem_get_info()[0] <= 8 << 20   # module load at most
+        assert free_first - torch.cuda.mem_get_info()[0] <= 16 << 20   # module load at most
         _check(sim, planes, first)
         assert np.any(first != 0)
         sim.step(37)
