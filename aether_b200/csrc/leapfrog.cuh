@@ -307,6 +307,35 @@ template <typename T> struct FusedSmem {
     T eze[2][kFusedMaxTY], eye[2][kFusedMaxTY];                // new E(k) of the column after it
 };
 
+// Load staging: each thread copies the values it reads at a plane (its pair of
+// the six fields, plus lane 0's x-1 neighbours, warp 0's row y-1, the column
+// warp's cell) into its own slot of a ring of stages with cp.async, planes
+// ahead of the march; it then waits only for its own copies (no barrier).
+template <typename T> struct alignas(16) FusedStage {
+    using T2 = typename Vec2<T>::type;
+    static constexpr int kRowThreads = 32 * (kFusedMaxTY + 1);
+    T2 f[6][kRowThreads];        // Hx Hy Hz Ex Ey Ez of each row thread's pair
+    T2 y[2][32];                 // Hz, Hx of row y0 - 1 (warp 0)
+    T c[6][32];                  // the column warp's cell: Hx Hy Hz Ex Ey Ez
+    T e[2][kFusedMaxTY + 1];     // Hz, Hy at x0 - 1 (lane 0 of each row warp)
+    T cy[2];                     // Hz, Hx of row y0 - 1 at the column after the tile
+};
+// stages in the ring: FP64 two (two CTAs fit an SM), FP32 three
+template <typename T> constexpr int fused_stages() { return sizeof(T) == 8 ? 2 : 3; }
+template <typename T> constexpr size_t fused_stage_bytes() { return fused_stages<T>() * sizeof(FusedStage<T>); }
+
+template <int BYTES> __device__ __forceinline__ void cp_async(void *smem, const void *gmem) {
+    const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+    if constexpr (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(s), "l"(gmem), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // One step over item (x0, y0, k0, k1): blockDim (32, TY + 2), TY <= kFusedMaxTY.
 // Warps 0 .. TY-1 own the rows, warp TY recomputes E of the row after them,
 // warp TY+1 (lane r for row r) recomputes E of the column after them.
@@ -338,6 +367,11 @@ __device__ __forceinline__ void fused_body(const FusedArgs<T, Tid> &A, int q, in
     const T *__restrict__ Hz = a.Hz;
     const Tid *__restrict__ mat = a.mat;
 
+    extern __shared__ __align__(16) unsigned char fused_dyn[];
+    FusedStage<T> *stage = reinterpret_cast<FusedStage<T> *>(fused_dyn);
+    constexpr int S = fused_stages<T>();
+    constexpr int TB = (int)sizeof(T);
+
     if (w == TY + 1) {
         // ---- the column warp: E of (ie, y0 + r) for r < hrows, lane r
         const bool on = lane < hrows;
@@ -345,17 +379,35 @@ __device__ __forceinline__ void fused_body(const FusedArgs<T, Tid> &A, int q, in
         const int jm0 = (y0 == 0) ? Ny - 1 : y0 - 1;
         const long long c = ie + (long long)j * Nx, cm = ie + (long long)j * a.mpitch;
         const long long cy = ie + (long long)jm0 * Nx;
+        const T *src[6] = {Hx, Hy, Hz, Ex, Ey, Ez};
+        auto issue = [&](int kq, int st) {
+            if (kq <= k1 && on) {
+                const long long o = (long long)(kq % Nz) * NxNy;
+#pragma unroll
+                for (int f = 0; f < 6; ++f) cp_async<TB>(&stage[st].c[f][lane], src[f] + c + o);
+                if (lane == 0) {
+                    cp_async<TB>(&stage[st].cy[0], Hz + cy + o);
+                    cp_async<TB>(&stage[st].cy[1], Hx + cy + o);
+                }
+            }
+            cp_async_commit();
+        };
+        for (int s0 = 0; s0 < S - 1; ++s0) issue(k0 + s0, s0);
         const int kb = (k0 == 0) ? Nz - 1 : k0 - 1;
         T hxp = __ldg(Hx + c + kb * NxNy), hyp = __ldg(Hy + c + kb * NxNy);
+        int m = __ldg(mat + cm + (long long)(k0 % Nz) * mNxNy);
         for (int kq = k0; kq <= k1; ++kq) {
             const int k = kq % Nz;
             const int buf = kq & 1;
-            const long long o = (long long)k * NxNy;
-            const T hx = __ldg(Hx + c + o), hy = __ldg(Hy + c + o), hz = __ldg(Hz + c + o);
-            const T ex = __ldg(Ex + c + o), ey = __ldg(Ey + c + o), ez = __ldg(Ez + c + o);
-            const int m = __ldg(mat + cm + (long long)k * mNxNy);
+            const int st = (kq - k0) % S;
+            issue(kq + S - 1, (kq - k0 + S - 1) % S);
+            const int m_next = (kq < k1) ? __ldg(mat + cm + (long long)((kq + 1) % Nz) * mNxNy) : 0;
+            cp_async_wait<S - 1>();
+            const FusedStage<T> &g = stage[st];
+            const T hx = g.c[0][lane], hy = g.c[1][lane], hz = g.c[2][lane];
+            const T ex = g.c[3][lane], ey = g.c[4][lane], ez = g.c[5][lane];
             T hzy = 0, hxy = 0;
-            if (lane == 0) { hzy = __ldg(Hz + cy + o); hxy = __ldg(Hx + cy + o); }
+            if (lane == 0) { hzy = g.cy[0]; hxy = g.cy[1]; }
             const T hz_up = __shfl_up_sync(kFullMask, hz, 1), hx_up = __shfl_up_sync(kFullMask, hx, 1);
             if (lane > 0) { hzy = hz_up; hxy = hx_up; }
             __syncthreads();
@@ -369,7 +421,9 @@ __device__ __forceinline__ void fused_body(const FusedArgs<T, Tid> &A, int q, in
             }
             hxp = hx;
             hyp = hy;
+            m = m_next;
         }
+        cp_async_wait<0>();
         return;   // no barrier follows the loop
     }
 
@@ -427,6 +481,58 @@ __device__ __forceinline__ void fused_body(const FusedArgs<T, Tid> &A, int q, in
     };
     if (pf)
         for (int kq = k0; kq <= min(k1, k0 + kFusedPrefetch - 1); ++kq) prefetch_plane(kq);
+    // staged copies of plane kq into stage st (every thread commits one group per plane)
+    const int tr = w * 32 + lane;
+    const T *src[6] = {Hx, Hy, Hz, Ex, Ey, Ez};
+    auto issue = [&](int kq, int st) {
+        if (kq <= k1 && active) {
+            const int kk = kq % Nz;
+            const long long o = (long long)kk * NxNy;
+            FusedStage<T> &g = stage[st];
+#pragma unroll
+            for (int f = 0; f < 6; ++f) {
+                if constexpr (ODD) {
+                    cp_async<TB>(&g.f[f][tr].x, src[f] + col + o);
+                    cp_async<TB>(&g.f[f][tr].y, src[f] + colb + o);
+                } else {
+                    cp_async<2 * TB>(&g.f[f][tr], src[f] + col + o);
+                }
+            }
+            if (lane == 0) {
+                cp_async<TB>(&g.e[0][w], Hz + im0 + (long long)j * Nx + o);
+                cp_async<TB>(&g.e[1][w], Hy + im0 + (long long)j * Nx + o);
+            }
+            if (r == 0) {
+                if constexpr (ODD) {
+                    cp_async<TB>(&g.y[0][lane].x, Hz + colym + o);
+                    cp_async<TB>(&g.y[0][lane].y, Hz + colymb + o);
+                    cp_async<TB>(&g.y[1][lane].x, Hx + colym + o);
+                    cp_async<TB>(&g.y[1][lane].y, Hx + colymb + o);
+                } else {
+                    cp_async<2 * TB>(&g.y[0][lane], Hz + colym + o);
+                    cp_async<2 * TB>(&g.y[1][lane], Hx + colym + o);
+                }
+            }
+        }
+        cp_async_commit();
+    };
+    auto load_ids = [&](int kq) {
+        I2 v;
+        v.x = 0;
+        v.y = 0;
+        if (active && kq <= k1) {
+            const long long om = (long long)(kq % Nz) * mNxNy;
+            if constexpr (ODD) {
+                v.x = __ldg(mat + colm + om);
+                v.y = __ldg(mat + colmb + om);
+            } else {
+                v = ldg2<I2>(mat + colm + om);
+            }
+        }
+        return v;
+    };
+    for (int s0 = 0; s0 < S - 1; ++s0) issue(k0 + s0, s0);
+    I2 mm = load_ids(k0);
     // H(k0 - 1): the z-1 neighbours of E(k0)
     const int kb = (k0 == 0) ? Nz - 1 : k0 - 1;
     T2 hxp, hyp, hzp;
@@ -443,20 +549,17 @@ __device__ __forceinline__ void fused_body(const FusedArgs<T, Tid> &A, int q, in
         const int buf = kq & 1;
         const long long o = (long long)k * NxNy;
         T2 hx, hy, hz, ex, ey, ez, hzy, hxy;
-        I2 mm;
         T hz_e = 0, hy_e = 0;                            // x-1 of lane 0
         if (pf && kq + kFusedPrefetch <= k1) prefetch_plane(kq + kFusedPrefetch);
+        issue(kq + S - 1, (kq - k0 + S - 1) % S);
+        const I2 mm_next = load_ids(kq + 1);
+        cp_async_wait<S - 1>();                          // this thread's copies of plane kq have landed
         if (active) {
-            hx = ld(Hx, col + o, colb + o); hy = ld(Hy, col + o, colb + o); hz = ld(Hz, col + o, colb + o);
-            ex = ld(Ex, col + o, colb + o); ey = ld(Ey, col + o, colb + o); ez = ld(Ez, col + o, colb + o);
-            if constexpr (ODD) {
-                mm.x = __ldg(mat + colm + (long long)k * mNxNy);
-                mm.y = __ldg(mat + colmb + (long long)k * mNxNy);
-            } else {
-                mm = ldg2<I2>(mat + colm + (long long)k * mNxNy);
-            }
-            if (lane == 0) { hz_e = __ldg(Hz + im0 + (long long)j * Nx + o); hy_e = __ldg(Hy + im0 + (long long)j * Nx + o); }
-            if (r == 0) { hzy = ld(Hz, colym + o, colymb + o); hxy = ld(Hx, colym + o, colymb + o); }
+            const FusedStage<T> &g = stage[(kq - k0) % S];
+            hx = g.f[0][tr]; hy = g.f[1][tr]; hz = g.f[2][tr];
+            ex = g.f[3][tr]; ey = g.f[4][tr]; ez = g.f[5][tr];
+            if (lane == 0) { hz_e = g.e[0][w]; hy_e = g.e[1][w]; }
+            if (r == 0) { hzy = g.y[0][lane]; hxy = g.y[1][lane]; }
             if (hrow) {   // rows read by the row above, and the column warp's x-1
                 sm.hz[buf][r][lane] = hz;
                 sm.hx[buf][r][lane] = hx;
@@ -509,7 +612,9 @@ __device__ __forceinline__ void fused_body(const FusedArgs<T, Tid> &A, int q, in
             hxp = hx; hyp = hy; hzp = hz;
             exp_ = nex; eyp = ney; ezp = nez;
         }
+        mm = mm_next;
     }
+    cp_async_wait<0>();
 }
 
 template <typename T, typename Tid, unsigned F> struct FusedBounds {
@@ -527,6 +632,19 @@ yee_fused(const __grid_constant__ FusedArgs<T, Tid> A, const int4 *__restrict__ 
     fused_body<T, Tid, F, ODD>(A, A.e.q, items[blockIdx.x]);
 }
 
+// One launch of one instantiation; its staging ring (dynamic shared memory,
+// above the 48 KiB default) is allowed once per instantiation.
+template <typename T, typename Tid, unsigned F, bool O>
+void launch_fused_one(const FusedArgs<T, Tid> &A, const int4 *p, int n, dim3 blk, cudaStream_t s) {
+    constexpr size_t dyn = fused_stage_bytes<T>();
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(yee_fused<T, Tid, F, O>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+        attr = true;
+    }
+    yee_fused<T, Tid, F, O><<<n, blk, dyn, s>>>(A, p);
+}
+
 template <typename T, typename Tid>
 void launch_fused_group_impl(const FusedArgs<T, Tid> &A, const int4 *items, int off, int n, int g, int ty,
                              cudaStream_t s) {
@@ -536,11 +654,11 @@ void launch_fused_group_impl(const FusedArgs<T, Tid> &A, const int4 *items, int 
     auto go = [&](auto odd) {
         constexpr bool O = decltype(odd)::value;
         switch (g) {
-            case kFusedInterior: yee_fused<T, Tid, 0, O><<<n, blk, 0, s>>>(A, p); break;
-            case kFusedPmlZ: yee_fused<T, Tid, kFPmlZ, O><<<n, blk, 0, s>>>(A, p); break;
-            case kFusedDisp: yee_fused<T, Tid, kFDisp, O><<<n, blk, 0, s>>>(A, p); break;
-            case kFusedPmlXY: yee_fused<T, Tid, kFPmlXY | kFPmlZ, O><<<n, blk, 0, s>>>(A, p); break;
-            default: yee_fused<T, Tid, kFPmlXY | kFPmlZ | kFDisp | kFMisc, O><<<n, blk, 0, s>>>(A, p); break;
+            case kFusedInterior: launch_fused_one<T, Tid, 0, O>(A, p, n, blk, s); break;
+            case kFusedPmlZ: launch_fused_one<T, Tid, kFPmlZ, O>(A, p, n, blk, s); break;
+            case kFusedDisp: launch_fused_one<T, Tid, kFDisp, O>(A, p, n, blk, s); break;
+            case kFusedPmlXY: launch_fused_one<T, Tid, kFPmlXY | kFPmlZ, O>(A, p, n, blk, s); break;
+            default: launch_fused_one<T, Tid, kFPmlXY | kFPmlZ | kFDisp | kFMisc, O>(A, p, n, blk, s); break;
         }
     };
     if (A.e.Nx % 2) go(std::true_type{});

@@ -118,8 +118,10 @@ void aefdtd_sim::construct(const aefdtd_grid_desc *d) {
     if (const char *pm = std::getenv("AEFDTD_PAIR")) pair_mask = unsigned(atoi(pm)) & 3u;
     pair_mask0 = pair_mask;
     h_reverse0 = h_reverse;
-    // fused time steps (AEFDTD_NO_FUSED=1: the split half-step kernels, same results in FP64)
-    if (std::getenv("AEFDTD_NO_FUSED")) use_fused = false;
+    // fused time steps: on by default where they measure faster (kFusedDefault),
+    // AEFDTD_FUSED=1 / 0 forces them on / off (same results in FP64 either way)
+    use_fused = kFusedDefault;
+    if (const char *fz = std::getenv("AEFDTD_FUSED")) use_fused = atoi(fz) != 0;
     if (const char *fy = std::getenv("AEFDTD_FUSED_TY")) fused_ty = std::clamp(atoi(fy), 1, kFusedMaxTY);
     if (const char *fk = std::getenv("AEFDTD_FUSED_KCHUNK")) fused_kchunk = std::max(0, atoi(fk));
     if (const char *ty = std::getenv("AEFDTD_TILE_Y")) {

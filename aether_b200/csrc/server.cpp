@@ -99,7 +99,8 @@ size_t estimate_job_bytes(const Job &j) {
     }
     // a job that runs alone in its subset takes the fused time step: a second
     // set of fields, E-side CPML psi and RC psi
-    if (g.mode != AEFDTD_MODE_OBLIQUE && !std::getenv("AEFDTD_NO_FUSED"))
+    const char *fz = std::getenv("AEFDTD_FUSED");
+    if (g.mode != AEFDTD_MODE_OBLIQUE && (fz ? atoi(fz) != 0 : kFusedDefault))
         b += 6 * N * es + 2 * (nxs * Ny * Nz + Nx * nys * Nz + Nx * Ny * nzs) * es + rc;
     const int seg = g.dft_block > 0 ? g.dft_block : 64;
     b += size_t(std::max(std::max(g.nt, j.steps), 1024)) * 12 * 8;        // plane-sum history

@@ -23,6 +23,8 @@
 
 namespace aefdtd {
 constexpr int kTileXHost = 32, kTileYHost = 4;   // kTileX, kTileY of yee.cuh
+// whether simulations take the fused time step unless AEFDTD_FUSED says otherwise
+constexpr bool kFusedDefault = false;
 }
 
 namespace aefdtd {

@@ -401,7 +401,7 @@ def batch_sample(n_cells=512, steps=256, seed=2024):
     # algorithmic bytes per step over all members (fused steps) against the L2
     # copy ceiling: the subsets are sized to stay in L2
     from aether_b200 import metrics as MT
-    fused_ok = os.environ.get("AEFDTD_NO_FUSED") is None
+    fused_ok = os.environ.get("AEFDTD_FUSED", "0") != "0"
     step_b = sum(MT.step_bytes(sc, A.FP32, fused=fused_ok) for sc in scenes)
     l2 = fdtd.copy_bandwidth(64 << 20, 50)
     l2_frac = step_b * done / dt / 1e9 / l2
@@ -527,7 +527,7 @@ def large_grid_sample(steps=128, seed=1234):
         e1.record(ext)
         e1.synchronize()
         ms = e0.elapsed_time(e1) / steps
-        sb = MT.step_bytes(sc, prec, fused=os.environ.get("AEFDTD_NO_FUSED") is None)
+        sb = MT.step_bytes(sc, prec, fused=os.environ.get("AEFDTD_FUSED", "0") != "0")
         out[name] = {"gcells": sc.cells / (ms * 1e-3) / 1e9, "ms_per_step": ms,
                      "step_frac": sb / (ms * 1e-3) / 1e9 / peak, "bytes_per_step": sb,
                      "device_gb": sim.dims().device_bytes / 1e9, "setup_seconds": setup}

@@ -28,9 +28,8 @@ def sha(f):
 
 
 def run(scene, pieces, fused):
-    old = os.environ.pop("AEFDTD_NO_FUSED", None)
-    if not fused:
-        os.environ["AEFDTD_NO_FUSED"] = "1"
+    old = os.environ.get("AEFDTD_FUSED")
+    os.environ["AEFDTD_FUSED"] = "1" if fused else "0"
     try:
         with fdtd.build_simulation(scene) as s:
             for n in pieces:
@@ -41,9 +40,10 @@ def run(scene, pieces, fused):
                 out["plane_sums"] = s.plane_sums()
             return out
     finally:
-        os.environ.pop("AEFDTD_NO_FUSED", None)
-        if old is not None:
-            os.environ["AEFDTD_NO_FUSED"] = old
+        if old is None:
+            os.environ.pop("AEFDTD_FUSED", None)
+        else:
+            os.environ["AEFDTD_FUSED"] = old
 
 
 SCENES = {
@@ -126,7 +126,12 @@ def test_fused_group_timings_cover_every_cell_once():
     """With group timing on, the fused groups report their owned cells in the
     E-side slots: together every cell once per step, nothing on the H side."""
     sc = SCENES["wide_sphere"](A.FP32)
-    with fdtd.build_simulation(sc) as s:
+    os.environ["AEFDTD_FUSED"] = "1"
+    try:
+        s = fdtd.build_simulation(sc)
+    finally:
+        os.environ.pop("AEFDTD_FUSED", None)
+    with s:
         s.enable_timing(True, mode=2)
         s.step(20)
         g = s.group_timings()

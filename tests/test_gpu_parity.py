@@ -146,7 +146,7 @@ def test_fp32_custom_mode_close_to_fp64_oracle():
 def test_interior_and_boundary_kernels_agree(prec, monkeypatch):
     """Items run by the curl-only interior kernels give the same cells as the
     full kernels: bit-identical in FP64, 1e-6 relative in FP32."""
-    monkeypatch.setenv("AEFDTD_NO_FUSED", "1")   # the split half-step kernels (the fused ones: test_fused.py)
+    monkeypatch.setenv("AEFDTD_FUSED", "0")   # the split half-step kernels (the fused ones: test_fused.py)
     sc = scenes.gold_sphere(precision=prec, nsteps=80)
     a = fdtd.run(sc)
     monkeypatch.setenv("AEFDTD_ALL_BOUNDARY", "1")
@@ -174,7 +174,7 @@ def test_concurrent_groups_match_serial_groups(name, monkeypatch):
 def test_z_chunking_does_not_change_results(kchunk, zunroll, monkeypatch):
     """Planes per work item and planes per interior-kernel iteration (odd
     chunks leave a one-plane tail in the two-plane loop) change no bit."""
-    monkeypatch.setenv("AEFDTD_NO_FUSED", "1")   # the split half-step kernels' items
+    monkeypatch.setenv("AEFDTD_FUSED", "0")   # the split half-step kernels' items
     sc = scenes.custom_box(nsteps=40)
     a = fdtd.run(sc)
     monkeypatch.setenv("AEFDTD_KCHUNK", kchunk)
@@ -201,7 +201,7 @@ def test_two_cells_per_thread_bit_identical(name, mask, monkeypatch):
     and flux bit-identical, including the periodic x wrap, ragged last items
     and odd Nx (which keeps one cell per thread)."""
     sc = _wide_cell(int(name[4:]), A.FP64) if name.startswith("wide") else getattr(scenes, name)(nsteps=120)
-    monkeypatch.setenv("AEFDTD_NO_FUSED", "1")   # the split half-step kernels
+    monkeypatch.setenv("AEFDTD_FUSED", "0")   # the split half-step kernels
     monkeypatch.setenv("AEFDTD_PAIR", "0")
     a = fdtd.run(sc)
     monkeypatch.setenv("AEFDTD_PAIR", mask)
@@ -216,7 +216,7 @@ def test_two_cells_per_thread_fp32_and_cell_cover(monkeypatch):
     """FP32 pair kernels within 1e-6 relative of one cell per thread, and the
     64- and 32-column items of each half-step still cover every cell once."""
     sc = _wide_cell(130, A.FP32, nsteps=100)
-    monkeypatch.setenv("AEFDTD_NO_FUSED", "1")   # the split half-step kernels
+    monkeypatch.setenv("AEFDTD_FUSED", "0")   # the split half-step kernels
     monkeypatch.setenv("AEFDTD_PAIR", "0")
     a = fdtd.run(sc)
     monkeypatch.setenv("AEFDTD_PAIR", "3")
@@ -260,7 +260,7 @@ def test_group_timing_mode_covers_every_cell_once(monkeypatch):
     """Mode-2 timing runs each group alone between events: same fields, and
     the groups of each half-step cover every cell of the grid once (split
     half-step kernels; the fused groups: test_fused.py)."""
-    monkeypatch.setenv("AEFDTD_NO_FUSED", "1")
+    monkeypatch.setenv("AEFDTD_FUSED", "0")
     sc = scenes.gold_sphere(nsteps=70)
     with fdtd.build_simulation(sc) as s1, fdtd.build_simulation(sc) as s2:
         s1.step(70)
