@@ -133,8 +133,8 @@ void aefdtd_sim::build_fused_work() {
         if ((f & ~(kPXY | kPZ)) == 0) return (int)kFusedPmlXY;
         return (int)kFusedAll;
     };
-    // chunk depth: fewest waves of resident CTAs (2 per SM in FP64, 3 in FP32), times the planes an item walks
-    const int slots = 148 * (fp64 ? 2 : 3);
+    // chunk depth: fewest waves of resident CTAs (1 per SM in FP64, 2 in FP32), times the planes an item walks
+    const int slots = 148 * (fp64 ? 1 : 2);
     fused_chunk = fused_kchunk;
     if (fused_chunk <= 0) {
         double best = 1e300;

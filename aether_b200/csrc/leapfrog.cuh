@@ -619,11 +619,9 @@ __device__ __forceinline__ void fused_body(const FusedArgs<T, Tid> &A, int q, in
 
 template <typename T, typename Tid, unsigned F> struct FusedBounds {
     static constexpr int kThreads = 32 * (kFusedMaxTY + 2);
-    // the curl-only and z-CPML variants keep two (FP64) or three (FP32) CTAs per
-    // SM; the variants with x/y CPML, poles or sources trade occupancy for
-    // fewer spills (they cover a small share of the cells)
-    static constexpr bool kHeavy = (F & (kFPmlXY | kFDisp | kFMisc)) != 0;
-    static constexpr int kMinBlocks = sizeof(T) == 8 ? (kHeavy ? 1 : 2) : (kHeavy ? 2 : 3);
+    // one (FP64) or two (FP32) CTAs per SM: registers for a march without
+    // spills (the staging ring keeps loads in flight at this occupancy)
+    static constexpr int kMinBlocks = sizeof(T) == 8 ? 1 : 2;
 };
 
 template <typename T, typename Tid, unsigned F, bool ODD>
