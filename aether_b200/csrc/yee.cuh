@@ -447,7 +447,9 @@ __device__ __forceinline__ void e_boundary_body(const StepArgs<T, Tid> &a, int q
             }
         }
 
-        // CPML and PEC planes in app_pml_Ex / Ey / Ez order.
+        // CPML and PEC planes in app_pml_Ex / Ey / Ez order. Every psi value the
+        // cell needs is loaded before any is stored (the six arrays are distinct),
+        // so the loads are in flight together.
         bool ze = false;
         int zn = 0;
         T bzk = 0, czk = 0;
@@ -456,21 +458,30 @@ __device__ __forceinline__ void e_boundary_body(const StepArgs<T, Tid> &a, int q
             zn = (k < a.pml_zm) ? k : k - (a.Nz - a.pml_zp) + a.pml_zm;
             if (ze) { bzk = __ldg(a.bz + k); czk = __ldg(a.cz + k); }
         }
+        const long long oy = i + (long long)yn * a.Nx + (long long)k * a.Nx * nys;
+        const long long ox = xn + (long long)j * nxs + (long long)k * nxs * a.Ny;
+        const long long oz = col + (long long)zn * NxNy;
+        T qy0 = 0, qy1 = 0, qx0 = 0, qx1 = 0, qz0 = 0, qz1 = 0;
+        if constexpr ((F & kFPmlXY) != 0) {
+            if (ye) { qy0 = a.psi_y0[oy]; qy1 = a.psi_y1[oy]; }
+            if (xe) { qx0 = a.psi_x0[ox]; qx1 = a.psi_x1[ox]; }
+        }
+        if constexpr ((F & kFPmlZ) != 0) {
+            if (ze) { qz0 = a.psi_z0[oz]; qz1 = a.psi_z1[oz]; }
+        }
         // Ex: y block, then z block
         if constexpr ((F & kFPmlXY) != 0) {
             if (ye) {
-                T *pp = a.psi_y0 + i + (long long)yn * a.Nx + (long long)k * a.Nx * nys;
-                const T ps = cpml_rec(byj, *pp, cyj, dHz_y);
-                *pp = ps;
+                const T ps = cpml_rec(byj, qy0, cyj, dHz_y);
+                a.psi_y0[oy] = ps;
                 nex += c.C4 * ps;
             }
             if (a.py && j == 0) nex = 0;
         }
         if constexpr ((F & kFPmlZ) != 0) {
             if (ze) {
-                T *pp = a.psi_z0 + col + (long long)zn * NxNy;
-                const T ps = cpml_rec(bzk, *pp, czk, dHy_z);
-                *pp = ps;
+                const T ps = cpml_rec(bzk, qz0, czk, dHy_z);
+                a.psi_z0[oz] = ps;
                 nex -= c.C4 * ps;
             }
             if (a.pz && k == 0) nex = 0;
@@ -478,18 +489,16 @@ __device__ __forceinline__ void e_boundary_body(const StepArgs<T, Tid> &a, int q
         // Ey: x block, then z block
         if constexpr ((F & kFPmlXY) != 0) {
             if (xe) {
-                T *pp = a.psi_x0 + xn + (long long)j * nxs + (long long)k * nxs * a.Ny;
-                const T ps = cpml_rec(bxi, *pp, cxi, dHz_x);
-                *pp = ps;
+                const T ps = cpml_rec(bxi, qx0, cxi, dHz_x);
+                a.psi_x0[ox] = ps;
                 ney -= c.C4 * ps;
             }
             if (a.px && i == 0) ney = 0;
         }
         if constexpr ((F & kFPmlZ) != 0) {
             if (ze) {
-                T *pp = a.psi_z1 + col + (long long)zn * NxNy;
-                const T ps = cpml_rec(bzk, *pp, czk, dHx_z);
-                *pp = ps;
+                const T ps = cpml_rec(bzk, qz1, czk, dHx_z);
+                a.psi_z1[oz] = ps;
                 ney += c.C4 * ps;
             }
             if (a.pz && k == 0) ney = 0;
@@ -497,16 +506,14 @@ __device__ __forceinline__ void e_boundary_body(const StepArgs<T, Tid> &a, int q
         // Ez: x block, then y block
         if constexpr ((F & kFPmlXY) != 0) {
             if (xe) {
-                T *pp = a.psi_x1 + xn + (long long)j * nxs + (long long)k * nxs * a.Ny;
-                const T ps = cpml_rec(bxi, *pp, cxi, dHy_x);
-                *pp = ps;
+                const T ps = cpml_rec(bxi, qx1, cxi, dHy_x);
+                a.psi_x1[ox] = ps;
                 nez += c.C4 * ps;
             }
             if (a.px && i == 0) nez = 0;
             if (ye) {
-                T *pp = a.psi_y1 + i + (long long)yn * a.Nx + (long long)k * a.Nx * nys;
-                const T ps = cpml_rec(byj, *pp, cyj, dHx_y);
-                *pp = ps;
+                const T ps = cpml_rec(byj, qy1, cyj, dHx_y);
+                a.psi_y1[oy] = ps;
                 nez -= c.C4 * ps;
             }
             if (a.py && j == 0) nez = 0;
@@ -647,21 +654,31 @@ __device__ __forceinline__ void h_boundary_body(const StepArgs<T, Tid> &a, int q
             zn = (k < a.pml_zm) ? k : k - (a.Nz - a.pml_zp) + a.pml_zm;
             if (zh) { bzk = __ldg(a.bz + k); czk = __ldg(a.cz + k); }
         }
+        // every psi load of the cell before any store (distinct arrays)
+        const long long oy = i + (long long)yn * a.Nx + (long long)k * a.Nx * nys;
+        const long long ox = xn + (long long)j * nxs + (long long)k * nxs * a.Ny;
+        const long long oz = col + (long long)zn * NxNy;
+        T qy0 = 0, qy1 = 0, qx0 = 0, qx1 = 0, qz0 = 0, qz1 = 0;
+        if constexpr ((F & kFPmlXY) != 0) {
+            if (yh) { qy0 = a.psi_y0[oy]; qy1 = a.psi_y1[oy]; }
+            if (xh) { qx0 = a.psi_x0[ox]; qx1 = a.psi_x1[ox]; }
+        }
+        if constexpr ((F & kFPmlZ) != 0) {
+            if (zh) { qz0 = a.psi_z0[oz]; qz1 = a.psi_z1[oz]; }
+        }
         // Hx: y block, then z block
         if constexpr ((F & kFPmlXY) != 0) {
             if (yh) {
-                T *pp = a.psi_y0 + i + (long long)yn * a.Nx + (long long)k * a.Nx * nys;
-                const T ps = cpml_rec(byj, *pp, cyj, dEz_y);
-                *pp = ps;
+                const T ps = cpml_rec(byj, qy0, cyj, dEz_y);
+                a.psi_y0[oy] = ps;
                 nhx -= a.dtm * ps;
             }
             if (a.py && j == a.Ny - 1) nhx = 0;
         }
         if constexpr ((F & kFPmlZ) != 0) {
             if (zh) {
-                T *pp = a.psi_z0 + col + (long long)zn * NxNy;
-                const T ps = cpml_rec(bzk, *pp, czk, dEy_z);
-                *pp = ps;
+                const T ps = cpml_rec(bzk, qz0, czk, dEy_z);
+                a.psi_z0[oz] = ps;
                 nhx += a.dtm * ps;
             }
             if (a.pz && k == a.Nz - 1) nhx = 0;
@@ -669,18 +686,16 @@ __device__ __forceinline__ void h_boundary_body(const StepArgs<T, Tid> &a, int q
         // Hy: x block, then z block
         if constexpr ((F & kFPmlXY) != 0) {
             if (xh) {
-                T *pp = a.psi_x0 + xn + (long long)j * nxs + (long long)k * nxs * a.Ny;
-                const T ps = cpml_rec(bxi, *pp, cxi, dEz_x);
-                *pp = ps;
+                const T ps = cpml_rec(bxi, qx0, cxi, dEz_x);
+                a.psi_x0[ox] = ps;
                 nhy += a.dtm * ps;
             }
             if (a.px && i == a.Nx - 1) nhy = 0;
         }
         if constexpr ((F & kFPmlZ) != 0) {
             if (zh) {
-                T *pp = a.psi_z1 + col + (long long)zn * NxNy;
-                const T ps = cpml_rec(bzk, *pp, czk, dEx_z);
-                *pp = ps;
+                const T ps = cpml_rec(bzk, qz1, czk, dEx_z);
+                a.psi_z1[oz] = ps;
                 nhy -= a.dtm * ps;
             }
             if (a.pz && k == a.Nz - 1) nhy = 0;
@@ -688,16 +703,14 @@ __device__ __forceinline__ void h_boundary_body(const StepArgs<T, Tid> &a, int q
         // Hz: x block, then y block
         if constexpr ((F & kFPmlXY) != 0) {
             if (xh) {
-                T *pp = a.psi_x1 + xn + (long long)j * nxs + (long long)k * nxs * a.Ny;
-                const T ps = cpml_rec(bxi, *pp, cxi, dEy_x);
-                *pp = ps;
+                const T ps = cpml_rec(bxi, qx1, cxi, dEy_x);
+                a.psi_x1[ox] = ps;
                 nhz -= a.dtm * ps;
             }
             if (a.px && i == a.Nx - 1) nhz = 0;
             if (yh) {
-                T *pp = a.psi_y1 + i + (long long)yn * a.Nx + (long long)k * a.Nx * nys;
-                const T ps = cpml_rec(byj, *pp, cyj, dEx_y);
-                *pp = ps;
+                const T ps = cpml_rec(byj, qy1, cyj, dEx_y);
+                a.psi_y1[oy] = ps;
                 nhz += a.dtm * ps;
             }
             if (a.py && j == a.Ny - 1) nhz = 0;
