@@ -40,11 +40,13 @@ UNITS = [
     ("oblique.cu", ["--fmad=false"]),
     ("runtime.cpp", None),
     ("fused.cpp", None),
+    ("tma.cpp", None),
     ("oblique_driver.cpp", None),
     ("batch.cpp", None),
     ("server.cpp", None),
 ]
-HEADERS = ["aefdtd_dev.hpp", "kernels.hpp", "sensors.cuh", "yee.cuh", "leapfrog.cuh", "sim.hpp"]
+HEADERS = ["aefdtd_dev.hpp", "kernels.hpp", "sensors.cuh", "yee.cuh", "leapfrog.cuh", "sim.hpp", "mbar.cuh",
+           "interior_tma.cuh"]
 
 
 def _stale(obj, deps):

@@ -15,6 +15,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <cuda.h>
 #include <vector_types.h>
 
 namespace aefdtd {
@@ -117,12 +118,37 @@ enum { kFusedInterior = 0, kFusedPmlZ = 1, kFusedDisp = 2, kFusedAll = 3, kFused
 // Item groups of one half-step: a device array of int4 items (x0, y0, k0,
 // k1) sorted by group; group g is items [off[g], off[g] + n[g]).
 enum { kGroupInterior = 0, kGroupPmlZ = 1, kGroupDisp = 2, kGroupAll = 3, kGroupPmlXY = 4, kGroups = 5 };
+// Staged interior half-steps (interior_tma.cuh): tiles of 64 x 8 columns
+// whose planes are brought into a shared-memory ring by tensor copies.
+constexpr int kTmaTileX = 64;
+constexpr int kTmaTileY = 8;
+// Tensor maps of one half-step's staged kernel over this simulation's own
+// field arrays (3-D, x y z in elements; s = element size).
+struct TmaMaps {
+    CUtensorMap w[2];   // x-halo blocks {64 + 16/s, 8, 1}: E side Hz, Hy; H side Ez, Ey
+    CUtensorMap c[2];   // periodic-wrap columns {16/s, 8, 1} of the same two arrays
+    CUtensorMap r[2];   // y-halo rows {64, 1, 1}: E side Hz, Hx; H side Ez, Ex
+    CUtensorMap b[4];   // own blocks {64, 8, 1}: E side Hx, Ex, Ey, Ez; H side Ex, Hx, Hy, Hz
+    CUtensorMap mat;    // own block of material ids (E side)
+};
+// One half-step's staged launch: units (x0, y0, k0, k1) taken by the CTAs
+// in turn through a device counter.
+struct TmaPlan {
+    TmaMaps maps;
+    const int4 *units;
+    int nunits;
+    int *ctr;           // [0] next unit, [1] CTAs done (the last CTA resets both)
+    int grid;           // CTAs per launch
+    int stages;         // ring stages (4 or 6)
+    long long cells;    // cells per launch
+};
 struct WorkSplit {
     int off[kGroups];
     int n[kGroups];
     int unroll;                     // z-planes per iteration of the interior kernels (1 or 2)
     int tile_y;                     // tile height: CTAs of 32 x tile_y threads (2, 4 or 8)
     unsigned pair_mask;             // bit g: group g runs the two-cells-per-thread kernels on 64-column items
+    const TmaPlan *tma = nullptr;   // set: the interior group is the staged kernel over these units
 };
 // x0 flag of a 32-column item in a group of 64-column (pair) items
 constexpr int kHalfItem = 1 << 30;

@@ -167,7 +167,11 @@ struct aefdtd_batch {
 aefdtd_batch::~aefdtd_batch() {
     set_device();
     for (auto &ln : lanes) if (ln.stream) cudaStreamSynchronize(ln.stream);
-    for (auto &m : members) m.sim->batch = nullptr;
+    for (auto &m : members) {
+        m.sim->batch = nullptr;
+        m.sim->tma_allowed = true;
+        m.sim->work_dirty = true;
+    }
     for (auto &u : subsets) u.release(dev_bytes);
     for (auto &ln : lanes) ln.destroy();
 }
@@ -758,6 +762,8 @@ void batch_detach(void *bp, aefdtd_sim *s) {
     }
     b->members.erase(b->members.begin() + i);
     s->batch = nullptr;
+    s->tma_allowed = true;
+    s->work_dirty = true;
 }
 }  // namespace aefdtd
 
@@ -846,6 +852,8 @@ aefdtd_status aefdtd_batch_add(aefdtd_batch *b, aefdtd_sim *s, int32_t steps) {
         if (s->Nz >= 32768) fail(AEFDTD_BAD_ARG, "batch members need Nz < 32768 (k1 << 16 in an int32 item)");
         s->set_device();
         s->finalize_tables();
+        s->tma_allowed = false;      // merged lists take every interior item
+        s->work_dirty = true;
         s->build_work();             // lists for its subset follow in build_subset
         if (!b->typed) {
             b->typed = true;

@@ -26,43 +26,20 @@
 
 #include "aefdtd_dev.hpp"
 #include "kernels.hpp"
+#include "mbar.cuh"
 
 namespace aefdtd {
 
 namespace {
 
-__device__ __forceinline__ uint32_t saddr(const void *p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
-
-__device__ __forceinline__ void bar_init(uint64_t *b, uint32_t n) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(b)), "r"(n) : "memory");
-}
-__device__ __forceinline__ void bar_expect_tx(uint64_t *b, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(b)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool bar_try(uint64_t *b, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(saddr(b)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
+using mbar::saddr;
+__device__ __forceinline__ void bar_init(uint64_t *b, uint32_t n) { mbar::init(b, n); }
+__device__ __forceinline__ void bar_expect_tx(uint64_t *b, uint32_t bytes) { mbar::expect_tx(b, bytes); }
 // gives up after `limit` SM cycles (2^32 by default, about 2 s)
 __device__ __forceinline__ bool bar_wait(uint64_t *b, uint32_t parity, long long limit) {
-    if (bar_try(b, parity)) return true;
-    const long long t0 = clock64();
-    while (!bar_try(b, parity))
-        if (clock64() - t0 > limit) return false;
-    return true;
+    return mbar::wait(b, parity, limit);
 }
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *b) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                 ::"r"(saddr(dst)), "l"(src), "r"(bytes), "r"(saddr(b))
-                 : "memory");
-}
+using mbar::bulk_g2s;
 __device__ __forceinline__ uint32_t to_tf32(float x) {
     uint32_t r;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));

@@ -124,6 +124,10 @@ void aefdtd_sim::construct(const aefdtd_grid_desc *d) {
     if (const char *fz = std::getenv("AEFDTD_FUSED")) use_fused = atoi(fz) != 0;
     if (const char *fy = std::getenv("AEFDTD_FUSED_TY")) fused_ty = std::clamp(atoi(fy), 1, kFusedMaxTY);
     if (const char *fk = std::getenv("AEFDTD_FUSED_KCHUNK")) fused_kchunk = std::max(0, atoi(fk));
+    if (const char *tm = std::getenv("AEFDTD_TMA")) use_tma = atoi(tm) != 0;
+    if (const char *tu = std::getenv("AEFDTD_TMA_UNIT")) tma_unit = std::clamp(atoi(tu), 1, 4096);
+    if (const char *tc = std::getenv("AEFDTD_TMA_CTAS")) tma_ctas = std::clamp(atoi(tc), 0, 2);
+    if (const char *tg = std::getenv("AEFDTD_TMA_STAGES")) tma_stages = atoi(tg) >= 6 ? 6 : 4;
     if (const char *ty = std::getenv("AEFDTD_TILE_Y")) {
         const int v = atoi(ty);
         tile_y = (v == 2 || v == 8) ? v : 4;
@@ -911,6 +915,8 @@ void aefdtd_sim::completion_check() {
 
 template <typename T, typename Tid>
 void aefdtd_sim::run_steps(int n) {
+    // the staged kernels' tensor maps bake in the field and id arrays
+    if (!work_dirty && (wsE.tma || wsH.tma) && !tma_maps_current()) work_dirty = true;
     if (work_dirty) { build_work(); graphs_dirty = true; fwork_dirty = true; }
     const bool fused = fused_eligible();
     if (fused) {
@@ -1269,6 +1275,79 @@ void aefdtd_sim::build_work() {
         if (f == kPXY || f == (kPXY | kPZ)) return (int)kGroupPmlXY;
         return (int)kGroupAll;
     };
+    // Staged interior units: 64 x 8 tiles (two 32-column tiles by 8 / ty
+    // rows) inside the grid, runs of planes where every covered tile is
+    // curl-only for the half-step, cut into units of at most tma_unit
+    // planes. Their tiles are taken out of the lists below; the other
+    // curl-only tiles run with the z-CPML group's kernels (which leave cells
+    // outside the z-CPML ranges at the curl update).
+    bool tma = tma_possible();
+    std::vector<unsigned char> taken[2];
+    std::vector<int> tunits[2];
+    long long tcells[2] = {0, 0};
+    if (tma) {
+        const int rb = kTmaTileY / ty, nA = Nx / kTmaTileX, nB = Ny / kTmaTileY;
+        for (int half = 0; half < 2; half++) {
+            taken[half].assign(size_t(tiles) * Nz, 0);
+            auto interior = [&](int A, int B, int k) {
+                for (int bb = 0; bb < rb; bb++)
+                    for (int aa = 0; aa < 2; aa++) {
+                        const unsigned f = feat[(size_t(k) * nty + B * rb + bb) * ntx + 2 * A + aa];
+                        if ((half == 0 ? group_e(f) : group_h(f)) != kGroupInterior) return false;
+                    }
+                return true;
+            };
+            std::vector<int4> runs;   // (x0, y0, k0, k1) of every curl-only run
+            long long planes = 0;
+            for (int B = 0; B < nB; B++)
+                for (int A = 0; A < nA; A++)
+                    for (int k = 0; k < Nz;) {
+                        if (!interior(A, B, k)) { k++; continue; }
+                        int ke = k + 1;
+                        while (ke < Nz && interior(A, B, ke)) ke++;
+                        runs.push_back(make_int4(A * kTmaTileX, B * kTmaTileY, k, ke));
+                        for (int kk = k; kk < ke; kk++)
+                            for (int bb = 0; bb < rb; bb++)
+                                for (int aa = 0; aa < 2; aa++) taken[half][(size_t(kk) * nty + B * rb + bb) * ntx + 2 * A + aa] = 1;
+                        tcells[half] += (long long)(ke - k) * kTmaTileX * kTmaTileY;
+                        planes += ke - k;
+                        k = ke;
+                    }
+            // Guided sizes: CTAs take units in list order, so a unit's length
+            // follows the planes still unassigned, R / (2 x CTAs) capped at
+            // tma_unit: long units first, single planes at the end, and the
+            // CTAs finish within about one plane of each other.
+            int nsm = 148;
+            AE_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+            const long long ctas = (long long)std::max(1, tma_ctas) * nsm;
+            // The H list runs top plane first (the planes E touched last), its
+            // runs cut from the top down.
+            if (half == 1) std::reverse(runs.begin(), runs.end());
+            long long rem = planes;
+            for (const int4 &r : runs)
+                for (int k = r.z, ke = r.w; k < ke;) {
+                    const int len = (int)std::clamp<long long>(rem / (2 * ctas), 1, tma_unit);
+                    if (half == 0) {
+                        const int zb = std::min(ke, k + len);
+                        tunits[half].insert(tunits[half].end(), {r.x, r.y, k, zb});
+                        rem -= zb - k;
+                        k = zb;
+                    } else {
+                        const int za = std::max(k, ke - len);
+                        tunits[half].insert(tunits[half].end(), {r.x, r.y, za, ke});
+                        rem -= ke - za;
+                        ke = za;
+                    }
+                }
+        }
+        tma = !tunits[0].empty() || !tunits[1].empty();
+        if (tma && !build_tma_maps()) tma = false;
+        if (!tma) {
+            taken[0].clear(); taken[1].clear();
+            tunits[0].clear(); tunits[1].clear();
+            tcells[0] = tcells[1] = 0;
+        }
+    }
     // items: within each tile (or pair of tiles) and z-chunk, runs of planes
     // of one group; dispersive E planes one plane per item (their cells carry
     // the pole state)
@@ -1279,9 +1358,12 @@ void aefdtd_sim::build_work() {
             for (int a = 0; a < ntx; a += step_a) {
                 const int z0 = c * kchunk, z1 = std::min(Nz, (c + 1) * kchunk);
                 for (int half = 0; half < 2; half++) {
+                    // -1: the tile's plane runs in a staged unit
                     auto grp = [&](int t, int k) {
-                        const unsigned f = feat[(size_t(k) * nty + b) * ntx + t];
-                        return half == 0 ? group_e(f) : group_h(f);
+                        const size_t fi = (size_t(k) * nty + b) * ntx + t;
+                        if (tma && taken[half][fi]) return -1;
+                        const int g = half == 0 ? group_e(feat[fi]) : group_h(feat[fi]);
+                        return (tma && g == kGroupInterior) ? (int)kGroupPmlZ : g;
                     };
                     auto emit = [&](int g, int x0, int za, int zb) {
                         std::vector<int> &dst = v[half][g];
@@ -1298,7 +1380,7 @@ void aefdtd_sim::build_work() {
                             int ze = z + 1;
                             if (!(half == 0 && g == kGroupDisp))
                                 while (ze < zb && grp(t, ze) == g) ze++;
-                            emit(g, t * tx | ((pmask >> g) & 1u ? kHalfItem : 0), z, ze);
+                            if (g >= 0) emit(g, t * tx | ((pmask >> g) & 1u ? kHalfItem : 0), z, ze);
                             z = ze;
                         }
                     };
@@ -1310,7 +1392,7 @@ void aefdtd_sim::build_work() {
                     // plane k pairs when both tiles (or the last, lone tile) are in one pair group
                     auto paired = [&](int k) {
                         const int g = grp(a, k);
-                        return ((pmask >> g) & 1u) && (!right || grp(a + 1, k) == g);
+                        return g >= 0 && ((pmask >> g) & 1u) && (!right || grp(a + 1, k) == g);
                     };
                     int z = z0;
                     while (z < z1) {
@@ -1358,6 +1440,37 @@ void aefdtd_sim::build_work() {
             grp_cells[half][g] = c;
         }
     }
+    // staged units: E then H
+    for (int half = 0; half < 2; half++) {
+        WorkSplit &w = half == 0 ? wsE : wsH;
+        w.tma = nullptr;
+        tma_plan[half].nunits = 0;
+    }
+    if (tma) {
+        std::vector<int> tu = tunits[0];
+        tu.insert(tu.end(), tunits[1].begin(), tunits[1].end());
+        tma_units.alloc(tu.size() * sizeof(int), dev_bytes);
+        AE_CUDA(cudaMemcpy(tma_units.p, tu.data(), tu.size() * sizeof(int), cudaMemcpyHostToDevice));
+        if (!tma_ctr.p) tma_ctr.alloc(4 * sizeof(int), dev_bytes);
+        AE_CUDA(cudaMemsetAsync(tma_ctr.p, 0, 4 * sizeof(int), stream));
+        int nsm = 148;
+        AE_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+        for (int half = 0; half < 2; half++) {
+            TmaPlan &p = tma_plan[half];
+            p.nunits = (int)(tunits[half].size() / 4);
+            p.units = tma_units.as<int4>() + (half ? tunits[0].size() / 4 : 0);
+            p.ctr = tma_ctr.as<int>() + 2 * half;
+            // tma_ctas 0: one unit per CTA; else units taken in turn by tma_ctas CTAs per SM
+            p.grid = tma_ctas == 0 ? p.nunits : std::min(p.nunits, tma_ctas * nsm);
+            p.stages = tma_stages;
+            p.cells = tcells[half];
+            if (p.nunits == 0) continue;
+            WorkSplit &w = half == 0 ? wsE : wsH;
+            w.tma = &p;
+            w.n[kGroupInterior] = p.grid;
+            grp_cells[half][kGroupInterior] = p.cells;
+        }
+    }
     items_host = all;
     items.alloc(std::max<size_t>(all.size(), 4) * sizeof(int), dev_bytes);
     graphs_dirty = true;   // captured segments point at the old lists
@@ -1372,6 +1485,8 @@ void aefdtd_sim::check_err() {
     AE_CUDA(cudaStreamSynchronize(stream));
     if (h) {
         AE_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), stream));
+        // a staged launch that gave up may have left its unit counters set
+        if (tma_ctr.p) AE_CUDA(cudaMemsetAsync(tma_ctr.p, 0, tma_ctr.n, stream));
         fail(AEFDTD_TIMEOUT, "a bounded device wait ran out");
     }
 }

@@ -374,6 +374,22 @@ struct aefdtd_sim {
     void swap_sets();
     template <typename T, typename Tid> void make_fused_args(FusedArgs<T, Tid> &A, const StepScalars *tbl, bool other);
     template <typename T, typename Tid> void enqueue_segment_fused(int L, StepScalars *tbl, bool record);
+    // staged interior half-steps (interior_tma.cuh): curl-only 64 x 8 tiles
+    // whose planes arrive through tensor copies. Not for batch members (their
+    // merged lists take every interior item) or the oblique driver (whose
+    // second grid runs on the same lists).
+    bool use_tma = false;            // AEFDTD_TMA
+    bool tma_allowed = true;         // cleared while the simulation is in a batch
+    int tma_unit = 8;                // planes per unit (AEFDTD_TMA_UNIT)
+    int tma_ctas = 0;                // AEFDTD_TMA_CTAS: 0 one unit per CTA; 1 or 2 CTAs per SM taking
+                                     // units in turn (persistent)
+    int tma_stages = 4;              // ring stages (AEFDTD_TMA_STAGES, 4 or 6)
+    TmaPlan tma_plan[2] = {};        // E, H half-step
+    DBuf tma_units, tma_ctr;
+    const void *tma_ptrs[7] = {};    // the arrays the maps were encoded over (fields, ids)
+    bool tma_possible() const;       // the grid and the mode allow the staged kernels
+    bool build_tma_maps();           // false when the driver refuses a map
+    bool tma_maps_current() const;
     // completion sensor, energy mode (CompletionSensor(coeff), s_completion.cpp)
     double cc_coeff = 0;            // > 0: enabled
     int cc_step = 500;              // checked after steps t with t % cc_step == 0
@@ -411,6 +427,8 @@ inline aefdtd_sim::~aefdtd_sim() {
     tables.release(t);
     for (auto &gx : graph_exec) if (gx.second) reap_graph(gx.second, device);
     items.release(t);
+    tma_units.release(t);
+    tma_ctr.release(t);
     fm_tbl.release(t);
     if (obl) {
         for (int c = 0; c < 6; c++) { obl->Fi[c].release(t); obl->psiEi[c].release(t); obl->psiHi[c].release(t); }

@@ -1064,6 +1064,12 @@ h_boundary_batch(const StepArgs<T, Tid> *__restrict__ args, int q, const int4 *_
     h_boundary_body<T, Tid, F>(args[b.w], q, batch_item(b));
 }
 
+}  // namespace aefdtd
+
+#include "interior_tma.cuh"
+
+namespace aefdtd {
+
 // ---- launchers: group g of a half-step's WorkSplit ------------------------
 template <typename T, typename Tid>
 void launch_e_group_impl(const StepArgs<T, Tid> &a, const int4 *items, const WorkSplit &w, int g, cudaStream_t s) {
@@ -1073,7 +1079,8 @@ void launch_e_group_impl(const StepArgs<T, Tid> &a, const int4 *items, const Wor
     const dim3 blk(kTileX, w.tile_y);
     switch (g) {
         case kGroupInterior:
-            if (w.pair_mask & (1u << kGroupInterior)) e_interior_v2<T, Tid, false><<<n, blk, 0, s>>>(a, p);
+            if (w.tma) launch_tma_impl<T, Tid, false>(a, *w.tma, s);
+            else if (w.pair_mask & (1u << kGroupInterior)) e_interior_v2<T, Tid, false><<<n, blk, 0, s>>>(a, p);
             else if (w.unroll >= 2) e_interior<T, Tid, 2><<<n, blk, 0, s>>>(a, p);
             else e_interior<T, Tid, 1><<<n, blk, 0, s>>>(a, p);
             break;
@@ -1096,7 +1103,8 @@ void launch_h_group_impl(const StepArgs<T, Tid> &a, const int4 *items, const Wor
     const dim3 blk(kTileX, w.tile_y);
     switch (g) {
         case kGroupInterior:
-            if (w.pair_mask & (1u << kGroupInterior)) h_interior_v2<T, Tid, false><<<n, blk, 0, s>>>(a, p);
+            if (w.tma) launch_tma_impl<T, Tid, true>(a, *w.tma, s);
+            else if (w.pair_mask & (1u << kGroupInterior)) h_interior_v2<T, Tid, false><<<n, blk, 0, s>>>(a, p);
             else if (w.unroll >= 2) h_interior<T, Tid, 2><<<n, blk, 0, s>>>(a, p);
             else h_interior<T, Tid, 1><<<n, blk, 0, s>>>(a, p);
             break;

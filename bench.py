@@ -275,6 +275,7 @@ def run_gpu_arm(args):
             "e_ms": e_ms / tsteps, "h_ms": h_ms / tsteps, "s_ms": s_ms / tsteps,
             "bytes": kb, "launches": launches, "clocks": cs.summary(), "cells": cells,
             "groups": groups, "step_bytes": MT.step_bytes(scene, fused=fused), "fused": fused,
+            "staged": not fused and os.environ.get("AEFDTD_TMA", "0") != "0",
         }
         sim.close()
         log(f"[{prec_name}] {results[prec_name]['gcells']:.2f} Gcell/s  E {e_ms / tsteps * 1e3:.1f} us  "
@@ -625,6 +626,9 @@ def main():
         if r["fused"]:
             kernel = f"yee_fused<{'double' if s == 8 else 'float'}, uint8, 0>"
             traffic_key = ("yee_fused", "fp64" if s == 8 else "fp32")
+        elif r["staged"]:
+            kernel = f"interior_tma<{'double' if s == 8 else 'float'}, uint8, E>"
+            traffic_key = ("interior_tma", "fp64" if s == 8 else "fp32")
         return {"bound": "hbm", "kernel": kernel, "achieved": ach, "peak": peak, "unit": "GB/s",
                 "frac": ach / peak, "peak_source": peak_kind, "traffic": profiled_traffic(*traffic_key),
                 "algorithmic_bytes_per_launch": b, "launch_us": ms * 1e3, "cells_per_launch": cells,
