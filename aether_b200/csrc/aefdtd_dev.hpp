@@ -280,6 +280,7 @@ template <typename T> struct AccumArgs {
     const T *S;              // [K][6][P]
     const double2 *WE, *WH;  // [nk][nl]
     double2 *acc;            // [6][nl][P]
+    int mma;                 // 1: the FP64 tensor-path kernel (dft_accumulate_mma), 0: FMA kernel
 };
 
 struct FluxArgs {

@@ -31,15 +31,23 @@ void aefdtd_sim::construct(const aefdtd_grid_desc *d) {
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) fail(AEFDTD_NO_DEVICE, "no CUDA device visible");
     if (device < 0 || device >= ndev) fail(AEFDTD_BAD_ARG, "device ordinal out of range");
     AE_CUDA(cudaSetDevice(device));
-    AE_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-    for (auto &x : side) AE_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+    // Stream priorities: the half-steps and sensors on the highest, the DFT
+    // blocks (which run beside the next segment's steps) on the lowest, so
+    // that free SM slots go to the step's kernels first. Captured kernels
+    // keep their stream's priority (graphs instantiate with node priorities).
+    // AEFDTD_PRIO=0: every stream at the default priority.
+    int lo = 0, hi = 0;
+    if (!(std::getenv("AEFDTD_PRIO") && atoi(std::getenv("AEFDTD_PRIO")) == 0))
+        AE_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    AE_CUDA(cudaStreamCreateWithPriority(&stream, cudaStreamNonBlocking, hi));
+    for (auto &x : side) AE_CUDA(cudaStreamCreateWithPriority(&x, cudaStreamNonBlocking, hi));
     AE_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
     for (auto &e : ev_join) AE_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    AE_CUDA(cudaStreamCreateWithFlags(&side_f, cudaStreamNonBlocking));
+    AE_CUDA(cudaStreamCreateWithPriority(&side_f, cudaStreamNonBlocking, lo));
     AE_CUDA(cudaEventCreateWithFlags(&ev_f_fork, cudaEventDisableTiming));
     AE_CUDA(cudaEventCreateWithFlags(&ev_f_join, cudaEventDisableTiming));
     for (int k = 0; k < 2; k++) {
-        AE_CUDA(cudaStreamCreateWithFlags(&side_s[k], cudaStreamNonBlocking));
+        AE_CUDA(cudaStreamCreateWithPriority(&side_s[k], cudaStreamNonBlocking, hi));
         AE_CUDA(cudaEventCreateWithFlags(&ev_s_fork[k], cudaEventDisableTiming));
         AE_CUDA(cudaEventCreateWithFlags(&ev_s_join[k], cudaEventDisableTiming));
     }
@@ -124,6 +132,7 @@ void aefdtd_sim::construct(const aefdtd_grid_desc *d) {
     if (const char *fz = std::getenv("AEFDTD_FUSED")) use_fused = atoi(fz) != 0;
     if (const char *fy = std::getenv("AEFDTD_FUSED_TY")) fused_ty = std::clamp(atoi(fy), 1, kFusedMaxTY);
     if (const char *fk = std::getenv("AEFDTD_FUSED_KCHUNK")) fused_kchunk = std::max(0, atoi(fk));
+    if (const char *dm = std::getenv("AEFDTD_DFT_MMA")) dft_mma = atoi(dm) != 0;
     if (const char *tm = std::getenv("AEFDTD_TMA")) use_tma = atoi(tm) != 0;
     if (const char *tu = std::getenv("AEFDTD_TMA_UNIT")) tma_unit = std::clamp(atoi(tu), 1, 4096);
     if (const char *tc = std::getenv("AEFDTD_TMA_CTAS")) tma_ctas = std::clamp(atoi(tc), 0, 2);
@@ -467,7 +476,8 @@ void aefdtd_sim::flush_block(PlaneSensor &s, int half, int n, const StepScalars 
     PhasorArgs pa{n, s.nl, Nt, Ntap, step0_ptr ? &step0_ptr->step : nullptr, step0_ptr ? 0 : step0, Dt,
                   s.wdev.as<double>(), s.WE.as<double2>(), s.WH.as<double2>()};
     launch_phasors(pa, st);
-    AccumArgs<T> aa{s.P, s.nl, n, s.S.as<T>() + hoff, s.WE.as<double2>(), s.WH.as<double2>(), s.acc.as<double2>()};
+    AccumArgs<T> aa{s.P, s.nl, n, s.S.as<T>() + hoff, s.WE.as<double2>(), s.WH.as<double2>(), s.acc.as<double2>(),
+                    dft_mma ? 1 : 0};
     launch_accumulate(aa, st);
     launches += 2;
 }
@@ -1079,7 +1089,7 @@ void aefdtd_sim::run_steps(int n) {
                 enqueue(false);
                 cudaGraph_t gr = nullptr;
                 AE_CUDA(cudaStreamEndCapture(stream, &gr));
-                AE_CUDA(cudaGraphInstantiate(&gx, gr, 0));
+                AE_CUDA(cudaGraphInstantiate(&gx, gr, cudaGraphInstantiateFlagUseNodePriority));
                 cudaGraphDestroy(gr);
                 graph_launches = launches - l0;
                 launches = l0;
@@ -1258,10 +1268,12 @@ void aefdtd_sim::build_work() {
     // AEFDTD_ALL_BOUNDARY=1 routes every item through the general kernels (same results)
     const bool all_boundary = std::getenv("AEFDTD_ALL_BOUNDARY") != nullptr;
     // group of a (tile, plane) for the E and the H half-step
+    // AEFDTD_MERGE_PZ=1: curl-only items run with the z-CPML items' kernels (one launch for both)
+    const bool merge_pz = std::getenv("AEFDTD_MERGE_PZ") != nullptr;
     auto group_e = [&](unsigned f) {
         if (all_boundary) return (int)kGroupAll;
         f = (f & ~kOSC) | ((f & kOSC) ? kMISC : 0);
-        if (f == 0) return (int)kGroupInterior;
+        if (f == 0) return merge_pz ? (int)kGroupPmlZ : (int)kGroupInterior;
         if (f == kPZ) return (int)kGroupPmlZ;
         if (f == kDISP) return (int)kGroupDisp;
         if (f == kPXY || f == (kPXY | kPZ)) return (int)kGroupPmlXY;
@@ -1270,7 +1282,7 @@ void aefdtd_sim::build_work() {
     auto group_h = [&](unsigned f) {
         if (all_boundary) return (int)kGroupAll;
         f &= (kPXY | kPZ | kMISC);
-        if (f == 0) return (int)kGroupInterior;
+        if (f == 0) return merge_pz ? (int)kGroupPmlZ : (int)kGroupInterior;
         if (f == kPZ) return (int)kGroupPmlZ;
         if (f == kPXY || f == (kPXY | kPZ)) return (int)kGroupPmlXY;
         return (int)kGroupAll;

@@ -39,8 +39,24 @@ void launch_phasors(const PhasorArgs &a, cudaStream_t s) {
     dft_phasors<<<(n + 255) / 256, 256, 0, s>>>(a);
 }
 template <typename T> static void acc_impl(const AccumArgs<T> &a, cudaStream_t s) {
-    dim3 g((a.P + 63) / 64, (a.nl + 63) / 64, 6);
-    dft_accumulate<<<g, 256, 0, s>>>(a);
+    const dim3 g((a.P + 63) / 64, (a.nl + 63) / 64, 6);
+    if (a.mma) {
+        constexpr int smem = dft_mma_smem<T>();
+        static bool attr = false;   // one instantiation per T
+        if (!attr) {
+            cudaFuncSetAttribute(dft_accumulate_mma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            attr = true;
+        }
+        dft_accumulate_mma<<<g, 256, smem, s>>>(a);
+        return;
+    }
+    constexpr int smem = dft_acc_smem<T>();
+    static bool attr = false;   // one instantiation per T
+    if (!attr) {
+        cudaFuncSetAttribute(dft_accumulate<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        attr = true;
+    }
+    dft_accumulate<<<g, 256, smem, s>>>(a);
 }
 void launch_accumulate(const AccumArgs<double> &a, cudaStream_t s) { acc_impl(a, s); }
 void launch_accumulate(const AccumArgs<float> &a, cudaStream_t s) { acc_impl(a, s); }

@@ -363,46 +363,97 @@ __global__ void dft_phasors(PhasorArgs a) {
 
 
 
+// cp.async of BYTES (4, 8 or 16) from global to shared memory; an invalid
+// source writes zeros (source size 0; the address is not read).
+template <int BYTES> __device__ __forceinline__ void cp_async_zfill(void *smem, const void *gmem, bool valid) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+    const uint32_t n = valid ? BYTES : 0;
+    if constexpr (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(gmem), "r"(n) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(d), "l"(gmem), "n"(BYTES), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_group() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait_group() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // One DFT block of one component: acc[c][l][p] += sum_k S[k][c][p] W_c[k][l],
 // as a tiled FP64 product. A CTA of 256 threads takes 64 points x 64
-// wavelengths and walks the K steps in slices of kDftKSlice: each slice of
-// samples (as FP64) and phasors is staged in shared memory, and each thread
-// keeps a 4-point x 4-wavelength block of complex partial sums in registers
-// (32 FMA per 6 shared-memory loads). Partial sums start from zero and add the
-// steps in order with FMA, then are added to the accumulators once, so a
-// one-step block is the reference's acc + round(coeff * t) exactly.
-// grid: (ceil(P / 64), ceil(nl / 64), 6)
-constexpr int kDftKSlice = 32;
+// wavelengths; each thread keeps a 4-point x 4-wavelength block of complex
+// partial sums in registers (32 FMA per 8 shared-memory loads of one
+// wavefront each). The K steps
+// arrive in slices of kDftKSlice samples and phasors, double-buffered with
+// cp.async so that the next slice loads while this one is multiplied; the
+// CTA's 64 x 64 accumulator tile is copied into shared memory at the start
+// (its latency hidden behind the products), the partial sums are added there
+// and the tile is written back with coalesced stores. Partial sums start
+// from zero and add the steps in order with FMA, then are added to the
+// accumulators once, so a one-step block is the reference's
+// acc + round(coeff * t) exactly.
+// grid: (ceil(P / 64), ceil(nl / 64), 6); dynamic shared memory dft_acc_smem<T>()
+constexpr int kDftKSlice = 16;
+template <typename T> constexpr int dft_acc_smem() {
+    return 64 * 64 * 16 + 2 * kDftKSlice * 64 * (int)sizeof(T) + 2 * kDftKSlice * 64 * 16;
+}
 template <typename T>
 __global__ void __launch_bounds__(256, 2) dft_accumulate(AccumArgs<T> a) {
-    __shared__ __align__(16) double sS[kDftKSlice][64];
-    __shared__ __align__(16) double2 sW[kDftKSlice][64];
+    extern __shared__ __align__(16) unsigned char dft_sm[];
+    double2 *sAcc = reinterpret_cast<double2 *>(dft_sm);                                       // [64 l][64 p]
+    double2 *sW = reinterpret_cast<double2 *>(dft_sm + 64 * 64 * 16);                          // [2][K][64 l]
+    T *sS = reinterpret_cast<T *>(dft_sm + 64 * 64 * 16 + 2 * kDftKSlice * 64 * 16);           // [2][K][64 p]
     const int tid = threadIdx.x;
     const int p0 = blockIdx.x * 64, l0 = blockIdx.y * 64, c = blockIdx.z;
     const double2 *W = (c < 3) ? a.WE : a.WH;
-    const int tp = tid & 15, tl = tid >> 4;   // points p0 + 4 tp .. +3, wavelengths l0 + 4 tl .. +3
+    // points p0 + tp + 16 i (a half-warp's sample loads are one contiguous
+    // 128-byte line), wavelengths l0 + 4 tl + f (two per warp: broadcast)
+    const int tp = tid & 15, tl = tid >> 4;
+    const int ns = (a.nk + kDftKSlice - 1) / kDftKSlice;
+    auto stage = [&](int sl) {
+        if (sl < ns) {
+            const int kt = sl * kDftKSlice, b = sl & 1;
+            for (int t = tid; t < kDftKSlice * 64; t += 256) {
+                const int kk = t >> 6, x = t & 63;
+                const bool kin = kt + kk < a.nk;
+                const bool sv = kin && p0 + x < a.P, wv = kin && l0 + x < a.nl;
+                cp_async_zfill<(int)sizeof(T)>(&sS[(b * kDftKSlice + kk) * 64 + x],
+                                               sv ? a.S + ((long long)(kt + kk) * 6 + c) * a.P + p0 + x : a.S, sv);
+                cp_async_zfill<16>(&sW[(b * kDftKSlice + kk) * 64 + x],
+                                   wv ? W + (long long)(kt + kk) * a.nl + l0 + x : W, wv);
+            }
+        }
+        cp_async_commit_group();   // empty groups keep the count uniform
+    };
+    stage(0);
+    stage(1);
+    // the accumulator tile, behind the first two slices
+    for (int t = tid; t < 64 * 64; t += 256) {
+        const int l = t >> 6, x = t & 63;
+        const bool in = l0 + l < a.nl && p0 + x < a.P;
+        cp_async_zfill<16>(&sAcc[t], in ? a.acc + ((long long)c * a.nl + l0 + l) * a.P + p0 + x : a.acc, in);
+    }
+    cp_async_commit_group();
     double re[4][4], im[4][4];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int f = 0; f < 4; ++f) { re[i][f] = 0; im[i][f] = 0; }
-    for (int kt = 0; kt < a.nk; kt += kDftKSlice) {
-        const int kn = min(kDftKSlice, a.nk - kt);
+    for (int sl = 0; sl < ns; ++sl) {
+        // groups so far: slices 0, 1, the tile, then slices 2 .. sl + 1
+        if (sl < 2) cp_async_wait_group<2>();
+        else cp_async_wait_group<1>();
         __syncthreads();
-        for (int t = tid; t < kDftKSlice * 64; t += 256) {
-            const int kk = t >> 6, x = t & 63;
-            const bool kin = kk < kn;
-            sS[kk][x] = (kin && p0 + x < a.P) ? (double)a.S[((long long)(kt + kk) * 6 + c) * a.P + p0 + x] : 0.0;
-            sW[kk][x] = (kin && l0 + x < a.nl) ? W[(long long)(kt + kk) * a.nl + l0 + x] : make_double2(0, 0);
-        }
-        __syncthreads();
-        for (int kk = 0; kk < kn; ++kk) {
-            const double2 s01 = *reinterpret_cast<const double2 *>(&sS[kk][4 * tp]);
-            const double2 s23 = *reinterpret_cast<const double2 *>(&sS[kk][4 * tp + 2]);
-            const double sv[4] = {s01.x, s01.y, s23.x, s23.y};
+        const int kn = min(kDftKSlice, a.nk - sl * kDftKSlice), b = sl & 1;
+        const T *S = sS + b * kDftKSlice * 64;
+        const double2 *Wb = sW + b * kDftKSlice * 64;
+        // threads whose wavelengths are all past nl (the last tile) leave the FP64 pipe to others
+        for (int kk = 0; kk < (l0 + 4 * tl < a.nl ? kn : 0); ++kk) {
+            double sv[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) sv[i] = (double)S[kk * 64 + tp + 16 * i];
             double2 wv[4];
 #pragma unroll
-            for (int f = 0; f < 4; ++f) wv[f] = sW[kk][4 * tl + f];
+            for (int f = 0; f < 4; ++f) wv[f] = Wb[kk * 64 + 4 * tl + f];
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -411,22 +462,135 @@ __global__ void __launch_bounds__(256, 2) dft_accumulate(AccumArgs<T> a) {
                     im[i][f] = fma(sv[i], wv[f].y, im[i][f]);
                 }
         }
+        __syncthreads();   // the buffer is free for slice sl + 2
+        stage(sl + 2);
     }
+    cp_async_wait_group<0>();
+    __syncthreads();
 #pragma unroll
-    for (int f = 0; f < 4; ++f) {
-        const int l = l0 + 4 * tl + f;
-        if (l >= a.nl) continue;
-        double2 *q = a.acc + ((long long)c * a.nl + l) * a.P;
+    for (int f = 0; f < 4; ++f)
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            const int p = p0 + 4 * tp + i;
-            if (p < a.P) {
-                double2 v = q[p];
-                v.x = v.x + re[i][f];
-                v.y = v.y + im[i][f];
-                q[p] = v;
+            double2 &v = sAcc[(4 * tl + f) * 64 + tp + 16 * i];
+            v.x = v.x + re[i][f];
+            v.y = v.y + im[i][f];
+        }
+    __syncthreads();
+    for (int t = tid; t < 64 * 64; t += 256) {
+        const int l = t >> 6, x = t & 63;
+        if (l0 + l < a.nl && p0 + x < a.P) a.acc[((long long)c * a.nl + l0 + l) * a.P + p0 + x] = sAcc[t];
+    }
+}
+
+// The same DFT block on the FP64 tensor path (mma.sync m8n8k4 f64; the
+// tcgen05 MMA has no FP64 kind): per component the real product
+// D[P x 2 nl] += S[P x K] W[K x 2 nl], columns (Re, Im) of each wavelength.
+// A CTA of 8 warps takes 64 points x 64 wavelengths (128 columns); each warp
+// 32 points x 32 columns as 4 x 4 tiles of 8 x 8, i.e. 16 accumulators of two
+// doubles per thread. Samples and phasors arrive in slices of
+// kDftMmaSlice steps, three buffers deep with cp.async (one barrier per
+// slice, two slices in flight); the accumulator tile is copied to shared
+// memory at the start, and the block's sums are added there and written
+// back with coalesced stores, as in dft_accumulate. Rows of the staged
+// slices are padded so that a fragment load (4 steps x 8 consecutive
+// points or columns) takes two wavefronts without bank conflicts. Warps
+// whose columns are all past nl skip their products. Products and sums are
+// FP64; within a group of four steps the order of the sums is the MMA's, so
+// spectra agree with dft_accumulate to rounding (a one-step block is still
+// round(s * w) added once).
+// grid: (ceil(P / 64), ceil(nl / 64), 6); dynamic shared memory dft_mma_smem<T>()
+constexpr int kDftMmaSlice = 8;
+constexpr int kDftMmaBufs = 3;
+constexpr int kDftSRow = 72;    // doubles per staged sample row (64 points + pad)
+constexpr int kDftWRow = 136;   // doubles per staged phasor row (128 columns + pad)
+template <typename T> constexpr int dft_mma_smem() {
+    return 64 * 64 * 16 + kDftMmaBufs * kDftMmaSlice * kDftWRow * 8 +
+           kDftMmaBufs * kDftMmaSlice * kDftSRow * (int)sizeof(T);
+}
+__device__ __forceinline__ void mma_f64_m8n8k4(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+template <typename T>
+__global__ void __launch_bounds__(256, 2) dft_accumulate_mma(AccumArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char dft_sm[];
+    double2 *sAcc = reinterpret_cast<double2 *>(dft_sm);                                   // [64 l][64 p]
+    double *sW = reinterpret_cast<double *>(dft_sm + 64 * 64 * 16);                        // [bufs][K][kDftWRow]
+    T *sS = reinterpret_cast<T *>(dft_sm + 64 * 64 * 16 + kDftMmaBufs * kDftMmaSlice * kDftWRow * 8);  // [bufs][K][kDftSRow]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int p0 = blockIdx.x * 64, l0 = blockIdx.y * 64, c = blockIdx.z;
+    const double2 *W = (c < 3) ? a.WE : a.WH;
+    const int ns = (a.nk + kDftMmaSlice - 1) / kDftMmaSlice;
+    auto stage = [&](int sl) {
+        if (sl < ns) {
+            const int kt = sl * kDftMmaSlice, b = sl % kDftMmaBufs;
+            for (int t = tid; t < kDftMmaSlice * 64; t += 256) {
+                const int kk = t >> 6, x = t & 63;
+                const bool kin = kt + kk < a.nk;
+                const bool sv = kin && p0 + x < a.P, wv = kin && l0 + x < a.nl;
+                cp_async_zfill<(int)sizeof(T)>(&sS[(b * kDftMmaSlice + kk) * kDftSRow + x],
+                                               sv ? a.S + ((long long)(kt + kk) * 6 + c) * a.P + p0 + x : a.S, sv);
+                cp_async_zfill<16>(&sW[(b * kDftMmaSlice + kk) * kDftWRow + 2 * x],
+                                   wv ? W + (long long)(kt + kk) * a.nl + l0 + x : W, wv);
             }
         }
+        cp_async_commit_group();   // empty groups keep the count uniform
+    };
+    stage(0);
+    stage(1);
+    for (int t = tid; t < 64 * 64; t += 256) {
+        const int l = t >> 6, x = t & 63;
+        const bool in = l0 + l < a.nl && p0 + x < a.P;
+        cp_async_zfill<16>(&sAcc[t], in ? a.acc + ((long long)c * a.nl + l0 + l) * a.P + p0 + x : a.acc, in);
+    }
+    cp_async_commit_group();
+    const int m0 = (warp & 1) * 32, n0 = (warp >> 1) * 32;   // warp tile: points m0.., columns n0..
+    const bool live = l0 + n0 / 2 < a.nl;
+    const int fr = lane & 3, fc = lane >> 2;                 // fragment: step row / point or column
+    double d[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) { d[i][j][0] = 0; d[i][j][1] = 0; }
+    for (int sl = 0; sl < ns; ++sl) {
+        // groups so far: slices 0, 1, the tile, then slices 2 .. sl + 1
+        if (sl < 2) cp_async_wait_group<2>();
+        else cp_async_wait_group<1>();
+        __syncthreads();   // slice sl visible; every warp is past slice sl - 1
+        stage(sl + 2);     // into the buffer slice sl - 1 used
+        if (!live) continue;
+        const int b = sl % kDftMmaBufs;
+        const T *S = sS + b * kDftMmaSlice * kDftSRow;
+        const double *Wb = sW + b * kDftMmaSlice * kDftWRow;
+#pragma unroll
+        for (int k4 = 0; k4 < kDftMmaSlice; k4 += 4) {
+            double af[4], bf[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) af[i] = (double)S[(k4 + fr) * kDftSRow + m0 + 8 * i + fc];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) bf[j] = Wb[(k4 + fr) * kDftWRow + n0 + 8 * j + fc];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) mma_f64_m8n8k4(d[i][j][0], d[i][j][1], af[i], bf[j]);
+        }
+    }
+    cp_async_wait_group<0>();
+    __syncthreads();
+    // D fragment: row (point) m0 + 8 i + lane / 4, columns n0 + 8 j + 2 (lane % 4) + {0, 1}
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            double2 &v = sAcc[((n0 + 8 * j) / 2 + fr) * 64 + m0 + 8 * i + fc];
+            v.x = v.x + d[i][j][0];
+            v.y = v.y + d[i][j][1];
+        }
+    __syncthreads();
+    for (int t = tid; t < 64 * 64; t += 256) {
+        const int l = t >> 6, x = t & 63;
+        if (l0 + l < a.nl && p0 + x < a.P) a.acc[((long long)c * a.nl + l0 + l) * a.P + p0 + x] = sAcc[t];
     }
 }
 

@@ -338,6 +338,9 @@ struct aefdtd_sim {
     DBuf tables;
     bool use_graphs = true;
     bool graphs_dirty = true;
+    // FP64-sample DFT blocks on the FP64 tensor path (mma.sync f64) rather than
+    // the FMA kernel (AEFDTD_DFT_MMA=0/1; the FP32 path uses dft_tc unless AEFDTD_NO_TC)
+    bool dft_mma = true;
     // tensor-core DFT wait bound and the withheld-copy test hook (aefdtd_test_hook)
     long long tc_wait_cycles = 1LL << 32;
     int tc_withhold_copy = 0;
@@ -381,7 +384,7 @@ struct aefdtd_sim {
     bool use_tma = false;            // AEFDTD_TMA
     bool tma_allowed = true;         // cleared while the simulation is in a batch
     int tma_unit = 8;                // planes per unit (AEFDTD_TMA_UNIT)
-    int tma_ctas = 0;                // AEFDTD_TMA_CTAS: 0 one unit per CTA; 1 or 2 CTAs per SM taking
+    int tma_ctas = 2;                // AEFDTD_TMA_CTAS: 0 one unit per CTA; 1 or 2 CTAs per SM taking
                                      // units in turn (persistent)
     int tma_stages = 4;              // ring stages (AEFDTD_TMA_STAGES, 4 or 6)
     TmaPlan tma_plan[2] = {};        // E, H half-step

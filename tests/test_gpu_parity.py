@@ -286,6 +286,31 @@ def test_fp32_tensor_core_dft_matches_simt_dft(monkeypatch):
         assert np.max(np.abs(fa - fb)) <= 1e-5 * np.max(np.abs(fb))
 
 
+def test_fp64_mma_dft_matches_fma_dft(monkeypatch):
+    """FP64 path: DFT blocks on the FP64 tensor path (mma.sync f64, the
+    default) against the FMA kernel on the same samples: accumulators within
+    1e-13 of their magnitude (only the order of the sums within four steps
+    differs); 201 wavelengths (a partial last wavelength tile) and 150 steps
+    (a partial last block)."""
+    sc = scenes.slab_tm(nsteps=150)
+    for s in sc.sensors:
+        s.nl = 201
+
+    def dft(env):
+        monkeypatch.setenv("AEFDTD_DFT_MMA", env)
+        with fdtd.build_simulation(sc) as sim:
+            sim.step(150)
+            sim.synchronize()
+            return [sim.sensor_dft(i) for i in range(len(sc.sensors))], [sim.sensor_flux(i) for i in range(len(sc.sensors))]
+
+    (da, fa), (db, fb) = dft("1"), dft("0")
+    for x, y in zip(da, db):
+        assert np.count_nonzero(y) > 0
+        assert np.max(np.abs(x - y)) <= 1e-13 * np.max(np.abs(y))
+    for x, y in zip(fa, fb):
+        assert np.max(np.abs(x - y)) <= 1e-12 * np.max(np.abs(y))
+
+
 def test_fp32_tensor_core_dft_many_wavelengths():
     """Two N tiles (2 nl > 256 columns) and a partial last block."""
     sc64 = scenes.slab_tm(nsteps=150)
