@@ -218,6 +218,20 @@ __global__ void __launch_bounds__(kDftTcThreads, 1) dft_accumulate_tc(const __gr
             }
             mma_commit(&bars[1]);
         }
+        // FP64 accumulators of this warp's 16-column chunks, one chunk ahead:
+        // the first chunk's loads go out before the MMA wait, each later one
+        // while the previous chunk is added and stored
+        auto load_chunk = [&](int col, double2 (&o)[8]) {
+            const int gn0 = 256 * t + col;
+            if (p < a.P && col < Nt) {
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    if (gn0 + 2 * q < 2 * a.nl)
+                        o[q] = __ldcs(a.acc + ((size_t)c * a.nl + ((gn0 >> 1) + q)) * a.P + p);
+            }
+        };
+        double2 cur[8], nxt[8];
+        load_chunk(16 * cg, cur);
         if (ok && !bar_wait(&bars[1], t & 1, a.wait_cycles)) ok = false;
         // every thread leaves the tile loop together: a failed wait on any
         // thread stops all of them before the next tile's copies
@@ -226,24 +240,20 @@ __global__ void __launch_bounds__(kDftTcThreads, 1) dft_accumulate_tc(const __gr
         tc_fence_after();
         for (int col = 16 * cg; col < Nt; col += 64) {
             const int gn0 = 256 * t + col;
-            double2 o[8];
-            if (p < a.P) {
-#pragma unroll
-                for (int q = 0; q < 8; ++q)
-                    if (gn0 + 2 * q < 2 * a.nl)
-                        o[q] = __ldcs(a.acc + ((size_t)c * a.nl + ((gn0 >> 1) + q)) * a.P + p);
-            }
+            load_chunk(col + 64, nxt);
             float v[16];
             ld16(tmem + tlane + (uint32_t)col, v);
             if (p < a.P) {
 #pragma unroll
                 for (int q = 0; q < 8; ++q)
                     if (gn0 + 2 * q < 2 * a.nl) {
-                        o[q].x += (double)v[2 * q];
-                        o[q].y += (double)v[2 * q + 1];
-                        __stcs(a.acc + ((size_t)c * a.nl + ((gn0 >> 1) + q)) * a.P + p, o[q]);
+                        cur[q].x += (double)v[2 * q];
+                        cur[q].y += (double)v[2 * q + 1];
+                        __stcs(a.acc + ((size_t)c * a.nl + ((gn0 >> 1) + q)) * a.P + p, cur[q]);
                     }
             }
+#pragma unroll
+            for (int q = 0; q < 8; ++q) cur[q] = nxt[q];
         }
         tc_fence_before();
         __syncthreads();   // TMEM and B read; next tile may overwrite both
