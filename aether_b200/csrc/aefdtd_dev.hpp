@@ -148,8 +148,17 @@ struct WorkSplit {
     int unroll;                     // z-planes per iteration of the interior kernels (1 or 2)
     int tile_y;                     // tile height: CTAs of 32 x tile_y threads (2, 4 or 8)
     unsigned pair_mask;             // bit g: group g runs the two-cells-per-thread kernels on 64-column items
+                                    // (x/y-CPML group: its y-only items, n_py of them at the group's end)
+    int n_py = 0;                   // x/y-CPML group: trailing items without x-CPML cells, on the pair kernel
     const TmaPlan *tma = nullptr;   // set: the interior group is the staged kernel over these units
 };
+// Kernel launches of one half-step's groups (the x/y-CPML group launches
+// two kernels when it holds both kinds of item).
+inline int group_kernels(const WorkSplit &w) {
+    int c = 0;
+    for (int g = 0; g < kGroups; g++) c += w.n[g] > 0;
+    return c + (w.n_py > 0 && w.n[kGroupPmlXY] > w.n_py);
+}
 // x0 flag of a 32-column item in a group of 64-column (pair) items
 constexpr int kHalfItem = 1 << 30;
 

@@ -274,6 +274,8 @@ template <typename T, typename Tid> void aefdtd_batch::build_subset(BatchSubset 
         w.unroll = 2;
         w.tile_y = sc.tile_y;
         w.pair_mask = 0;
+        w.n_py = 0;
+        w.tma = nullptr;
         for (int g = 0; g < kGroups; g++) {
             w.off[g] = (int)(all.size() / 4);
             // H: members in reverse order (each member's H list is top plane
@@ -366,8 +368,9 @@ template <typename T, typename Tid> void aefdtd_batch::enqueue_steps(BatchSubset
     const auto *sa = u.sargs.as<SensorStepArgs<T>>();
     const int4 *it = u.items.as<int4>();
     const int2 *blk = u.blkmap.as<int2>();
-    int groups = 0;
-    for (int g = 0; g < kGroups; g++) groups += (u.wsE.n[g] > 0) + (u.wsH.n[g] > 0);
+    // a lone member launches its own lists (solo: run_groups below takes m0's)
+    int groups = u.solo ? group_kernels(u.members[0]->wsE) + group_kernels(u.members[0]->wsH)
+                        : group_kernels(u.wsE) + group_kernels(u.wsH);
     // a lone member: its own arguments as launch parameters, its own lists
     aefdtd_sim *m0 = u.members[0];
     StepArgs<T, Tid> se, sh, se_i, sh_i;

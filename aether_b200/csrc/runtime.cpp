@@ -122,8 +122,9 @@ void aefdtd_sim::construct(const aefdtd_grid_desc *d) {
     if (const char *pf = std::getenv("AEFDTD_PREFETCH")) prefetch_l2 = std::clamp(atoi(pf), 0, 3);
     if (const char *hr = std::getenv("AEFDTD_HREV")) h_reverse = atoi(hr) != 0 ? 1 : 0;
     // two cells per thread: FP32 interior and z-CPML items, FP64 z-CPML items
-    pair_mask = fp64 ? (1u << kGroupPmlZ) : (1u << kGroupInterior) | (1u << kGroupPmlZ);
-    if (const char *pm = std::getenv("AEFDTD_PAIR")) pair_mask = unsigned(atoi(pm)) & 3u;
+    // and the y-only items of the x/y-CPML group
+    pair_mask = (fp64 ? (1u << kGroupPmlZ) : (1u << kGroupInterior) | (1u << kGroupPmlZ)) | (1u << kGroupPmlXY);
+    if (const char *pm = std::getenv("AEFDTD_PAIR")) pair_mask = unsigned(atoi(pm)) & 0x13u;
     pair_mask0 = pair_mask;
     h_reverse0 = h_reverse;
     // fused time steps: on by default where they measure faster (kFusedDefault),
@@ -671,8 +672,7 @@ void aefdtd_sim::enqueue_segment(int L, StepScalars *tbl, bool record) {
     make_step_args(ea, ha, tbl);
     if (obl) make_step_args(ea_i, ha_i, tbl, 1);   // the oblique driver's imaginary grid
     const int4 *wi = items.as<int4>();
-    int groups = 0;
-    for (int g = 0; g < kGroups; g++) groups += (wsE.n[g] > 0) + (wsH.n[g] > 0);
+    int groups = group_kernels(wsE) + group_kernels(wsH);
     if (obl) groups *= 2;
     SensorStepArgs<T> sa;
     make_sensor_args(sa, tbl);
@@ -1209,7 +1209,11 @@ void aefdtd_sim::accumulate_timing(int L) {
 // even Nx only) take 64-column items where both 32-column tiles of a pair
 // fall in the group, and 32-column items flagged kHalfItem elsewhere.
 void aefdtd_sim::build_work() {
-    const unsigned pmask = (Nx % 2 == 0) ? pair_mask & ((1u << kGroupInterior) | (1u << kGroupPmlZ)) : 0u;
+    // host-only list index of the x/y-CPML group's y-only tiles (two cells per
+    // thread); appended to the x/y-CPML group's items, counted in WorkSplit::n_py
+    constexpr int kGroupPY = kGroups;
+    unsigned pmask = (Nx % 2 == 0) ? pair_mask & ((1u << kGroupInterior) | (1u << kGroupPmlZ)) : 0u;
+    if (Nx % 2 == 0 && (pair_mask & (1u << kGroupPmlXY))) pmask |= 1u << kGroupPY;
     const int tx = kTileXHost, ty = tile_y;
     const int ntx = (Nx + tx - 1) / tx, nty = (Ny + ty - 1) / ty;
     const long long tiles = (long long)ntx * nty;
@@ -1223,7 +1227,9 @@ void aefdtd_sim::build_work() {
     }
     const int nch = (Nz + kchunk - 1) / kchunk;
     // feature mask per (tile, plane) (kF* of yee.cuh); oscillator boxes matter to E only
-    constexpr unsigned kPXY = 1, kPZ = 2, kDISP = 4, kMISC = 8, kOSC = 16;
+    // kPXY: an x-CPML cell or PEC plane; kPY: a y-CPML cell or PEC plane (both
+    // take the x/y-CPML group; tiles with kPY alone may take the pair kernel)
+    constexpr unsigned kPXY = 1, kPZ = 2, kDISP = 4, kMISC = 8, kOSC = 16, kPY = 32;
     std::vector<unsigned char> feat(size_t(tiles) * Nz, 0);
     auto mark_range = [&](int x0, int x1, int y0, int y1, int z0, int z1, unsigned f) {   // half-open cell ranges
         if (x0 >= x1 || y0 >= y1 || z0 >= z1) return;
@@ -1237,8 +1243,8 @@ void aefdtd_sim::build_work() {
         mark_range(Nx - std::max(pml[1], 1), Nx, 0, Ny, 0, Nz, kPXY);
     }
     if (py) {
-        mark_range(0, Nx, 0, std::max(pml[2], 1), 0, Nz, kPXY);
-        mark_range(0, Nx, Ny - std::max(pml[3], 1), Ny, 0, Nz, kPXY);
+        mark_range(0, Nx, 0, std::max(pml[2], 1), 0, Nz, kPY);
+        mark_range(0, Nx, Ny - std::max(pml[3], 1), Ny, 0, Nz, kPY);
     }
     if (pz) {
         mark_range(0, Nx, 0, Ny, 0, std::max(pml[4], 1), kPZ);
@@ -1273,6 +1279,7 @@ void aefdtd_sim::build_work() {
     auto group_e = [&](unsigned f) {
         if (all_boundary) return (int)kGroupAll;
         f = (f & ~kOSC) | ((f & kOSC) ? kMISC : 0);
+        f = (f & ~kPY) | ((f & kPY) ? kPXY : 0);
         if (f == 0) return merge_pz ? (int)kGroupPmlZ : (int)kGroupInterior;
         if (f == kPZ) return (int)kGroupPmlZ;
         if (f == kDISP) return (int)kGroupDisp;
@@ -1281,6 +1288,7 @@ void aefdtd_sim::build_work() {
     };
     auto group_h = [&](unsigned f) {
         if (all_boundary) return (int)kGroupAll;
+        f = (f & ~kPY) | ((f & kPY) ? kPXY : 0);
         f &= (kPXY | kPZ | kMISC);
         if (f == 0) return merge_pz ? (int)kGroupPmlZ : (int)kGroupInterior;
         if (f == kPZ) return (int)kGroupPmlZ;
@@ -1363,7 +1371,7 @@ void aefdtd_sim::build_work() {
     // items: within each tile (or pair of tiles) and z-chunk, runs of planes
     // of one group; dispersive E planes one plane per item (their cells carry
     // the pole state)
-    std::vector<int> v[2][kGroups];
+    std::vector<int> v[2][kGroups + 1];
     const int step_a = pmask ? 2 : 1;
     for (int c = 0; c < nch; c++)
         for (int b = 0; b < nty; b++)
@@ -1375,6 +1383,7 @@ void aefdtd_sim::build_work() {
                         const size_t fi = (size_t(k) * nty + b) * ntx + t;
                         if (tma && taken[half][fi]) return -1;
                         const int g = half == 0 ? group_e(feat[fi]) : group_h(feat[fi]);
+                        if (g == kGroupPmlXY && ((pmask >> kGroupPY) & 1u) && !(feat[fi] & kPXY)) return kGroupPY;
                         return (tma && g == kGroupInterior) ? (int)kGroupPmlZ : g;
                     };
                     auto emit = [&](int g, int x0, int za, int zb) {
@@ -1427,7 +1436,7 @@ void aefdtd_sim::build_work() {
     // when the fields are about the size of L2 (126 MB) or smaller.
     const size_t field_bytes = size_t(6) * Nx * Ny * Nz * (fp64 ? 8 : 4);
     if (h_reverse > 0 || (h_reverse < 0 && field_bytes <= (size_t(128) << 20)))
-        for (int g = 0; g < kGroups; g++) {
+        for (int g = 0; g <= kGroups; g++) {
             std::vector<int> &h = v[1][g];
             const size_t n = h.size() / 4;
             for (size_t a = 0, b = n ? n - 1 : 0; a < b; a++, b--)
@@ -1439,17 +1448,27 @@ void aefdtd_sim::build_work() {
         w.unroll = zunroll;
         w.tile_y = tile_y;
         w.pair_mask = pmask;
-        for (int g = 0; g < kGroups; g++) {
-            w.off[g] = (int)(all.size() / 4);
-            w.n[g] = (int)(v[half][g].size() / 4);
-            all.insert(all.end(), v[half][g].begin(), v[half][g].end());
+        auto cells_of = [&](int g) {
             long long c = 0;
             for (size_t k = 0; k < v[half][g].size(); k += 4) {
                 const int *it = &v[half][g][k];
                 const int x0 = it[0] & ~kHalfItem, gw = ((pmask >> g) & 1u) && !(it[0] & kHalfItem) ? 2 * tx : tx;
                 c += (long long)(std::min(x0 + gw, Nx) - x0) * (std::min(it[1] + ty, Ny) - it[1]) * (it[3] - it[2]);
             }
-            grp_cells[half][g] = c;
+            return c;
+        };
+        for (int g = 0; g < kGroups; g++) {
+            w.off[g] = (int)(all.size() / 4);
+            w.n[g] = (int)(v[half][g].size() / 4);
+            all.insert(all.end(), v[half][g].begin(), v[half][g].end());
+            grp_cells[half][g] = cells_of(g);
+            if (g == kGroupPmlXY) {
+                // the y-only pair items follow the group's one-cell items
+                w.n_py = (int)(v[half][kGroupPY].size() / 4);
+                w.n[g] += w.n_py;
+                all.insert(all.end(), v[half][kGroupPY].begin(), v[half][kGroupPY].end());
+                grp_cells[half][g] += cells_of(kGroupPY);
+            }
         }
     }
     // staged units: E then H

@@ -764,7 +764,11 @@ template <typename V, typename P> __device__ __forceinline__ V ldg2(const P *p) 
 template <typename V, typename P> __device__ __forceinline__ V ld2(const P *p) { return *reinterpret_cast<const V *>(p); }
 template <typename V, typename P> __device__ __forceinline__ void st2(P *p, V v) { *reinterpret_cast<V *>(p) = v; }
 
-template <typename T, typename Tid, bool PZ>
+// PY: the item's cells may also lie in a y-CPML range or on the j = 0 PEC
+// plane, but in no x-CPML range: the y psi recursions and PEC of app_pml_Ex
+// and app_pml_Ez (fdtd_pml.cpp:504-735) are applied in the general kernel's
+// order (Ex: y block, then z block; Ez: y block).
+template <typename T, typename Tid, bool PZ, bool PY = false>
 __device__ __forceinline__ void e_interior_v2_body(const StepArgs<T, Tid> &a, int q, int4 it) {
     using T2 = typename Vec2<T>::type;
     using I2 = typename IdPair<Tid>::type;
@@ -796,6 +800,16 @@ __device__ __forceinline__ void e_interior_v2_body(const StepArgs<T, Tid> &a, in
     const int kmi = (it.z == 0) ? a.Nz - 1 : it.z - 1;
     T2 hx_km = ldg2<T2>(Hx + col + kmi * NxNy);
     T2 hy_km = ldg2<T2>(Hy + col + kmi * NxNy);
+    // E-side y range [1, pml_ym) and [Ny - pml_yp + 1, Ny) (fdtd_pml.cpp:518,527); one row per warp
+    bool ye = false;
+    int yn = 0;
+    T byj = 0, cyj = 0;
+    const int nys = a.pml_ym + a.pml_yp;
+    if constexpr (PY) {
+        ye = a.py && ((j >= 1 && j < a.pml_ym) || (j >= a.Ny - a.pml_yp + 1));
+        yn = (j < a.pml_ym) ? j : j - (a.Ny - a.pml_yp) + a.pml_ym;
+        if (ye) { byj = __ldg(a.by + j); cyj = __ldg(a.cy + j); }
+    }
     if (a.prefetch & 1) {
         for (int k = it.z; k < it.w; ++k) {
             const long long o = (long long)k * NxNy;
@@ -811,10 +825,26 @@ __device__ __forceinline__ void e_interior_v2_body(const StepArgs<T, Tid> &a, in
                     prefetch_l2(a.psi_z1 + col + (long long)zn * NxNy);
                 }
             }
+            if constexpr (PY) {
+                if (ye) {
+                    const long long oy = ic + (long long)yn * a.Nx + (long long)k * a.Nx * nys;
+                    prefetch_l2(a.psi_y0 + oy);
+                    prefetch_l2(a.psi_y1 + oy);
+                }
+            }
         }
     }
     for (int k = it.z; k < it.w; ++k) {
         const long long o = (long long)k * NxNy;
+        T2 qy0, qy1;
+        long long oy = 0;
+        if constexpr (PY) {
+            if (ye) {
+                oy = ic + (long long)yn * a.Nx + (long long)k * a.Nx * nys;
+                qy0 = ld2<T2>(a.psi_y0 + oy);
+                qy1 = ld2<T2>(a.psi_y1 + oy);
+            }
+        }
         const T2 hx = ldg2<T2>(Hx + col + o), hy = ldg2<T2>(Hy + col + o), hz = ldg2<T2>(Hz + col + o);
         const T2 hz_jm = ldg2<T2>(Hz + coly + o), hx_jm = ldg2<T2>(Hx + coly + o);
         T hz_edge = 0, hy_edge = 0;
@@ -851,6 +881,26 @@ __device__ __forceinline__ void e_interior_v2_body(const StepArgs<T, Tid> &a, in
         ne.y = (C1b * ex.y + (C2yb * iky) * (hz.y - hz_jm.y)) - (C2zb * ikz) * (hy.y - hy_km.y);
         nf.y = (C1b * ey.y + (C2zb * ikz) * (hx.y - hx_km.y)) - (C2xb * ikx.y) * (hz.y - hz.x);
         ng.y = (C1b * ez.y + (C2xb * ikx.y) * (hy.y - hy.x)) - (C2yb * iky) * (hx.y - hx_jm.y);
+        if constexpr (PY) {
+            // Ex: y block (before the z block); Ez: y block (no x block here)
+            if (ye) {
+                const T C4a = __ldg(&ca->C4), C4b = __ldg(&cb->C4);
+                T2 ps0, ps1;
+                ps0.x = cpml_rec(byj, qy0.x, cyj, hz.x - hz_jm.x);   // Ex: PsiExy
+                ps0.y = cpml_rec(byj, qy0.y, cyj, hz.y - hz_jm.y);
+                ne.x += C4a * ps0.x;
+                ne.y += C4b * ps0.y;
+                ps1.x = cpml_rec(byj, qy1.x, cyj, hx.x - hx_jm.x);   // Ez: PsiEzy
+                ps1.y = cpml_rec(byj, qy1.y, cyj, hx.y - hx_jm.y);
+                ng.x -= C4a * ps1.x;
+                ng.y -= C4b * ps1.y;
+                if (act) {
+                    st2<T2>(a.psi_y0 + oy, ps0);
+                    st2<T2>(a.psi_y1 + oy, ps1);
+                }
+            }
+            if (a.py && j == 0) { ne.x = 0; ne.y = 0; ng.x = 0; ng.y = 0; }
+        }
         if constexpr (PZ) {
             if (ze) {
                 const T C4a = __ldg(&ca->C4), C4b = __ldg(&cb->C4);
@@ -880,7 +930,9 @@ __device__ __forceinline__ void e_interior_v2_body(const StepArgs<T, Tid> &a, in
     }
 }
 
-template <typename T, typename Tid, bool PZ>
+// PY: as for E, with the H-side y range, psi recursions and j = Ny - 1 PEC of
+// app_pml_Hx and app_pml_Hz (fdtd_pml.cpp:737-1164).
+template <typename T, typename Tid, bool PZ, bool PY = false>
 __device__ __forceinline__ void h_interior_v2_body(const StepArgs<T, Tid> &a, int q, int4 it) {
     using T2 = typename Vec2<T>::type;
     const int lane = threadIdx.x;
@@ -911,6 +963,16 @@ __device__ __forceinline__ void h_interior_v2_body(const StepArgs<T, Tid> &a, in
     const T ay = a.dtdmy * __ldg(a.iky + j);
     T2 ex = ldg2<T2>(Ex + col + it.z * NxNy);
     T2 ey = ldg2<T2>(Ey + col + it.z * NxNy);
+    // H-side y range [0, pml_ym) and [Ny - pml_yp, Ny - 1) (fdtd_pml.cpp:783,792); one row per warp
+    bool yh = false;
+    int yn = 0;
+    T byj = 0, cyj = 0;
+    const int nys = a.pml_ym + a.pml_yp;
+    if constexpr (PY) {
+        yh = a.py && ((j < a.pml_ym) || (j >= a.Ny - a.pml_yp && j < a.Ny - 1));
+        yn = (j < a.pml_ym) ? j : j - (a.Ny - a.pml_yp) + a.pml_ym;
+        if (yh) { byj = __ldg(a.by + j); cyj = __ldg(a.cy + j); }
+    }
     if (a.prefetch & 1) {
         for (int k = it.z; k < it.w; ++k) {
             const int kp = (k == a.Nz - 1) ? 0 : k + 1;
@@ -926,11 +988,27 @@ __device__ __forceinline__ void h_interior_v2_body(const StepArgs<T, Tid> &a, in
                     prefetch_l2(a.psi_z1 + col + (long long)zn * NxNy);
                 }
             }
+            if constexpr (PY) {
+                if (yh) {
+                    const long long oy = ic + (long long)yn * a.Nx + (long long)k * a.Nx * nys;
+                    prefetch_l2(a.psi_y0 + oy);
+                    prefetch_l2(a.psi_y1 + oy);
+                }
+            }
         }
     }
     for (int k = it.z; k < it.w; ++k) {
         const int kp = (k == a.Nz - 1) ? 0 : k + 1;
         const long long o = (long long)k * NxNy, op = (long long)kp * NxNy;
+        T2 qy0, qy1;
+        long long oy = 0;
+        if constexpr (PY) {
+            if (yh) {
+                oy = ic + (long long)yn * a.Nx + (long long)k * a.Nx * nys;
+                qy0 = ld2<T2>(a.psi_y0 + oy);
+                qy1 = ld2<T2>(a.psi_y1 + oy);
+            }
+        }
         const T2 ex_kp = ldg2<T2>(Ex + col + op), ey_kp = ldg2<T2>(Ey + col + op);
         const T2 ez = ldg2<T2>(Ez + col + o);
         const T2 ez_jp = ldg2<T2>(Ez + coly + o), ex_jp = ldg2<T2>(Ex + coly + o);
@@ -963,6 +1041,25 @@ __device__ __forceinline__ void h_interior_v2_body(const StepArgs<T, Tid> &a, in
         nh.y = hx.y + (az * (ey_kp.y - ey.y) - ay * (ez_jp.y - ez.y));
         ni.y = hy.y + (ax.y * (ez_ip1 - ez.y) - az * (ex_kp.y - ex.y));
         nk.y = hz.y + (ay * (ex_jp.y - ex.y) - ax.y * (ey_ip1 - ey.y));
+        if constexpr (PY) {
+            // Hx: y block (before the z block); Hz: y block (no x block here)
+            if (yh) {
+                T2 ps0, ps1;
+                ps0.x = cpml_rec(byj, qy0.x, cyj, ez_jp.x - ez.x);   // Hx: PsiHxy
+                ps0.y = cpml_rec(byj, qy0.y, cyj, ez_jp.y - ez.y);
+                nh.x -= a.dtm * ps0.x;
+                nh.y -= a.dtm * ps0.y;
+                ps1.x = cpml_rec(byj, qy1.x, cyj, ex_jp.x - ex.x);   // Hz: PsiHzy
+                ps1.y = cpml_rec(byj, qy1.y, cyj, ex_jp.y - ex.y);
+                nk.x += a.dtm * ps1.x;
+                nk.y += a.dtm * ps1.y;
+                if (act) {
+                    st2<T2>(a.psi_y0 + oy, ps0);
+                    st2<T2>(a.psi_y1 + oy, ps1);
+                }
+            }
+            if (a.py && j == a.Ny - 1) { nh.x = 0; nh.y = 0; nk.x = 0; nk.y = 0; }
+        }
         if constexpr (PZ) {
             if (zh) {
                 T2 ps0, ps1;
@@ -1035,6 +1132,18 @@ h_interior_v2(const __grid_constant__ StepArgs<T, Tid> a, const int4 *__restrict
     h_interior_v2_body<T, Tid, PZ>(a, a.q, items[blockIdx.x]);
 }
 
+// y-CPML items without x-CPML cells: two cells per thread, y and z psi
+template <typename T, typename Tid>
+__global__ void __launch_bounds__(kMaxTileThreads, InteriorBounds<T, 2, true>::kMinBlocksVec2)
+e_pmly_v2(const __grid_constant__ StepArgs<T, Tid> a, const int4 *__restrict__ items) {
+    e_interior_v2_body<T, Tid, true, true>(a, a.q, items[blockIdx.x]);
+}
+template <typename T, typename Tid>
+__global__ void __launch_bounds__(kMaxTileThreads, InteriorBounds<T, 2, true>::kMinBlocksVec2)
+h_pmly_v2(const __grid_constant__ StepArgs<T, Tid> a, const int4 *__restrict__ items) {
+    h_interior_v2_body<T, Tid, true, true>(a, a.q, items[blockIdx.x]);
+}
+
 // Batched forms: item (x0, y0, k0 | k1 << 16, instance), arguments of the
 // instance from a device array, q the step's index in every member's table.
 __device__ __forceinline__ int4 batch_item(int4 b) { return make_int4(b.x, b.y, b.z & 0xffff, b.z >> 16); }
@@ -1090,7 +1199,11 @@ void launch_e_group_impl(const StepArgs<T, Tid> &a, const int4 *items, const Wor
             else e_interior<T, Tid, 1, true><<<n, blk, 0, s>>>(a, p);
             break;
         case kGroupDisp: e_boundary<T, Tid, kFDisp><<<n, blk, 0, s>>>(a, p); break;
-        case kGroupPmlXY: e_boundary<T, Tid, kFPmlXY | kFPmlZ><<<n, blk, 0, s>>>(a, p); break;
+        case kGroupPmlXY:
+            // items with x-CPML cells first (one cell per thread), then the y-only pairs
+            if (n > w.n_py) e_boundary<T, Tid, kFPmlXY | kFPmlZ><<<n - w.n_py, blk, 0, s>>>(a, p);
+            if (w.n_py > 0) e_pmly_v2<T, Tid><<<w.n_py, blk, 0, s>>>(a, p + (n - w.n_py));
+            break;
         default: e_boundary<T, Tid, kFAll><<<n, blk, 0, s>>>(a, p); break;
     }
 }
@@ -1113,7 +1226,10 @@ void launch_h_group_impl(const StepArgs<T, Tid> &a, const int4 *items, const Wor
             else if (w.unroll >= 2) h_interior<T, Tid, 2, true><<<n, blk, 0, s>>>(a, p);
             else h_interior<T, Tid, 1, true><<<n, blk, 0, s>>>(a, p);
             break;
-        case kGroupPmlXY: h_boundary<T, Tid, kFPmlXY | kFPmlZ><<<n, blk, 0, s>>>(a, p); break;
+        case kGroupPmlXY:
+            if (n > w.n_py) h_boundary<T, Tid, kFPmlXY | kFPmlZ><<<n - w.n_py, blk, 0, s>>>(a, p);
+            if (w.n_py > 0) h_pmly_v2<T, Tid><<<w.n_py, blk, 0, s>>>(a, p + (n - w.n_py));
+            break;
         default: h_boundary<T, Tid, kFAll><<<n, blk, 0, s>>>(a, p); break;
     }
 }
