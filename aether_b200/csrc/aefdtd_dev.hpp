@@ -141,6 +141,8 @@ struct TmaPlan {
     int grid;           // CTAs per launch
     int stages;         // ring stages (4 or 6)
     long long cells;    // cells per launch
+    long long wait_cycles;   // bound of each mbarrier wait
+    int withhold;            // test hook: the producer issues no copy and arrives on no stage
 };
 struct WorkSplit {
     int off[kGroups];

@@ -33,7 +33,6 @@ namespace aefdtd {
 
 constexpr int kTmaConsumers = kTmaTileY;                // one warp per tile row
 constexpr int kTmaThreads = 32 * (kTmaConsumers + 1);   // plus the producer warp
-constexpr long long kTmaWaitCycles = 1LL << 32;         // about 2 s at 1.9 GHz
 constexpr int kTmaHalo = 1, kTmaWrapX = 2, kTmaStop = 4; // stage header flags
 
 // Byte layout of one ring stage.
@@ -53,10 +52,12 @@ template <typename T, typename Tid> struct TmaStage {
 };
 
 // Producer: one thread. HS: the H half-step.
+// limit: bound of each wait (SM cycles); withhold (test hook): no copy and
+// no arrive on any data stage, so the consumers' waits run out.
 template <typename T, typename Tid, int S, bool HS>
 __device__ __forceinline__ void tma_produce(const StepArgs<T, Tid> &a, const TmaMaps &m, const int4 *units,
                                             int nunits, int *ctr, unsigned char *sm, uint64_t *full,
-                                            uint64_t *empty, volatile int *abort) {
+                                            uint64_t *empty, volatile int *abort, long long limit, int withhold) {
     using L = TmaStage<T, Tid>;
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
@@ -73,7 +74,7 @@ __device__ __forceinline__ void tma_produce(const StepArgs<T, Tid> &a, const Tma
     const bool one = (int)gridDim.x == nunits;
     int u = one ? (int)blockIdx.x : atomicAdd(ctr, 1);
     for (;;) {
-        if (!mbar::wait_or_abort(&empty[st], ph ^ 1, kTmaWaitCycles, abort)) { ok = false; break; }
+        if (!mbar::wait_or_abort(&empty[st], ph ^ 1, limit, abort)) { ok = false; break; }
         int4 *hdr = reinterpret_cast<int4 *>(sm + st * L::kBytes + L::oHdr);
         if (u >= nunits) {   // no unit left: a stop stage without copies
             *hdr = make_int4(0, 0, 0, kTmaStop);
@@ -90,10 +91,13 @@ __device__ __forceinline__ void tma_produce(const StepArgs<T, Tid> &a, const Tma
                           : (y0 == 0 ? a.Ny - 1 : y0 - 1);
         const int flags = wrapx ? kTmaWrapX : 0;
         for (int p = -1; p < k1 - k0; ++p) {
-            if (p >= 0 && !mbar::wait_or_abort(&empty[st], ph ^ 1, kTmaWaitCycles, abort)) { ok = false; break; }
+            if (p >= 0 && !mbar::wait_or_abort(&empty[st], ph ^ 1, limit, abort)) { ok = false; break; }
             unsigned char *b = sm + st * L::kBytes;
             uint64_t *f = &full[st];
-            if (p < 0) {
+            if (withhold) {
+                // test hook: the stage's header only
+                *reinterpret_cast<int4 *>(b + L::oHdr) = make_int4(x0, y0, 0, flags | (p < 0 ? kTmaHalo : 0));
+            } else if (p < 0) {
                 // the z-neighbour plane: own columns of Hx and Hy (E) or Ex and Ey (H)
                 const int k = HS ? (k1 == a.Nz ? 0 : k1) : (k0 == 0 ? a.Nz - 1 : k0 - 1);
                 *reinterpret_cast<int4 *>(b + L::oHdr) = make_int4(x0, y0, k, flags | kTmaHalo);
@@ -129,7 +133,7 @@ __device__ __forceinline__ void tma_produce(const StepArgs<T, Tid> &a, const Tma
         atomicExch(a.err, 1);
         for (int d = 1; d <= min(issued, S); ++d) {
             const int s = (st - d + S) % S;
-            mbar::wait(&full[s], s < st ? ph : ph ^ 1, kTmaWaitCycles);
+            if (!withhold) mbar::wait(&full[s], s < st ? ph : ph ^ 1, limit);
         }
     }
     // the last CTA to finish resets the counters for the next launch
@@ -144,7 +148,7 @@ __device__ __forceinline__ void tma_produce(const StepArgs<T, Tid> &a, const Tma
 
 template <typename T, typename Tid, int S>
 __device__ __forceinline__ void e_tma_consume(const StepArgs<T, Tid> &a, unsigned char *sm, uint64_t *full,
-                                              uint64_t *empty, volatile int *abort) {
+                                              uint64_t *empty, volatile int *abort, long long limit) {
     using L = TmaStage<T, Tid>;
     using V = typename Vec2<T>::type;
     using P = typename IdPair<Tid>::type;
@@ -154,7 +158,7 @@ __device__ __forceinline__ void e_tma_consume(const StepArgs<T, Tid> &a, unsigne
     uint32_t ph = 0;
     T hxm0 = 0, hxm1 = 0, hym0 = 0, hym1 = 0, ikx0 = 0, ikx1 = 0, iky = 0;
     for (;;) {
-        if (!mbar::wait_or_abort(&full[st], ph, kTmaWaitCycles, abort)) {
+        if (!mbar::wait_or_abort(&full[st], ph, limit, abort)) {
             *abort = 1;
             atomicExch(a.err, 1);
             return;
@@ -221,7 +225,7 @@ __device__ __forceinline__ void e_tma_consume(const StepArgs<T, Tid> &a, unsigne
 
 template <typename T, typename Tid, int S>
 __device__ __forceinline__ void h_tma_consume(const StepArgs<T, Tid> &a, unsigned char *sm, uint64_t *full,
-                                              uint64_t *empty, volatile int *abort) {
+                                              uint64_t *empty, volatile int *abort, long long limit) {
     using L = TmaStage<T, Tid>;
     using V = typename Vec2<T>::type;
     constexpr int X = kTmaTileX, B1 = kTmaTileX * kTmaTileY;
@@ -230,7 +234,7 @@ __device__ __forceinline__ void h_tma_consume(const StepArgs<T, Tid> &a, unsigne
     uint32_t ph = 0;
     T exp0 = 0, exp1 = 0, eyp0 = 0, eyp1 = 0, ax0 = 0, ax1 = 0, ay = 0;
     for (;;) {
-        if (!mbar::wait_or_abort(&full[st], ph, kTmaWaitCycles, abort)) {
+        if (!mbar::wait_or_abort(&full[st], ph, limit, abort)) {
             *abort = 1;
             atomicExch(a.err, 1);
             return;
@@ -299,7 +303,7 @@ __device__ __forceinline__ void h_tma_consume(const StepArgs<T, Tid> &a, unsigne
 template <typename T, typename Tid, bool HS, int S>
 __global__ void __launch_bounds__(kTmaThreads, 2)
 interior_tma(const __grid_constant__ StepArgs<T, Tid> a, const __grid_constant__ TmaMaps m,
-             const int4 *__restrict__ units, int nunits, int *ctr) {
+             const int4 *__restrict__ units, int nunits, int *ctr, long long limit, int withhold) {
     __shared__ __align__(8) uint64_t full[S], empty[S];
     __shared__ int abort_flag;
     extern __shared__ __align__(128) unsigned char tma_dsm[];
@@ -315,11 +319,11 @@ interior_tma(const __grid_constant__ StepArgs<T, Tid> a, const __grid_constant__
     __syncthreads();
     if (threadIdx.x >= 32 * kTmaConsumers) {
         if (threadIdx.x == 32 * kTmaConsumers)
-            tma_produce<T, Tid, S, HS>(a, m, units, nunits, ctr, sm, full, empty, &abort_flag);
+            tma_produce<T, Tid, S, HS>(a, m, units, nunits, ctr, sm, full, empty, &abort_flag, limit, withhold);
         return;
     }
-    if constexpr (HS) h_tma_consume<T, Tid, S>(a, sm, full, empty, &abort_flag);
-    else e_tma_consume<T, Tid, S>(a, sm, full, empty, &abort_flag);
+    if constexpr (HS) h_tma_consume<T, Tid, S>(a, sm, full, empty, &abort_flag, limit);
+    else e_tma_consume<T, Tid, S>(a, sm, full, empty, &abort_flag, limit);
 }
 
 template <typename T, typename Tid, bool HS, int S> void launch_tma_one(const StepArgs<T, Tid> &a, const TmaPlan &p, cudaStream_t s) {
@@ -329,7 +333,8 @@ template <typename T, typename Tid, bool HS, int S> void launch_tma_one(const St
         cudaFuncSetAttribute(interior_tma<T, Tid, HS, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         attr = true;
     }
-    interior_tma<T, Tid, HS, S><<<p.grid, kTmaThreads, smem, s>>>(a, p.maps, p.units, p.nunits, p.ctr);
+    interior_tma<T, Tid, HS, S><<<p.grid, kTmaThreads, smem, s>>>(a, p.maps, p.units, p.nunits, p.ctr, p.wait_cycles,
+                                                                  p.withhold);
 }
 template <typename T, typename Tid, bool HS> void launch_tma_impl(const StepArgs<T, Tid> &a, const TmaPlan &p, cudaStream_t s) {
     if (p.stages >= 6) launch_tma_one<T, Tid, HS, 6>(a, p, s);

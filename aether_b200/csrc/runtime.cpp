@@ -1494,6 +1494,8 @@ void aefdtd_sim::build_work() {
             // tma_ctas 0: one unit per CTA; else units taken in turn by tma_ctas CTAs per SM
             p.grid = tma_ctas == 0 ? p.nunits : std::min(p.nunits, tma_ctas * nsm);
             p.stages = tma_stages;
+            p.wait_cycles = tma_wait_cycles;
+            p.withhold = tma_withhold;
             p.cells = tcells[half];
             if (p.nunits == 0) continue;
             WorkSplit &w = half == 0 ? wsE : wsH;
@@ -1546,6 +1548,7 @@ void aefdtd_sim::zero_state() {
     for (auto &b : psiE) if (b.p) AE_CUDA(cudaMemsetAsync(b.p, 0, b.n, stream));
     for (auto &b : psiH) if (b.p) AE_CUDA(cudaMemsetAsync(b.p, 0, b.n, stream));
     if (psi.p) AE_CUDA(cudaMemsetAsync(psi.p, 0, psi.n, stream));
+    if (tma_ctr.p) AE_CUDA(cudaMemsetAsync(tma_ctr.p, 0, tma_ctr.n, stream));
     if (obl) {
         for (int c = 0; c < 6; c++) {
             DBuf *b[3] = {&obl->Fi[c], &obl->psiEi[c], &obl->psiHi[c]};
@@ -2374,6 +2377,13 @@ aefdtd_status aefdtd_test_hook(aefdtd_sim *s, int32_t what, int64_t value) {
             s->tc_wait_cycles = value;
         } else if (what == AEFDTD_TEST_DFT_WITHHOLD_COPY) {
             s->tc_withhold_copy = value ? 1 : 0;
+        } else if (what == AEFDTD_TEST_STAGED_WAIT_CYCLES) {
+            if (value < 1) fail(AEFDTD_BAD_ARG, "wait bound must be at least 1 cycle");
+            s->tma_wait_cycles = value;
+            for (auto &p : s->tma_plan) p.wait_cycles = value;
+        } else if (what == AEFDTD_TEST_STAGED_WITHHOLD_COPY) {
+            s->tma_withhold = value ? 1 : 0;
+            for (auto &p : s->tma_plan) p.withhold = s->tma_withhold;
         } else {
             fail(AEFDTD_BAD_ARG, "unknown test hook");
         }

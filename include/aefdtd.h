@@ -439,6 +439,14 @@ aefdtd_status aefdtd_probe_copy_bandwidth(int32_t device, size_t bytes, int32_t 
  * (aefdtd_reset, then step again). */
 #define AEFDTD_TEST_DFT_WAIT_CYCLES 1
 #define AEFDTD_TEST_DFT_WITHHOLD_COPY 2
+/* The same for the staged interior half-steps (AEFDTD_TMA=1): the bound of
+ * each of their mbarrier waits (default 2^32 cycles), and (value 1) a
+ * producer that issues no tensor copy and arrives on no stage, so that the
+ * consumers' first wait runs out; every CTA then raises its abort flag, the
+ * producer waits (bounded) for its stages, and the next synchronising call
+ * returns AEFDTD_TIMEOUT. */
+#define AEFDTD_TEST_STAGED_WAIT_CYCLES 3
+#define AEFDTD_TEST_STAGED_WITHHOLD_COPY 4
 aefdtd_status aefdtd_test_hook(aefdtd_sim *sim, int32_t what, int64_t value);
 
 /* ---- batches: many simulations advanced together ----------------------

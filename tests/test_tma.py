@@ -19,8 +19,10 @@ import pytest
 
 import oracle_lib
 from aether_b200 import _abi as A
+from aether_b200 import _lib
 from aether_b200 import configs as CF
 from aether_b200 import fdtd
+from aether_b200._lib import AefdtdError
 
 pytestmark = pytest.mark.gpu
 
@@ -137,3 +139,43 @@ def test_tma_fp64_full_cell_matches_reference_core():
     ref = oracle_lib.run(sc, "ref", nsteps=200)
     got = run(sc, [200], tma=True)
     assert sha(got["fields"]) == sha(ref["fields"])
+
+
+STAGED_WAIT, STAGED_WITHHOLD = 3, 4   # AEFDTD_TEST_STAGED_WAIT_CYCLES, AEFDTD_TEST_STAGED_WITHHOLD_COPY
+TIMEOUT = 3
+
+
+def test_staged_wait_runs_out_then_handle_recovers():
+    """Bounded waits of the staged kernels: the test hook withholds every
+    tensor copy (and the stage arrives), so the consumers' first wait runs
+    out after 2^20 cycles; each CTA raises its abort flag and the error flag,
+    and the step's synchronising call returns AEFDTD_TIMEOUT with no GPU
+    fault. After the hook is cleared and the handle reset, a run gives the
+    fields of a fresh handle bit for bit (the unit counters were cleared)."""
+    sc = SCENES["cell128"](A.FP64)
+    want = run(sc, [64], tma=True)
+    lib = _lib.load()
+    saved = {k: os.environ.get(k) for k in ("AEFDTD_TMA", "AEFDTD_FUSED")}
+    os.environ.update({"AEFDTD_TMA": "1", "AEFDTD_FUSED": "0"})
+    try:
+        s = fdtd.build_simulation(sc)
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    with s:
+        _lib.check(lib.aefdtd_test_hook(s._h, STAGED_WAIT, 1 << 20))
+        _lib.check(lib.aefdtd_test_hook(s._h, STAGED_WITHHOLD, 1))
+        with pytest.raises(AefdtdError) as e:
+            s.step(64)
+            s.synchronize()
+        assert e.value.status == TIMEOUT
+        s.synchronize()   # the flag was read and cleared
+        _lib.check(lib.aefdtd_test_hook(s._h, STAGED_WITHHOLD, 0))
+        _lib.check(lib.aefdtd_test_hook(s._h, STAGED_WAIT, 1 << 32))
+        s.reset()
+        s.step(64)
+        s.synchronize()
+        assert sha(s.fields()) == sha(want["fields"])
