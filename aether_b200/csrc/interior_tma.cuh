@@ -51,6 +51,34 @@ template <typename T, typename Tid> struct TmaStage {
                   "tensor-copy destinations stay 128-byte aligned");
 };
 
+// z-CPML planes of a half-step: E [1, pml_zm) and [Nz - pml_zp + 1, Nz); H
+// [0, pml_zm) and [Nz - pml_zp, Nz - 1) (fdtd_pml.cpp:547,559,775,784).
+template <typename T, typename Tid>
+__device__ __forceinline__ bool zpsi_range(const StepArgs<T, Tid> &a, bool hs, int k) {
+    if (!a.pz) return false;
+    return hs ? (k < a.pml_zm || (k >= a.Nz - a.pml_zp && k < a.Nz - 1))
+              : ((k >= 1 && k < a.pml_zm) || k >= a.Nz - a.pml_zp + 1);
+}
+// The z psi pair (PsiE/Hxz, PsiE/Hyz) of one lane's two cells at one plane,
+// loaded ahead of the plane that uses it.
+template <typename T> struct ZPsi {
+    using V = typename Vec2<T>::type;
+    V p0, p1;
+    int i = -1, j = -1, k = -1;
+    __device__ __forceinline__ bool has(int ii, int jj, int kk) const { return i == ii && j == jj && k == kk; }
+    template <typename Tid> __device__ __forceinline__ long long index(const StepArgs<T, Tid> &a, int ii, int jj, int kk) const {
+        const int zn = (kk < a.pml_zm) ? kk : kk - (a.Nz - a.pml_zp) + a.pml_zm;
+        return ii + (long long)jj * a.Nx + (long long)zn * a.NxNy;
+    }
+    template <typename Tid> __device__ __forceinline__ void fetch(const StepArgs<T, Tid> &a, bool hs, int ii, int jj, int kk) {
+        if (!zpsi_range(a, hs, kk)) return;
+        const long long o = index(a, ii, jj, kk);
+        p0 = *reinterpret_cast<const V *>(a.psi_z0 + o);
+        p1 = *reinterpret_cast<const V *>(a.psi_z1 + o);
+        i = ii; j = jj; k = kk;
+    }
+};
+
 // Producer: one thread. HS: the H half-step.
 // limit: bound of each wait (SM cycles); withhold (test hook): no copy and
 // no arrive on any data stage, so the consumers' waits run out.
@@ -157,6 +185,8 @@ __device__ __forceinline__ void e_tma_consume(const StepArgs<T, Tid> &a, unsigne
     int st = 0;
     uint32_t ph = 0;
     T hxm0 = 0, hxm1 = 0, hym0 = 0, hym1 = 0, ikx0 = 0, ikx1 = 0, iky = 0;
+    // z-CPML psi of the lane's pair, loaded one plane ahead (tagged by tile and plane)
+    ZPsi<T> zp;
     for (;;) {
         if (!mbar::wait_or_abort(&full[st], ph, limit, abort)) {
             *abort = 1;
@@ -175,6 +205,7 @@ __device__ __forceinline__ void e_tma_consume(const StepArgs<T, Tid> &a, unsigne
             const V hy = *reinterpret_cast<const V *>(W1 + w * L::WX + L::hx + c);
             hxm0 = hx.x; hxm1 = hx.y; hym0 = hy.x; hym1 = hy.y;
             ikx0 = __ldg(a.ikx + x0 + c); ikx1 = __ldg(a.ikx + x0 + c + 1); iky = __ldg(a.iky + y0 + w);
+            zp.fetch(a, false, x0 + c, y0 + w, k == a.Nz - 1 ? 0 : k + 1);   // the unit's first plane
         } else {
             const T *R0 = reinterpret_cast<const T *>(b + L::oR0);   // Hz row y - 1
             const T *R1 = reinterpret_cast<const T *>(b + L::oR1);   // Hx row y - 1
@@ -210,12 +241,34 @@ __device__ __forceinline__ void e_tma_consume(const StepArgs<T, Tid> &a, unsigne
                 ney[q] = (C1 * eyq + (C2z * ikz) * (hxq - hxm)) - (C2x * ikx) * (hzq - hzim);
                 nez[q] = (C1 * ezq + (C2x * ikx) * (hyq - hyim)) - (C2y * iky) * (hxq - hxjm);
             }
+            if (zpsi_range(a, false, k)) {
+                // z-CPML planes: PsiExz, PsiEyz in app_pml_Ex / Ey order (after the curl update)
+                if (!zp.has(x0 + c, y0 + w, k)) zp.fetch(a, false, x0 + c, y0 + w, k);
+                const T bzk = __ldg(a.bz + k), czk = __ldg(a.cz + k);
+                V ps0, ps1;
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const T C4 = __ldg(&(a.coef + (q ? mp.y : mp.x))->C4);
+                    const T hxq = q ? hx.y : hx.x, hyq = q ? hy.y : hy.x;
+                    const T hxm = q ? hxm1 : hxm0, hym = q ? hym1 : hym0;
+                    const T p0 = cpml_rec(bzk, q ? zp.p0.y : zp.p0.x, czk, hyq - hym);
+                    const T p1 = cpml_rec(bzk, q ? zp.p1.y : zp.p1.x, czk, hxq - hxm);
+                    nex[q] -= C4 * p0;
+                    ney[q] += C4 * p1;
+                    if (q) { ps0.y = p0; ps1.y = p1; } else { ps0.x = p0; ps1.x = p1; }
+                }
+                const long long pz = zp.index(a, x0 + c, y0 + w, k);
+                *reinterpret_cast<V *>(a.psi_z0 + pz) = ps0;
+                *reinterpret_cast<V *>(a.psi_z1 + pz) = ps1;
+            }
+            if (a.pz && k == 0) { nex[0] = 0; nex[1] = 0; ney[0] = 0; ney[1] = 0; }
             const long long id = (x0 + c) + (long long)(y0 + w) * a.Nx + (long long)k * a.NxNy;
             V o;
             o.x = nex[0]; o.y = nex[1]; *reinterpret_cast<V *>(a.Ex + id) = o;
             o.x = ney[0]; o.y = ney[1]; *reinterpret_cast<V *>(a.Ey + id) = o;
             o.x = nez[0]; o.y = nez[1]; *reinterpret_cast<V *>(a.Ez + id) = o;
             hxm0 = hx.x; hxm1 = hx.y; hym0 = hy.x; hym1 = hy.y;
+            if (k + 1 < a.Nz) zp.fetch(a, false, x0 + c, y0 + w, k + 1);   // the next plane, while this stage is released
         }
         __syncwarp();
         if (l == 0) mbar::arrive(&empty[st]);
@@ -233,6 +286,7 @@ __device__ __forceinline__ void h_tma_consume(const StepArgs<T, Tid> &a, unsigne
     int st = 0;
     uint32_t ph = 0;
     T exp0 = 0, exp1 = 0, eyp0 = 0, eyp1 = 0, ax0 = 0, ax1 = 0, ay = 0;
+    ZPsi<T> zp;
     for (;;) {
         if (!mbar::wait_or_abort(&full[st], ph, limit, abort)) {
             *abort = 1;
@@ -253,6 +307,7 @@ __device__ __forceinline__ void h_tma_consume(const StepArgs<T, Tid> &a, unsigne
             ax0 = a.dtdmx * __ldg(a.ikx + x0 + c);
             ax1 = a.dtdmx * __ldg(a.ikx + x0 + c + 1);
             ay = a.dtdmy * __ldg(a.iky + y0 + w);
+            zp.fetch(a, true, x0 + c, y0 + w, k == 0 ? a.Nz - 1 : k - 1);   // the unit's first (top) plane
         } else {
             const T *R0 = reinterpret_cast<const T *>(b + L::oR0);   // Ez row y + 1
             const T *R1 = reinterpret_cast<const T *>(b + L::oR1);   // Ex row y + 1
@@ -286,12 +341,33 @@ __device__ __forceinline__ void h_tma_consume(const StepArgs<T, Tid> &a, unsigne
                 nhy[q] = hyq + (ax * (ezip - ezq) - az * (exkp - exq));
                 nhz[q] = hzq + (ay * (exjp - exq) - ax * (eyip - eyq));
             }
+            if (zpsi_range(a, true, k)) {
+                // z-CPML planes: PsiHxz, PsiHyz in app_pml_Hx / Hy order (after the curl update)
+                if (!zp.has(x0 + c, y0 + w, k)) zp.fetch(a, true, x0 + c, y0 + w, k);
+                const T bzk = __ldg(a.bz + k), czk = __ldg(a.cz + k);
+                V ps0, ps1;
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const T exq = q ? ex.y : ex.x, eyq = q ? ey.y : ey.x;
+                    const T exkp = q ? exp1 : exp0, eykp = q ? eyp1 : eyp0;
+                    const T p0 = cpml_rec(bzk, q ? zp.p0.y : zp.p0.x, czk, eykp - eyq);
+                    const T p1 = cpml_rec(bzk, q ? zp.p1.y : zp.p1.x, czk, exkp - exq);
+                    nhx[q] += a.dtm * p0;
+                    nhy[q] -= a.dtm * p1;
+                    if (q) { ps0.y = p0; ps1.y = p1; } else { ps0.x = p0; ps1.x = p1; }
+                }
+                const long long pz = zp.index(a, x0 + c, y0 + w, k);
+                *reinterpret_cast<V *>(a.psi_z0 + pz) = ps0;
+                *reinterpret_cast<V *>(a.psi_z1 + pz) = ps1;
+            }
+            if (a.pz && k == a.Nz - 1) { nhx[0] = 0; nhx[1] = 0; nhy[0] = 0; nhy[1] = 0; }
             const long long id = (x0 + c) + (long long)(y0 + w) * a.Nx + (long long)k * a.NxNy;
             V o;
             o.x = nhx[0]; o.y = nhx[1]; *reinterpret_cast<V *>(a.Hx + id) = o;
             o.x = nhy[0]; o.y = nhy[1]; *reinterpret_cast<V *>(a.Hy + id) = o;
             o.x = nhz[0]; o.y = nhz[1]; *reinterpret_cast<V *>(a.Hz + id) = o;
             exp0 = ex.x; exp1 = ex.y; eyp0 = ey.x; eyp1 = ey.y;
+            if (k > 0) zp.fetch(a, true, x0 + c, y0 + w, k - 1);   // the next plane down
         }
         __syncwarp();
         if (l == 0) mbar::arrive(&empty[st]);

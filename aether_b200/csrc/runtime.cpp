@@ -138,6 +138,8 @@ void aefdtd_sim::construct(const aefdtd_grid_desc *d) {
     if (const char *tu = std::getenv("AEFDTD_TMA_UNIT")) tma_unit = std::clamp(atoi(tu), 1, 4096);
     if (const char *tc = std::getenv("AEFDTD_TMA_CTAS")) tma_ctas = std::clamp(atoi(tc), 0, 2);
     if (const char *tg = std::getenv("AEFDTD_TMA_STAGES")) tma_stages = atoi(tg) >= 6 ? 6 : 4;
+    if (const char *tr = std::getenv("AEFDTD_TMA_RESERVE")) tma_reserve = std::clamp(atoi(tr), 0, 128);
+    if (const char *tz = std::getenv("AEFDTD_TMA_PZ")) tma_pz = atoi(tz) != 0;
     if (const char *ty = std::getenv("AEFDTD_TILE_Y")) {
         const int v = atoi(ty);
         tile_y = (v == 2 || v == 8) ? v : 4;
@@ -1309,11 +1311,13 @@ void aefdtd_sim::build_work() {
         const int rb = kTmaTileY / ty, nA = Nx / kTmaTileX, nB = Ny / kTmaTileY;
         for (int half = 0; half < 2; half++) {
             taken[half].assign(size_t(tiles) * Nz, 0);
+            // curl-only or z-CPML-only planes of every covered tile
             auto interior = [&](int A, int B, int k) {
                 for (int bb = 0; bb < rb; bb++)
                     for (int aa = 0; aa < 2; aa++) {
                         const unsigned f = feat[(size_t(k) * nty + B * rb + bb) * ntx + 2 * A + aa];
-                        if ((half == 0 ? group_e(f) : group_h(f)) != kGroupInterior) return false;
+                        const int g = half == 0 ? group_e(f) : group_h(f);
+                        if (g != kGroupInterior && !(g == kGroupPmlZ && tma_pz)) return false;
                     }
                 return true;
             };
@@ -1339,7 +1343,7 @@ void aefdtd_sim::build_work() {
             // CTAs finish within about one plane of each other.
             int nsm = 148;
             AE_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
-            const long long ctas = (long long)std::max(1, tma_ctas) * nsm;
+            const long long ctas = (long long)std::max(1, tma_ctas) * std::max(1, nsm - tma_reserve);
             // The H list runs top plane first (the planes E touched last), its
             // runs cut from the top down.
             if (half == 1) std::reverse(runs.begin(), runs.end());
@@ -1492,7 +1496,7 @@ void aefdtd_sim::build_work() {
             p.units = tma_units.as<int4>() + (half ? tunits[0].size() / 4 : 0);
             p.ctr = tma_ctr.as<int>() + 2 * half;
             // tma_ctas 0: one unit per CTA; else units taken in turn by tma_ctas CTAs per SM
-            p.grid = tma_ctas == 0 ? p.nunits : std::min(p.nunits, tma_ctas * nsm);
+            p.grid = tma_ctas == 0 ? p.nunits : std::min(p.nunits, tma_ctas * std::max(1, nsm - tma_reserve));
             p.stages = tma_stages;
             p.wait_cycles = tma_wait_cycles;
             p.withhold = tma_withhold;

@@ -387,6 +387,8 @@ struct aefdtd_sim {
     int tma_ctas = 2;                // AEFDTD_TMA_CTAS: 0 one unit per CTA; 1 or 2 CTAs per SM taking
                                      // units in turn (persistent)
     int tma_stages = 4;              // ring stages (AEFDTD_TMA_STAGES, 4 or 6)
+    int tma_reserve = 0;             // SMs left to the concurrent boundary groups (AEFDTD_TMA_RESERVE)
+    bool tma_pz = true;              // staged tiles may hold z-CPML planes (AEFDTD_TMA_PZ)
     long long tma_wait_cycles = 1LL << 32;   // wait bound and withheld-copy test hook (aefdtd_test_hook)
     int tma_withhold = 0;
     TmaPlan tma_plan[2] = {};        // E, H half-step

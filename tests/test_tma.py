@@ -1,5 +1,6 @@
-"""Staged interior half-steps (AEFDTD_TMA=1): curl-only 64 x 8 tiles whose
-planes reach shared memory through tensor copies (interior_tma.cuh).
+"""Staged interior half-steps (AEFDTD_TMA=1): curl-only and z-CPML 64 x 8
+tiles whose planes reach shared memory through tensor copies
+(interior_tma.cuh); every scene below has z-CPML planes in its staged tiles.
 
 FP64: fields, plane sums and flux bit-identical to the one-cell kernels
 (AEFDTD_TMA=0) on every tile situation the staged kernels meet: both periodic
