@@ -436,7 +436,7 @@ def batch_sample(n_cells=512, steps=256, seed=2024):
                     "8 of the cells stepped one at a time as plain FP64 simulations, device-timed"}
 
 
-def serving_sample(n_jobs=32, rate=1.5, seed=77, fp64_check=2, **server_opts):
+def serving_sample(n_jobs=32, rate=1.5, seed=77, fp64_check=8, **server_opts):
     """Serving: a seeded Poisson stream (rate jobs/s) of the batch sample's unit cells
     plus 10% large cells (period U(640, 1280) nm -> up to 256 x 256 cells,
     z = 384), step budgets U(4000, 20000), 101 wavelengths, FP32, served with
