@@ -85,7 +85,7 @@ class BatchOpts(C.Structure):
     _fields_ = [
         ("abi_version", C.c_int32), ("device", C.c_int32), ("l2_budget_bytes", C.c_int64),
         ("tile_y", C.c_int32), ("kchunk", C.c_int32), ("use_graphs", C.c_int32), ("graph_steps", C.c_int32),
-        ("lanes", C.c_int32), ("reserved", C.c_int32),
+        ("lanes", C.c_int32), ("persistent", C.c_int32),
     ]
 
 
@@ -95,7 +95,7 @@ BATCH_MAX_CLASSES = 32
 class BatchInfo(C.Structure):
     _fields_ = [
         ("n_members", C.c_int32), ("n_active", C.c_int32), ("n_subsets", C.c_int32), ("n_classes", C.c_int32),
-        ("n_lanes", C.c_int32), ("reserved", C.c_int32),
+        ("n_lanes", C.c_int32), ("n_persistent", C.c_int32),
         ("cells", C.c_int64), ("member_bytes", C.c_int64), ("batch_bytes", C.c_int64),
         ("l2_budget_bytes", C.c_int64), ("launches", C.c_uint64),
         ("class_key", C.c_int32 * BATCH_MAX_CLASSES), ("class_tile_y", C.c_int32 * BATCH_MAX_CLASSES),

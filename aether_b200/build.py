@@ -46,7 +46,7 @@ UNITS = [
     ("server.cpp", None),
 ]
 HEADERS = ["aefdtd_dev.hpp", "kernels.hpp", "sensors.cuh", "yee.cuh", "leapfrog.cuh", "sim.hpp", "mbar.cuh",
-           "interior_tma.cuh"]
+           "interior_tma.cuh", "batch_persist.cuh", "pulse.cuh"]
 
 
 def _stale(obj, deps):

@@ -164,6 +164,31 @@ inline int group_kernels(const WorkSplit &w) {
 // x0 flag of a 32-column item in a group of 64-column (pair) items
 constexpr int kHalfItem = 1 << 30;
 
+// ---- persistent batch kernel (batch_persist.cuh)
+// A unit: a band of tile rows (every x tile) of one member times one z-chunk
+// of its work items. Its items for each half-step, the units it waits on,
+// and the plane-sum planes it holds.
+struct PsUnit {
+    int m;              // member (index into the argument arrays)
+    int e_off, e_n;     // E items [e_off, e_off + e_n)
+    int h_off, h_n;     // H items
+    int nb[4];          // waited on: before E the y-1 and z-1 units, before H the y+1 and z+1 units
+    int band, j0, j1;   // plane-sum band: rows [j0, j1)
+    int planes;         // bit 0: the band's reflection plane kr is in this unit; bit 1: the transmission plane kt
+};
+template <typename T> struct SensorStepArgs;
+template <typename T, typename Tid> struct PersistArgs {
+    const StepArgs<T, Tid> *ea, *ha;   // per member
+    const SensorStepArgs<T> *sa;       // per member: nbp = bands, partial [steps][bands][12]
+    const PsUnit *units;
+    const int4 *items;                 // (x0, y0, k0 | k1 << 16, group)
+    int nunits, steps;
+    int *prog;                         // per unit: half-steps finished in this launch (zero at launch)
+    int *flags;                        // [0]: device error flag (1: a wait ran out), [1]: abort
+    long long wait_cycles;             // bound of each wait
+    int withhold;                      // test hook: unit 0 never reports its progress
+};
+
 // ---- sensor-path launch arguments (kernels in sensors.cuh)
 
 struct PulseDev {

@@ -65,8 +65,15 @@ struct BatchSubset {
     bool fused = false;            // a lone member that takes the fused time step
     bool built = false;
     bool solo = false;             // one member: its own single-simulation kernels and work lists
+    // one persistent launch per chunk (batch_persist.cuh): units, their items,
+    // progress counters, per-member sensor arguments and band partials
+    bool ps = false;
+    DBuf ps_units, ps_items, ps_prog, ps_sargs, ps_part;
+    int ps_nunits = 0, ps_grid = 0, ps_ty = 4;
     void release(size_t &t) {
         items.release(t);
+        ps_units.release(t); ps_items.release(t); ps_prog.release(t); ps_sargs.release(t); ps_part.release(t);
+        ps = false;
         argsE.release(t); argsH.release(t); sargs.release(t);
         if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
         if (graph_b) { cudaGraphExecDestroy(graph_b); graph_b = nullptr; }
@@ -128,6 +135,10 @@ struct aefdtd_batch {
     int next_solo_class = -1;   // size-class keys below zero: members that never share a subset
     int graph_steps = 32;          // steps per captured chunk (a divisor of seg_len)
     bool h_reverse = false;        // H pass over the members in reverse order (measured slower on L2-sized subsets)
+    int persistent = 0;            // subsets run each chunk as one persistent launch (batch_persist.cuh)
+    DBuf ps_flags;                 // persistent launches: [0] device error flag, [1] abort
+    bool ps_direct = false;        // the persistent launch did not capture into a graph: launched directly
+    std::map<int, int> ps_capacity;   // resident persistent CTAs per tile height
     uint64_t launches = 0;
     size_t dev_bytes = 0;
 
@@ -145,12 +156,17 @@ struct aefdtd_batch {
         for (auto &m : members) m.placed = false;
         layout_dirty = true;
     }
+    // subsets whose state stays in the 126 MB L2 between steps
+    static bool l2_resident(const BatchSubset &u) { return u.bytes <= (96ull << 20); }
     bool fits(const BatchSubset &u, size_t b) const {
         return u.members.empty() || l2_budget < 0 || (long long)(u.bytes + b) <= l2_budget;
     }
     void place(BatchMember &m);
     void update_layout();
     template <typename T, typename Tid> void build_subset(BatchSubset &u);
+    template <typename T, typename Tid>
+    void build_persist(BatchSubset &u, const std::vector<SensorStepArgs<T>> &sa);
+    void check_persist();
     template <typename T, typename Tid> void enqueue_steps(BatchSubset &u, int L, Lane &ln);
     template <typename T, typename Tid> void run_segment(BatchSubset &u, int L, Lane &ln);
     void sync_lanes() {
@@ -173,6 +189,7 @@ aefdtd_batch::~aefdtd_batch() {
         m.sim->work_dirty = true;
     }
     for (auto &u : subsets) u.release(dev_bytes);
+    ps_flags.release(dev_bytes);
     for (auto &ln : lanes) ln.destroy();
 }
 
@@ -248,9 +265,13 @@ template <typename T, typename Tid> void aefdtd_batch::build_subset(BatchSubset 
     // A lone member keeps its own work lists (two-cell items, L2-ordered H
     // lists) and kernels; merged members take one-cell, forward lists.
     u.solo = u.members.size() == 1;
+    // the persistent launch takes every member's one-cell, forward lists;
+    // oblique members and completion sensors keep the split launches
+    u.ps = persistent != 0;
+    for (aefdtd_sim *s : u.members) u.ps = u.ps && !s->obl && s->cc_coeff <= 0;
     for (aefdtd_sim *s : u.members) {
-        const unsigned pm = u.solo ? s->pair_mask0 : 0u;
-        const int hr = u.solo ? s->h_reverse0 : 0;
+        const unsigned pm = (u.solo && !u.ps) ? s->pair_mask0 : 0u;
+        const int hr = (u.solo && !u.ps) ? s->h_reverse0 : 0;
         if (s->pair_mask != pm || s->h_reverse != hr || s->work_dirty) {
             s->pair_mask = pm;
             s->h_reverse = hr;
@@ -262,7 +283,7 @@ template <typename T, typename Tid> void aefdtd_batch::build_subset(BatchSubset 
     // FT-mode completion sensor, whose check steps need the ring snapshots of
     // the batched path)
     aefdtd_sim *m0 = u.members[0];
-    u.fused = u.solo && m0->fused_eligible() && !m0->ccft;
+    u.fused = !u.ps && u.solo && m0->fused_eligible() && !m0->ccft;
     if (u.fused) {
         if (m0->fwork_dirty) m0->build_fused_work();
         m0->ensure_other_set();
@@ -307,6 +328,8 @@ template <typename T, typename Tid> void aefdtd_batch::build_subset(BatchSubset 
         aefdtd_sim *s = u.members[li];
         const StepScalars *tbl = s->tables.as<StepScalars>();
         s->make_step_args(ea[li], ha[li], tbl);
+        // members that stay in L2 take no up-front L2 prefetch of each item's planes
+        if (l2_resident(u)) ea[li].prefetch = ha[li].prefetch = 0;
         s->make_sensor_args(sa[li], tbl);
         if (sa[li].nbp > 0) {
             u.nplane++;
@@ -322,7 +345,112 @@ template <typename T, typename Tid> void aefdtd_batch::build_subset(BatchSubset 
     u.nblk = (int)blk.size();
     u.blkmap.alloc(std::max<size_t>(blk.size(), 1) * sizeof(int2), dev_bytes);
     if (!blk.empty()) AE_CUDA(cudaMemcpy(u.blkmap.p, blk.data(), blk.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    if (u.ps) build_persist<T, Tid>(u, sa);
     u.built = true;
+}
+
+// Units of the persistent launch (batch_persist.cuh): per member, a band of
+// tile_y rows times a z-chunk of kchunk planes; each unit holds the member's
+// items of that band and chunk (every group, tagged with its group) and the
+// four units it waits on. Normal-mode members get their plane sums per band.
+template <typename T, typename Tid>
+void aefdtd_batch::build_persist(BatchSubset &u, const std::vector<SensorStepArgs<T>> &sa) {
+    const int ty = u.members[0]->tile_y;
+    const size_t n = u.members.size();
+    std::vector<size_t> part_off(n, 0);
+    size_t part_n = 0;
+    for (size_t li = 0; li < n; li++) {
+        const aefdtd_sim *s = u.members[li];
+        if (s->tile_y != ty) fail(AEFDTD_BAD_ARG, "members of a subset share their tile height");
+        if (sa[li].nbp > 0) {
+            part_off[li] = part_n;
+            part_n += size_t(seg_len) * ((s->Ny + ty - 1) / ty) * 12;
+        }
+    }
+    u.ps_part.alloc(std::max<size_t>(part_n, 1) * sizeof(double), dev_bytes);
+    std::vector<PsUnit> units;
+    std::vector<int4> items;
+    std::vector<SensorStepArgs<T>> psa(n);
+    for (size_t li = 0; li < n; li++) {
+        const aefdtd_sim *s = u.members[li];
+        const int kc = s->kchunk, nb = (s->Ny + ty - 1) / ty, nch = (s->Nz + kc - 1) / kc;
+        const int base = (int)units.size();
+        std::vector<std::vector<int4>> eb(size_t(nb) * nch), hb(size_t(nb) * nch);
+        for (int half = 0; half < 2; half++) {
+            const WorkSplit &w = half ? s->wsH : s->wsE;
+            auto &dst = half ? hb : eb;
+            for (int g = 0; g < kGroups; g++)
+                for (int k = 0; k < w.n[g]; k++) {
+                    const int *it = &s->items_host[size_t(w.off[g] + k) * 4];
+                    const int x0 = it[0], y0 = it[1], k0 = it[2], k1 = it[3];
+                    const int b = y0 / ty, c = k0 / kc;
+                    if ((x0 & kHalfItem) || y0 % ty || k1 <= k0 || (k1 - 1) / kc != c)
+                        fail(AEFDTD_BAD_ARG, "a work item does not fit the persistent units");
+                    dst[size_t(c) * nb + b].push_back(make_int4(x0, y0, k0 | (k1 << 16), g));
+                }
+        }
+        auto id = [&](int c, int b) { return base + c * nb + b; };
+        for (int c = 0; c < nch; c++)
+            for (int b = 0; b < nb; b++) {
+                PsUnit U{};
+                U.m = (int)li;
+                U.e_off = (int)items.size();
+                items.insert(items.end(), eb[size_t(c) * nb + b].begin(), eb[size_t(c) * nb + b].end());
+                U.e_n = (int)items.size() - U.e_off;
+                U.h_off = (int)items.size();
+                items.insert(items.end(), hb[size_t(c) * nb + b].begin(), hb[size_t(c) * nb + b].end());
+                U.h_n = (int)items.size() - U.h_off;
+                U.nb[0] = id(c, (b + nb - 1) % nb);
+                U.nb[1] = id((c + nch - 1) % nch, b);
+                U.nb[2] = id(c, (b + 1) % nb);
+                U.nb[3] = id((c + 1) % nch, b);
+                U.band = b;
+                U.j0 = b * ty;
+                U.j1 = std::min(s->Ny, U.j0 + ty);
+                if (sa[li].nbp > 0) {
+                    const int z0 = c * kc, z1 = std::min(s->Nz, z0 + kc);
+                    if (sa[li].kr >= z0 && sa[li].kr < z1) U.planes |= 1;
+                    if (sa[li].kt >= z0 && sa[li].kt < z1) U.planes |= 2;
+                }
+                units.push_back(U);
+            }
+        psa[li] = sa[li];
+        if (sa[li].nbp > 0) {
+            psa[li].nbp = nb;
+            psa[li].partial = u.ps_part.as<double>() + part_off[li];
+        }
+    }
+    u.ps_nunits = (int)units.size();
+    u.ps_ty = ty;
+    u.ps_units.alloc(sizeof(PsUnit) * units.size(), dev_bytes);
+    AE_CUDA(cudaMemcpy(u.ps_units.p, units.data(), sizeof(PsUnit) * units.size(), cudaMemcpyHostToDevice));
+    u.ps_items.alloc(std::max<size_t>(items.size(), 1) * sizeof(int4), dev_bytes);
+    if (!items.empty())
+        AE_CUDA(cudaMemcpy(u.ps_items.p, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice));
+    u.ps_sargs.alloc(sizeof(SensorStepArgs<T>) * n, dev_bytes);
+    AE_CUDA(cudaMemcpy(u.ps_sargs.p, psa.data(), sizeof(SensorStepArgs<T>) * n, cudaMemcpyHostToDevice));
+    u.ps_prog.alloc(sizeof(int) * units.size(), dev_bytes);
+    if (!ps_flags.p) {
+        ps_flags.alloc(2 * sizeof(int), dev_bytes);
+        AE_CUDA(cudaMemset(ps_flags.p, 0, 2 * sizeof(int)));
+    }
+    auto cap = ps_capacity.find(ty);
+    if (cap == ps_capacity.end()) cap = ps_capacity.emplace(ty, persist_capacity<T, Tid>(ty)).first;
+    if (cap->second <= 0) fail(AEFDTD_CUDA_ERROR, "the persistent batch kernel does not fit on the device");
+    // the lanes share the device: each subset's launch takes its share of the resident CTAs
+    u.ps_grid = std::max(1, std::min(u.ps_nunits, cap->second / std::max(1, n_lanes)));
+}
+
+// The device error flag of the persistent launches: a wait that ran out
+// leaves the members' fields part-way through a chunk (reset them).
+void aefdtd_batch::check_persist() {
+    if (!ps_flags.p) return;
+    int h[2] = {0, 0};
+    AE_CUDA(cudaMemcpy(h, ps_flags.p, sizeof(h), cudaMemcpyDeviceToHost));
+    if (h[0] || h[1]) {
+        AE_CUDA(cudaMemset(ps_flags.p, 0, sizeof(h)));
+        fail(AEFDTD_TIMEOUT, "a bounded wait of the persistent batch launch ran out");
+    }
 }
 
 // Same fork/join scheme as a single simulation's half-step (runtime.cpp, run_groups).
@@ -365,6 +493,29 @@ template <typename T, typename Tid> void aefdtd_batch::enqueue_steps(BatchSubset
     }
     const auto *ea = u.argsE.as<StepArgs<T, Tid>>();
     const auto *ha = u.argsH.as<StepArgs<T, Tid>>();
+    if (u.ps) {
+        // one cooperative launch for all L steps, then the plane sums of every member
+        AE_CUDA(cudaMemsetAsync(u.ps_prog.p, 0, sizeof(int) * u.ps_nunits, ln.stream));
+        PersistArgs<T, Tid> pa{};
+        pa.ea = ea;
+        pa.ha = ha;
+        pa.sa = u.ps_sargs.as<SensorStepArgs<T>>();
+        pa.units = u.ps_units.as<PsUnit>();
+        pa.items = u.ps_items.as<int4>();
+        pa.nunits = u.ps_nunits;
+        pa.steps = L;
+        pa.prog = u.ps_prog.as<int>();
+        pa.flags = ps_flags.as<int>();
+        pa.wait_cycles = u.members[0]->ps_wait_cycles;
+        pa.withhold = u.members[0]->ps_withhold;
+        AE_CUDA(launch_persist(pa, u.ps_grid, u.ps_ty, ln.stream));
+        launches++;
+        if (u.nplane > 0) {
+            launch_plane_reduce_batch(u.ps_sargs.as<SensorStepArgs<T>>(), (int)u.members.size(), L, ln.stream);
+            launches++;
+        }
+        return;
+    }
     const auto *sa = u.sargs.as<SensorStepArgs<T>>();
     const int4 *it = u.items.as<int4>();
     const int2 *blk = u.blkmap.as<int2>();
@@ -374,7 +525,10 @@ template <typename T, typename Tid> void aefdtd_batch::enqueue_steps(BatchSubset
     // a lone member: its own arguments as launch parameters, its own lists
     aefdtd_sim *m0 = u.members[0];
     StepArgs<T, Tid> se, sh, se_i, sh_i;
-    if (u.solo) m0->make_step_args(se, sh, m0->tables.as<StepScalars>());
+    if (u.solo) {
+        m0->make_step_args(se, sh, m0->tables.as<StepScalars>());
+        if (l2_resident(u)) se.prefetch = sh.prefetch = 0;
+    }
     // an oblique member (always alone): its imaginary grid on the same lists, and its R/T sums
     const bool obl = u.solo && m0->obl;
     if (obl) {
@@ -454,7 +608,7 @@ template <typename T, typename Tid> void aefdtd_batch::run_segment(BatchSubset &
     std::vector<StepScalars> host(seg_len);
     int done = 0;
     while (done < L) {
-        const bool graph = opts.use_graphs >= 0 && L - done >= graph_steps;
+        const bool graph = opts.use_graphs >= 0 && !(u.ps && ps_direct) && L - done >= graph_steps;
         const int C = graph ? graph_steps : L - done;
         for (aefdtd_sim *s : u.members) {
             for (int q = 0; q < C; q++) s->fill_scalars(s->tstep + q, q, host[q]);
@@ -485,16 +639,37 @@ template <typename T, typename Tid> void aefdtd_batch::run_segment(BatchSubset &
             if (!gx) {
                 const uint64_t l0 = launches;
                 AE_CUDA(cudaStreamBeginCapture(ln.stream, cudaStreamCaptureModeThreadLocal));
-                enqueue_steps<T, Tid>(u, C, ln);
+                Error err{AEFDTD_OK, ""};
+                try {
+                    enqueue_steps<T, Tid>(u, C, ln);
+                } catch (const Error &e) {
+                    err = e;
+                }
                 cudaGraph_t gr = nullptr;
-                AE_CUDA(cudaStreamEndCapture(ln.stream, &gr));
-                AE_CUDA(cudaGraphInstantiate(&gx, gr, 0));
-                cudaGraphDestroy(gr);
-                u.graph_launches = launches - l0;
+                cudaError_t ec = cudaStreamEndCapture(ln.stream, &gr);
+                if (err.st == AEFDTD_OK && ec == cudaSuccess) ec = cudaGraphInstantiate(&gx, gr, 0);
+                if (gr) cudaGraphDestroy(gr);
+                const uint64_t captured = launches - l0;
                 launches = l0;
+                if (err.st != AEFDTD_OK || ec != cudaSuccess) {
+                    gx = nullptr;
+                    // a device that cannot capture the cooperative launch runs it directly
+                    if (!u.ps) {
+                        if (err.st != AEFDTD_OK) throw err;
+                        AE_CUDA(ec);
+                    }
+                    cudaGetLastError();
+                    ps_direct = true;
+                } else {
+                    u.graph_launches = captured;
+                }
             }
-            AE_CUDA(cudaGraphLaunch(gx, ln.stream));
-            launches += u.graph_launches;
+            if (gx) {
+                AE_CUDA(cudaGraphLaunch(gx, ln.stream));
+                launches += u.graph_launches;
+            } else {
+                enqueue_steps<T, Tid>(u, C, ln);
+            }
         } else {
             enqueue_steps<T, Tid>(u, C, ln);
         }
@@ -654,6 +829,7 @@ template <typename T, typename Tid> int aefdtd_batch::advance(int max_steps) {
     }
     sync_lanes();
     AE_CUDA(cudaGetLastError());
+    check_persist();
     return most;
 }
 
@@ -663,11 +839,13 @@ template <typename T, typename Tid> double aefdtd_batch::time_segments(int reps)
     update_layout();
     for (size_t k = 0; k < subsets.size(); k++) run_segment<T, Tid>(subsets[k], seg_len, lanes[k % n_lanes]);
     sync_lanes();
+    check_persist();
     int a = 0, b = 0;   // host clock over all lanes (the device is idle before)
     const auto t0 = std::chrono::steady_clock::now();
     for (int r = 0; r < reps; r++)
         for (size_t k = 0; k < subsets.size(); k++) run_segment<T, Tid>(subsets[k], seg_len, lanes[k % n_lanes]);
     sync_lanes();
+    check_persist();
     (void)a; (void)b;
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -726,23 +904,26 @@ template <typename T, typename Tid> void aefdtd_batch::autotune() {
             }
         apply(cls, pick);
     }
-    // L2 budget and lanes over all members
+    // L2 budget, lanes and the persistent launch over all members
     for (auto &m : members) m.remaining = 1 << 30;
     double best = 1e30;
     long long pick = budget0;
-    int pick_lanes = n_lanes;
-    for (long long b : {48LL << 20, 96LL << 20, -1LL})
-        for (int nl : {1, 2, 4}) {
-            if (b < 0 && nl > 1) continue;   // one subset per class: lanes only split classes
-            l2_budget = b;
-            n_lanes = nl;
-            drop_layout();
-            restart();
-            const double t = time_segments<T, Tid>(1);
-            if (t < best) { best = t; pick = b; pick_lanes = nl; }
-        }
+    int pick_lanes = n_lanes, pick_ps = persistent;
+    for (int ps : {0, 1})
+        for (long long b : {48LL << 20, 96LL << 20, -1LL})
+            for (int nl : {1, 2, 4}) {
+                if (b < 0 && nl > 1) continue;   // one subset per class: lanes only split classes
+                l2_budget = b;
+                n_lanes = nl;
+                persistent = ps;
+                drop_layout();
+                restart();
+                const double t = time_segments<T, Tid>(1);
+                if (t < best) { best = t; pick = b; pick_lanes = nl; pick_ps = ps; }
+            }
     l2_budget = pick;
     n_lanes = pick_lanes;
+    persistent = pick_ps;
     drop_layout();
     restart();
     for (size_t i = 0; i < members.size(); i++) members[i].remaining = saved[i];
@@ -824,6 +1005,8 @@ aefdtd_status aefdtd_batch_create(const aefdtd_batch_opts *opts, aefdtd_batch **
         for (auto &ln : b->lanes) ln.create();
         b->stream = b->lanes[0].stream;
         if (b->opts.lanes > 0) b->n_lanes = std::min(b->opts.lanes, kMaxLanes);
+        b->persistent = b->opts.persistent != 0;
+        if (const char *ps = std::getenv("AEFDTD_BATCH_PERSIST")) b->persistent = atoi(ps) != 0;
     });
     if (st != AEFDTD_OK) {
         delete b;
@@ -964,6 +1147,8 @@ aefdtd_status aefdtd_batch_get_info(aefdtd_batch *b, aefdtd_batch_info *info) {
         }
         info->n_subsets = (int32_t)b->subsets.size();
         info->n_lanes = b->n_lanes;
+        info->n_persistent = 0;
+        for (const auto &u : b->subsets) info->n_persistent += u.built && u.ps;
         info->l2_budget_bytes = b->l2_budget;
         info->launches = b->launches;
         info->batch_bytes = (int64_t)b->dev_bytes;

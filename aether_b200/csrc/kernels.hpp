@@ -32,6 +32,18 @@ AEFDTD_DECL_FUSED(double, uint16_t)
 AEFDTD_DECL_FUSED(float, uint8_t)
 AEFDTD_DECL_FUSED(float, uint16_t)
 #undef AEFDTD_DECL_FUSED
+// yee_f64.cu (--fmad=false) and yee_f32.cu: the persistent batch kernel
+// (batch_persist.cuh), one cooperative launch of `grid` CTAs of 32 x ty
+// threads; persist_capacity: such CTAs resident on the current device at once
+template <typename T, typename Tid> int persist_capacity(int ty);
+#define AEFDTD_DECL_PERSIST(T, Tid)                                                                    \
+    cudaError_t launch_persist(const PersistArgs<T, Tid> &p, int grid, int ty, cudaStream_t s);        \
+    template <> int persist_capacity<T, Tid>(int ty);
+AEFDTD_DECL_PERSIST(double, uint8_t)
+AEFDTD_DECL_PERSIST(double, uint16_t)
+AEFDTD_DECL_PERSIST(float, uint8_t)
+AEFDTD_DECL_PERSIST(float, uint16_t)
+#undef AEFDTD_DECL_PERSIST
 AEFDTD_DECL_YEE(double, uint8_t)
 AEFDTD_DECL_YEE(double, uint16_t)
 AEFDTD_DECL_YEE(float, uint8_t)

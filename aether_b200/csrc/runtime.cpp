@@ -2388,6 +2388,11 @@ aefdtd_status aefdtd_test_hook(aefdtd_sim *s, int32_t what, int64_t value) {
         } else if (what == AEFDTD_TEST_STAGED_WITHHOLD_COPY) {
             s->tma_withhold = value ? 1 : 0;
             for (auto &p : s->tma_plan) p.withhold = s->tma_withhold;
+        } else if (what == AEFDTD_TEST_PERSIST_WAIT_CYCLES) {
+            if (value < 1) fail(AEFDTD_BAD_ARG, "wait bound must be at least 1 cycle");
+            s->ps_wait_cycles = value;
+        } else if (what == AEFDTD_TEST_PERSIST_WITHHOLD) {
+            s->ps_withhold = value ? 1 : 0;
         } else {
             fail(AEFDTD_BAD_ARG, "unknown test hook");
         }

@@ -344,6 +344,9 @@ struct aefdtd_sim {
     // tensor-core DFT wait bound and the withheld-copy test hook (aefdtd_test_hook)
     long long tc_wait_cycles = 1LL << 32;
     int tc_withhold_copy = 0;
+    // persistent batch launch: wait bound and withheld-progress test hook (aefdtd_test_hook)
+    long long ps_wait_cycles = 1LL << 31;
+    int ps_withhold = 0;
     // captured segments, keyed by table slot, pending-flush state and the
     // sensors' buffer halves (the pointers a segment's launches bake in)
     std::map<uint64_t, cudaGraphExec_t> graph_exec;

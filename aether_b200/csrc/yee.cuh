@@ -59,6 +59,17 @@ template <typename T> __device__ __forceinline__ T cpml_rec(T b, T psi, T c, T d
 // L2 prefetch hint for the line holding p (no register result, no wait).
 __device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
+// Loads of the other field family (and of the oblique driver's other grid).
+// Within one half-step launch those arrays do not change, so they go through
+// the read-only path. In the persistent batch kernel (batch_persist.cuh) other
+// CTAs rewrite them during the launch: Coh selects ordinary cached loads
+// (ld.global.ca), which the kernel's acquire of a neighbour's progress counter
+// orders after that neighbour's stores; read-only-path data may stay stale.
+template <bool Coh, typename X> __device__ __forceinline__ X ldf(const X *p) {
+    if constexpr (Coh) return __ldca(p);
+    else return __ldg(p);
+}
+
 // Boundary-item features (bit mask per item; a kernel compiled for set F may
 // run any item whose mask is a subset of F).
 constexpr unsigned kFPmlXY = 1;   // a cell in an x or y CPML range or PEC plane
@@ -76,7 +87,7 @@ constexpr unsigned kFAll = 15;
 // other feature): the psi_z recursions and PEC of app_pml_Ex/Ey
 // (fdtd_pml.cpp:504-735) are applied after the curl update, in the general
 // kernel's order.
-template <typename T, typename Tid, int U, bool PZ = false>
+template <typename T, typename Tid, int U, bool PZ = false, bool Coh = false>
 __device__ __forceinline__ void e_interior_body(const StepArgs<T, Tid> &a, int q, int4 it) {
     // coefficients through the read-only path: short-lived CTAs skip a table fill and barrier
     const int i = it.x + threadIdx.x, j = it.y + threadIdx.y;
@@ -99,8 +110,8 @@ __device__ __forceinline__ void e_interior_body(const StepArgs<T, Tid> &a, int q
     const MatCoef<T> *__restrict__ coef = a.coef;
     const T ikx = __ldg(a.ikx + i), iky = __ldg(a.iky + j);
     const int kmi = (it.z == 0) ? a.Nz - 1 : it.z - 1;
-    T hx_km = __ldg(Hx + col + kmi * NxNy);
-    T hy_km = __ldg(Hy + col + kmi * NxNy);
+    T hx_km = ldf<Coh>(Hx + col + kmi * NxNy);
+    T hy_km = ldf<Coh>(Hy + col + kmi * NxNy);
     if (a.prefetch & 1) {
         // every plane of the item into L2 up front: only the first iteration
         // waits on DRAM; the y-1 row lines are fetched by row 0 only
@@ -129,9 +140,9 @@ __device__ __forceinline__ void e_interior_body(const StepArgs<T, Tid> &a, int q
         for (int u = 0; u < U; ++u) {
             // planes past the chunk end re-read its last plane (not stored)
             const long long o = (long long)min(k + u, it.w - 1) * NxNy;
-            hx[u] = __ldg(Hx + col + o); hy[u] = __ldg(Hy + col + o); hz[u] = __ldg(Hz + col + o);
-            hz_jm[u] = __ldg(Hz + coly + o); hx_jm[u] = __ldg(Hx + coly + o);
-            hz_im[u] = __ldg(Hz + colx + o); hy_im[u] = __ldg(Hy + colx + o);
+            hx[u] = ldf<Coh>(Hx + col + o); hy[u] = ldf<Coh>(Hy + col + o); hz[u] = ldf<Coh>(Hz + col + o);
+            hz_jm[u] = ldf<Coh>(Hz + coly + o); hx_jm[u] = ldf<Coh>(Hx + coly + o);
+            hz_im[u] = ldf<Coh>(Hz + colx + o); hy_im[u] = ldf<Coh>(Hy + colx + o);
             ex[u] = Ex[col + o]; ey[u] = Ey[col + o]; ez[u] = Ez[col + o];
             m[u] = __ldg(mat + colm + (long long)min(k + u, it.w - 1) * mNxNy);
             if constexpr (PZ) {
@@ -186,7 +197,7 @@ __device__ __forceinline__ void e_interior_body(const StepArgs<T, Tid> &a, int q
 
 // PZ: as for E, with the H-side z range, psi recursions and z = Nz-1 PEC of
 // app_pml_Hx/Hy (fdtd_pml.cpp:737-929).
-template <typename T, typename Tid, int U, bool PZ = false>
+template <typename T, typename Tid, int U, bool PZ = false, bool Coh = false>
 __device__ __forceinline__ void h_interior_body(const StepArgs<T, Tid> &a, int q, int4 it) {
     const int i = it.x + threadIdx.x, j = it.y + threadIdx.y;
     if (i >= a.Nx || j >= a.Ny) return;
@@ -204,8 +215,8 @@ __device__ __forceinline__ void h_interior_body(const StepArgs<T, Tid> &a, int q
     T *__restrict__ Hz = a.Hz;
     const T ax = a.dtdmx * __ldg(a.ikx + i);
     const T ay = a.dtdmy * __ldg(a.iky + j);
-    T ex = __ldg(Ex + col + it.z * NxNy);
-    T ey = __ldg(Ey + col + it.z * NxNy);
+    T ex = ldf<Coh>(Ex + col + it.z * NxNy);
+    T ey = ldf<Coh>(Ey + col + it.z * NxNy);
     if (a.prefetch & 1) {
         // every plane of the item (and the E plane above it) into L2 up front;
         // the y+1 row lines are fetched by the last row only
@@ -234,10 +245,10 @@ __device__ __forceinline__ void h_interior_body(const StepArgs<T, Tid> &a, int q
             const int kk = min(k + u, it.w - 1);
             const int kp = (kk == a.Nz - 1) ? 0 : kk + 1;
             const long long o = (long long)kk * NxNy, op = (long long)kp * NxNy;
-            ex_kp[u] = __ldg(Ex + col + op); ey_kp[u] = __ldg(Ey + col + op);
-            ez[u] = __ldg(Ez + col + o);
-            ez_jp[u] = __ldg(Ez + coly + o); ex_jp[u] = __ldg(Ex + coly + o);
-            ez_ip[u] = __ldg(Ez + colx + o); ey_ip[u] = __ldg(Ey + colx + o);
+            ex_kp[u] = ldf<Coh>(Ex + col + op); ey_kp[u] = ldf<Coh>(Ey + col + op);
+            ez[u] = ldf<Coh>(Ez + col + o);
+            ez_jp[u] = ldf<Coh>(Ez + coly + o); ex_jp[u] = ldf<Coh>(Ex + coly + o);
+            ez_ip[u] = ldf<Coh>(Ez + colx + o); ey_ip[u] = ldf<Coh>(Ey + colx + o);
             hx[u] = Hx[col + o]; hy[u] = Hy[col + o]; hz[u] = Hz[col + o];
             if constexpr (PZ) {
                 // H-side z range [0, pml_zm) and [Nz - pml_zp, Nz - 1) (fdtd_pml.cpp:775,784)
@@ -296,7 +307,7 @@ __device__ __forceinline__ T bloch_ghost(int bloch, T own, T other, double c, do
 }
 
 // ---- boundary items: the phases of feature set F ---------------------------
-template <typename T, typename Tid, unsigned F>
+template <typename T, typename Tid, unsigned F, bool Coh = false>
 __device__ __forceinline__ void e_boundary_body(const StepArgs<T, Tid> &a, int q, int4 it) {
     const int i = it.x + threadIdx.x, j = it.y + threadIdx.y;
     if (i >= a.Nx || j >= a.Ny) return;
@@ -358,24 +369,24 @@ __device__ __forceinline__ void e_boundary_body(const StepArgs<T, Tid> &a, int q
             }
     }
     const int kmi = (k0 == 0) ? a.Nz - 1 : k0 - 1;
-    T hx_km = __ldg(Hx + col + kmi * NxNy);
-    T hy_km = __ldg(Hy + col + kmi * NxNy);
+    T hx_km = ldf<Coh>(Hx + col + kmi * NxNy);
+    T hy_km = ldf<Coh>(Hy + col + kmi * NxNy);
 
     for (int k = k0; k < k1; ++k) {
         const long long id = col + k * NxNy;
-        const T hx = __ldg(Hx + id), hy = __ldg(Hy + id), hz = __ldg(Hz + id);
-        T hz_jm = __ldg(Hz + coly + k * NxNy), hx_jm = __ldg(Hx + coly + k * NxNy);
-        T hz_im = __ldg(Hz + colx + k * NxNy), hy_im = __ldg(Hy + colx + k * NxNy);
+        const T hx = ldf<Coh>(Hx + id), hy = ldf<Coh>(Hy + id), hz = ldf<Coh>(Hz + id);
+        T hz_jm = ldf<Coh>(Hz + coly + k * NxNy), hx_jm = ldf<Coh>(Hx + coly + k * NxNy);
+        T hz_im = ldf<Coh>(Hz + colx + k * NxNy), hy_im = ldf<Coh>(Hy + colx + k * NxNy);
         if constexpr ((F & kFMisc) != 0) {
             // oblique driver: H ghosts past the y = 0 and x = 0 edges (set before update_E)
             if (a.bloch) {
                 if (j == 0) {
-                    hz_jm = bloch_ghost(a.bloch, hz_jm, __ldg(a.oHz + coly + k * NxNy), a.byr, a.byi);
-                    hx_jm = bloch_ghost(a.bloch, hx_jm, __ldg(a.oHx + coly + k * NxNy), a.byr, a.byi);
+                    hz_jm = bloch_ghost(a.bloch, hz_jm, ldf<Coh>(a.oHz + coly + k * NxNy), a.byr, a.byi);
+                    hx_jm = bloch_ghost(a.bloch, hx_jm, ldf<Coh>(a.oHx + coly + k * NxNy), a.byr, a.byi);
                 }
                 if (i == 0) {
-                    hz_im = bloch_ghost(a.bloch, hz_im, __ldg(a.oHz + colx + k * NxNy), a.bxr, a.bxi);
-                    hy_im = bloch_ghost(a.bloch, hy_im, __ldg(a.oHy + colx + k * NxNy), a.bxr, a.bxi);
+                    hz_im = bloch_ghost(a.bloch, hz_im, ldf<Coh>(a.oHz + colx + k * NxNy), a.bxr, a.bxi);
+                    hy_im = bloch_ghost(a.bloch, hy_im, ldf<Coh>(a.oHy + colx + k * NxNy), a.bxr, a.bxi);
                 }
             }
         }
@@ -555,7 +566,7 @@ __device__ __forceinline__ void e_boundary_body(const StepArgs<T, Tid> &a, int q
     }
 }
 
-template <typename T, typename Tid, unsigned F>
+template <typename T, typename Tid, unsigned F, bool Coh = false>
 __device__ __forceinline__ void h_boundary_body(const StepArgs<T, Tid> &a, int q, int4 it) {
     const int i = it.x + threadIdx.x, j = it.y + threadIdx.y;
     if (i >= a.Nx || j >= a.Ny) return;
@@ -613,26 +624,26 @@ __device__ __forceinline__ void h_boundary_body(const StepArgs<T, Tid> &a, int q
                 }
             }
     }
-    T ex = __ldg(Ex + col + k0 * NxNy);
-    T ey = __ldg(Ey + col + k0 * NxNy);
+    T ex = ldf<Coh>(Ex + col + k0 * NxNy);
+    T ey = ldf<Coh>(Ey + col + k0 * NxNy);
 
     for (int k = k0; k < k1; ++k) {
         const long long id = col + k * NxNy;
         const int kp = (k == a.Nz - 1) ? 0 : k + 1;
-        const T ex_kp = __ldg(Ex + col + kp * NxNy), ey_kp = __ldg(Ey + col + kp * NxNy);
-        const T ez = __ldg(Ez + id);
-        T ez_jp = __ldg(Ez + coly + k * NxNy), ex_jp = __ldg(Ex + coly + k * NxNy);
-        T ez_ip = __ldg(Ez + colx + k * NxNy), ey_ip = __ldg(Ey + colx + k * NxNy);
+        const T ex_kp = ldf<Coh>(Ex + col + kp * NxNy), ey_kp = ldf<Coh>(Ey + col + kp * NxNy);
+        const T ez = ldf<Coh>(Ez + id);
+        T ez_jp = ldf<Coh>(Ez + coly + k * NxNy), ex_jp = ldf<Coh>(Ex + coly + k * NxNy);
+        T ez_ip = ldf<Coh>(Ez + colx + k * NxNy), ey_ip = ldf<Coh>(Ey + colx + k * NxNy);
         if constexpr ((F & kFMisc) != 0) {
             // oblique driver: E ghosts past the y = Ny-1 and x = Nx-1 edges (set after inject_E)
             if (a.bloch) {
                 if (j == a.Ny - 1) {
-                    ez_jp = bloch_ghost(a.bloch, ez_jp, __ldg(a.oEz + coly + k * NxNy), a.byr, a.byi);
-                    ex_jp = bloch_ghost(a.bloch, ex_jp, __ldg(a.oEx + coly + k * NxNy), a.byr, a.byi);
+                    ez_jp = bloch_ghost(a.bloch, ez_jp, ldf<Coh>(a.oEz + coly + k * NxNy), a.byr, a.byi);
+                    ex_jp = bloch_ghost(a.bloch, ex_jp, ldf<Coh>(a.oEx + coly + k * NxNy), a.byr, a.byi);
                 }
                 if (i == a.Nx - 1) {
-                    ez_ip = bloch_ghost(a.bloch, ez_ip, __ldg(a.oEz + colx + k * NxNy), a.bxr, a.bxi);
-                    ey_ip = bloch_ghost(a.bloch, ey_ip, __ldg(a.oEy + colx + k * NxNy), a.bxr, a.bxi);
+                    ez_ip = bloch_ghost(a.bloch, ez_ip, ldf<Coh>(a.oEz + colx + k * NxNy), a.bxr, a.bxi);
+                    ey_ip = bloch_ghost(a.bloch, ey_ip, ldf<Coh>(a.oEy + colx + k * NxNy), a.bxr, a.bxi);
                 }
             }
         }

@@ -2,6 +2,7 @@
 // so that every multiply and add rounds separately, in the reference's order.
 #include "kernels.hpp"
 #include "yee.cuh"
+#include "batch_persist.cuh"
 
 namespace aefdtd {
 void launch_e_group(const StepArgs<double, uint8_t> &a, const int4 *items, const WorkSplit &w, int g, cudaStream_t s) {
@@ -32,4 +33,12 @@ void launch_h_group_batch(const StepArgs<double, uint16_t> *args, int q, const i
                           cudaStream_t s) {
     launch_h_group_batch_impl(args, q, items, w, g, s);
 }
+cudaError_t launch_persist(const PersistArgs<double, uint8_t> &p, int grid, int ty, cudaStream_t s) {
+    return launch_persist_impl(p, grid, ty, s);
+}
+template <> int persist_capacity<double, uint8_t>(int ty) { return persist_capacity_impl<double, uint8_t>(ty); }
+cudaError_t launch_persist(const PersistArgs<double, uint16_t> &p, int grid, int ty, cudaStream_t s) {
+    return launch_persist_impl(p, grid, ty, s);
+}
+template <> int persist_capacity<double, uint16_t>(int ty) { return persist_capacity_impl<double, uint16_t>(ty); }
 }  // namespace aefdtd

@@ -314,12 +314,14 @@ def run(scene, nsteps=None, want_fields=True):
 class Batch:
     """Many simulations advanced together (include/aefdtd.h, aefdtd_batch_*):
     merged launches per work-item group over all members of an L2-sized
-    subset, one captured graph per subset and segment. Members are ordinary
+    subset, one captured graph per subset and segment; with persistent=True
+    each chunk of a subset is one persistent cooperative launch instead. Members are ordinary
     Simulations (normal, custom or oblique mode; a completion sensor, set
     before they join, ends them at their completion step); the batch keeps
     references to them while they are members."""
 
-    def __init__(self, l2_budget_bytes=0, tile_y=0, kchunk=0, use_graphs=True, device=0, graph_steps=0, lanes=0):
+    def __init__(self, l2_budget_bytes=0, tile_y=0, kchunk=0, use_graphs=True, device=0, graph_steps=0, lanes=0,
+                 persistent=False):
         self._lib = load()
         o = A.BatchOpts()
         o.abi_version = A.ABI_VERSION
@@ -329,6 +331,7 @@ class Batch:
         o.use_graphs = 0 if use_graphs else -1
         o.graph_steps = int(graph_steps)
         o.lanes = int(lanes)
+        o.persistent = 1 if persistent else 0
         self._h = C.c_void_p()
         st = self._lib.aefdtd_batch_create(C.byref(o), C.byref(self._h))
         if st != 0:
@@ -401,6 +404,7 @@ class Batch:
         self._c(self._lib.aefdtd_batch_get_info(self._h, C.byref(i)))
         k = min(i.n_classes, A.BATCH_MAX_CLASSES)
         return {"n_members": i.n_members, "n_active": i.n_active, "n_subsets": i.n_subsets, "n_lanes": i.n_lanes,
+                "n_persistent": i.n_persistent,
                 "cells": i.cells,
                 "member_bytes": i.member_bytes, "batch_bytes": i.batch_bytes,
                 "l2_budget_bytes": i.l2_budget_bytes, "launches": i.launches,

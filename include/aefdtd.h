@@ -447,6 +447,14 @@ aefdtd_status aefdtd_probe_copy_bandwidth(int32_t device, size_t bytes, int32_t 
  * returns AEFDTD_TIMEOUT. */
 #define AEFDTD_TEST_STAGED_WAIT_CYCLES 3
 #define AEFDTD_TEST_STAGED_WITHHOLD_COPY 4
+/* The same for the persistent batch launch (aefdtd_batch_opts.persistent),
+ * set on a member before its batch builds the member's subset: the bound of
+ * each wait on a neighbour's progress counter (default 2^31 cycles), and
+ * (value 1) a launch in which the subset's first unit never reports its
+ * progress, so that its neighbours' waits run out; every CTA then leaves at
+ * its next wait and the advance returns AEFDTD_TIMEOUT. */
+#define AEFDTD_TEST_PERSIST_WAIT_CYCLES 5
+#define AEFDTD_TEST_PERSIST_WITHHOLD 6
 aefdtd_status aefdtd_test_hook(aefdtd_sim *sim, int32_t what, int64_t value);
 
 /* ---- batches: many simulations advanced together ----------------------
@@ -472,12 +480,19 @@ typedef struct aefdtd_batch_opts {
     int32_t use_graphs;       /* < 0: no CUDA graphs (direct launches) */
     int32_t graph_steps;      /* steps per captured graph of a subset; 0 -> 32 */
     int32_t lanes;            /* subsets running concurrently (1..8); 0 -> 2 until autotuned */
-    int32_t reserved;
+    int32_t persistent;       /* 1: each subset's chunk of steps runs as ONE persistent cooperative launch
+                               * (CTAs own bands x z-chunks of the members and wait only on their
+                               * neighbours' progress counters, every wait bounded); 0: one launch per
+                               * work-item group and half-step; the autotuner times both. Subsets
+                               * holding an oblique member or a completion sensor always take the
+                               * split launches. FP64 fields are bit-identical either way; plane sums
+                               * are added per row band instead of per block (last bits differ). */
 } aefdtd_batch_opts;
 
 #define AEFDTD_BATCH_MAX_CLASSES 32
 typedef struct aefdtd_batch_info {
-    int32_t n_members, n_active, n_subsets, n_classes, n_lanes, reserved;
+    int32_t n_members, n_active, n_subsets, n_classes, n_lanes;
+    int32_t n_persistent;     /* subsets on the persistent launch */
     int64_t cells;            /* total cells of the active members */
     int64_t member_bytes;     /* device memory held by all members */
     int64_t batch_bytes;      /* device memory held by the batch itself (work lists, argument arrays) */

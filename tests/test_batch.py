@@ -116,10 +116,16 @@ def test_autotune_then_run_matches_alone():
         for c in info["classes"]:
             assert c["tile_y"] in (2, 4, 8) and c["kchunk"] in (4, 8)
         assert all(s.dims().step == 0 for s in sims)
-        assert b.run(10 ** 6) == steps
+        first = b.advance(64)
+        # the persistent launch adds the plane sums per row band (last bits differ)
+        persistent = b.info()["n_persistent"] > 0
+        assert first + b.run(10 ** 6) == steps
         for s, (f, p) in zip(sims, want):
             assert np.array_equal(s.fields(), f)
-            assert np.array_equal(s.plane_sums(), p)
+            if persistent:
+                assert rel(s.plane_sums(), p) < 1e-12
+            else:
+                assert np.array_equal(s.plane_sums(), p)
     for s in sims:
         s.close()
 
