@@ -20,10 +20,11 @@
 // These are also the only units that read the values the unit is about to
 // overwrite, in the half-step it waits for, so the same waits order the
 // overwrites. Each unit has a progress counter (half-steps finished in this
-// launch): the owning CTA's barrier, a fence and a release store publish it;
-// the waiting CTA's first thread acquires it, fences, and the CTA's barrier
-// passes that on to its other threads, whose loads of neighbour fields are
-// ordinary cached loads (yee.cuh, ldf<true>), never the read-only path.
+// launch): the owning CTA's barrier, then an acq_rel fence and a store by its
+// first thread publish it; the waiting CTA's first thread reads it with an
+// acquire load, and the CTA's barrier passes that on to its other threads,
+// whose loads of neighbour fields are ordinary cached loads (yee.cuh,
+// ldf<true>), never the read-only path.
 // Waits only ever look back one half-step and every CTA finishes a half-step
 // before starting the next, so with all CTAs resident (cooperative launch)
 // every wait ends. Each wait is still bounded: one that runs out raises the
@@ -46,8 +47,10 @@ __device__ __forceinline__ int ps_ld_acquire(const int *p) {
     asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
+// The release orders every store of the CTA before it: they precede it
+// through the CTA barrier (fence.acq_rel at gpu scope, then a relaxed store).
 __device__ __forceinline__ void ps_st_release(int *p, int v) {
-    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+    asm volatile("fence.acq_rel.gpu;\n\tst.relaxed.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
 // First thread of a CTA: until units a and b have both finished `need`
@@ -166,7 +169,6 @@ __global__ void __launch_bounds__(kPsMaxThreads, sizeof(T) == 8 ? 1 : 2)
                         *abort = 1;
                         atomicExch(P.flags, 1);
                     }
-                    __threadfence();
                     go = ok;
                 }
                 __syncthreads();
@@ -189,10 +191,7 @@ __global__ void __launch_bounds__(kPsMaxThreads, sizeof(T) == 8 ? 1 : 2)
                     for (int k = 0; k < U.h_n; ++k) ps_h_item<T, Tid>(a, q, P.items[U.h_off + k]);
                 }
                 __syncthreads();
-                if (lead && !(P.withhold && u == 0)) {
-                    __threadfence();
-                    ps_st_release(P.prog + u, h + 1);
-                }
+                if (lead && !(P.withhold && u == 0)) ps_st_release(P.prog + u, h + 1);
             }
         }
     }
