@@ -1278,13 +1278,15 @@ void aefdtd_sim::build_work() {
     // group of a (tile, plane) for the E and the H half-step
     // AEFDTD_MERGE_PZ=1: curl-only items run with the z-CPML items' kernels (one launch for both)
     const bool merge_pz = std::getenv("AEFDTD_MERGE_PZ") != nullptr;
+    // AEFDTD_MERGE_DISP=1: dispersive-only items run with the general kernels (one launch for both)
+    const bool merge_disp = std::getenv("AEFDTD_MERGE_DISP") != nullptr;
     auto group_e = [&](unsigned f) {
         if (all_boundary) return (int)kGroupAll;
         f = (f & ~kOSC) | ((f & kOSC) ? kMISC : 0);
         f = (f & ~kPY) | ((f & kPY) ? kPXY : 0);
         if (f == 0) return merge_pz ? (int)kGroupPmlZ : (int)kGroupInterior;
         if (f == kPZ) return (int)kGroupPmlZ;
-        if (f == kDISP) return (int)kGroupDisp;
+        if (f == kDISP) return merge_disp ? (int)kGroupAll : (int)kGroupDisp;
         if (f == kPXY || f == (kPXY | kPZ)) return (int)kGroupPmlXY;
         return (int)kGroupAll;
     };
