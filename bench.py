@@ -571,6 +571,23 @@ def profile_run(args):
     from aether_b200 import configs as CF
     from aether_b200 import fdtd
     prec = A.FP32 if args.profile == "fp32" else A.FP64
+    if args.profile_grid in ("batch", "batch-persistent"):
+        # 8 of the batch sample's nanodisk cells, one subset each, 64 steps in one chunk of
+        # direct launches (split groups, or one persistent launch per subset)
+        import numpy as np
+        rng = np.random.default_rng(2024)
+        scenes = [CF.metasurface_cell(rng, precision=prec, nsteps=8000, nl=101, flux_planes=False)
+                  for _ in range(8)]
+        sims = [fdtd.build_simulation(sc) for sc in scenes]
+        with fdtd.Batch(l2_budget_bytes=48 << 20, tile_y=4, kchunk=8, lanes=1, use_graphs=False,
+                        persistent=args.profile_grid == "batch-persistent") as b:
+            for s in sims:
+                b.add(s, STEPS_PER_BENCH_STEP * args.segments)
+            b.run(STEPS_PER_BENCH_STEP * args.segments)
+            log(f"profile run: batch of 8 cells, {args.profile}, {b.info()['launches']} launches")
+        for s in sims:
+            s.close()
+        return
     if args.profile_grid == "large":
         # the large grid's scene at 384 x 384 x 192 (CPML on six faces, spheres, oscillator)
         sc = CF.random_spheres_scene(n_total=(384, 384, 192), n_dielectric=60, n_lorentz=6, seed=1234,
@@ -598,8 +615,9 @@ def main():
     ap.add_argument("--no-accuracy", action="store_true", help="skip the FP32-vs-FP64 spectrum error runs")
     ap.add_argument("--profile", choices=["fp32", "fp64"], help="direct-launch run for ncu (no timing)")
     ap.add_argument("--segments", type=int, default=2)
-    ap.add_argument("--profile-grid", choices=["bench", "large"], default="bench",
-                    help="--profile on the bench grid or on the large grid's scene at 384 x 384 x 192")
+    ap.add_argument("--profile-grid", choices=["bench", "large", "batch", "batch-persistent"], default="bench",
+                    help="--profile on the bench grid, on the large grid's scene at 384 x 384 x 192, or on a "
+                         "batch of 8 nanodisk cells (split or persistent launches)")
     args = ap.parse_args()
     if args.profile:
         profile_run(args)
