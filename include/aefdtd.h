@@ -486,7 +486,9 @@ typedef struct aefdtd_batch_opts {
                                * work-item group and half-step; the autotuner times both. Subsets
                                * holding an oblique member or a completion sensor always take the
                                * split launches. FP64 fields are bit-identical either way; plane sums
-                               * are added per row band instead of per block (last bits differ). */
+                               * are added per row band instead of per block (last bits differ). A
+                               * wait that runs out makes the advance return AEFDTD_TIMEOUT and leaves
+                               * the members part-way through a chunk: reset them before reuse. */
 } aefdtd_batch_opts;
 
 #define AEFDTD_BATCH_MAX_CLASSES 32

@@ -149,3 +149,38 @@ def test_persistent_wait_runs_out_then_members_recover():
     finally:
         for s in sims:
             s.close()
+
+
+
+def test_fp64_persistent_16bit_material_ids():
+    """300 materials (16-bit ids) on the persistent launch: fields equal the run alone."""
+    sc = CF.random_spheres_scene(n_total=(70, 40, 44), dx=5 * NM, pml=6, n_dielectric=300, n_lorentz=2, seed=3,
+                                 r_range=(3 * NM, 8 * NM), nsteps=80, precision=A.FP64)
+    steps = 80
+    want = alone(sc, steps)
+    got, info = run_batch([sc], steps)
+    assert info["n_persistent"] == 1
+    assert np.array_equal(got[0][0], want[0])
+
+
+def test_fp64_oblique_member_keeps_split_launches():
+    """An oblique member (two coupled grids) keeps the split launches in its
+    own subset of a persistent batch; the normal-mode member beside it takes
+    the persistent launch. Both members' fields equal their runs alone."""
+    scenes = [cells(13, n=1)[0], CF.oblique_scene(nsteps=80)]
+    steps = 80
+    want = [alone(sc, steps)[0] for sc in scenes]
+    sims = [fdtd.build_simulation(sc) for sc in scenes]
+    try:
+        with fdtd.Batch(persistent=True) as b:
+            for s in sims:
+                b.add(s, steps)
+            first = b.advance(32)
+            info = b.info()
+            assert first + b.run(10 ** 6) == steps
+            assert info["n_subsets"] == 2 and info["n_persistent"] == 1
+            for s, w in zip(sims, want):
+                assert np.array_equal(s.fields(), w)
+    finally:
+        for s in sims:
+            s.close()
