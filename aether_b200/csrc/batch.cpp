@@ -125,7 +125,10 @@ struct aefdtd_batch {
     bool typed = false, fp64 = false;
     int id_bytes = 1, seg_len = 64;
     Lane lanes[kMaxLanes];
-    int n_lanes = 2;               // subsets running concurrently
+    int n_lanes = 2;               // most subsets running concurrently
+    // L2 bytes that the subsets running at once may hold together: a subset of
+    // b bytes shares the device with at most lane_window / b - 1 others of its class
+    long long lane_window = 96LL << 20;
     cudaStream_t stream = nullptr; // lanes[0].stream
     std::vector<BatchMember> members;
     std::vector<BatchSubset> subsets;
@@ -155,6 +158,21 @@ struct aefdtd_batch {
         subsets.clear();
         for (auto &m : members) m.placed = false;
         layout_dirty = true;
+    }
+    // lanes that the subsets of u's size class take in turn: as many as fit the
+    // window when subsets are sized for L2, all of them otherwise
+    int lanes_for(const BatchSubset &u) const {
+        if (l2_budget < 0) return n_lanes;
+        const long long b = std::max<long long>((long long)u.bytes, 1);
+        return (int)std::clamp<long long>(lane_window / b, 1, n_lanes);
+    }
+    // lane of every subset: within a size class the subsets go round-robin over
+    // lanes_for() lanes (subsets of one class are consecutive after a full layout)
+    std::vector<int> lane_plan() const {
+        std::vector<int> lane(subsets.size());
+        std::map<int, int> seen;
+        for (size_t k = 0; k < subsets.size(); k++) lane[k] = seen[subsets[k].cls]++ % lanes_for(subsets[k]);
+        return lane;
     }
     // subsets whose state stays in the 126 MB L2 between steps
     static bool l2_resident(const BatchSubset &u) { return u.bytes <= (96ull << 20); }
@@ -438,7 +456,7 @@ void aefdtd_batch::build_persist(BatchSubset &u, const std::vector<SensorStepArg
     if (cap == ps_capacity.end()) cap = ps_capacity.emplace(ty, persist_capacity<T, Tid>(ty)).first;
     if (cap->second <= 0) fail(AEFDTD_CUDA_ERROR, "the persistent batch kernel does not fit on the device");
     // the lanes share the device: each subset's launch takes its share of the resident CTAs
-    u.ps_grid = std::max(1, std::min(u.ps_nunits, cap->second / std::max(1, n_lanes)));
+    u.ps_grid = std::max(1, std::min(u.ps_nunits, cap->second / lanes_for(u)));
 }
 
 // The device error flag of the persistent launches: a wait that ran out
@@ -800,6 +818,7 @@ template <typename T, typename Tid> int aefdtd_batch::advance(int max_steps) {
     // subsets round-robin over the lanes; each subset's segments are queued
     // in turn (stream order within a lane, concurrency across lanes)
     std::vector<int> done(subsets.size(), 0);
+    const std::vector<int> lane = lane_plan();
     int most = 0;
     bool more = true;
     while (more) {
@@ -812,11 +831,11 @@ template <typename T, typename Tid> int aefdtd_batch::advance(int max_steps) {
             if (L <= 0) { done[k] = -done[k] - 1; continue; }
             std::vector<int> t0;
             for (aefdtd_sim *s : u.members) t0.push_back(s->tstep);
-            run_segment<T, Tid>(u, L, lanes[k % n_lanes]);
+            run_segment<T, Tid>(u, L, lanes[lane[k]]);
             for (size_t i = 0; i < u.members.size(); i++) {
                 aefdtd_sim *s = u.members[i];
                 if (s->cc_coeff > 0 && !s->cc_done &&
-                    batch_completion_check(s, t0[i], s->tstep, lanes[k % n_lanes].stream))
+                    batch_completion_check(s, t0[i], s->tstep, lanes[lane[k]].stream))
                     rec(s).remaining = 0;
             }
             done[k] += L;
@@ -837,13 +856,14 @@ template <typename T, typename Tid> int aefdtd_batch::advance(int max_steps) {
 // segment (which captures the graphs).
 template <typename T, typename Tid> double aefdtd_batch::time_segments(int reps) {
     update_layout();
-    for (size_t k = 0; k < subsets.size(); k++) run_segment<T, Tid>(subsets[k], seg_len, lanes[k % n_lanes]);
+    const std::vector<int> lane = lane_plan();
+    for (size_t k = 0; k < subsets.size(); k++) run_segment<T, Tid>(subsets[k], seg_len, lanes[lane[k]]);
     sync_lanes();
     check_persist();
     int a = 0, b = 0;   // host clock over all lanes (the device is idle before)
     const auto t0 = std::chrono::steady_clock::now();
     for (int r = 0; r < reps; r++)
-        for (size_t k = 0; k < subsets.size(); k++) run_segment<T, Tid>(subsets[k], seg_len, lanes[k % n_lanes]);
+        for (size_t k = 0; k < subsets.size(); k++) run_segment<T, Tid>(subsets[k], seg_len, lanes[lane[k]]);
     sync_lanes();
     check_persist();
     (void)a; (void)b;
@@ -1005,6 +1025,7 @@ aefdtd_status aefdtd_batch_create(const aefdtd_batch_opts *opts, aefdtd_batch **
         for (auto &ln : b->lanes) ln.create();
         b->stream = b->lanes[0].stream;
         if (b->opts.lanes > 0) b->n_lanes = std::min(b->opts.lanes, kMaxLanes);
+        if (const char *lw = std::getenv("AEFDTD_LANE_WINDOW_MIB")) b->lane_window = std::max(1LL, atoll(lw)) << 20;
         b->persistent = b->opts.persistent != 0;
         if (const char *ps = std::getenv("AEFDTD_BATCH_PERSIST")) b->persistent = atoi(ps) != 0;
     });

@@ -37,7 +37,8 @@ def rel(a, b):
 
 @pytest.mark.parametrize("opts", [dict(), dict(l2_budget_bytes=1), dict(l2_budget_bytes=-1),
                                   dict(tile_y=2, kchunk=16), dict(tile_y=8, kchunk=4), dict(use_graphs=False),
-                                  dict(graph_steps=7), dict(graph_steps=64), dict(l2_budget_bytes=1, lanes=3)])
+                                  dict(graph_steps=7), dict(graph_steps=64), dict(l2_budget_bytes=1, lanes=3),
+                                  dict(l2_budget_bytes=1, lanes=8)])
 def test_fp64_batch_members_bit_identical_to_alone(opts):
     scenes = cells(3)
     steps = 150
