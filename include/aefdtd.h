@@ -479,7 +479,9 @@ typedef struct aefdtd_batch_opts {
     int32_t kchunk;           /* planes per work item (0 -> each simulation's heuristic) until autotuned */
     int32_t use_graphs;       /* < 0: no CUDA graphs (direct launches) */
     int32_t graph_steps;      /* steps per captured graph of a subset; 0 -> 32 */
-    int32_t lanes;            /* subsets running concurrently (1..8); 0 -> 2 until autotuned */
+    int32_t lanes;            /* most subsets running concurrently (1..8); 0 -> 2 until autotuned. With
+                               * L2-sized subsets (l2_budget_bytes >= 0) a subset of b bytes runs beside
+                               * at most 96 MiB / b - 1 others, so that they stay in L2 together */
     int32_t persistent;       /* 1: each subset's chunk of steps runs as ONE persistent cooperative launch
                                * (CTAs own bands x z-chunks of the members and wait only on their
                                * neighbours' progress counters, every wait bounded); 0: one launch per
