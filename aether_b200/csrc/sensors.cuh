@@ -22,8 +22,6 @@
 
 namespace aefdtd {
 
-
-
 // Block b of the plane-sum partials of step q (scalars a.sc[q]) into part[b*12 + c].
 template <typename T>
 __device__ __forceinline__ void plane_partial(const SensorStepArgs<T> &a, int b, int q, double *part) {
