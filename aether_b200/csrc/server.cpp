@@ -255,16 +255,17 @@ aefdtd_status aefdtd_server_create(const aefdtd_server_opts *opts, aefdtd_server
         } else {
             v->opts.abi_version = AEFDTD_ABI_VERSION;
         }
-        // defaults measured on a Poisson stream of 32 unit-cell jobs, 10% large cells:
-        // 256 steps per poll and one merged subset per size class gave p50 5.2 s,
-        // p99 16.4 s, 36.5 Gcell/s, against 7.5 s, 19.6 s, 33.5 Gcell/s for 64 steps
-        // and 48 MiB subsets
+        // defaults measured on a Poisson stream of 32 unit-cell jobs, 10% large cells
+        // (the batch's L2-resident members without an up-front L2 prefetch, lanes
+        // sized by subset bytes): 256 steps per poll and the batch's L2-sized
+        // subsets (48 MiB) gave p50 1.6 s, p99 6.1 s, 45.6 Gcell/s, against 4.0 s,
+        // 13.3 s, 38.5 Gcell/s for one merged subset per size class and 3.0 s,
+        // 7.6 s, 44.0 Gcell/s for 64 steps per poll
         if (v->opts.segment_steps <= 0) v->opts.segment_steps = 256;
         if (v->opts.lookahead <= 0) v->opts.lookahead = 16;
         aefdtd_batch_opts bo = v->opts.batch;
         bo.abi_version = AEFDTD_ABI_VERSION;
         bo.device = v->opts.device;
-        if (bo.l2_budget_bytes == 0) bo.l2_budget_bytes = -1;
         aefdtd_status b = aefdtd_batch_create(&bo, &v->batch);
         if (b != AEFDTD_OK) fail(b, "batch creation failed");
         size_t fr = 0, tot = 0;

@@ -555,7 +555,8 @@ typedef struct aefdtd_server_opts {
     int32_t lookahead;        /* queued jobs that may pass one that does not fit; 0 -> 16 */
     int32_t reserved;
     aefdtd_batch_opts batch;  /* options of the batch (abi_version and device are set by the server;
-                                 l2_budget_bytes 0 -> no limit: one merged subset per size class) */
+                                 l2_budget_bytes as for a batch: 0 -> 48 MiB L2-sized subsets,
+                                 < 0 -> no limit: one merged subset per size class) */
 } aefdtd_server_opts;
 
 typedef struct aefdtd_job_desc {
