@@ -183,7 +183,7 @@ struct aefdtd_batch {
     void update_layout();
     template <typename T, typename Tid> void build_subset(BatchSubset &u);
     template <typename T, typename Tid>
-    void build_persist(BatchSubset &u, const std::vector<SensorStepArgs<T>> &sa);
+    bool build_persist(BatchSubset &u, const std::vector<SensorStepArgs<T>> &sa);
     void check_persist();
     template <typename T, typename Tid> void enqueue_steps(BatchSubset &u, int L, Lane &ln);
     template <typename T, typename Tid> void run_segment(BatchSubset &u, int L, Lane &ln);
@@ -363,7 +363,12 @@ template <typename T, typename Tid> void aefdtd_batch::build_subset(BatchSubset 
     u.nblk = (int)blk.size();
     u.blkmap.alloc(std::max<size_t>(blk.size(), 1) * sizeof(int2), dev_bytes);
     if (!blk.empty()) AE_CUDA(cudaMemcpy(u.blkmap.p, blk.data(), blk.size() * sizeof(int2), cudaMemcpyHostToDevice));
-    if (u.ps) build_persist<T, Tid>(u, sa);
+    // a subset whose lists do not cut into units keeps the split launches
+    if (u.ps && !build_persist<T, Tid>(u, sa)) {
+        u.ps_units.release(dev_bytes); u.ps_items.release(dev_bytes); u.ps_prog.release(dev_bytes);
+        u.ps_sargs.release(dev_bytes); u.ps_part.release(dev_bytes);
+        u.ps = false;
+    }
     u.built = true;
 }
 
@@ -371,15 +376,17 @@ template <typename T, typename Tid> void aefdtd_batch::build_subset(BatchSubset 
 // tile_y rows times a z-chunk of kchunk planes; each unit holds the member's
 // items of that band and chunk (every group, tagged with its group) and the
 // four units it waits on. Normal-mode members get their plane sums per band.
+// False (nothing launched) when the members' tile heights differ or an item
+// crosses a band or z-chunk.
 template <typename T, typename Tid>
-void aefdtd_batch::build_persist(BatchSubset &u, const std::vector<SensorStepArgs<T>> &sa) {
+bool aefdtd_batch::build_persist(BatchSubset &u, const std::vector<SensorStepArgs<T>> &sa) {
     const int ty = u.members[0]->tile_y;
     const size_t n = u.members.size();
     std::vector<size_t> part_off(n, 0);
     size_t part_n = 0;
     for (size_t li = 0; li < n; li++) {
         const aefdtd_sim *s = u.members[li];
-        if (s->tile_y != ty) fail(AEFDTD_BAD_ARG, "members of a subset share their tile height");
+        if (s->tile_y != ty) return false;
         if (sa[li].nbp > 0) {
             part_off[li] = part_n;
             part_n += size_t(seg_len) * ((s->Ny + ty - 1) / ty) * 12;
@@ -402,8 +409,7 @@ void aefdtd_batch::build_persist(BatchSubset &u, const std::vector<SensorStepArg
                     const int *it = &s->items_host[size_t(w.off[g] + k) * 4];
                     const int x0 = it[0], y0 = it[1], k0 = it[2], k1 = it[3];
                     const int b = y0 / ty, c = k0 / kc;
-                    if ((x0 & kHalfItem) || y0 % ty || k1 <= k0 || (k1 - 1) / kc != c)
-                        fail(AEFDTD_BAD_ARG, "a work item does not fit the persistent units");
+                    if ((x0 & kHalfItem) || y0 % ty || k1 <= k0 || (k1 - 1) / kc != c) return false;
                     dst[size_t(c) * nb + b].push_back(make_int4(x0, y0, k0 | (k1 << 16), g));
                 }
         }
@@ -457,6 +463,7 @@ void aefdtd_batch::build_persist(BatchSubset &u, const std::vector<SensorStepArg
     if (cap->second <= 0) fail(AEFDTD_CUDA_ERROR, "the persistent batch kernel does not fit on the device");
     // the lanes share the device: each subset's launch takes its share of the resident CTAs
     u.ps_grid = std::max(1, std::min(u.ps_nunits, cap->second / lanes_for(u)));
+    return true;
 }
 
 // The device error flag of the persistent launches: a wait that ran out
